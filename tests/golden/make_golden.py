@@ -1,0 +1,133 @@
+"""Generate the golden fixtures in tests/golden/ by RUNNING THE REFERENCE.
+
+Needs the reference compiled from its own sources (``make -C oracle ref``,
+which reads the reference tree). Inputs come from tests/golden/gen.py (exact
+integer-derived floats), outputs come from the reference's own code:
+  * oracle/_ref/libe8qref.so  - BranchLevels, FixedScale, EncodeVectorAtScale,
+    BuildRefineTables, PackCoarseRow/PackRefineBlock, FhtKac4Rotator
+  * oracle/_ref/e8qlib_ref    - the reference's pybind11 module: E8qIndex
+    build / save (E8AX, parsed for codes, g1, h3, ids) / plain search
+    (set_disable_prune(True)) / estimate.
+
+Usage: python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, HERE)
+
+import oracle as O  # noqa: E402
+from gen import det_mixture, det_normal, det_unit  # noqa: E402
+
+ROT_CASES = [(64, 0), (100, 1), (128, 7), (768, 3), (960, 5)]
+ENC_DIMS = [64, 128, 960]
+ENC_ROWS = {64: 96, 128: 64, 960: 24}
+# (name, dim, bits, n, nlist, seed, sigma, nq, k, nprobe)
+INDEX_CASES = [
+    ("d96_b4", 96, 4, 1500, 8, 11, 0.5, 20, 10, 3),
+    ("d100_b1", 100, 1, 800, 4, 12, 0.5, 12, 10, 2),
+    ("d128_b9", 128, 9, 600, 4, 13, 0.5, 12, 16, 4),
+    ("d960_b6", 960, 6, 300, 4, 14, 0.4, 8, 10, 2),
+    ("d64_b2_k128", 64, 2, 700, 5, 15, 0.5, 6, 128, 5),
+]
+
+
+def main() -> None:
+    R = O.ref_lib()
+    E = O.ref_module()
+    if R is None or E is None:
+        raise SystemExit("build the reference first: make -C oracle ref")
+
+    # ---- levels, scales, refine tables --------------------------------
+    lv = {}
+    for b in range(1, 14):
+        for br in (0, 1):
+            a = np.zeros(1 << b, np.float64)
+            R.ref_branch_levels(b, br, a)
+            lv[f"sha_b{b}_br{br}"] = np.frombuffer(hashlib.sha256(a.tobytes()).digest(), np.uint8)
+            if b <= 8:
+                lv[f"lev_b{b}_br{br}"] = a
+        lv[f"scale_b{b}"] = np.float64(R.ref_fixed_scale(b))
+        t = np.zeros(2 * max(256, 1 << b), np.float32)
+        R.ref_refine_tables(b, 960, t)
+        lv[f"sha_tab_b{b}_pd960"] = np.frombuffer(hashlib.sha256(t.tobytes()).digest(), np.uint8)
+        w = np.zeros(2, np.float64)
+        R.ref_scan_class_means(b, w)
+        lv[f"wcls_b{b}"] = w
+    np.savez_compressed(os.path.join(HERE, "levels.npz"), **lv)
+
+    # ---- rotator -------------------------------------------------------
+    rot = {}
+    for dim, seed in ROT_CASES:
+        nb = R.ref_rotator_sign_bytes(dim, seed)
+        s = np.zeros(nb, np.uint8)
+        R.ref_rotator_signs(dim, seed, s)
+        x = det_normal(100 + dim + seed, (4, dim))
+        y = np.zeros((4, O.padded_dim(dim)), np.float32)
+        R.ref_rotate(dim, seed, x, 4, y)
+        rot[f"signs_{dim}_{seed}"] = s
+        rot[f"rot_{dim}_{seed}"] = y
+    np.savez_compressed(os.path.join(HERE, "rotator.npz"), **rot)
+
+    # ---- encoder -------------------------------------------------------
+    enc = {}
+    for pd in ENC_DIMS:
+        u = det_unit(200 + pd, ENC_ROWS[pd], pd)
+        for b in range(1, 14):
+            dg, br = O.ref_encode(u, b)
+            enc[f"digits_{pd}_b{b}"] = dg
+            enc[f"branch_{pd}_b{b}"] = br
+    # packed blocks (reference on-disk layout) for the first rows at pd=64
+    for b in range(1, 14):
+        dg = enc[f"digits_64_b{b}"].reshape(-1, 8)[:64]
+        brs = enc[f"branch_64_b{b}"].reshape(-1)[:64]
+        rowa = np.zeros(64, np.uint8)
+        refine = np.zeros((64, 16), np.uint8)
+        for i in range(64):
+            ra = np.zeros(1, np.uint8)
+            rf = np.zeros(16, np.uint8)
+            R.ref_pack_block(np.ascontiguousarray(dg[i]), int(brs[i]), b, ra, rf)
+            rowa[i] = ra[0]
+            refine[i] = rf
+        enc[f"rowa_b{b}"] = rowa
+        enc[f"refine_b{b}"] = refine
+    np.savez_compressed(os.path.join(HERE, "encode.npz"), **enc)
+
+    # ---- whole indexes -------------------------------------------------
+    for name, dim, bits, n, nlist, seed, sigma, nq, k, nprobe in INDEX_CASES:
+        x, cm, lab = det_mixture(seed, n, dim, nlist, sigma)
+        q = det_mixture(seed + 1000, nq, dim, nlist, sigma)[0]
+        idx = E.E8qIndex(dim, bits, seed)
+        idx.build(x, cm, lab, num_threads=4)
+        idx.set_disable_prune(True)
+        with tempfile.TemporaryDirectory() as d:
+            p = os.path.join(d, "i.e8ax")
+            idx.save(p)
+            P = O.parse_e8ax(p)
+        ids, dists = idx.search(q, k, nprobe, 1)
+        est_ids = ids[:, :3].astype(np.uint32)
+        est = np.array([[idx.estimate(q[i], int(g)) if g != 0xFFFFFFFF else np.nan
+                         for g in est_ids[i]] for i in range(nq)], np.float32)
+        np.savez_compressed(
+            os.path.join(HERE, f"index_{name}.npz"),
+            params=np.array([dim, bits, n, nlist, seed, nq, k, nprobe], np.int64),
+            sigma=np.float64(sigma),
+            ids=P["ids"], mean_rot=P["mean_rot"], centroid_rot=P["centroid_rot"], cn2=P["cn2"],
+            list_begin=P["list_begin"], digits=P["digits"], branch=P["branch"], g1=P["g1"],
+            h3=P["h3"], rowa=P["rowa"], refine=P["refine"], signs=P["signs"],
+            search_ids=ids, search_dists=dists, est_ids=est_ids, est=est,
+            memory_bytes=np.int64(idx.memory_bytes))
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()
