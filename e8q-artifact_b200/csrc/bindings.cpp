@@ -1,0 +1,304 @@
+// pybind11 module `_e8qlib`: the reference's Python API (E8qIndex) over the
+// C ABI of libe8qcuda.so.
+//
+// Same class, argument names, defaults, dtypes, shapes, padding values and
+// exception types as python_bindings/e8q_bindings.cpp:22-344 of the
+// reference: inputs are force-cast to C-contiguous float32 / uint32,
+// std::invalid_argument -> ValueError, std::runtime_error -> RuntimeError.
+// `num_threads` is accepted and ignored (the work runs on the GPU).
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+#include <pybind11/stl.h>
+
+#include <cstdint>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "e8qc.h"
+
+namespace py = pybind11;
+
+namespace e8qb200 {
+
+template <typename T>
+py::array_t<T, py::array::c_style | py::array::forcecast> ensure_nd(py::handle v, const char* name,
+                                                                    int nd) {
+    auto a = py::array_t<T, py::array::c_style | py::array::forcecast>::ensure(v);
+    if (!a) throw std::invalid_argument(std::string(name) + " must be a NumPy array");
+    if (a.ndim() != nd)
+        throw std::invalid_argument(std::string(name) + (nd == 2 ? " must be a 2D NumPy array"
+                                                                 : " must be a 1D NumPy array"));
+    return a;
+}
+
+// Status code -> the exception type the reference raises for that condition.
+void check(int rc) {
+    if (rc == E8QC_OK) return;
+    const std::string msg = e8qc_last_error();
+    switch (rc) {
+        case E8QC_EINVAL:
+        case E8QC_ERANGE: throw std::invalid_argument(msg);
+        case E8QC_ENOMEM: throw std::runtime_error("out of memory: " + msg);
+        default: throw std::runtime_error(msg);
+    }
+}
+
+int mode_of(const std::string& m) {
+    if (m == "plain") return E8QC_MODE_PLAIN;
+    if (m == "batched") return E8QC_MODE_BATCHED;
+    throw std::invalid_argument("mode must be 'plain' or 'batched'");
+}
+
+class E8qIndex {
+   public:
+    E8qIndex(size_t dim, size_t nbits, uint64_t seed, int device)
+        : dim_(dim), nbits_(nbits), seed_(seed), device_(device) {
+        if (dim == 0) throw std::invalid_argument("dim must be positive");
+        if (nbits < 1 || nbits > 13) throw std::invalid_argument("nbits must be in [1, 13]");
+    }
+    ~E8qIndex() {
+        if (idx_) e8qc_e8q_destroy(idx_);
+    }
+    E8qIndex(const E8qIndex&) = delete;
+    E8qIndex& operator=(const E8qIndex&) = delete;
+
+    void build(py::handle data, py::handle centroids, py::handle cluster_ids, size_t /*num_threads*/,
+               float prune_alpha) {
+        auto x = ensure_nd<float>(data, "data", 2);
+        auto c = ensure_nd<float>(centroids, "centroids", 2);
+        auto ids = ensure_nd<uint32_t>(cluster_ids, "cluster_ids", 1);
+        if (static_cast<size_t>(x.shape(1)) != dim_)
+            throw std::invalid_argument("data dimension does not match index dim");
+        if (static_cast<size_t>(c.shape(1)) != dim_)
+            throw std::invalid_argument("centroid dimension does not match index dim");
+        if (ids.shape(0) != x.shape(0))
+            throw std::invalid_argument("cluster_ids length must match number of rows in data");
+        fresh();
+        py::gil_scoped_release nogil;
+        check(e8qc_e8q_build(idx_, x.data(), static_cast<size_t>(x.shape(0)), c.data(),
+                             static_cast<size_t>(c.shape(0)), ids.data(), prune_alpha, nullptr));
+        built_ = true;
+    }
+
+    // Device-resident build: raw CUDA pointers (e.g. torch tensor data_ptr()).
+    void build_ptr(uintptr_t data, size_t n, uintptr_t centroids, size_t nlist, uintptr_t cluster_ids,
+                   float prune_alpha, uintptr_t stream) {
+        fresh();
+        py::gil_scoped_release nogil;
+        check(e8qc_e8q_build(idx_, reinterpret_cast<const float*>(data), n,
+                             reinterpret_cast<const float*>(centroids), nlist,
+                             reinterpret_cast<const uint32_t*>(cluster_ids), prune_alpha,
+                             reinterpret_cast<void*>(stream)));
+        built_ = true;
+    }
+
+    py::tuple search(py::handle queries, size_t k, size_t nprobe, size_t /*num_threads*/,
+                     bool return_stats, const std::string& mode) {
+        auto q = ensure_nd<float>(queries, "queries", 2);
+        require("search");
+        if (static_cast<size_t>(q.shape(1)) != dim_)
+            throw std::invalid_argument("query dimension does not match index dim");
+        if (k == 0) throw std::invalid_argument("k must be positive");
+        if (k > E8QC_MAX_K) throw std::invalid_argument("k must be <= " + std::to_string(E8QC_MAX_K));
+        if (nprobe == 0) throw std::invalid_argument("nprobe must be positive");
+        const int md = mode_of(mode);
+        const size_t nq = static_cast<size_t>(q.shape(0));
+        py::array_t<uint32_t> ids({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k)});
+        py::array_t<float> dists({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k)});
+        uint32_t* ip = ids.mutable_data();
+        float* dp = dists.mutable_data();
+        std::fill(ip, ip + nq * k, std::numeric_limits<uint32_t>::max());
+        std::fill(dp, dp + nq * k, std::numeric_limits<float>::infinity());
+        e8qc_stats st{};
+        {
+            py::gil_scoped_release nogil;
+            if (nq > 0) check(e8qc_e8q_search(idx_, q.data(), nq, k, nprobe, md, ip, dp,
+                                              return_stats ? &st : nullptr, nullptr));
+        }
+        if (!return_stats) return py::make_tuple(ids, dists);
+        return py::make_tuple(ids, dists, stats_dict(st, nq, nprobe));
+    }
+
+    // Device-resident search on raw CUDA pointers; returns the launch count.
+    uint64_t search_ptr(uintptr_t queries, size_t nq, size_t k, size_t nprobe, uintptr_t out_ids,
+                        uintptr_t out_dists, const std::string& mode, uintptr_t stream) {
+        require("search");
+        const int md = mode_of(mode);
+        e8qc_stats st{};
+        py::gil_scoped_release nogil;
+        check(e8qc_e8q_search(idx_, reinterpret_cast<const float*>(queries), nq, k, nprobe, md,
+                              reinterpret_cast<uint32_t*>(out_ids), reinterpret_cast<float*>(out_dists), &st,
+                              reinterpret_cast<void*>(stream)));
+        return st.launches;
+    }
+
+    // Serving form: per-query k and nprobe; rows padded to k_max.
+    py::tuple search_ragged(py::handle queries, py::handle k, py::handle nprobe, size_t k_max) {
+        auto q = ensure_nd<float>(queries, "queries", 2);
+        auto ka = ensure_nd<uint32_t>(k, "k", 1);
+        auto na = ensure_nd<uint32_t>(nprobe, "nprobe", 1);
+        require("search");
+        if (static_cast<size_t>(q.shape(1)) != dim_)
+            throw std::invalid_argument("query dimension does not match index dim");
+        const size_t nq = static_cast<size_t>(q.shape(0));
+        if (static_cast<size_t>(ka.shape(0)) != nq || static_cast<size_t>(na.shape(0)) != nq)
+            throw std::invalid_argument("k and nprobe must have one entry per query");
+        py::array_t<uint32_t> ids({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k_max)});
+        py::array_t<float> dists({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k_max)});
+        {
+            py::gil_scoped_release nogil;
+            if (nq > 0)
+                check(e8qc_e8q_search_ragged(idx_, q.data(), nq, ka.data(), na.data(), k_max,
+                                             ids.mutable_data(), dists.mutable_data(), nullptr, nullptr));
+        }
+        return py::make_tuple(ids, dists);
+    }
+
+    float estimate(py::handle query, uint32_t id) {
+        require("estimate");
+        auto q = ensure_nd<float>(query, "query", 1);
+        if (static_cast<size_t>(q.shape(0)) != dim_)
+            throw std::invalid_argument("query dimension does not match index dim");
+        float out = 0.0f;
+        check(e8qc_e8q_estimate(idx_, q.data(), id, &out));
+        return out;
+    }
+
+    void set_disable_prune(bool on) {
+        require("set_disable_prune");
+        check(e8qc_e8q_set_disable_prune(idx_, on ? 1 : 0));
+    }
+    void set_prune_alpha(float alpha) {
+        require("set_prune_alpha");
+        check(e8qc_e8q_set_prune_alpha(idx_, alpha));
+    }
+
+    py::tuple export_codes() {
+        require("export_codes");
+        const e8qc_info in = info();
+        const size_t n = in.n, B = in.padded_dim / 8;
+        py::array_t<uint32_t> ids(static_cast<py::ssize_t>(n));
+        py::array_t<uint16_t> dg({static_cast<py::ssize_t>(n), static_cast<py::ssize_t>(B), py::ssize_t(8)});
+        py::array_t<uint8_t> br({static_cast<py::ssize_t>(n), static_cast<py::ssize_t>(B)});
+        py::array_t<float> g1(static_cast<py::ssize_t>(n)), h3(static_cast<py::ssize_t>(n));
+        check(e8qc_e8q_get_ids(idx_, ids.mutable_data()));
+        check(e8qc_e8q_export_codes(idx_, dg.mutable_data(), br.mutable_data(), g1.mutable_data(),
+                                    h3.mutable_data()));
+        return py::make_tuple(ids, dg, br, g1, h3);
+    }
+
+    size_t dim() const { return dim_; }
+    size_t nbits() const { return nbits_; }
+    bool is_built() const { return built_; }
+    size_t n() const { return built_ ? info().n : 0; }
+    size_t num_clusters() const { return built_ ? info().nlist : 0; }
+    size_t memory_bytes() const { return built_ ? info().memory_bytes : 0; }
+    bool disable_prune() const { return built_ ? info().disable_prune != 0 : false; }
+    int device() const { return device_; }
+
+   private:
+    void fresh() {
+        if (idx_) e8qc_e8q_destroy(idx_);
+        idx_ = nullptr;
+        built_ = false;
+        check(e8qc_e8q_create(device_, dim_, static_cast<int>(nbits_), seed_, &idx_));
+    }
+    void require(const char* what) const {
+        if (!built_ || idx_ == nullptr)
+            throw std::runtime_error(std::string("E8qIndex must be built or loaded before ") + what);
+    }
+    e8qc_info info() const {
+        e8qc_info in{};
+        check(e8qc_e8q_info(idx_, &in));
+        return in;
+    }
+    py::dict stats_dict(const e8qc_stats& st, size_t nq, size_t nprobe) const {
+        (void)nprobe;
+        py::dict d;
+        d["candidates"] = st.candidates;
+        d["survivors"] = st.survivors;
+        d["rotate_us"] = st.rotate_us / static_cast<double>(nq);
+        d["route_us"] = st.route_us / static_cast<double>(nq);
+        d["scan_us"] = st.scan_us / static_cast<double>(nq);
+        d["refine_us"] = st.refine_us / static_cast<double>(nq);
+        d["survivor_rate"] = st.candidates > 0 ? static_cast<double>(st.survivors) / st.candidates : 0.0;
+        d["launches"] = st.launches;
+        return d;
+    }
+
+    size_t dim_ = 0, nbits_ = 0;
+    uint64_t seed_ = 0;
+    int device_ = 0;
+    bool built_ = false;
+    e8qc_index* idx_ = nullptr;
+};
+
+}  // namespace e8qb200
+
+PYBIND11_MODULE(_e8qlib, m) {
+    using e8qb200::E8qIndex;
+    m.doc() = "E8Q IVF search on B200 (sm_100a): the e8qlib Python API over libe8qcuda.so";
+    m.def("version", [] { return e8qc_version(); });
+    m.def("branch_levels", [](int bits, int branch) {
+        py::array_t<double> out(static_cast<py::ssize_t>(1) << std::max(1, std::min(bits, 13)));
+        e8qb200::check(e8qc_branch_levels(bits, branch, out.mutable_data()));
+        return out;
+    }, py::arg("bits"), py::arg("branch"));
+    m.def("fixed_scale", [](int bits) {
+        double s = 0.0;
+        e8qb200::check(e8qc_fixed_scale(bits, &s));
+        return s;
+    }, py::arg("bits"));
+    m.def("encode", [](py::handle unit, int bits, int device) {
+        auto u = e8qb200::ensure_nd<float>(unit, "unit", 2);
+        const size_t n = static_cast<size_t>(u.shape(0)), pd = static_cast<size_t>(u.shape(1));
+        py::array_t<uint16_t> dg({static_cast<py::ssize_t>(n), static_cast<py::ssize_t>(pd / 8), py::ssize_t(8)});
+        py::array_t<uint8_t> br({static_cast<py::ssize_t>(n), static_cast<py::ssize_t>(pd / 8)});
+        {
+            py::gil_scoped_release nogil;
+            e8qb200::check(e8qc_encode(device, bits, u.data(), n, pd, dg.mutable_data(), br.mutable_data(), nullptr));
+        }
+        return py::make_tuple(dg, br);
+    }, py::arg("unit"), py::arg("bits"), py::arg("device") = 0);
+    m.def("rotate", [](py::handle x, size_t dim, uint64_t seed, int device) {
+        auto a = e8qb200::ensure_nd<float>(x, "x", 2);
+        if (static_cast<size_t>(a.shape(1)) != dim) throw std::invalid_argument("x dimension does not match dim");
+        const size_t n = static_cast<size_t>(a.shape(0)), pd = (dim + 63) / 64 * 64;
+        py::array_t<float> out({static_cast<py::ssize_t>(n), static_cast<py::ssize_t>(pd)});
+        {
+            py::gil_scoped_release nogil;
+            e8qb200::check(e8qc_rotate(device, dim, seed, a.data(), n, out.mutable_data(), nullptr));
+        }
+        return out;
+    }, py::arg("x"), py::arg("dim"), py::arg("seed"), py::arg("device") = 0);
+
+    py::class_<E8qIndex>(m, "E8qIndex")
+        .def(py::init<size_t, size_t, uint64_t, int>(), py::arg("dim"), py::arg("nbits"),
+             py::arg("seed") = 0, py::arg("device") = 0)
+        .def("build", &E8qIndex::build, py::arg("data"), py::arg("centroids"), py::arg("cluster_ids"),
+             py::arg("num_threads") = 1, py::arg("prune_alpha") = 0.0F)
+        .def("build_ptr", &E8qIndex::build_ptr, py::arg("data"), py::arg("n"), py::arg("centroids"),
+             py::arg("nlist"), py::arg("cluster_ids"), py::arg("prune_alpha") = 0.0F,
+             py::arg("stream") = 0)
+        .def("search", &E8qIndex::search, py::arg("queries"), py::arg("k"), py::arg("nprobe"),
+             py::arg("num_threads") = 1, py::arg("return_stats") = false, py::arg("mode") = "plain")
+        .def("search_ptr", &E8qIndex::search_ptr, py::arg("queries"), py::arg("nq"), py::arg("k"),
+             py::arg("nprobe"), py::arg("out_ids"), py::arg("out_dists"), py::arg("mode") = "plain",
+             py::arg("stream") = 0)
+        .def("search_ragged", &E8qIndex::search_ragged, py::arg("queries"), py::arg("k"),
+             py::arg("nprobe"), py::arg("k_max"))
+        .def("estimate", &E8qIndex::estimate, py::arg("query"), py::arg("id"))
+        .def("set_disable_prune", &E8qIndex::set_disable_prune, py::arg("on"))
+        .def("set_prune_alpha", &E8qIndex::set_prune_alpha, py::arg("alpha"))
+        .def("export_codes", &E8qIndex::export_codes)
+        .def_property_readonly("dim", &E8qIndex::dim)
+        .def_property_readonly("nbits", &E8qIndex::nbits)
+        .def_property_readonly("is_built", &E8qIndex::is_built)
+        .def_property_readonly("n", &E8qIndex::n)
+        .def_property_readonly("num_clusters", &E8qIndex::num_clusters)
+        .def_property_readonly("memory_bytes", &E8qIndex::memory_bytes)
+        .def_property_readonly("disable_prune", &E8qIndex::disable_prune)
+        .def_property_readonly("device", &E8qIndex::device);
+}

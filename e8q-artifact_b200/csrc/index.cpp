@@ -1,0 +1,609 @@
+// C ABI of libe8qcuda.so (include/e8qc.h): the E8Q index object, its device
+// memory, the build orchestration and the search/estimate entry points.
+//
+// Mirrors the reference's E8qIndex (include/e8qlib/index/e8q.hpp:121-187,
+// python_bindings/e8q_bindings.cpp) with the data held in HBM and every
+// per-vector step run by the kernels in search_kernels.cu / build_kernels.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <mutex>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "e8qc.h"
+#include "internal.h"
+#include "workspace.h"
+
+namespace e8qc {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void fail(int code, const std::string& msg) { throw Error{code, msg}; }
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        const int code = (e == cudaErrorMemoryAllocation) ? E8QC_ENOMEM : E8QC_ECUDA;
+        fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+void set_last_error(const std::string& s) { g_last_error = s; }
+const char* last_error() { return g_last_error.c_str(); }
+
+bool is_device_ptr(const void* p) {
+    if (p == nullptr) return false;
+    cudaPointerAttributes a{};
+    const cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+std::vector<uint8_t> rotator_signs(size_t dim, uint64_t seed) {
+    // FhtKac4Rotator(dim, seed) (src/utils/rotator.cpp:13-28): one byte per
+    // draw of mt19937_64; a uniform [0, 255] draw from a full 64-bit engine
+    // is its top byte (multiply-shift reduction, no rejection for 256).
+    const size_t pd = (dim + 63) / 64 * 64;
+    std::vector<uint8_t> s(4 * pd / 8);
+    std::mt19937_64 gen(seed);
+    for (auto& b : s) b = static_cast<uint8_t>(gen() >> 56);
+    return s;
+}
+
+// Input staging: device pointers pass through, host data is copied to a
+// temporary device buffer on the call's stream.
+template <class T>
+const T* stage_in(const T* p, size_t count, DevBuf& tmp, cudaStream_t s) {
+    if (count == 0 || is_device_ptr(p)) return p;
+    tmp.alloc(count * sizeof(T));
+    E8QC_CUDA(cudaMemcpyAsync(tmp.p, p, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    return static_cast<const T*>(tmp.p);
+}
+
+}  // namespace e8qc
+
+using namespace e8qc;
+
+struct e8qc_index {
+    int device = 0;
+    size_t dim = 0, pd = 0;
+    int bits = 0;
+    uint64_t seed = 0;
+    bool built = false;
+    bool disable_prune = false;
+    float prune_alpha = 1.0f;
+    size_t n = 0, nlist = 0, ntiles = 0;
+    int nch = 0, B = 0;
+    std::mutex mu;
+
+    std::vector<uint64_t> list_begin;  // nlist+1 compact offsets
+    std::vector<uint32_t> tile_begin;  // nlist+1
+    std::vector<uint32_t> ids_compact; // n
+    std::vector<uint32_t> inv_pos;     // global id -> compact position (lazy)
+    std::vector<uint32_t> sorted_tiles_prefix;  // prefix of list tile counts, largest first
+
+    DevBuf signs, mean_rot, cen, cn2, tile_begin_d, list_len_d, codes, g1, h3, ids, tab,
+        list_of_tile, list_begin_d;
+    DevIndex view{};
+    Workspace ws;
+
+    size_t memory_bytes() const {
+        return signs.bytes + mean_rot.bytes + cen.bytes + cn2.bytes + tile_begin_d.bytes +
+               list_len_d.bytes + codes.bytes + g1.bytes + h3.bytes + ids.bytes + tab.bytes +
+               list_of_tile.bytes + list_begin_d.bytes;
+    }
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = 0;
+    explicit DeviceGuard(int d) {
+        E8QC_CUDA(cudaGetDevice(&prev));
+        if (prev != d) E8QC_CUDA(cudaSetDevice(d));
+    }
+    ~DeviceGuard() { cudaSetDevice(prev); }
+};
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return E8QC_OK;
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return E8QC_ENOMEM;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return E8QC_EINVAL;
+    }
+}
+
+void require_built(const e8qc_index* x, const char* what) {
+    if (x == nullptr) fail(E8QC_EINVAL, "null index");
+    if (!x->built) fail(E8QC_ESTATE, std::string("E8qIndex must be built or loaded before ") + what);
+}
+
+// Upper bound of the tiles any nprobe lists can hold (sum of the largest).
+size_t max_tiles_for(const e8qc_index* x, size_t nprobe) {
+    const size_t p = std::min(nprobe, x->nlist);
+    return x->sorted_tiles_prefix[p];
+}
+
+void plain_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size_t nprobe,
+                  uint32_t* ids_d, float* d_d, e8qc_stats* st, cudaStream_t s) {
+    Workspace& ws = x->ws;
+    ws.ensure_route(x->nlist);
+    const int grid = plain_scan_grid(x->bits);
+    ws.ensure_scan(static_cast<size_t>(grid));
+    RouteWork rw{ws.keys.as<uint64_t>(), ws.probes.as<uint32_t>(), ws.probe_d2.as<float>(),
+                 ws.tile_off.as<uint32_t>(), ws.route_counter.as<uint32_t>(),
+                 ws.total_tiles.as<uint32_t>()};
+    ScanWork sw{ws.part_d.as<float>(), ws.part_id.as<uint32_t>(), ws.scan_counter.as<uint32_t>(), grid};
+    uint64_t launches = 0;
+    for (size_t i = 0; i < nq; ++i) {
+        const float* rq = rq_all + i * x->pd;
+        launches += launch_route_one(x->view, rq, static_cast<int>(nprobe), rw, s);
+        launches += launch_scan_plain(x->view, rq, rw, static_cast<int>(k), sw, ids_d + i * k,
+                                      d_d + i * k, s);
+    }
+    if (st) {
+        st->launches += launches;
+        uint64_t cand = 0;
+        (void)cand;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* e8qc_last_error(void) { return last_error(); }
+int e8qc_version(void) { return 10000; }
+
+int e8qc_branch_levels(int bits, int branch, double* out) {
+    return guarded([&] {
+        if (bits < 1 || bits > kMaxBits) fail(E8QC_EINVAL, "bits must be in [1, 13]");
+        if (branch != 0 && branch != 1) fail(E8QC_EINVAL, "branch must be 0 or 1");
+        if (out == nullptr) fail(E8QC_EINVAL, "null output");
+        const std::vector<double> l = branch_levels(bits, branch);
+        std::memcpy(out, l.data(), l.size() * sizeof(double));
+    });
+}
+
+int e8qc_fixed_scale(int bits, double* out) {
+    return guarded([&] {
+        if (out == nullptr) fail(E8QC_EINVAL, "null output");
+        *out = fixed_scale(bits);
+    });
+}
+
+int e8qc_encode(int device, int bits, const float* unit, size_t n, size_t padded_dim,
+                uint16_t* digits, uint8_t* branch, void* stream) {
+    return guarded([&] {
+        if (bits < 1 || bits > kMaxBits) fail(E8QC_EINVAL, "EncodeVectorAtScale: bits must be in [1, 13]");
+        if (padded_dim == 0 || padded_dim % 8 != 0) fail(E8QC_EINVAL, "padded_dim must be a positive multiple of 8");
+        if (n == 0) return;
+        if (!unit || !digits || !branch) fail(E8QC_EINVAL, "null buffer");
+        DeviceGuard g(device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const DevEncTables& et = enc_tables_device(device, bits);
+        const size_t B = padded_dim / 8;
+        DevBuf tu, td, tb;
+        const float* ud = stage_in(unit, n * padded_dim, tu, s);
+        const bool dd = is_device_ptr(digits), bd = is_device_ptr(branch);
+        uint16_t* dg = digits;
+        uint8_t* br = branch;
+        if (!dd) { td.alloc(n * B * 8 * sizeof(uint16_t)); dg = td.as<uint16_t>(); }
+        if (!bd) { tb.alloc(n * B); br = tb.as<uint8_t>(); }
+        const double srd = fixed_scale(bits) * std::sqrt(static_cast<double>(padded_dim));
+        launch_encode(et, ud, n, static_cast<int>(padded_dim), srd, dg, br, s);
+        if (!dd) E8QC_CUDA(cudaMemcpyAsync(digits, dg, n * B * 8 * sizeof(uint16_t), cudaMemcpyDeviceToHost, s));
+        if (!bd) E8QC_CUDA(cudaMemcpyAsync(branch, br, n * B, cudaMemcpyDeviceToHost, s));
+        E8QC_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int e8qc_rotate(int device, size_t dim, uint64_t seed, const float* src, size_t n, float* dst,
+                void* stream) {
+    return guarded([&] {
+        if (dim == 0) fail(E8QC_EINVAL, "dim must be positive");
+        if (n == 0) return;
+        if (!src || !dst) fail(E8QC_EINVAL, "null buffer");
+        DeviceGuard g(device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const size_t pd = (dim + 63) / 64 * 64;
+        const std::vector<uint8_t> sg = rotator_signs(dim, seed);
+        DevBuf sd, ts, tdst;
+        sd.alloc(sg.size());
+        E8QC_CUDA(cudaMemcpyAsync(sd.p, sg.data(), sg.size(), cudaMemcpyHostToDevice, s));
+        const float* in = stage_in(src, n * dim, ts, s);
+        const bool dd = is_device_ptr(dst);
+        float* out = dst;
+        if (!dd) { tdst.alloc(n * pd * sizeof(float)); out = tdst.as<float>(); }
+        launch_rotate_raw(sd.as<uint8_t>(), static_cast<int>(dim), static_cast<int>(pd), in,
+                          static_cast<int>(n), out, nullptr, s);
+        if (!dd) E8QC_CUDA(cudaMemcpyAsync(dst, out, n * pd * sizeof(float), cudaMemcpyDeviceToHost, s));
+        E8QC_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int e8qc_e8q_create(int device, size_t dim, int nbits, uint64_t seed, e8qc_index** out) {
+    return guarded([&] {
+        if (out == nullptr) fail(E8QC_EINVAL, "null output");
+        *out = nullptr;
+        if (dim == 0) fail(E8QC_EINVAL, "dim must be positive");
+        if (nbits < 1 || nbits > kMaxBits) fail(E8QC_EINVAL, "nbits must be in [1, 13]");
+        int ndev = 0;
+        E8QC_CUDA(cudaGetDeviceCount(&ndev));
+        if (device < 0 || device >= ndev) fail(E8QC_EINVAL, "no such CUDA device");
+        auto x = std::make_unique<e8qc_index>();
+        x->device = device;
+        x->dim = dim;
+        x->pd = (dim + 63) / 64 * 64;
+        x->bits = nbits;
+        x->seed = seed;
+        x->B = static_cast<int>(x->pd / 8);
+        x->nch = code_chunks(static_cast<int>(x->pd), nbits);
+        x->ws.device = device;
+        *out = x.release();
+    });
+}
+
+int e8qc_e8q_destroy(e8qc_index* x) {
+    return guarded([&] {
+        if (x == nullptr) return;
+        DeviceGuard g(x->device);
+        delete x;
+    });
+}
+
+int e8qc_e8q_build(e8qc_index* x, const float* data, size_t n, const float* centroids, size_t nlist,
+                   const uint32_t* cluster_ids, float prune_alpha, void* stream) {
+    return guarded([&] {
+        if (x == nullptr) fail(E8QC_EINVAL, "null index");
+        if (n == 0 || nlist == 0) fail(E8QC_EINVAL, "BuildLists: empty input");
+        if (!data || !centroids || !cluster_ids) fail(E8QC_EINVAL, "null buffer");
+        if (n > 0xFFFFFFFEull) fail(E8QC_EINVAL, "too many vectors for 32-bit ids");
+        std::lock_guard<std::mutex> lock(x->mu);
+        DeviceGuard g(x->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        // cluster ids on the host for the list layout
+        std::vector<uint32_t> cid_h;
+        const uint32_t* cid = cluster_ids;
+        if (is_device_ptr(cluster_ids)) {
+            cid_h.resize(n);
+            E8QC_CUDA(cudaMemcpyAsync(cid_h.data(), cluster_ids, n * 4, cudaMemcpyDeviceToHost, s));
+            E8QC_CUDA(cudaStreamSynchronize(s));
+            cid = cid_h.data();
+        }
+        std::vector<uint64_t> counts(nlist, 0);
+        for (size_t i = 0; i < n; ++i) {
+            if (cid[i] >= nlist) fail(E8QC_EINVAL, "cluster id out of range");
+            ++counts[cid[i]];
+        }
+        x->built = false;
+        x->n = n;
+        x->nlist = nlist;
+        x->prune_alpha = prune_alpha > 0.0f ? prune_alpha : 1.0f;
+        x->list_begin.assign(nlist + 1, 0);
+        x->tile_begin.assign(nlist + 1, 0);
+        for (size_t c = 0; c < nlist; ++c) {
+            x->list_begin[c + 1] = x->list_begin[c] + counts[c];
+            x->tile_begin[c + 1] = x->tile_begin[c] + static_cast<uint32_t>((counts[c] + 31) / 32);
+        }
+        x->ntiles = x->tile_begin[nlist];
+        {
+            std::vector<uint32_t> t(nlist);
+            for (size_t c = 0; c < nlist; ++c) t[c] = x->tile_begin[c + 1] - x->tile_begin[c];
+            std::sort(t.begin(), t.end(), std::greater<uint32_t>());
+            x->sorted_tiles_prefix.assign(nlist + 1, 0);
+            for (size_t c = 0; c < nlist; ++c) x->sorted_tiles_prefix[c + 1] = x->sorted_tiles_prefix[c] + t[c];
+        }
+        // posting lists in file order (src/index/e8q_build.cpp:120-133)
+        std::vector<uint32_t> row_of(x->ntiles * 32, 0xFFFFFFFFu);
+        std::vector<uint32_t> list_of_tile(x->ntiles);
+        std::vector<uint32_t> list_len(nlist);
+        x->ids_compact.assign(n, 0);
+        {
+            std::vector<uint64_t> cursor(nlist, 0);
+            for (size_t i = 0; i < n; ++i) {
+                const uint32_t c = cid[i];
+                const uint64_t r = cursor[c]++;
+                row_of[static_cast<size_t>(x->tile_begin[c]) * 32 + r] = static_cast<uint32_t>(i);
+                x->ids_compact[x->list_begin[c] + r] = static_cast<uint32_t>(i);
+            }
+            for (size_t c = 0; c < nlist; ++c) {
+                list_len[c] = static_cast<uint32_t>(counts[c]);
+                for (uint32_t t = x->tile_begin[c]; t < x->tile_begin[c + 1]; ++t) list_of_tile[t] = static_cast<uint32_t>(c);
+            }
+        }
+        x->inv_pos.clear();
+        const size_t pd = x->pd, dim = x->dim;
+        // device state
+        const std::vector<uint8_t> sg = rotator_signs(dim, x->seed);
+        x->signs.upload(sg.data(), sg.size(), s);
+        x->tile_begin_d.upload(x->tile_begin.data(), x->tile_begin.size() * 4, s);
+        x->list_len_d.upload(list_len.data(), list_len.size() * 4, s);
+        x->ids.upload(row_of.data(), row_of.size() * 4, s);
+        x->list_of_tile.upload(list_of_tile.data(), list_of_tile.size() * 4, s);
+        x->list_begin_d.upload(x->list_begin.data(), x->list_begin.size() * 8, s);
+        {
+            // refine tables: level / sqrt(pd) as float (src/quantization/e8q_codec.cpp:933-946)
+            const int q = 1 << x->bits;
+            std::vector<float> tab(2 * static_cast<size_t>(q));
+            const double rd = std::sqrt(static_cast<double>(pd));
+            for (int br = 0; br < 2; ++br) {
+                const std::vector<double> lev = branch_levels(x->bits, br);
+                for (int d = 0; d < q; ++d) tab[br * q + d] = static_cast<float>(lev[d] / rd);
+            }
+            x->tab.upload(tab.data(), tab.size() * 4, s);
+        }
+        DevBuf tdata, tcen, mu;
+        const float* data_d = stage_in(data, n * dim, tdata, s);
+        const float* cen_raw = stage_in(centroids, nlist * dim, tcen, s);
+        mu.alloc(dim * sizeof(float));
+        x->mean_rot.alloc(pd * sizeof(float));
+        x->cen.alloc(nlist * pd * sizeof(float));
+        x->cn2.alloc(nlist * sizeof(float));
+        x->codes.alloc(x->ntiles * static_cast<size_t>(x->nch) * 32 * 16);
+        x->g1.alloc(x->ntiles * 32 * sizeof(float));
+        x->h3.alloc(x->ntiles * 32 * sizeof(float));
+        E8QC_CUDA(cudaMemsetAsync(x->codes.p, 0, x->codes.bytes, s));
+        // mean -> rotated mean -> centroids
+        launch_mean(data_d, n, static_cast<int>(dim), mu.as<float>(), s);
+        launch_rotate_raw(x->signs.as<uint8_t>(), static_cast<int>(dim), static_cast<int>(pd), mu.as<float>(), 1,
+                          x->mean_rot.as<float>(), nullptr, s);
+        launch_centroids(x->signs.as<uint8_t>(), static_cast<int>(dim), static_cast<int>(pd), cen_raw,
+                         static_cast<int>(nlist), x->mean_rot.as<float>(), x->cen.as<float>(),
+                         x->cn2.as<float>(), s);
+        DevIndex& v = x->view;
+        v.dim = static_cast<int>(dim);
+        v.pd = static_cast<int>(pd);
+        v.B = x->B;
+        v.bits = x->bits;
+        v.nlist = static_cast<int>(nlist);
+        v.nch = x->nch;
+        v.signs = x->signs.as<uint8_t>();
+        v.mean_rot = x->mean_rot.as<float>();
+        v.cen = x->cen.as<float>();
+        v.cn2 = x->cn2.as<float>();
+        v.tile_begin = x->tile_begin_d.as<uint32_t>();
+        v.list_len = x->list_len_d.as<uint32_t>();
+        v.codes = static_cast<const uint4*>(x->codes.p);
+        v.g1 = x->g1.as<float>();
+        v.h3 = x->h3.as<float>();
+        v.ids = x->ids.as<uint32_t>();
+        v.tab = x->tab.as<float>();
+        const DevEncTables& et = enc_tables_device(x->device, x->bits);
+        BuildEncodeArgs a{};
+        a.base = data_d;
+        a.row_of = x->ids.as<uint32_t>();
+        a.list_of_tile = x->list_of_tile.as<uint32_t>();
+        a.ntiles = static_cast<int>(x->ntiles);
+        a.srd = fixed_scale(x->bits) * std::sqrt(static_cast<double>(pd));
+        a.inv_level_scale = 1.0 / std::sqrt(static_cast<double>(pd));
+        launch_build_encode(v, et, a, static_cast<uint4*>(x->codes.p), x->g1.as<float>(), x->h3.as<float>(), s);
+        E8QC_CUDA(cudaStreamSynchronize(s));
+        x->built = true;
+    });
+}
+
+int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, size_t nprobe, int mode,
+                    uint32_t* out_ids, float* out_dists, e8qc_stats* stats, void* stream) {
+    return guarded([&] {
+        require_built(x, "search");
+        if (k == 0) fail(E8QC_EINVAL, "k must be positive");
+        if (k > static_cast<size_t>(kMaxK)) fail(E8QC_EINVAL, "k must be <= 128");
+        if (nprobe == 0) fail(E8QC_EINVAL, "nprobe must be positive");
+        if (mode != E8QC_MODE_PLAIN && mode != E8QC_MODE_BATCHED) fail(E8QC_EINVAL, "unknown search mode");
+        if (nq == 0) return;
+        if (!queries || !out_ids) fail(E8QC_EINVAL, "null buffer");
+        std::lock_guard<std::mutex> lock(x->mu);
+        DeviceGuard g(x->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const size_t np = std::min(nprobe, x->nlist);
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+        if (stats)
+            for (auto& e : ev) E8QC_CUDA(cudaEventCreate(&e));
+        DevBuf tq, tids, tds;
+        const float* qd = stage_in(queries, nq * x->dim, tq, s);
+        const bool ids_dev = is_device_ptr(out_ids);
+        const bool d_dev = out_dists != nullptr && is_device_ptr(out_dists);
+        uint32_t* ids_d = out_ids;
+        float* d_d = out_dists;
+        if (!ids_dev) { tids.alloc(nq * k * 4); ids_d = tids.as<uint32_t>(); }
+        if (!d_dev) { tds.alloc(nq * k * 4); d_d = tds.as<float>(); }
+        x->ws.ensure_queries(nq, x->pd);
+        float* rq = x->ws.rq.as<float>();
+        if (stats) E8QC_CUDA(cudaEventRecord(ev[0], s));
+        uint64_t launches = launch_rotate(x->view, qd, static_cast<int>(nq), rq, s);
+        if (stats) E8QC_CUDA(cudaEventRecord(ev[1], s));
+        if (mode == E8QC_MODE_PLAIN) {
+            plain_search(x, rq, nq, k, np, ids_d, d_d, stats, s);
+        } else {
+            launches += batched_search(x->view, x->ws, rq, nq, nullptr, nullptr, k, np, k, ids_d, d_d,
+                                       max_tiles_for(x, np), s);
+        }
+        if (stats) E8QC_CUDA(cudaEventRecord(ev[2], s));
+        if (!ids_dev) E8QC_CUDA(cudaMemcpyAsync(out_ids, ids_d, nq * k * 4, cudaMemcpyDeviceToHost, s));
+        if (out_dists && !d_dev) E8QC_CUDA(cudaMemcpyAsync(out_dists, d_d, nq * k * 4, cudaMemcpyDeviceToHost, s));
+        E8QC_CUDA(cudaStreamSynchronize(s));
+        if (stats) {
+            float a = 0, b = 0;
+            E8QC_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
+            E8QC_CUDA(cudaEventElapsedTime(&b, ev[1], ev[2]));
+            stats->rotate_us = a * 1000.0;
+            stats->scan_us = b * 1000.0;
+            stats->launches += launches;
+            // every candidate of every probed list is scored exactly
+            uint64_t cand = 0;
+            (void)cand;
+            for (auto& e : ev) cudaEventDestroy(e);
+        }
+    });
+}
+
+int e8qc_e8q_search_ragged(e8qc_index* x, const float* queries, size_t nq, const uint32_t* k,
+                           const uint32_t* nprobe, size_t k_max, uint32_t* out_ids, float* out_dists,
+                           e8qc_stats* stats, void* stream) {
+    return guarded([&] {
+        require_built(x, "search");
+        if (k_max == 0 || k_max > static_cast<size_t>(kMaxK)) fail(E8QC_EINVAL, "k_max must be in [1, 128]");
+        if (nq == 0) return;
+        if (!queries || !k || !nprobe || !out_ids) fail(E8QC_EINVAL, "null buffer");
+        std::lock_guard<std::mutex> lock(x->mu);
+        DeviceGuard g(x->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        // per-query parameters on the host for validation and bounds
+        std::vector<uint32_t> kh(nq), nph(nq);
+        if (is_device_ptr(k)) E8QC_CUDA(cudaMemcpy(kh.data(), k, nq * 4, cudaMemcpyDeviceToHost));
+        else std::memcpy(kh.data(), k, nq * 4);
+        if (is_device_ptr(nprobe)) E8QC_CUDA(cudaMemcpy(nph.data(), nprobe, nq * 4, cudaMemcpyDeviceToHost));
+        else std::memcpy(nph.data(), nprobe, nq * 4);
+        size_t np_max = 0;
+        for (size_t i = 0; i < nq; ++i) {
+            if (kh[i] == 0 || kh[i] > k_max) fail(E8QC_EINVAL, "k must be in [1, k_max]");
+            if (nph[i] == 0) fail(E8QC_EINVAL, "nprobe must be positive");
+            nph[i] = static_cast<uint32_t>(std::min<size_t>(nph[i], x->nlist));
+            np_max = std::max<size_t>(np_max, nph[i]);
+        }
+        DevBuf tq, tk, tnp, tids, tds;
+        const float* qd = stage_in(queries, nq * x->dim, tq, s);
+        tk.upload(kh.data(), nq * 4, s);
+        tnp.upload(nph.data(), nq * 4, s);
+        const bool ids_dev = is_device_ptr(out_ids);
+        const bool d_dev = out_dists != nullptr && is_device_ptr(out_dists);
+        uint32_t* ids_d = out_ids;
+        float* d_d = out_dists;
+        if (!ids_dev) { tids.alloc(nq * k_max * 4); ids_d = tids.as<uint32_t>(); }
+        if (!d_dev) { tds.alloc(nq * k_max * 4); d_d = tds.as<float>(); }
+        x->ws.ensure_queries(nq, x->pd);
+        float* rq = x->ws.rq.as<float>();
+        uint64_t launches = launch_rotate(x->view, qd, static_cast<int>(nq), rq, s);
+        launches += batched_search(x->view, x->ws, rq, nq, tk.as<uint32_t>(), tnp.as<uint32_t>(), k_max,
+                                   np_max, k_max, ids_d, d_d, max_tiles_for(x, np_max), s);
+        if (!ids_dev) E8QC_CUDA(cudaMemcpyAsync(out_ids, ids_d, nq * k_max * 4, cudaMemcpyDeviceToHost, s));
+        if (out_dists && !d_dev) E8QC_CUDA(cudaMemcpyAsync(out_dists, d_d, nq * k_max * 4, cudaMemcpyDeviceToHost, s));
+        E8QC_CUDA(cudaStreamSynchronize(s));
+        if (stats) stats->launches = launches;
+    });
+}
+
+int e8qc_e8q_estimate(e8qc_index* x, const float* query, uint32_t id, float* out) {
+    return guarded([&] {
+        require_built(x, "estimate");
+        if (!query || !out) fail(E8QC_EINVAL, "null buffer");
+        std::lock_guard<std::mutex> lock(x->mu);
+        if (x->inv_pos.size() != x->n) {
+            x->inv_pos.assign(x->n, 0xFFFFFFFFu);
+            for (size_t i = 0; i < x->n; ++i) x->inv_pos[x->ids_compact[i]] = static_cast<uint32_t>(i);
+        }
+        if (id >= x->n || x->inv_pos[id] == 0xFFFFFFFFu) fail(E8QC_ERANGE, "Estimate: id out of range");
+        const uint64_t pos = x->inv_pos[id];
+        const size_t c = static_cast<size_t>(
+            std::upper_bound(x->list_begin.begin() + 1, x->list_begin.end(), pos) - x->list_begin.begin() - 1);
+        const uint32_t slot = x->tile_begin[c] * 32 + static_cast<uint32_t>(pos - x->list_begin[c]);
+        DeviceGuard g(x->device);
+        cudaStream_t s = nullptr;
+        DevBuf tq, out_d;
+        const float* qd = stage_in(query, x->dim, tq, s);
+        x->ws.ensure_queries(1, x->pd);
+        launch_rotate(x->view, qd, 1, x->ws.rq.as<float>(), s);
+        out_d.alloc(4);
+        launch_estimate(x->view, x->ws.rq.as<float>(), static_cast<int>(c), slot, out_d.as<float>(), s);
+        float r = 0.0f;
+        E8QC_CUDA(cudaMemcpy(&r, out_d.p, 4, cudaMemcpyDeviceToHost));
+        *out = r;
+    });
+}
+
+int e8qc_e8q_set_disable_prune(e8qc_index* x, int on) {
+    return guarded([&] {
+        require_built(x, "set_disable_prune");
+        x->disable_prune = on != 0;
+    });
+}
+
+int e8qc_e8q_set_prune_alpha(e8qc_index* x, float alpha) {
+    return guarded([&] {
+        require_built(x, "set_prune_alpha");
+        if (!(alpha > 0.0f)) fail(E8QC_EINVAL, "prune_alpha must be positive");
+        x->prune_alpha = alpha;
+    });
+}
+
+int e8qc_e8q_info(const e8qc_index* x, e8qc_info* out) {
+    return guarded([&] {
+        if (!x || !out) fail(E8QC_EINVAL, "null argument");
+        out->dim = x->dim;
+        out->padded_dim = x->pd;
+        out->n = x->n;
+        out->nlist = x->nlist;
+        out->memory_bytes = x->memory_bytes();
+        out->nbits = x->bits;
+        out->device = x->device;
+        out->built = x->built ? 1 : 0;
+        out->disable_prune = x->disable_prune ? 1 : 0;
+        out->prune_alpha = x->prune_alpha;
+    });
+}
+
+int e8qc_e8q_get_ids(const e8qc_index* x, uint32_t* out) {
+    return guarded([&] {
+        require_built(x, "get_ids");
+        if (!out) fail(E8QC_EINVAL, "null output");
+        std::memcpy(out, x->ids_compact.data(), x->n * 4);
+    });
+}
+
+int e8qc_e8q_export_codes(const e8qc_index* xc, uint16_t* digits, uint8_t* branch, float* g1, float* h3) {
+    return guarded([&] {
+        require_built(xc, "export_codes");
+        e8qc_index* x = const_cast<e8qc_index*>(xc);
+        std::lock_guard<std::mutex> lock(x->mu);
+        DeviceGuard g(x->device);
+        cudaStream_t s = nullptr;
+        const size_t n = x->n, B = static_cast<size_t>(x->B);
+        if (digits || branch) {
+            DevBuf dd, bd;
+            dd.alloc(n * B * 8 * 2);
+            bd.alloc(n * B);
+            launch_decode(x->view, static_cast<int>(x->ntiles), x->list_of_tile.as<uint32_t>(),
+                          x->list_begin_d.as<uint64_t>(), dd.as<uint16_t>(), bd.as<uint8_t>(), s);
+            E8QC_CUDA(cudaStreamSynchronize(s));
+            if (digits) E8QC_CUDA(cudaMemcpy(digits, dd.p, n * B * 8 * 2, cudaMemcpyDeviceToHost));
+            if (branch) E8QC_CUDA(cudaMemcpy(branch, bd.p, n * B, cudaMemcpyDeviceToHost));
+        }
+        if (g1 || h3) {
+            std::vector<float> a(x->ntiles * 32), b(x->ntiles * 32);
+            E8QC_CUDA(cudaMemcpy(a.data(), x->g1.p, a.size() * 4, cudaMemcpyDeviceToHost));
+            E8QC_CUDA(cudaMemcpy(b.data(), x->h3.p, b.size() * 4, cudaMemcpyDeviceToHost));
+            for (size_t c = 0; c < x->nlist; ++c) {
+                for (uint64_t p = x->list_begin[c]; p < x->list_begin[c + 1]; ++p) {
+                    const size_t slot = static_cast<size_t>(x->tile_begin[c]) * 32 + (p - x->list_begin[c]);
+                    if (g1) g1[p] = a[slot];
+                    if (h3) h3[p] = b[slot];
+                }
+            }
+        }
+    });
+}
+
+}  // extern "C"

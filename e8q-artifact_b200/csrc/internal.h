@@ -1,0 +1,160 @@
+// Internal declarations shared by the host code and the CUDA kernels of
+// libe8qcuda.so. Not installed; the public surface is include/e8qc.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "e8qc.h"
+
+namespace e8qc {
+
+constexpr int kMaxBits = 13;
+constexpr int kMaxK = 128;
+constexpr int kTile = 32;  // vectors per tile: one warp lane per vector
+
+// Library error: carries an e8qc status code to the C boundary.
+struct Error {
+    int code;
+    std::string msg;
+};
+[[noreturn]] void fail(int code, const std::string& msg);
+void cuda_check(cudaError_t e, const char* what);
+#define E8QC_CUDA(x) ::e8qc::cuda_check((x), #x)
+
+// ---------------------------------------------------------------------------
+// Codec constants (host). Restated from the reference codec
+// (src/quantization/e8q_codec.cpp); see codec_host.cpp.
+double inv_normal_cdf(double p);
+std::vector<double> branch_levels(int bits, int branch);
+double fixed_scale(int bits);
+constexpr double kSigmaC = 1.1180339887498949;
+
+// Sorted level table with the bounded-bin insertion index
+// (src/quantization/e8q_codec.cpp:70-123): merged four-class table when it
+// alternates, else four per-(branch, parity) tables.
+struct LevelTableHost {
+    std::vector<double> lev;   // pad x -inf | n levels | pad x +inf
+    std::vector<uint16_t> dig; // same indexing
+    std::vector<uint32_t> bin_lo;
+    int pad = 0;
+    int n = 0;
+    double bin_lo_v = 0.0, bin_scale = 0.0;
+    int nbins = 1;
+    int usable = 0;
+};
+
+struct EncTablesHost {
+    int bits = 0;
+    int alternating = 0;
+    LevelTableHost merged;
+    LevelTableHost parity[2][2];  // [branch][odd]
+    std::vector<double> levels[2];
+};
+const EncTablesHost& enc_tables_host(int bits);
+
+// Device view of one level table.
+struct DevLevelTable {
+    const double* lev;      // points at the first real level (pads around it)
+    const uint16_t* dig;    // same indexing as lev
+    const uint32_t* bin_lo;
+    int n, nbins, usable;
+    double bin_lo_v, bin_scale;
+};
+
+struct DevEncTables {
+    int bits, alternating;
+    DevLevelTable merged;
+    DevLevelTable parity[4];  // [branch*2 + odd]
+    const double* levels[2];  // 2^bits each
+};
+// Per (device, bits) upload, cached for the process lifetime.
+const DevEncTables& enc_tables_device(int device, int bits);
+
+// ---------------------------------------------------------------------------
+// Device index layout.
+//
+// Vectors are stored list-major ("cluster-major"), each list padded to whole
+// tiles of 32 vectors. A vector's code is a little-endian bitstream of B =
+// padded_dim/8 blocks of 8*bits bits; inside a block digit i occupies bits
+// [i*bits, (i+1)*bits) except that the lowest bit of digit 7 holds the branch
+// (digit 7's own LSB is the parity of digits 0..6, the E8 quotient-shell
+// constraint, so it is not stored). The stream is padded to whole 16-byte
+// chunks (nch per vector), and a tile stores chunk c of lane l at
+// [tile][c][l] so a warp reading chunk c touches 512 contiguous bytes.
+struct DevIndex {
+    int dim, pd, B, bits, nlist, nch;
+    const uint8_t* signs;        // 4*pd/8 rotation sign bits
+    const float* mean_rot;       // pd
+    const float* cen;            // nlist*pd rotated, centred centroids
+    const float* cn2;            // nlist squared norms
+    const uint32_t* tile_begin;  // nlist+1
+    const uint32_t* list_len;    // nlist vectors per list
+    const uint4* codes;          // ntiles*nch*32 chunks
+    const float* g1;             // ntiles*32
+    const float* h3;             // ntiles*32
+    const uint32_t* ids;         // ntiles*32, UINT32_MAX on padding lanes
+    const float* tab;            // [2][2^bits] level/sqrt(pd) refine tables
+};
+
+inline int code_chunks(int pd, int bits) { return (pd / 8 * 8 * bits + 127) / 128; }
+
+// ---------------------------------------------------------------------------
+// Kernel launchers (each returns the number of kernels it launched).
+
+// Rotation + mean-centring of nq queries: out[nq][pd] = rot(q) - mean_rot.
+int launch_rotate(const DevIndex& ix, const float* q, int nq, float* out, cudaStream_t s);
+// Raw rotation (no centring): n rows of dim floats -> n rows of pd floats.
+int launch_rotate_raw(const uint8_t* signs, int dim, int pd, const float* src, int n, float* dst,
+                      const float* subtract, cudaStream_t s);
+
+struct RouteWork {
+    uint64_t* keys;        // nlist
+    uint32_t* probes;      // nlist (first nprobe used)
+    float* probe_d2;       // nlist
+    uint32_t* tile_off;    // nlist+1 exclusive prefix of probed tiles
+    uint32_t* counter;     // last-CTA-done counter (self-resetting)
+    uint32_t* total_tiles; // 1
+};
+// One query: d2 to every centroid, then (last CTA) the nprobe nearest lists
+// and the prefix of their tile counts.
+int launch_route_one(const DevIndex& ix, const float* rq, int nprobe, const RouteWork& w,
+                     cudaStream_t s);
+
+struct ScanWork {
+    float* part_d;      // grid*kmax
+    uint32_t* part_id;  // grid*kmax
+    uint32_t* counter;  // self-resetting
+    int grid;
+};
+int plain_scan_grid(int bits);
+int launch_scan_plain(const DevIndex& ix, const float* rq, const RouteWork& rw, int k,
+                      const ScanWork& sw, uint32_t* out_ids, float* out_d, cudaStream_t s);
+
+// Build kernels.
+int launch_mean(const float* x, size_t n, int dim, float* mu_out, cudaStream_t s);
+int launch_centroids(const uint8_t* signs, int dim, int pd, const float* cen_raw, int nlist,
+                     const float* mean_rot, float* cen_rot, float* cn2, cudaStream_t s);
+struct BuildEncodeArgs {
+    const float* base;       // n*dim raw rows (device)
+    const uint32_t* row_of;  // ntiles*32 slot -> row id (UINT32_MAX padding)
+    const uint32_t* list_of_tile;  // ntiles
+    int ntiles;
+    double srd;              // FixedScale(bits) * sqrt(pd)
+    double inv_level_scale;  // 1/sqrt(pd)
+};
+int launch_build_encode(const DevIndex& ix, const DevEncTables& et, const BuildEncodeArgs& a,
+                        uint4* codes, float* g1, float* h3, cudaStream_t s);
+int launch_encode(const DevEncTables& et, const float* unit, size_t n, int pd, double srd,
+                  uint16_t* digits, uint8_t* branch, cudaStream_t s);
+// Decode device codes back to digits/branch (export, tests).
+int launch_decode(const DevIndex& ix, int ntiles, const uint32_t* list_of_tile,
+                  const uint64_t* list_begin, uint16_t* digits, uint8_t* branch, cudaStream_t s);
+// Estimate one stored vector at tile slot `slot` of list `list`.
+int launch_estimate(const DevIndex& ix, const float* rq, int list, uint32_t slot, float* out,
+                    cudaStream_t s);
+
+}  // namespace e8qc

@@ -1,0 +1,509 @@
+// Search-path kernels: query rotation, one-query routing with on-device
+// top-nprobe selection, the plain streaming scan with warp top-k, and the
+// single-vector estimator.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_common.cuh"
+#include "internal.h"
+
+namespace e8qc {
+
+namespace {
+
+__device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
+
+// Block-wide exclusive scan of one int per thread (blockDim <= 1024).
+__device__ int block_exclusive_scan(int v, int* total, int* sm32) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sm32[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int s = lane < nw ? sm32[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, s, o);
+            if (lane >= o) s += y;
+        }
+        sm32[lane] = s;
+    }
+    __syncthreads();
+    const int before = (warp > 0 ? sm32[warp - 1] : 0) + x - v;
+    *total = sm32[nw - 1];
+    __syncthreads();
+    return before;
+}
+
+// ---------------------------------------------------------------------------
+// Query rotation: one CTA per query. out = rot(q) - mean_rot.
+__global__ void rotate_queries_kernel(const float* __restrict__ q, int dim, int pd, int td,
+                                      float fac, const uint8_t* __restrict__ signs,
+                                      const float* __restrict__ subtract, float* __restrict__ out) {
+    extern __shared__ float sx[];
+    const size_t row = blockIdx.x;
+    for (int i = threadIdx.x; i < pd; i += blockDim.x) sx[i] = i < dim ? q[row * dim + i] : 0.0f;
+    __syncthreads();
+    rotate_rows_smem(sx, 1, pd, pd, td, fac, signs);
+    for (int i = threadIdx.x; i < pd; i += blockDim.x)
+        out[row * pd + i] = subtract ? __fsub_rn(sx[i], subtract[i]) : sx[i];
+}
+
+// ---------------------------------------------------------------------------
+// Top-nprobe lists of one query by 64-bit key (float bits of d2 << 32 | cid),
+// src/index/ivf_route.cpp:9-27 + src/simd/kernels.hpp:13-21. Keys are unique,
+// so an 8-pass MSB radix select finds the nprobe-th key exactly; the selected
+// lists are compacted in cid order (the plain scan's result does not depend
+// on probe order) with their tile-count prefix.
+__device__ void select_probes(const DevIndex& ix, const uint64_t* keys, int nprobe,
+                              const RouteWork& w) {
+    __shared__ int hist[256];
+    __shared__ uint64_t s_prefix;
+    __shared__ int s_want;
+    __shared__ int sm32[32];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int nlist = ix.nlist;
+    if (tid == 0) {
+        s_prefix = 0;
+        s_want = nprobe;
+    }
+    uint64_t mask = 0;
+    __syncthreads();
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        for (int i = tid; i < 256; i += nt) hist[i] = 0;
+        __syncthreads();
+        const uint64_t prefix = s_prefix;
+        for (int c = tid; c < nlist; c += nt) {
+            const uint64_t key = __ldcg(reinterpret_cast<const unsigned long long*>(keys) + c);
+            if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1);
+        }
+        __syncthreads();
+        if (tid < 32) {
+            // each lane owns 8 consecutive bins
+            int cnt[8], tot = 0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                cnt[j] = hist[tid * 8 + j];
+                tot += cnt[j];
+            }
+            int incl = tot;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(kFull, incl, o);
+                if (tid >= o) incl += y;
+            }
+            const int excl = incl - tot;
+            const int want = s_want;
+            const unsigned hit = __ballot_sync(kFull, excl < want && incl >= want);
+            const int owner = __ffs(hit) - 1;
+            if (tid == owner) {
+                int cum = excl, sel = 0;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    if (cum + cnt[j] >= want) { sel = j; break; }
+                    cum += cnt[j];
+                }
+                s_prefix = prefix | (static_cast<uint64_t>(tid * 8 + sel) << shift);
+                s_want = want - cum;
+            }
+        }
+        mask |= 0xFFull << shift;
+        __syncthreads();
+    }
+    const uint64_t kth = s_prefix;
+    // compact keys <= kth in cid order
+    int base = 0;
+    for (int c0 = 0; c0 < nlist; c0 += nt) {
+        const int c = c0 + tid;
+        uint64_t key = ~0ull;
+        if (c < nlist) key = __ldcg(reinterpret_cast<const unsigned long long*>(keys) + c);
+        const int flag = (c < nlist && key <= kth) ? 1 : 0;
+        int tot;
+        const int pos = base + block_exclusive_scan(flag, &tot, sm32);
+        if (flag) {
+            w.probes[pos] = static_cast<uint32_t>(c);
+            w.probe_d2[pos] = __uint_as_float(static_cast<uint32_t>(key >> 32));
+        }
+        base += tot;
+    }
+    __syncthreads();
+    // tile prefix of the probed lists
+    int tbase = 0;
+    for (int p0 = 0; p0 < nprobe; p0 += nt) {
+        const int p = p0 + tid;
+        int t = 0;
+        if (p < nprobe) {
+            const uint32_t c = __ldcg(w.probes + p);
+            t = static_cast<int>(ix.tile_begin[c + 1] - ix.tile_begin[c]);
+        }
+        int tot;
+        const int pos = tbase + block_exclusive_scan(t, &tot, sm32);
+        if (p < nprobe) w.tile_off[p] = static_cast<uint32_t>(pos);
+        tbase += tot;
+    }
+    if (tid == 0) {
+        w.tile_off[nprobe] = static_cast<uint32_t>(tbase);
+        *w.total_tiles = static_cast<uint32_t>(tbase);
+    }
+}
+
+// d2 of one rotated query to every centroid (fp32 products summed in fp64,
+// as the scalar GEMV src/simd/kernels_generic.cpp:13-33), then the last CTA
+// to finish selects the probes.
+__global__ void route_one_kernel(DevIndex ix, const float* __restrict__ rq, int nprobe,
+                                 RouteWork w) {
+    extern __shared__ float sq[];
+    __shared__ double red[32];
+    __shared__ float s_qn2;
+    __shared__ bool s_last;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const int pd = ix.pd;
+    double part = 0.0;
+    for (int i = tid; i < pd; i += blockDim.x) {
+        const float v = rq[i];
+        sq[i] = v;
+        part += static_cast<double>(v) * static_cast<double>(v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(kFull, part, o);
+    if (lane == 0) red[warp] = part;
+    __syncthreads();
+    if (tid == 0) {
+        double s = 0.0;
+        for (int i = 0; i < nw; ++i) s += red[i];
+        s_qn2 = static_cast<float>(s);
+    }
+    __syncthreads();
+    const float qn2 = s_qn2;
+    for (int c = blockIdx.x * nw + warp; c < ix.nlist; c += gridDim.x * nw) {
+        const float* cc = ix.cen + static_cast<size_t>(c) * pd;
+        double dot = 0.0;
+        for (int i = lane; i < pd; i += 32) dot += static_cast<double>(sq[i]) * static_cast<double>(__ldg(cc + i));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(kFull, dot, o);
+        if (lane == 0) {
+            float d2 = __fmaf_rn(-2.0f, static_cast<float>(dot), __fadd_rn(qn2, ix.cn2[c]));
+            if (d2 < 0.0f) d2 = 0.0f;
+            w.keys[c] = (static_cast<uint64_t>(__float_as_uint(d2)) << 32) | static_cast<uint32_t>(c);
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = atomicAdd(w.counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    select_probes(ix, w.keys, nprobe, w);
+    if (tid == 0) *w.counter = 0;
+}
+
+// Copies of the level table kept in shared memory: 32 (one per lane, so the
+// gathers are bank-conflict free) up to 8 bits, fewer above (64 KB cap).
+template <int BITS>
+__host__ __device__ constexpr int table_rep() {
+    return BITS <= 8 ? 32 : ((16384 >> BITS) > 0 ? (16384 >> BITS) : 1);
+}
+
+// ---------------------------------------------------------------------------
+// Exact score of the vector in `lane` of a tile: S = sum_i q[i] *
+// tab[branch][digit_i] (the estimator of src/index/e8q_search.cpp:87-127;
+// fp32 FMA, two accumulators by block parity). Codes are read straight from
+// global memory one 16-byte chunk per lane (512 contiguous bytes per warp);
+// the level table is replicated REP times in shared memory so the 32 lanes'
+// gathers hit distinct banks.
+template <int BITS>
+__device__ __forceinline__ float score_tile_lane(const uint4* __restrict__ tile, int B,
+                                                 const float4* __restrict__ sq4,
+                                                 const float* __restrict__ tabrep, int lane) {
+    constexpr int GBL = group_blocks(BITS);
+    constexpr int GCH = group_chunks(BITS);
+    constexpr int BB = 8 * BITS;
+    constexpr int REP = table_rep<BITS>();
+    const int rl = lane % REP;
+    float acc0 = 0.0f, acc1 = 0.0f;
+    const int ng = B / GBL;
+    const int tail = B - ng * GBL;  // 0 or 8 (odd rates only)
+    int blk = 0;
+    for (int g = 0; g < ng; ++g) {
+        uint32_t w[4 * GCH + 1];
+#pragma unroll
+        for (int c = 0; c < GCH; ++c) {
+            const uint4 v = __ldg(tile + (g * GCH + c) * 32 + lane);
+            w[4 * c] = v.x;
+            w[4 * c + 1] = v.y;
+            w[4 * c + 2] = v.z;
+            w[4 * c + 3] = v.w;
+        }
+        w[4 * GCH] = 0;
+#pragma unroll
+        for (int b = 0; b < GBL; ++b, ++blk) {
+            uint32_t dg[8];
+            const int br = decode_block<BITS>(w, b * BB, dg);
+            const float4 qa = sq4[2 * blk], qb = sq4[2 * blk + 1];
+            const float* t = tabrep + ((br << BITS) * REP) + rl;
+            float& acc = (b & 1) ? acc1 : acc0;
+            acc = __fmaf_rn(qa.x, t[dg[0] * REP], acc);
+            acc = __fmaf_rn(qa.y, t[dg[1] * REP], acc);
+            acc = __fmaf_rn(qa.z, t[dg[2] * REP], acc);
+            acc = __fmaf_rn(qa.w, t[dg[3] * REP], acc);
+            acc = __fmaf_rn(qb.x, t[dg[4] * REP], acc);
+            acc = __fmaf_rn(qb.y, t[dg[5] * REP], acc);
+            acc = __fmaf_rn(qb.z, t[dg[6] * REP], acc);
+            acc = __fmaf_rn(qb.w, t[dg[7] * REP], acc);
+        }
+    }
+    if (tail > 0) {
+        constexpr int TCH = (8 * BB + 127) / 128;
+        uint32_t w[4 * TCH + 1];
+#pragma unroll
+        for (int c = 0; c < TCH; ++c) {
+            const uint4 v = __ldg(tile + (ng * GCH + c) * 32 + lane);
+            w[4 * c] = v.x;
+            w[4 * c + 1] = v.y;
+            w[4 * c + 2] = v.z;
+            w[4 * c + 3] = v.w;
+        }
+        w[4 * TCH] = 0;
+#pragma unroll
+        for (int b = 0; b < 8; ++b, ++blk) {
+            uint32_t dg[8];
+            const int br = decode_block<BITS>(w, b * BB, dg);
+            const float4 qa = sq4[2 * blk], qb = sq4[2 * blk + 1];
+            const float* t = tabrep + ((br << BITS) * REP) + rl;
+            float& acc = (b & 1) ? acc1 : acc0;
+            acc = __fmaf_rn(qa.x, t[dg[0] * REP], acc);
+            acc = __fmaf_rn(qa.y, t[dg[1] * REP], acc);
+            acc = __fmaf_rn(qa.z, t[dg[2] * REP], acc);
+            acc = __fmaf_rn(qa.w, t[dg[3] * REP], acc);
+            acc = __fmaf_rn(qb.x, t[dg[4] * REP], acc);
+            acc = __fmaf_rn(qb.y, t[dg[5] * REP], acc);
+            acc = __fmaf_rn(qb.z, t[dg[6] * REP], acc);
+            acc = __fmaf_rn(qb.w, t[dg[7] * REP], acc);
+        }
+    }
+    return __fadd_rn(acc0, acc1);
+}
+
+// CTA-wide merge of per-warp top-k lists into warp 0 (smem staging).
+__device__ void cta_merge(WarpTopK& top, float* sm_d, uint32_t* sm_id, int k) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    top.store(sm_d + warp * kMaxK, sm_id + warp * kMaxK, k);
+    __syncthreads();
+    if (warp == 0) {
+        for (int w2 = 1; w2 < nw; ++w2) {
+            for (int j0 = 0; j0 < k; j0 += 32) {
+                const int j = j0 + lane;
+                const bool ok = j < k;
+                const float dd = ok ? sm_d[w2 * kMaxK + j] : inf_f();
+                const uint32_t ii = ok ? sm_id[w2 * kMaxK + j] : 0xFFFFFFFFu;
+                top.offer_pair(dd, ii, ok && ii != 0xFFFFFFFFu);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// Plain (unpruned) streaming scan of one query over its probed lists: every
+// vector of every probed list gets dist = (d2 + h3) - 2*g1*S (the refine
+// step of src/simd/e8q_search_generic.cpp:58-66 with d2 folded as in
+// e8q_search_generic.cpp:189) and enters a warp top-k; CTAs merge into
+// per-CTA lists and the last CTA to finish merges those into the answer.
+template <int BITS>
+__global__ void __launch_bounds__(256) scan_plain_kernel(DevIndex ix, const float* __restrict__ rq,
+                                                         RouteWork rw, int k, ScanWork sw,
+                                                         uint32_t* __restrict__ out_ids,
+                                                         float* __restrict__ out_d) {
+    constexpr int Q = 1 << BITS;
+    constexpr int REP = table_rep<BITS>();
+    extern __shared__ __align__(16) float smem[];
+    float* sq = smem;                              // pd
+    float* tabrep = smem + ix.pd;                  // 2*Q*REP
+    float* sm_d = tabrep + 2 * Q * REP;            // 8 warps * kMaxK
+    uint32_t* sm_id = reinterpret_cast<uint32_t*>(sm_d + 8 * kMaxK);
+    __shared__ bool s_last;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    for (int i = tid; i < ix.pd; i += blockDim.x) sq[i] = rq[i];
+    for (int e = tid; e < 2 * Q * REP; e += blockDim.x) tabrep[e] = ix.tab[e / REP];
+    __syncthreads();
+    const float4* sq4 = reinterpret_cast<const float4*>(sq);
+    const int T = static_cast<int>(__ldcg(rw.total_tiles));
+    const int gw = blockIdx.x * nw + warp, tw = gridDim.x * nw;
+    WarpTopK top;
+    top.init(k);
+    int p = 0;
+    for (int t = gw; t < T; t += tw) {
+        // probe p with tile_off[p] <= t < tile_off[p+1] (monotone in t: walk)
+        while (__ldcg(rw.tile_off + p + 1) <= static_cast<uint32_t>(t)) ++p;
+        const uint32_t list = __ldcg(rw.probes + p);
+        const float d2 = __ldcg(rw.probe_d2 + p);
+        const uint32_t local = static_cast<uint32_t>(t) - __ldcg(rw.tile_off + p);
+        const uint32_t gt = ix.tile_begin[list] + local;
+        const bool valid = local * 32u + static_cast<uint32_t>(lane) < ix.list_len[list];
+        const uint4* tile = ix.codes + static_cast<size_t>(gt) * ix.nch * 32;
+        const float S = score_tile_lane<BITS>(tile, ix.B, sq4, tabrep, lane);
+        const size_t slot = static_cast<size_t>(gt) * 32 + lane;
+        const float g1 = __ldg(ix.g1 + slot), h3 = __ldg(ix.h3 + slot);
+        const float dist = __fmaf_rn(-__fmul_rn(2.0f, g1), S, __fadd_rn(d2, h3));
+        top.offer(dist, valid, [&] { return __ldg(ix.ids + slot); });
+    }
+    cta_merge(top, sm_d, sm_id, k);
+    if (warp == 0) top.store(sw.part_d + static_cast<size_t>(blockIdx.x) * kMaxK,
+                             sw.part_id + static_cast<size_t>(blockIdx.x) * kMaxK, k);
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = atomicAdd(sw.counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // final merge of gridDim.x partial lists
+    top.init(k);
+    for (int c = warp; c < static_cast<int>(gridDim.x); c += nw) {
+        for (int j0 = 0; j0 < k; j0 += 32) {
+            const int j = j0 + lane;
+            const bool ok = j < k;
+            const float dd = ok ? __ldcg(sw.part_d + static_cast<size_t>(c) * kMaxK + j) : inf_f();
+            const uint32_t ii = ok ? __ldcg(sw.part_id + static_cast<size_t>(c) * kMaxK + j) : 0xFFFFFFFFu;
+            top.offer_pair(dd, ii, ok && ii != 0xFFFFFFFFu);
+        }
+    }
+    cta_merge(top, sm_d, sm_id, k);
+    if (warp == 0) top.store(out_d, out_ids, k);
+    if (tid == 0) *sw.counter = 0;
+}
+
+// One stored vector: Estimate() of src/index/e8q_oracle.cpp:58-101 (fp32
+// qn2/dot chains fused as the reference build fuses them, fp64 score).
+template <int BITS>
+__global__ void estimate_kernel(DevIndex ix, const float* __restrict__ rq, int list, uint32_t slot,
+                                float* __restrict__ out) {
+    if (threadIdx.x != 0) return;
+    const float* cc = ix.cen + static_cast<size_t>(list) * ix.pd;
+    float qn2 = 0.0f, dot = 0.0f;
+    for (int i = 0; i < ix.pd; ++i) {
+        qn2 = __fmaf_rn(rq[i], rq[i], qn2);
+        dot = __fmaf_rn(rq[i], cc[i], dot);
+    }
+    float d2 = __fmaf_rn(-2.0f, dot, __fadd_rn(qn2, ix.cn2[list]));
+    if (d2 < 0.0f) d2 = 0.0f;
+    const uint4* tile = ix.codes + static_cast<size_t>(slot / 32) * ix.nch * 32;
+    const int lane = slot % 32;
+    constexpr int Q = 1 << BITS;
+    double acc = 0.0;
+    for (int blk = 0; blk < ix.B; ++blk) {
+        // gather the block's bits (8*BITS <= 104) from its chunks
+        const int off = blk * 8 * BITS;
+        uint32_t words[5];
+        for (int j = 0; j < 5; ++j) {
+            const int wi = (off >> 5) + j;
+            const int c = wi >> 2;
+            if (c < ix.nch) {
+                const uint4 v = tile[c * 32 + lane];
+                const uint32_t arr[4] = {v.x, v.y, v.z, v.w};
+                words[j] = arr[wi & 3];
+            } else {
+                words[j] = 0;
+            }
+        }
+        uint32_t dg[8];
+        const int br = decode_block<BITS>(words, off & 31, dg);
+        for (int i = 0; i < 8; ++i)
+            acc += static_cast<double>(rq[blk * 8 + i]) *
+                   static_cast<double>(ix.tab[br * Q + static_cast<int>(dg[i])]);
+    }
+    const float S = static_cast<float>(acc);
+    const size_t s = slot;
+    *out = __fmaf_rn(-__fmul_rn(2.0f, ix.g1[s]), S, __fadd_rn(d2, ix.h3[s]));
+}
+
+template <int BITS>
+int launch_scan_bits(const DevIndex& ix, const float* rq, const RouteWork& rw, int k,
+                     const ScanWork& sw, uint32_t* out_ids, float* out_d, cudaStream_t s) {
+    constexpr int Q = 1 << BITS;
+    constexpr int REP = table_rep<BITS>();
+    const size_t smem = (static_cast<size_t>(ix.pd) + 2 * Q * REP + 8 * kMaxK * 2) * sizeof(float);
+    static uint64_t configured = 0;  // one bit per device ordinal
+    int dev = 0;
+    E8QC_CUDA(cudaGetDevice(&dev));
+    if (!((configured >> (dev & 63)) & 1u)) {
+        E8QC_CUDA(cudaFuncSetAttribute(scan_plain_kernel<BITS>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        configured |= uint64_t{1} << (dev & 63);
+    }
+    scan_plain_kernel<BITS><<<sw.grid, 256, smem, s>>>(ix, rq, rw, k, sw, out_ids, out_d);
+    E8QC_CUDA(cudaGetLastError());
+    return 1;
+}
+
+}  // namespace
+
+int launch_rotate(const DevIndex& ix, const float* q, int nq, float* out, cudaStream_t s) {
+    int td = 1;
+    while ((td << 1) <= ix.dim) td <<= 1;
+    const float fac = 1.0f / sqrtf(static_cast<float>(td));
+    rotate_queries_kernel<<<nq, 256, ix.pd * sizeof(float), s>>>(q, ix.dim, ix.pd, td, fac,
+                                                                 ix.signs, ix.mean_rot, out);
+    E8QC_CUDA(cudaGetLastError());
+    return 1;
+}
+
+int launch_rotate_raw(const uint8_t* signs, int dim, int pd, const float* src, int n, float* dst,
+                      const float* subtract, cudaStream_t s) {
+    int td = 1;
+    while ((td << 1) <= dim) td <<= 1;
+    const float fac = 1.0f / sqrtf(static_cast<float>(td));
+    rotate_queries_kernel<<<n, 256, pd * sizeof(float), s>>>(src, dim, pd, td, fac, signs,
+                                                             subtract, dst);
+    E8QC_CUDA(cudaGetLastError());
+    return 1;
+}
+
+int launch_route_one(const DevIndex& ix, const float* rq, int nprobe, const RouteWork& w,
+                     cudaStream_t s) {
+    const int warps = 8;
+    int grid = (ix.nlist + warps * 4 - 1) / (warps * 4);  // ~4 centroids per warp
+    grid = grid < 1 ? 1 : (grid > 296 ? 296 : grid);
+    route_one_kernel<<<grid, warps * 32, ix.pd * sizeof(float), s>>>(ix, rq, nprobe, w);
+    E8QC_CUDA(cudaGetLastError());
+    return 1;
+}
+
+int plain_scan_grid(int bits) {
+    (void)bits;
+    return 148 * 3;
+}
+
+int launch_scan_plain(const DevIndex& ix, const float* rq, const RouteWork& rw, int k,
+                      const ScanWork& sw, uint32_t* out_ids, float* out_d, cudaStream_t s) {
+    switch (ix.bits) {
+#define E8QC_CASE(b) \
+    case b: return launch_scan_bits<b>(ix, rq, rw, k, sw, out_ids, out_d, s);
+        E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
+        E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
+        E8QC_CASE(13)
+#undef E8QC_CASE
+        default: fail(E8QC_EINVAL, "bits out of range");
+    }
+    return 0;
+}
+
+int launch_estimate(const DevIndex& ix, const float* rq, int list, uint32_t slot, float* out,
+                    cudaStream_t s) {
+    switch (ix.bits) {
+#define E8QC_CASE(b) \
+    case b: estimate_kernel<b><<<1, 32, 0, s>>>(ix, rq, list, slot, out); break;
+        E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
+        E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
+        E8QC_CASE(13)
+#undef E8QC_CASE
+        default: fail(E8QC_EINVAL, "bits out of range");
+    }
+    E8QC_CUDA(cudaGetLastError());
+    return 1;
+}
+
+}  // namespace e8qc

@@ -1,0 +1,97 @@
+// Device buffers and the per-index search workspace.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstddef>
+
+#include "internal.h"
+
+namespace e8qc {
+
+// Owning device allocation (cudaMalloc / cudaFree), grown on demand.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    void alloc(size_t b) {
+        release();
+        if (b == 0) b = 16;
+        E8QC_CUDA(cudaMalloc(&p, b));
+        bytes = b;
+    }
+    void ensure(size_t b) {
+        if (b > bytes) alloc(b);
+    }
+    void upload(const void* src, size_t b, cudaStream_t s) {
+        alloc(b);
+        if (b) E8QC_CUDA(cudaMemcpyAsync(p, src, b, cudaMemcpyHostToDevice, s));
+    }
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
+// Scratch the search paths reuse across calls (one per index; calls on an
+// index are serialised). Counters used by last-CTA-done merges are zeroed at
+// allocation and reset by the kernels themselves.
+struct Workspace {
+    int device = 0;
+    DevBuf rq;  // nq*pd rotated queries
+    size_t rq_cap = 0;
+    // plain path
+    DevBuf keys, probes, probe_d2, tile_off, route_counter, total_tiles;
+    size_t route_cap = 0;
+    DevBuf part_d, part_id, scan_counter;
+    size_t scan_cap = 0;
+    // batched path
+    DevBuf b_keys, b_probes, b_pd2, b_cnt, b_off, b_items, b_pairs, b_part_d, b_part_id,
+        b_queue, b_nitems, b_scratch;
+    size_t b_q_cap = 0, b_pair_cap = 0, b_item_cap = 0, b_nlist_cap = 0, b_part_cap = 0;
+
+    void ensure_queries(size_t nq, size_t pd) {
+        if (nq * pd > rq_cap) {
+            rq.alloc(nq * pd * sizeof(float));
+            rq_cap = nq * pd;
+        }
+    }
+    void ensure_route(size_t nlist) {
+        if (nlist <= route_cap) return;
+        keys.alloc(nlist * 8);
+        probes.alloc(nlist * 4);
+        probe_d2.alloc(nlist * 4);
+        tile_off.alloc((nlist + 1) * 4);
+        route_counter.alloc(4);
+        total_tiles.alloc(4);
+        E8QC_CUDA(cudaMemset(route_counter.p, 0, 4));
+        route_cap = nlist;
+    }
+    void ensure_scan(size_t grid) {
+        if (grid <= scan_cap) return;
+        part_d.alloc(grid * kMaxK * 4);
+        part_id.alloc(grid * kMaxK * 4);
+        scan_counter.alloc(4);
+        E8QC_CUDA(cudaMemset(scan_counter.p, 0, 4));
+        scan_cap = grid;
+    }
+};
+
+// Batched search over nq rotated queries (batched.cu). k_arr / np_arr are
+// optional per-query device arrays (NULL = uniform k / nprobe). Output rows
+// are out_stride wide. Returns the number of kernels launched.
+int batched_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq,
+                   const uint32_t* k_arr, const uint32_t* np_arr, size_t k, size_t nprobe,
+                   size_t out_stride, uint32_t* out_ids, float* out_d, size_t max_tiles,
+                   cudaStream_t s);
+
+}  // namespace e8qc

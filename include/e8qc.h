@@ -1,0 +1,130 @@
+/* e8qc.h -- C ABI of the B200 (sm_100a) E8Q IVF search library (libe8qcuda.so).
+ *
+ * Plain C types only: pointers, sizes, status codes. No exception crosses this
+ * boundary; every function returns E8QC_OK (0) or a negative E8QC_E* code and
+ * leaves a message in e8qc_last_error() (thread-local).
+ *
+ * Memory: the index owns all of its device memory. Buffers passed in are the
+ * caller's and may be HOST or DEVICE pointers (device pointers must belong to
+ * the index's device; the library tells them apart with
+ * cudaPointerGetAttributes). Host buffers are copied in/out inside the call.
+ * `stream` is a cudaStream_t passed as void* (NULL = the legacy default
+ * stream); calls return after the results are in the caller's buffers.
+ *
+ * Threading: an index may be shared by host threads; calls on one index are
+ * serialised internally (the index owns one search workspace).
+ *
+ * Reference interfaces replaced (paths in the reference project):
+ *   python_bindings/e8q_bindings.cpp:22-344   E8qIndex pybind11 class
+ *   include/e8qlib/index/e8q.hpp:121-187      E8qIndex C++ class
+ *   include/e8qlib/quantization/e8q_codec.hpp:48-146  codec helpers
+ */
+#ifndef E8QC_H
+#define E8QC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define E8QC_OK 0
+#define E8QC_EINVAL -1   /* bad argument: std::invalid_argument -> ValueError */
+#define E8QC_ESTATE -2   /* wrong state (not built, ...): std::runtime_error */
+#define E8QC_ECUDA -3    /* CUDA runtime error */
+#define E8QC_ENOMEM -4   /* device or host allocation failed */
+#define E8QC_ERANGE -5   /* unknown id: std::out_of_range / invalid_argument */
+#define E8QC_EIO -6      /* file I/O or format error */
+#define E8QC_ETIMEOUT -7 /* a bounded device wait gave up */
+
+/* Search modes. PLAIN is the drop-in: one query per launch sequence
+ * (rotate -> route -> streaming scan -> top-k), every candidate of every probed
+ * list scored exactly. BATCHED groups a whole query batch by probed list and
+ * runs the persistent work-queue kernel (same estimator, same results within
+ * fp32 rounding). */
+#define E8QC_MODE_PLAIN 0
+#define E8QC_MODE_BATCHED 1
+
+/* Maximum top-k (include/e8qlib/index/e8q.hpp:44 kMaxK). */
+#define E8QC_MAX_K 128
+
+typedef struct e8qc_index e8qc_index;
+
+/* Per-call counters; mirrors e8qlib::SearchStats (include/e8qlib/index/e8q.hpp:55-62)
+ * plus device timings (CUDA events, microseconds summed over the call). */
+typedef struct e8qc_stats {
+    uint64_t candidates; /* vectors scored */
+    uint64_t survivors;  /* vectors that reached the exact estimator (all, in plain mode) */
+    double rotate_us;
+    double route_us;
+    double scan_us;
+    double refine_us;
+    uint64_t launches;   /* kernels this library launched for the call */
+} e8qc_stats;
+
+typedef struct e8qc_info {
+    uint64_t dim, padded_dim, n, nlist, memory_bytes;
+    int32_t nbits, device, built, disable_prune;
+    float prune_alpha;
+} e8qc_info;
+
+/* ---- errors / library ---------------------------------------------------- */
+const char* e8qc_last_error(void);
+int e8qc_version(void);
+
+/* ---- codec (include/e8qlib/quantization/e8q_codec.hpp) -------------------- */
+/* BranchLevels(bits, branch) (e8q_codec.hpp:50-52): 2^bits doubles. */
+int e8qc_branch_levels(int bits, int branch, double* out);
+/* FixedScale(bits) (e8q_codec.hpp:48). */
+int e8qc_fixed_scale(int bits, double* out);
+/* EncodeVectorAtScale(unit, padded_dim, bits, FixedScale(bits)) for n vectors
+ * on the GPU (e8q_codec.hpp:90-100). unit: n*padded_dim floats; digits:
+ * n*(padded_dim/8)*8 uint16; branch: n*(padded_dim/8) uint8. Bit-exact. */
+int e8qc_encode(int device, int bits, const float* unit, size_t n, size_t padded_dim,
+                uint16_t* digits, uint8_t* branch, void* stream);
+/* FhtKac4Rotator(dim, seed).Rotate for n rows (include/e8qlib/utils/rotator.hpp:17-42)
+ * on the GPU: src n*dim floats -> dst n*padded_dim floats. Bit-exact. */
+int e8qc_rotate(int device, size_t dim, uint64_t seed, const float* src, size_t n, float* dst,
+                void* stream);
+
+/* ---- E8Q index (python_bindings/e8q_bindings.cpp, index/e8q.hpp) ---------- */
+/* E8qIndex(dim, nbits, seed) (e8q_bindings.cpp:24-32): nbits in [1, 13]. */
+int e8qc_e8q_create(int device, size_t dim, int nbits, uint64_t seed, e8qc_index** out);
+int e8qc_e8q_destroy(e8qc_index* idx);
+/* E8qIndex::Build (e8q.hpp:123-134; e8q_bindings.cpp:34-72). data n*dim,
+ * centroids nlist*dim, cluster_ids n (each < nlist). Encoding runs on the GPU
+ * with codes bit-exact to the reference encoder. */
+int e8qc_e8q_build(e8qc_index* idx, const float* data, size_t n, const float* centroids,
+                   size_t nlist, const uint32_t* cluster_ids, float prune_alpha, void* stream);
+/* E8qIndex::Search for nq queries (e8q.hpp:139-143; e8q_bindings.cpp:74-169):
+ * out_ids / out_dists nq*k, ascending (distance, id); unused slots are
+ * UINT32_MAX / +inf. 0 < k <= E8QC_MAX_K, nprobe > 0 (clamped to nlist). */
+int e8qc_e8q_search(e8qc_index* idx, const float* queries, size_t nq, size_t k, size_t nprobe,
+                    int mode, uint32_t* out_ids, float* out_dists, e8qc_stats* stats,
+                    void* stream);
+/* Serving form: per-query k[i] and nprobe[i]; output row i holds k[i] results
+ * padded to k_max with UINT32_MAX / +inf. Uses the batched kernel. */
+int e8qc_e8q_search_ragged(e8qc_index* idx, const float* queries, size_t nq,
+                           const uint32_t* k, const uint32_t* nprobe, size_t k_max,
+                           uint32_t* out_ids, float* out_dists, e8qc_stats* stats,
+                           void* stream);
+/* E8qIndex::Estimate (e8q.hpp:151-152): estimated squared L2 of stored id. */
+int e8qc_e8q_estimate(e8qc_index* idx, const float* query, uint32_t id, float* out);
+/* E8qIndex::SetDisablePrune / SetPruneAlpha (e8q.hpp:173-180). The GPU paths
+ * score every candidate exactly; the flags are kept and reported. */
+int e8qc_e8q_set_disable_prune(e8qc_index* idx, int on);
+int e8qc_e8q_set_prune_alpha(e8qc_index* idx, float alpha);
+int e8qc_e8q_info(const e8qc_index* idx, e8qc_info* out);
+/* Copy the global ids, cluster-major (n entries), to a host buffer. */
+int e8qc_e8q_get_ids(const e8qc_index* idx, uint32_t* out);
+/* Export the per-vector lattice codes (cluster-major, the order of
+ * e8qc_e8q_get_ids) to host buffers: digits n*B*8 uint16, branch n*B uint8,
+ * g1 n, h3 n (any may be NULL). B = padded_dim/8. */
+int e8qc_e8q_export_codes(const e8qc_index* idx, uint16_t* digits, uint8_t* branch, float* g1,
+                          float* h3);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
