@@ -1,0 +1,414 @@
+#!/usr/bin/env python
+"""E8Q IVF search on B200 -- benchmark (one JSON line on rank 0).
+
+Workload (N=1 headline): 1M x 960-d float32 base drawn on the GPU from a
+seeded 1,024-component Gaussian mixture (centres N(0, diag(lambda)), members
+centre + 0.4 N(0, diag(lambda)), lambda_i ~ i^-0.5 normalised to mean 1; the
+sqrt(lambda) scaling applies to both draws), cluster_ids = generating
+component, centroids = per-list means; 10,240 queries from the same mixture;
+E8Q nbits=6 (the lowest rate whose recall@10 clears 0.95 on this mixture),
+k=10, nprobe=64; one step = one batch of 4,096 queries through the search
+path. Synthetic data stands in for the public corpora (no network).
+
+  value  : QPS with queries already in HBM (E8qIndex.search_ptr), CUDA events
+           on the launching stream, max over ranks; --gpus N runs N replicas
+           (the index fits one GPU; no data-path collective), scaling "weak".
+  e2e    : the same QPS through E8qIndex.search(numpy) with pinned host query
+           buffers: H2D of the queries and D2H of ids+dists inside the timing.
+  roofline: the dominant scan kernel, algorithmic bytes (codes + g1/h3 of every
+           scored candidate) per launch / CUDA-event launch time, against the
+           measured HBM copy bandwidth.
+  cpu_baseline: the reference's own CPU search (compiled from its sources into
+           oracle/_ref), all host cores, a bounded sample of the same workload.
+
+--impl reference times that reference CPU search as the measured arm.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "e8q-artifact_b200"))
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--path", choices=["plain", "batched"], default="plain")
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--dim", type=int, default=960)
+    ap.add_argument("--nlist", type=int, default=1024)
+    ap.add_argument("--nbits", type=int, default=6)
+    ap.add_argument("--k", type=int, default=10)
+    ap.add_argument("--nprobe", type=int, default=64)
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--pool", type=int, default=10240)
+    ap.add_argument("--gt", type=int, default=1000, help="queries with FP64 ground truth")
+    ap.add_argument("--plain-batch", type=int, default=1024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--seed", type=int, default=0)
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+def workload_name(a):
+    return (f"E8Q IVF search, {a.n // 1000}k x {a.dim}-d Gaussian mixture ({a.nlist} lists, "
+            f"lambda_i ~ i^-0.5), nbits={a.nbits}, k={a.k}, nprobe={a.nprobe}, "
+            f"query batch {a.batch}")
+
+
+def gen_data(a, device, rank):
+    """The mixture on `device` (torch), seeded; queries differ per rank."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(1000 + a.seed)
+    lam = torch.arange(1, a.dim + 1, device=device, dtype=torch.float64) ** -0.5
+    lam = lam / lam.mean()
+    s = lam.sqrt().float()
+    cen = torch.randn(a.nlist, a.dim, generator=g, device=device) * s
+    lab = torch.randint(0, a.nlist, (a.n,), generator=g, device=device)
+    x = torch.empty(a.n, a.dim, device=device)
+    step = 1 << 18
+    for i in range(0, a.n, step):
+        j = min(a.n, i + step)
+        x[i:j] = cen[lab[i:j]] + 0.4 * torch.randn(j - i, a.dim, generator=g, device=device) * s
+    cm = torch.zeros(a.nlist, a.dim, device=device, dtype=torch.float64)
+    cm.index_add_(0, lab, x.double())
+    cnt = torch.bincount(lab, minlength=a.nlist).clamp_min(1).double()
+    cm = (cm / cnt[:, None]).float()
+    gq = torch.Generator(device=device)
+    gq.manual_seed(2000 + a.seed + 7919 * rank)
+    lq = torch.randint(0, a.nlist, (a.pool,), generator=gq, device=device)
+    q = cen[lq] + 0.4 * torch.randn(a.pool, a.dim, generator=gq, device=device) * s
+    return x.contiguous(), cm.contiguous(), lab.to(torch.int32).contiguous(), q.contiguous()
+
+
+def ground_truth(x, q, k):
+    """FP64 brute-force top-k over the raw vectors."""
+    import torch
+
+    xd = x.double()
+    xn = (xd * xd).sum(1)
+    out = []
+    for i in range(0, q.shape[0], 256):
+        qd = q[i:i + 256].double()
+        d = (qd * qd).sum(1, keepdim=True) + xn[None, :] - 2.0 * qd @ xd.T
+        out.append(torch.topk(d, k, dim=1, largest=False).indices)
+    return torch.cat(out).cpu().numpy()
+
+
+def recall_at(ids, gt, k=10):
+    hit = 0
+    for r, g in zip(ids[:, :k], gt[:, :k]):
+        hit += len(set(r.tolist()) & set(g.tolist()))
+    return hit / (gt.shape[0] * k)
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.p = None
+        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
+                                 else ".", f".clocks_{os.getpid()}_{dev}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap,utilization.gpu",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p:
+            time.sleep(0.15)
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.p or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in open(self.path):
+            parts = [t.strip() for t in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), parts[3:7], float(parts[7])))
+            except ValueError:
+                continue
+        os.remove(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        busy = [r for r in rows if r[3] > 0] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in busy for i, v in enumerate(r[2]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in busy), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(busy)}
+
+
+def cpu_baseline(a, x_host, cm_host, lab_host, q_host, gt, steps=None, warmup=None):
+    """The reference's own CPU search on this host, all cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    E = O.ref_module()
+    if E is None:
+        return None
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    ref = E.E8qIndex(a.dim, a.nbits, a.seed)
+    ref.build(x_host, cm_host, lab_host.astype(np.uint32), num_threads=cores)
+    build_s = time.perf_counter() - t0
+    out = {"cores": cores, "build_s": round(build_s, 2)}
+    sample = min(2048, q_host.shape[0])
+    qs = q_host[:sample]
+    ref.search(qs[:64], a.k, a.nprobe, cores)
+    t0 = time.perf_counter()
+    ids, _ = ref.search(qs, a.k, a.nprobe, cores)
+    pruned_qps = sample / (time.perf_counter() - t0)
+    out["pruned_qps"] = pruned_qps
+    out["pruned_recall"] = recall_at(ids[:gt.shape[0]], gt[:min(sample, gt.shape[0])], a.k)
+    ref.set_disable_prune(True)
+    ps = min(512, sample)
+    t0 = time.perf_counter()
+    ids_p, _ = ref.search(qs[:ps], a.k, a.nprobe, cores)
+    out["plain_qps"] = ps / (time.perf_counter() - t0)
+    out["plain_recall"] = recall_at(ids_p, gt[:ps], a.k)
+    ref.set_disable_prune(False)
+    out["ref"] = ref
+    return out
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    if a.impl == "reference":
+        return run_reference(a, rank, world, dist)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import e8qlib
+
+    pk, pk_kind = peaks()
+    x, cm, lab, q = gen_data(a, dev, rank)
+    gt = ground_truth(x, q[:a.gt], a.k)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    idx = e8qlib.E8qIndex(a.dim, a.nbits, a.seed, device=local)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    idx.build_ptr(x.data_ptr(), a.n, cm.data_ptr(), a.nlist, lab.data_ptr(), 0.0, sp)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+
+    nb = a.batch if a.path == "batched" else a.plain_batch
+    out_ids = torch.empty(nb, a.k, dtype=torch.int32, device=dev)
+    out_d = torch.empty(nb, a.k, dtype=torch.float32, device=dev)
+    nbat = max(1, a.pool // nb)
+
+    def step(i, mode, b=nb):
+        qi = q[(i % nbat) * b:(i % nbat) * b + b]
+        return idx.search_ptr(qi.data_ptr(), b, a.k, a.nprobe, out_ids.data_ptr(), out_d.data_ptr(),
+                              mode, sp)
+
+    # recall of the measured path on the ground-truth queries
+    rec_ids = np.zeros((a.gt, a.k), np.uint32)
+    for i in range(0, a.gt, nb):
+        b = min(nb, a.gt - i)
+        idx.search_ptr(q[i:i + b].data_ptr(), b, a.k, a.nprobe, out_ids.data_ptr(), out_d.data_ptr(),
+                       a.path, sp)
+        torch.cuda.synchronize()
+        rec_ids[i:i + b] = out_ids[:b].cpu().numpy().view(np.uint32)
+    recall = recall_at(rec_ids, gt, a.k)
+
+    for i in range(a.warmup):
+        step(i, a.path)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for i in range(a.steps):
+            launches += step(a.warmup + i, a.path)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        dist.barrier()
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    total_q = a.steps * nb * world
+    value = total_q / (ms / 1000.0)
+
+    # roofline of the dominant kernel: profiled pass (events around each scan)
+    idx.profile_start()
+    for i in range(min(a.steps, 4)):
+        step(i, a.path)
+    torch.cuda.synchronize()
+    prof = idx.profile_stop()
+    algo_per_launch = prof["algo_bytes"] / max(1, prof["scan_launches"])
+    t_launch = prof["scan_ms"] / max(1, prof["scan_launches"]) / 1000.0
+    achieved = algo_per_launch / t_launch / 1e9 if t_launch > 0 else 0.0
+    peak = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None,
+                "kernel": "scan_plain_kernel" if a.path == "plain" else "batched scan",
+                "algo_bytes_per_launch": int(algo_per_launch),
+                "launch_us": round(t_launch * 1e6, 2), "peak_kind": pk_kind}
+
+    # e2e through the public numpy API with pinned host queries
+    qh = torch.empty(a.pool, a.dim, dtype=torch.float32, pin_memory=True)
+    qh.copy_(q.cpu())
+    qn = qh.numpy()
+    for i in range(2):
+        idx.search(qn[:nb], a.k, a.nprobe, mode=a.path)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(a.steps):
+        j = i % nbat
+        idx.search(qn[j * nb:(j + 1) * nb], a.k, a.nprobe, mode=a.path)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": round(total_q / (e2e_ms / 1000.0), 1), "unit": "QPS",
+           "h2d_bytes_per_step": nb * a.dim * 4, "d2h_bytes_per_step": nb * a.k * 8}
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        xh = x.cpu().numpy()
+        cb = cpu_baseline(a, xh, cm.cpu().numpy(), lab.cpu().numpy(), q.cpu().numpy(), gt)
+        if cb is not None:
+            cb.pop("ref", None)
+            cpu = {"value": round(cb["pruned_qps"], 1), "unit": "QPS", "cores": cb["cores"],
+                   "kind": "reference",
+                   "sample": (f"2048 queries of this workload through the reference E8qIndex.search "
+                              f"(production pruned path, {cb['cores']} threads); plain scan "
+                              f"(set_disable_prune) {cb['plain_qps']:.1f} QPS on 512 queries"),
+                   "recall_at_10": round(cb["pruned_recall"], 4),
+                   "plain_qps": round(cb["plain_qps"], 1), "plain_recall_at_10": round(cb["plain_recall"], 4),
+                   "build_s": cb["build_s"]}
+
+    line = {
+        "metric": "QPS@recall10>=0.95 (E8Q IVF search, 1 query batch per step)",
+        "value": round(value, 1), "unit": "QPS", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (u8 lattice codes)",
+        "data": "synthetic (seeded Gaussian mixture generated on the GPU)",
+        "config": {"workload": workload_name(a), "n": a.n, "dim": a.dim, "nlist": a.nlist,
+                   "nbits": a.nbits, "k": a.k, "nprobe": a.nprobe, "query_batch": nb,
+                   "path": a.path, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (codes %.0f MB > 126 MB)" % (idx.memory_bytes / 1e6)},
+        "recall_at_10": round(recall, 4), "build_s": round(build_s, 2),
+        "clocks": clk.summary(), "gpu_launches": int(launches), "roofline": roofline,
+        "e2e": e2e, "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_reference(a, rank, world, dist):
+    """--impl reference: the reference's CPU search as the measured arm
+    (rank 0 only under torchrun)."""
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    import torch
+
+    dev = torch.device("cuda", 0) if torch.cuda.is_available() else torch.device("cpu")
+    x, cm, lab, q = gen_data(a, dev, 0)
+    gt = ground_truth(x, q[:a.gt], a.k)
+    xh, cmh, labh, qh = (t.cpu().numpy() for t in (x, cm, lab, q))
+    del x
+    cb = cpu_baseline(a, xh, cmh, labh, qh, gt)
+    if cb is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (make -C oracle ref)"}))
+        return
+    ref = cb.pop("ref")
+    cores = cb["cores"]
+    nb = 1024
+    nbat = max(1, a.pool // nb)
+    for i in range(a.warmup):
+        ref.search(qh[(i % nbat) * nb:(i % nbat + 1) * nb], a.k, a.nprobe, cores)
+    t0 = time.perf_counter()
+    for i in range(a.steps):
+        j = (a.warmup + i) % nbat
+        ref.search(qh[j * nb:(j + 1) * nb], a.k, a.nprobe, cores)
+    sec = time.perf_counter() - t0
+    value = a.steps * nb / sec
+    line = {"impl": "reference", "metric": "QPS@recall10>=0.95 (E8Q IVF search, 1 query batch per step)",
+            "value": round(value, 1), "unit": "QPS", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": round(sec * 1000 / a.steps, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32", "data": "synthetic (same seeded mixture)",
+            "config": {"workload": workload_name(a) + " (reference CPU, production pruned search)",
+                       "n": a.n, "dim": a.dim, "nlist": a.nlist, "nbits": a.nbits, "k": a.k,
+                       "nprobe": a.nprobe, "query_batch": nb},
+            "recall_at_10": round(cb["pruned_recall"], 4),
+            "cpu_baseline": {"value": round(value, 1), "unit": "QPS", "cores": cores, "kind": "reference",
+                             "sample": f"{nb} queries per step, {cores} threads, reference E8qIndex.search"},
+            "e2e": {"value": round(value, 1), "unit": "QPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "plain_qps": round(cb["plain_qps"], 1), "build_s": cb["build_s"]}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

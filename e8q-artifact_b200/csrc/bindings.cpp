@@ -189,6 +189,23 @@ class E8qIndex {
         return py::make_tuple(ids, dg, br, g1, h3);
     }
 
+    void profile_start() {
+        require("profile");
+        check(e8qc_e8q_profile(idx_, 1, nullptr));
+    }
+    py::dict profile_stop() {
+        require("profile");
+        e8qc_profile p{};
+        check(e8qc_e8q_profile(idx_, 0, &p));
+        py::dict d;
+        d["scan_launches"] = p.scan_launches;
+        d["scan_ms"] = p.scan_ms;
+        d["candidates"] = p.candidates;
+        d["algo_bytes"] = p.algo_bytes;
+        d["queries"] = p.queries;
+        return d;
+    }
+
     size_t dim() const { return dim_; }
     size_t nbits() const { return nbits_; }
     bool is_built() const { return built_; }
@@ -293,6 +310,8 @@ PYBIND11_MODULE(_e8qlib, m) {
         .def("set_disable_prune", &E8qIndex::set_disable_prune, py::arg("on"))
         .def("set_prune_alpha", &E8qIndex::set_prune_alpha, py::arg("alpha"))
         .def("export_codes", &E8qIndex::export_codes)
+        .def("profile_start", &E8qIndex::profile_start)
+        .def("profile_stop", &E8qIndex::profile_stop)
         .def_property_readonly("dim", &E8qIndex::dim)
         .def_property_readonly("nbits", &E8qIndex::nbits)
         .def_property_readonly("is_built", &E8qIndex::is_built)

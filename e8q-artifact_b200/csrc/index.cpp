@@ -18,6 +18,7 @@
 
 #include "e8qc.h"
 #include "internal.h"
+#include "scan_plain.h"
 #include "workspace.h"
 
 namespace e8qc {
@@ -93,14 +94,16 @@ struct e8qc_index {
     std::vector<uint32_t> sorted_tiles_prefix;  // prefix of list tile counts, largest first
 
     DevBuf signs, mean_rot, cen, cn2, tile_begin_d, list_len_d, codes, g1, h3, ids, tab,
-        list_of_tile, list_begin_d;
+        list_of_tile, list_begin_d, list_order;
     DevIndex view{};
     Workspace ws;
+    bool profiling = false;
+    e8qc_profile prof{};
 
     size_t memory_bytes() const {
         return signs.bytes + mean_rot.bytes + cen.bytes + cn2.bytes + tile_begin_d.bytes +
                list_len_d.bytes + codes.bytes + g1.bytes + h3.bytes + ids.bytes + tab.bytes +
-               list_of_tile.bytes + list_begin_d.bytes;
+               list_of_tile.bytes + list_begin_d.bytes + list_order.bytes;
     }
 };
 
@@ -147,24 +150,53 @@ void plain_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size_
                   uint32_t* ids_d, float* d_d, e8qc_stats* st, cudaStream_t s) {
     Workspace& ws = x->ws;
     ws.ensure_route(x->nlist);
-    const int grid = plain_scan_grid(x->bits);
+    // grid: one CTA per SM (the kernel fills an SM's shared memory), fewer
+    // when the largest possible probe set has fewer tiles than that
+    const ScanGeo geo = plain_scan_geo(x->view, 1536);
+    const size_t max_tiles = max_tiles_for(x, nprobe);
+    int sms = 148;
+    E8QC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device));
+    int grid = static_cast<int>(std::min<size_t>(max_tiles, static_cast<size_t>(sms)));
+    grid = std::max(grid, 1);
     ws.ensure_scan(static_cast<size_t>(grid));
     RouteWork rw{ws.keys.as<uint64_t>(), ws.probes.as<uint32_t>(), ws.probe_d2.as<float>(),
                  ws.tile_off.as<uint32_t>(), ws.route_counter.as<uint32_t>(),
                  ws.total_tiles.as<uint32_t>()};
-    ScanWork sw{ws.part_d.as<float>(), ws.part_id.as<uint32_t>(), ws.scan_counter.as<uint32_t>(), grid};
+    ScanWork sw{ws.part_d.as<float>(), ws.part_id.as<uint32_t>(), ws.scan_counter.as<uint32_t>(),
+                ws.err.as<uint32_t>(), grid};
+
     uint64_t launches = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::vector<uint32_t> probes;
+    if (x->profiling) {
+        E8QC_CUDA(cudaEventCreate(&e0));
+        E8QC_CUDA(cudaEventCreate(&e1));
+        probes.resize(nprobe);
+    }
     for (size_t i = 0; i < nq; ++i) {
         const float* rq = rq_all + i * x->pd;
         launches += launch_route_one(x->view, rq, static_cast<int>(nprobe), rw, s);
-        launches += launch_scan_plain(x->view, rq, rw, static_cast<int>(k), sw, ids_d + i * k,
-                                      d_d + i * k, s);
+        if (x->profiling) E8QC_CUDA(cudaEventRecord(e0, s));
+        launches += launch_scan_plain(x->view, rq, rw, static_cast<int>(nprobe), static_cast<int>(k), sw,
+                                      geo, ids_d + i * k, d_d + i * k, s);
+        if (x->profiling) {
+            E8QC_CUDA(cudaEventRecord(e1, s));
+            E8QC_CUDA(cudaMemcpyAsync(probes.data(), rw.probes, nprobe * 4, cudaMemcpyDeviceToHost, s));
+            E8QC_CUDA(cudaStreamSynchronize(s));
+            float ms = 0.0f;
+            E8QC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            uint64_t cand = 0;
+            for (uint32_t c : probes) cand += x->list_begin[c + 1] - x->list_begin[c];
+            x->prof.scan_launches += 1;
+            x->prof.scan_ms += ms;
+            x->prof.candidates += cand;
+            x->prof.algo_bytes += cand * (static_cast<uint64_t>(x->bits) * x->pd / 8 + 8);
+            x->prof.queries += 1;
+        }
     }
-    if (st) {
-        st->launches += launches;
-        uint64_t cand = 0;
-        (void)cand;
-    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (st) st->launches += launches;
 }
 
 }  // namespace
@@ -343,6 +375,14 @@ int e8qc_e8q_build(e8qc_index* x, const float* data, size_t n, const float* cent
         x->list_of_tile.upload(list_of_tile.data(), list_of_tile.size() * 4, s);
         x->list_begin_d.upload(x->list_begin.data(), x->list_begin.size() * 8, s);
         {
+            // batched work queue order: longest list first (LPT)
+            std::vector<uint32_t> order(nlist);
+            for (size_t c = 0; c < nlist; ++c) order[c] = static_cast<uint32_t>(c);
+            std::stable_sort(order.begin(), order.end(),
+                             [&](uint32_t a, uint32_t b) { return counts[a] > counts[b]; });
+            x->list_order.upload(order.data(), order.size() * 4, s);
+        }
+        {
             // refine tables: level / sqrt(pd) as float (src/quantization/e8q_codec.cpp:933-946)
             const int q = 1 << x->bits;
             std::vector<float> tab(2 * static_cast<size_t>(q));
@@ -389,6 +429,7 @@ int e8qc_e8q_build(e8qc_index* x, const float* data, size_t n, const float* cent
         v.h3 = x->h3.as<float>();
         v.ids = x->ids.as<uint32_t>();
         v.tab = x->tab.as<float>();
+        v.list_order = x->list_order.as<uint32_t>();
         const DevEncTables& et = enc_tables_device(x->device, x->bits);
         BuildEncodeArgs a{};
         a.base = data_d;
@@ -443,7 +484,7 @@ int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, si
         if (stats) E8QC_CUDA(cudaEventRecord(ev[2], s));
         if (!ids_dev) E8QC_CUDA(cudaMemcpyAsync(out_ids, ids_d, nq * k * 4, cudaMemcpyDeviceToHost, s));
         if (out_dists && !d_dev) E8QC_CUDA(cudaMemcpyAsync(out_dists, d_d, nq * k * 4, cudaMemcpyDeviceToHost, s));
-        E8QC_CUDA(cudaStreamSynchronize(s));
+        x->ws.check_error(s);
         if (stats) {
             float a = 0, b = 0;
             E8QC_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
@@ -501,7 +542,7 @@ int e8qc_e8q_search_ragged(e8qc_index* x, const float* queries, size_t nq, const
                                    np_max, k_max, ids_d, d_d, max_tiles_for(x, np_max), s);
         if (!ids_dev) E8QC_CUDA(cudaMemcpyAsync(out_ids, ids_d, nq * k_max * 4, cudaMemcpyDeviceToHost, s));
         if (out_dists && !d_dev) E8QC_CUDA(cudaMemcpyAsync(out_dists, d_d, nq * k_max * 4, cudaMemcpyDeviceToHost, s));
-        E8QC_CUDA(cudaStreamSynchronize(s));
+        x->ws.check_error(s);
         if (stats) stats->launches = launches;
     });
 }
@@ -562,6 +603,20 @@ int e8qc_e8q_info(const e8qc_index* x, e8qc_info* out) {
         out->built = x->built ? 1 : 0;
         out->disable_prune = x->disable_prune ? 1 : 0;
         out->prune_alpha = x->prune_alpha;
+    });
+}
+
+int e8qc_e8q_profile(e8qc_index* x, int enable, e8qc_profile* out) {
+    return guarded([&] {
+        if (x == nullptr) fail(E8QC_EINVAL, "null index");
+        std::lock_guard<std::mutex> lock(x->mu);
+        if (enable) {
+            x->prof = e8qc_profile{};
+            x->profiling = true;
+        } else {
+            x->profiling = false;
+            if (out) *out = x->prof;
+        }
     });
 }
 

@@ -98,6 +98,7 @@ struct DevIndex {
     const float* h3;             // ntiles*32
     const uint32_t* ids;         // ntiles*32, UINT32_MAX on padding lanes
     const float* tab;            // [2][2^bits] level/sqrt(pd) refine tables
+    const uint32_t* list_order;  // nlist list ids, longest list first
 };
 
 inline int code_chunks(int pd, int bits) { return (pd / 8 * 8 * bits + 127) / 128; }
@@ -128,11 +129,9 @@ struct ScanWork {
     float* part_d;      // grid*kmax
     uint32_t* part_id;  // grid*kmax
     uint32_t* counter;  // self-resetting
+    uint32_t* err;      // device error word (bounded waits that gave up)
     int grid;
 };
-int plain_scan_grid(int bits);
-int launch_scan_plain(const DevIndex& ix, const float* rq, const RouteWork& rw, int k,
-                      const ScanWork& sw, uint32_t* out_ids, float* out_d, cudaStream_t s);
 
 // Build kernels.
 int launch_mean(const float* x, size_t n, int dim, float* mu_out, cudaStream_t s);

@@ -1,0 +1,377 @@
+// Plain one-query streaming scan (the drop-in search path).
+//
+// Every vector of every probed list gets the exact estimator
+//   dist = (d2 + h3) - 2*g1*S,   S = sum_i q[i] * level[branch][digit_i] / sqrt(D)
+// (src/simd/e8q_search_generic.cpp:58-66 with d2 folded as at :189) and enters
+// a warp top-k; CTAs merge into per-CTA lists and the last CTA to finish
+// merges those into the answer.
+//
+// Data movement: each warp owns a two-stage ring in shared memory and pulls
+// its tiles' code bytes with cp.async.bulk (one bulk copy per segment of a
+// 32-vector tile, completion on an mbarrier), so every warp keeps up to two
+// segments in flight while it decodes. Lane l decodes vector l of the tile:
+// chunk c of lane l sits at [c][l] (16 bytes), so the lanes' reads of one
+// chunk row are 512 contiguous bytes. Level values come from a shared-memory
+// table replicated once per lane (bank-conflict-free gathers).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "device_common.cuh"
+#include "internal.h"
+#include "scan_plain.h"
+#include "tma.cuh"
+
+namespace e8qc {
+
+namespace {
+
+__device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
+
+constexpr int kMaxWarps = 32;
+constexpr int kToffCap = 1024;  // tile offsets cached in shared memory
+
+__device__ __forceinline__ float lds_f32(uint32_t addr) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+    return v;
+}
+
+// log2 of the byte stride between consecutive level entries: REP per-lane
+// copies of 4 bytes each.
+__host__ __device__ constexpr int entry_shift(int bits) {
+    return table_rep(bits) == 32 ? 7 : table_rep(bits) == 16 ? 6 : table_rep(bits) == 8 ? 5
+         : table_rep(bits) == 4 ? 4 : table_rep(bits) == 2 ? 3 : 2;
+}
+
+// Field of WIDTH bits at bit offset OFF of w[], returned already shifted to a
+// byte offset into the table (left by SH = entry_shift).
+template <int OFF, int WIDTH, int SH>
+__device__ __forceinline__ uint32_t field_xs(const uint32_t* w) {
+    constexpr int wi = OFF >> 5, sh = OFF & 31;
+    constexpr uint32_t m = ((1u << WIDTH) - 1u) << SH;
+    if constexpr (sh >= SH) {
+        return __funnelshift_r(w[wi], w[wi + 1], sh - SH) & m;
+    } else {
+        return (w[wi] << (SH - sh)) & m;
+    }
+}
+
+// One block: 8 digits (digit 7's LSB = parity of digits 0..6, its stored LSB
+// slot = branch) -> 8 level gathers from this lane's table copy -> 8 FMAs.
+template <int BITS, int OFF>
+__device__ __forceinline__ void block_fma(const uint32_t* w, uint32_t tb_addr, const float4 qa, const float4 qb,
+                                          float& acc) {
+    constexpr int SH = entry_shift(BITS);
+    constexpr uint32_t LSB = 1u << SH;
+    const uint32_t f0 = field_xs<OFF + 0 * BITS, BITS, SH>(w);
+    const uint32_t f1 = field_xs<OFF + 1 * BITS, BITS, SH>(w);
+    const uint32_t f2 = field_xs<OFF + 2 * BITS, BITS, SH>(w);
+    const uint32_t f3 = field_xs<OFF + 3 * BITS, BITS, SH>(w);
+    const uint32_t f4 = field_xs<OFF + 4 * BITS, BITS, SH>(w);
+    const uint32_t f5 = field_xs<OFF + 5 * BITS, BITS, SH>(w);
+    const uint32_t f6 = field_xs<OFF + 6 * BITS, BITS, SH>(w);
+    const uint32_t f7 = field_xs<OFF + 7 * BITS, BITS, SH>(w);
+    const uint32_t par = f0 ^ f1 ^ f2 ^ f3 ^ f4 ^ f5 ^ f6;      // bit SH = parity
+    const uint32_t d7 = (f7 & ~LSB) | (par & LSB);
+    const uint32_t base = tb_addr + ((f7 & LSB) << BITS);        // branch table
+    acc = __fmaf_rn(qa.x, lds_f32(base + f0), acc);
+    acc = __fmaf_rn(qa.y, lds_f32(base + f1), acc);
+    acc = __fmaf_rn(qa.z, lds_f32(base + f2), acc);
+    acc = __fmaf_rn(qa.w, lds_f32(base + f3), acc);
+    acc = __fmaf_rn(qb.x, lds_f32(base + f4), acc);
+    acc = __fmaf_rn(qb.y, lds_f32(base + f5), acc);
+    acc = __fmaf_rn(qb.z, lds_f32(base + f6), acc);
+    acc = __fmaf_rn(qb.w, lds_f32(base + d7), acc);
+}
+
+template <int BITS, int NBLK, int B0>
+struct BlockRun {
+    __device__ __forceinline__ static void run(const uint32_t* w, uint32_t tb_addr, const float4* sq4, int qblk,
+                                               float& acc0, float& acc1) {
+        if constexpr (B0 < NBLK) {
+            const float4 qa = sq4[2 * (qblk + B0)], qb = sq4[2 * (qblk + B0) + 1];
+            block_fma<BITS, B0 * 8 * BITS>(w, tb_addr, qa, qb, (B0 & 1) ? acc1 : acc0);
+            BlockRun<BITS, NBLK, B0 + 1>::run(w, tb_addr, sq4, qblk, acc0, acc1);
+        }
+    }
+};
+
+// Decode + accumulate NBLK consecutive blocks whose NCH chunks start at
+// `sbuf` (chunk-row major, 32 lanes per row); query blocks start at `qblk`.
+template <int BITS, int NBLK, int NCH>
+__device__ __forceinline__ void accumulate_blocks(const uint4* __restrict__ sbuf, int lane,
+                                                  const float4* __restrict__ sq4, int qblk, uint32_t tb_addr,
+                                                  float& acc0, float& acc1) {
+    uint32_t w[4 * NCH + 1];
+#pragma unroll
+    for (int c = 0; c < NCH; ++c) {
+        const uint4 v = sbuf[c * 32 + lane];
+        w[4 * c] = v.x;
+        w[4 * c + 1] = v.y;
+        w[4 * c + 2] = v.z;
+        w[4 * c + 3] = v.w;
+    }
+    w[4 * NCH] = 0;
+    BlockRun<BITS, NBLK, 0>::run(w, tb_addr, sq4, qblk, acc0, acc1);
+}
+
+// Largest p in [0, nprobe) with off[p] <= t (empty lists share offsets; the
+// largest such p is the list that holds tile t).
+__device__ __forceinline__ int find_probe(const uint32_t* off, int nprobe, uint32_t t) {
+    int lo = 0, hi = nprobe;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= t) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// CTA-wide merge of per-warp top-k lists into warp 0 (smem staging).
+__device__ void cta_merge(WarpTopK& top, float* sm_d, uint32_t* sm_id, int k) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    top.store(sm_d + warp * kMaxK, sm_id + warp * kMaxK, k);
+    __syncthreads();
+    if (warp == 0) {
+        for (int w2 = 1; w2 < nw; ++w2) {
+            for (int j0 = 0; j0 < k; j0 += 32) {
+                const int j = j0 + lane;
+                const bool ok = j < k;
+                const float dd = ok ? sm_d[w2 * kMaxK + j] : inf_f();
+                const uint32_t ii = ok ? sm_id[w2 * kMaxK + j] : 0xFFFFFFFFu;
+                top.offer_pair(dd, ii, ok && ii != 0xFFFFFFFFu);
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <int BITS>
+__global__ void __launch_bounds__(kMaxWarps * 32, 1) scan_plain_kernel(
+    DevIndex ix, const float* __restrict__ rq, RouteWork rw, int nprobe, int k, ScanWork sw, ScanGeo geo,
+    uint32_t* __restrict__ out_ids, float* __restrict__ out_d) {
+    constexpr int GBL = group_blocks(BITS), GCH = group_chunks(BITS);
+    constexpr int TCH = (64 * BITS + 127) / 128;
+    constexpr int Q = 1 << BITS;
+    constexpr int REP = table_rep(BITS);
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nw = blockDim.x >> 5, nt = blockDim.x;
+    const int pd = ix.pd;
+    // shared-memory carve (see scan_smem_bytes)
+    unsigned char* ring = smem;                                       // nw * 2 * seg_bytes
+    float* tabrep = reinterpret_cast<float*>(ring + nw * 2 * geo.seg_bytes);  // 2*Q*REP
+    float* sq = tabrep + 2 * Q * REP;                                 // pd
+    uint32_t* soff = reinterpret_cast<uint32_t*>(sq + pd);           // kToffCap + 1
+    float* sm_d = reinterpret_cast<float*>(soff + kToffCap + 1);      // nw * kMaxK
+    uint32_t* sm_id = reinterpret_cast<uint32_t*>(sm_d + nw * kMaxK);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(
+        (reinterpret_cast<uintptr_t>(sm_id + nw * kMaxK) + 7) & ~uintptr_t(7));  // nw * 2
+    __shared__ bool s_last;
+
+    for (int i = tid; i < pd; i += nt) sq[i] = rq[i];
+    for (int e = tid; e < 2 * Q * REP; e += nt) tabrep[e] = ix.tab[e / REP];
+    const bool off_in_smem = nprobe <= kToffCap;
+    if (off_in_smem)
+        for (int i = tid; i <= nprobe; i += nt) soff[i] = __ldcg(rw.tile_off + i);
+    if (lane == 0) {
+        mbar_init(&bars[2 * warp], 1);
+        mbar_init(&bars[2 * warp + 1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    const uint32_t* off = off_in_smem ? soff : rw.tile_off;
+    const float4* sq4 = reinterpret_cast<const float4*>(sq);
+    // byte address of this lane's table copy (entry e at e*REP*4 + copy*4)
+    const uint32_t tb_addr = smem_addr(tabrep) + static_cast<uint32_t>(lane % REP) * 4u;
+    const uint32_t T = __ldcg(rw.total_tiles);
+    // tiles dealt round-robin over CTAs, then over the CTA's warps
+    const uint32_t G = gridDim.x;
+    const uint32_t per_cta = T > blockIdx.x ? (T - blockIdx.x + G - 1) / G : 0;
+    const uint32_t ntile_w = per_cta > static_cast<uint32_t>(warp)
+                                 ? (per_cta - warp + nw - 1) / static_cast<uint32_t>(nw) : 0;
+    const int nseg = geo.nseg;
+    const uint32_t J = ntile_w * static_cast<uint32_t>(nseg);
+    unsigned char* my_ring = ring + warp * 2 * geo.seg_bytes;
+    auto tile_of = [&](uint32_t j) { return (static_cast<uint32_t>(warp) + (j / nseg) * nw) * G + blockIdx.x; };
+
+    auto seg_range = [&](int seg, int& c0, int& cnt) {
+        if (geo.tail && seg == nseg - 1) {
+            c0 = geo.ng * GCH;
+            cnt = TCH;
+        } else {
+            const int g0 = seg * geo.U;
+            const int g1 = min(geo.ng, g0 + geo.U);
+            c0 = g0 * GCH;
+            cnt = (g1 - g0) * GCH;
+        }
+    };
+    auto issue = [&](uint32_t j) {
+        const uint32_t t = tile_of(j);
+        const int seg = static_cast<int>(j % nseg);
+        const int p = find_probe(off, nprobe, t);
+        const uint32_t list = __ldcg(rw.probes + p);
+        const uint32_t gt = __ldg(ix.tile_begin + list) + (t - off[p]);
+        int c0, cnt;
+        seg_range(seg, c0, cnt);
+        const int st = static_cast<int>(j & 1);
+        const uint32_t bytes = static_cast<uint32_t>(cnt) * 512u;
+        mbar_arrive_expect_tx(&bars[2 * warp + st], bytes);
+        bulk_g2s(my_ring + st * geo.seg_bytes, ix.codes + (static_cast<size_t>(gt) * ix.nch + c0) * 32, bytes,
+                 &bars[2 * warp + st]);
+    };
+
+    WarpTopK top;
+    top.init(k);
+    if (lane == 0) {
+        if (J > 0) issue(0);
+        if (J > 1) issue(1);
+    }
+    uint32_t phase[2] = {0u, 0u};
+    float acc0 = 0.0f, acc1 = 0.0f;
+    bool ok = true;
+    for (uint32_t j = 0; j < J; ++j) {
+        const int st = static_cast<int>(j & 1);
+        const bool got = mbar_wait_bounded(&bars[2 * warp + st], phase[st]);
+        phase[st] ^= 1u;
+        if (!__all_sync(kFull, got)) {
+            ok = false;
+            break;
+        }
+        const int seg = static_cast<int>(j % nseg);
+        const uint4* sbuf = reinterpret_cast<const uint4*>(my_ring + st * geo.seg_bytes);
+        if (geo.tail && seg == nseg - 1) {
+            accumulate_blocks<BITS, 8, TCH>(sbuf, lane, sq4, geo.ng * GBL, tb_addr, acc0, acc1);
+        } else {
+            const int g0 = seg * geo.U;
+            const int g1 = min(geo.ng, g0 + geo.U);
+            for (int g = g0; g < g1; ++g)
+                accumulate_blocks<BITS, GBL, GCH>(sbuf + (g - g0) * GCH * 32, lane, sq4, g * GBL, tb_addr, acc0,
+                                                  acc1);
+        }
+        __syncwarp();
+        if (lane == 0 && j + 2 < J) issue(j + 2);
+        if (seg == nseg - 1) {
+            const uint32_t t = tile_of(j);
+            const int p = find_probe(off, nprobe, t);
+            const uint32_t list = __ldcg(rw.probes + p);
+            const float d2 = __ldcg(rw.probe_d2 + p);
+            const uint32_t local = t - off[p];
+            const uint32_t gt = __ldg(ix.tile_begin + list) + local;
+            const bool valid = local * 32u + static_cast<uint32_t>(lane) < __ldg(ix.list_len + list);
+            const size_t slot = static_cast<size_t>(gt) * 32 + lane;
+            const float S = __fadd_rn(acc0, acc1);
+            const float g1 = __ldg(ix.g1 + slot), h3 = __ldg(ix.h3 + slot);
+            const float dist = __fmaf_rn(-__fmul_rn(2.0f, g1), S, __fadd_rn(d2, h3));
+            top.offer(dist, valid, [&] { return __ldg(ix.ids + slot); });
+            acc0 = 0.0f;
+            acc1 = 0.0f;
+        }
+    }
+    if (!ok && lane == 0) atomicOr(sw.err, kErrWaitTimeout);
+    cta_merge(top, sm_d, sm_id, k);
+    if (warp == 0) top.store(sw.part_d + static_cast<size_t>(blockIdx.x) * kMaxK,
+                             sw.part_id + static_cast<size_t>(blockIdx.x) * kMaxK, k);
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = atomicAdd(sw.counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // final merge: the CTA stages the partial lists in shared memory (the
+    // ring is free now) with coalesced loads, then each warp offers a share
+    top.init(k);
+    const int Gi = static_cast<int>(gridDim.x);
+    const int cap = (nw * 2 * geo.seg_bytes) / 8;  // entries per staging round
+    float* st_d = reinterpret_cast<float*>(ring);
+    uint32_t* st_i = reinterpret_cast<uint32_t*>(ring) + cap;
+    const int total = Gi * k;
+    for (int e0 = 0; e0 < total; e0 += cap) {
+        const int m = min(cap, total - e0);
+        __syncthreads();
+        for (int e = tid; e < m; e += nt) {
+            const int c = (e0 + e) / k, jj = (e0 + e) - c * k;
+            st_d[e] = __ldcg(sw.part_d + static_cast<size_t>(c) * kMaxK + jj);
+            st_i[e] = __ldcg(sw.part_id + static_cast<size_t>(c) * kMaxK + jj);
+        }
+        __syncthreads();
+        for (int e = warp * 32; e < m; e += nw * 32) {
+            const int i = e + lane;
+            const bool okj = i < m;
+            const float dd = okj ? st_d[i] : inf_f();
+            const uint32_t ii = okj ? st_i[i] : 0xFFFFFFFFu;
+            top.offer_pair(dd, ii, okj && ii != 0xFFFFFFFFu);
+        }
+    }
+    cta_merge(top, sm_d, sm_id, k);
+    if (warp == 0) top.store(out_d, out_ids, k);
+    if (tid == 0) *sw.counter = 0;
+}
+
+template <int BITS>
+int launch_bits(const DevIndex& ix, const float* rq, const RouteWork& rw, int nprobe, int k, const ScanWork& sw,
+                const ScanGeo& geo, uint32_t* out_ids, float* out_d, cudaStream_t s) {
+    const size_t smem = scan_smem_bytes(ix, geo);
+    // dynamic shared-memory opt-in, raised per device as needed
+    static size_t configured[64] = {};
+    int dev = 0;
+    E8QC_CUDA(cudaGetDevice(&dev));
+    if (configured[dev & 63] < smem) {
+        E8QC_CUDA(cudaFuncSetAttribute(scan_plain_kernel<BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem)));
+        configured[dev & 63] = smem;
+    }
+    scan_plain_kernel<BITS><<<sw.grid, geo.warps * 32, smem, s>>>(ix, rq, rw, nprobe, k, sw, geo, out_ids, out_d);
+    E8QC_CUDA(cudaGetLastError());
+    return 1;
+}
+
+}  // namespace
+
+ScanGeo plain_scan_geo(const DevIndex& ix, size_t max_seg_bytes) {
+    ScanGeo g{};
+    const int gbl = group_blocks(ix.bits), gch = group_chunks(ix.bits);
+    g.ng = ix.B / gbl;
+    g.tail = (ix.B % gbl) != 0 ? 1 : 0;
+    const int group_bytes = gch * 512;
+    const int tch = (64 * ix.bits + 127) / 128;
+    int U = static_cast<int>(max_seg_bytes / group_bytes);
+    if (U < 1) U = 1;
+    if (U > g.ng && g.ng > 0) U = g.ng;
+    g.U = U;
+    g.nseg = (g.ng + U - 1) / U + g.tail;
+    int seg_chunks = U * gch;
+    if (g.tail && tch > seg_chunks) seg_chunks = tch;
+    g.seg_bytes = ((seg_chunks * 512) + 127) & ~127;
+    // as many warps (<= 32) as the 227 KB shared-memory budget allows
+    g.warps = kMaxWarps;
+    while (g.warps > 4 && scan_smem_bytes(ix, g) > 225 * 1024) g.warps -= 4;
+    return g;
+}
+
+size_t scan_smem_bytes(const DevIndex& ix, const ScanGeo& geo) {
+    const int q = 1 << ix.bits;
+    size_t b = static_cast<size_t>(geo.warps) * 2 * geo.seg_bytes;
+    b += static_cast<size_t>(2) * q * table_rep(ix.bits) * 4;
+    b += static_cast<size_t>(ix.pd) * 4;
+    b += static_cast<size_t>(kToffCap + 1) * 4;
+    b += static_cast<size_t>(geo.warps) * kMaxK * 8;
+    b += 8 + static_cast<size_t>(geo.warps) * 2 * 8;
+    return b;
+}
+
+int launch_scan_plain(const DevIndex& ix, const float* rq, const RouteWork& rw, int nprobe, int k,
+                      const ScanWork& sw, const ScanGeo& geo, uint32_t* out_ids, float* out_d, cudaStream_t s) {
+    switch (ix.bits) {
+#define E8QC_CASE(b) \
+    case b: return launch_bits<b>(ix, rq, rw, nprobe, k, sw, geo, out_ids, out_d, s);
+        E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
+        E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
+        E8QC_CASE(13)
+#undef E8QC_CASE
+        default: fail(E8QC_EINVAL, "bits out of range");
+    }
+    return 0;
+}
+
+}  // namespace e8qc

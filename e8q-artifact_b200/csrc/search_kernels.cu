@@ -1,8 +1,10 @@
 // Search-path kernels: query rotation, one-query routing with on-device
-// top-nprobe selection, the plain streaming scan with warp top-k, and the
-// single-vector estimator.
+// top-nprobe selection, and the single-vector estimator. (The plain scan is
+// in scan_plain.cu, the batched path in batched.cu.)
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <algorithm>
 
 #include "device_common.cuh"
 #include "internal.h"
@@ -60,14 +62,20 @@ __global__ void rotate_queries_kernel(const float* __restrict__ q, int dim, int 
 // so an 8-pass MSB radix select finds the nprobe-th key exactly; the selected
 // lists are compacted in cid order (the plain scan's result does not depend
 // on probe order) with their tile-count prefix.
-__device__ void select_probes(const DevIndex& ix, const uint64_t* keys, int nprobe,
-                              const RouteWork& w) {
+__device__ void select_probes(const DevIndex& ix, const uint64_t* gkeys, int nprobe,
+                              const RouteWork& w, unsigned long long* skeys) {
     __shared__ int hist[256];
     __shared__ uint64_t s_prefix;
     __shared__ int s_want;
     __shared__ int sm32[32];
     const int tid = threadIdx.x, nt = blockDim.x;
     const int nlist = ix.nlist;
+    // keys in shared memory when they fit (one coalesced pass), else L2
+    const unsigned long long* keys = reinterpret_cast<const unsigned long long*>(gkeys);
+    if (skeys != nullptr) {
+        for (int c = tid; c < nlist; c += nt) skeys[c] = __ldcg(keys + c);
+        keys = skeys;
+    }
     if (tid == 0) {
         s_prefix = 0;
         s_want = nprobe;
@@ -79,7 +87,7 @@ __device__ void select_probes(const DevIndex& ix, const uint64_t* keys, int npro
         __syncthreads();
         const uint64_t prefix = s_prefix;
         for (int c = tid; c < nlist; c += nt) {
-            const uint64_t key = __ldcg(reinterpret_cast<const unsigned long long*>(keys) + c);
+            const uint64_t key = skeys ? keys[c] : __ldcg(keys + c);
             if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1);
         }
         __syncthreads();
@@ -121,7 +129,7 @@ __device__ void select_probes(const DevIndex& ix, const uint64_t* keys, int npro
     for (int c0 = 0; c0 < nlist; c0 += nt) {
         const int c = c0 + tid;
         uint64_t key = ~0ull;
-        if (c < nlist) key = __ldcg(reinterpret_cast<const unsigned long long*>(keys) + c);
+        if (c < nlist) key = skeys ? keys[c] : __ldcg(keys + c);
         const int flag = (c < nlist && key <= kth) ? 1 : 0;
         int tot;
         const int pos = base + block_exclusive_scan(flag, &tot, sm32);
@@ -156,8 +164,8 @@ __device__ void select_probes(const DevIndex& ix, const uint64_t* keys, int npro
 // as the scalar GEMV src/simd/kernels_generic.cpp:13-33), then the last CTA
 // to finish selects the probes.
 __global__ void route_one_kernel(DevIndex ix, const float* __restrict__ rq, int nprobe,
-                                 RouteWork w) {
-    extern __shared__ float sq[];
+                                 RouteWork w, unsigned s_dyn_bytes) {
+    extern __shared__ __align__(16) float sq[];
     __shared__ double red[32];
     __shared__ float s_qn2;
     __shared__ bool s_last;
@@ -180,10 +188,32 @@ __global__ void route_one_kernel(DevIndex ix, const float* __restrict__ rq, int 
     }
     __syncthreads();
     const float qn2 = s_qn2;
+    // one centroid per warp iteration; each lane loads its float4s of the row
+    // first (one memory latency per row), then accumulates in fp64
     for (int c = blockIdx.x * nw + warp; c < ix.nlist; c += gridDim.x * nw) {
-        const float* cc = ix.cen + static_cast<size_t>(c) * pd;
+        const float4* cc = reinterpret_cast<const float4*>(ix.cen + static_cast<size_t>(c) * pd);
+        const float4* q4 = reinterpret_cast<const float4*>(sq);
+        const int n4 = pd >> 2;
         double dot = 0.0;
-        for (int i = lane; i < pd; i += 32) dot += static_cast<double>(sq[i]) * static_cast<double>(__ldg(cc + i));
+        for (int base = 0; base < n4; base += 8 * 32) {
+            float4 v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int i = base + j * 32 + lane;
+                v[j] = i < n4 ? __ldg(cc + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int i = base + j * 32 + lane;
+                if (i < n4) {
+                    const float4 qv = q4[i];
+                    dot += static_cast<double>(qv.x) * static_cast<double>(v[j].x);
+                    dot += static_cast<double>(qv.y) * static_cast<double>(v[j].y);
+                    dot += static_cast<double>(qv.z) * static_cast<double>(v[j].z);
+                    dot += static_cast<double>(qv.w) * static_cast<double>(v[j].w);
+                }
+            }
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(kFull, dot, o);
         if (lane == 0) {
@@ -198,182 +228,12 @@ __global__ void route_one_kernel(DevIndex ix, const float* __restrict__ rq, int 
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    select_probes(ix, w.keys, nprobe, w);
+    // the dynamic shared buffer (query, then free) holds the keys if they fit
+    unsigned long long* skeys =
+        (static_cast<size_t>(ix.nlist) * 8 <= s_dyn_bytes) ? reinterpret_cast<unsigned long long*>(sq) : nullptr;
+    __syncthreads();
+    select_probes(ix, w.keys, nprobe, w, skeys);
     if (tid == 0) *w.counter = 0;
-}
-
-// Copies of the level table kept in shared memory: 32 (one per lane, so the
-// gathers are bank-conflict free) up to 8 bits, fewer above (64 KB cap).
-template <int BITS>
-__host__ __device__ constexpr int table_rep() {
-    return BITS <= 8 ? 32 : ((16384 >> BITS) > 0 ? (16384 >> BITS) : 1);
-}
-
-// ---------------------------------------------------------------------------
-// Exact score of the vector in `lane` of a tile: S = sum_i q[i] *
-// tab[branch][digit_i] (the estimator of src/index/e8q_search.cpp:87-127;
-// fp32 FMA, two accumulators by block parity). Codes are read straight from
-// global memory one 16-byte chunk per lane (512 contiguous bytes per warp);
-// the level table is replicated REP times in shared memory so the 32 lanes'
-// gathers hit distinct banks.
-template <int BITS>
-__device__ __forceinline__ float score_tile_lane(const uint4* __restrict__ tile, int B,
-                                                 const float4* __restrict__ sq4,
-                                                 const float* __restrict__ tabrep, int lane) {
-    constexpr int GBL = group_blocks(BITS);
-    constexpr int GCH = group_chunks(BITS);
-    constexpr int BB = 8 * BITS;
-    constexpr int REP = table_rep<BITS>();
-    const int rl = lane % REP;
-    float acc0 = 0.0f, acc1 = 0.0f;
-    const int ng = B / GBL;
-    const int tail = B - ng * GBL;  // 0 or 8 (odd rates only)
-    int blk = 0;
-    for (int g = 0; g < ng; ++g) {
-        uint32_t w[4 * GCH + 1];
-#pragma unroll
-        for (int c = 0; c < GCH; ++c) {
-            const uint4 v = __ldg(tile + (g * GCH + c) * 32 + lane);
-            w[4 * c] = v.x;
-            w[4 * c + 1] = v.y;
-            w[4 * c + 2] = v.z;
-            w[4 * c + 3] = v.w;
-        }
-        w[4 * GCH] = 0;
-#pragma unroll
-        for (int b = 0; b < GBL; ++b, ++blk) {
-            uint32_t dg[8];
-            const int br = decode_block<BITS>(w, b * BB, dg);
-            const float4 qa = sq4[2 * blk], qb = sq4[2 * blk + 1];
-            const float* t = tabrep + ((br << BITS) * REP) + rl;
-            float& acc = (b & 1) ? acc1 : acc0;
-            acc = __fmaf_rn(qa.x, t[dg[0] * REP], acc);
-            acc = __fmaf_rn(qa.y, t[dg[1] * REP], acc);
-            acc = __fmaf_rn(qa.z, t[dg[2] * REP], acc);
-            acc = __fmaf_rn(qa.w, t[dg[3] * REP], acc);
-            acc = __fmaf_rn(qb.x, t[dg[4] * REP], acc);
-            acc = __fmaf_rn(qb.y, t[dg[5] * REP], acc);
-            acc = __fmaf_rn(qb.z, t[dg[6] * REP], acc);
-            acc = __fmaf_rn(qb.w, t[dg[7] * REP], acc);
-        }
-    }
-    if (tail > 0) {
-        constexpr int TCH = (8 * BB + 127) / 128;
-        uint32_t w[4 * TCH + 1];
-#pragma unroll
-        for (int c = 0; c < TCH; ++c) {
-            const uint4 v = __ldg(tile + (ng * GCH + c) * 32 + lane);
-            w[4 * c] = v.x;
-            w[4 * c + 1] = v.y;
-            w[4 * c + 2] = v.z;
-            w[4 * c + 3] = v.w;
-        }
-        w[4 * TCH] = 0;
-#pragma unroll
-        for (int b = 0; b < 8; ++b, ++blk) {
-            uint32_t dg[8];
-            const int br = decode_block<BITS>(w, b * BB, dg);
-            const float4 qa = sq4[2 * blk], qb = sq4[2 * blk + 1];
-            const float* t = tabrep + ((br << BITS) * REP) + rl;
-            float& acc = (b & 1) ? acc1 : acc0;
-            acc = __fmaf_rn(qa.x, t[dg[0] * REP], acc);
-            acc = __fmaf_rn(qa.y, t[dg[1] * REP], acc);
-            acc = __fmaf_rn(qa.z, t[dg[2] * REP], acc);
-            acc = __fmaf_rn(qa.w, t[dg[3] * REP], acc);
-            acc = __fmaf_rn(qb.x, t[dg[4] * REP], acc);
-            acc = __fmaf_rn(qb.y, t[dg[5] * REP], acc);
-            acc = __fmaf_rn(qb.z, t[dg[6] * REP], acc);
-            acc = __fmaf_rn(qb.w, t[dg[7] * REP], acc);
-        }
-    }
-    return __fadd_rn(acc0, acc1);
-}
-
-// CTA-wide merge of per-warp top-k lists into warp 0 (smem staging).
-__device__ void cta_merge(WarpTopK& top, float* sm_d, uint32_t* sm_id, int k) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    top.store(sm_d + warp * kMaxK, sm_id + warp * kMaxK, k);
-    __syncthreads();
-    if (warp == 0) {
-        for (int w2 = 1; w2 < nw; ++w2) {
-            for (int j0 = 0; j0 < k; j0 += 32) {
-                const int j = j0 + lane;
-                const bool ok = j < k;
-                const float dd = ok ? sm_d[w2 * kMaxK + j] : inf_f();
-                const uint32_t ii = ok ? sm_id[w2 * kMaxK + j] : 0xFFFFFFFFu;
-                top.offer_pair(dd, ii, ok && ii != 0xFFFFFFFFu);
-            }
-        }
-    }
-    __syncthreads();
-}
-
-// Plain (unpruned) streaming scan of one query over its probed lists: every
-// vector of every probed list gets dist = (d2 + h3) - 2*g1*S (the refine
-// step of src/simd/e8q_search_generic.cpp:58-66 with d2 folded as in
-// e8q_search_generic.cpp:189) and enters a warp top-k; CTAs merge into
-// per-CTA lists and the last CTA to finish merges those into the answer.
-template <int BITS>
-__global__ void __launch_bounds__(256) scan_plain_kernel(DevIndex ix, const float* __restrict__ rq,
-                                                         RouteWork rw, int k, ScanWork sw,
-                                                         uint32_t* __restrict__ out_ids,
-                                                         float* __restrict__ out_d) {
-    constexpr int Q = 1 << BITS;
-    constexpr int REP = table_rep<BITS>();
-    extern __shared__ __align__(16) float smem[];
-    float* sq = smem;                              // pd
-    float* tabrep = smem + ix.pd;                  // 2*Q*REP
-    float* sm_d = tabrep + 2 * Q * REP;            // 8 warps * kMaxK
-    uint32_t* sm_id = reinterpret_cast<uint32_t*>(sm_d + 8 * kMaxK);
-    __shared__ bool s_last;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    for (int i = tid; i < ix.pd; i += blockDim.x) sq[i] = rq[i];
-    for (int e = tid; e < 2 * Q * REP; e += blockDim.x) tabrep[e] = ix.tab[e / REP];
-    __syncthreads();
-    const float4* sq4 = reinterpret_cast<const float4*>(sq);
-    const int T = static_cast<int>(__ldcg(rw.total_tiles));
-    const int gw = blockIdx.x * nw + warp, tw = gridDim.x * nw;
-    WarpTopK top;
-    top.init(k);
-    int p = 0;
-    for (int t = gw; t < T; t += tw) {
-        // probe p with tile_off[p] <= t < tile_off[p+1] (monotone in t: walk)
-        while (__ldcg(rw.tile_off + p + 1) <= static_cast<uint32_t>(t)) ++p;
-        const uint32_t list = __ldcg(rw.probes + p);
-        const float d2 = __ldcg(rw.probe_d2 + p);
-        const uint32_t local = static_cast<uint32_t>(t) - __ldcg(rw.tile_off + p);
-        const uint32_t gt = ix.tile_begin[list] + local;
-        const bool valid = local * 32u + static_cast<uint32_t>(lane) < ix.list_len[list];
-        const uint4* tile = ix.codes + static_cast<size_t>(gt) * ix.nch * 32;
-        const float S = score_tile_lane<BITS>(tile, ix.B, sq4, tabrep, lane);
-        const size_t slot = static_cast<size_t>(gt) * 32 + lane;
-        const float g1 = __ldg(ix.g1 + slot), h3 = __ldg(ix.h3 + slot);
-        const float dist = __fmaf_rn(-__fmul_rn(2.0f, g1), S, __fadd_rn(d2, h3));
-        top.offer(dist, valid, [&] { return __ldg(ix.ids + slot); });
-    }
-    cta_merge(top, sm_d, sm_id, k);
-    if (warp == 0) top.store(sw.part_d + static_cast<size_t>(blockIdx.x) * kMaxK,
-                             sw.part_id + static_cast<size_t>(blockIdx.x) * kMaxK, k);
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) s_last = atomicAdd(sw.counter, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    // final merge of gridDim.x partial lists
-    top.init(k);
-    for (int c = warp; c < static_cast<int>(gridDim.x); c += nw) {
-        for (int j0 = 0; j0 < k; j0 += 32) {
-            const int j = j0 + lane;
-            const bool ok = j < k;
-            const float dd = ok ? __ldcg(sw.part_d + static_cast<size_t>(c) * kMaxK + j) : inf_f();
-            const uint32_t ii = ok ? __ldcg(sw.part_id + static_cast<size_t>(c) * kMaxK + j) : 0xFFFFFFFFu;
-            top.offer_pair(dd, ii, ok && ii != 0xFFFFFFFFu);
-        }
-    }
-    cta_merge(top, sm_d, sm_id, k);
-    if (warp == 0) top.store(out_d, out_ids, k);
-    if (tid == 0) *sw.counter = 0;
 }
 
 // One stored vector: Estimate() of src/index/e8q_oracle.cpp:58-101 (fp32
@@ -420,25 +280,6 @@ __global__ void estimate_kernel(DevIndex ix, const float* __restrict__ rq, int l
     *out = __fmaf_rn(-__fmul_rn(2.0f, ix.g1[s]), S, __fadd_rn(d2, ix.h3[s]));
 }
 
-template <int BITS>
-int launch_scan_bits(const DevIndex& ix, const float* rq, const RouteWork& rw, int k,
-                     const ScanWork& sw, uint32_t* out_ids, float* out_d, cudaStream_t s) {
-    constexpr int Q = 1 << BITS;
-    constexpr int REP = table_rep<BITS>();
-    const size_t smem = (static_cast<size_t>(ix.pd) + 2 * Q * REP + 8 * kMaxK * 2) * sizeof(float);
-    static uint64_t configured = 0;  // one bit per device ordinal
-    int dev = 0;
-    E8QC_CUDA(cudaGetDevice(&dev));
-    if (!((configured >> (dev & 63)) & 1u)) {
-        E8QC_CUDA(cudaFuncSetAttribute(scan_plain_kernel<BITS>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        configured |= uint64_t{1} << (dev & 63);
-    }
-    scan_plain_kernel<BITS><<<sw.grid, 256, smem, s>>>(ix, rq, rw, k, sw, out_ids, out_d);
-    E8QC_CUDA(cudaGetLastError());
-    return 1;
-}
-
 }  // namespace
 
 int launch_rotate(const DevIndex& ix, const float* q, int nq, float* out, cudaStream_t s) {
@@ -465,30 +306,23 @@ int launch_rotate_raw(const uint8_t* signs, int dim, int pd, const float* src, i
 int launch_route_one(const DevIndex& ix, const float* rq, int nprobe, const RouteWork& w,
                      cudaStream_t s) {
     const int warps = 8;
-    int grid = (ix.nlist + warps * 4 - 1) / (warps * 4);  // ~4 centroids per warp
-    grid = grid < 1 ? 1 : (grid > 296 ? 296 : grid);
-    route_one_kernel<<<grid, warps * 32, ix.pd * sizeof(float), s>>>(ix, rq, nprobe, w);
+    int grid = (ix.nlist + warps - 1) / warps;  // one centroid per warp
+    grid = grid < 1 ? 1 : (grid > 1184 ? 1184 : grid);
+    // dynamic shared memory: the query, reused by the last CTA for the keys
+    size_t dyn = std::max<size_t>(ix.pd * sizeof(float), std::min<size_t>(ix.nlist * 8, 64 * 1024));
+    if (dyn > 48 * 1024) {
+        static size_t configured[64] = {};
+        int dev = 0;
+        E8QC_CUDA(cudaGetDevice(&dev));
+        if (configured[dev & 63] < dyn) {
+            E8QC_CUDA(cudaFuncSetAttribute(route_one_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(dyn)));
+            configured[dev & 63] = dyn;
+        }
+    }
+    route_one_kernel<<<grid, warps * 32, dyn, s>>>(ix, rq, nprobe, w, static_cast<unsigned>(dyn));
     E8QC_CUDA(cudaGetLastError());
     return 1;
-}
-
-int plain_scan_grid(int bits) {
-    (void)bits;
-    return 148 * 3;
-}
-
-int launch_scan_plain(const DevIndex& ix, const float* rq, const RouteWork& rw, int k,
-                      const ScanWork& sw, uint32_t* out_ids, float* out_d, cudaStream_t s) {
-    switch (ix.bits) {
-#define E8QC_CASE(b) \
-    case b: return launch_scan_bits<b>(ix, rq, rw, k, sw, out_ids, out_d, s);
-        E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
-        E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
-        E8QC_CASE(13)
-#undef E8QC_CASE
-        default: fail(E8QC_EINVAL, "bits out of range");
-    }
-    return 0;
 }
 
 int launch_estimate(const DevIndex& ix, const float* rq, int list, uint32_t slot, float* out,

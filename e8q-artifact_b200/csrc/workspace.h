@@ -54,11 +54,33 @@ struct Workspace {
     size_t route_cap = 0;
     DevBuf part_d, part_id, scan_counter;
     size_t scan_cap = 0;
-    // batched path
-    DevBuf b_keys, b_probes, b_pd2, b_cnt, b_off, b_items, b_pairs, b_part_d, b_part_id,
-        b_queue, b_nitems, b_scratch;
-    size_t b_q_cap = 0, b_pair_cap = 0, b_item_cap = 0, b_nlist_cap = 0, b_part_cap = 0;
+    DevBuf err;  // device error word written by bounded waits
+    uint32_t* err_host = nullptr;
+    // batched path (grown on demand by batched_search)
+    DevBuf b_keys, b_qn2, b_probes, b_pd2, b_pos, b_pair_q, b_pair_d2, b_cnt, b_off, b_fill, b_items,
+        b_nitems, b_part_d, b_part_id;
 
+    ~Workspace() {
+        if (err_host) cudaFreeHost(err_host);
+    }
+    void ensure_err() {
+        if (err.p) return;
+        err.alloc(4);
+        E8QC_CUDA(cudaMemset(err.p, 0, 4));
+        E8QC_CUDA(cudaMallocHost(&err_host, 4));
+    }
+    // Synchronise the stream and turn a kernel-reported wait timeout into an
+    // error (the word is cleared for the next call).
+    void check_error(cudaStream_t s) {
+        ensure_err();
+        E8QC_CUDA(cudaMemcpyAsync(err_host, err.p, 4, cudaMemcpyDeviceToHost, s));
+        E8QC_CUDA(cudaStreamSynchronize(s));
+        if (*err_host != 0) {
+            E8QC_CUDA(cudaMemsetAsync(err.p, 0, 4, s));
+            E8QC_CUDA(cudaStreamSynchronize(s));
+            fail(E8QC_ETIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
+        }
+    }
     void ensure_queries(size_t nq, size_t pd) {
         if (nq * pd > rq_cap) {
             rq.alloc(nq * pd * sizeof(float));
@@ -77,6 +99,7 @@ struct Workspace {
         route_cap = nlist;
     }
     void ensure_scan(size_t grid) {
+        ensure_err();
         if (grid <= scan_cap) return;
         part_d.alloc(grid * kMaxK * 4);
         part_id.alloc(grid * kMaxK * 4);

@@ -116,6 +116,19 @@ int e8qc_e8q_estimate(e8qc_index* idx, const float* query, uint32_t id, float* o
 int e8qc_e8q_set_disable_prune(e8qc_index* idx, int on);
 int e8qc_e8q_set_prune_alpha(e8qc_index* idx, float alpha);
 int e8qc_e8q_info(const e8qc_index* idx, e8qc_info* out);
+/* Scan-kernel profile: while enabled, every call records CUDA events around
+ * each launch of the dominant scan kernel on the call's stream and counts the
+ * candidates it scored (plain mode reads the probe lists back once per query,
+ * so timings of the calls themselves are perturbed). enable=1 resets and
+ * starts; enable=0 stops and fills *out (may be NULL). */
+typedef struct e8qc_profile {
+    uint64_t scan_launches;  /* dominant-kernel launches timed */
+    double scan_ms;          /* summed CUDA-event time of those launches */
+    uint64_t candidates;     /* (query, vector) pairs scored */
+    uint64_t algo_bytes;     /* candidates * (bits*padded_dim/8 + 8): codes + g1/h3 */
+    uint64_t queries;
+} e8qc_profile;
+int e8qc_e8q_profile(e8qc_index* idx, int enable, e8qc_profile* out);
 /* Copy the global ids, cluster-major (n entries), to a host buffer. */
 int e8qc_e8q_get_ids(const e8qc_index* idx, uint32_t* out);
 /* Export the per-vector lattice codes (cluster-major, the order of
