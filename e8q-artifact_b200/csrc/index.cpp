@@ -201,6 +201,20 @@ void plain_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size_
 
 }  // namespace
 
+namespace e8qc {
+// Read-only view of a built index for the no-allocation plain search
+// (noalloc.cu). Throws like every entry point when the index is not built.
+void plain_context(e8qc_index* x, size_t nprobe, DevIndex* view, int* device, size_t* nlist, size_t* dim,
+                   size_t* max_tiles) {
+    require_built(x, "search");
+    *view = x->view;
+    *device = x->device;
+    *nlist = x->nlist;
+    *dim = x->dim;
+    *max_tiles = max_tiles_for(x, nprobe);
+}
+}  // namespace e8qc
+
 // ---------------------------------------------------------------------------
 extern "C" {
 

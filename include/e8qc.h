@@ -129,6 +129,21 @@ typedef struct e8qc_profile {
     uint64_t queries;
 } e8qc_profile;
 int e8qc_e8q_profile(e8qc_index* idx, int enable, e8qc_profile* out);
+/* Plain search that allocates nothing (no counterpart in the reference; an
+ * addition of this library). For callers that cannot let a search allocate
+ * device memory: a serving process whose HBM is reserved by its framework's
+ * caching allocator, a request handler that must not stall other streams
+ * (cudaFree synchronises the device), a JNI/cgo host with a fixed memory
+ * budget. Same kernels and results as e8qc_e8q_search(..., E8QC_MODE_PLAIN),
+ * but the scratch is a fixed 2.4 MB static device array per device (held
+ * until the process exits) and queries (nq*dim), out_ids and out_dists
+ * (nq*k) must be DEVICE pointers. Limits: nlist <= 65536, padded_dim <= 4096;
+ * larger indexes return E8QC_EINVAL. The first call on a device resolves the
+ * array's address (make it before any stream capture). All calls share the
+ * array: calls whose GPU work overlaps race and must be serialised by the
+ * caller. Returns after the results are in out_ids / out_dists. */
+int e8qc_e8q_search_plain_noalloc(e8qc_index* idx, const float* queries, size_t nq, size_t k,
+                                  size_t nprobe, uint32_t* out_ids, float* out_dists, void* stream);
 /* Copy the global ids, cluster-major (n entries), to a host buffer. */
 int e8qc_e8q_get_ids(const e8qc_index* idx, uint32_t* out);
 /* Export the per-vector lattice codes (cluster-major, the order of
