@@ -291,6 +291,20 @@ PYBIND11_MODULE(_e8qlib, m) {
         return out;
     }, py::arg("x"), py::arg("dim"), py::arg("seed"), py::arg("device") = 0);
 
+    m.def("tc_i8_gemm", [](py::handle a, py::handle b, int reps, int grid, int device) {
+        auto A = e8qb200::ensure_nd<int8_t>(a, "A", 2);
+        auto B = e8qb200::ensure_nd<int8_t>(b, "B", 2);
+        if (A.shape(0) != 128 || A.shape(1) != B.shape(1)) throw std::invalid_argument("A must be 128 x k, B n x k");
+        const int n = static_cast<int>(B.shape(0)), k = static_cast<int>(A.shape(1));
+        py::array_t<int32_t> C({py::ssize_t(128), static_cast<py::ssize_t>(n)});
+        float ms = 0.0f;
+        {
+            py::gil_scoped_release nogil;
+            e8qb200::check(e8qc_tc_i8_gemm(device, A.data(), B.data(), n, k, reps, grid, C.mutable_data(), &ms));
+        }
+        return py::make_tuple(C, ms);
+    }, py::arg("A"), py::arg("B"), py::arg("reps") = 1, py::arg("grid") = 1, py::arg("device") = 0);
+
     py::class_<E8qIndex>(m, "E8qIndex")
         .def(py::init<size_t, size_t, uint64_t, int>(), py::arg("dim"), py::arg("nbits"),
              py::arg("seed") = 0, py::arg("device") = 0)

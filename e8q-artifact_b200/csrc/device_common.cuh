@@ -77,13 +77,22 @@ struct WarpTopK {
 
     // Per-lane offer: lane candidate (dist, id) with `want` true where the lane
     // has a candidate. The id is only needed when the distance can tie or beat
-    // the threshold, so it is fetched through `get_id` lazily.
+    // the threshold, so it is fetched through `get_id` lazily. When several
+    // lanes pass and k <= 32, the 32 candidates are bitonic-sorted and merged
+    // into the list in one pass; otherwise they are inserted one at a time.
     template <class GetId>
     __device__ void offer(float dist, bool want, GetId get_id) {
         bool maybe = want && !(dist > thr_d);
         uint32_t cid = 0xFFFFFFFFu;
         if (maybe) cid = get_id();
         unsigned m = __ballot_sync(kFull, maybe && better(dist, cid, thr_d, thr_id));
+        if (m == 0) return;
+        if (k <= 32 && __popc(m) >= 2) {
+            const int lane = threadIdx.x & 31;
+            const bool in = (m >> lane) & 1u;
+            merge32(in ? dist : __int_as_float(0x7f800000), in ? cid : 0xFFFFFFFFu);
+            return;
+        }
         while (m) {
             const int src = __ffs(m) - 1;
             const float cd = __shfl_sync(kFull, dist, src);
@@ -92,6 +101,37 @@ struct WarpTopK {
             m &= ~(1u << src);
             m &= __ballot_sync(kFull, maybe && better(dist, cid, thr_d, thr_id));
         }
+    }
+
+    // k <= 32: merge one candidate per lane into slot 0 (sorted) in one pass:
+    // bitonic sort of the candidates, reverse, lane-wise min against the list
+    // (the 32 smallest of the union, a bitonic sequence), bitonic clean-up.
+    __device__ void merge32(float cd, uint32_t ci) {
+        const int lane = threadIdx.x & 31;
+#pragma unroll
+        for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+            for (int j = kk >> 1; j > 0; j >>= 1) {
+                const float pd = __shfl_xor_sync(kFull, cd, j);
+                const uint32_t pi = __shfl_xor_sync(kFull, ci, j);
+                const bool asc = (lane & kk) == 0;
+                const bool lower = (lane & j) == 0;
+                const bool take = (lower == asc) ? better(pd, pi, cd, ci) : better(cd, ci, pd, pi);
+                if (take) { cd = pd; ci = pi; }
+            }
+        }
+        const float rd = __shfl_sync(kFull, cd, 31 - lane);
+        const uint32_t ri = __shfl_sync(kFull, ci, 31 - lane);
+        if (better(rd, ri, d[0], id[0])) { d[0] = rd; id[0] = ri; }
+#pragma unroll
+        for (int j = 16; j > 0; j >>= 1) {
+            const float pd = __shfl_xor_sync(kFull, d[0], j);
+            const uint32_t pi = __shfl_xor_sync(kFull, id[0], j);
+            const bool lower = (lane & j) == 0;
+            const bool take = lower ? better(pd, pi, d[0], id[0]) : better(d[0], id[0], pd, pi);
+            if (take) { d[0] = pd; id[0] = pi; }
+        }
+        refresh_threshold();
     }
 
     __device__ void offer_pair(float dist, uint32_t cid, bool want) {
@@ -111,6 +151,38 @@ struct WarpTopK {
         }
     }
 };
+
+// ---------------------------------------------------------------------------
+// Block-wide bitonic sort (ascending by `better`) of pn entries held in shared
+// memory; pn is a power of two, unused entries hold (+inf, UINT32_MAX). All
+// threads of the block must call it.
+__device__ inline void block_bitonic_sort(float* sd, uint32_t* si, int pn) {
+    for (int kk = 2; kk <= pn; kk <<= 1) {
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < pn; i += blockDim.x) {
+                const int p = i ^ j;
+                if (p > i) {
+                    const bool asc = (i & kk) == 0;
+                    const float a = sd[i], b = sd[p];
+                    const uint32_t ai = si[i], bi = si[p];
+                    if (asc ? better(b, bi, a, ai) : better(a, ai, b, bi)) {
+                        sd[i] = b;
+                        sd[p] = a;
+                        si[i] = bi;
+                        si[p] = ai;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__host__ __device__ inline int next_pow2(int v) {
+    int p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
 
 // ---------------------------------------------------------------------------
 // FHT-Kac-4 rotation of `rows` vectors held in shared memory (row stride

@@ -6,20 +6,20 @@
 // a warp top-k; CTAs merge into per-CTA lists and the last CTA to finish
 // merges those into the answer.
 //
-// Data movement: each warp owns a two-stage ring in shared memory and pulls
-// its tiles' code bytes with cp.async.bulk (one bulk copy per segment of a
-// 32-vector tile, completion on an mbarrier), so every warp keeps up to two
-// segments in flight while it decodes. Lane l decodes vector l of the tile:
-// chunk c of lane l sits at [c][l] (16 bytes), so the lanes' reads of one
-// chunk row are 512 contiguous bytes. Level values come from a shared-memory
-// table replicated once per lane (bank-conflict-free gathers).
+// Data movement: lane l decodes vector l of a 32-vector tile; chunk c of lane
+// l sits at [c][l] (16 bytes), so a warp's read of one chunk row is 512
+// contiguous bytes. Each warp runs a kStages-deep cp.async pipeline over its
+// jobs (one chunk-group of a tile each): every lane copies exactly the 16-byte
+// entries it will decode into the warp's ring slot, so completion is a plain
+// per-thread cp.async.wait_group (no spinning, no cross-lane hand-off). Level
+// values come from a shared-memory table replicated once per lane
+// (bank-conflict-free gathers). Tiles are dealt round-robin over CTAs.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "device_common.cuh"
 #include "internal.h"
 #include "scan_plain.h"
-#include "tma.cuh"
 
 namespace e8qc {
 
@@ -27,13 +27,28 @@ namespace {
 
 __device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
 
-constexpr int kMaxWarps = 32;
+constexpr int kMaxWarps = 16;
+constexpr int kStages = 4;      // bulk-copy stages in flight per warp
 constexpr int kToffCap = 1024;  // tile offsets cached in shared memory
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
 
 __device__ __forceinline__ float lds_f32(uint32_t addr) {
     float v;
-    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+    asm("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
     return v;
+}
+
+// 16-byte global -> shared async copy (L2 only), and the group fences.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // log2 of the byte stride between consecutive level entries: REP per-lane
@@ -127,24 +142,38 @@ __device__ __forceinline__ int find_probe(const uint32_t* off, int nprobe, uint3
     return lo;
 }
 
-// CTA-wide merge of per-warp top-k lists into warp 0 (smem staging).
+// CTA-wide merge of the per-warp top-k lists: all lists into shared memory,
+// one block bitonic sort, warp 0 reloads the first k (sm_d/sm_id hold
+// nw*kMaxK >= next_pow2(nw*k) entries).
 __device__ void cta_merge(WarpTopK& top, float* sm_d, uint32_t* sm_id, int k) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    top.store(sm_d + warp * kMaxK, sm_id + warp * kMaxK, k);
+    top.store(sm_d + warp * k, sm_id + warp * k, k);
+    const int n = nw * k, pn = next_pow2(n);
+    for (int i = n + threadIdx.x; i < pn; i += blockDim.x) {
+        sm_d[i] = inf_f();
+        sm_id[i] = 0xFFFFFFFFu;
+    }
     __syncthreads();
+    block_bitonic_sort(sm_d, sm_id, pn);
     if (warp == 0) {
-        for (int w2 = 1; w2 < nw; ++w2) {
-            for (int j0 = 0; j0 < k; j0 += 32) {
-                const int j = j0 + lane;
-                const bool ok = j < k;
-                const float dd = ok ? sm_d[w2 * kMaxK + j] : inf_f();
-                const uint32_t ii = ok ? sm_id[w2 * kMaxK + j] : 0xFFFFFFFFu;
-                top.offer_pair(dd, ii, ok && ii != 0xFFFFFFFFu);
-            }
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const int j = s * 32 + lane;
+            top.d[s] = j < k ? sm_d[j] : inf_f();
+            top.id[s] = j < k ? sm_id[j] : 0xFFFFFFFFu;
         }
+        top.refresh_threshold();
     }
     __syncthreads();
 }
+
+// Where one tile of the warp's share lives and what its epilogue needs.
+struct TileInfo {
+    const uint4* src;  // first chunk row of the tile
+    float d2;          // query-to-list distance
+    uint32_t slot0;    // first padded slot of the tile
+    uint32_t nvalid;   // vectors of the tile that exist (<= 32)
+};
 
 template <int BITS>
 __global__ void __launch_bounds__(kMaxWarps * 32, 1) scan_plain_kernel(
@@ -159,14 +188,12 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) scan_plain_kernel(
     const int nw = blockDim.x >> 5, nt = blockDim.x;
     const int pd = ix.pd;
     // shared-memory carve (see scan_smem_bytes)
-    unsigned char* ring = smem;                                       // nw * 2 * seg_bytes
-    float* tabrep = reinterpret_cast<float*>(ring + nw * 2 * geo.seg_bytes);  // 2*Q*REP
+    unsigned char* ring = smem;                                       // nw * kStages * seg_bytes
+    float* tabrep = reinterpret_cast<float*>(ring + nw * kStages * geo.seg_bytes);  // 2*Q*REP
     float* sq = tabrep + 2 * Q * REP;                                 // pd
     uint32_t* soff = reinterpret_cast<uint32_t*>(sq + pd);           // kToffCap + 1
     float* sm_d = reinterpret_cast<float*>(soff + kToffCap + 1);      // nw * kMaxK
     uint32_t* sm_id = reinterpret_cast<uint32_t*>(sm_d + nw * kMaxK);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(
-        (reinterpret_cast<uintptr_t>(sm_id + nw * kMaxK) + 7) & ~uintptr_t(7));  // nw * 2
     __shared__ bool s_last;
 
     for (int i = tid; i < pd; i += nt) sq[i] = rq[i];
@@ -174,11 +201,6 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) scan_plain_kernel(
     const bool off_in_smem = nprobe <= kToffCap;
     if (off_in_smem)
         for (int i = tid; i <= nprobe; i += nt) soff[i] = __ldcg(rw.tile_off + i);
-    if (lane == 0) {
-        mbar_init(&bars[2 * warp], 1);
-        mbar_init(&bars[2 * warp + 1], 1);
-        fence_barrier_init();
-    }
     __syncthreads();
     const uint32_t* off = off_in_smem ? soff : rw.tile_off;
     const float4* sq4 = reinterpret_cast<const float4*>(sq);
@@ -190,85 +212,80 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) scan_plain_kernel(
     const uint32_t per_cta = T > blockIdx.x ? (T - blockIdx.x + G - 1) / G : 0;
     const uint32_t ntile_w = per_cta > static_cast<uint32_t>(warp)
                                  ? (per_cta - warp + nw - 1) / static_cast<uint32_t>(nw) : 0;
-    const int nseg = geo.nseg;
-    const uint32_t J = ntile_w * static_cast<uint32_t>(nseg);
-    unsigned char* my_ring = ring + warp * 2 * geo.seg_bytes;
-    auto tile_of = [&](uint32_t j) { return (static_cast<uint32_t>(warp) + (j / nseg) * nw) * G + blockIdx.x; };
-
-    auto seg_range = [&](int seg, int& c0, int& cnt) {
-        if (geo.tail && seg == nseg - 1) {
-            c0 = geo.ng * GCH;
-            cnt = TCH;
-        } else {
-            const int g0 = seg * geo.U;
-            const int g1 = min(geo.ng, g0 + geo.U);
-            c0 = g0 * GCH;
-            cnt = (g1 - g0) * GCH;
-        }
-    };
-    auto issue = [&](uint32_t j) {
-        const uint32_t t = tile_of(j);
-        const int seg = static_cast<int>(j % nseg);
+    // jobs: the groups of each of this warp's tiles (plus the tail half-group)
+    const int jpt = geo.ng + geo.tail;  // jobs per tile
+    const uint32_t J = ntile_w * static_cast<uint32_t>(jpt);
+    // per-warp ring of kStages chunk-group slots; lane l copies and later
+    // reads only its own 16-byte entries, so the pipeline is lane-private
+    const uint32_t ring_lane = smem_addr(ring) + static_cast<uint32_t>(warp * kStages * geo.seg_bytes) +
+                               static_cast<uint32_t>(lane) * 16u;
+    auto tile_of = [&](uint32_t i) { return (static_cast<uint32_t>(warp) + i * nw) * G + blockIdx.x; };
+    // every lane resolves the same tile (broadcast loads, no divergence)
+    auto resolve = [&](uint32_t i) {
+        TileInfo ti{nullptr, 0.0f, 0u, 0u};
+        if (i >= ntile_w) return ti;
+        const uint32_t t = tile_of(i);
         const int p = find_probe(off, nprobe, t);
         const uint32_t list = __ldcg(rw.probes + p);
-        const uint32_t gt = __ldg(ix.tile_begin + list) + (t - off[p]);
-        int c0, cnt;
-        seg_range(seg, c0, cnt);
-        const int st = static_cast<int>(j & 1);
-        const uint32_t bytes = static_cast<uint32_t>(cnt) * 512u;
-        mbar_arrive_expect_tx(&bars[2 * warp + st], bytes);
-        bulk_g2s(my_ring + st * geo.seg_bytes, ix.codes + (static_cast<size_t>(gt) * ix.nch + c0) * 32, bytes,
-                 &bars[2 * warp + st]);
+        const uint32_t local = t - off[p];
+        const uint32_t gt = __ldg(ix.tile_begin + list) + local;
+        const uint32_t len = __ldg(ix.list_len + list);
+        ti.src = ix.codes + static_cast<size_t>(gt) * ix.nch * 32;
+        ti.d2 = __ldcg(rw.probe_d2 + p);
+        ti.slot0 = gt * 32u;
+        ti.nvalid = min(32u, len - local * 32u);
+        return ti;
+    };
+    // the issue side walks the jobs ahead of the consume side with its own
+    // tile cursor; both resolve a tile once (broadcast loads)
+    uint32_t iss_i = 0xFFFFFFFFu;
+    TileInfo iss{nullptr, 0.0f, 0u, 0u};
+    auto issue = [&](uint32_t j) {
+        if (j < J) {
+            const uint32_t i = j / jpt;
+            if (i != iss_i) {
+                iss_i = i;
+                iss = resolve(i);
+            }
+            const int g = static_cast<int>(j % jpt);
+            const int c0 = g * GCH;
+            const int cnt = g < geo.ng ? GCH : TCH;
+            const uint32_t dst = ring_lane + static_cast<uint32_t>((j % kStages) * geo.seg_bytes);
+            const uint4* src = iss.src + c0 * 32 + lane;
+            for (int c = 0; c < cnt; ++c) cp_async16(dst + c * 512u, src + c * 32);
+        }
+        cp_async_commit();  // empty groups keep the group count uniform
     };
 
     WarpTopK top;
     top.init(k);
-    if (lane == 0) {
-        if (J > 0) issue(0);
-        if (J > 1) issue(1);
-    }
-    uint32_t phase[2] = {0u, 0u};
+    uint32_t issued = 0;
+    for (; issued < kStages - 1; ++issued) issue(issued);
     float acc0 = 0.0f, acc1 = 0.0f;
-    bool ok = true;
     for (uint32_t j = 0; j < J; ++j) {
-        const int st = static_cast<int>(j & 1);
-        const bool got = mbar_wait_bounded(&bars[2 * warp + st], phase[st]);
-        phase[st] ^= 1u;
-        if (!__all_sync(kFull, got)) {
-            ok = false;
-            break;
-        }
-        const int seg = static_cast<int>(j % nseg);
-        const uint4* sbuf = reinterpret_cast<const uint4*>(my_ring + st * geo.seg_bytes);
-        if (geo.tail && seg == nseg - 1) {
+        cp_async_wait<kStages - 2>();  // job j's group has landed (this lane's copies)
+        const int g = static_cast<int>(j % jpt);
+        const uint4* sbuf = reinterpret_cast<const uint4*>(ring + warp * kStages * geo.seg_bytes +
+                                                           (j % kStages) * geo.seg_bytes);
+        if (g < geo.ng)
+            accumulate_blocks<BITS, GBL, GCH>(sbuf, lane, sq4, g * GBL, tb_addr, acc0, acc1);
+        else
             accumulate_blocks<BITS, 8, TCH>(sbuf, lane, sq4, geo.ng * GBL, tb_addr, acc0, acc1);
-        } else {
-            const int g0 = seg * geo.U;
-            const int g1 = min(geo.ng, g0 + geo.U);
-            for (int g = g0; g < g1; ++g)
-                accumulate_blocks<BITS, GBL, GCH>(sbuf + (g - g0) * GCH * 32, lane, sq4, g * GBL, tb_addr, acc0,
-                                                  acc1);
-        }
-        __syncwarp();
-        if (lane == 0 && j + 2 < J) issue(j + 2);
-        if (seg == nseg - 1) {
-            const uint32_t t = tile_of(j);
-            const int p = find_probe(off, nprobe, t);
-            const uint32_t list = __ldcg(rw.probes + p);
-            const float d2 = __ldcg(rw.probe_d2 + p);
-            const uint32_t local = t - off[p];
-            const uint32_t gt = __ldg(ix.tile_begin + list) + local;
-            const bool valid = local * 32u + static_cast<uint32_t>(lane) < __ldg(ix.list_len + list);
-            const size_t slot = static_cast<size_t>(gt) * 32 + lane;
+        if (g == jpt - 1) {
+            const TileInfo cur = resolve(j / jpt);
+            const size_t slot = static_cast<size_t>(cur.slot0) + lane;
+            const bool valid = static_cast<uint32_t>(lane) < cur.nvalid;
             const float S = __fadd_rn(acc0, acc1);
             const float g1 = __ldg(ix.g1 + slot), h3 = __ldg(ix.h3 + slot);
-            const float dist = __fmaf_rn(-__fmul_rn(2.0f, g1), S, __fadd_rn(d2, h3));
+            const float dist = __fmaf_rn(-__fmul_rn(2.0f, g1), S, __fadd_rn(cur.d2, h3));
             top.offer(dist, valid, [&] { return __ldg(ix.ids + slot); });
             acc0 = 0.0f;
             acc1 = 0.0f;
         }
+        // job j's slot is free: this lane read its own entries above
+        issue(issued++);
     }
-    if (!ok && lane == 0) atomicOr(sw.err, kErrWaitTimeout);
+    cp_async_wait<0>();
     cta_merge(top, sm_d, sm_id, k);
     if (warp == 0) top.store(sw.part_d + static_cast<size_t>(blockIdx.x) * kMaxK,
                              sw.part_id + static_cast<size_t>(blockIdx.x) * kMaxK, k);
@@ -278,28 +295,16 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) scan_plain_kernel(
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    // final merge: the CTA stages the partial lists in shared memory (the
-    // ring is free now) with coalesced loads, then each warp offers a share
+    // final merge: each warp folds a share of the per-CTA lists into its own
+    // top-k (batched bitonic merges), then one CTA merge
     top.init(k);
     const int Gi = static_cast<int>(gridDim.x);
-    const int cap = (nw * 2 * geo.seg_bytes) / 8;  // entries per staging round
-    float* st_d = reinterpret_cast<float*>(ring);
-    uint32_t* st_i = reinterpret_cast<uint32_t*>(ring) + cap;
-    const int total = Gi * k;
-    for (int e0 = 0; e0 < total; e0 += cap) {
-        const int m = min(cap, total - e0);
-        __syncthreads();
-        for (int e = tid; e < m; e += nt) {
-            const int c = (e0 + e) / k, jj = (e0 + e) - c * k;
-            st_d[e] = __ldcg(sw.part_d + static_cast<size_t>(c) * kMaxK + jj);
-            st_i[e] = __ldcg(sw.part_id + static_cast<size_t>(c) * kMaxK + jj);
-        }
-        __syncthreads();
-        for (int e = warp * 32; e < m; e += nw * 32) {
-            const int i = e + lane;
-            const bool okj = i < m;
-            const float dd = okj ? st_d[i] : inf_f();
-            const uint32_t ii = okj ? st_i[i] : 0xFFFFFFFFu;
+    for (int c = warp; c < Gi; c += nw) {
+        for (int j0 = 0; j0 < k; j0 += 32) {
+            const int jj = j0 + lane;
+            const bool okj = jj < k;
+            const float dd = okj ? __ldcg(sw.part_d + static_cast<size_t>(c) * kMaxK + jj) : inf_f();
+            const uint32_t ii = okj ? __ldcg(sw.part_id + static_cast<size_t>(c) * kMaxK + jj) : 0xFFFFFFFFu;
             top.offer_pair(dd, ii, okj && ii != 0xFFFFFFFFu);
         }
     }
@@ -343,20 +348,20 @@ ScanGeo plain_scan_geo(const DevIndex& ix, size_t max_seg_bytes) {
     int seg_chunks = U * gch;
     if (g.tail && tch > seg_chunks) seg_chunks = tch;
     g.seg_bytes = ((seg_chunks * 512) + 127) & ~127;
-    // as many warps (<= 32) as the 227 KB shared-memory budget allows
+    // as many warps (a power of two <= 16) as the 227 KB shared-memory budget allows
     g.warps = kMaxWarps;
-    while (g.warps > 4 && scan_smem_bytes(ix, g) > 225 * 1024) g.warps -= 4;
+    while (g.warps > 2 && scan_smem_bytes(ix, g) > 225 * 1024) g.warps /= 2;  // powers of two
     return g;
 }
 
 size_t scan_smem_bytes(const DevIndex& ix, const ScanGeo& geo) {
     const int q = 1 << ix.bits;
-    size_t b = static_cast<size_t>(geo.warps) * 2 * geo.seg_bytes;
+    size_t b = static_cast<size_t>(geo.warps) * kStages * geo.seg_bytes;
     b += static_cast<size_t>(2) * q * table_rep(ix.bits) * 4;
     b += static_cast<size_t>(ix.pd) * 4;
     b += static_cast<size_t>(kToffCap + 1) * 4;
     b += static_cast<size_t>(geo.warps) * kMaxK * 8;
-    b += 8 + static_cast<size_t>(geo.warps) * 2 * 8;
+    b += 16;
     return b;
 }
 

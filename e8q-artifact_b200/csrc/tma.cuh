@@ -40,18 +40,21 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         : "memory");
 }
 
+// try_wait with a suspend-time hint: the thread sleeps until the phase
+// completes or ~1 ms passes, instead of spinning on issue slots.
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     uint32_t ok = 0;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}" : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(phase)
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(phase), "r"(1000000u)
         : "memory");
     return ok != 0;
 }
 
-// Wait for `phase` of `bar` with an iteration cap (each try_wait may itself
-// suspend for a bounded, hardware-chosen time). Returns false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, uint32_t max_iter = 1u << 22) {
+// Wait for `phase` of `bar` with an iteration cap (each try_wait suspends for
+// at most ~1 ms). Returns false on timeout (about 2 s).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, uint32_t max_iter = 2048u) {
     for (uint32_t i = 0; i < max_iter; ++i)
         if (mbar_try_wait(bar, phase)) return true;
     return false;

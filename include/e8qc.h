@@ -144,6 +144,13 @@ int e8qc_e8q_profile(e8qc_index* idx, int enable, e8qc_profile* out);
  * caller. Returns after the results are in out_ids / out_dists. */
 int e8qc_e8q_search_plain_noalloc(e8qc_index* idx, const float* queries, size_t nq, size_t k,
                                   size_t nprobe, uint32_t* out_ids, float* out_dists, void* stream);
+/* INT8 tensor-core self-test / throughput probe (no reference counterpart):
+ * C[128 x n] = A[128 x k] * B[n x k]^T (int8 x int8 -> int32, K-major rows)
+ * through tcgen05 kind::i8 with the accumulator in TMEM; `grid` CTAs each
+ * repeat the product `reps` times (CTA 0 writes C); *ms = kernel time.
+ * n: multiple of 16 in [16, 256]; k: multiple of 32 in [32, 256]. */
+int e8qc_tc_i8_gemm(int device, const int8_t* A, const int8_t* B, int n, int k, int reps, int grid,
+                    int32_t* C, float* ms);
 /* Copy the global ids, cluster-major (n entries), to a host buffer. */
 int e8qc_e8q_get_ids(const e8qc_index* idx, uint32_t* out);
 /* Export the per-vector lattice codes (cluster-major, the order of
