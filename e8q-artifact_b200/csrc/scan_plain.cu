@@ -28,7 +28,8 @@ namespace {
 __device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
 
 constexpr int kMaxWarps = 16;
-constexpr int kStages = 4;      // bulk-copy stages in flight per warp
+constexpr int kStages = 4;      // cp.async stages in flight per warp
+constexpr int kParts = 4;       // warps sharing one tile
 constexpr int kToffCap = 1024;  // tile offsets cached in shared memory
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -194,6 +195,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) scan_plain_kernel(
     uint32_t* soff = reinterpret_cast<uint32_t*>(sq + pd);           // kToffCap + 1
     float* sm_d = reinterpret_cast<float*>(soff + kToffCap + 1);      // nw * kMaxK
     uint32_t* sm_id = reinterpret_cast<uint32_t*>(sm_d + nw * kMaxK);
+    float* spart = reinterpret_cast<float*>(sm_id + nw * kMaxK);     // 2 * nw * 32
     __shared__ bool s_last;
 
     for (int i = tid; i < pd; i += nt) sq[i] = rq[i];
@@ -207,23 +209,29 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) scan_plain_kernel(
     // byte address of this lane's table copy (entry e at e*REP*4 + copy*4)
     const uint32_t tb_addr = smem_addr(tabrep) + static_cast<uint32_t>(lane % REP) * 4u;
     const uint32_t T = __ldcg(rw.total_tiles);
-    // tiles dealt round-robin over CTAs, then over the CTA's warps
+    // tiles dealt round-robin over CTAs, then over the CTA's tile groups; a
+    // group of `parts` warps shares each tile, warp `pi` decoding a contiguous
+    // range of its chunk-groups
     const uint32_t G = gridDim.x;
     const uint32_t per_cta = T > blockIdx.x ? (T - blockIdx.x + G - 1) / G : 0;
-    const uint32_t ntile_w = per_cta > static_cast<uint32_t>(warp)
-                                 ? (per_cta - warp + nw - 1) / static_cast<uint32_t>(nw) : 0;
-    // jobs: the groups of each of this warp's tiles (plus the tail half-group)
-    const int jpt = geo.ng + geo.tail;  // jobs per tile
-    const uint32_t J = ntile_w * static_cast<uint32_t>(jpt);
+    const int parts = nw < kParts ? nw : kParts;
+    const int ngrp = nw / parts;
+    const int gi = warp / parts, pi = warp % parts;
+    const uint32_t ntile_g = per_cta > static_cast<uint32_t>(gi)
+                                 ? (per_cta - gi + ngrp - 1) / static_cast<uint32_t>(ngrp) : 0;
+    const int jpt = geo.ng + geo.tail;  // chunk-group jobs per tile
+    const int j_lo = (pi * jpt) / parts, j_hi = ((pi + 1) * jpt) / parts;
+    const int jmine = j_hi - j_lo;
+    const uint32_t J = ntile_g * static_cast<uint32_t>(jmine);
     // per-warp ring of kStages chunk-group slots; lane l copies and later
     // reads only its own 16-byte entries, so the pipeline is lane-private
     const uint32_t ring_lane = smem_addr(ring) + static_cast<uint32_t>(warp * kStages * geo.seg_bytes) +
                                static_cast<uint32_t>(lane) * 16u;
-    auto tile_of = [&](uint32_t i) { return (static_cast<uint32_t>(warp) + i * nw) * G + blockIdx.x; };
+    auto tile_of = [&](uint32_t i) { return (static_cast<uint32_t>(gi) + i * ngrp) * G + blockIdx.x; };
     // every lane resolves the same tile (broadcast loads, no divergence)
     auto resolve = [&](uint32_t i) {
         TileInfo ti{nullptr, 0.0f, 0u, 0u};
-        if (i >= ntile_w) return ti;
+        if (i >= ntile_g) return ti;
         const uint32_t t = tile_of(i);
         const int p = find_probe(off, nprobe, t);
         const uint32_t list = __ldcg(rw.probes + p);
@@ -242,12 +250,12 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) scan_plain_kernel(
     TileInfo iss{nullptr, 0.0f, 0u, 0u};
     auto issue = [&](uint32_t j) {
         if (j < J) {
-            const uint32_t i = j / jpt;
+            const uint32_t i = j / jmine;
             if (i != iss_i) {
                 iss_i = i;
                 iss = resolve(i);
             }
-            const int g = static_cast<int>(j % jpt);
+            const int g = j_lo + static_cast<int>(j % jmine);
             const int c0 = g * GCH;
             const int cnt = g < geo.ng ? GCH : TCH;
             const uint32_t dst = ring_lane + static_cast<uint32_t>((j % kStages) * geo.seg_bytes);
@@ -261,29 +269,35 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) scan_plain_kernel(
     top.init(k);
     uint32_t issued = 0;
     for (; issued < kStages - 1; ++issued) issue(issued);
-    float acc0 = 0.0f, acc1 = 0.0f;
-    for (uint32_t j = 0; j < J; ++j) {
-        cp_async_wait<kStages - 2>();  // job j's group has landed (this lane's copies)
-        const int g = static_cast<int>(j % jpt);
-        const uint4* sbuf = reinterpret_cast<const uint4*>(ring + warp * kStages * geo.seg_bytes +
-                                                           (j % kStages) * geo.seg_bytes);
-        if (g < geo.ng)
-            accumulate_blocks<BITS, GBL, GCH>(sbuf, lane, sq4, g * GBL, tb_addr, acc0, acc1);
-        else
-            accumulate_blocks<BITS, 8, TCH>(sbuf, lane, sq4, geo.ng * GBL, tb_addr, acc0, acc1);
-        if (g == jpt - 1) {
-            const TileInfo cur = resolve(j / jpt);
+    // partial scores of a tile's parts, double-buffered by tile parity
+    float* my_part = spart + gi * 2 * parts * 32;
+    uint32_t j = 0;
+    for (uint32_t i = 0; i < ntile_g; ++i) {
+        float acc0 = 0.0f, acc1 = 0.0f;
+        for (int jj = 0; jj < jmine; ++jj, ++j) {
+            cp_async_wait<kStages - 2>();  // job j's group has landed (this lane's copies)
+            const int g = j_lo + jj;
+            const uint4* sbuf = reinterpret_cast<const uint4*>(ring + warp * kStages * geo.seg_bytes +
+                                                               (j % kStages) * geo.seg_bytes);
+            if (g < geo.ng)
+                accumulate_blocks<BITS, GBL, GCH>(sbuf, lane, sq4, g * GBL, tb_addr, acc0, acc1);
+            else
+                accumulate_blocks<BITS, 8, TCH>(sbuf, lane, sq4, geo.ng * GBL, tb_addr, acc0, acc1);
+            // job j's slot is free: this lane read its own entries above
+            issue(issued++);
+        }
+        my_part[((i & 1) * parts + pi) * 32 + lane] = __fadd_rn(acc0, acc1);
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + gi), "r"(parts * 32) : "memory");
+        if (pi == 0) {
+            float S = my_part[((i & 1) * parts) * 32 + lane];
+            for (int q = 1; q < parts; ++q) S = __fadd_rn(S, my_part[((i & 1) * parts + q) * 32 + lane]);
+            const TileInfo cur = resolve(i);
             const size_t slot = static_cast<size_t>(cur.slot0) + lane;
             const bool valid = static_cast<uint32_t>(lane) < cur.nvalid;
-            const float S = __fadd_rn(acc0, acc1);
             const float g1 = __ldg(ix.g1 + slot), h3 = __ldg(ix.h3 + slot);
             const float dist = __fmaf_rn(-__fmul_rn(2.0f, g1), S, __fadd_rn(cur.d2, h3));
             top.offer(dist, valid, [&] { return __ldg(ix.ids + slot); });
-            acc0 = 0.0f;
-            acc1 = 0.0f;
         }
-        // job j's slot is free: this lane read its own entries above
-        issue(issued++);
     }
     cp_async_wait<0>();
     cta_merge(top, sm_d, sm_id, k);
@@ -295,16 +309,29 @@ __global__ void __launch_bounds__(kMaxWarps * 32, 1) scan_plain_kernel(
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    // final merge: each warp folds a share of the per-CTA lists into its own
-    // top-k (batched bitonic merges), then one CTA merge
+    // final merge: stage the per-CTA lists in shared memory (the ring is free
+    // now) with coalesced loads, each warp folds a share into its own top-k
+    // (batched bitonic merges), then one CTA merge
     top.init(k);
     const int Gi = static_cast<int>(gridDim.x);
-    for (int c = warp; c < Gi; c += nw) {
-        for (int j0 = 0; j0 < k; j0 += 32) {
-            const int jj = j0 + lane;
-            const bool okj = jj < k;
-            const float dd = okj ? __ldcg(sw.part_d + static_cast<size_t>(c) * kMaxK + jj) : inf_f();
-            const uint32_t ii = okj ? __ldcg(sw.part_id + static_cast<size_t>(c) * kMaxK + jj) : 0xFFFFFFFFu;
+    const int cap = (nw * kStages * geo.seg_bytes) / 8;
+    float* st_d = reinterpret_cast<float*>(ring);
+    uint32_t* st_i = reinterpret_cast<uint32_t*>(ring) + cap;
+    const int total = Gi * k;
+    for (int e0 = 0; e0 < total; e0 += cap) {
+        const int m = min(cap, total - e0);
+        __syncthreads();
+        for (int e = tid; e < m; e += nt) {
+            const int c = (e0 + e) / k, jj = (e0 + e) - c * k;
+            st_d[e] = __ldcg(sw.part_d + static_cast<size_t>(c) * kMaxK + jj);
+            st_i[e] = __ldcg(sw.part_id + static_cast<size_t>(c) * kMaxK + jj);
+        }
+        __syncthreads();
+        for (int e = warp * 32; e < m; e += nw * 32) {
+            const int i = e + lane;
+            const bool okj = i < m;
+            const float dd = okj ? st_d[i] : inf_f();
+            const uint32_t ii = okj ? st_i[i] : 0xFFFFFFFFu;
             top.offer_pair(dd, ii, okj && ii != 0xFFFFFFFFu);
         }
     }
@@ -361,6 +388,7 @@ size_t scan_smem_bytes(const DevIndex& ix, const ScanGeo& geo) {
     b += static_cast<size_t>(ix.pd) * 4;
     b += static_cast<size_t>(kToffCap + 1) * 4;
     b += static_cast<size_t>(geo.warps) * kMaxK * 8;
+    b += static_cast<size_t>(2) * geo.warps * 32 * 4;
     b += 16;
     return b;
 }
