@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--path", choices=["plain", "batched"], default="plain")
+    ap.add_argument("--path", choices=["plain", "batched", "precision"], default="plain")
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--dim", type=int, default=960)
     ap.add_argument("--nlist", type=int, default=1024)
@@ -71,6 +71,26 @@ def peaks():
             d = json.load(f)
         return d, "measured"
     return PEAKS_FALLBACK, "fallback"
+
+
+def int8_peak(device):
+    """Dense int8 tensor-core rate (TOPS, 2 ops per multiply-add) of this GPU,
+    measured with the library's tcgen05 kind::i8 probe: one CTA per SM, each
+    issuing back-to-back 128x256x256 MMAs from shared memory."""
+    import e8qlib
+    import torch
+
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    rng = np.random.default_rng(0)
+    A = rng.integers(-8, 8, (128, 256), dtype=np.int8)
+    B = rng.integers(-8, 8, (256, 256), dtype=np.int8)
+    reps = 4000
+    e8qlib.tc_i8_gemm(A, B, reps=10, grid=sms, device=device)
+    best = 0.0
+    for _ in range(3):
+        _, ms = e8qlib.tc_i8_gemm(A, B, reps=reps, grid=sms, device=device)
+        best = max(best, 2.0 * 128 * 256 * 256 * reps * sms / (ms / 1000.0) / 1e12)
+    return best
 
 
 def workload_name(a):
@@ -247,7 +267,7 @@ def main():
     torch.cuda.synchronize()
     build_s = time.perf_counter() - t0
 
-    nb = a.batch if a.path == "batched" else a.plain_batch
+    nb = a.batch if a.path in ("batched", "precision") else a.plain_batch
     out_ids = torch.empty(nb, a.k, dtype=torch.int32, device=dev)
     out_d = torch.empty(nb, a.k, dtype=torch.float32, device=dev)
     nbat = max(1, a.pool // nb)
@@ -300,11 +320,26 @@ def main():
     t_launch = prof["scan_ms"] / max(1, prof["scan_launches"]) / 1000.0
     achieved = algo_per_launch / t_launch / 1e9 if t_launch > 0 else 0.0
     peak = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
+    kernel = {"plain": "scan_plain_kernel", "batched": "batched_scan_kernel",
+              "precision": "precision_scan_kernel"}[a.path]
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None,
-                "kernel": "scan_plain_kernel" if a.path == "plain" else "batched scan",
+                "frac": round(achieved / peak, 4), "traffic": None, "kernel": kernel,
                 "algo_bytes_per_launch": int(algo_per_launch),
                 "launch_us": round(t_launch * 1e6, 2), "peak_kind": pk_kind}
+    if a.path == "precision":
+        # tensor roofline: int8 multiply-adds (2 ops each) of every scored
+        # (query, vector) pair over the padded dimension, against the int8
+        # tcgen05 MMA rate measured on this GPU by the library's own probe
+        pd = (a.dim + 63) // 64 * 64
+        ops = 2.0 * prof["candidates"] * pd / max(1, prof["scan_launches"])
+        i8_peak = int8_peak(local)
+        tops = ops / t_launch / 1e12 if t_launch > 0 else 0.0
+        roofline = {"bound": "tensor", "achieved": round(tops, 1), "peak": round(i8_peak, 1),
+                    "unit": "TFLOP/s", "frac": round(tops / i8_peak, 4), "traffic": None, "kernel": kernel,
+                    "ops_per_launch": ops, "launch_us": round(t_launch * 1e6, 2),
+                    "peak_kind": "int8 dense tcgen05 MMA rate measured in this run (e8qlib.tc_i8_gemm, "
+                                 "148 CTAs x 128x256x256 back-to-back MMAs)",
+                    "hbm_achieved_gbs": round(achieved, 1), "hbm_peak_gbs": peak}
 
     # e2e through the public numpy API with pinned host queries
     qh = torch.empty(a.pool, a.dim, dtype=torch.float32, pin_memory=True)
@@ -347,7 +382,9 @@ def main():
         "metric": "QPS@recall10>=0.95 (E8Q IVF search, 1 query batch per step)",
         "value": round(value, 1), "unit": "QPS", "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "fp32 (u8 lattice codes)",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": ("int8 tensor-core candidates + fp32 exact rescoring (u8 lattice codes)"
+                  if a.path == "precision" else "fp32 (u8 lattice codes)"),
         "data": "synthetic (seeded Gaussian mixture generated on the GPU)",
         "config": {"workload": workload_name(a), "n": a.n, "dim": a.dim, "nlist": a.nlist,
                    "nbits": a.nbits, "k": a.k, "nprobe": a.nprobe, "query_batch": nb,

@@ -212,11 +212,11 @@ __global__ void select_kernel(const uint64_t* __restrict__ keys, int nlist, cons
     }
 }
 
-// Items: list order `order`, per list ceil(cnt / QT) items. One CTA scans the
+// Items: list order `order`, per list ceil(cnt / qt) items. One CTA scans the
 // lists (nlist is small) and writes pair offsets and item descriptors.
 __global__ void items_kernel(const uint32_t* __restrict__ list_cnt, const uint32_t* __restrict__ order,
                              int nlist, uint32_t* __restrict__ pair_off, uint32_t* __restrict__ fill,
-                             uint4* __restrict__ items, uint32_t* __restrict__ n_items, int item_cap) {
+                             uint4* __restrict__ items, uint32_t* __restrict__ n_items, int item_cap, uint32_t qt) {
     __shared__ int sm32[32];
     __shared__ uint32_t s_pairs, s_items;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
@@ -229,7 +229,7 @@ __global__ void items_kernel(const uint32_t* __restrict__ list_cnt, const uint32
         const int i = i0 + tid;
         const uint32_t L = i < nlist ? order[i] : 0;
         const uint32_t cnt = i < nlist ? list_cnt[L] : 0;
-        const uint32_t nit = (cnt + kQT - 1) / kQT;
+        const uint32_t nit = (cnt + qt - 1) / qt;
         // two block scans (pairs, items)
         uint32_t xp = cnt, xi = nit;
 #pragma unroll
@@ -268,7 +268,7 @@ __global__ void items_kernel(const uint32_t* __restrict__ list_cnt, const uint32
             for (uint32_t t = 0; t < nit; ++t) {
                 const uint32_t idx = ibase + t;
                 if (static_cast<int>(idx) < item_cap)
-                    items[idx] = make_uint4(L, pbase + t * kQT, min(static_cast<uint32_t>(kQT), cnt - t * kQT), 0u);
+                    items[idx] = make_uint4(L, pbase + t * qt, min(qt, cnt - t * qt), 0u);
             }
         }
         __syncthreads();
@@ -357,7 +357,10 @@ __global__ void __launch_bounds__(kBT) batched_scan_kernel(
         __syncthreads();
         const uint32_t len = ix.list_len[L];
         const uint32_t tile0 = ix.tile_begin[L];
-        if (tid == 0) atomicAdd(cand_count, static_cast<unsigned long long>(len) * m);
+        if (tid == 0) {
+            atomicAdd(cand_count, static_cast<unsigned long long>(len) * m);  // (query, vector) pairs
+            atomicAdd(cand_count + 1, static_cast<unsigned long long>(len));  // vectors read
+        }
         for (uint32_t v0 = 0; v0 < len; v0 += kVT) {
             float acc[4][8];
 #pragma unroll
@@ -551,17 +554,13 @@ size_t batched_scan_smem(const DevIndex& ix, int k_max) {
     return (static_cast<size_t>(2) * kKC * kQT + 2 * kKC * kVT + 2 * (1 << ix.bits) + 2 * kQT * k_max) * 4;
 }
 
-int batched_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* k_arr,
-                   const uint32_t* np_arr, size_t k, size_t nprobe, size_t out_stride, uint32_t* out_ids,
-                   float* out_d, size_t max_tiles, cudaStream_t s) {
-    (void)max_tiles;
-    if (nq == 0) return 0;
+int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* np_arr,
+                    size_t nprobe, size_t part_width, int qt, cudaStream_t s) {
     const int nlist = ix.nlist;
-    const int k_max = static_cast<int>(k);
     const int np_max = static_cast<int>(nprobe);
     const size_t npairs = nq * static_cast<size_t>(np_max);
-    // upper bound of items: pairs/QT + one partial item per list
-    const size_t item_cap = npairs / kQT + static_cast<size_t>(nlist) + 1;
+    // upper bound of items: pairs/qt + one partial item per list
+    const size_t item_cap = npairs / qt + static_cast<size_t>(nlist) + 1;
     ws.b_keys.ensure(nq * static_cast<size_t>(nlist) * 8);
     ws.b_qn2.ensure(nq * 4);
     ws.b_probes.ensure(npairs * 4);
@@ -573,9 +572,9 @@ int batched_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq
     ws.b_off.ensure(static_cast<size_t>(nlist) * 4);
     ws.b_fill.ensure(static_cast<size_t>(nlist) * 4);
     ws.b_items.ensure(item_cap * 16);
-    ws.b_nitems.ensure(16);
-    ws.b_part_d.ensure(npairs * k_max * 4);
-    ws.b_part_id.ensure(npairs * k_max * 4);
+    ws.b_nitems.ensure(32);
+    ws.b_part_d.ensure(npairs * part_width * 4);
+    ws.b_part_id.ensure(npairs * part_width * 4);
     int launches = 0;
     qn2_kernel<<<static_cast<unsigned>(nq), 256, 0, s>>>(rq, ix.pd, ws.b_qn2.as<float>());
     ++launches;
@@ -584,7 +583,7 @@ int batched_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq
                                         ws.b_keys.as<uint64_t>());
     ++launches;
     E8QC_CUDA(cudaMemsetAsync(ws.b_cnt.p, 0, static_cast<size_t>(nlist) * 4, s));
-    E8QC_CUDA(cudaMemsetAsync(ws.b_nitems.p, 0, 16, s));  // [0] n_items, [1] head, [2..3] candidates
+    E8QC_CUDA(cudaMemsetAsync(ws.b_nitems.p, 0, 32, s));  // [0] n_items, [1] head, [2..5] pair/vector counts
     const size_t sel_smem = static_cast<size_t>(nlist) * 8;
     if (sel_smem > 200 * 1024) fail(E8QC_EINVAL, "batched route supports at most 25600 lists");
     if (sel_smem > 48 * 1024)
@@ -597,16 +596,30 @@ int batched_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq
     uint32_t* nitems = ws.b_nitems.as<uint32_t>();
     items_kernel<<<1, 1024, 0, s>>>(ws.b_cnt.as<uint32_t>(), ix.list_order, nlist, ws.b_off.as<uint32_t>(),
                                     ws.b_fill.as<uint32_t>(), ws.b_items.as<uint4>(), nitems,
-                                    static_cast<int>(item_cap));
+                                    static_cast<int>(item_cap), static_cast<uint32_t>(qt));
     ++launches;
     scatter_kernel<<<static_cast<unsigned>((npairs + 255) / 256), 256, 0, s>>>(
         ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(), static_cast<int>(nq), np_arr, np_max, np_max,
         ws.b_off.as<uint32_t>(), ws.b_fill.as<uint32_t>(), ws.b_pair_q.as<uint32_t>(), ws.b_pair_d2.as<float>(),
         ws.b_pos.as<uint32_t>());
     ++launches;
+    E8QC_CUDA(cudaGetLastError());
+    return launches;
+}
+
+int batched_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* k_arr,
+                   const uint32_t* np_arr, size_t k, size_t nprobe, size_t out_stride, uint32_t* out_ids,
+                   float* out_d, size_t max_tiles, cudaStream_t s) {
+    (void)max_tiles;
+    if (nq == 0) return 0;
+    const int k_max = static_cast<int>(k);
+    const int np_max = static_cast<int>(nprobe);
+    int launches = batched_prepare(ix, ws, rq, nq, np_arr, nprobe, k, kQT, s);
+    uint32_t* nitems = ws.b_nitems.as<uint32_t>();
     const size_t smem = batched_scan_smem(ix, k_max);
     int dev = 0;
     E8QC_CUDA(cudaGetDevice(&dev));
+    ws.mark_scan(false, s);
     switch (ix.bits) {
 #define E8QC_CASE(b) \
     case b: launch_batched_scan<b>(ix, rq, ws, nitems, k_arr, k_max, smem, dev, s); break;
@@ -616,6 +629,7 @@ int batched_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq
 #undef E8QC_CASE
         default: fail(E8QC_EINVAL, "bits out of range");
     }
+    ws.mark_scan(true, s);
     ++launches;
     merge_kernel<<<static_cast<unsigned>((nq + 3) / 4), 128, 0, s>>>(
         ws.b_part_d.as<float>(), ws.b_part_id.as<uint32_t>(), ws.b_pos.as<uint32_t>(), static_cast<int>(nq), np_arr,

@@ -48,7 +48,8 @@ void check(int rc) {
 int mode_of(const std::string& m) {
     if (m == "plain") return E8QC_MODE_PLAIN;
     if (m == "batched") return E8QC_MODE_BATCHED;
-    throw std::invalid_argument("mode must be 'plain' or 'batched'");
+    if (m == "precision") return E8QC_MODE_PRECISION;
+    throw std::invalid_argument("mode must be 'plain', 'batched' or 'precision'");
 }
 
 class E8qIndex {
@@ -135,7 +136,9 @@ class E8qIndex {
     }
 
     // Serving form: per-query k and nprobe; rows padded to k_max.
-    py::tuple search_ragged(py::handle queries, py::handle k, py::handle nprobe, size_t k_max) {
+    py::tuple search_ragged(py::handle queries, py::handle k, py::handle nprobe, size_t k_max,
+                            const std::string& mode) {
+        const int md = mode_of(mode);
         auto q = ensure_nd<float>(queries, "queries", 2);
         auto ka = ensure_nd<uint32_t>(k, "k", 1);
         auto na = ensure_nd<uint32_t>(nprobe, "nprobe", 1);
@@ -150,8 +153,8 @@ class E8qIndex {
         {
             py::gil_scoped_release nogil;
             if (nq > 0)
-                check(e8qc_e8q_search_ragged(idx_, q.data(), nq, ka.data(), na.data(), k_max,
-                                             ids.mutable_data(), dists.mutable_data(), nullptr, nullptr));
+                check(e8qc_e8q_search_ragged_mode(idx_, q.data(), nq, ka.data(), na.data(), k_max, md,
+                                                  ids.mutable_data(), dists.mutable_data(), nullptr, nullptr));
         }
         return py::make_tuple(ids, dists);
     }
@@ -203,6 +206,7 @@ class E8qIndex {
         d["candidates"] = p.candidates;
         d["algo_bytes"] = p.algo_bytes;
         d["queries"] = p.queries;
+        d["list_vectors"] = p.list_vectors;
         return d;
     }
 
@@ -319,7 +323,7 @@ PYBIND11_MODULE(_e8qlib, m) {
              py::arg("nprobe"), py::arg("out_ids"), py::arg("out_dists"), py::arg("mode") = "plain",
              py::arg("stream") = 0)
         .def("search_ragged", &E8qIndex::search_ragged, py::arg("queries"), py::arg("k"),
-             py::arg("nprobe"), py::arg("k_max"))
+             py::arg("nprobe"), py::arg("k_max"), py::arg("mode") = "batched")
         .def("estimate", &E8qIndex::estimate, py::arg("query"), py::arg("id"))
         .def("set_disable_prune", &E8qIndex::set_disable_prune, py::arg("on"))
         .def("set_prune_alpha", &E8qIndex::set_prune_alpha, py::arg("alpha"))

@@ -19,6 +19,7 @@
 #include "e8qc.h"
 #include "internal.h"
 #include "scan_plain.h"
+#include "precision.h"
 #include "workspace.h"
 
 namespace e8qc {
@@ -197,6 +198,44 @@ void plain_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size_
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (st) st->launches += launches;
+}
+
+// Batched or precision search of nq rotated queries; while profiling, times
+// the scan kernel with CUDA events and reads back its pair / vector counters.
+uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, const uint32_t* k_arr,
+                        const uint32_t* np_arr, size_t k, size_t np, uint32_t* ids_d, float* d_d, cudaStream_t s) {
+    Workspace& ws = x->ws;
+    if (x->profiling) {
+        E8QC_CUDA(cudaEventCreate(&ws.scan_ev0));
+        E8QC_CUDA(cudaEventCreate(&ws.scan_ev1));
+    }
+    struct Drop {
+        Workspace& w;
+        ~Drop() {
+            if (w.scan_ev0) cudaEventDestroy(w.scan_ev0);
+            if (w.scan_ev1) cudaEventDestroy(w.scan_ev1);
+            w.scan_ev0 = w.scan_ev1 = nullptr;
+        }
+    } drop{ws};
+    int launches = 0;
+    if (mode == E8QC_MODE_PRECISION)
+        launches = precision_search(x->view, ws, rq, nq, k_arr, np_arr, k, np, k, ids_d, d_d, s);
+    else
+        launches = batched_search(x->view, ws, rq, nq, k_arr, np_arr, k, np, k, ids_d, d_d, max_tiles_for(x, np), s);
+    if (x->profiling) {
+        uint64_t cnt[2] = {0, 0};
+        E8QC_CUDA(cudaMemcpyAsync(cnt, ws.b_nitems.as<uint32_t>() + 2, 16, cudaMemcpyDeviceToHost, s));
+        E8QC_CUDA(cudaStreamSynchronize(s));
+        float ms = 0.0f;
+        E8QC_CUDA(cudaEventElapsedTime(&ms, ws.scan_ev0, ws.scan_ev1));
+        x->prof.scan_launches += 1;
+        x->prof.scan_ms += ms;
+        x->prof.candidates += cnt[0];
+        x->prof.list_vectors += cnt[1];
+        x->prof.algo_bytes += cnt[1] * (static_cast<uint64_t>(x->bits) * x->pd / 8 + 8);
+        x->prof.queries += nq;
+    }
+    return static_cast<uint64_t>(launches);
 }
 
 }  // namespace
@@ -444,6 +483,7 @@ int e8qc_e8q_build(e8qc_index* x, const float* data, size_t n, const float* cent
         v.ids = x->ids.as<uint32_t>();
         v.tab = x->tab.as<float>();
         v.list_order = x->list_order.as<uint32_t>();
+        v.list_of_tile = x->list_of_tile.as<uint32_t>();
         const DevEncTables& et = enc_tables_device(x->device, x->bits);
         BuildEncodeArgs a{};
         a.base = data_d;
@@ -465,7 +505,8 @@ int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, si
         if (k == 0) fail(E8QC_EINVAL, "k must be positive");
         if (k > static_cast<size_t>(kMaxK)) fail(E8QC_EINVAL, "k must be <= 128");
         if (nprobe == 0) fail(E8QC_EINVAL, "nprobe must be positive");
-        if (mode != E8QC_MODE_PLAIN && mode != E8QC_MODE_BATCHED) fail(E8QC_EINVAL, "unknown search mode");
+        if (mode != E8QC_MODE_PLAIN && mode != E8QC_MODE_BATCHED && mode != E8QC_MODE_PRECISION)
+            fail(E8QC_EINVAL, "unknown search mode");
         if (nq == 0) return;
         if (!queries || !out_ids) fail(E8QC_EINVAL, "null buffer");
         std::lock_guard<std::mutex> lock(x->mu);
@@ -492,8 +533,7 @@ int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, si
         if (mode == E8QC_MODE_PLAIN) {
             plain_search(x, rq, nq, k, np, ids_d, d_d, stats, s);
         } else {
-            launches += batched_search(x->view, x->ws, rq, nq, nullptr, nullptr, k, np, k, ids_d, d_d,
-                                       max_tiles_for(x, np), s);
+            launches += grouped_search(x, mode, rq, nq, nullptr, nullptr, k, np, ids_d, d_d, s);
         }
         if (stats) E8QC_CUDA(cudaEventRecord(ev[2], s));
         if (!ids_dev) E8QC_CUDA(cudaMemcpyAsync(out_ids, ids_d, nq * k * 4, cudaMemcpyDeviceToHost, s));
@@ -517,8 +557,17 @@ int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, si
 int e8qc_e8q_search_ragged(e8qc_index* x, const float* queries, size_t nq, const uint32_t* k,
                            const uint32_t* nprobe, size_t k_max, uint32_t* out_ids, float* out_dists,
                            e8qc_stats* stats, void* stream) {
+    return e8qc_e8q_search_ragged_mode(x, queries, nq, k, nprobe, k_max, E8QC_MODE_BATCHED, out_ids, out_dists,
+                                       stats, stream);
+}
+
+int e8qc_e8q_search_ragged_mode(e8qc_index* x, const float* queries, size_t nq, const uint32_t* k,
+                                const uint32_t* nprobe, size_t k_max, int mode, uint32_t* out_ids,
+                                float* out_dists, e8qc_stats* stats, void* stream) {
     return guarded([&] {
         require_built(x, "search");
+        if (mode != E8QC_MODE_BATCHED && mode != E8QC_MODE_PRECISION)
+            fail(E8QC_EINVAL, "ragged search runs the batched or precision mode");
         if (k_max == 0 || k_max > static_cast<size_t>(kMaxK)) fail(E8QC_EINVAL, "k_max must be in [1, 128]");
         if (nq == 0) return;
         if (!queries || !k || !nprobe || !out_ids) fail(E8QC_EINVAL, "null buffer");
@@ -552,8 +601,8 @@ int e8qc_e8q_search_ragged(e8qc_index* x, const float* queries, size_t nq, const
         x->ws.ensure_queries(nq, x->pd);
         float* rq = x->ws.rq.as<float>();
         uint64_t launches = launch_rotate(x->view, qd, static_cast<int>(nq), rq, s);
-        launches += batched_search(x->view, x->ws, rq, nq, tk.as<uint32_t>(), tnp.as<uint32_t>(), k_max,
-                                   np_max, k_max, ids_d, d_d, max_tiles_for(x, np_max), s);
+        launches += grouped_search(x, mode, rq, nq, tk.as<uint32_t>(), tnp.as<uint32_t>(), k_max, np_max, ids_d,
+                                   d_d, s);
         if (!ids_dev) E8QC_CUDA(cudaMemcpyAsync(out_ids, ids_d, nq * k_max * 4, cudaMemcpyDeviceToHost, s));
         if (out_dists && !d_dev) E8QC_CUDA(cudaMemcpyAsync(out_dists, d_d, nq * k_max * 4, cudaMemcpyDeviceToHost, s));
         x->ws.check_error(s);

@@ -99,6 +99,7 @@ struct DevIndex {
     const uint32_t* ids;         // ntiles*32, UINT32_MAX on padding lanes
     const float* tab;            // [2][2^bits] level/sqrt(pd) refine tables
     const uint32_t* list_order;  // nlist list ids, longest list first
+    const uint32_t* list_of_tile;  // ntiles: the list each tile belongs to
 };
 
 inline int code_chunks(int pd, int bits) { return (pd / 8 * 8 * bits + 127) / 128; }

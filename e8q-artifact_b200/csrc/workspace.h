@@ -59,6 +59,15 @@ struct Workspace {
     // batched path (grown on demand by batched_search)
     DevBuf b_keys, b_qn2, b_probes, b_pd2, b_pos, b_pair_q, b_pair_d2, b_cnt, b_off, b_fill, b_items,
         b_nitems, b_part_d, b_part_id;
+    // precision path: int8 queries, per-query scale and sum
+    DevBuf p_q8, p_scale, p_sum;
+    // optional CUDA events around the batched / precision scan kernel (set by
+    // the caller while profiling; recorded on the launch stream)
+    cudaEvent_t scan_ev0 = nullptr, scan_ev1 = nullptr;
+    void mark_scan(bool end, cudaStream_t s) {
+        cudaEvent_t e = end ? scan_ev1 : scan_ev0;
+        if (e) E8QC_CUDA(cudaEventRecord(e, s));
+    }
 
     ~Workspace() {
         if (err_host) cudaFreeHost(err_host);
@@ -116,5 +125,12 @@ int batched_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq
                    const uint32_t* k_arr, const uint32_t* np_arr, size_t k, size_t nprobe,
                    size_t out_stride, uint32_t* out_ids, float* out_d, size_t max_tiles,
                    cudaStream_t s);
+
+// Route + per-query select + grouping of (query, list) pairs into work items
+// of up to qt queries per list (shared by the batched and precision paths);
+// partial-result buffers hold part_width entries per pair. Returns the number
+// of kernels launched.
+int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* np_arr,
+                    size_t nprobe, size_t part_width, int qt, cudaStream_t s);
 
 }  // namespace e8qc

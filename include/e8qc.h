@@ -45,6 +45,13 @@ extern "C" {
  * fp32 rounding). */
 #define E8QC_MODE_PLAIN 0
 #define E8QC_MODE_BATCHED 1
+/* PRECISION (an addition of this library, no counterpart in the reference):
+ * batch grouped by list as in BATCHED, but candidates are generated on the
+ * INT8 tensor cores from an integer proxy of the codes and int8 queries; each
+ * query's best max(64, 4k) (at most 128) proxy candidates are then rescored
+ * with the exact estimator. Distances returned are exact; recall against the
+ * exact scan is measured, not guaranteed. */
+#define E8QC_MODE_PRECISION 2
 
 /* Maximum top-k (include/e8qlib/index/e8q.hpp:44 kMaxK). */
 #define E8QC_MAX_K 128
@@ -109,6 +116,12 @@ int e8qc_e8q_search_ragged(e8qc_index* idx, const float* queries, size_t nq,
                            const uint32_t* k, const uint32_t* nprobe, size_t k_max,
                            uint32_t* out_ids, float* out_dists, e8qc_stats* stats,
                            void* stream);
+/* Ragged search with an explicit mode (E8QC_MODE_BATCHED or
+ * E8QC_MODE_PRECISION); e8qc_e8q_search_ragged is this with BATCHED. An
+ * addition of this library: the serving loop's entry for mixed batches. */
+int e8qc_e8q_search_ragged_mode(e8qc_index* idx, const float* queries, size_t nq, const uint32_t* k,
+                                const uint32_t* nprobe, size_t k_max, int mode, uint32_t* out_ids,
+                                float* out_dists, e8qc_stats* stats, void* stream);
 /* E8qIndex::Estimate (e8q.hpp:151-152): estimated squared L2 of stored id. */
 int e8qc_e8q_estimate(e8qc_index* idx, const float* query, uint32_t id, float* out);
 /* E8qIndex::SetDisablePrune / SetPruneAlpha (e8q.hpp:173-180). The GPU paths
@@ -127,6 +140,7 @@ typedef struct e8qc_profile {
     uint64_t candidates;     /* (query, vector) pairs scored */
     uint64_t algo_bytes;     /* candidates * (bits*padded_dim/8 + 8): codes + g1/h3 */
     uint64_t queries;
+    uint64_t list_vectors;   /* vectors read from the lists (batched modes: once per work item) */
 } e8qc_profile;
 int e8qc_e8q_profile(e8qc_index* idx, int enable, e8qc_profile* out);
 /* Plain search that allocates nothing (no counterpart in the reference; an
