@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--path", choices=["plain", "batched", "precision"], default="plain")
+    ap.add_argument("--path", choices=["plain", "batched", "precision"], default="precision")
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--dim", type=int, default=960)
     ap.add_argument("--nlist", type=int, default=1024)
@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--gt", type=int, default=1000, help="queries with FP64 ground truth")
     ap.add_argument("--plain-batch", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the open-loop serving leg")
+    ap.add_argument("--serve-seconds", type=float, default=3.0)
+    ap.add_argument("--serve-loads", default="0.3,0.6", help="offered load as fractions of the batch QPS")
     ap.add_argument("--seed", type=int, default=0)
     return ap.parse_args()
 
@@ -200,6 +203,50 @@ class Clocks:
         reasons = sorted({names[i] for r in busy for i, v in enumerate(r[2]) if v.lower() == "active"})
         return {"sm_mhz": statistics.median(r[0] for r in busy), "sm_max_mhz": max(r[1] for r in rows),
                 "reasons": reasons, "samples": len(busy)}
+
+
+def serve_open_loop(e8qlib, idx, mode, qn, k, nprobe, rate_qps, seconds, seed, max_batch):
+    """Open-loop Poisson arrivals through e8qlib.Server: requests of U{1..64}
+    queries (k, nprobe fixed), exponential inter-arrival times at rate_qps /
+    32.5 requests per second; one thread submits on schedule, another collects.
+    Returns the server's stats (latency submit -> results ready)."""
+    import threading
+
+    rng = np.random.default_rng(seed)
+    req_rate = rate_qps / 32.5
+    n_req = max(1, int(req_rate * seconds))
+    gaps = rng.exponential(1.0 / req_rate, n_req)
+    sizes = rng.integers(1, 65, n_req)
+    starts = rng.integers(0, qn.shape[0] - 64, n_req)
+    srv = e8qlib.Server(idx, mode=mode, max_batch=max_batch, max_k=max(k, 1), slots=2)
+    ids = []
+    done = threading.Event()
+
+    def collect():
+        i = 0
+        while i < n_req:
+            if i < len(ids):
+                srv.result(ids[i], timeout_ms=-1)
+                i += 1
+            else:
+                time.sleep(0.0002)
+        done.set()
+
+    th = threading.Thread(target=collect)
+    th.start()
+    t = time.perf_counter()
+    for j in range(n_req):
+        t += gaps[j]
+        while time.perf_counter() < t:
+            pass
+        ids.append(srv.submit(qn[starts[j]:starts[j] + sizes[j]], k, nprobe))
+    done.wait()
+    th.join()
+    st = srv.stats()
+    srv.stop()
+    st["offered_qps"] = round(rate_qps, 1)
+    st["requests"] = n_req
+    return st
 
 
 def cpu_baseline(a, x_host, cm_host, lab_host, q_host, gt, steps=None, warmup=None):
@@ -363,6 +410,35 @@ def main():
     e2e = {"value": round(total_q / (e2e_ms / 1000.0), 1), "unit": "QPS",
            "h2d_bytes_per_step": nb * a.dim * 4, "d2h_bytes_per_step": nb * a.k * 8}
 
+    # the plain one-query-per-launch GPU scan on the same index (the drop-in
+    # path the batched modes are compared against), a short device-resident run
+    plain_qps = None
+    if a.path != "plain":
+        pb = 256
+        pi = torch.empty(pb, a.k, dtype=torch.int32, device=dev)
+        pdd = torch.empty(pb, a.k, dtype=torch.float32, device=dev)
+        idx.search_ptr(q.data_ptr(), 32, a.k, a.nprobe, pi.data_ptr(), pdd.data_ptr(), "plain", sp)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        idx.search_ptr(q[pb:2 * pb].data_ptr(), pb, a.k, a.nprobe, pi.data_ptr(), pdd.data_ptr(), "plain", sp)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        plain_qps = pb / (p0.elapsed_time(p1) / 1000.0)
+
+    # serving: open-loop Poisson load through the server at fractions of the
+    # measured batch throughput
+    serving = None
+    if a.path != "plain" and not a.no_serve:
+        serving = []
+        for frac in [float(f) for f in a.serve_loads.split(",") if f]:
+            st = serve_open_loop(e8qlib, idx, a.path, qn, a.k, a.nprobe, frac * value, a.serve_seconds,
+                                 a.seed + 7, a.batch)
+            serving.append({"offered_qps": st["offered_qps"], "achieved_qps": round(st["qps"], 1),
+                            "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
+                            "max_ms": round(st["max_ms"], 3), "requests": st["requests"],
+                            "mean_batch_queries": round(st["mean_batch_queries"], 1)})
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         xh = x.cpu().numpy()
@@ -393,6 +469,8 @@ def main():
         "recall_at_10": round(recall, 4), "build_s": round(build_s, 2),
         "clocks": clk.summary(), "gpu_launches": int(launches), "roofline": roofline,
         "e2e": e2e, "cpu_baseline": cpu,
+        "plain_gpu_qps": None if plain_qps is None else round(plain_qps, 1),
+        "serving": serving,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -216,7 +216,8 @@ __global__ void select_kernel(const uint64_t* __restrict__ keys, int nlist, cons
 // lists (nlist is small) and writes pair offsets and item descriptors.
 __global__ void items_kernel(const uint32_t* __restrict__ list_cnt, const uint32_t* __restrict__ order,
                              int nlist, uint32_t* __restrict__ pair_off, uint32_t* __restrict__ fill,
-                             uint4* __restrict__ items, uint32_t* __restrict__ n_items, int item_cap, uint32_t qt) {
+                             uint4* __restrict__ items, uint32_t* __restrict__ n_items, int item_cap, uint32_t qt,
+                             uint32_t align) {
     __shared__ int sm32[32];
     __shared__ uint32_t s_pairs, s_items;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
@@ -229,9 +230,10 @@ __global__ void items_kernel(const uint32_t* __restrict__ list_cnt, const uint32
         const int i = i0 + tid;
         const uint32_t L = i < nlist ? order[i] : 0;
         const uint32_t cnt = i < nlist ? list_cnt[L] : 0;
+        const uint32_t cpad = (cnt + align - 1) / align * align;  // each list's pairs start aligned
         const uint32_t nit = (cnt + qt - 1) / qt;
         // two block scans (pairs, items)
-        uint32_t xp = cnt, xi = nit;
+        uint32_t xp = cpad, xi = nit;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t yp = __shfl_up_sync(kFull, xp, o), yi = __shfl_up_sync(kFull, xi, o);
@@ -260,7 +262,7 @@ __global__ void items_kernel(const uint32_t* __restrict__ list_cnt, const uint32
             wi[lane] = si;
         }
         __syncthreads();
-        const uint32_t pbase = s_pairs + (warp > 0 ? wp[warp - 1] : 0) + xp - cnt;
+        const uint32_t pbase = s_pairs + (warp > 0 ? wp[warp - 1] : 0) + xp - cpad;
         const uint32_t ibase = s_items + (warp > 0 ? wi[warp - 1] : 0) + xi - nit;
         if (i < nlist) {
             pair_off[L] = pbase;
@@ -555,10 +557,12 @@ size_t batched_scan_smem(const DevIndex& ix, int k_max) {
 }
 
 int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* np_arr,
-                    size_t nprobe, size_t part_width, int qt, cudaStream_t s) {
+                    size_t nprobe, size_t part_width, int qt, int align, cudaStream_t s) {
     const int nlist = ix.nlist;
     const int np_max = static_cast<int>(nprobe);
     const size_t npairs = nq * static_cast<size_t>(np_max);
+    // pair slots: aligned list starts leave up to align-1 unused slots per list
+    const size_t pslots = npairs + static_cast<size_t>(align - 1) * nlist;
     // upper bound of items: pairs/qt + one partial item per list
     const size_t item_cap = npairs / qt + static_cast<size_t>(nlist) + 1;
     ws.b_keys.ensure(nq * static_cast<size_t>(nlist) * 8);
@@ -566,8 +570,8 @@ int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t n
     ws.b_probes.ensure(npairs * 4);
     ws.b_pd2.ensure(npairs * 4);
     ws.b_pos.ensure(npairs * 4);
-    ws.b_pair_q.ensure(npairs * 4);
-    ws.b_pair_d2.ensure(npairs * 4);
+    ws.b_pair_q.ensure(pslots * 4);
+    ws.b_pair_d2.ensure(pslots * 4);
     ws.b_cnt.ensure(static_cast<size_t>(nlist) * 4);
     ws.b_off.ensure(static_cast<size_t>(nlist) * 4);
     ws.b_fill.ensure(static_cast<size_t>(nlist) * 4);
@@ -596,8 +600,11 @@ int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t n
     uint32_t* nitems = ws.b_nitems.as<uint32_t>();
     items_kernel<<<1, 1024, 0, s>>>(ws.b_cnt.as<uint32_t>(), ix.list_order, nlist, ws.b_off.as<uint32_t>(),
                                     ws.b_fill.as<uint32_t>(), ws.b_items.as<uint4>(), nitems,
-                                    static_cast<int>(item_cap), static_cast<uint32_t>(qt));
+                                    static_cast<int>(item_cap), static_cast<uint32_t>(qt),
+                                    static_cast<uint32_t>(align));
     ++launches;
+    // unused slots keep the query id UINT32_MAX
+    if (align > 1) E8QC_CUDA(cudaMemsetAsync(ws.b_pair_q.p, 0xFF, pslots * 4, s));
     scatter_kernel<<<static_cast<unsigned>((npairs + 255) / 256), 256, 0, s>>>(
         ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(), static_cast<int>(nq), np_arr, np_max, np_max,
         ws.b_off.as<uint32_t>(), ws.b_fill.as<uint32_t>(), ws.b_pair_q.as<uint32_t>(), ws.b_pair_d2.as<float>(),
@@ -614,7 +621,7 @@ int batched_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq
     if (nq == 0) return 0;
     const int k_max = static_cast<int>(k);
     const int np_max = static_cast<int>(nprobe);
-    int launches = batched_prepare(ix, ws, rq, nq, np_arr, nprobe, k, kQT, s);
+    int launches = batched_prepare(ix, ws, rq, nq, np_arr, nprobe, k, kQT, 1, s);
     uint32_t* nitems = ws.b_nitems.as<uint32_t>();
     const size_t smem = batched_scan_smem(ix, k_max);
     int dev = 0;

@@ -14,6 +14,7 @@
 #include <limits>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "e8qc.h"
@@ -254,6 +255,110 @@ class E8qIndex {
     int device_ = 0;
     bool built_ = false;
     e8qc_index* idx_ = nullptr;
+
+   public:
+    e8qc_index* handle(const char* what) const {
+        require(what);
+        return idx_;
+    }
+};
+
+// Serving loop over one index (an addition of this library; see
+// e8qc_server_* in e8qc.h). Holds a reference to the Python index so it
+// outlives the server.
+class Server {
+   public:
+    Server(py::object index, const std::string& mode, size_t max_batch, size_t max_k, size_t max_nprobe,
+           size_t memory_budget, int slots)
+        : index_(index) {
+        E8qIndex& ix = index.cast<E8qIndex&>();
+        dim_ = ix.dim();
+        e8qc_server_config c{};
+        c.mode = mode_of(mode);
+        if (c.mode == E8QC_MODE_PLAIN) throw std::invalid_argument("the server runs 'batched' or 'precision'");
+        c.max_batch_queries = max_batch;
+        c.max_k = max_k;
+        c.max_nprobe = max_nprobe;
+        c.memory_budget = memory_budget;
+        c.slots = slots;
+        e8qc_index* h = ix.handle("serve");
+        py::gil_scoped_release nogil;
+        check(e8qc_server_start(h, &c, &srv_));
+    }
+    ~Server() {
+        try {
+            stop();
+        } catch (...) {
+        }
+    }
+    uint64_t submit(py::handle queries, size_t k, size_t nprobe) {
+        if (!srv_) throw std::runtime_error("server is stopped");
+        auto q = ensure_nd<float>(queries, "queries", 2);
+        if (static_cast<size_t>(q.shape(1)) != dim_)
+            throw std::invalid_argument("query dimension does not match index dim");
+        const size_t nq = static_cast<size_t>(q.shape(0));
+        uint64_t id = 0;
+        {
+            py::gil_scoped_release nogil;
+            check(e8qc_server_submit(srv_, q.data(), nq, k, nprobe, &id));
+        }
+        shapes_[id] = {nq, k};
+        return id;
+    }
+    py::object result(uint64_t id, int timeout_ms) {
+        if (!srv_) throw std::runtime_error("server is stopped");
+        auto it = shapes_.find(id);
+        if (it == shapes_.end()) throw py::index_error("unknown or already collected request id");
+        const size_t nq = it->second.first, k = it->second.second;
+        py::array_t<uint32_t> ids({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k)});
+        py::array_t<float> dists({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k)});
+        int done = 0, rc = 0;
+        {
+            py::gil_scoped_release nogil;
+            rc = e8qc_server_poll(srv_, id, timeout_ms, ids.mutable_data(), dists.mutable_data(), &done);
+        }
+        if (done) shapes_.erase(id);
+        check(rc);
+        if (!done) return py::none();
+        return py::make_tuple(ids, dists);
+    }
+    py::dict stats(bool reset) {
+        if (!srv_) throw std::runtime_error("server is stopped");
+        e8qc_server_stats st{};
+        check(e8qc_server_get_stats(srv_, reset ? 1 : 0, &st));
+        py::dict d;
+        d["submitted"] = st.submitted;
+        d["rejected"] = st.rejected;
+        d["completed"] = st.completed;
+        d["failed"] = st.failed;
+        d["queries_completed"] = st.queries_completed;
+        d["batches"] = st.batches;
+        d["p50_ms"] = st.p50_ms;
+        d["p99_ms"] = st.p99_ms;
+        d["mean_ms"] = st.mean_ms;
+        d["max_ms"] = st.max_ms;
+        d["qps"] = st.qps;
+        d["mean_batch_queries"] = st.mean_batch_queries;
+        d["peak_batch_bytes"] = st.peak_batch_bytes;
+        return d;
+    }
+    void stop() {
+        if (!srv_) return;
+        e8qc_server* s = srv_;
+        srv_ = nullptr;
+        int rc = 0;
+        {
+            py::gil_scoped_release nogil;
+            rc = e8qc_server_stop(s);
+        }
+        check(rc);
+    }
+
+   private:
+    py::object index_;
+    size_t dim_ = 0;
+    e8qc_server* srv_ = nullptr;
+    std::unordered_map<uint64_t, std::pair<size_t, size_t>> shapes_;
 };
 
 }  // namespace e8qb200
@@ -308,6 +413,17 @@ PYBIND11_MODULE(_e8qlib, m) {
         }
         return py::make_tuple(C, ms);
     }, py::arg("A"), py::arg("B"), py::arg("reps") = 1, py::arg("grid") = 1, py::arg("device") = 0);
+
+    py::class_<e8qb200::Server>(m, "Server")
+        .def(py::init<py::object, const std::string&, size_t, size_t, size_t, size_t, int>(), py::arg("index"),
+             py::arg("mode") = "precision", py::arg("max_batch") = 4096, py::arg("max_k") = 128,
+             py::arg("max_nprobe") = 0, py::arg("memory_budget") = 0, py::arg("slots") = 2)
+        .def("submit", &e8qb200::Server::submit, py::arg("queries"), py::arg("k"), py::arg("nprobe"))
+        .def("result", &e8qb200::Server::result, py::arg("request_id"), py::arg("timeout_ms") = -1)
+        .def("stats", &e8qb200::Server::stats, py::arg("reset") = false)
+        .def("stop", &e8qb200::Server::stop)
+        .def("__enter__", [](py::object self) { return self; })
+        .def("__exit__", [](e8qb200::Server& s, py::args) { s.stop(); });
 
     py::class_<E8qIndex>(m, "E8qIndex")
         .def(py::init<size_t, size_t, uint64_t, int>(), py::arg("dim"), py::arg("nbits"),

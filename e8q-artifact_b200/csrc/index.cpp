@@ -96,6 +96,7 @@ struct e8qc_index {
 
     DevBuf signs, mean_rot, cen, cn2, tile_begin_d, list_len_d, codes, g1, h3, ids, tab,
         list_of_tile, list_begin_d, list_order;
+    DevBuf proxy;  // int8 proxy plane of the precision mode, built on its first search
     DevIndex view{};
     Workspace ws;
     bool profiling = false;
@@ -104,7 +105,7 @@ struct e8qc_index {
     size_t memory_bytes() const {
         return signs.bytes + mean_rot.bytes + cen.bytes + cn2.bytes + tile_begin_d.bytes +
                list_len_d.bytes + codes.bytes + g1.bytes + h3.bytes + ids.bytes + tab.bytes +
-               list_of_tile.bytes + list_begin_d.bytes + list_order.bytes;
+               list_of_tile.bytes + list_begin_d.bytes + list_order.bytes + proxy.bytes;
     }
 };
 
@@ -218,10 +219,16 @@ uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, con
         }
     } drop{ws};
     int launches = 0;
+    if (mode == E8QC_MODE_PRECISION && x->view.proxy == nullptr) {
+        x->proxy.alloc(proxy_plane_bytes(x->view, x->ntiles));
+        launches += launch_build_proxy(x->view, static_cast<int>(x->ntiles), x->proxy.as<uint4>(), s);
+        x->view.proxy = x->proxy.as<uint4>();
+    }
     if (mode == E8QC_MODE_PRECISION)
-        launches = precision_search(x->view, ws, rq, nq, k_arr, np_arr, k, np, k, ids_d, d_d, s);
+        launches += precision_search(x->view, ws, rq, nq, k_arr, np_arr, k, np, k, ids_d, d_d,
+                                     max_tiles_for(x, np) * 32, s);
     else
-        launches = batched_search(x->view, ws, rq, nq, k_arr, np_arr, k, np, k, ids_d, d_d, max_tiles_for(x, np), s);
+        launches += batched_search(x->view, ws, rq, nq, k_arr, np_arr, k, np, k, ids_d, d_d, max_tiles_for(x, np), s);
     if (x->profiling) {
         uint64_t cnt[2] = {0, 0};
         E8QC_CUDA(cudaMemcpyAsync(cnt, ws.b_nitems.as<uint32_t>() + 2, 16, cudaMemcpyDeviceToHost, s));
@@ -241,6 +248,74 @@ uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, con
 }  // namespace
 
 namespace e8qc {
+// ---- serving-loop support (server.cpp) ----
+
+// Index facts the server needs; throws when the index is not built.
+void server_index_info(e8qc_index* x, size_t* dim, size_t* nlist, int* device) {
+    require_built(x, "serve");
+    *dim = x->dim;
+    *nlist = x->nlist;
+    *device = x->device;
+}
+
+// One-time preparation for a mode (the precision proxy plane), under the
+// index lock, synchronised.
+void server_prepare(e8qc_index* x, int mode) {
+    require_built(x, "serve");
+    std::lock_guard<std::mutex> lock(x->mu);
+    DeviceGuard g(x->device);
+    if (mode == E8QC_MODE_PRECISION && x->view.proxy == nullptr) {
+        x->proxy.alloc(proxy_plane_bytes(x->view, x->ntiles));
+        launch_build_proxy(x->view, static_cast<int>(x->ntiles), x->proxy.as<uint4>(), nullptr);
+        E8QC_CUDA(cudaStreamSynchronize(nullptr));
+        x->view.proxy = x->proxy.as<uint4>();
+    }
+}
+
+// Upper bound of the device scratch one ragged call of nq queries needs
+// (workspace buffers plus the caller's query / k / nprobe / result buffers).
+size_t search_bytes(const e8qc_index* x, int mode, size_t nq, size_t k_max, size_t np_max) {
+    const size_t np = std::min(np_max, x->nlist), nlist = x->nlist, pd = x->pd;
+    const size_t npairs = nq * np;
+    const size_t align = mode == E8QC_MODE_PRECISION ? 8 : 1;
+    const size_t pslots = npairs + (align - 1) * nlist;
+    size_t b = nq * (x->dim * 4 + pd * 4 + k_max * 8 + 8);  // queries, rotated queries, results, k/nprobe
+    b += nq * nlist * 8 + nq * 4;                             // route keys, norms
+    b += npairs * 12 + pslots * 8 + nlist * 12;               // probes, d2, positions; pair rows; list counters
+    b += (npairs / 64 + nlist + 1) * 16 + 32;                 // work items
+    if (mode == E8QC_MODE_PRECISION) {
+        const size_t rows_q = max_tiles_for(x, np) * 32;  // proxy rows one query can need
+        const size_t chunk = std::max<size_t>(1, std::min<size_t>(nq, (size_t(2) << 30) / std::max<size_t>(1, rows_q * 4)));
+        b += nq * (pd + 8) + nlist * 8;                       // int8 queries, scales, row bases
+        b += chunk * rows_q * 4;                              // proxy rows of one chunk
+        b += ((pslots + 7) / 8 * 8 + 128) * pd;               // gathered int8 query rows
+    } else {
+        b += npairs * k_max * 8;                              // per-pair partial top-k
+    }
+    return b;
+}
+
+// Enqueue a ragged batched / precision search of nq device-resident queries
+// (not rotated) on stream s with its own workspace: no host synchronisation,
+// no index lock (the index is read-only while serving). Kernel wait timeouts
+// land in ws's error word.
+uint64_t server_enqueue(e8qc_index* x, Workspace& ws, int mode, const float* q_dev, size_t nq,
+                        const uint32_t* k_dev, const uint32_t* np_dev, size_t k_max, size_t np_max,
+                        uint32_t* ids_dev, float* d_dev, cudaStream_t s) {
+    const size_t np = std::min(np_max, x->nlist);
+    ws.ensure_queries(nq, x->pd);
+    ws.ensure_err();
+    float* rq = ws.rq.as<float>();
+    uint64_t launches = launch_rotate(x->view, q_dev, static_cast<int>(nq), rq, s);
+    if (mode == E8QC_MODE_PRECISION)
+        launches += precision_search(x->view, ws, rq, nq, k_dev, np_dev, k_max, np, k_max, ids_dev, d_dev,
+                                     max_tiles_for(x, np) * 32, s);
+    else
+        launches += batched_search(x->view, ws, rq, nq, k_dev, np_dev, k_max, np, k_max, ids_dev, d_dev,
+                                   max_tiles_for(x, np), s);
+    return launches;
+}
+
 // Read-only view of a built index for the no-allocation plain search
 // (noalloc.cu). Throws like every entry point when the index is not built.
 void plain_context(e8qc_index* x, size_t nprobe, DevIndex* view, int* device, size_t* nlist, size_t* dim,
@@ -471,6 +546,7 @@ int e8qc_e8q_build(e8qc_index* x, const float* data, size_t n, const float* cent
         v.bits = x->bits;
         v.nlist = static_cast<int>(nlist);
         v.nch = x->nch;
+        v.ntiles = static_cast<int>(x->ntiles);
         v.signs = x->signs.as<uint8_t>();
         v.mean_rot = x->mean_rot.as<float>();
         v.cen = x->cen.as<float>();
@@ -484,6 +560,8 @@ int e8qc_e8q_build(e8qc_index* x, const float* data, size_t n, const float* cent
         v.tab = x->tab.as<float>();
         v.list_order = x->list_order.as<uint32_t>();
         v.list_of_tile = x->list_of_tile.as<uint32_t>();
+        x->proxy.release();  // a rebuild invalidates the precision plane
+        v.proxy = nullptr;
         const DevEncTables& et = enc_tables_device(x->device, x->bits);
         BuildEncodeArgs a{};
         a.base = data_d;

@@ -87,6 +87,7 @@ const DevEncTables& enc_tables_device(int device, int bits);
 // [tile][c][l] so a warp reading chunk c touches 512 contiguous bytes.
 struct DevIndex {
     int dim, pd, B, bits, nlist, nch;
+    int ntiles;                  // 32-slot tiles over all lists
     const uint8_t* signs;        // 4*pd/8 rotation sign bits
     const float* mean_rot;       // pd
     const float* cen;            // nlist*pd rotated, centred centroids
@@ -100,6 +101,7 @@ struct DevIndex {
     const float* tab;            // [2][2^bits] level/sqrt(pd) refine tables
     const uint32_t* list_order;  // nlist list ids, longest list first
     const uint32_t* list_of_tile;  // ntiles: the list each tile belongs to
+    const uint4* proxy;            // precision mode's int8 proxy plane, or NULL until built
 };
 
 inline int code_chunks(int pd, int bits) { return (pd / 8 * 8 * bits + 127) / 128; }

@@ -10,13 +10,23 @@
 // close to linear in t + eta near the centre,
 //   S ~ S' = alpha * shift / (4 qs) * (2 S8 + sum(q8)),   shift = 2^max(0, bits-7)
 // (alpha: a weighted least-squares fit of table against t + eta). The proxy
-// distance D' = (d2 + h3) - 2*g1*S' ranks candidates: each query keeps its
-// top-C by D' per probed list, and a final kernel merges them per query,
-// rescores the C candidates with the exact estimator of the plain scan
-// (src/simd/e8q_search_generic.cpp:58-66; same table and per-block FMA chain,
-// blocks summed in order into two alternating accumulators) and keeps the
-// top-k. A rescored distance depends only on (query, vector), so results do
-// not depend on what else is in the batch.
+// distance D' = (d2 + h3) - 2*g1*S' of every (query, vector) pair is written
+// to a scratch row per (query, list) pair in HBM (4 bytes per pair: far less
+// than the codes the pair stands for); a per-query kernel then selects the
+// query's best C proxies over all its rows, rescores those C candidates with
+// the exact estimator of the plain scan (src/simd/e8q_search_generic.cpp:58-66;
+// same table and per-block FMA chain, blocks summed in order into two
+// alternating accumulators) and keeps the top-k. A rescored distance depends
+// only on (query, vector), so results do not depend on what else is in the
+// batch.
+//
+// The proxies of every vector are decoded once into an int8 "proxy plane"
+// stored in the MMA operand layout (built on the first precision search), and
+// the int8 query rows of a batch are gathered per (query, list) pair into the
+// same layout, so the scan kernel moves both operands with 2D tensor-map (TMA)
+// loads and does no decoding.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -39,11 +49,10 @@ namespace {
 
 __device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
 
-constexpr int kPT = 128;  // threads (one warpgroup: 4 warps x 32 TMEM lanes)
-constexpr int kPM = 128;  // queries per MMA tile (M)
+constexpr int kPM = 128;  // pair rows per MMA tile (M = TMEM lanes)
 constexpr int kPN = 256;  // vectors per MMA tile (N)
 constexpr int kPK = 64;   // dimensions per staged K-chunk (2 MMAs of K = 32)
-constexpr uint32_t kCols = 256;  // TMEM columns: one int32 accumulator per vector
+constexpr size_t kScratchBudget = size_t(2) << 30;  // proxy rows per call chunk (bytes)
 
 // Per-query int8 quantisation: q8 = rint(q * 127 / max|q|); per-query factor
 // coef / qs and sum(q8).
@@ -81,11 +90,45 @@ __global__ void quantize_kernel(const float* __restrict__ rq, int pd, float coef
     }
 }
 
-// 32-bit word `w` of the code stream of the vector in lane `lane` of tile gt.
-__device__ __forceinline__ uint32_t code_word(const DevIndex& ix, uint32_t gt, int lane, int w) {
-    const uint32_t* base =
-        reinterpret_cast<const uint32_t*>(ix.codes + (static_cast<size_t>(gt) * ix.nch + (w >> 2)) * 32 + lane);
-    return __ldg(base + (w & 3));
+// Start of each list's proxy rows: rowbase[L] = sum over lists L' < L of
+// (pairs probing L') * stride(L'), stride = the list's padded slots (whole
+// 32-vector tiles, so every row starts 128-byte aligned). One CTA of 1024
+// threads.
+__global__ void rowbase_kernel(const uint32_t* __restrict__ list_cnt, const uint32_t* __restrict__ tile_begin,
+                               int nlist, unsigned long long* __restrict__ rowbase) {
+    __shared__ unsigned long long wsum[32];
+    __shared__ unsigned long long carry;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    if (tid == 0) carry = 0;
+    __syncthreads();
+    for (int i0 = 0; i0 < nlist; i0 += blockDim.x) {
+        const int i = i0 + tid;
+        const unsigned long long v =
+            i < nlist ? static_cast<unsigned long long>(list_cnt[i]) * ((tile_begin[i + 1] - tile_begin[i]) * 32ull)
+                      : 0ull;
+        unsigned long long x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            unsigned long long s = lane < nw ? wsum[lane] : 0ull;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long y = __shfl_up_sync(kFull, s, o);
+                if (lane >= o) s += y;
+            }
+            wsum[lane] = s;
+        }
+        __syncthreads();
+        if (i < nlist) rowbase[i] = carry + (warp > 0 ? wsum[warp - 1] : 0ull) + x - v;
+        __syncthreads();
+        if (tid == 0) carry += wsum[nw - 1];
+        __syncthreads();
+    }
 }
 
 // Proxy integers of one block (8 dims) as 8 packed int8.
@@ -105,197 +148,318 @@ __device__ __forceinline__ uint2 block_proxy(const uint32_t* w, int base) {
     return make_uint2(lo, hi);
 }
 
-// Persistent proxy scan over work items (one list, up to 128 queries): for
-// each 256-vector tile of the list, K-chunks of 64 dimensions are staged in
-// shared memory (queries: int8 copies; vectors: decoded proxy integers) in the
-// K-major no-swizzle layout, double-buffered, and one thread issues the two
-// kind::i8 MMAs of a chunk into the 128 x 256 int32 accumulator in TMEM. The
-// epilogue reads the accumulator row of its query (thread r = TMEM lane r)
-// and keeps the query's top-C proxy distances in shared memory.
+// Proxy plane: slot s, dimension i at byte (s/8)*8*pd + (i/16)*128 + (s%8)*16
+// + i%16 -- 8-slot row groups of 16-byte core-matrix rows, the K-major
+// no-swizzle operand layout of tcgen05, so the 64-dimension K-chunk kc of a
+// row group is the 512 contiguous bytes at (s/8)*8*pd + kc*512. One thread per
+// (slot, K-chunk): the slot's 2*BITS code words for those 64 dimensions,
+// decoded into 64 proxies (four 16-byte stores; 8 consecutive slots fill 128
+// contiguous bytes).
 template <int BITS>
-__global__ void __launch_bounds__(kPT, 1) precision_scan_kernel(
-    DevIndex ix, const int8_t* __restrict__ q8, const float* __restrict__ qscale, const float* __restrict__ qsum,
+__global__ void __launch_bounds__(256) build_proxy_kernel(DevIndex ix, int nslots, unsigned char* __restrict__ plane) {
+    constexpr int NW = 2 * BITS;
+    const int slot = blockIdx.x * 256 + threadIdx.x;
+    const int kc = blockIdx.y;
+    if (slot >= nslots) return;
+    const uint32_t* base =
+        reinterpret_cast<const uint32_t*>(ix.codes + static_cast<size_t>(slot >> 5) * ix.nch * 32) + (slot & 31) * 4;
+    uint32_t w[NW + 1];
+#pragma unroll
+    for (int j = 0; j < NW; j += 2) {
+        const int wi = kc * NW + j;  // even: 8-byte aligned inside the lane's 16-byte entry
+        const uint2 v = __ldg(reinterpret_cast<const uint2*>(base + (wi >> 2) * 128 + (wi & 3)));
+        w[j] = v.x;
+        w[j + 1] = v.y;
+    }
+    w[NW] = 0u;
+    uint32_t o[16];
+#pragma unroll
+    for (int blk = 0; blk < 8; ++blk) {
+        const uint2 pr = block_proxy<BITS>(w, blk * 8 * BITS);
+        o[2 * blk] = pr.x;
+        o[2 * blk + 1] = pr.y;
+    }
+    unsigned char* dst = plane + static_cast<size_t>(slot >> 3) * 8 * ix.pd + kc * 512 + (slot & 7) * 16;
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+        *reinterpret_cast<uint4*>(dst + c * 128) = make_uint4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
+}
+
+// Query side of the MMA: the int8 query of every pair slot in the same row-
+// group layout as the proxy plane (a list's pairs start at a multiple of 8, so
+// a 128-pair work item is 16 whole row groups). Slots holding no pair, and the
+// 128 rows past the end, are zero. Thread order: row within group fastest.
+__global__ void gather_a8_kernel(const int8_t* __restrict__ q8, const uint32_t* __restrict__ pair_q, size_t pslots,
+                                 size_t rows, int pd, unsigned char* __restrict__ a8) {
+    const size_t e = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int nc = pd / 16;
+    const size_t r8 = e & 7, rest = e >> 3;
+    const size_t c = rest % nc, g = rest / nc;
+    const size_t row = g * 8 + r8;
+    if (row >= rows) return;
+    const uint32_t qq = row < pslots ? pair_q[row] : 0xFFFFFFFFu;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (qq != 0xFFFFFFFFu) v = *reinterpret_cast<const uint4*>(q8 + static_cast<size_t>(qq) * pd + c * 16);
+    *reinterpret_cast<uint4*>(a8 + g * 8 * pd + c * 128 + r8 * 16) = v;
+}
+
+// Persistent, warp-specialised proxy scan. Work items (one list, up to 128
+// pair rows) come from a device queue; the producer takes them and publishes
+// each through a 4-slot ring in shared memory (ifull / iempty mbarriers), so
+// every role walks the same item -> 256-vector tile -> 64-dimension K-chunk
+// sequence:
+//   warp 0 (producer): per chunk, two 2D tensor-map (TMA) loads -- 16 query
+//     row groups and 32 proxy row groups of 512 B (the chunk's 64 dimensions)
+//     -- into a kStages ring, completing on full[s] (expect-tx);
+//   warp 1 (one thread): waits full[s], issues the chunk's two kind::i8 MMAs
+//     (M = 128 rows, N = 256 vectors, K = 32 each) into accumulator t % 2 of
+//     two 256-column TMEM buffers, commits to empty[s]; after a tile's last
+//     chunk commits to tfull[b];
+//   warps 2..5 (epilogue): thread r of warp w owns pair row 32*(w%4) + lane
+//     (the TMEM lane quarter the warp may read). Per tile the warp stages the
+//     tile's (-2*g1, h3) in its own shared table (prefetched one tile ahead
+//     within an item), reads its row of the accumulator 32 columns at a time,
+//     writes its row's 32 proxy distances as eight 16-byte stores, then
+//     arrives on tempty[b].
+// Every wait is bounded; a timeout sets a CTA-wide abort flag that ends all
+// roles' loops, is reported through the error word, and the CTA frees its TMEM
+// after its outstanding copies and MMAs have completed (or a last bounded wait
+// for them ran out). No role waits on a barrier that another role can skip.
+constexpr int kStages = 6;
+constexpr int kScanThreads = 192;
+constexpr uint32_t kScanCols = 512;
+constexpr int kStageBytes = kPM * kPK + kPN * kPK;  // 8 KB queries + 16 KB proxies
+constexpr int kRing = 4;                            // items in flight between roles
+
+__global__ void __launch_bounds__(kScanThreads, 1) precision_scan_kernel(
+    DevIndex ix, const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+    const uint32_t* __restrict__ pair_q,
+    const float* __restrict__ pair_d2, const float* __restrict__ qscale, const float* __restrict__ qsum,
     const uint4* __restrict__ items, const uint32_t* __restrict__ n_items, uint32_t* __restrict__ head,
-    const uint32_t* __restrict__ pair_q, const float* __restrict__ pair_d2, int C, float* __restrict__ part_d,
-    uint32_t* __restrict__ part_slot, unsigned long long* __restrict__ cand_count, uint32_t* __restrict__ err) {
+    const uint32_t* __restrict__ pair_off, const unsigned long long* __restrict__ rowbase, float* __restrict__ prox,
+    unsigned long long* __restrict__ counts, uint32_t* __restrict__ err) {
     extern __shared__ __align__(1024) unsigned char psm[];
-    unsigned char* sA = psm;                                      // 2 x kPM x kPK
-    unsigned char* sB = psm + 2 * kPM * kPK;                      // 2 x kPN x kPK
-    float* tc_d = reinterpret_cast<float*>(sB + 2 * kPN * kPK);  // kPM x C
-    uint32_t* tc_i = reinterpret_cast<uint32_t*>(tc_d + kPM * C);
+    float2* ghtab = reinterpret_cast<float2*>(psm + kStages * kStageBytes);  // 4 warps x kPN
+    __shared__ __align__(8) uint64_t full[kStages], empty[kStages], tfull[2], tempty[2], ifull[kRing],
+        iempty[kRing], fin;
+    __shared__ uint4 s_items[kRing];
     __shared__ uint32_t s_tmem;
-    __shared__ __align__(8) uint64_t s_bar[2];
-    __shared__ uint4 s_item;
-    __shared__ uint32_t s_q[kPM];
-    __shared__ float s_d2[kPM], s_sc[kPM], s_sum[kPM];
-    const int tid = threadIdx.x, warp = tid >> 5;
+    __shared__ volatile int s_abort;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int pd = ix.pd, nK = pd / kPK;
     if (warp == 0) {
-        tc::tmem_alloc(&s_tmem, kCols);
+        tc::tmem_alloc(&s_tmem, kScanCols);
         tc::tmem_relinquish();
     }
     if (tid == 0) {
-        mbar_init(&s_bar[0], 1);
-        mbar_init(&s_bar[1], 1);
+        for (int i = 0; i < kStages; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < kRing; ++i) {
+            mbar_init(&ifull[i], 1);
+            mbar_init(&iempty[i], 5);  // the MMA thread + one lane per epilogue warp
+        }
+        mbar_init(&tfull[0], 1);
+        mbar_init(&tfull[1], 1);
+        mbar_init(&tempty[0], 4);
+        mbar_init(&tempty[1], 4);
+        mbar_init(&fin, 1);
+        s_abort = 0;
         fence_barrier_init();
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = s_tmem;
-    const uint32_t idesc = tc::idesc_i8(kPM, kPN);
-    const uint32_t sbo = (kPK / 16) * 128u;
     const uint32_t NI = *n_items;
-    uint32_t ck = 0;  // K-chunks committed so far: buffer ck & 1, phase (ck >> 1) & 1
-    bool ok = true;   // uniform across the CTA (every decision goes through a barrier)
-    for (;;) {
-        __syncthreads();
-        if (tid == 0) {
-            const uint32_t it = atomicAdd(head, 1u);
-            s_item = it < NI ? items[it] : make_uint4(0xFFFFFFFFu, 0, 0, 0);
-        }
-        __syncthreads();
-        const uint4 item = s_item;
-        if (item.x == 0xFFFFFFFFu) break;
-        const uint32_t L = item.x, pbase = item.y;
-        const int m = static_cast<int>(item.z);
-        {
-            const bool in = tid < m;
-            const uint32_t qq = in ? pair_q[pbase + tid] : 0u;
-            s_q[tid] = qq;
-            s_d2[tid] = in ? pair_d2[pbase + tid] : 0.0f;
-            s_sc[tid] = in ? qscale[qq] : 0.0f;
-            s_sum[tid] = in ? qsum[qq] : 0.0f;
-        }
-        for (int e = tid; e < kPM * C; e += kPT) {
-            tc_d[e] = inf_f();
-            tc_i[e] = 0xFFFFFFFFu;
-        }
-        const uint32_t len = ix.list_len[L];
-        const uint32_t tile0 = ix.tile_begin[L];
-        if (tid == 0) {
-            atomicAdd(cand_count, static_cast<unsigned long long>(len) * m);  // (query, vector) pairs
-            atomicAdd(cand_count + 1, static_cast<unsigned long long>(len));  // vectors read
-        }
-        __syncthreads();
-        float thr = inf_f();  // this thread's query: C-th best proxy distance so far
-        const int r = tid;    // query row == TMEM lane
-        for (uint32_t v0 = 0; v0 < len && ok; v0 += kPN) {
-            for (int kc = 0; kc < nK; ++kc, ++ck) {
-                const int b = static_cast<int>(ck & 1u);
-                bool mine = true;
-                if (ck >= 2) mine = mbar_wait_bounded(&s_bar[b], ((ck - 2) >> 1) & 1u);  // buffer b free
-                unsigned char* A = sA + b * kPM * kPK;
-                unsigned char* Bm = sB + b * kPN * kPK;
-                // A: 128 query rows x 64 int8
-                for (int e = tid; e < kPM * 4; e += kPT) {
-                    const int row = e >> 2, c16 = e & 3;
-                    uint4 v = make_uint4(0, 0, 0, 0);
-                    if (row < m)
-                        v = *reinterpret_cast<const uint4*>(q8 + static_cast<size_t>(s_q[row]) * pd + kc * kPK +
-                                                            c16 * 16);
-                    *reinterpret_cast<uint4*>(A + tc::il_offset(row, c16 * 16, kPK)) = v;
-                }
-                // B: 256 vectors x 8 blocks of proxy integers
-                for (int e = tid; e < kPN * 8; e += kPT) {
-                    const int vv = e >> 3, blk = e & 7;
-                    const uint32_t vi = v0 + vv;
-                    uint2 pv = make_uint2(0, 0);
-                    if (vi < len) {
-                        const uint32_t gt = tile0 + (vi >> 5);
-                        const int vl = static_cast<int>(vi & 31u);
-                        const int bit0 = (kc * 8 + blk) * 8 * BITS;
-                        uint32_t w[6];
-#pragma unroll
-                        for (int j = 0; j < 5; ++j)
-                            w[j] = (j * 32 < (bit0 & 31) + 8 * BITS) ? code_word(ix, gt, vl, (bit0 >> 5) + j) : 0u;
-                        w[5] = 0u;
-                        pv = block_proxy<BITS>(w, bit0 & 31);
+
+    if (warp == 0) {
+        // ---- producer ----
+        uint32_t f = 0;  // chunk fills issued
+        for (uint32_t n = 0; !s_abort; ++n) {
+            const uint32_t j = n % kRing;
+            if (n >= kRing && !mbar_wait_or_abort(&iempty[j], ((n / kRing) - 1) & 1u, &s_abort)) break;
+            if (lane == 0) {
+                const uint32_t it = atomicAdd(head, 1u);
+                s_items[j] = it < NI ? items[it] : make_uint4(0xFFFFFFFFu, 0, 0, 0);
+                mbar_arrive(&ifull[j]);
+            }
+            __syncwarp();
+            const uint4 item = s_items[j];
+            if (item.x == 0xFFFFFFFFu) break;
+            const uint32_t L = item.x, pbase = item.y;
+            const uint32_t len = ix.list_len[L], tile0 = ix.tile_begin[L];
+            const int arow = static_cast<int>(pbase >> 3);  // the item's first query row group
+            for (uint32_t v0 = 0; v0 < len && !s_abort; v0 += kPN) {
+                const int brow = static_cast<int>((tile0 * 32u + v0) >> 3);  // the tile's first proxy row group
+                for (int kc = 0; kc < nK; ++kc, ++f) {
+                    const int st = static_cast<int>(f % kStages);
+                    if (f >= static_cast<uint32_t>(kStages) &&
+                        !mbar_wait_or_abort(&empty[st], ((f / kStages) - 1) & 1u, &s_abort))
+                        break;
+                    if (lane == 0) {
+                        unsigned char* sA = psm + st * kStageBytes;
+                        unsigned char* sB = sA + kPM * kPK;
+                        mbar_arrive_expect_tx(&full[st], kStageBytes);
+                        // boxes of 32 (B) and 16 (A) row groups x 512 bytes (128 u32 at x = kc * 128)
+                        tma_load_2d(sB, &map_b, kc * 128, brow, &full[st]);
+                        tma_load_2d(sA, &map_a, kc * 128, arow, &full[st]);
                     }
-                    *reinterpret_cast<uint2*>(Bm + tc::il_offset(vv, blk * 8, kPK)) = pv;
-                }
-                tc::fence_smem_to_async();
-                tc::fence_before_sync();
-                ok = __syncthreads_and(mine ? 1 : 0) != 0;
-                tc::fence_after_sync();
-                if (!ok) break;
-                if (tid == 0) {
-                    const uint32_t a0 = tc::saddr(A), b0 = tc::saddr(Bm);
-#pragma unroll
-                    for (int s = 0; s < kPK / 32; ++s)
-                        tc::mma_i8(tmem, tc::smem_desc(a0 + 256u * s, 128u, sbo),
-                                   tc::smem_desc(b0 + 256u * s, 128u, sbo), idesc, (kc > 0 || s > 0) ? 1u : 0u);
-                    tc::mma_commit(&s_bar[b]);
+                    __syncwarp();
                 }
             }
-            if (!ok) break;
-            // the tile's last commit covers all its MMAs
-            const uint32_t last = ck - 1;
-            const bool done = mbar_wait_bounded(&s_bar[last & 1u], (last >> 1) & 1u);
-            ok = __syncthreads_and(done ? 1 : 0) != 0;
-            if (!ok) break;
-            tc::fence_after_sync();
-            const float sc = s_sc[r], sum = s_sum[r], d2 = s_d2[r];
-            float* ld = tc_d + r * C;
-            uint32_t* li = tc_i + r * C;
-            for (int c0 = 0; c0 < kPN; c0 += 8) {
-                uint32_t acc[8];
-                tc::tmem_ld8(tmem + ((static_cast<uint32_t>(warp) * 32u) << 16) + static_cast<uint32_t>(c0), acc);
-                tc::tmem_ld_wait();
-                if (r < m) {
+        }
+        // copies still in flight land before the CTA can exit
+        if (s_abort && lane == 0)
+            for (uint32_t g = f > kStages ? f - kStages : 0; g < f; ++g)
+                (void)mbar_wait_bounded(&full[g % kStages], (g / kStages) & 1u, 100u);
+    } else if (warp == 1) {
+        // ---- MMA issuer ----
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_i8(kPM, kPN);
+            const uint32_t sbo = (kPK / 16) * 128u;
+            uint32_t c = 0, t = 0;
+            bool issued = false;
+            for (uint32_t n = 0; !s_abort; ++n) {
+                const uint32_t j = n % kRing;
+                if (!mbar_wait_or_abort(&ifull[j], (n / kRing) & 1u, &s_abort)) break;
+                const uint4 item = s_items[j];
+                if (item.x == 0xFFFFFFFFu) break;
+                const uint32_t len = ix.list_len[item.x];
+                for (uint32_t v0 = 0; v0 < len && !s_abort; v0 += kPN, ++t) {
+                    const uint32_t b = t & 1u;
+                    if (t >= 2 && !mbar_wait_or_abort(&tempty[b], ((t >> 1) - 1) & 1u, &s_abort)) break;
+                    tc::fence_after_sync();
+                    const uint32_t d_tmem = tmem + b * 256u;
+                    for (int kc = 0; kc < nK; ++kc, ++c) {
+                        const int st = static_cast<int>(c % kStages);
+                        if (!mbar_wait_or_abort(&full[st], (c / kStages) & 1u, &s_abort)) break;
+                        tc::fence_after_sync();
+                        const uint32_t a0 = tc::saddr(psm + st * kStageBytes), b0 = a0 + kPM * kPK;
 #pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const uint32_t vi = v0 + c0 + j;
-                        if (vi >= len) break;
-                        const uint32_t slot = (tile0 + (vi >> 5)) * 32u + (vi & 31u);
-                        const float g1 = __ldg(ix.g1 + slot), h3 = __ldg(ix.h3 + slot);
-                        const float Sp = sc * __fmaf_rn(2.0f, static_cast<float>(static_cast<int>(acc[j])), sum);
-                        const float dp = __fmaf_rn(-__fmul_rn(2.0f, g1), Sp, __fadd_rn(d2, h3));
-                        if (dp < thr) {  // sorted insertion into this query's list
-                            int pos = C - 1;
-                            while (pos > 0 && ld[pos - 1] > dp) {
-                                ld[pos] = ld[pos - 1];
-                                li[pos] = li[pos - 1];
-                                --pos;
+                        for (int s2 = 0; s2 < kPK / 32; ++s2)
+                            tc::mma_i8(d_tmem, tc::smem_desc(a0 + 256u * s2, 128u, sbo),
+                                       tc::smem_desc(b0 + 256u * s2, 128u, sbo), idesc, (kc > 0 || s2 > 0) ? 1u : 0u);
+                        tc::mma_commit(&empty[st]);
+                        issued = true;
+                    }
+                    if (s_abort) break;
+                    tc::mma_commit(&tfull[b]);
+                }
+                mbar_arrive(&iempty[j]);
+            }
+            // every MMA issued has completed before TMEM is released
+            if (issued) {
+                tc::mma_commit(&fin);
+                (void)mbar_wait_bounded(&fin, 0u, 200u);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue ----
+        const int q4 = warp & 3;  // TMEM lane quarter this warp may read
+        const int r = q4 * 32 + lane;
+        float2* gh = ghtab + (warp - 2) * kPN;
+        uint32_t t = 0;
+        for (uint32_t n = 0; !s_abort; ++n) {
+            const uint32_t j = n % kRing;
+            if (!mbar_wait_or_abort(&ifull[j], (n / kRing) & 1u, &s_abort)) break;
+            const uint4 item = s_items[j];
+            if (item.x == 0xFFFFFFFFu) break;
+            const uint32_t L = item.x, pbase = item.y;
+            const int m = static_cast<int>(item.z);
+            const uint32_t len = ix.list_len[L], tile0 = ix.tile_begin[L];
+            const uint32_t stride = (ix.tile_begin[L + 1] - tile0) * 32u;
+            float sc = 0.0f, sum = 0.0f, d2 = 0.0f;
+            float* row = prox;
+            if (r < m) {
+                const uint32_t qq = pair_q[pbase + r];
+                sc = qscale[qq];
+                sum = qsum[qq];
+                d2 = pair_d2[pbase + r];
+                row = prox + rowbase[L] + static_cast<unsigned long long>(pbase + r - pair_off[L]) * stride;
+            }
+            if (warp == 2 && lane == 0) {
+                atomicAdd(counts, static_cast<unsigned long long>(len) * m);  // (query, vector) pairs
+                atomicAdd(counts + 1, static_cast<unsigned long long>(len));  // vectors read
+            }
+            // (g1, h3) of columns 4*lane.. and 128 + 4*lane.. of a tile (zero past the padded list)
+            const float4* g4 = reinterpret_cast<const float4*>(ix.g1 + tile0 * 32u);
+            const float4* h4 = reinterpret_cast<const float4*>(ix.h3 + tile0 * 32u);
+            float4 ga = make_float4(0.f, 0.f, 0.f, 0.f), gb = ga, ha = ga, hb = ga;
+            auto fetch = [&](uint32_t v0) {
+                const uint32_t ca = v0 + 4 * lane, cb = ca + 128;
+                ga = ca < stride ? __ldg(g4 + (ca >> 2)) : make_float4(0.f, 0.f, 0.f, 0.f);
+                ha = ca < stride ? __ldg(h4 + (ca >> 2)) : make_float4(0.f, 0.f, 0.f, 0.f);
+                gb = cb < stride ? __ldg(g4 + (cb >> 2)) : make_float4(0.f, 0.f, 0.f, 0.f);
+                hb = cb < stride ? __ldg(h4 + (cb >> 2)) : make_float4(0.f, 0.f, 0.f, 0.f);
+            };
+            fetch(0);
+            for (uint32_t v0 = 0; v0 < len; v0 += kPN, ++t) {
+                const uint32_t b = t & 1u;
+                __syncwarp();  // every lane is done reading the previous tile's table
+                gh[4 * lane + 0] = make_float2(-__fmul_rn(2.0f, ga.x), ha.x);
+                gh[4 * lane + 1] = make_float2(-__fmul_rn(2.0f, ga.y), ha.y);
+                gh[4 * lane + 2] = make_float2(-__fmul_rn(2.0f, ga.z), ha.z);
+                gh[4 * lane + 3] = make_float2(-__fmul_rn(2.0f, ga.w), ha.w);
+                gh[128 + 4 * lane + 0] = make_float2(-__fmul_rn(2.0f, gb.x), hb.x);
+                gh[128 + 4 * lane + 1] = make_float2(-__fmul_rn(2.0f, gb.y), hb.y);
+                gh[128 + 4 * lane + 2] = make_float2(-__fmul_rn(2.0f, gb.z), hb.z);
+                gh[128 + 4 * lane + 3] = make_float2(-__fmul_rn(2.0f, gb.w), hb.w);
+                __syncwarp();
+                if (v0 + kPN < len) fetch(v0 + kPN);  // next tile of this item, in flight meanwhile
+                if (!mbar_wait_or_abort(&tfull[b], (t >> 1) & 1u, &s_abort)) break;
+                tc::fence_after_sync();
+                for (uint32_t c0 = 0; c0 < static_cast<uint32_t>(kPN) && v0 + c0 < len; c0 += 32) {
+                    uint32_t acc[32];
+#pragma unroll
+                    for (int jj = 0; jj < 4; ++jj) {
+                        uint32_t(&part)[8] = *reinterpret_cast<uint32_t(*)[8]>(acc + 8 * jj);
+                        tc::tmem_ld8(tmem + ((static_cast<uint32_t>(q4) * 32u) << 16) + b * 256u + c0 + 8 * jj,
+                                     part);
+                    }
+                    tc::tmem_ld_wait();
+                    if (r < m) {
+                        // columns past len land in the row's tile padding (rows are whole tiles)
+                        float4* dst = reinterpret_cast<float4*>(row + v0 + c0);
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            float o[4];
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) {
+                                const float2 cg = gh[c0 + 4 * q + e];
+                                const float Sp =
+                                    sc * __fmaf_rn(2.0f, static_cast<float>(static_cast<int>(acc[4 * q + e])), sum);
+                                o[e] = __fmaf_rn(cg.x, Sp, __fadd_rn(d2, cg.y));
                             }
-                            ld[pos] = dp;
-                            li[pos] = slot;
-                            thr = ld[C - 1];
+                            dst[q] = make_float4(o[0], o[1], o[2], o[3]);
                         }
                     }
                 }
+                tc::fence_before_sync();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&tempty[b]);
             }
-            tc::fence_before_sync();
-            __syncthreads();  // TMEM reads done before the next tile's MMAs overwrite it
-        }
-        if (!ok) break;
-        // the item's per-pair candidate lists
-        for (int e = tid; e < m * C; e += kPT) {
-            const int q = e / C, j = e - q * C;
-            const size_t o = static_cast<size_t>(pbase + q) * C + j;
-            part_d[o] = tc_d[q * C + j];
-            part_slot[o] = tc_i[q * C + j];
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&iempty[j]);
         }
     }
-    if (!ok) {
-        // a wait gave up: report, give in-flight MMAs one more bounded wait
-        if (tid == 0) atomicOr(err, kErrWaitTimeout);
-        if (ck > 0) (void)mbar_wait_bounded(&s_bar[(ck - 1) & 1u], ((ck - 1) >> 1) & 1u, 256u);
-    }
-    tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, kCols);
+    if (s_abort && tid == 0) atomicOr(err, kErrWaitTimeout);
+    tc::fence_after_sync();
+    if (warp == 0) tc::tmem_dealloc(tmem, kScanCols);
 }
 
-// Per query (one warp): merge the query's per-list candidate lists into its
-// top-C by proxy distance, rescore those exactly, keep the top-k.
+// Per query (one warp): best C proxies over the query's rows, exact rescoring
+// of those candidates, top-k by exact distance.
 template <int BITS>
 __global__ void __launch_bounds__(128) precision_final_kernel(
-    DevIndex ix, const float* __restrict__ rq, const float* __restrict__ part_d,
-    const uint32_t* __restrict__ part_slot, int C, const uint32_t* __restrict__ pos_of,
-    const uint32_t* __restrict__ probes, const float* __restrict__ pd2, int nq, const uint32_t* __restrict__ np_arr,
-    int np_max, const uint32_t* __restrict__ k_arr, int k_uniform, int out_stride, uint32_t* __restrict__ out_ids,
-    float* __restrict__ out_d) {
+    DevIndex ix, const float* __restrict__ rq, const float* __restrict__ prox,
+    const unsigned long long* __restrict__ rowbase, const uint32_t* __restrict__ pair_off,
+    const uint32_t* __restrict__ pos_of, const uint32_t* __restrict__ probes, const float* __restrict__ pd2, int nq,
+    const uint32_t* __restrict__ np_arr, int np_max, const uint32_t* __restrict__ k_arr, int k_uniform, int C,
+    int out_stride, uint32_t* __restrict__ out_ids, float* __restrict__ out_d) {
     constexpr int Q = 1 << BITS;
     constexpr int REP = table_rep(BITS);
     constexpr int GBL = group_blocks(BITS), GCH = group_chunks(BITS);
@@ -314,17 +478,30 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
     if (q >= nq) return;
     const int np = np_arr ? static_cast<int>(np_arr[q]) : np_max;
     const int kq = k_arr ? static_cast<int>(k_arr[q]) : k_uniform;
-    // 1. top-C candidates of this query by proxy distance (slot as tie-break)
+    const uint32_t* pr = probes + static_cast<size_t>(q) * np_max;
+    // 1. best C proxies (slot as tie-break)
     WarpTopK cand;
     cand.init(C);
     for (int p = 0; p < np; ++p) {
-        const size_t base = static_cast<size_t>(pos_of[static_cast<size_t>(q) * np_max + p]) * C;
-        for (int j0 = 0; j0 < C; j0 += 32) {
-            const int j = j0 + lane;
-            const bool in = j < C;
-            const float dd = in ? part_d[base + j] : inf_f();
-            const uint32_t ss = in ? part_slot[base + j] : 0xFFFFFFFFu;
-            cand.offer_pair(dd, ss, in && ss != 0xFFFFFFFFu);
+        const uint32_t L = pr[p];
+        const uint32_t len = ix.list_len[L];
+        const uint32_t t0 = ix.tile_begin[L];
+        const uint32_t stride = (ix.tile_begin[L + 1] - t0) * 32u;
+        const uint32_t pos = pos_of[static_cast<size_t>(q) * np_max + p];
+        const float4* row = reinterpret_cast<const float4*>(
+            prox + rowbase[L] + static_cast<unsigned long long>(pos - pair_off[L]) * stride);
+        const uint32_t slot0 = t0 * 32u;
+        // 256 values per step: two independent 16-byte loads per lane in flight
+        for (uint32_t v0 = 0; v0 < len; v0 += 256) {
+            float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
+            const uint32_t va = v0 + lane * 4, vb = v0 + 128 + lane * 4;
+            if (va < len) a = __ldcs(row + (va >> 2));
+            if (vb < len) b = __ldcs(row + (vb >> 2));
+            const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) cand.offer_pair(av[j], slot0 + va + j, va + j < len);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) cand.offer_pair(bv[j], slot0 + vb + j, vb + j < len);
         }
     }
     // 2. exact rescoring of candidate (s, lane); 3. top-k by exact distance
@@ -332,7 +509,6 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
     top.init(kq);
     const uint32_t tb_addr = static_cast<uint32_t>(__cvta_generic_to_shared(tabrep)) + (lane % REP) * 4u;
     const float4* sq4 = reinterpret_cast<const float4*>(myq);
-    const uint32_t* pr = probes + static_cast<size_t>(q) * np_max;
     const int ng = (pd / 8) / GBL;
     const bool tail = ((pd / 8) % GBL) != 0;
 #pragma unroll
@@ -376,33 +552,68 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
     }
 }
 
-size_t scan_smem(int C) { return static_cast<size_t>(2) * kPM * kPK + 2 * kPN * kPK + static_cast<size_t>(kPM) * C * 8; }
+constexpr size_t kScanSmem = static_cast<size_t>(kStages) * kStageBytes + static_cast<size_t>(4) * kPN * 8;
 
-template <int BITS>
-int launch_precision(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* k_arr,
-                     const uint32_t* np_arr, int k_max, int np_max, int C, int out_stride, uint32_t* out_ids,
-                     float* out_d, cudaStream_t s) {
-    int dev = 0;
-    E8QC_CUDA(cudaGetDevice(&dev));
-    const size_t smem = scan_smem(C);
-    static size_t configured[64] = {};
-    if (configured[dev & 63] < smem) {
-        E8QC_CUDA(cudaFuncSetAttribute(precision_scan_kernel<BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem)));
-        configured[dev & 63] = smem;
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        E8QC_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p) fail(E8QC_ECUDA, "cuTensorMapEncodeTiled is unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
     }
-    int sms = 148, per_sm = 1;
+    return fn;
+}
+
+// A row-group plane (rows of 8 * pd bytes, seen as 2 * pd u32) as a 2D tensor
+// map whose box is box_rows row groups x 512 bytes (one K-chunk).
+CUtensorMap plane_map(const void* base, size_t row_groups, int pd, uint32_t box_rows) {
+    CUtensorMap m;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(2 * pd), static_cast<cuuint64_t>(row_groups)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(8) * pd};
+    const cuuint32_t box[2] = {128u, box_rows};
+    const cuuint32_t estr[2] = {1u, 1u};
+    const CUresult r = encode_tiled()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<void*>(base), dims, strides,
+                                      box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) fail(E8QC_ECUDA, "cuTensorMapEncodeTiled failed");
+    return m;
+}
+
+void launch_scan(const DevIndex& ix, Workspace& ws, size_t a_rows, size_t plane_slots, cudaStream_t s) {
+    int dev = 0, sms = 148;
+    E8QC_CUDA(cudaGetDevice(&dev));
+    static bool configured[64] = {};
+    if (!configured[dev & 63]) {
+        E8QC_CUDA(cudaFuncSetAttribute(precision_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(kScanSmem)));
+        configured[dev & 63] = true;
+    }
     E8QC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    E8QC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, precision_scan_kernel<BITS>, kPT, smem));
-    per_sm = std::max(1, std::min(per_sm, 2));  // 2 x 256 TMEM columns fill an SM
     uint32_t* nitems = ws.b_nitems.as<uint32_t>();
     ws.mark_scan(false, s);
-    precision_scan_kernel<BITS><<<sms * per_sm, kPT, smem, s>>>(
-        ix, ws.p_q8.as<int8_t>(), ws.p_scale.as<float>(), ws.p_sum.as<float>(), ws.b_items.as<uint4>(), nitems,
-        nitems + 1, ws.b_pair_q.as<uint32_t>(), ws.b_pair_d2.as<float>(), C, ws.b_part_d.as<float>(),
-        ws.b_part_id.as<uint32_t>(), reinterpret_cast<unsigned long long*>(nitems + 2), ws.err.as<uint32_t>());
+    // one CTA per SM: the two accumulators take all 512 TMEM columns
+    const CUtensorMap map_a = plane_map(ws.p_a8.p, a_rows / 8, ix.pd, 16);
+    const CUtensorMap map_b = plane_map(ix.proxy, plane_slots / 8, ix.pd, 32);
+    precision_scan_kernel<<<sms, kScanThreads, kScanSmem, s>>>(
+        ix, map_a, map_b, ws.b_pair_q.as<uint32_t>(), ws.b_pair_d2.as<float>(),
+        ws.p_scale.as<float>(), ws.p_sum.as<float>(), ws.b_items.as<uint4>(), nitems, nitems + 1,
+        ws.b_off.as<uint32_t>(), ws.p_rowbase.as<unsigned long long>(), ws.p_prox.as<float>(),
+        reinterpret_cast<unsigned long long*>(nitems + 2), ws.err.as<uint32_t>());
     E8QC_CUDA(cudaGetLastError());
     ws.mark_scan(true, s);
+}
+
+// Per-query selection + exact rescoring of one chunk of queries.
+template <int BITS>
+int launch_final(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* k_arr,
+                 const uint32_t* np_arr, int k_max, int np_max, int C, int out_stride, uint32_t* out_ids,
+                 float* out_d, cudaStream_t s) {
+    int dev = 0;
+    E8QC_CUDA(cudaGetDevice(&dev));
     constexpr int REP = table_rep(BITS);
     const size_t fsmem = (static_cast<size_t>(2) * (1 << BITS) * REP + 4 * static_cast<size_t>(ix.pd)) * 4;
     static size_t fconfigured[64] = {};
@@ -412,11 +623,20 @@ int launch_precision(const DevIndex& ix, Workspace& ws, const float* rq, size_t 
         fconfigured[dev & 63] = fsmem;
     }
     precision_final_kernel<BITS><<<static_cast<unsigned>((nq + 3) / 4), 128, fsmem, s>>>(
-        ix, rq, ws.b_part_d.as<float>(), ws.b_part_id.as<uint32_t>(), C, ws.b_pos.as<uint32_t>(),
-        ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(), static_cast<int>(nq), np_arr, np_max, k_arr, k_max,
-        out_stride, out_ids, out_d);
+        ix, rq, ws.p_prox.as<float>(), ws.p_rowbase.as<unsigned long long>(), ws.b_off.as<uint32_t>(),
+        ws.b_pos.as<uint32_t>(), ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(), static_cast<int>(nq), np_arr,
+        np_max, k_arr, k_max, C, out_stride, out_ids, out_d);
     E8QC_CUDA(cudaGetLastError());
-    return 2;
+    return 1;
+}
+
+template <int BITS>
+int launch_build_proxy_bits(const DevIndex& ix, int ntiles, uint4* plane, cudaStream_t s) {
+    const int nslots = ntiles * 32;
+    dim3 g(static_cast<unsigned>((nslots + 255) / 256), static_cast<unsigned>(ix.pd / kPK));
+    build_proxy_kernel<BITS><<<g, 256, 0, s>>>(ix, nslots, reinterpret_cast<unsigned char*>(plane));
+    E8QC_CUDA(cudaGetLastError());
+    return 1;
 }
 
 }  // namespace
@@ -439,36 +659,79 @@ double precision_alpha(int bits, int pd) {
     return sxx > 0.0 ? sxy / sxx : 0.0;
 }
 
-int precision_candidates(int k) { return std::min(kMaxK, std::max(64, 4 * k)); }
+size_t proxy_plane_bytes(const DevIndex& ix, size_t ntiles) {
+    return (ntiles * 32 + kPN) * static_cast<size_t>(ix.pd);
+}
 
-int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* k_arr,
-                     const uint32_t* np_arr, size_t k, size_t nprobe, size_t out_stride, uint32_t* out_ids,
-                     float* out_d, cudaStream_t s) {
-    if (nq == 0) return 0;
+int launch_build_proxy(const DevIndex& ix, int ntiles, uint4* plane, cudaStream_t s) {
     if (ix.pd % kPK != 0) fail(E8QC_EINVAL, "precision search needs the padded dimension to be a multiple of 64");
-    const int C = precision_candidates(static_cast<int>(k));
-    int launches = batched_prepare(ix, ws, rq, nq, np_arr, nprobe, static_cast<size_t>(C), kPM, s);
-    ws.p_q8.ensure(nq * static_cast<size_t>(ix.pd));
-    ws.p_scale.ensure(nq * 4);
-    ws.p_sum.ensure(nq * 4);
-    ws.ensure_err();
-    const int shift = ix.bits > 7 ? (1 << (ix.bits - 7)) : 1;
-    const float coef = static_cast<float>(precision_alpha(ix.bits, ix.pd) * shift / 4.0);
-    quantize_kernel<<<static_cast<unsigned>(nq), 256, 0, s>>>(rq, ix.pd, coef, ws.p_q8.as<int8_t>(),
-                                                              ws.p_scale.as<float>(), ws.p_sum.as<float>());
-    E8QC_CUDA(cudaGetLastError());
-    ++launches;
+    // the slots past the last tile are read by the last MMA tile: zero them
+    E8QC_CUDA(cudaMemsetAsync(plane, 0, proxy_plane_bytes(ix, ntiles), s));
     switch (ix.bits) {
-#define E8QC_CASE(b)                                                                                                 \
-    case b:                                                                                                          \
-        launches += launch_precision<b>(ix, ws, rq, nq, k_arr, np_arr, static_cast<int>(k), static_cast<int>(nprobe), \
-                                        C, static_cast<int>(out_stride), out_ids, out_d, s);                         \
-        break;
+#define E8QC_CASE(b) \
+    case b: return 1 + launch_build_proxy_bits<b>(ix, ntiles, plane, s);
         E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
         E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
         E8QC_CASE(13)
 #undef E8QC_CASE
         default: fail(E8QC_EINVAL, "bits out of range");
+    }
+    return 0;
+}
+
+int precision_candidates(int k) { return std::min(kMaxK, std::max(64, 4 * k)); }
+
+int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* k_arr,
+                     const uint32_t* np_arr, size_t k, size_t nprobe, size_t out_stride, uint32_t* out_ids,
+                     float* out_d, size_t rows_per_query, cudaStream_t s) {
+    if (nq == 0) return 0;
+    if (ix.pd % kPK != 0) fail(E8QC_EINVAL, "precision search needs the padded dimension to be a multiple of 64");
+    if (ix.proxy == nullptr) fail(E8QC_ESTATE, "precision search needs the proxy plane (launch_build_proxy)");
+    const int C = precision_candidates(static_cast<int>(k));
+    const int shift = ix.bits > 7 ? (1 << (ix.bits - 7)) : 1;
+    const float coef = static_cast<float>(precision_alpha(ix.bits, ix.pd) * shift / 4.0);
+    // proxy rows of a chunk of queries stay within the scratch budget
+    const size_t per_q = std::max<size_t>(1, rows_per_query) * sizeof(float);
+    const size_t chunk = std::max<size_t>(1, std::min(nq, kScratchBudget / per_q));
+    ws.ensure_err();
+    int launches = 0;
+    for (size_t off = 0; off < nq; off += chunk) {
+        const size_t n = std::min(chunk, nq - off);
+        const float* rqc = rq + off * ix.pd;
+        const uint32_t* kc = k_arr ? k_arr + off : nullptr;
+        const uint32_t* npc = np_arr ? np_arr + off : nullptr;
+        launches += batched_prepare(ix, ws, rqc, n, npc, nprobe, 0, kPM, 8, s);
+        const size_t pslots = n * nprobe + static_cast<size_t>(7) * ix.nlist;
+        const size_t arows = (pslots + 7) / 8 * 8 + kPM;  // an item reads up to 128 rows from its start
+        ws.p_q8.ensure(n * static_cast<size_t>(ix.pd));
+        ws.p_scale.ensure(n * 4);
+        ws.p_sum.ensure(n * 4);
+        ws.p_rowbase.ensure(static_cast<size_t>(ix.nlist) * 8);
+        ws.p_prox.ensure(n * per_q);
+        ws.p_a8.ensure(arows * ix.pd);
+        rowbase_kernel<<<1, 1024, 0, s>>>(ws.b_cnt.as<uint32_t>(), ix.tile_begin, ix.nlist,
+                                          ws.p_rowbase.as<unsigned long long>());
+        quantize_kernel<<<static_cast<unsigned>(n), 256, 0, s>>>(rqc, ix.pd, coef, ws.p_q8.as<int8_t>(),
+                                                                 ws.p_scale.as<float>(), ws.p_sum.as<float>());
+        const size_t ga = arows * (ix.pd / 16);
+        gather_a8_kernel<<<static_cast<unsigned>((ga + 255) / 256), 256, 0, s>>>(
+            ws.p_q8.as<int8_t>(), ws.b_pair_q.as<uint32_t>(), pslots, arows, ix.pd, ws.p_a8.as<unsigned char>());
+        E8QC_CUDA(cudaGetLastError());
+        launch_scan(ix, ws, arows, static_cast<size_t>(ix.ntiles) * 32 + kPN, s);
+        launches += 4;
+        switch (ix.bits) {
+#define E8QC_CASE(b)                                                                                          \
+    case b:                                                                                                   \
+        launches += launch_final<b>(ix, ws, rqc, n, kc, npc, static_cast<int>(k), static_cast<int>(nprobe), C, \
+                                    static_cast<int>(out_stride), out_ids + off * out_stride,                 \
+                                    out_d + off * out_stride, s);                                             \
+        break;
+            E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
+            E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
+            E8QC_CASE(13)
+#undef E8QC_CASE
+            default: fail(E8QC_EINVAL, "bits out of range");
+        }
     }
     return launches;
 }

@@ -16,12 +16,22 @@ namespace e8qc {
 // rate's encoding scale).
 double precision_alpha(int bits, int pd);
 
+// Bytes of the int8 proxy plane: the padded slots (plus one MMA tile of 256
+// slots read past the last list) x pd.
+size_t proxy_plane_bytes(const DevIndex& ix, size_t ntiles);
+
+// Decode every slot's code into the proxy plane (layout in precision.cu).
+int launch_build_proxy(const DevIndex& ix, int ntiles, uint4* plane, cudaStream_t s);
+
 // Candidates kept per query for exact rescoring at a given k.
 int precision_candidates(int k);
 
 // Search nq rotated queries; same argument meaning as batched_search.
+// rows_per_query bounds the vectors one query's probes can reach (the padded
+// slots of the nprobe longest lists): the proxy scratch of a chunk of queries
+// is sized from it, and batches whose scratch would exceed 2 GiB run in chunks.
 int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* k_arr,
                      const uint32_t* np_arr, size_t k, size_t nprobe, size_t out_stride, uint32_t* out_ids,
-                     float* out_d, cudaStream_t s);
+                     float* out_d, size_t rows_per_query, cudaStream_t s);
 
 }  // namespace e8qc

@@ -1,8 +1,9 @@
 // Bulk-copy (TMA, cp.async.bulk) and mbarrier helpers for sm_100a, with
-// bounded waits: a wait that runs out of iterations reports failure instead
-// of spinning forever, and the caller records it in a device error word.
+// bounded waits: a wait that runs out of time reports failure instead of
+// spinning forever, and the caller records it in a device error word.
 #pragma once
 
+#include <cuda.h>
 #include <stdint.h>
 
 namespace e8qc {
@@ -40,24 +41,94 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         : "memory");
 }
 
-// try_wait with a suspend-time hint: the thread sleeps until the phase
-// completes or ~1 ms passes, instead of spinning on issue slots.
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+// One 2D tensor-map (TMA) tile load into shared memory completing on `bar`:
+// box origin (x, y) in elements of the map (x * element size must be a
+// multiple of 16 bytes). `map` is the address of a __grid_constant__ kernel
+// parameter.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// One bulk shared -> global copy (16-byte aligned addresses, size a multiple
+// of 16), tracked by this thread's bulk groups.
+__device__ __forceinline__ void bulk_s2g(void* gdst, const void* ssrc, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_addr(ssrc)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// At most N of this thread's bulk groups still reading shared memory.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+// At most N of this thread's bulk groups not yet complete.
+template <int N>
+__device__ __forceinline__ void bulk_wait() {
+    asm volatile("cp.async.bulk.wait_group %0;" ::"n"(N) : "memory");
+}
+// Generic-proxy shared-memory writes -> visible to the bulk-copy (async) proxy.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Plain arrival (count 1) on `bar`.
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Non-blocking test of the phase with parity `phase` (true once it completed).
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t phase) {
     uint32_t ok = 0;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}"
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
         : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(phase), "r"(1000000u)
+        : "r"(smem_addr(bar)), "r"(phase)
         : "memory");
     return ok != 0;
 }
 
-// Wait for `phase` of `bar` with an iteration cap (each try_wait suspends for
-// at most ~1 ms). Returns false on timeout (about 2 s).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, uint32_t max_iter = 2048u) {
-    for (uint32_t i = 0; i < max_iter; ++i)
-        if (mbar_try_wait(bar, phase)) return true;
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Poll `phase` of `bar` (non-blocking tests, a short sleep between tests once
+// the first few fail), giving up after about max_ms of device time, or as soon
+// as *abort (when given) is set by another role of the CTA; a timeout sets
+// *abort. Returns false when it gave up.
+__device__ __forceinline__ bool mbar_wait_poll(uint64_t* bar, uint32_t phase, volatile int* abort, uint32_t max_ms) {
+    for (int i = 0; i < 32; ++i)
+        if (mbar_test(bar, phase)) return true;
+    const uint64_t t0 = global_ns();
+    const uint64_t limit = static_cast<uint64_t>(max_ms) * 1000000ull;
+    for (uint32_t i = 0; i < (1u << 30); ++i) {
+        if (mbar_test(bar, phase)) return true;
+        __nanosleep(32);
+        if ((i & 15u) == 15u) {
+            if (abort && *abort) return false;
+            if (global_ns() - t0 > limit) break;
+        }
+    }
+    if (abort) *abort = 1;
     return false;
+}
+
+// Wait for `phase` of `bar`, giving up after about max_ms milliseconds.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, uint32_t max_ms = 2000u) {
+    return mbar_wait_poll(bar, phase, nullptr, max_ms);
+}
+
+// Like mbar_wait_bounded, but also gives up as soon as *abort is set (another
+// role of the CTA timed out), and sets *abort itself on timeout.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t phase, volatile int* abort,
+                                                   uint32_t max_ms = 2000u) {
+    return mbar_wait_poll(bar, phase, abort, max_ms);
 }
 
 }  // namespace e8qc

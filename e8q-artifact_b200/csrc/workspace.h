@@ -59,8 +59,9 @@ struct Workspace {
     // batched path (grown on demand by batched_search)
     DevBuf b_keys, b_qn2, b_probes, b_pd2, b_pos, b_pair_q, b_pair_d2, b_cnt, b_off, b_fill, b_items,
         b_nitems, b_part_d, b_part_id;
-    // precision path: int8 queries, per-query scale and sum
-    DevBuf p_q8, p_scale, p_sum;
+    // precision path: int8 queries, per-query scale and sum, per-list row
+    // bases, the proxy-distance rows and the gathered int8 query rows
+    DevBuf p_q8, p_scale, p_sum, p_rowbase, p_prox, p_a8;
     // optional CUDA events around the batched / precision scan kernel (set by
     // the caller while profiling; recorded on the launch stream)
     cudaEvent_t scan_ev0 = nullptr, scan_ev1 = nullptr;
@@ -127,10 +128,11 @@ int batched_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq
                    cudaStream_t s);
 
 // Route + per-query select + grouping of (query, list) pairs into work items
-// of up to qt queries per list (shared by the batched and precision paths);
-// partial-result buffers hold part_width entries per pair. Returns the number
-// of kernels launched.
+// of up to qt queries per list (shared by the batched and precision paths).
+// Each list's pairs start at a multiple of `align` (unused slots hold query
+// id UINT32_MAX); partial-result buffers hold part_width entries per pair.
+// Returns the number of kernels launched.
 int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* np_arr,
-                    size_t nprobe, size_t part_width, int qt, cudaStream_t s);
+                    size_t nprobe, size_t part_width, int qt, int align, cudaStream_t s);
 
 }  // namespace e8qc

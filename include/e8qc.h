@@ -173,6 +173,54 @@ int e8qc_e8q_get_ids(const e8qc_index* idx, uint32_t* out);
 int e8qc_e8q_export_codes(const e8qc_index* idx, uint16_t* digits, uint8_t* branch, float* g1,
                           float* h3);
 
+/* ---- Serving loop (no reference counterpart; the suggested
+ * e8qc_serve_{start,submit,poll,stop} of the port plan) ----
+ * A server owns a dispatcher and a completion thread over one built index.
+ * Requests (nq queries sharing k and nprobe) are copied at submit and wait in
+ * a FIFO until admitted: whenever one of `slots` batch slots is free, the
+ * dispatcher takes pending requests in order while the batch stays within
+ * max_batch_queries and its device-scratch estimate within memory_budget,
+ * and enqueues the batch (H2D copy, rotate, route, grouped scan, D2H copy) on
+ * the slot's own stream and workspace without waiting for it. Requests that
+ * arrive while batches run join the next free slot (continuous batching);
+ * batches on different slots overlap on the device. A query's result does
+ * not depend on the batch it ran in. The index must not be rebuilt or
+ * destroyed while a server runs on it. */
+typedef struct e8qc_server e8qc_server;
+typedef struct e8qc_server_config {
+    int mode;                 /* E8QC_MODE_BATCHED or E8QC_MODE_PRECISION */
+    size_t max_batch_queries; /* queries per device batch (0 = 4096) */
+    size_t max_k;             /* largest k a request may ask for (0 = 128) */
+    size_t max_nprobe;        /* largest nprobe a request may ask for (0 = nlist) */
+    size_t memory_budget;     /* device scratch bytes one batch may use (0 = 4 GiB) */
+    int slots;                /* batches in flight (0 = 2) */
+} e8qc_server_config;
+typedef struct e8qc_server_stats {
+    uint64_t submitted, rejected, completed, failed, queries_completed, batches;
+    double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> results ready, over completed requests */
+    double qps;                             /* queries completed / (last completion - first submit) */
+    double mean_batch_queries;
+    uint64_t peak_batch_bytes;              /* largest admitted batch estimate */
+} e8qc_server_stats;
+int e8qc_server_start(e8qc_index* idx, const e8qc_server_config* cfg, e8qc_server** out);
+/* Copy nq host queries (dim floats each) into a new request; *request_id
+ * identifies it. E8QC_EINVAL for bad k / nprobe, E8QC_ENOMEM when the request
+ * alone exceeds the memory budget or max_batch_queries, E8QC_ESTATE after stop. */
+int e8qc_server_submit(e8qc_server* srv, const float* queries, size_t nq, size_t k, size_t nprobe,
+                       uint64_t* request_id);
+/* Wait up to timeout_ms (negative: forever) for a request. On completion
+ * (*done = 1) the results (nq*k ids and distances, host buffers; either may be
+ * NULL) are copied out and the request is released; the return value is the
+ * request's own status (a failed batch reports its error). *done = 0 on
+ * timeout. E8QC_ERANGE for an unknown or already collected id. */
+int e8qc_server_poll(e8qc_server* srv, uint64_t request_id, int timeout_ms, uint32_t* out_ids, float* out_dists,
+                     int* done);
+/* Counters and latency percentiles; reset = 1 clears them after the read. */
+int e8qc_server_get_stats(e8qc_server* srv, int reset, e8qc_server_stats* out);
+/* Stop accepting requests, finish the batches in flight, fail the requests
+ * still pending (E8QC_ESTATE), join the threads and free the server. */
+int e8qc_server_stop(e8qc_server* srv);
+
 #ifdef __cplusplus
 }
 #endif
