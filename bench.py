@@ -218,7 +218,7 @@ def serve_open_loop(e8qlib, idx, mode, qn, k, nprobe, rate_qps, seconds, seed, m
     gaps = rng.exponential(1.0 / req_rate, n_req)
     sizes = rng.integers(1, 65, n_req)
     starts = rng.integers(0, qn.shape[0] - 64, n_req)
-    srv = e8qlib.Server(idx, mode=mode, max_batch=max_batch, max_k=max(k, 1), slots=2)
+    srv = e8qlib.Server(idx, mode=mode, max_batch=max_batch, max_k=max(k, 1), max_nprobe=nprobe, slots=2)
     ids = []
     done = threading.Event()
 
@@ -374,19 +374,19 @@ def main():
                 "algo_bytes_per_launch": int(algo_per_launch),
                 "launch_us": round(t_launch * 1e6, 2), "peak_kind": pk_kind}
     if a.path == "precision":
-        # tensor roofline: int8 multiply-adds (2 ops each) of every scored
-        # (query, vector) pair over the padded dimension, against the int8
-        # tcgen05 MMA rate measured on this GPU by the library's own probe
+        # the scan streams int8 proxy rows + (g1, h3) per vector of each work
+        # item and writes a 4-byte proxy distance per (query, vector) pair: its
+        # binding roof is HBM. Beside it, the tensor side: int8 multiply-adds
+        # (2 ops each) of every pair over the padded dimension against the int8
+        # tcgen05 MMA rate measured on this GPU by the library's own probe.
         pd = (a.dim + 63) // 64 * 64
         ops = 2.0 * prof["candidates"] * pd / max(1, prof["scan_launches"])
         i8_peak = int8_peak(local)
         tops = ops / t_launch / 1e12 if t_launch > 0 else 0.0
-        roofline = {"bound": "tensor", "achieved": round(tops, 1), "peak": round(i8_peak, 1),
-                    "unit": "TFLOP/s", "frac": round(tops / i8_peak, 4), "traffic": None, "kernel": kernel,
-                    "ops_per_launch": ops, "launch_us": round(t_launch * 1e6, 2),
-                    "peak_kind": "int8 dense tcgen05 MMA rate measured in this run (e8qlib.tc_i8_gemm, "
-                                 "148 CTAs x 128x256x256 back-to-back MMAs)",
-                    "hbm_achieved_gbs": round(achieved, 1), "hbm_peak_gbs": peak}
+        roofline.update({"tensor_achieved_tops": round(tops, 1), "tensor_peak_tops": round(i8_peak, 1),
+                         "tensor_frac": round(tops / i8_peak, 4),
+                         "tensor_peak_kind": "int8 dense tcgen05 MMA rate measured in this run "
+                                             "(e8qlib.tc_i8_gemm, 148 CTAs x 128x256x256 back-to-back MMAs)"})
 
     # e2e through the public numpy API with pinned host queries
     qh = torch.empty(a.pool, a.dim, dtype=torch.float32, pin_memory=True)

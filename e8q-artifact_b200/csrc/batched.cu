@@ -590,15 +590,24 @@ int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t n
     E8QC_CUDA(cudaMemsetAsync(ws.b_nitems.p, 0, 32, s));  // [0] n_items, [1] head, [2..5] pair/vector counts
     const size_t sel_smem = static_cast<size_t>(nlist) * 8;
     if (sel_smem > 200 * 1024) fail(E8QC_EINVAL, "batched route supports at most 25600 lists");
-    if (sel_smem > 48 * 1024)
-        E8QC_CUDA(cudaFuncSetAttribute(select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(sel_smem)));
+    {
+        // raised once per device (also keeps the call out of captured sequences)
+        int dev = 0;
+        E8QC_CUDA(cudaGetDevice(&dev));
+        static size_t configured[64] = {};
+        if (sel_smem > 48 * 1024 && configured[dev & 63] < sel_smem) {
+            E8QC_CUDA(cudaFuncSetAttribute(select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(sel_smem)));
+            configured[dev & 63] = sel_smem;
+        }
+    }
     select_kernel<<<static_cast<unsigned>(nq), 256, sel_smem, s>>>(
         ws.b_keys.as<uint64_t>(), nlist, np_arr, np_max, np_max, ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(),
         ws.b_cnt.as<uint32_t>());
     ++launches;
     uint32_t* nitems = ws.b_nitems.as<uint32_t>();
-    items_kernel<<<1, 1024, 0, s>>>(ws.b_cnt.as<uint32_t>(), ix.list_order, nlist, ws.b_off.as<uint32_t>(),
+    items_kernel<<<1, 1024, 0, s>>>(ws.b_cnt.as<uint32_t>(), ix.list_order + (ws.sched ? nlist : 0), nlist,
+                                    ws.b_off.as<uint32_t>(),
                                     ws.b_fill.as<uint32_t>(), ws.b_items.as<uint4>(), nitems,
                                     static_cast<int>(item_cap), static_cast<uint32_t>(qt),
                                     static_cast<uint32_t>(align));

@@ -10,6 +10,7 @@
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <limits>
 #include <stdexcept>
@@ -193,6 +194,21 @@ class E8qIndex {
         return py::make_tuple(ids, dg, br, g1, h3);
     }
 
+    py::dict autotune(const std::string& mode, size_t nq, size_t k, size_t nprobe) {
+        require("autotune");
+        e8qc_tuning t{};
+        {
+            py::gil_scoped_release nogil;
+            check(e8qc_e8q_autotune(idx_, mode_of(mode), nq, k, nprobe, &t));
+        }
+        py::dict d;
+        d["schedule"] = t.schedule == 0 ? "longest_list_first" : "list_id_order";
+        d["stages"] = t.stages;
+        d["best_ms"] = t.best_ms;
+        d["default_ms"] = t.default_ms;
+        return d;
+    }
+
     void profile_start() {
         require("profile");
         check(e8qc_e8q_profile(idx_, 1, nullptr));
@@ -261,6 +277,58 @@ class E8qIndex {
         require(what);
         return idx_;
     }
+};
+
+// Captured search plan (see e8qc_plan_* in e8qc.h): one CUDA graph per
+// batch size bucket. Holds a reference to the Python index.
+class Plan {
+   public:
+    Plan(py::object index, const std::string& mode, size_t max_queries, size_t k_max, size_t nprobe_max,
+         bool autotune)
+        : index_(index), k_max_(k_max) {
+        E8qIndex& ix = index.cast<E8qIndex&>();
+        dim_ = ix.dim();
+        const int md = mode_of(mode);
+        if (md == E8QC_MODE_PLAIN) throw std::invalid_argument("plans run 'batched' or 'precision'");
+        e8qc_index* h = ix.handle("plan");
+        py::gil_scoped_release nogil;
+        check(e8qc_plan_create(h, md, max_queries, k_max, nprobe_max, autotune ? 1 : 0, &plan_));
+    }
+    ~Plan() {
+        if (plan_) e8qc_plan_destroy(plan_);
+    }
+    py::tuple run(py::handle queries, py::handle k, py::handle nprobe) {
+        auto q = ensure_nd<float>(queries, "queries", 2);
+        if (static_cast<size_t>(q.shape(1)) != dim_)
+            throw std::invalid_argument("query dimension does not match index dim");
+        const size_t nq = static_cast<size_t>(q.shape(0));
+        std::vector<uint32_t> kv(nq), nv(nq);
+        auto fill = [&](py::handle h, std::vector<uint32_t>& v, const char* name) {
+            if (py::isinstance<py::int_>(h)) {
+                std::fill(v.begin(), v.end(), h.cast<uint32_t>());
+            } else {
+                auto a = ensure_nd<uint32_t>(h, name, 1);
+                if (static_cast<size_t>(a.shape(0)) != nq)
+                    throw std::invalid_argument(std::string(name) + " must have one entry per query");
+                std::copy(a.data(), a.data() + nq, v.begin());
+            }
+        };
+        fill(k, kv, "k");
+        fill(nprobe, nv, "nprobe");
+        py::array_t<uint32_t> ids({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k_max_)});
+        py::array_t<float> dists({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k_max_)});
+        if (nq > 0) {
+            py::gil_scoped_release nogil;
+            check(e8qc_plan_run(plan_, q.data(), nq, kv.data(), nv.data(), ids.mutable_data(), dists.mutable_data(),
+                                nullptr));
+        }
+        return py::make_tuple(ids, dists);
+    }
+
+   private:
+    py::object index_;
+    size_t dim_ = 0, k_max_ = 0;
+    e8qc_plan* plan_ = nullptr;
 };
 
 // Serving loop over one index (an addition of this library; see
@@ -414,6 +482,12 @@ PYBIND11_MODULE(_e8qlib, m) {
         return py::make_tuple(C, ms);
     }, py::arg("A"), py::arg("B"), py::arg("reps") = 1, py::arg("grid") = 1, py::arg("device") = 0);
 
+    py::class_<e8qb200::Plan>(m, "Plan")
+        .def(py::init<py::object, const std::string&, size_t, size_t, size_t, bool>(), py::arg("index"),
+             py::arg("mode") = "precision", py::arg("max_queries") = 4096, py::arg("k_max") = 10,
+             py::arg("nprobe_max") = 64, py::arg("autotune") = true)
+        .def("run", &e8qb200::Plan::run, py::arg("queries"), py::arg("k"), py::arg("nprobe"));
+
     py::class_<e8qb200::Server>(m, "Server")
         .def(py::init<py::object, const std::string&, size_t, size_t, size_t, size_t, int>(), py::arg("index"),
              py::arg("mode") = "precision", py::arg("max_batch") = 4096, py::arg("max_k") = 128,
@@ -441,6 +515,7 @@ PYBIND11_MODULE(_e8qlib, m) {
         .def("search_ragged", &E8qIndex::search_ragged, py::arg("queries"), py::arg("k"),
              py::arg("nprobe"), py::arg("k_max"), py::arg("mode") = "batched")
         .def("estimate", &E8qIndex::estimate, py::arg("query"), py::arg("id"))
+        .def("autotune", &E8qIndex::autotune, py::arg("mode"), py::arg("nq"), py::arg("k"), py::arg("nprobe"))
         .def("set_disable_prune", &E8qIndex::set_disable_prune, py::arg("on"))
         .def("set_prune_alpha", &E8qIndex::set_prune_alpha, py::arg("alpha"))
         .def("export_codes", &E8qIndex::export_codes)

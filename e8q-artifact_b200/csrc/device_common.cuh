@@ -93,6 +93,13 @@ struct WarpTopK {
             merge32(in ? dist : __int_as_float(0x7f800000), in ? cid : 0xFFFFFFFFu);
             return;
         }
+        if (k > 32 && __popc(m) >= 4) {
+            const int lane = threadIdx.x & 31;
+            const bool in = (m >> lane) & 1u;
+            if (k <= 64) merge_wide<2>(in ? dist : __int_as_float(0x7f800000), in ? cid : 0xFFFFFFFFu);
+            else merge_wide<4>(in ? dist : __int_as_float(0x7f800000), in ? cid : 0xFFFFFFFFu);
+            return;
+        }
         while (m) {
             const int src = __ffs(m) - 1;
             const float cd = __shfl_sync(kFull, dist, src);
@@ -101,6 +108,76 @@ struct WarpTopK {
             m &= ~(1u << src);
             m &= __ballot_sync(kFull, maybe && better(dist, cid, thr_d, thr_id));
         }
+    }
+
+    // Bitonic sort of one value per lane across the warp, ascending.
+    __device__ __forceinline__ static void sort32(float& cd, uint32_t& ci) {
+        const int lane = threadIdx.x & 31;
+#pragma unroll
+        for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+            for (int j = kk >> 1; j > 0; j >>= 1) {
+                const float pd = __shfl_xor_sync(kFull, cd, j);
+                const uint32_t pi = __shfl_xor_sync(kFull, ci, j);
+                const bool asc = (lane & kk) == 0;
+                const bool lower = (lane & j) == 0;
+                const bool take = (lower == asc) ? better(pd, pi, cd, ci) : better(cd, ci, pd, pi);
+                if (take) {
+                    cd = pd;
+                    ci = pi;
+                }
+            }
+        }
+    }
+
+    // 32 < k <= 32*S: merge one candidate per lane into the S-slot sorted list
+    // in one pass. The list (32S ascending) followed by 32S entries that hold
+    // the candidates in descending order after 32(S-1) +inf is bitonic; its
+    // lower half is min(list, that tail) element-wise -- only the last slot can
+    // change -- and a bitonic clean-up of the lower half (slot pairs in
+    // registers, then shuffles within each slot) sorts it.
+    template <int S>
+    __device__ void merge_wide(float cd, uint32_t ci) {
+        const int lane = threadIdx.x & 31;
+        sort32(cd, ci);
+        const float rd = __shfl_sync(kFull, cd, 31 - lane);  // descending
+        const uint32_t ri = __shfl_sync(kFull, ci, 31 - lane);
+        if (better(rd, ri, d[S - 1], id[S - 1])) {
+            d[S - 1] = rd;
+            id[S - 1] = ri;
+        }
+#pragma unroll
+        for (int js = S / 2; js >= 1; js >>= 1) {  // distances of 32*js: slot s with slot s + js
+#pragma unroll
+            for (int s0 = 0; s0 < S; ++s0) {
+                if ((s0 & js) == 0) {
+                    const int s1 = s0 + js;
+                    if (better(d[s1], id[s1], d[s0], id[s0])) {
+                        const float td = d[s0];
+                        const uint32_t ti = id[s0];
+                        d[s0] = d[s1];
+                        id[s0] = id[s1];
+                        d[s1] = td;
+                        id[s1] = ti;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 16; j > 0; j >>= 1) {
+            const bool lower = (lane & j) == 0;
+#pragma unroll
+            for (int s0 = 0; s0 < S; ++s0) {
+                const float pd = __shfl_xor_sync(kFull, d[s0], j);
+                const uint32_t pi = __shfl_xor_sync(kFull, id[s0], j);
+                const bool take = lower ? better(pd, pi, d[s0], id[s0]) : better(d[s0], id[s0], pd, pi);
+                if (take) {
+                    d[s0] = pd;
+                    id[s0] = pi;
+                }
+            }
+        }
+        refresh_threshold();
     }
 
     // k <= 32: merge one candidate per lane into slot 0 (sorted) in one pass:

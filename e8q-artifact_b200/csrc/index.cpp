@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <random>
@@ -97,6 +98,9 @@ struct e8qc_index {
     DevBuf signs, mean_rot, cen, cn2, tile_begin_d, list_len_d, codes, g1, h3, ids, tab,
         list_of_tile, list_begin_d, list_order;
     DevBuf proxy;  // int8 proxy plane of the precision mode, built on its first search
+    // autotuned (schedule, stages) per (mode, log2 batch size, log2 nprobe)
+    std::mutex tune_mu;
+    std::map<uint64_t, std::pair<int, int>> tuned;
     DevIndex view{};
     Workspace ws;
     bool profiling = false;
@@ -201,6 +205,84 @@ void plain_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size_
     if (st) st->launches += launches;
 }
 
+// ---- autotuning of the grouped paths ----
+int log2_ceil(size_t v) {
+    int b = 0;
+    while ((size_t(1) << b) < v) ++b;
+    return b;
+}
+uint64_t tune_key(int mode, size_t nq, size_t np) {
+    return (static_cast<uint64_t>(mode) << 32) | (static_cast<uint64_t>(log2_ceil(nq)) << 16) |
+           static_cast<uint64_t>(log2_ceil(np));
+}
+// The tuned (schedule, stages) of this batch shape, or the defaults (0, 6).
+void apply_tuning(e8qc_index* x, Workspace& ws, int mode, size_t nq, size_t np) {
+    std::lock_guard<std::mutex> lock(x->tune_mu);
+    auto it = x->tuned.find(tune_key(mode, nq, np));
+    ws.sched = it == x->tuned.end() ? 0 : it->second.first;
+    ws.stages = it == x->tuned.end() ? 6 : it->second.second;
+}
+
+struct TuneResult {
+    int sched, stages;
+    double best_ms, default_ms;
+};
+
+// Time every (schedule, stages) setting on nq synthetic queries with uniform
+// k / nprobe and keep the fastest for this batch shape. Candidate settings
+// change only the work order and the scan's ring depth, never the results.
+TuneResult autotune_run(e8qc_index* x, Workspace& ws, int mode, size_t nq, size_t k, size_t np, cudaStream_t s) {
+    np = std::min(np, x->nlist);
+    DevBuf rq, ids, d;
+    rq.alloc(nq * x->pd * 4);
+    ids.alloc(nq * k * 4);
+    d.alloc(nq * k * 4);
+    launch_synth_queries(x->view, static_cast<int>(nq), 0x5EEDull, rq.as<float>(), s);
+    ws.ensure_err();
+    auto run = [&] {
+        if (mode == E8QC_MODE_PRECISION)
+            precision_search(x->view, ws, rq.as<float>(), nq, nullptr, nullptr, k, np, k, ids.as<uint32_t>(),
+                             d.as<float>(), max_tiles_for(x, np) * 32, s);
+        else
+            batched_search(x->view, ws, rq.as<float>(), nq, nullptr, nullptr, k, np, k, ids.as<uint32_t>(),
+                           d.as<float>(), max_tiles_for(x, np), s);
+    };
+    cudaEvent_t e0, e1;
+    E8QC_CUDA(cudaEventCreate(&e0));
+    E8QC_CUDA(cudaEventCreate(&e1));
+    struct Ev {
+        cudaEvent_t a, b;
+        ~Ev() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } ev{e0, e1};
+    TuneResult best{0, 6, 1e30, 0.0};
+    const int nst = mode == E8QC_MODE_PRECISION ? 3 : 1;
+    const int stage_opts[3] = {6, 4, 8};
+    for (int sched = 0; sched < 2; ++sched) {
+        for (int si = 0; si < nst; ++si) {
+            ws.sched = sched;
+            ws.stages = stage_opts[si];
+            run();  // warm-up (sizes buffers, sets kernel attributes)
+            E8QC_CUDA(cudaEventRecord(e0, s));
+            for (int r = 0; r < 3; ++r) run();
+            E8QC_CUDA(cudaEventRecord(e1, s));
+            ws.check_error(s);
+            float ms = 0.0f;
+            E8QC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            const double t = ms / 3.0;
+            if (sched == 0 && si == 0) best.default_ms = t;
+            if (t < best.best_ms) best = TuneResult{sched, stage_opts[si], t, best.default_ms};
+        }
+    }
+    ws.sched = best.sched;
+    ws.stages = best.stages;
+    std::lock_guard<std::mutex> lock(x->tune_mu);
+    x->tuned[tune_key(mode, nq, np)] = {best.sched, best.stages};
+    return best;
+}
+
 // Batched or precision search of nq rotated queries; while profiling, times
 // the scan kernel with CUDA events and reads back its pair / vector counters.
 uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, const uint32_t* k_arr,
@@ -219,6 +301,7 @@ uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, con
         }
     } drop{ws};
     int launches = 0;
+    apply_tuning(x, ws, mode, nq, np);
     if (mode == E8QC_MODE_PRECISION && x->view.proxy == nullptr) {
         x->proxy.alloc(proxy_plane_bytes(x->view, x->ntiles));
         launches += launch_build_proxy(x->view, static_cast<int>(x->ntiles), x->proxy.as<uint4>(), s);
@@ -239,7 +322,13 @@ uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, con
         x->prof.scan_ms += ms;
         x->prof.candidates += cnt[0];
         x->prof.list_vectors += cnt[1];
-        x->prof.algo_bytes += cnt[1] * (static_cast<uint64_t>(x->bits) * x->pd / 8 + 8);
+        // algorithmic bytes of the scan kernel: per vector read by a work item its
+        // codes + (g1, h3) (batched), or its int8 proxy row + (g1, h3) plus 4
+        // bytes of proxy distance written per (query, vector) pair (precision)
+        if (mode == E8QC_MODE_PRECISION)
+            x->prof.algo_bytes += cnt[1] * (static_cast<uint64_t>(x->pd) + 8) + cnt[0] * 4;
+        else
+            x->prof.algo_bytes += cnt[1] * (static_cast<uint64_t>(x->bits) * x->pd / 8 + 8);
         x->prof.queries += nq;
     }
     return static_cast<uint64_t>(launches);
@@ -298,14 +387,16 @@ size_t search_bytes(const e8qc_index* x, int mode, size_t nq, size_t k_max, size
 // Enqueue a ragged batched / precision search of nq device-resident queries
 // (not rotated) on stream s with its own workspace: no host synchronisation,
 // no index lock (the index is read-only while serving). Kernel wait timeouts
-// land in ws's error word.
+// land in ws's error word. apply_tuned: take the autotuned setting of this
+// batch shape (else ws's own setting is used, as a captured plan fixes it).
 uint64_t server_enqueue(e8qc_index* x, Workspace& ws, int mode, const float* q_dev, size_t nq,
                         const uint32_t* k_dev, const uint32_t* np_dev, size_t k_max, size_t np_max,
-                        uint32_t* ids_dev, float* d_dev, cudaStream_t s) {
+                        uint32_t* ids_dev, float* d_dev, cudaStream_t s, bool apply_tuned) {
     const size_t np = std::min(np_max, x->nlist);
     ws.ensure_queries(nq, x->pd);
     ws.ensure_err();
     float* rq = ws.rq.as<float>();
+    if (apply_tuned) apply_tuning(x, ws, mode, nq, np);
     uint64_t launches = launch_rotate(x->view, q_dev, static_cast<int>(nq), rq, s);
     if (mode == E8QC_MODE_PRECISION)
         launches += precision_search(x->view, ws, rq, nq, k_dev, np_dev, k_max, np, k_max, ids_dev, d_dev,
@@ -314,6 +405,20 @@ uint64_t server_enqueue(e8qc_index* x, Workspace& ws, int mode, const float* q_d
         launches += batched_search(x->view, ws, rq, nq, k_dev, np_dev, k_max, np, k_max, ids_dev, d_dev,
                                    max_tiles_for(x, np), s);
     return launches;
+}
+
+// Autotune one batch shape with a caller's workspace (plans); returns the
+// chosen schedule / stages and leaves them set in ws.
+void plan_autotune(e8qc_index* x, Workspace& ws, int mode, size_t nq, size_t k, size_t np, cudaStream_t s,
+                   int* sched, int* stages) {
+    const TuneResult r = autotune_run(x, ws, mode, nq, k, np, s);
+    *sched = r.sched;
+    *stages = r.stages;
+}
+
+// The stored tuning of a batch shape (defaults when none) into ws.
+void plan_stored_tuning(e8qc_index* x, Workspace& ws, int mode, size_t nq, size_t np) {
+    apply_tuning(x, ws, mode, nq, np);
 }
 
 // Read-only view of a built index for the no-allocation plain search
@@ -503,10 +608,10 @@ int e8qc_e8q_build(e8qc_index* x, const float* data, size_t n, const float* cent
         x->list_of_tile.upload(list_of_tile.data(), list_of_tile.size() * 4, s);
         x->list_begin_d.upload(x->list_begin.data(), x->list_begin.size() * 8, s);
         {
-            // batched work queue order: longest list first (LPT)
-            std::vector<uint32_t> order(nlist);
-            for (size_t c = 0; c < nlist; ++c) order[c] = static_cast<uint32_t>(c);
-            std::stable_sort(order.begin(), order.end(),
+            // batched work queue orders: longest list first (LPT), then list id order
+            std::vector<uint32_t> order(2 * nlist);
+            for (size_t c = 0; c < nlist; ++c) order[c] = order[nlist + c] = static_cast<uint32_t>(c);
+            std::stable_sort(order.begin(), order.begin() + nlist,
                              [&](uint32_t a, uint32_t b) { return counts[a] > counts[b]; });
             x->list_order.upload(order.data(), order.size() * 4, s);
         }
@@ -744,6 +849,26 @@ int e8qc_e8q_info(const e8qc_index* x, e8qc_info* out) {
         out->built = x->built ? 1 : 0;
         out->disable_prune = x->disable_prune ? 1 : 0;
         out->prune_alpha = x->prune_alpha;
+    });
+}
+
+int e8qc_e8q_autotune(e8qc_index* x, int mode, size_t nq, size_t k, size_t nprobe, e8qc_tuning* out) {
+    return guarded([&] {
+        require_built(x, "autotune");
+        if (mode != E8QC_MODE_BATCHED && mode != E8QC_MODE_PRECISION)
+            fail(E8QC_EINVAL, "autotune covers E8QC_MODE_BATCHED and E8QC_MODE_PRECISION");
+        if (nq == 0 || k == 0 || k > static_cast<size_t>(kMaxK) || nprobe == 0)
+            fail(E8QC_EINVAL, "nq, nprobe must be positive and k in [1, 128]");
+        std::lock_guard<std::mutex> lock(x->mu);
+        DeviceGuard g(x->device);
+        cudaStream_t s = nullptr;
+        if (mode == E8QC_MODE_PRECISION && x->view.proxy == nullptr) {
+            x->proxy.alloc(proxy_plane_bytes(x->view, x->ntiles));
+            launch_build_proxy(x->view, static_cast<int>(x->ntiles), x->proxy.as<uint4>(), s);
+            x->view.proxy = x->proxy.as<uint4>();
+        }
+        const TuneResult r = autotune_run(x, x->ws, mode, nq, k, nprobe, s);
+        if (out) *out = e8qc_tuning{r.sched, r.stages, r.best_ms, r.default_ms};
     });
 }
 

@@ -99,7 +99,7 @@ struct DevIndex {
     const float* h3;             // ntiles*32
     const uint32_t* ids;         // ntiles*32, UINT32_MAX on padding lanes
     const float* tab;            // [2][2^bits] level/sqrt(pd) refine tables
-    const uint32_t* list_order;  // nlist list ids, longest list first
+    const uint32_t* list_order;  // 2 x nlist list ids: longest list first, then list id order
     const uint32_t* list_of_tile;  // ntiles: the list each tile belongs to
     const uint4* proxy;            // precision mode's int8 proxy plane, or NULL until built
 };
@@ -111,6 +111,8 @@ inline int code_chunks(int pd, int bits) { return (pd / 8 * 8 * bits + 127) / 12
 
 // Rotation + mean-centring of nq queries: out[nq][pd] = rot(q) - mean_rot.
 int launch_rotate(const DevIndex& ix, const float* q, int nq, float* out, cudaStream_t s);
+// nq synthetic rotated queries near the index's lists (tuning runs).
+int launch_synth_queries(const DevIndex& ix, int nq, unsigned long long seed, float* out, cudaStream_t s);
 // Raw rotation (no centring): n rows of dim floats -> n rows of pd floats.
 int launch_rotate_raw(const uint8_t* signs, int dim, int pd, const float* src, int n, float* dst,
                       const float* subtract, cudaStream_t s);

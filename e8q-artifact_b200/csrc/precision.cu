@@ -225,12 +225,12 @@ __global__ void gather_a8_kernel(const int8_t* __restrict__ q8, const uint32_t* 
 // roles' loops, is reported through the error word, and the CTA frees its TMEM
 // after its outstanding copies and MMAs have completed (or a last bounded wait
 // for them ran out). No role waits on a barrier that another role can skip.
-constexpr int kStages = 6;
 constexpr int kScanThreads = 192;
 constexpr uint32_t kScanCols = 512;
 constexpr int kStageBytes = kPM * kPK + kPN * kPK;  // 8 KB queries + 16 KB proxies
 constexpr int kRing = 4;                            // items in flight between roles
 
+template <int kStages>
 __global__ void __launch_bounds__(kScanThreads, 1) precision_scan_kernel(
     DevIndex ix, const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
     const uint32_t* __restrict__ pair_q,
@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
     constexpr int TCH = (64 * BITS + 127) / 128;
     extern __shared__ __align__(16) float fsm[];
     float* tabrep = fsm;               // 2*Q*REP
-    float* sq = tabrep + 2 * Q * REP;  // 4 warps x pd
+    float* sq = tabrep + 2 * Q * REP;  // 4 warps x pd, then 4 warps x kMaxK candidate slots
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int e = tid; e < 2 * Q * REP; e += blockDim.x) tabrep[e] = ix.tab[e / REP];
     const int q = blockIdx.x * 4 + warp;
@@ -479,42 +479,117 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
     const int np = np_arr ? static_cast<int>(np_arr[q]) : np_max;
     const int kq = k_arr ? static_cast<int>(k_arr[q]) : k_uniform;
     const uint32_t* pr = probes + static_cast<size_t>(q) * np_max;
-    // 1. best C proxies (slot as tie-break)
+    // 1. best C proxies (slot as tie-break). Row metadata for 32 probes at a
+    //    time sits in registers (lane j: probe w0 + j) and is read by shuffle;
+    //    values stream 512 per step, the next step's loads in flight while
+    //    the current step is offered.
     WarpTopK cand;
     cand.init(C);
-    for (int p = 0; p < np; ++p) {
-        const uint32_t L = pr[p];
-        const uint32_t len = ix.list_len[L];
-        const uint32_t t0 = ix.tile_begin[L];
-        const uint32_t stride = (ix.tile_begin[L + 1] - t0) * 32u;
-        const uint32_t pos = pos_of[static_cast<size_t>(q) * np_max + p];
-        const float4* row = reinterpret_cast<const float4*>(
-            prox + rowbase[L] + static_cast<unsigned long long>(pos - pair_off[L]) * stride);
-        const uint32_t slot0 = t0 * 32u;
-        // 256 values per step: two independent 16-byte loads per lane in flight
-        for (uint32_t v0 = 0; v0 < len; v0 += 256) {
-            float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a;
-            const uint32_t va = v0 + lane * 4, vb = v0 + 128 + lane * 4;
-            if (va < len) a = __ldcs(row + (va >> 2));
-            if (vb < len) b = __ldcs(row + (vb >> 2));
-            const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
-#pragma unroll
-            for (int j = 0; j < 4; ++j) cand.offer_pair(av[j], slot0 + va + j, va + j < len);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) cand.offer_pair(bv[j], slot0 + vb + j, vb + j < len);
+    int w0 = -32;
+    unsigned long long m_off = 0;  // this lane's row: float offset into prox
+    uint32_t m_len = 0, m_slot0 = 0;
+    auto load_window = [&](int base) {
+        w0 = base;
+        const int p = base + lane;
+        m_off = 0;
+        m_len = 0;
+        m_slot0 = 0;
+        if (p < np) {
+            const uint32_t L = pr[p];
+            const uint32_t t0 = ix.tile_begin[L];
+            const uint32_t stride = (ix.tile_begin[L + 1] - t0) * 32u;
+            const uint32_t pos = pos_of[static_cast<size_t>(q) * np_max + p];
+            m_off = rowbase[L] + static_cast<unsigned long long>(pos - pair_off[L]) * stride;
+            m_len = ix.list_len[L];
+            m_slot0 = t0 * 32u;
         }
+    };
+    struct Step {
+        int p;
+        uint32_t v0, len, slot0;
+        unsigned long long off;
+    };
+    // the step after (p, v0 + 512), skipping empty rows; p == np when done
+    auto advance = [&](int p, uint32_t v0, uint32_t len) {
+        Step st{p, v0 + 512, len, 0, 0};
+        if (st.v0 >= len) {
+            st.p = p + 1;
+            st.v0 = 0;
+            for (;; ++st.p) {
+                if (st.p >= np) break;
+                if (st.p >= w0 + 32) load_window(w0 + 32);
+                const uint32_t l = __shfl_sync(kFull, m_len, st.p - w0);
+                if (l > 0) break;
+            }
+        }
+        if (st.p < np) {
+            st.len = __shfl_sync(kFull, m_len, st.p - w0);
+            st.slot0 = __shfl_sync(kFull, m_slot0, st.p - w0);
+            st.off = __shfl_sync(kFull, m_off, st.p - w0);
+        }
+        return st;
+    };
+    auto load_step = [&](const Step& st, float4 (&x)[4]) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t va = st.v0 + 128 * j + 4 * lane;
+            x[j] = (st.p < np && va < st.len) ? __ldcs(reinterpret_cast<const float4*>(prox + st.off) + (va >> 2))
+                                              : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    };
+    load_window(0);
+    Step cur = advance(-1, 0, 0);  // first non-empty row
+    float4 cx[4];
+    load_step(cur, cx);
+    while (cur.p < np) {
+        const Step nxt = advance(cur.p, cur.v0, cur.len);
+        float4 nx[4];
+        load_step(nxt, nx);
+        // fast filter: most steps hold no value that can enter the list
+        bool any = false;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t va = cur.v0 + 128 * j + 4 * lane;
+            any |= (va + 0 < cur.len && !(cx[j].x > cand.thr_d)) || (va + 1 < cur.len && !(cx[j].y > cand.thr_d)) ||
+                   (va + 2 < cur.len && !(cx[j].z > cand.thr_d)) || (va + 3 < cur.len && !(cx[j].w > cand.thr_d));
+        }
+        // one offer site (a rolled loop keeps the code small): value t of this
+        // lane is column v0 + 128*(t/4) + 4*lane + t%4; the 16 loaded values
+        // rotate through cx[0].x
+        const int nt = __any_sync(kFull, any) ? 16 : 0;
+#pragma unroll 1
+        for (int t = 0; t < nt; ++t) {
+            const uint32_t va = cur.v0 + 128 * (t >> 2) + 4 * lane + (t & 3);
+            cand.offer_pair(cx[0].x, cur.slot0 + va, va < cur.len);
+            cx[0].x = cx[0].y; cx[0].y = cx[0].z; cx[0].z = cx[0].w; cx[0].w = cx[1].x;
+            cx[1].x = cx[1].y; cx[1].y = cx[1].z; cx[1].z = cx[1].w; cx[1].w = cx[2].x;
+            cx[2].x = cx[2].y; cx[2].y = cx[2].z; cx[2].z = cx[2].w; cx[2].w = cx[3].x;
+            cx[3].x = cx[3].y; cx[3].y = cx[3].z; cx[3].z = cx[3].w;
+        }
+        cur = nxt;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cx[j] = nx[j];
     }
-    // 2. exact rescoring of candidate (s, lane); 3. top-k by exact distance
+    // 2. exact rescoring of candidate (s, lane); 3. top-k by exact distance.
+    //    The candidates' slots go through shared memory so the loop below
+    //    stays rolled (one offer site).
+    uint32_t* cslots = reinterpret_cast<uint32_t*>(sq + 4 * pd) + warp * kMaxK;
+    {
+#pragma unroll
+        for (int s2 = 0; s2 < 4; ++s2)
+            if (s2 * 32 < C) cslots[s2 * 32 + lane] = cand.id[s2];
+        __syncwarp();
+    }
     WarpTopK top;
     top.init(kq);
     const uint32_t tb_addr = static_cast<uint32_t>(__cvta_generic_to_shared(tabrep)) + (lane % REP) * 4u;
     const float4* sq4 = reinterpret_cast<const float4*>(myq);
     const int ng = (pd / 8) / GBL;
     const bool tail = ((pd / 8) % GBL) != 0;
-#pragma unroll
+#pragma unroll 1
     for (int s = 0; s < 4; ++s) {
         if (s * 32 >= C) break;
-        const uint32_t slot = cand.id[s];
+        const uint32_t slot = cslots[s * 32 + lane];
         const bool live = s * 32 + lane < C && slot != 0xFFFFFFFFu;
         float dist = inf_f();
         uint32_t gid = 0xFFFFFFFFu;
@@ -552,7 +627,9 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
     }
 }
 
-constexpr size_t kScanSmem = static_cast<size_t>(kStages) * kStageBytes + static_cast<size_t>(4) * kPN * 8;
+constexpr size_t scan_smem(int stages) {
+    return static_cast<size_t>(stages) * kStageBytes + static_cast<size_t>(4) * kPN * 8;
+}
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against the driver library).
@@ -583,28 +660,39 @@ CUtensorMap plane_map(const void* base, size_t row_groups, int pd, uint32_t box_
     return m;
 }
 
-void launch_scan(const DevIndex& ix, Workspace& ws, size_t a_rows, size_t plane_slots, cudaStream_t s) {
+template <int STAGES>
+void launch_scan_stages(const DevIndex& ix, Workspace& ws, const CUtensorMap& map_a, const CUtensorMap& map_b,
+                        cudaStream_t s) {
     int dev = 0, sms = 148;
     E8QC_CUDA(cudaGetDevice(&dev));
+    constexpr size_t smem = scan_smem(STAGES);
     static bool configured[64] = {};
     if (!configured[dev & 63]) {
-        E8QC_CUDA(cudaFuncSetAttribute(precision_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(kScanSmem)));
+        E8QC_CUDA(cudaFuncSetAttribute(precision_scan_kernel<STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem)));
         configured[dev & 63] = true;
     }
     E8QC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     uint32_t* nitems = ws.b_nitems.as<uint32_t>();
     ws.mark_scan(false, s);
     // one CTA per SM: the two accumulators take all 512 TMEM columns
-    const CUtensorMap map_a = plane_map(ws.p_a8.p, a_rows / 8, ix.pd, 16);
-    const CUtensorMap map_b = plane_map(ix.proxy, plane_slots / 8, ix.pd, 32);
-    precision_scan_kernel<<<sms, kScanThreads, kScanSmem, s>>>(
-        ix, map_a, map_b, ws.b_pair_q.as<uint32_t>(), ws.b_pair_d2.as<float>(),
-        ws.p_scale.as<float>(), ws.p_sum.as<float>(), ws.b_items.as<uint4>(), nitems, nitems + 1,
-        ws.b_off.as<uint32_t>(), ws.p_rowbase.as<unsigned long long>(), ws.p_prox.as<float>(),
-        reinterpret_cast<unsigned long long*>(nitems + 2), ws.err.as<uint32_t>());
+    precision_scan_kernel<STAGES><<<sms, kScanThreads, smem, s>>>(
+        ix, map_a, map_b, ws.b_pair_q.as<uint32_t>(), ws.b_pair_d2.as<float>(), ws.p_scale.as<float>(),
+        ws.p_sum.as<float>(), ws.b_items.as<uint4>(), nitems, nitems + 1, ws.b_off.as<uint32_t>(),
+        ws.p_rowbase.as<unsigned long long>(), ws.p_prox.as<float>(), reinterpret_cast<unsigned long long*>(nitems + 2),
+        ws.err.as<uint32_t>());
     E8QC_CUDA(cudaGetLastError());
     ws.mark_scan(true, s);
+}
+
+void launch_scan(const DevIndex& ix, Workspace& ws, size_t a_rows, size_t plane_slots, cudaStream_t s) {
+    const CUtensorMap map_a = plane_map(ws.p_a8.p, a_rows / 8, ix.pd, 16);
+    const CUtensorMap map_b = plane_map(ix.proxy, plane_slots / 8, ix.pd, 32);
+    switch (ws.stages) {
+        case 4: launch_scan_stages<4>(ix, ws, map_a, map_b, s); break;
+        case 8: launch_scan_stages<8>(ix, ws, map_a, map_b, s); break;
+        default: launch_scan_stages<6>(ix, ws, map_a, map_b, s); break;
+    }
 }
 
 // Per-query selection + exact rescoring of one chunk of queries.
@@ -615,7 +703,7 @@ int launch_final(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, 
     int dev = 0;
     E8QC_CUDA(cudaGetDevice(&dev));
     constexpr int REP = table_rep(BITS);
-    const size_t fsmem = (static_cast<size_t>(2) * (1 << BITS) * REP + 4 * static_cast<size_t>(ix.pd)) * 4;
+    const size_t fsmem = (static_cast<size_t>(2) * (1 << BITS) * REP + 4 * static_cast<size_t>(ix.pd) + 4 * kMaxK) * 4;
     static size_t fconfigured[64] = {};
     if (fsmem > 48 * 1024 && fconfigured[dev & 63] < fsmem) {
         E8QC_CUDA(cudaFuncSetAttribute(precision_final_kernel<BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -325,6 +325,28 @@ int launch_route_one(const DevIndex& ix, const float* rq, int nprobe, const Rout
     return 1;
 }
 
+// Synthetic rotated queries for tuning runs: row i = 0.75 * c_a + 0.25 * c_b
+// for two centroids picked by a hash of (seed, i) -- points near the lists,
+// so routing and list loads look like a real batch's.
+__global__ void synth_queries_kernel(const float* __restrict__ cen, int nlist, int pd, unsigned long long seed,
+                                     float* __restrict__ out) {
+    unsigned long long h = seed + 0x9E3779B97F4A7C15ull * (blockIdx.x + 1ull);
+    h = (h ^ (h >> 30)) * 0xBF58476D1CE4E5B9ull;
+    h = (h ^ (h >> 27)) * 0x94D049BB133111EBull;
+    h ^= h >> 31;
+    const int a = static_cast<int>((h & 0xFFFFFFFFull) % static_cast<unsigned>(nlist));
+    const int b = static_cast<int>((h >> 32) % static_cast<unsigned>(nlist));
+    for (int i = threadIdx.x; i < pd; i += blockDim.x)
+        out[static_cast<size_t>(blockIdx.x) * pd + i] =
+            0.75f * cen[static_cast<size_t>(a) * pd + i] + 0.25f * cen[static_cast<size_t>(b) * pd + i];
+}
+
+int launch_synth_queries(const DevIndex& ix, int nq, unsigned long long seed, float* out, cudaStream_t s) {
+    synth_queries_kernel<<<nq, 256, 0, s>>>(ix.cen, ix.nlist, ix.pd, seed, out);
+    E8QC_CUDA(cudaGetLastError());
+    return 1;
+}
+
 int launch_estimate(const DevIndex& ix, const float* rq, int list, uint32_t slot, float* out,
                     cudaStream_t s) {
     switch (ix.bits) {

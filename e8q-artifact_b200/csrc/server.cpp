@@ -1,14 +1,16 @@
 // Serving loop: continuous batching of search requests over one index.
 //
-// submit() copies a request's queries to the host and queues it. The
-// dispatcher thread waits for a free batch slot and pending requests, admits
-// requests in FIFO order while the batch stays within max_batch_queries and
-// its device-scratch estimate within the memory budget, packs their queries
-// and per-query k / nprobe into the slot's pinned staging, and enqueues the
-// batch on the slot's stream: H2D copies, rotate + route + grouped scan
-// (batched or precision mode, with the slot's own workspace), D2H copies, an
-// event. It never waits for the GPU, so a second slot's batch is queued while
-// the first runs. The completion thread waits on slots in dispatch order,
+// At start the server sizes its batches: max_admit = the largest batch (up
+// to max_batch_queries) whose device scratch at (max_k, max_nprobe) fits the
+// memory budget; every slot then holds a captured plan for 64, 128, ...
+// max_admit queries (own workspace, autotuned settings). submit() copies a
+// request's queries to the host and queues it. The dispatcher thread waits
+// for a free slot and pending requests, admits requests in FIFO order while
+// the batch stays within max_admit queries, packs their queries and per-query
+// k / nprobe into the slot's pinned staging, and enqueues the batch on the
+// slot's stream: H2D copies, one graph launch (rotate + route + grouped scan,
+// batched or precision mode), D2H copies, an event. It never waits for the
+// GPU, so a second slot's batch is queued while the first runs. The completion thread waits on slots in dispatch order,
 // checks the slot's device error word, copies each request's rows out of the
 // staging and wakes its pollers; latencies are submit -> results ready.
 #include <cuda_runtime.h>
@@ -36,9 +38,10 @@ void set_last_error(const std::string& s);
 void server_index_info(e8qc_index* x, size_t* dim, size_t* nlist, int* device);
 void server_prepare(e8qc_index* x, int mode);
 size_t search_bytes(const e8qc_index* x, int mode, size_t nq, size_t k_max, size_t np_max);
-uint64_t server_enqueue(e8qc_index* x, Workspace& ws, int mode, const float* q_dev, size_t nq,
-                        const uint32_t* k_dev, const uint32_t* np_dev, size_t k_max, size_t np_max,
-                        uint32_t* ids_dev, float* d_dev, cudaStream_t s);
+e8qc_plan* plan_make(e8qc_index* idx, int mode, size_t max_q, size_t k_max, size_t np_max, bool autotune);
+void plan_enqueue(e8qc_plan* P, const float* queries, size_t nq, const uint32_t* k, const uint32_t* nprobe,
+                  uint32_t* out_ids, float* out_dists, cudaStream_t s);
+void plan_check(e8qc_plan* P, cudaStream_t s);
 }  // namespace e8qc
 
 using namespace e8qc;
@@ -70,15 +73,15 @@ struct PinnedBuf {
 struct Slot {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
-    Workspace ws;
+    e8qc_plan* plan = nullptr;  // captured graphs of this slot's batch sizes, own workspace
     PinnedBuf<float> hq, hd;
     PinnedBuf<uint32_t> hk, hnp, hids;
-    DevBuf q, k, np, ids, d;
     std::vector<std::shared_ptr<Request>> reqs;
-    size_t nq = 0, k_max = 0, bytes = 0;
+    size_t nq = 0, bytes = 0;
     int error = 0;
     std::string error_msg;
     ~Slot() {
+        if (plan) e8qc_plan_destroy(plan);
         if (done) cudaEventDestroy(done);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -90,6 +93,7 @@ struct e8qc_server {
     e8qc_index* idx = nullptr;
     e8qc_server_config cfg{};
     size_t dim = 0, nlist = 0;
+    size_t max_admit = 0;  // largest batch the budget admits at (max_k, max_nprobe); the plans' size
     int device = 0;
     std::mutex mu;
     std::condition_variable cv_dispatch, cv_complete, cv_done;
@@ -116,9 +120,10 @@ int fail_status(std::string& msg, const std::exception& e) {
     return E8QC_ECUDA;
 }
 
-// Pack and enqueue one admitted batch on its slot (dispatcher thread, no lock).
+// Pack one admitted batch into its slot's pinned staging and enqueue it as
+// one captured graph launch (dispatcher thread, no lock).
 void launch_batch(e8qc_server* S, Slot& sl) {
-    size_t row = 0, np_max = 0;
+    size_t row = 0;
     for (auto& r : sl.reqs) {
         std::memcpy(sl.hq.p + row * S->dim, r->q.data(), r->nq * S->dim * sizeof(float));
         for (size_t i = 0; i < r->nq; ++i) {
@@ -126,18 +131,9 @@ void launch_batch(e8qc_server* S, Slot& sl) {
             sl.hnp.p[row + i] = static_cast<uint32_t>(r->nprobe);
         }
         row += r->nq;
-        np_max = std::max(np_max, std::min(r->nprobe, S->nlist));
     }
-    const size_t nq = sl.nq, km = sl.k_max;
-    cudaStream_t s = sl.stream;
-    E8QC_CUDA(cudaMemcpyAsync(sl.q.p, sl.hq.p, nq * S->dim * sizeof(float), cudaMemcpyHostToDevice, s));
-    E8QC_CUDA(cudaMemcpyAsync(sl.k.p, sl.hk.p, nq * 4, cudaMemcpyHostToDevice, s));
-    E8QC_CUDA(cudaMemcpyAsync(sl.np.p, sl.hnp.p, nq * 4, cudaMemcpyHostToDevice, s));
-    server_enqueue(S->idx, sl.ws, S->cfg.mode, sl.q.as<float>(), nq, sl.k.as<uint32_t>(), sl.np.as<uint32_t>(), km,
-                   np_max, sl.ids.as<uint32_t>(), sl.d.as<float>(), s);
-    E8QC_CUDA(cudaMemcpyAsync(sl.hids.p, sl.ids.p, nq * km * 4, cudaMemcpyDeviceToHost, s));
-    E8QC_CUDA(cudaMemcpyAsync(sl.hd.p, sl.d.p, nq * km * 4, cudaMemcpyDeviceToHost, s));
-    E8QC_CUDA(cudaEventRecord(sl.done, s));
+    plan_enqueue(sl.plan, sl.hq.p, sl.nq, sl.hk.p, sl.hnp.p, sl.hids.p, sl.hd.p, sl.stream);
+    E8QC_CUDA(cudaEventRecord(sl.done, sl.stream));
 }
 
 void dispatcher_main(e8qc_server* S) {
@@ -154,27 +150,20 @@ void dispatcher_main(e8qc_server* S) {
         Slot& sl = *S->slots[si];
         // admission: FIFO while the batch fits both limits
         sl.reqs.clear();
-        size_t nq = 0, km = 0, np = 0, bytes = 0;
-        while (!S->pending.empty()) {
-            const auto& r = S->pending.front();
-            const size_t nq2 = nq + r->nq, km2 = std::max(km, r->k);
-            const size_t np2 = std::max(np, std::min(r->nprobe, S->nlist));
-            const size_t b2 = search_bytes(S->idx, S->cfg.mode, nq2, km2, np2);
-            if (nq2 > S->cfg.max_batch_queries || (b2 > S->cfg.memory_budget && !sl.reqs.empty())) break;
-            sl.reqs.push_back(r);
+        // (the slot's plan reserved the scratch of max_admit queries at
+        // (max_k, max_nprobe), the largest batch within the memory budget)
+        size_t nq = 0;
+        while (!S->pending.empty() && nq + S->pending.front()->nq <= S->max_admit) {
+            nq += S->pending.front()->nq;
+            sl.reqs.push_back(S->pending.front());
             S->pending.pop_front();
-            nq = nq2;
-            km = km2;
-            np = np2;
-            bytes = b2;
         }
         S->free_slots.pop_front();
         sl.nq = nq;
-        sl.k_max = km;
-        sl.bytes = bytes;
+        sl.bytes = search_bytes(S->idx, S->cfg.mode, nq, S->cfg.max_k, S->cfg.max_nprobe);
         sl.error = 0;
         sl.error_msg.clear();
-        S->peak_bytes = std::max<uint64_t>(S->peak_bytes, bytes);
+        S->peak_bytes = std::max<uint64_t>(S->peak_bytes, sl.bytes);
         lk.unlock();
         try {
             launch_batch(S, sl);
@@ -201,7 +190,7 @@ void completer_main(e8qc_server* S) {
         if (st == 0) {
             try {
                 E8QC_CUDA(cudaEventSynchronize(sl.done));
-                sl.ws.check_error(sl.stream);
+                plan_check(sl.plan, sl.stream);
             } catch (const std::exception& e) {
                 st = fail_status(sl.error_msg, e);
             }
@@ -213,8 +202,8 @@ void completer_main(e8qc_server* S) {
                 r->ids.resize(r->nq * r->k);
                 r->d.resize(r->nq * r->k);
                 for (size_t i = 0; i < r->nq; ++i) {
-                    std::memcpy(&r->ids[i * r->k], sl.hids.p + (row + i) * sl.k_max, r->k * 4);
-                    std::memcpy(&r->d[i * r->k], sl.hd.p + (row + i) * sl.k_max, r->k * 4);
+                    std::memcpy(&r->ids[i * r->k], sl.hids.p + (row + i) * S->cfg.max_k, r->k * 4);
+                    std::memcpy(&r->d[i * r->k], sl.hd.p + (row + i) * S->cfg.max_k, r->k * 4);
                 }
             }
             row += r->nq;
@@ -285,21 +274,25 @@ extern "C" int e8qc_server_start(e8qc_index* idx, const e8qc_server_config* cfg,
         } restore{prev};
         server_prepare(idx, S->cfg.mode);
         const size_t B = S->cfg.max_batch_queries, K = S->cfg.max_k;
+        // the largest batch whose scratch at (max_k, max_nprobe) fits the budget
+        size_t nw = 1;
+        for (size_t step = B; step > 0; step >>= 1)
+            while (nw + step <= B &&
+                   search_bytes(idx, S->cfg.mode, nw + step, K, S->cfg.max_nprobe) <= S->cfg.memory_budget)
+                nw += step;
+        S->max_admit = nw;
         for (int i = 0; i < S->cfg.slots; ++i) {
             auto sl = std::make_unique<Slot>();
             E8QC_CUDA(cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking));
             E8QC_CUDA(cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming));
-            sl->ws.device = S->device;
-            sl->hq.alloc(B * S->dim);
-            sl->hk.alloc(B);
-            sl->hnp.alloc(B);
-            sl->hids.alloc(B * K);
-            sl->hd.alloc(B * K);
-            sl->q.alloc(B * S->dim * 4);
-            sl->k.alloc(B * 4);
-            sl->np.alloc(B * 4);
-            sl->ids.alloc(B * K * 4);
-            sl->d.alloc(B * K * 4);
+            sl->hq.alloc(nw * S->dim);
+            sl->hk.alloc(nw);
+            sl->hnp.alloc(nw);
+            sl->hids.alloc(nw * K);
+            sl->hd.alloc(nw * K);
+            // captured graphs for batches of 64, 128, ... nw queries; the first
+            // slot autotunes each size, the others take the stored settings
+            sl->plan = plan_make(idx, S->cfg.mode, nw, K, S->cfg.max_nprobe, i == 0);
             S->free_slots.push_back(i);
             S->slots.push_back(std::move(sl));
         }
@@ -317,9 +310,7 @@ extern "C" int e8qc_server_submit(e8qc_server* S, const float* queries, size_t n
         if (nq == 0 || !queries) fail(E8QC_EINVAL, "a request needs at least one query");
         if (k == 0 || k > S->cfg.max_k) fail(E8QC_EINVAL, "k must be in [1, max_k]");
         if (nprobe == 0 || nprobe > S->cfg.max_nprobe) fail(E8QC_EINVAL, "nprobe must be in [1, max_nprobe]");
-        const bool too_big = nq > S->cfg.max_batch_queries ||
-                             search_bytes(S->idx, S->cfg.mode, nq, k, std::min(nprobe, S->nlist)) >
-                                 S->cfg.memory_budget;
+        const bool too_big = nq > S->max_admit;
         {
             std::lock_guard<std::mutex> lk(S->mu);
             if (S->stopping) fail(E8QC_ESTATE, "server is stopping");

@@ -62,6 +62,11 @@ struct Workspace {
     // precision path: int8 queries, per-query scale and sum, per-list row
     // bases, the proxy-distance rows and the gathered int8 query rows
     DevBuf p_q8, p_scale, p_sum, p_rowbase, p_prox, p_a8;
+    // tuning of the grouped paths (chosen by the autotuner): work-queue order
+    // (0: longest list first, 1: list id order) and the precision scan's
+    // shared-memory ring depth (4, 6 or 8 K-chunk stages)
+    int sched = 0;
+    int stages = 6;
     // optional CUDA events around the batched / precision scan kernel (set by
     // the caller while profiling; recorded on the launch stream)
     cudaEvent_t scan_ev0 = nullptr, scan_ev1 = nullptr;

@@ -138,7 +138,9 @@ typedef struct e8qc_profile {
     uint64_t scan_launches;  /* dominant-kernel launches timed */
     double scan_ms;          /* summed CUDA-event time of those launches */
     uint64_t candidates;     /* (query, vector) pairs scored */
-    uint64_t algo_bytes;     /* candidates * (bits*padded_dim/8 + 8): codes + g1/h3 */
+    uint64_t algo_bytes;     /* plain: candidates * (bits*padded_dim/8 + 8), codes + g1/h3; batched:
+                                list_vectors * (bits*padded_dim/8 + 8); precision: list_vectors *
+                                (padded_dim + 8) int8 proxies + g1/h3, plus 4 per candidate written */
     uint64_t queries;
     uint64_t list_vectors;   /* vectors read from the lists (batched modes: once per work item) */
 } e8qc_profile;
@@ -173,6 +175,36 @@ int e8qc_e8q_get_ids(const e8qc_index* idx, uint32_t* out);
 int e8qc_e8q_export_codes(const e8qc_index* idx, uint16_t* digits, uint8_t* branch, float* g1,
                           float* h3);
 
+/* ---- Autotuning and captured plans (no reference counterpart) ---- */
+typedef struct e8qc_tuning {
+    int schedule;      /* work-queue order: 0 longest list first, 1 list id order */
+    int stages;        /* precision scan K-chunk ring depth: 4, 6 or 8 (6 in batched mode) */
+    double best_ms;    /* one batch with the chosen setting (CUDA events) */
+    double default_ms; /* one batch with the default setting (schedule 0, 6 stages) */
+} e8qc_tuning;
+/* Time the tunable settings of mode E8QC_MODE_BATCHED / E8QC_MODE_PRECISION
+ * on nq synthetic queries (mixtures of the index's centroids) with k and
+ * nprobe, and keep the fastest for this batch shape (power-of-two buckets of
+ * nq and nprobe): later searches of that shape use it. Settings change the
+ * order of work only; results are identical under every setting. */
+int e8qc_e8q_autotune(e8qc_index* idx, int mode, size_t nq, size_t k, size_t nprobe, e8qc_tuning* out);
+
+/* A captured search plan: for batch sizes 64, 128, ... up to max_queries it
+ * autotunes (if asked), sizes its own workspace and captures the whole ragged
+ * search (rotate, route, select, group, scan, merge / rescore) as one CUDA
+ * graph. e8qc_plan_run pads a batch of nq <= max_queries queries (k[i] <=
+ * k_max, nprobe[i] <= nprobe_max; host arrays) to the next captured size and
+ * launches that graph on `stream`; queries and outputs may be host or device
+ * pointers; out rows are k_max wide; it returns once the results are in the
+ * outputs. One plan runs one batch at a time. The index must not be rebuilt
+ * while a plan exists. */
+typedef struct e8qc_plan e8qc_plan;
+int e8qc_plan_create(e8qc_index* idx, int mode, size_t max_queries, size_t k_max, size_t nprobe_max, int autotune,
+                     e8qc_plan** out);
+int e8qc_plan_run(e8qc_plan* plan, const float* queries, size_t nq, const uint32_t* k, const uint32_t* nprobe,
+                  uint32_t* out_ids, float* out_dists, void* stream);
+int e8qc_plan_destroy(e8qc_plan* plan);
+
 /* ---- Serving loop (no reference counterpart; the suggested
  * e8qc_serve_{start,submit,poll,stop} of the port plan) ----
  * A server owns a dispatcher and a completion thread over one built index.
@@ -184,7 +216,9 @@ int e8qc_e8q_export_codes(const e8qc_index* idx, uint16_t* digits, uint8_t* bran
  * the slot's own stream and workspace without waiting for it. Requests that
  * arrive while batches run join the next free slot (continuous batching);
  * batches on different slots overlap on the device. A query's result does
- * not depend on the batch it ran in. The index must not be rebuilt or
+ * not depend on the batch it ran in. At start every slot runs, once, the
+ * largest batch the budget admits at (max_k, max_nprobe), so its scratch is
+ * allocated before the first request. The index must not be rebuilt or
  * destroyed while a server runs on it. */
 typedef struct e8qc_server e8qc_server;
 typedef struct e8qc_server_config {
