@@ -8,16 +8,25 @@ sqrt(lambda) scaling applies to both draws), cluster_ids = generating
 component, centroids = per-list means; 10,240 queries from the same mixture;
 E8Q nbits=6 (the lowest rate whose recall@10 clears 0.95 on this mixture),
 k=10, nprobe=64; one step = one batch of 4,096 queries through the search
-path. Synthetic data stands in for the public corpora (no network).
+path (default --path precision: int8 tensor-core candidates + exact
+rescoring; --path batched / plain measure the other modes). Synthetic data
+stands in for the public corpora (no network).
 
   value  : QPS with queries already in HBM (E8qIndex.search_ptr), CUDA events
            on the launching stream, max over ranks; --gpus N runs N replicas
            (the index fits one GPU; no data-path collective), scaling "weak".
   e2e    : the same QPS through E8qIndex.search(numpy) with pinned host query
-           buffers: H2D of the queries and D2H of ids+dists inside the timing.
-  roofline: the dominant scan kernel, algorithmic bytes (codes + g1/h3 of every
-           scored candidate) per launch / CUDA-event launch time, against the
-           measured HBM copy bandwidth.
+           buffers: H2D of the queries and D2H of ids+dists inside the timing
+           (events; host_wall_qps is the same loop by the host clock).
+  roofline: the dominant scan kernel's algorithmic bytes per launch over its
+           CUDA-event time against the measured HBM copy bandwidth -- for the
+           precision scan: int8 proxy row + g1/h3 per vector of each work item
+           plus 4 bytes of proxy distance written per (query, vector) pair;
+           beside it the int8 tensor ops against an int8 MMA rate measured in
+           the run with the library's tcgen05 probe.
+  plain_gpu_qps: the plain one-query-per-launch GPU scan on the same index.
+  serving: open-loop Poisson load through e8qlib.Server (U{1..64} queries per
+           request) at fractions of `value`: achieved QPS, p50/p99/max ms.
   cpu_baseline: the reference's own CPU search (compiled from its sources into
            oracle/_ref), all host cores, a bounded sample of the same workload.
 
@@ -396,19 +405,22 @@ def main():
         idx.search(qn[:nb], a.k, a.nprobe, mode=a.path)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0 = time.perf_counter()
     e0.record(stream)
     for i in range(a.steps):
         j = i % nbat
         idx.search(qn[j * nb:(j + 1) * nb], a.k, a.nprobe, mode=a.path)
     e1.record(stream)
     torch.cuda.synchronize()
+    e2e_wall_ms = (time.perf_counter() - w0) * 1000.0
     e2e_ms = e0.elapsed_time(e1)
     if dist:
         t = torch.tensor([e2e_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e = {"value": round(total_q / (e2e_ms / 1000.0), 1), "unit": "QPS",
-           "h2d_bytes_per_step": nb * a.dim * 4, "d2h_bytes_per_step": nb * a.k * 8}
+           "h2d_bytes_per_step": nb * a.dim * 4, "d2h_bytes_per_step": nb * a.k * 8,
+           "host_wall_qps": round(total_q / (e2e_wall_ms / 1000.0), 1)}
 
     # the plain one-query-per-launch GPU scan on the same index (the drop-in
     # path the batched modes are compared against), a short device-resident run

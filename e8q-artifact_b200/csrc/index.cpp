@@ -68,7 +68,7 @@ std::vector<uint8_t> rotator_signs(size_t dim, uint64_t seed) {
 template <class T>
 const T* stage_in(const T* p, size_t count, DevBuf& tmp, cudaStream_t s) {
     if (count == 0 || is_device_ptr(p)) return p;
-    tmp.alloc(count * sizeof(T));
+    tmp.ensure(count * sizeof(T));
     E8QC_CUDA(cudaMemcpyAsync(tmp.p, p, count * sizeof(T), cudaMemcpyHostToDevice, s));
     return static_cast<const T*>(tmp.p);
 }
@@ -700,14 +700,18 @@ int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, si
         cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
         if (stats)
             for (auto& e : ev) E8QC_CUDA(cudaEventCreate(&e));
-        DevBuf tq, tids, tds;
+        // host-buffer staging lives in the workspace (grown, never freed per call:
+        // cudaFree would synchronise the device on every search)
+        DevBuf& tq = x->ws.stage_q;
+        DevBuf& tids = x->ws.stage_ids;
+        DevBuf& tds = x->ws.stage_d;
         const float* qd = stage_in(queries, nq * x->dim, tq, s);
         const bool ids_dev = is_device_ptr(out_ids);
         const bool d_dev = out_dists != nullptr && is_device_ptr(out_dists);
         uint32_t* ids_d = out_ids;
         float* d_d = out_dists;
-        if (!ids_dev) { tids.alloc(nq * k * 4); ids_d = tids.as<uint32_t>(); }
-        if (!d_dev) { tds.alloc(nq * k * 4); d_d = tds.as<float>(); }
+        if (!ids_dev) { tids.ensure(nq * k * 4); ids_d = tids.as<uint32_t>(); }
+        if (!d_dev) { tds.ensure(nq * k * 4); d_d = tds.as<float>(); }
         x->ws.ensure_queries(nq, x->pd);
         float* rq = x->ws.rq.as<float>();
         if (stats) E8QC_CUDA(cudaEventRecord(ev[0], s));
@@ -771,16 +775,22 @@ int e8qc_e8q_search_ragged_mode(e8qc_index* x, const float* queries, size_t nq, 
             nph[i] = static_cast<uint32_t>(std::min<size_t>(nph[i], x->nlist));
             np_max = std::max<size_t>(np_max, nph[i]);
         }
-        DevBuf tq, tk, tnp, tids, tds;
+        DevBuf& tq = x->ws.stage_q;
+        DevBuf& tk = x->ws.stage_k;
+        DevBuf& tnp = x->ws.stage_np;
+        DevBuf& tids = x->ws.stage_ids;
+        DevBuf& tds = x->ws.stage_d;
         const float* qd = stage_in(queries, nq * x->dim, tq, s);
-        tk.upload(kh.data(), nq * 4, s);
-        tnp.upload(nph.data(), nq * 4, s);
+        tk.ensure(nq * 4);
+        tnp.ensure(nq * 4);
+        E8QC_CUDA(cudaMemcpyAsync(tk.p, kh.data(), nq * 4, cudaMemcpyHostToDevice, s));
+        E8QC_CUDA(cudaMemcpyAsync(tnp.p, nph.data(), nq * 4, cudaMemcpyHostToDevice, s));
         const bool ids_dev = is_device_ptr(out_ids);
         const bool d_dev = out_dists != nullptr && is_device_ptr(out_dists);
         uint32_t* ids_d = out_ids;
         float* d_d = out_dists;
-        if (!ids_dev) { tids.alloc(nq * k_max * 4); ids_d = tids.as<uint32_t>(); }
-        if (!d_dev) { tds.alloc(nq * k_max * 4); d_d = tds.as<float>(); }
+        if (!ids_dev) { tids.ensure(nq * k_max * 4); ids_d = tids.as<uint32_t>(); }
+        if (!d_dev) { tds.ensure(nq * k_max * 4); d_d = tds.as<float>(); }
         x->ws.ensure_queries(nq, x->pd);
         float* rq = x->ws.rq.as<float>();
         uint64_t launches = launch_rotate(x->view, qd, static_cast<int>(nq), rq, s);

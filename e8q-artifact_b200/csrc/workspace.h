@@ -48,6 +48,8 @@ struct DevBuf {
 struct Workspace {
     int device = 0;
     DevBuf rq;  // nq*pd rotated queries
+    // staging of host-buffer calls: queries, per-query k / nprobe, results
+    DevBuf stage_q, stage_k, stage_np, stage_ids, stage_d;
     size_t rq_cap = 0;
     // plain path
     DevBuf keys, probes, probe_d2, tile_off, route_counter, total_tiles;

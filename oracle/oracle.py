@@ -71,6 +71,23 @@ def lib() -> C.CDLL:
         L.orc_e8q_route.argtypes = [C.c_void_p, _f32p, C.c_size_t, _u32p, _f32p]
         L.orc_e8q_search.argtypes = [C.c_void_p, _f32p, C.c_size_t, C.c_size_t, C.c_size_t,
                                      _u32p, _f32p, C.c_int]
+        L.orc_me8q_variance.argtypes = [_f32p, C.c_size_t, C.c_size_t, C.c_size_t, _f32p]
+        L.orc_me8q_allocate.argtypes = [_f32p, C.c_size_t, C.c_float, C.c_int, C.c_double,
+                                        C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
+        L.orc_me8q_allocate.restype = C.c_int
+        L.orc_me8q_build.argtypes = [_f32p, _f32p, _u32p, C.c_size_t, C.c_size_t, C.c_size_t,
+                                     C.POINTER(C.c_size_t), C.POINTER(C.c_int), C.c_int, C.c_uint64,
+                                     C.c_int, C.c_int]
+        L.orc_me8q_build.restype = C.c_void_p
+        L.orc_me8q_free.argtypes = [C.c_void_p]
+        L.orc_me8q_shape.argtypes = [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
+                                     C.POINTER(C.c_int)]
+        L.orc_me8q_codes.argtypes = [C.c_void_p, C.c_size_t, _u16p, _u8p, _f32p, _f32p]
+        L.orc_me8q_ids.argtypes = [C.c_void_p, _u32p]
+        L.orc_me8q_estimate.argtypes = [C.c_void_p, _f32p, C.c_uint32]
+        L.orc_me8q_estimate.restype = C.c_float
+        L.orc_me8q_search.argtypes = [C.c_void_p, _f32p, C.c_size_t, C.c_size_t, C.c_size_t,
+                                      _u32p, _f32p, C.c_int]
         _lib = L
     return _lib
 
@@ -336,3 +353,163 @@ def parse_e8ax(path: str) -> dict:
     out.update(rowa=rowa, refine=refine[:, :stride], g1=g1, h3=h3, digits=digits,
                branch=branch)
     return out
+
+
+# ---- ME8Q (mixed-rate) -----------------------------------------------------
+
+ME8Q_DEFAULT_ROT_SEED = 0x5EED1234  # include/e8qlib/index/me8q.hpp:38 (BuildOptions::rot_seed)
+
+
+def me8q_variance(base: np.ndarray) -> np.ndarray:
+    """detail::DatasetVariance (src/index/me8q_common.cpp:11-35)."""
+    base = np.ascontiguousarray(base, np.float32)
+    n, dim = base.shape
+    out = np.zeros(dim, np.float32)
+    lib().orc_me8q_variance(base, dim, n, dim, out)
+    return out
+
+
+def me8q_allocate(var_padded: np.ndarray, avg_bits: float, max_bits: int = 13, extra_bits: float = 0.0):
+    """SAQ DP plan over the padded dimension: [(len, bits), ...]."""
+    v = np.ascontiguousarray(var_padded, np.float32)
+    pd = v.shape[0]
+    lens = (C.c_size_t * (pd // 64 + 1))()
+    bits = (C.c_int * (pd // 64 + 1))()
+    nr = lib().orc_me8q_allocate(v, pd, avg_bits, max_bits, extra_bits, lens, bits)
+    return [(int(lens[i]), int(bits[i])) for i in range(nr)]
+
+
+def parse_plan_spec(spec: str, pd: int):
+    """detail::ParsePlanSpec (src/index/me8q_common.cpp:37-68)."""
+    plan = []
+    for tok in spec.split(","):
+        if not tok:
+            continue
+        ln, b = tok.split(":")
+        ln, b = int(ln), int(b)
+        if ln <= 0 or ln % 64 or b < 0 or b > 13:
+            raise ValueError("plan_spec: bad run " + tok)
+        plan.append((ln, b))
+    if sum(p[0] for p in plan) != pd:
+        raise ValueError("plan_spec: runs do not cover the padded dims")
+    return plan
+
+
+class OracleMe8qIndex:
+    """The restated ME8Q index (plain SearchIVF path) as a Python object."""
+
+    def __init__(self, data, centroids, cluster_ids, avg_bits=4.0, seed=0, variance=None, drop_energy=True,
+                 plan_spec="", extra_budget_bits=0.0, max_bits=13, threads=8):
+        data = np.ascontiguousarray(data, np.float32)
+        centroids = np.ascontiguousarray(centroids, np.float32)
+        cluster_ids = np.ascontiguousarray(cluster_ids, np.uint32)
+        self.n, self.dim = data.shape
+        self.nlist = centroids.shape[0]
+        self.pd = padded_dim(self.dim)
+        if plan_spec:
+            self.plan = parse_plan_spec(plan_spec, self.pd)
+        else:
+            var = np.zeros(self.pd, np.float32)
+            var[:self.dim] = me8q_variance(data) if variance is None else np.asarray(variance, np.float32)
+            self.plan = me8q_allocate(var, avg_bits, max_bits, extra_budget_bits)
+        rot_seed = seed if seed != 0 else ME8Q_DEFAULT_ROT_SEED
+        lens = (C.c_size_t * len(self.plan))(*[p[0] for p in self.plan])
+        bits = (C.c_int * len(self.plan))(*[p[1] for p in self.plan])
+        self._p = lib().orc_me8q_build(data, centroids, cluster_ids, self.n, self.dim, self.nlist, lens, bits,
+                                       len(self.plan), rot_seed, 1 if drop_energy else 0, threads)
+        n, pd, nc = C.c_size_t(), C.c_size_t(), C.c_int()
+        lib().orc_me8q_shape(self._p, C.byref(n), C.byref(pd), C.byref(nc))
+        self.ncoded = nc.value
+        self.ids = np.zeros(self.n, np.uint32)
+        lib().orc_me8q_ids(self._p, self.ids)
+
+    def __del__(self):
+        if getattr(self, "_p", None):
+            lib().orc_me8q_free(self._p)
+            self._p = None
+
+    def codes(self, pos):
+        """(digits [pd] u16, branch [pd/8] u8, coef [ncoded], h2 [ncoded]) at cluster-major pos."""
+        dg = np.zeros(self.pd, np.uint16)
+        br = np.zeros(self.pd // 8, np.uint8)
+        cf = np.zeros(max(self.ncoded, 1), np.float32)
+        h2 = np.zeros(max(self.ncoded, 1), np.float32)
+        lib().orc_me8q_codes(self._p, pos, dg, br, cf, h2)
+        return dg, br, cf[:self.ncoded], h2[:self.ncoded]
+
+    def estimate(self, q, gid):
+        return lib().orc_me8q_estimate(self._p, np.ascontiguousarray(q, np.float32), gid)
+
+    def search(self, queries, k, nprobe, threads=8):
+        queries = np.ascontiguousarray(np.atleast_2d(queries), np.float32)
+        nq = queries.shape[0]
+        ids = np.zeros((nq, k), np.uint32)
+        dists = np.zeros((nq, k), np.float32)
+        lib().orc_me8q_search(self._p, queries, nq, k, nprobe, ids, dists, threads)
+        return ids, dists
+
+
+def parse_me8q(path: str) -> dict:
+    """Fields of a reference-written ME8Q index file (src/index/me8q_io.cpp:29-65,
+    ME8QIDXX), with every row's segment codes unpacked (digits 0..6 at `bits`
+    each, digit 7 without its parity bit at bits-1, branch in the block's top
+    bit: src/quantization/me8q_codec.cpp:109-127) and its (coef, h2) pairs."""
+    with open(path, "rb") as f:
+        raw = f.read()
+    off = [0]
+
+    def take(fmt):
+        v = struct.unpack_from(fmt, raw, off[0])
+        off[0] += struct.calcsize(fmt)
+        return v
+
+    assert raw[:8] == b"ME8QIDXX"
+    off[0] = 8
+    n, dim, pd, nlist, bpv = take("<5Q")
+    take("<f")
+    take("<4i")
+    (nplan,) = take("<Q")
+    plan = []
+    for _ in range(nplan):
+        ln, b = take("<Qi")
+        plan.append((ln, b))
+
+    def arr(count, dt):
+        a = np.frombuffer(raw, dt, count, off[0]).copy()
+        off[0] += a.nbytes
+        return a
+
+    centroids = arr(nlist * pd, np.float32).reshape(nlist, pd)
+    ids = arr(n, np.uint32)
+    list_begin = arr(nlist + 1, np.uint64)
+    byte_begin = arr(nlist + 1, np.uint64)
+    codes = arr(int(byte_begin[-1]), np.uint8)
+    coded = [(sum(p[0] for p in plan[:i]), p[0], p[1]) for i, p in enumerate(plan) if p[1] > 0]
+    nseg = len(coded)
+    stride = nseg * 8 + sum(ln // 8 * b for _, ln, b in coded)
+    digits = np.zeros((n, pd), np.uint16)
+    branch = np.zeros((n, pd // 8), np.uint8)
+    coef = np.zeros((n, nseg), np.float32)
+    h2 = np.zeros((n, nseg), np.float32)
+    for c in range(nlist):
+        for r in range(int(list_begin[c + 1] - list_begin[c])):
+            pos = int(list_begin[c]) + r
+            row = codes[int(byte_begin[c]) + r * stride:int(byte_begin[c]) + (r + 1) * stride]
+            fac = row[:nseg * 8].view(np.float32)
+            coef[pos] = fac[0::2]
+            h2[pos] = fac[1::2]
+            cur = nseg * 8
+            for doff, ln, b in coded:
+                for blk in range(ln // 8):
+                    x = int.from_bytes(row[cur:cur + b].tobytes(), "little")
+                    cur += b
+                    par = 0
+                    for i in range(7):
+                        f = (x >> (b * i)) & ((1 << b) - 1)
+                        digits[pos, doff + blk * 8 + i] = f
+                        par ^= f & 1
+                    f7 = (x >> (b * 7)) & ((1 << (b - 1)) - 1)
+                    digits[pos, doff + blk * 8 + 7] = (f7 << 1) | par
+                    branch[pos, doff // 8 + blk] = (x >> (8 * b - 1)) & 1
+    return {"n": n, "dim": dim, "pd": pd, "nlist": nlist, "plan": plan, "centroids": centroids, "ids": ids,
+            "list_begin": list_begin, "digits": digits, "branch": branch, "coef": coef, "h2": h2}

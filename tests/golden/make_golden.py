@@ -39,6 +39,13 @@ INDEX_CASES = [
     ("d960_b6", 960, 6, 300, 4, 14, 0.4, 8, 10, 2),
     ("d64_b2_k128", 64, 2, 700, 5, 15, 0.5, 6, 128, 5),
 ]
+# ME8Q: (name, dim, avg_bits, seed, plan_spec, n, nlist, sigma, nq, k, nprobe)
+ME8Q_CASES = [
+    ("me8q_d200_spec", 200, 4.0, 0, "64:6,64:4,64:3,64:0", 1500, 12, 0.5, 10, 10, 5),
+    ("me8q_d200_a4", 200, 4.0, 7, "", 1500, 12, 0.5, 10, 10, 5),
+    ("me8q_d150_a3", 150, 3.0, 0, "", 1200, 10, 0.5, 8, 16, 4),
+    ("me8q_d96_a6", 96, 6.0, 11, "", 900, 8, 0.5, 8, 10, 3),
+]
 
 
 def main() -> None:
@@ -126,6 +133,27 @@ def main() -> None:
             h3=P["h3"], rowa=P["rowa"], refine=P["refine"], signs=P["signs"],
             search_ids=ids, search_dists=dists, est_ids=est_ids, est=est,
             memory_bytes=np.int64(idx.memory_bytes))
+    # ---- ME8Q indexes (single-threaded reference build: its 4-thread build
+    # differed on one block of one row in a probe, so the pinned fixtures come
+    # from one thread; prune_alpha 1e-9 makes its search the plain scan) -------
+    for name, dim, avg, seed, spec, n, nlist, sigma, nq, k, nprobe in ME8Q_CASES:
+        x, cm, lab = det_mixture(seed + 5000 + dim, n, dim, nlist, sigma)
+        q = det_mixture(seed + 6000 + dim, nq, dim, nlist, sigma)[0]
+        idx = E.Me8qIndex(dim, avg, seed)
+        idx.build(x, cm, lab, num_threads=1, plan_spec=spec, prune_alpha=1e-9)
+        with tempfile.TemporaryDirectory() as d:
+            pth = os.path.join(d, "i.me8q")
+            idx.save(pth)
+            P = O.parse_me8q(pth)
+        ids, dists = idx.search(q, k, nprobe, 1)
+        est_ids = np.arange(0, n, max(1, n // 25), dtype=np.uint32)
+        est = np.array([[idx.estimate(q[i], int(g)) for g in est_ids] for i in range(nq)], np.float32)
+        np.savez_compressed(
+            os.path.join(HERE, f"{name}.npz"),
+            params=np.array([dim, seed, n, nlist, nq, k, nprobe], np.int64), avg_bits=np.float64(avg),
+            sigma=np.float64(sigma), plan_spec=np.array(spec), plan=np.array(P["plan"], np.int64),
+            ids=P["ids"], list_begin=P["list_begin"], digits=P["digits"], branch=P["branch"], coef=P["coef"],
+            h2=P["h2"], search_ids=ids, search_dists=dists, est_ids=est_ids, est=est)
     print("golden fixtures written to", HERE)
 
 
