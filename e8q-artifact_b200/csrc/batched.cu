@@ -22,6 +22,7 @@
 
 #include "device_common.cuh"
 #include "internal.h"
+#include "me8q.h"
 #include "workspace.h"
 
 namespace e8qc {
@@ -485,6 +486,197 @@ __global__ void __launch_bounds__(kBT) batched_scan_kernel(
     }
 }
 
+// ME8Q: half of a 64-dim chunk (4 blocks, 32 dims) of one vector at rate B,
+// decoded to levels scaled by the vector's coef for the chunk's run.
+template <int B>
+__device__ __forceinline__ void me8q_decode_half(const DevIndex& ix, uint32_t gt, int vl, bool live, int w0,
+                                                 const float* __restrict__ lev, float cf, float* Lb, int kk0,
+                                                 int v) {
+    uint32_t w[B + 1];
+#pragma unroll
+    for (int j = 0; j < B; ++j) w[j] = live ? code_word(ix, gt, vl, w0 + j) : 0u;
+    w[B] = 0u;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        uint32_t par = 0, dg[8];
+        const int base = b * 8 * B;
+#pragma unroll
+        for (int i = 0; i < 7; ++i) {
+            dg[i] = field(w, base + i * B, B);
+            par ^= dg[i];
+        }
+        const uint32_t f7 = field(w, base + 7 * B, B);
+        dg[7] = (f7 & ~1u) | (par & 1u);
+        const float* t = lev + ((f7 & 1u) ? (1 << B) : 0);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) Lb[(kk0 + b * 8 + i) * kVT + v] = live ? __fmul_rn(cf, __ldg(t + dg[i])) : 0.0f;
+    }
+}
+
+// ME8Q persistent scan: the batched kernel's structure with one rate per
+// 64-dim chunk (a run never splits a chunk). With the coef of each segment
+// folded into its decoded levels, sum_s coef_s S_s is one contraction q . L',
+// and the estimator d2 + sum_s (h2_s - 2 coef_s S_s) (src/index/
+// me8q_search.cpp:74-95) becomes d2 + hsum - 2 q . L'.
+__global__ void __launch_bounds__(kBT) me8q_scan_kernel(
+    Me8qView mv, const float* __restrict__ rq, const uint4* __restrict__ items, const uint32_t* __restrict__ n_items,
+    uint32_t* __restrict__ head, const uint32_t* __restrict__ pair_q, const float* __restrict__ pair_d2,
+    const uint32_t* __restrict__ k_arr, int k_uniform, int k_max, float* __restrict__ part_d,
+    uint32_t* __restrict__ part_id, unsigned long long* __restrict__ cand_count) {
+    extern __shared__ __align__(16) float bsm[];
+    const DevIndex& ix = mv.base;
+    float* Qs = bsm;                 // 2 * kKC * kQT
+    float* Ls = Qs + 2 * kKC * kQT;  // 2 * kKC * kVT
+    float* tk_d = Ls + 2 * kKC * kVT;
+    uint32_t* tk_i = reinterpret_cast<uint32_t*>(tk_d + kQT * k_max);
+    __shared__ uint4 s_item;
+    __shared__ uint32_t s_q[kQT];
+    __shared__ float s_d2[kQT];
+    __shared__ int s_k[kQT];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int pd = ix.pd;
+    const int nK = mv.nchunks;
+    const int tq = tid >> 4, tv = tid & 15;
+    const uint32_t NI = *n_items;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) {
+            const uint32_t it = atomicAdd(head, 1u);
+            s_item = it < NI ? items[it] : make_uint4(0xFFFFFFFFu, 0, 0, 0);
+        }
+        __syncthreads();
+        const uint4 item = s_item;
+        if (item.x == 0xFFFFFFFFu) break;
+        const uint32_t L = item.x, pbase = item.y;
+        const int m = static_cast<int>(item.z);
+        if (tid < kQT) {
+            const bool ok = tid < m;
+            const uint32_t qq = ok ? pair_q[pbase + tid] : 0u;
+            s_q[tid] = qq;
+            s_d2[tid] = ok ? pair_d2[pbase + tid] : 0.0f;
+            s_k[tid] = ok ? (k_arr ? static_cast<int>(k_arr[qq]) : k_uniform) : 0;
+        }
+        for (int e = tid; e < kQT * k_max; e += kBT) {
+            tk_d[e] = inf_f();
+            tk_i[e] = 0xFFFFFFFFu;
+        }
+        __syncthreads();
+        const uint32_t len = ix.list_len[L];
+        const uint32_t tile0 = ix.tile_begin[L];
+        if (tid == 0) {
+            atomicAdd(cand_count, static_cast<unsigned long long>(len) * m);
+            atomicAdd(cand_count + 1, static_cast<unsigned long long>(len));
+        }
+        for (uint32_t v0 = 0; v0 < len; v0 += kVT) {
+            float acc[4][8];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+            for (int kc = 0; kc < nK; ++kc) {
+                float* Qb = Qs + (kc & 1) * kKC * kQT;
+                float* Lb = Ls + (kc & 1) * kKC * kVT;
+                {
+                    const int q = tid & 63, part = tid >> 6;
+                    const float* src = rq + static_cast<size_t>(s_q[q]) * pd + kc * kKC + part * 16;
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        const float4 val = q < m ? *reinterpret_cast<const float4*>(src + 4 * r)
+                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+                        const int kk = part * 16 + 4 * r;
+                        Qb[(kk + 0) * kQT + q] = val.x;
+                        Qb[(kk + 1) * kQT + q] = val.y;
+                        Qb[(kk + 2) * kQT + q] = val.z;
+                        Qb[(kk + 3) * kQT + q] = val.w;
+                    }
+                }
+                {
+                    const Me8qChunk ch = mv.chunks[kc];
+                    const int v = tid & 127, h = tid >> 7;
+                    const uint32_t vi = v0 + v;
+                    const bool live = vi < len;
+                    const uint32_t gt = tile0 + (vi >> 5);
+                    const int vl = static_cast<int>(vi & 31);
+                    const size_t slot = static_cast<size_t>(gt) * 32 + vl;
+                    const float cf = live && ch.coded >= 0
+                                         ? __ldg(mv.coef + static_cast<size_t>(ch.coded) * mv.nslots + slot)
+                                         : 0.0f;
+                    const int w0 = ch.word0 + h * ch.bits;  // 4 blocks = bits words
+                    const float* lev = mv.levels + ch.lev;
+                    switch (ch.bits) {
+#define E8QC_DEC(B) \
+    case B: me8q_decode_half<B>(ix, gt, vl, live, w0, lev, cf, Lb, h * 32, v); break;
+                        E8QC_DEC(1) E8QC_DEC(2) E8QC_DEC(3) E8QC_DEC(4) E8QC_DEC(5) E8QC_DEC(6) E8QC_DEC(7)
+                        E8QC_DEC(8) E8QC_DEC(9) E8QC_DEC(10) E8QC_DEC(11) E8QC_DEC(12) E8QC_DEC(13)
+#undef E8QC_DEC
+                        default:  // a dropped run inside the coded prefix contributes nothing
+                            for (int i = 0; i < 32; ++i) Lb[(h * 32 + i) * kVT + v] = 0.0f;
+                            break;
+                    }
+                }
+                __syncthreads();
+#pragma unroll 4
+                for (int kk = 0; kk < kKC; ++kk) {
+                    const float4 a = *reinterpret_cast<const float4*>(Qb + kk * kQT + tq * 4);
+                    const float4 b0 = *reinterpret_cast<const float4*>(Lb + kk * kVT + tv * 4);
+                    const float4 b1 = *reinterpret_cast<const float4*>(Lb + kk * kVT + 64 + tv * 4);
+                    const float av[4] = {a.x, a.y, a.z, a.w};
+                    const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) acc[i][j] = __fmaf_rn(av[i], bv[j], acc[i][j]);
+                }
+            }
+            __syncthreads();
+            float* D = Ls;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int vv = j < 4 ? tv * 4 + j : 64 + tv * 4 + (j - 4);
+                const uint32_t vi = v0 + vv;
+                const bool live = vi < len;
+                const size_t slot = static_cast<size_t>(tile0 + (vi >> 5)) * 32 + (vi & 31);
+                const float hs = live ? __ldg(mv.hsum + slot) : 0.0f;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int q = tq * 4 + i;
+                    D[q * kVT + vv] = live ? __fmaf_rn(-2.0f, acc[i][j], __fadd_rn(s_d2[q], hs)) : inf_f();
+                }
+            }
+            __syncthreads();
+            for (int q = warp; q < m; q += kBT / 32) {
+                const int kq = s_k[q];
+                WarpTopK top;
+                top.init(kq);
+#pragma unroll
+                for (int s2 = 0; s2 < 4; ++s2) {
+                    const int j = s2 * 32 + lane;
+                    if (j < kq) {
+                        top.d[s2] = tk_d[q * k_max + j];
+                        top.id[s2] = tk_i[q * k_max + j];
+                    }
+                }
+                top.refresh_threshold();
+                for (int c = 0; c < kVT; c += 32) {
+                    const uint32_t vi = v0 + c + lane;
+                    const bool live = vi < len;
+                    const float dist = D[q * kVT + c + lane];
+                    const size_t slot = static_cast<size_t>(tile0 + (vi >> 5)) * 32 + (vi & 31);
+                    top.offer(dist, live, [&] { return __ldg(ix.ids + slot); });
+                }
+                top.store(tk_d + q * k_max, tk_i + q * k_max, kq);
+            }
+            __syncthreads();
+        }
+        for (int e = tid; e < m * k_max; e += kBT) {
+            const int q = e / k_max, j = e - q * k_max;
+            const size_t o = static_cast<size_t>(pbase + q) * k_max + j;
+            part_d[o] = tk_d[e];
+            part_id[o] = tk_i[e];
+        }
+    }
+}
+
 // Per-query merge of its nprobe partial lists into the final top-k row.
 __global__ void merge_kernel(const float* __restrict__ part_d, const uint32_t* __restrict__ part_id,
                              const uint32_t* __restrict__ pos_of, int nq, const uint32_t* __restrict__ np_arr,
@@ -653,6 +845,42 @@ int batched_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq
     ++launches;
     E8QC_CUDA(cudaGetLastError());
     return launches;
+}
+
+int me8q_grouped_search(const Me8qView& v, Workspace& ws, const float* rq, size_t nq, const uint32_t* k_arr,
+                        const uint32_t* np_arr, size_t k, size_t nprobe, size_t out_stride, uint32_t* out_ids,
+                        float* out_d, cudaStream_t s) {
+    if (nq == 0) return 0;
+    const int k_max = static_cast<int>(k);
+    const int np_max = static_cast<int>(nprobe);
+    int launches = batched_prepare(v.base, ws, rq, nq, np_arr, nprobe, k, kQT, 1, s);
+    int dev = 0;
+    E8QC_CUDA(cudaGetDevice(&dev));
+    const size_t smem = (static_cast<size_t>(2) * kKC * kQT + 2 * kKC * kVT + 2 * kQT * k_max) * 4;
+    static size_t configured[64] = {};
+    if (configured[dev & 63] < smem) {
+        E8QC_CUDA(cudaFuncSetAttribute(me8q_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       static_cast<int>(smem)));
+        configured[dev & 63] = smem;
+    }
+    int sms = 148, per_sm = 1;
+    E8QC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    E8QC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, me8q_scan_kernel, kBT, smem));
+    per_sm = std::max(1, per_sm);
+    uint32_t* nitems = ws.b_nitems.as<uint32_t>();
+    ws.mark_scan(false, s);
+    me8q_scan_kernel<<<sms * per_sm, kBT, smem, s>>>(
+        v, rq, ws.b_items.as<uint4>(), nitems, nitems + 1, ws.b_pair_q.as<uint32_t>(), ws.b_pair_d2.as<float>(), k_arr,
+        k_max, k_max, ws.b_part_d.as<float>(), ws.b_part_id.as<uint32_t>(),
+        reinterpret_cast<unsigned long long*>(nitems + 2));
+    E8QC_CUDA(cudaGetLastError());
+    ws.mark_scan(true, s);
+    ++launches;
+    merge_kernel<<<static_cast<unsigned>((nq + 3) / 4), 128, 0, s>>>(
+        ws.b_part_d.as<float>(), ws.b_part_id.as<uint32_t>(), ws.b_pos.as<uint32_t>(), static_cast<int>(nq), np_arr,
+        np_max, np_max, k_arr, k_max, k_max, static_cast<int>(out_stride), out_ids, out_d);
+    E8QC_CUDA(cudaGetLastError());
+    return launches + 1;
 }
 
 }  // namespace e8qc

@@ -429,6 +429,158 @@ class Server {
     std::unordered_map<uint64_t, std::pair<size_t, size_t>> shapes_;
 };
 
+// Me8qIndex (python_bindings/me8q_bindings.cpp:22-269 of the reference): same
+// constructor, build / search / estimate arguments, properties and errors;
+// `device` is this library's addition. save / load are not part of the
+// device path.
+class Me8qIndex {
+   public:
+    Me8qIndex(size_t dim, float avg_bits, uint64_t seed, int device)
+        : dim_(dim), avg_bits_(avg_bits), seed_(seed), device_(device) {
+        if (dim == 0) throw std::invalid_argument("dim must be positive");
+        if (!(avg_bits > 0.0F)) throw std::invalid_argument("avg_bits must be positive");
+    }
+    ~Me8qIndex() {
+        if (idx_) e8qc_me8q_destroy(idx_);
+    }
+    Me8qIndex(const Me8qIndex&) = delete;
+    Me8qIndex& operator=(const Me8qIndex&) = delete;
+
+    void build(py::handle data, py::handle centroids, py::handle cluster_ids, size_t /*num_threads*/,
+               py::handle variance, bool drop_energy, float prune_alpha, const std::string& plan_spec,
+               double extra_budget_bits) {
+        auto x = ensure_nd<float>(data, "data", 2);
+        auto c = ensure_nd<float>(centroids, "centroids", 2);
+        auto ids = ensure_nd<uint32_t>(cluster_ids, "cluster_ids", 1);
+        if (static_cast<size_t>(x.shape(1)) != dim_)
+            throw std::invalid_argument("data dimension does not match index dim");
+        if (static_cast<size_t>(c.shape(1)) != dim_)
+            throw std::invalid_argument("centroid dimension does not match index dim");
+        if (ids.shape(0) != x.shape(0))
+            throw std::invalid_argument("cluster_ids length must match number of rows in data");
+        py::array_t<float, py::array::c_style | py::array::forcecast> var;
+        e8qc_me8q_build_opts o{};
+        if (!variance.is_none()) {
+            var = ensure_nd<float>(variance, "variance", 1);
+            if (static_cast<size_t>(var.shape(0)) != dim_)
+                throw std::invalid_argument("variance length must match dim");
+            o.variance = var.data();
+        }
+        o.plan_spec = plan_spec.c_str();
+        o.drop_energy = drop_energy ? 1 : 0;
+        o.prune_alpha = prune_alpha;
+        o.extra_budget_bits = extra_budget_bits;
+        if (idx_) e8qc_me8q_destroy(idx_);
+        idx_ = nullptr;
+        built_ = false;
+        check(e8qc_me8q_create(device_, dim_, avg_bits_, seed_, &idx_));
+        {
+            py::gil_scoped_release nogil;
+            check(e8qc_me8q_build(idx_, x.data(), static_cast<size_t>(x.shape(0)), c.data(),
+                                  static_cast<size_t>(c.shape(0)), ids.data(), &o, nullptr));
+        }
+        built_ = true;
+    }
+
+    py::tuple search(py::handle queries, size_t k, size_t nprobe, size_t /*num_threads*/, bool return_stats) {
+        auto q = ensure_nd<float>(queries, "queries", 2);
+        require("search");
+        if (static_cast<size_t>(q.shape(1)) != dim_)
+            throw std::invalid_argument("query dimension does not match index dim");
+        if (k == 0) throw std::invalid_argument("k must be positive");
+        if (k > E8QC_MAX_K) throw std::invalid_argument("k must be <= " + std::to_string(E8QC_MAX_K));
+        if (nprobe == 0) throw std::invalid_argument("nprobe must be positive");
+        const size_t nq = static_cast<size_t>(q.shape(0));
+        py::array_t<uint32_t> ids({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k)});
+        py::array_t<float> dists({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k)});
+        uint32_t* ip = ids.mutable_data();
+        float* dp = dists.mutable_data();
+        std::fill(ip, ip + nq * k, std::numeric_limits<uint32_t>::max());
+        std::fill(dp, dp + nq * k, std::numeric_limits<float>::infinity());
+        e8qc_stats st{};
+        {
+            py::gil_scoped_release nogil;
+            if (nq > 0) check(e8qc_me8q_search(idx_, q.data(), nq, k, nprobe, ip, dp, return_stats ? &st : nullptr,
+                                               nullptr));
+        }
+        if (!return_stats) return py::make_tuple(ids, dists);
+        py::dict d;
+        const double dn = nq > 0 ? static_cast<double>(nq) : 1.0;
+        d["candidates"] = st.candidates;
+        d["survivors"] = st.survivors;
+        d["route_us"] = st.route_us / dn;
+        d["scan_us"] = st.scan_us / dn;
+        d["survivor_rate"] = st.candidates > 0 ? static_cast<double>(st.survivors) / st.candidates : 0.0;
+        d["launches"] = st.launches;
+        return py::make_tuple(ids, dists, d);
+    }
+
+    float estimate(py::handle query, uint32_t id) {
+        require("estimate");
+        auto q = ensure_nd<float>(query, "query", 1);
+        if (static_cast<size_t>(q.shape(0)) != dim_)
+            throw std::invalid_argument("query dimension does not match index dim");
+        float out = 0.0f;
+        const int rc = e8qc_me8q_estimate(idx_, q.data(), id, &out);
+        if (rc == E8QC_ERANGE) throw py::index_error(e8qc_last_error());
+        check(rc);
+        return out;
+    }
+
+    // (ids, digits n x pd, branch n x pd/8, coef n x ncoded, h2 n x ncoded),
+    // cluster-major.
+    py::tuple export_codes() {
+        require("export_codes");
+        const e8qc_me8q_meta in = info();
+        const auto n = static_cast<py::ssize_t>(in.n), pd = static_cast<py::ssize_t>(in.padded_dim),
+                   nc = static_cast<py::ssize_t>(in.ncoded);
+        py::array_t<uint32_t> ids(n);
+        py::array_t<uint16_t> dg({n, pd});
+        py::array_t<uint8_t> br({n, pd / 8});
+        py::array_t<float> cf({n, nc}), h2({n, nc});
+        check(e8qc_me8q_get_ids(idx_, ids.mutable_data()));
+        check(e8qc_me8q_export_codes(idx_, dg.mutable_data(), br.mutable_data(), cf.mutable_data(), h2.mutable_data()));
+        return py::make_tuple(ids, dg, br, cf, h2);
+    }
+
+    size_t dim() const { return dim_; }
+    float avg_bits() const { return avg_bits_; }
+    bool is_built() const { return built_; }
+    size_t n() const { return idx_ ? info().n : 0; }
+    size_t num_clusters() const { return idx_ ? info().nlist : 0; }
+    double bits_per_dim() const { return idx_ ? info().bits_per_dim : 0.0; }
+    size_t memory_bytes() const { return idx_ ? info().memory_bytes : 0; }
+    int device() const { return device_; }
+    std::vector<std::pair<size_t, int>> plan() const {
+        std::vector<std::pair<size_t, int>> out;
+        if (!idx_) return out;
+        size_t cnt = 0;
+        check(e8qc_me8q_plan(idx_, nullptr, nullptr, 0, &cnt));
+        std::vector<size_t> lens(cnt);
+        std::vector<int> bits(cnt);
+        check(e8qc_me8q_plan(idx_, lens.data(), bits.data(), cnt, &cnt));
+        for (size_t i = 0; i < cnt; ++i) out.emplace_back(lens[i], bits[i]);
+        return out;
+    }
+
+   private:
+    void require(const char* what) const {
+        if (!built_ || idx_ == nullptr)
+            throw std::runtime_error(std::string("Me8qIndex must be built or loaded before ") + what);
+    }
+    e8qc_me8q_meta info() const {
+        e8qc_me8q_meta in{};
+        check(e8qc_me8q_info(idx_, &in));
+        return in;
+    }
+    size_t dim_ = 0;
+    float avg_bits_ = 4.0F;
+    uint64_t seed_ = 0;
+    int device_ = 0;
+    bool built_ = false;
+    e8qc_me8q* idx_ = nullptr;
+};
+
 }  // namespace e8qb200
 
 PYBIND11_MODULE(_e8qlib, m) {
@@ -498,6 +650,26 @@ PYBIND11_MODULE(_e8qlib, m) {
         .def("stop", &e8qb200::Server::stop)
         .def("__enter__", [](py::object self) { return self; })
         .def("__exit__", [](e8qb200::Server& s, py::args) { s.stop(); });
+
+    py::class_<e8qb200::Me8qIndex>(m, "Me8qIndex")
+        .def(py::init<size_t, float, uint64_t, int>(), py::arg("dim"), py::arg("avg_bits") = 4.0F,
+             py::arg("seed") = 0, py::arg("device") = 0)
+        .def("build", &e8qb200::Me8qIndex::build, py::arg("data"), py::arg("centroids"), py::arg("cluster_ids"),
+             py::arg("num_threads") = 1, py::arg("variance") = py::none(), py::arg("drop_energy") = true,
+             py::arg("prune_alpha") = 0.0F, py::arg("plan_spec") = "", py::arg("extra_budget_bits") = 0.0)
+        .def("search", &e8qb200::Me8qIndex::search, py::arg("queries"), py::arg("k"), py::arg("nprobe"),
+             py::arg("num_threads") = 1, py::arg("return_stats") = false)
+        .def("estimate", &e8qb200::Me8qIndex::estimate, py::arg("query"), py::arg("id"))
+        .def("export_codes", &e8qb200::Me8qIndex::export_codes)
+        .def_property_readonly("dim", &e8qb200::Me8qIndex::dim)
+        .def_property_readonly("avg_bits", &e8qb200::Me8qIndex::avg_bits)
+        .def_property_readonly("is_built", &e8qb200::Me8qIndex::is_built)
+        .def_property_readonly("n", &e8qb200::Me8qIndex::n)
+        .def_property_readonly("num_clusters", &e8qb200::Me8qIndex::num_clusters)
+        .def_property_readonly("bits_per_dim", &e8qb200::Me8qIndex::bits_per_dim)
+        .def_property_readonly("memory_bytes", &e8qb200::Me8qIndex::memory_bytes)
+        .def_property_readonly("plan", &e8qb200::Me8qIndex::plan)
+        .def_property_readonly("device", &e8qb200::Me8qIndex::device);
 
     py::class_<E8qIndex>(m, "E8qIndex")
         .def(py::init<size_t, size_t, uint64_t, int>(), py::arg("dim"), py::arg("nbits"),

@@ -356,6 +356,42 @@ __global__ void encode_kernel(DevEncTables et, const float* __restrict__ unit, s
     branch[e] = static_cast<uint8_t>(br);
 }
 
+// ME8Q segment encoder (SegmentCodec::EncodeInto, src/quantization/
+// me8q_codec.cpp:69-97): one thread per (row, block) of one coded run. The
+// run's rotated residual rr and its fp64 norm^2 give unit = float(rr * (1 /
+// sqrt(norm^2))); the block is then encoded like an E8Q block of a len-dim
+// vector (scale * sqrt(len)). A zero-norm run stays the all-zero codeword.
+__global__ void me8q_encode_kernel(DevEncTables et, const float* __restrict__ rr, int pd,
+                                   const double* __restrict__ norm2, int ncoded, int run, int off, int len,
+                                   size_t n, double srd, uint16_t* __restrict__ digits,
+                                   uint8_t* __restrict__ branch) {
+    const int nb = len / 8;
+    const size_t e = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= n * static_cast<size_t>(nb)) return;
+    const size_t r = e / nb;
+    const int blk = static_cast<int>(e - r * nb);
+    uint16_t* dg = digits + r * pd + off + blk * 8;
+    const double n2 = norm2[r * ncoded + run];
+    if (!(n2 > 0.0)) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) dg[i] = 0;
+        branch[r * (pd / 8) + off / 8 + blk] = 0;
+        return;
+    }
+    const double inv = 1.0 / sqrt(n2);
+    double v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float u = static_cast<float>(static_cast<double>(rr[r * pd + off + blk * 8 + i]) * inv);
+        v[i] = static_cast<double>(u) * srd;
+    }
+    uint16_t out[8];
+    const int br = encode_block(v, et, out);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) dg[i] = out[i];
+    branch[r * (pd / 8) + off / 8 + blk] = static_cast<uint8_t>(br);
+}
+
 // Export: decode every padded slot back to digits/branch, cluster-major
 // compact order (positions of padding lanes are skipped).
 __global__ void decode_kernel(DevIndex ix, int ntiles, const uint32_t* __restrict__ list_of_tile,
@@ -446,6 +482,16 @@ int launch_encode(const DevEncTables& et, const float* unit, size_t n, int pd, d
     if (total == 0) return 0;
     encode_kernel<<<static_cast<unsigned>((total + 127) / 128), 128, 0, s>>>(et, unit, n, pd, srd, digits,
                                                                               branch);
+    E8QC_CUDA(cudaGetLastError());
+    return 1;
+}
+
+int launch_me8q_encode(const DevEncTables& et, const float* rr, int pd, const double* norm2, int ncoded, int run,
+                       int off, int len, size_t n, double srd, uint16_t* digits, uint8_t* branch, cudaStream_t s) {
+    const size_t total = n * static_cast<size_t>(len / 8);
+    if (total == 0) return 0;
+    me8q_encode_kernel<<<static_cast<unsigned>((total + 127) / 128), 128, 0, s>>>(et, rr, pd, norm2, ncoded, run, off,
+                                                                                   len, n, srd, digits, branch);
     E8QC_CUDA(cudaGetLastError());
     return 1;
 }

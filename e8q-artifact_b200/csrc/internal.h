@@ -154,6 +154,12 @@ int launch_build_encode(const DevIndex& ix, const DevEncTables& et, const BuildE
                         uint4* codes, float* g1, float* h3, cudaStream_t s);
 int launch_encode(const DevEncTables& et, const float* unit, size_t n, int pd, double srd,
                   uint16_t* digits, uint8_t* branch, cudaStream_t s);
+// ME8Q: encode one coded run (offset off, len dims) of n rows whose rotated
+// residuals are rr (n x pd) with fp64 norms^2 norm2 (n x ncoded, column run);
+// srd = FixedScale(bits) * sqrt(len). Writes digits (n x pd) and branch
+// (n x pd/8) for the run's dims.
+int launch_me8q_encode(const DevEncTables& et, const float* rr, int pd, const double* norm2, int ncoded, int run,
+                       int off, int len, size_t n, double srd, uint16_t* digits, uint8_t* branch, cudaStream_t s);
 // Decode device codes back to digits/branch (export, tests).
 int launch_decode(const DevIndex& ix, int ntiles, const uint32_t* list_of_tile,
                   const uint64_t* list_begin, uint16_t* digits, uint8_t* branch, cudaStream_t s);

@@ -1,0 +1,673 @@
+// ME8Q (mixed-rate E8Q) index: host side of the C ABI (e8qc_me8q_*).
+//
+// Build (include/e8qlib/index/me8q.hpp:71-84, src/index/me8q_build.cpp:42-311):
+// per-dimension variance (given, or on the device), SAQ's DP plan over 64-dim
+// blocks (src/quantization/me8q_plan.cpp:47-167) or a manual "L:B,..." plan,
+// one FHT-Kac-4 rotator per coded run (seeds stepped by the golden ratio),
+// then on the device, per chunk of rows: residual to the list centroid,
+// per-run rotation and norms, the E8Q block encoder per run, (coef, h2) fits
+// and packing. Search: per-run query rotation, then the grouped exact scan of
+// batched.cu (me8q_grouped_search).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "e8qc.h"
+#include "internal.h"
+#include "me8q.h"
+#include "workspace.h"
+
+namespace e8qc {
+void set_last_error(const std::string& s);
+bool is_device_ptr(const void* p);
+std::vector<uint8_t> rotator_signs(size_t dim, uint64_t seed);
+}  // namespace e8qc
+
+using namespace e8qc;
+
+namespace {
+
+constexpr size_t kSegDim = 64;
+constexpr int kMaxBitsMe8q = 13;
+constexpr uint64_t kDefaultRotSeed = 0x5EED1234ULL;  // BuildOptions::rot_seed (me8q.hpp:38)
+constexpr uint64_t kGolden = 0x9E3779B97F4A7C15ULL;
+
+using Plan = std::vector<std::pair<size_t, int>>;
+
+// SAQ's DP: runs of whole 64-dim blocks at 1..max_bits bits (cost sum var /
+// 2^b), a trailing dropped run priced at its variance, budget counted in
+// units of 64 bits (b*j + 1 per run), at most nblocks/2 runs for avg_bits >=
+// 2, and SAQ's acceptance rule (a complete plan replaces the best only when
+// 1% cheaper).
+Plan allocate(const std::vector<float>& var, size_t pd, float avg_bits, int max_bits, double extra_bits) {
+    const size_t nb = pd / kSegDim;
+    const double budget = static_cast<double>(avg_bits) * static_cast<double>(pd) + extra_bits + 64.0;
+    const size_t units = (budget > 0.0 ? static_cast<size_t>(budget) : 0) / kSegDim;
+    const size_t max_segs = avg_bits < 2.0F ? nb : nb / 2;
+    std::vector<double> p1(nb + 1, 0.0);
+    for (size_t b = 0; b < nb; ++b) {
+        double s = 0.0;
+        for (size_t k = 0; k < kSegDim; ++k) s += static_cast<double>(var[b * kSegDim + k]);
+        p1[b + 1] = p1[b] + s;
+    }
+    const size_t si = nb + 1, st = units + 1;
+    std::vector<double> f((max_segs + 1) * si * st, DBL_MAX);
+    std::vector<uint32_t> pred(f.size(), 0);
+    auto at = [&](size_t ns, size_t i, size_t t) { return (ns * si + i) * st + t; };
+    f[at(0, 0, 0)] = 0.0;
+    double best = DBL_MAX;
+    size_t ans_ns = 0, ans_t = 0;
+    for (size_t ns = 0; ns <= max_segs; ++ns)
+        for (size_t i = 0; i <= nb; ++i)
+            for (size_t t = 0; t <= units; ++t) {
+                const double cur = f[at(ns, i, t)];
+                if (cur >= DBL_MAX) continue;
+                if (i == nb) {
+                    if (cur * 1.01 < best) {
+                        best = cur;
+                        ans_ns = ns;
+                        ans_t = t;
+                    }
+                    continue;
+                }
+                if (ns == max_segs) continue;
+                for (size_t j = 1; i + j <= nb; ++j) {
+                    const double vsum = p1[i + j] - p1[i];
+                    for (int b = 1; b <= max_bits; ++b) {
+                        const size_t t2 = t + static_cast<size_t>(b) * j + 1;
+                        if (t2 > units) break;
+                        const double v = cur + vsum / static_cast<double>(int64_t{1} << b);
+                        const size_t to = at(ns + 1, i + j, t2);
+                        if (v < f[to]) {
+                            f[to] = v;
+                            pred[to] = static_cast<uint32_t>((i << 4) | static_cast<size_t>(b));
+                        }
+                    }
+                }
+                const double rest = p1[nb] - p1[i];
+                const size_t to = at(ns + 1, nb, t);
+                if (cur + rest < f[to]) {
+                    f[to] = cur + rest;
+                    pred[to] = static_cast<uint32_t>(i << 4);
+                }
+            }
+    if (best >= DBL_MAX) return Plan{{pd, 0}};  // no feasible plan: everything dropped
+    Plan plan;
+    size_t ns = ans_ns, i = nb, t = ans_t;
+    while (i > 0) {
+        const uint32_t p = pred[at(ns, i, t)];
+        const size_t prev = p >> 4;
+        const int b = static_cast<int>(p & 0xFu);
+        plan.push_back({(i - prev) * kSegDim, b});
+        --ns;
+        if (b != 0) t -= static_cast<size_t>(b) * (i - prev) + 1;
+        i = prev;
+    }
+    std::reverse(plan.begin(), plan.end());
+    return plan;
+}
+
+// "L:B,L:B,..." (src/index/me8q_common.cpp:37-68): empty tokens skipped,
+// numbers read like atol, L a positive multiple of 64, B in [0, 13], the
+// runs covering the padded dimension exactly.
+Plan parse_plan(const std::string& spec, size_t pd) {
+    Plan plan;
+    size_t total = 0;
+    std::string tok;
+    auto take = [&] {
+        if (tok.empty()) return;
+        const size_t colon = tok.find(':');
+        if (colon == std::string::npos) fail(E8QC_EINVAL, "plan_spec: expected L:B, got " + tok);
+        const long len = std::strtol(tok.c_str(), nullptr, 10);
+        const long bits = std::strtol(tok.c_str() + colon + 1, nullptr, 10);
+        if (len <= 0 || len % static_cast<long>(kSegDim) != 0 || bits < 0 || bits > kMaxBitsMe8q)
+            fail(E8QC_EINVAL, "plan_spec: bad run " + tok);
+        plan.emplace_back(static_cast<size_t>(len), static_cast<int>(bits));
+        total += static_cast<size_t>(len);
+        tok.clear();
+    };
+    for (const char ch : spec) {
+        if (ch == ',') take();
+        else tok.push_back(ch);
+    }
+    take();
+    if (total != pd)
+        fail(E8QC_EINVAL, "plan_spec: runs cover " + std::to_string(total) + " of " + std::to_string(pd) +
+                              " padded dims");
+    return plan;
+}
+
+struct DeviceGuard {
+    int prev = 0;
+    explicit DeviceGuard(int d) {
+        E8QC_CUDA(cudaGetDevice(&prev));
+        E8QC_CUDA(cudaSetDevice(d));
+    }
+    ~DeviceGuard() { cudaSetDevice(prev); }
+};
+
+int guarded(const std::function<void()>& f) {
+    try {
+        f();
+        return E8QC_OK;
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("host allocation failed");
+        return E8QC_ENOMEM;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return E8QC_EINVAL;
+    }
+}
+
+}  // namespace
+
+struct e8qc_me8q {
+    int device = 0;
+    size_t dim = 0, pd = 0;
+    float avg_bits = 4.0F;
+    uint64_t seed = 0;
+    bool built = false;
+    size_t n = 0, nlist = 0, ntiles = 0, nslots = 0;
+    int nch = 0, ncoded = 0, route_dim = 0;
+    size_t bytes_per_vector = 0;
+    Plan plan;
+    std::vector<Me8qRun> runs;
+    std::vector<Me8qChunk> chunks;
+    std::vector<uint64_t> list_begin;
+    std::vector<uint32_t> tile_begin, ids_compact, inv_pos;
+    std::vector<float> cen_host;  // padded centroids (estimate)
+    DevBuf runs_d, chunks_d, levels, signs, cen_pad, cen_rot, cn2, tile_begin_d, list_len_d, list_order_d,
+        list_of_tile_d, ids, codes, coef, h2, hsum, list_begin_d;
+    Me8qView view{};
+    Workspace ws;
+    std::mutex mu;
+    size_t memory_bytes() const {
+        return runs_d.bytes + chunks_d.bytes + levels.bytes + signs.bytes + cen_pad.bytes + cen_rot.bytes + cn2.bytes +
+               tile_begin_d.bytes + list_len_d.bytes + list_order_d.bytes + list_of_tile_d.bytes + ids.bytes +
+               codes.bytes + coef.bytes + h2.bytes + hsum.bytes + list_begin_d.bytes;
+    }
+};
+
+namespace {
+
+void require_built(const e8qc_me8q* x, const char* what) {
+    if (x == nullptr) fail(E8QC_EINVAL, "null index");
+    if (!x->built) fail(E8QC_ESTATE, std::string("Me8qIndex must be built or loaded before ") + what);
+}
+
+// Plan -> run descriptors, rotator signs, chunk table and level tables.
+void layout_plan(e8qc_me8q* x, uint64_t rot_seed, cudaStream_t s) {
+    x->runs.clear();
+    x->chunks.clear();
+    std::vector<uint8_t> sg_all;
+    std::vector<float> lev_all;
+    int lev_off[kMaxBitsMe8q + 1];
+    std::fill(lev_off, lev_off + kMaxBitsMe8q + 1, -1);
+    uint64_t sd = rot_seed;
+    size_t off = 0, word = 0;
+    int coded = 0;
+    for (const auto& seg : x->plan) {
+        Me8qRun r{};
+        r.off = static_cast<int>(off);
+        r.len = static_cast<int>(seg.first);
+        r.bits = seg.second;
+        r.coded = seg.second != 0 ? coded : -1;
+        int td = 1;
+        while ((td << 1) <= r.len) td <<= 1;
+        r.td = td;
+        r.fac = 1.0f / std::sqrt(static_cast<float>(td));
+        r.soff = static_cast<int>(sg_all.size());
+        r.word0 = static_cast<int>(word);
+        if (seg.second != 0) {
+            sd += kGolden;  // BuildRunRotators (me8q_build.cpp:29-40)
+            const std::vector<uint8_t> sg = rotator_signs(seg.first, sd);
+            sg_all.insert(sg_all.end(), sg.begin(), sg.end());
+            if (lev_off[seg.second] < 0) {
+                lev_off[seg.second] = static_cast<int>(lev_all.size());
+                for (int br = 0; br < 2; ++br) {
+                    const std::vector<double> lv = branch_levels(seg.second, br);
+                    for (double d : lv) lev_all.push_back(static_cast<float>(d));
+                }
+            }
+            word += seg.first * static_cast<size_t>(seg.second) / 32;
+            ++coded;
+        }
+        x->runs.push_back(r);
+        off += seg.first;
+    }
+    x->ncoded = coded;
+    x->route_dim = static_cast<int>(x->pd);
+    for (auto it = x->plan.rbegin(); it != x->plan.rend() && it->second == 0; ++it)
+        x->route_dim -= static_cast<int>(it->first);
+    for (const auto& r : x->runs) {
+        if (r.off >= x->route_dim) break;
+        for (int c = 0; c < r.len / 64; ++c)
+            x->chunks.push_back(Me8qChunk{r.bits, r.coded, r.word0 + c * 2 * r.bits, r.bits ? lev_off[r.bits] : 0});
+    }
+    const size_t stream_bits = word * 32;
+    x->nch = static_cast<int>(std::max<size_t>(1, (stream_bits + 127) / 128));
+    x->bytes_per_vector = static_cast<size_t>(coded) * 8;
+    for (const auto& seg : x->plan)
+        if (seg.second) x->bytes_per_vector += seg.first / 8 * static_cast<size_t>(seg.second);
+    if (lev_all.empty()) lev_all.push_back(0.0f);
+    if (sg_all.empty()) sg_all.push_back(0);
+    x->runs_d.upload(x->runs.data(), x->runs.size() * sizeof(Me8qRun), s);
+    std::vector<Me8qChunk> chunk_tab = x->chunks;
+    if (chunk_tab.empty()) chunk_tab.push_back(Me8qChunk{0, -1, 0, 0});  // all runs dropped
+    x->chunks_d.upload(chunk_tab.data(), chunk_tab.size() * sizeof(Me8qChunk), s);
+    x->levels.upload(lev_all.data(), lev_all.size() * 4, s);
+    x->signs.upload(sg_all.data(), sg_all.size(), s);
+}
+
+void fill_view(e8qc_me8q* x) {
+    Me8qView& v = x->view;
+    v = Me8qView{};
+    DevIndex& b = v.base;
+    b.dim = static_cast<int>(x->dim);
+    b.pd = static_cast<int>(x->pd);
+    b.B = static_cast<int>(x->pd / 8);
+    b.bits = 0;
+    b.nlist = static_cast<int>(x->nlist);
+    b.nch = x->nch;
+    b.ntiles = static_cast<int>(x->ntiles);
+    b.cen = x->cen_rot.as<float>();
+    b.cn2 = x->cn2.as<float>();
+    b.tile_begin = x->tile_begin_d.as<uint32_t>();
+    b.list_len = x->list_len_d.as<uint32_t>();
+    b.codes = static_cast<const uint4*>(x->codes.p);
+    b.ids = x->ids.as<uint32_t>();
+    b.list_order = x->list_order_d.as<uint32_t>();
+    b.list_of_tile = x->list_of_tile_d.as<uint32_t>();
+    v.coef = x->coef.as<float>();
+    v.h2 = x->h2.as<float>();
+    v.hsum = x->hsum.as<float>();
+    v.runs = x->runs_d.as<Me8qRun>();
+    v.chunks = x->chunks_d.as<Me8qChunk>();
+    v.levels = x->levels.as<float>();
+    v.signs = x->signs.as<uint8_t>();
+    v.nruns = static_cast<int>(x->runs.size());
+    v.ncoded = x->ncoded;
+    v.nchunks = static_cast<int>(x->chunks.size());
+    v.route_dim = x->route_dim;
+    v.nslots = x->nslots;
+}
+
+void build(e8qc_me8q* x, const float* data, size_t n, const float* centroids, size_t nlist, const uint32_t* cluster_ids,
+           const e8qc_me8q_build_opts* o, cudaStream_t s) {
+    const size_t dim = x->dim, pd = x->pd;
+    DevBuf tdata;
+    const float* xd = data;
+    if (!is_device_ptr(data)) {
+        tdata.alloc(n * dim * 4);
+        E8QC_CUDA(cudaMemcpyAsync(tdata.p, data, n * dim * 4, cudaMemcpyHostToDevice, s));
+        xd = tdata.as<float>();
+    }
+    std::vector<float> cen(nlist * dim);
+    if (is_device_ptr(centroids)) E8QC_CUDA(cudaMemcpy(cen.data(), centroids, cen.size() * 4, cudaMemcpyDeviceToHost));
+    else std::memcpy(cen.data(), centroids, cen.size() * 4);
+    std::vector<uint32_t> cid(n);
+    if (is_device_ptr(cluster_ids)) E8QC_CUDA(cudaMemcpy(cid.data(), cluster_ids, n * 4, cudaMemcpyDeviceToHost));
+    else std::memcpy(cid.data(), cluster_ids, n * 4);
+    for (size_t i = 0; i < n; ++i)
+        if (cid[i] >= nlist) fail(E8QC_EINVAL, "cluster_ids out of range");
+    // ---- plan ----
+    const int max_bits = (o && o->max_bits > 0) ? o->max_bits : kMaxBitsMe8q;
+    if (max_bits < 1 || max_bits > kMaxBitsMe8q) fail(E8QC_EINVAL, "max_bits must be in [1, 13]");
+    if (o && o->plan_spec && o->plan_spec[0]) {
+        x->plan = parse_plan(o->plan_spec, pd);
+    } else {
+        std::vector<float> var(pd, 0.0f);
+        if (o && o->variance) {
+            if (is_device_ptr(o->variance)) E8QC_CUDA(cudaMemcpy(var.data(), o->variance, dim * 4, cudaMemcpyDeviceToHost));
+            else std::memcpy(var.data(), o->variance, dim * 4);
+        } else {
+            DevBuf vd;
+            vd.alloc(dim * 4);
+            launch_me8q_variance(xd, n, static_cast<int>(dim), vd.as<float>(), s);
+            E8QC_CUDA(cudaMemcpyAsync(var.data(), vd.p, dim * 4, cudaMemcpyDeviceToHost, s));
+            E8QC_CUDA(cudaStreamSynchronize(s));
+        }
+        x->plan = allocate(var, pd, x->avg_bits, max_bits, o ? o->extra_budget_bits : 0.0);
+    }
+    if (x->plan.size() > 256) fail(E8QC_EINVAL, "a plan may have at most 256 runs");
+    const uint64_t rot_seed = x->seed != 0 ? x->seed : kDefaultRotSeed;
+    layout_plan(x, rot_seed, s);
+    // ---- lists: tiles of 32 slots, rows in file order within a list ----
+    x->n = n;
+    x->nlist = nlist;
+    std::vector<uint32_t> cnt(nlist, 0);
+    for (size_t i = 0; i < n; ++i) ++cnt[cid[i]];
+    x->list_begin.assign(nlist + 1, 0);
+    x->tile_begin.assign(nlist + 1, 0);
+    for (size_t c = 0; c < nlist; ++c) {
+        x->list_begin[c + 1] = x->list_begin[c] + cnt[c];
+        x->tile_begin[c + 1] = x->tile_begin[c] + (cnt[c] + 31) / 32;
+    }
+    x->ntiles = x->tile_begin[nlist];
+    x->nslots = x->ntiles * 32;
+    std::vector<uint32_t> slot_of_row(n), slot_ids(std::max<size_t>(1, x->nslots), 0xFFFFFFFFu), fillc(nlist, 0);
+    x->ids_compact.assign(n, 0);
+    for (size_t i = 0; i < n; ++i) {
+        const uint32_t c = cid[i];
+        const uint32_t local = fillc[c]++;
+        slot_of_row[i] = x->tile_begin[c] * 32 + local;
+        slot_ids[slot_of_row[i]] = static_cast<uint32_t>(i);
+        x->ids_compact[x->list_begin[c] + local] = static_cast<uint32_t>(i);
+    }
+    x->inv_pos.clear();
+    std::vector<uint32_t> list_len(nlist), list_of_tile(std::max<size_t>(1, x->ntiles), 0), order(2 * nlist);
+    for (size_t c = 0; c < nlist; ++c) {
+        list_len[c] = cnt[c];
+        for (uint32_t t = x->tile_begin[c]; t < x->tile_begin[c + 1]; ++t) list_of_tile[t] = static_cast<uint32_t>(c);
+        order[c] = order[nlist + c] = static_cast<uint32_t>(c);
+    }
+    std::stable_sort(order.begin(), order.begin() + nlist, [&](uint32_t a, uint32_t b) { return cnt[a] > cnt[b]; });
+    x->tile_begin_d.upload(x->tile_begin.data(), x->tile_begin.size() * 4, s);
+    x->list_len_d.upload(list_len.data(), nlist * 4, s);
+    x->list_order_d.upload(order.data(), order.size() * 4, s);
+    x->list_of_tile_d.upload(list_of_tile.data(), list_of_tile.size() * 4, s);
+    x->ids.upload(slot_ids.data(), slot_ids.size() * 4, s);
+    x->list_begin_d.upload(x->list_begin.data(), x->list_begin.size() * 8, s);
+    // ---- centroids: padded, per-run rotated, ||.||^2 (ivf_common.hpp:43-54) ----
+    x->cen_host.assign(nlist * pd, 0.0f);
+    for (size_t c = 0; c < nlist; ++c) std::memcpy(&x->cen_host[c * pd], &cen[c * dim], dim * 4);
+    x->cen_pad.upload(x->cen_host.data(), x->cen_host.size() * 4, s);
+    x->cen_rot.alloc(nlist * pd * 4);
+    x->codes.alloc(std::max<size_t>(1, x->ntiles) * x->nch * 32 * 16);
+    E8QC_CUDA(cudaMemsetAsync(x->codes.p, 0, x->codes.bytes, s));
+    const size_t nc = std::max(1, x->ncoded);
+    x->coef.alloc(nc * std::max<size_t>(1, x->nslots) * 4);
+    x->h2.alloc(nc * std::max<size_t>(1, x->nslots) * 4);
+    x->hsum.alloc(std::max<size_t>(1, x->nslots) * 4);
+    E8QC_CUDA(cudaMemsetAsync(x->coef.p, 0, x->coef.bytes, s));
+    E8QC_CUDA(cudaMemsetAsync(x->h2.p, 0, x->h2.bytes, s));
+    x->cn2.alloc(nlist * 4);
+    fill_view(x);
+    launch_me8q_prep(x->cen_pad.as<float>(), pd, static_cast<int>(pd), static_cast<int>(pd), nullptr, nullptr, x->view,
+                     0, nlist, x->cen_rot.as<float>(), nullptr, nullptr, s);
+    {
+        std::vector<float> cr(nlist * pd), n2(nlist);
+        E8QC_CUDA(cudaMemcpyAsync(cr.data(), x->cen_rot.p, cr.size() * 4, cudaMemcpyDeviceToHost, s));
+        E8QC_CUDA(cudaStreamSynchronize(s));
+        for (size_t c = 0; c < nlist; ++c) {
+            double acc = 0.0;
+            for (size_t d = 0; d < pd; ++d) acc = std::fma(static_cast<double>(cr[c * pd + d]), static_cast<double>(cr[c * pd + d]), acc);
+            n2[c] = static_cast<float>(acc);
+        }
+        E8QC_CUDA(cudaMemcpyAsync(x->cn2.p, n2.data(), nlist * 4, cudaMemcpyHostToDevice, s));
+        E8QC_CUDA(cudaStreamSynchronize(s));
+    }
+    // ---- encode in chunks of rows ----
+    DevBuf cid_d, slot_d, rr, norm2, drop, dg, br;
+    cid_d.upload(cid.data(), n * 4, s);
+    slot_d.upload(slot_of_row.data(), n * 4, s);
+    const size_t chunk = std::min<size_t>(n, 1u << 18);
+    rr.alloc(chunk * pd * 4);
+    norm2.alloc(chunk * nc * 8);
+    drop.alloc(chunk * 8);
+    dg.alloc(chunk * pd * 2);
+    br.alloc(chunk * (pd / 8));
+    const int dev = x->device;
+    const bool drop_energy = o ? o->drop_energy != 0 : true;
+    for (size_t r0 = 0; r0 < n; r0 += chunk) {
+        const size_t m = std::min(chunk, n - r0);
+        launch_me8q_prep(xd, dim, static_cast<int>(dim), static_cast<int>(pd), x->cen_pad.as<float>(),
+                         cid_d.as<uint32_t>(), x->view, r0, m, rr.as<float>(), norm2.as<double>(), drop.as<double>(), s);
+        for (const auto& run : x->runs) {
+            if (run.bits == 0) continue;
+            const double srd = fixed_scale(run.bits) * std::sqrt(static_cast<double>(run.len));
+            launch_me8q_encode(enc_tables_device(dev, run.bits), rr.as<float>(), static_cast<int>(pd), norm2.as<double>(),
+                               x->ncoded, run.coded, run.off, run.len, m, srd, dg.as<uint16_t>(), br.as<uint8_t>(), s);
+        }
+        launch_me8q_fits_pack(x->view, rr.as<float>(), dg.as<uint16_t>(), br.as<uint8_t>(), norm2.as<double>(),
+                              drop.as<double>(), cid_d.as<uint32_t>(), x->cen_rot.as<float>(), static_cast<int>(pd), r0, m,
+                              slot_d.as<uint32_t>(), drop_energy, static_cast<uint4*>(x->codes.p), x->coef.as<float>(),
+                              x->h2.as<float>(), s);
+    }
+    launch_me8q_hsum(x->view, x->hsum.as<float>(), s);
+    E8QC_CUDA(cudaStreamSynchronize(s));
+    x->built = true;
+}
+
+}  // namespace
+
+extern "C" {
+
+int e8qc_me8q_allocate(const float* var_padded, size_t padded_dim, float avg_bits, int max_bits,
+                       double extra_budget_bits, size_t* lens, int* bits, size_t cap, size_t* count) {
+    return guarded([&] {
+        if (!var_padded || !count) fail(E8QC_EINVAL, "null argument");
+        if (padded_dim == 0 || padded_dim % kSegDim != 0) fail(E8QC_EINVAL, "padded_dim must be a multiple of 64");
+        if (!(avg_bits > 0.0F)) fail(E8QC_EINVAL, "avg_bits must be positive");
+        if (max_bits < 1 || max_bits > kMaxBitsMe8q) fail(E8QC_EINVAL, "max_bits must be in [1, 13]");
+        const std::vector<float> var(var_padded, var_padded + padded_dim);
+        const Plan plan = allocate(var, padded_dim, avg_bits, max_bits, extra_budget_bits);
+        *count = plan.size();
+        for (size_t i = 0; i < plan.size() && i < cap; ++i) {
+            if (lens) lens[i] = plan[i].first;
+            if (bits) bits[i] = plan[i].second;
+        }
+    });
+}
+
+int e8qc_me8q_parse_plan(const char* spec, size_t padded_dim, size_t* lens, int* bits, size_t cap, size_t* count) {
+    return guarded([&] {
+        if (!spec || !count) fail(E8QC_EINVAL, "null argument");
+        const Plan plan = parse_plan(spec, padded_dim);
+        *count = plan.size();
+        for (size_t i = 0; i < plan.size() && i < cap; ++i) {
+            if (lens) lens[i] = plan[i].first;
+            if (bits) bits[i] = plan[i].second;
+        }
+    });
+}
+
+int e8qc_me8q_create(int device, size_t dim, float avg_bits, uint64_t seed, e8qc_me8q** out) {
+    return guarded([&] {
+        if (!out) fail(E8QC_EINVAL, "null output");
+        if (dim == 0) fail(E8QC_EINVAL, "dim must be positive");
+        if (dim > 16384) fail(E8QC_EINVAL, "dim must be <= 16384");
+        if (!(avg_bits > 0.0F)) fail(E8QC_EINVAL, "avg_bits must be positive");
+        int ndev = 0;
+        E8QC_CUDA(cudaGetDeviceCount(&ndev));
+        if (device < 0 || device >= ndev) fail(E8QC_EINVAL, "no such CUDA device");
+        auto* x = new e8qc_me8q();
+        x->device = device;
+        x->dim = dim;
+        x->pd = (dim + kSegDim - 1) / kSegDim * kSegDim;
+        x->avg_bits = avg_bits;
+        x->seed = seed;
+        x->ws.device = device;
+        *out = x;
+    });
+}
+
+int e8qc_me8q_destroy(e8qc_me8q* x) {
+    return guarded([&] {
+        if (!x) return;
+        DeviceGuard g(x->device);
+        delete x;
+    });
+}
+
+int e8qc_me8q_build(e8qc_me8q* x, const float* data, size_t n, const float* centroids, size_t nlist,
+                    const uint32_t* cluster_ids, const e8qc_me8q_build_opts* opts, void* stream) {
+    return guarded([&] {
+        if (!x) fail(E8QC_EINVAL, "null index");
+        if (!data || !centroids || !cluster_ids || n == 0 || nlist == 0) fail(E8QC_EINVAL, "Me8qIndex::Build: empty input");
+        std::lock_guard<std::mutex> lock(x->mu);
+        DeviceGuard g(x->device);
+        x->built = false;
+        build(x, data, n, centroids, nlist, cluster_ids, opts, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int e8qc_me8q_search(e8qc_me8q* x, const float* queries, size_t nq, size_t k, size_t nprobe, uint32_t* out_ids,
+                     float* out_dists, e8qc_stats* stats, void* stream) {
+    return guarded([&] {
+        require_built(x, "search");
+        if (k == 0) fail(E8QC_EINVAL, "k must be positive");
+        if (k > static_cast<size_t>(kMaxK)) fail(E8QC_EINVAL, "k must be <= 128");
+        if (nprobe == 0) fail(E8QC_EINVAL, "nprobe must be positive");
+        if (nq == 0) return;
+        if (!queries || !out_ids) fail(E8QC_EINVAL, "null buffer");
+        std::lock_guard<std::mutex> lock(x->mu);
+        DeviceGuard g(x->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        const size_t np = std::min(nprobe, x->nlist);
+        Workspace& ws = x->ws;
+        const float* qd = queries;
+        if (!is_device_ptr(queries)) {
+            ws.stage_q.ensure(nq * x->dim * 4);
+            E8QC_CUDA(cudaMemcpyAsync(ws.stage_q.p, queries, nq * x->dim * 4, cudaMemcpyHostToDevice, s));
+            qd = ws.stage_q.as<float>();
+        }
+        const bool ids_dev = is_device_ptr(out_ids), d_dev = out_dists && is_device_ptr(out_dists);
+        uint32_t* ids_d = out_ids;
+        float* d_d = out_dists;
+        if (!ids_dev) {
+            ws.stage_ids.ensure(nq * k * 4);
+            ids_d = ws.stage_ids.as<uint32_t>();
+        }
+        if (!d_dev) {
+            ws.stage_d.ensure(nq * k * 4);
+            d_d = ws.stage_d.as<float>();
+        }
+        ws.ensure_queries(nq, x->pd);
+        ws.ensure_err();
+        launch_me8q_prep(qd, x->dim, static_cast<int>(x->dim), static_cast<int>(x->pd), nullptr, nullptr, x->view, 0, nq,
+                         ws.rq.as<float>(), nullptr, nullptr, s);
+        const int launches = 1 + me8q_grouped_search(x->view, ws, ws.rq.as<float>(), nq, nullptr, nullptr, k, np, k,
+                                                     ids_d, d_d, s);
+        if (!ids_dev) E8QC_CUDA(cudaMemcpyAsync(out_ids, ids_d, nq * k * 4, cudaMemcpyDeviceToHost, s));
+        if (out_dists && !d_dev) E8QC_CUDA(cudaMemcpyAsync(out_dists, d_d, nq * k * 4, cudaMemcpyDeviceToHost, s));
+        ws.check_error(s);
+        if (stats) {
+            std::memset(stats, 0, sizeof(*stats));
+            uint64_t cntv[2] = {0, 0};
+            E8QC_CUDA(cudaMemcpyAsync(cntv, ws.b_nitems.as<uint32_t>() + 2, 16, cudaMemcpyDeviceToHost, s));
+            E8QC_CUDA(cudaStreamSynchronize(s));
+            stats->candidates = cntv[0];
+            stats->survivors = cntv[0];
+            stats->launches = static_cast<uint64_t>(launches);
+        }
+    });
+}
+
+int e8qc_me8q_estimate(e8qc_me8q* x, const float* query, uint32_t id, float* out) {
+    return guarded([&] {
+        require_built(x, "estimate");
+        if (!query || !out) fail(E8QC_EINVAL, "null buffer");
+        std::lock_guard<std::mutex> lock(x->mu);
+        if (x->inv_pos.size() != x->n) {
+            x->inv_pos.assign(x->n, 0xFFFFFFFFu);
+            for (size_t i = 0; i < x->n; ++i) x->inv_pos[x->ids_compact[i]] = static_cast<uint32_t>(i);
+        }
+        if (id >= x->n || x->inv_pos[id] == 0xFFFFFFFFu) fail(E8QC_ERANGE, "Me8qIndex::Estimate: unknown id");
+        const uint64_t pos = x->inv_pos[id];
+        const size_t c = static_cast<size_t>(
+            std::upper_bound(x->list_begin.begin() + 1, x->list_begin.end(), pos) - x->list_begin.begin() - 1);
+        const uint32_t slot = x->tile_begin[c] * 32 + static_cast<uint32_t>(pos - x->list_begin[c]);
+        DeviceGuard g(x->device);
+        cudaStream_t s = nullptr;
+        std::vector<float> qpad(x->pd, 0.0f);
+        if (is_device_ptr(query)) E8QC_CUDA(cudaMemcpy(qpad.data(), query, x->dim * 4, cudaMemcpyDeviceToHost));
+        else std::memcpy(qpad.data(), query, x->dim * 4);
+        DevBuf qp, rq, o;
+        qp.upload(qpad.data(), x->pd * 4, s);
+        rq.alloc(x->pd * 4);
+        o.alloc(4);
+        launch_me8q_prep(qp.as<float>(), x->pd, static_cast<int>(x->pd), static_cast<int>(x->pd), nullptr, nullptr, x->view,
+                         0, 1, rq.as<float>(), nullptr, nullptr, s);
+        launch_me8q_estimate(x->view, rq.as<float>(), qp.as<float>(), x->cen_pad.as<float>(), static_cast<uint32_t>(c), slot,
+                             o.as<float>(), s);
+        E8QC_CUDA(cudaMemcpy(out, o.p, 4, cudaMemcpyDeviceToHost));
+    });
+}
+
+int e8qc_me8q_info(const e8qc_me8q* x, e8qc_me8q_meta* out) {
+    return guarded([&] {
+        if (!x || !out) fail(E8QC_EINVAL, "null argument");
+        e8qc_me8q_meta in{};
+        in.n = x->n;
+        in.dim = x->dim;
+        in.padded_dim = x->pd;
+        in.nlist = x->nlist;
+        in.nruns = x->plan.size();
+        in.ncoded = static_cast<size_t>(x->ncoded);
+        in.route_dim = static_cast<size_t>(x->route_dim);
+        in.bytes_per_vector = x->bytes_per_vector;
+        in.bits_per_dim = x->dim ? 8.0 * static_cast<double>(x->bytes_per_vector) / static_cast<double>(x->dim) : 0.0;
+        in.memory_bytes = x->memory_bytes();
+        in.avg_bits = x->avg_bits;
+        in.is_built = x->built ? 1 : 0;
+        *out = in;
+    });
+}
+
+int e8qc_me8q_plan(const e8qc_me8q* x, size_t* lens, int* bits, size_t cap, size_t* count) {
+    return guarded([&] {
+        if (!x || !count) fail(E8QC_EINVAL, "null argument");
+        *count = x->plan.size();
+        for (size_t i = 0; i < x->plan.size() && i < cap; ++i) {
+            if (lens) lens[i] = x->plan[i].first;
+            if (bits) bits[i] = x->plan[i].second;
+        }
+    });
+}
+
+int e8qc_me8q_get_ids(const e8qc_me8q* x, uint32_t* out) {
+    return guarded([&] {
+        require_built(x, "get_ids");
+        if (!out) fail(E8QC_EINVAL, "null buffer");
+        std::memcpy(out, x->ids_compact.data(), x->n * 4);
+    });
+}
+
+int e8qc_me8q_export_codes(e8qc_me8q* x, uint16_t* digits, uint8_t* branch, float* coef, float* h2) {
+    return guarded([&] {
+        require_built(x, "export_codes");
+        std::lock_guard<std::mutex> lock(x->mu);
+        DeviceGuard g(x->device);
+        cudaStream_t s = nullptr;
+        const size_t n = x->n, pd = x->pd;
+        if (digits || branch) {
+            DevBuf dd, bb;
+            dd.alloc(n * pd * 2);
+            bb.alloc(n * (pd / 8));
+            launch_me8q_decode(x->view, static_cast<int>(x->ntiles), x->list_of_tile_d.as<uint32_t>(),
+                               x->list_begin_d.as<uint64_t>(), static_cast<int>(pd), dd.as<uint16_t>(), bb.as<uint8_t>(), s);
+            if (digits) E8QC_CUDA(cudaMemcpy(digits, dd.p, n * pd * 2, cudaMemcpyDeviceToHost));
+            if (branch) E8QC_CUDA(cudaMemcpy(branch, bb.p, n * (pd / 8), cudaMemcpyDeviceToHost));
+        }
+        if (coef || h2) {
+            const size_t nc = static_cast<size_t>(x->ncoded);
+            std::vector<float> cf(nc * x->nslots), hh(nc * x->nslots);
+            if (nc) {
+                E8QC_CUDA(cudaMemcpy(cf.data(), x->coef.p, cf.size() * 4, cudaMemcpyDeviceToHost));
+                E8QC_CUDA(cudaMemcpy(hh.data(), x->h2.p, hh.size() * 4, cudaMemcpyDeviceToHost));
+            }
+            for (size_t c = 0; c < x->nlist; ++c)
+                for (uint64_t p = x->list_begin[c]; p < x->list_begin[c + 1]; ++p) {
+                    const size_t slot = static_cast<size_t>(x->tile_begin[c]) * 32 + (p - x->list_begin[c]);
+                    for (size_t q = 0; q < nc; ++q) {
+                        if (coef) coef[p * nc + q] = cf[q * x->nslots + slot];
+                        if (h2) h2[p * nc + q] = hh[q * x->nslots + slot];
+                    }
+                }
+        }
+    });
+}
+
+}  // extern "C"

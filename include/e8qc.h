@@ -175,6 +175,59 @@ int e8qc_e8q_get_ids(const e8qc_index* idx, uint32_t* out);
 int e8qc_e8q_export_codes(const e8qc_index* idx, uint16_t* digits, uint8_t* branch, float* g1,
                           float* h3);
 
+/* ---- ME8Q: mixed-rate index (e8qlib::me8q::Me8qIndex, include/e8qlib/index/me8q.hpp:66-140) ---- */
+typedef struct e8qc_me8q e8qc_me8q;
+/* BuildOptions (me8q.hpp:31-52) plus the optional per-dimension variance of
+ * Build (me8q.hpp:76-80). plan_spec "L:B,L:B,..." (runs of 64-dim multiples
+ * covering the padded dim) overrides the DP plan; max_bits <= 0 means 13.
+ * prune_alpha is accepted for interface parity: the device scan scores every
+ * vector of the probed lists exactly, so results do not depend on it. */
+typedef struct e8qc_me8q_build_opts {
+    const float* variance; /* dim floats, host or device; NULL: computed from data */
+    const char* plan_spec; /* NULL or "": DP plan */
+    int drop_energy;       /* add the dropped dims' residual energy to the last run's h2 */
+    float prune_alpha;
+    double extra_budget_bits;
+    int max_bits;
+} e8qc_me8q_build_opts;
+typedef struct e8qc_me8q_meta {
+    uint64_t n, dim, padded_dim, nlist, nruns, ncoded, route_dim, bytes_per_vector, memory_bytes;
+    double bits_per_dim; /* 8 * bytes_per_vector / dim (me8q_io.cpp:176-181) */
+    float avg_bits;
+    int is_built;
+} e8qc_me8q_meta;
+/* Allocate (src/quantization/me8q_plan.cpp:47-167): SAQ's DP plan for a
+ * per-dimension variance padded to padded_dim (a multiple of 64). Host only.
+ * *count runs; up to cap (len, bits) pairs written. */
+int e8qc_me8q_allocate(const float* var_padded, size_t padded_dim, float avg_bits, int max_bits,
+                       double extra_budget_bits, size_t* lens, int* bits, size_t cap, size_t* count);
+/* detail::ParsePlanSpec (src/index/me8q_common.cpp:37-68): "L:B,..." with
+ * L a positive multiple of 64, B in [0, 13], lens summing to padded_dim;
+ * E8QC_EINVAL otherwise. Host only. */
+int e8qc_me8q_parse_plan(const char* spec, size_t padded_dim, size_t* lens, int* bits, size_t cap, size_t* count);
+/* Me8qIndex(dim, avg_bits, seed): seed 0 keeps the default rotator seed. */
+int e8qc_me8q_create(int device, size_t dim, float avg_bits, uint64_t seed, e8qc_me8q** out);
+int e8qc_me8q_destroy(e8qc_me8q* idx);
+/* Me8qIndex::Build (me8q_build.cpp:42-311): data n x dim, centroids nlist x
+ * dim, cluster_ids n; host or device pointers; opts may be NULL. */
+int e8qc_me8q_build(e8qc_me8q* idx, const float* data, size_t n, const float* centroids, size_t nlist,
+                    const uint32_t* cluster_ids, const e8qc_me8q_build_opts* opts, void* stream);
+/* Me8qIndex::SearchIVF (me8q_search.cpp:136-236): out rows of k ids /
+ * distances, ascending; k <= 128. Host or device pointers. */
+int e8qc_me8q_search(e8qc_me8q* idx, const float* queries, size_t nq, size_t k, size_t nprobe,
+                     uint32_t* out_ids, float* out_dists, e8qc_stats* stats, void* stream);
+/* Me8qIndex::Estimate (me8q_measure.cpp:41-66); E8QC_ERANGE for an unknown id. */
+int e8qc_me8q_estimate(e8qc_me8q* idx, const float* query, uint32_t id, float* out);
+int e8qc_me8q_info(const e8qc_me8q* idx, e8qc_me8q_meta* out);
+/* The plan (shared_plan, me8q.hpp:135): *count runs; up to cap (len, bits) written. */
+int e8qc_me8q_plan(const e8qc_me8q* idx, size_t* lens, int* bits, size_t cap, size_t* count);
+/* Global ids, cluster-major (n entries). */
+int e8qc_me8q_get_ids(const e8qc_me8q* idx, uint32_t* out);
+/* Per vector, cluster-major: digits n*padded_dim uint16 and branch
+ * n*padded_dim/8 uint8 of every coded run (zeros in dropped runs), coef and
+ * h2 n*ncoded floats (any may be NULL). */
+int e8qc_me8q_export_codes(e8qc_me8q* idx, uint16_t* digits, uint8_t* branch, float* coef, float* h2);
+
 /* ---- Autotuning and captured plans (no reference counterpart) ---- */
 typedef struct e8qc_tuning {
     int schedule;      /* work-queue order: 0 longest list first, 1 list id order */

@@ -320,6 +320,8 @@ static void warm_tables(int bits) {
     }
 }
 
+void orc_warm_tables(int bits) { warm_tables(bits); }
+
 /* NearestInTable: src/quantization/e8q_codec.cpp:233-256. */
 static void nearest_in_table(double v, const level_table* t, uint16_t* digit, double* cost) {
     const double* lev = t->buf;

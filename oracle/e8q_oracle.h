@@ -34,6 +34,10 @@ void orc_scan_class_means(int bits, double w_cls[2]);
 /* 1 when the merged four-class table of this rate alternates (the encoder's
  * single-search path), 0 when the encoder uses the four parity tables. */
 int orc_merged_alternating(int bits);
+/* Build the encoder's lookup tables for `bits` (they are created lazily and
+ * are not safe to create from several threads at once: call this before a
+ * parallel region that encodes). */
+void orc_warm_tables(int bits);
 
 /* ---- encoder ------------------------------------------------------------ */
 /* n unit vectors (padded_dim floats each) -> digits[n][B][8], branch[n][B]. */

@@ -203,6 +203,8 @@ orc_me8q_index* orc_me8q_build(const float* base, const float* centroids, const 
             }
         }
     make_runs(x, plan_len, plan_bits, nplan, rot_seed);
+    for (int r = 0; r < nplan; ++r)
+        if (plan_bits[r] != 0) orc_warm_tables(plan_bits[r]); /* before the threads share them */
     /* padded centroids, per-run rotation, norms (CentroidNorm2,
      * include/e8qlib/index/ivf_common.hpp:43-54) */
     x->centroids = (float*)calloc(nlist * pd, sizeof(float));
