@@ -73,6 +73,12 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     ap.add_argument("--serve-loads", default="0.3,0.6", help="offered load as fractions of the batch QPS")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-me8q", action="store_true", help="skip the ME8Q leg")
+    ap.add_argument("--me8q-n", type=int, default=10_000_000)
+    ap.add_argument("--me8q-dim", type=int, default=768)
+    ap.add_argument("--me8q-nlist", type=int, default=4096)
+    ap.add_argument("--me8q-avg-bits", type=float, default=4.0)
+    ap.add_argument("--me8q-nprobes", default="16,32,64,128")
     return ap.parse_args()
 
 
@@ -139,17 +145,29 @@ def gen_data(a, device, rank):
 
 
 def ground_truth(x, q, k):
-    """FP64 brute-force top-k over the raw vectors."""
+    """FP64 brute-force top-k over the raw vectors (base in chunks of 1M rows)."""
     import torch
 
-    xd = x.double()
-    xn = (xd * xd).sum(1)
-    out = []
-    for i in range(0, q.shape[0], 256):
-        qd = q[i:i + 256].double()
-        d = (qd * qd).sum(1, keepdim=True) + xn[None, :] - 2.0 * qd @ xd.T
-        out.append(torch.topk(d, k, dim=1, largest=False).indices)
-    return torch.cat(out).cpu().numpy()
+    best_d, best_i = None, None
+    for c0 in range(0, x.shape[0], 1 << 20):
+        xd = x[c0:c0 + (1 << 20)].double()
+        xn = (xd * xd).sum(1)
+        dd, ii = [], []
+        for i in range(0, q.shape[0], 256):
+            qd = q[i:i + 256].double()
+            d = (qd * qd).sum(1, keepdim=True) + xn[None, :] - 2.0 * qd @ xd.T
+            t = torch.topk(d, min(k, d.shape[1]), dim=1, largest=False)
+            dd.append(t.values)
+            ii.append(t.indices + c0)
+        dd, ii = torch.cat(dd), torch.cat(ii)
+        if best_d is None:
+            best_d, best_i = dd, ii
+        else:
+            cd, ci = torch.cat([best_d, dd], 1), torch.cat([best_i, ii], 1)
+            t = torch.topk(cd, k, dim=1, largest=False)
+            best_d, best_i = t.values, torch.gather(ci, 1, t.indices)
+        del xd
+    return best_i.cpu().numpy()
 
 
 def recall_at(ids, gt, k=10):
@@ -214,11 +232,12 @@ class Clocks:
                 "reasons": reasons, "samples": len(busy)}
 
 
-def serve_open_loop(e8qlib, idx, mode, qn, k, nprobe, rate_qps, seconds, seed, max_batch):
+def serve_open_loop(e8qlib, idx, mode, qn, ks, nprobes, rate_qps, seconds, seed, max_batch):
     """Open-loop Poisson arrivals through e8qlib.Server: requests of U{1..64}
-    queries (k, nprobe fixed), exponential inter-arrival times at rate_qps /
-    32.5 requests per second; one thread submits on schedule, another collects.
-    Returns the server's stats (latency submit -> results ready)."""
+    queries, k and nprobe drawn uniformly per request from `ks` / `nprobes`,
+    exponential inter-arrival times at rate_qps / 32.5 requests per second;
+    one thread submits on schedule, another collects. Returns the server's
+    stats (latency submit -> results ready)."""
     import threading
 
     rng = np.random.default_rng(seed)
@@ -227,7 +246,10 @@ def serve_open_loop(e8qlib, idx, mode, qn, k, nprobe, rate_qps, seconds, seed, m
     gaps = rng.exponential(1.0 / req_rate, n_req)
     sizes = rng.integers(1, 65, n_req)
     starts = rng.integers(0, qn.shape[0] - 64, n_req)
-    srv = e8qlib.Server(idx, mode=mode, max_batch=max_batch, max_k=max(k, 1), max_nprobe=nprobe, slots=2)
+    kreq = rng.choice(np.asarray(ks), n_req)
+    npreq = rng.choice(np.asarray(nprobes), n_req)
+    srv = e8qlib.Server(idx, mode=mode, max_batch=max_batch, max_k=int(max(ks)), max_nprobe=int(max(nprobes)),
+                        slots=2)
     ids = []
     done = threading.Event()
 
@@ -248,7 +270,7 @@ def serve_open_loop(e8qlib, idx, mode, qn, k, nprobe, rate_qps, seconds, seed, m
         t += gaps[j]
         while time.perf_counter() < t:
             pass
-        ids.append(srv.submit(qn[starts[j]:starts[j] + sizes[j]], k, nprobe))
+        ids.append(srv.submit(qn[starts[j]:starts[j] + sizes[j]], int(kreq[j]), int(npreq[j])))
     done.wait()
     th.join()
     st = srv.stats()
@@ -288,6 +310,179 @@ def cpu_baseline(a, x_host, cm_host, lab_host, q_host, gt, steps=None, warmup=No
     out["plain_recall"] = recall_at(ids_p, gt[:ps], a.k)
     ref.set_disable_prune(False)
     out["ref"] = ref
+    return out
+
+
+def gen_me8q(a, device):
+    """ME8Q workload on `device`: z ~ N(0, diag(i^-0.8)), x = normalise(R z)
+    with a seeded Haar rotation R (QR of a Gaussian); full-rank PCA (fp64
+    covariance + eigh) gives the base, queries and per-dimension variance the
+    index is built on; lists from 4,096 seeded rows refined by 3 Lloyd steps.
+    Returns (x_raw, base_pca, q_raw, q_pca, variance, centroids, labels)."""
+    import torch
+
+    n, d, nl = a.me8q_n, a.me8q_dim, a.me8q_nlist
+    g = torch.Generator(device=device)
+    g.manual_seed(3000 + a.seed)
+    R, _ = torch.linalg.qr(torch.randn(d, d, generator=g, device=device, dtype=torch.float64))
+    sd = (torch.arange(1, d + 1, device=device, dtype=torch.float64) ** -0.4).float()
+    Rf = R.float()
+
+    def draw(m, gen):
+        out = torch.empty(m, d, device=device)
+        for i in range(0, m, 1 << 20):
+            j = min(m, i + (1 << 20))
+            z = torch.randn(j - i, d, generator=gen, device=device) * sd
+            v = z @ Rf.T
+            out[i:j] = v / v.norm(dim=1, keepdim=True)
+        return out
+
+    x = draw(n, g)
+    gq = torch.Generator(device=device)
+    gq.manual_seed(4000 + a.seed)
+    q = draw(a.pool, gq)
+    mean = x.double().mean(0)
+    cov = torch.zeros(d, d, device=device, dtype=torch.float64)
+    for i in range(0, n, 1 << 19):
+        c = x[i:i + (1 << 19)].double() - mean
+        cov += c.T @ c
+    cov /= n
+    evals, evecs = torch.linalg.eigh(cov)
+    order = torch.argsort(evals, descending=True)
+    V = evecs[:, order].float()
+    var = evals[order].clamp_min(0).float().contiguous()
+    meanf = mean.float()
+    xp = torch.empty_like(x)
+    for i in range(0, n, 1 << 20):
+        xp[i:i + (1 << 20)] = (x[i:i + (1 << 20)] - meanf) @ V
+    qp = ((q - meanf) @ V).contiguous()
+    # lists: seeded rows, 3 Lloyd steps, final assignment
+    cen = xp[torch.randperm(n, generator=g, device=device)[:nl]].clone()
+    lab = torch.empty(n, dtype=torch.int64, device=device)
+
+    def assign():
+        cn = (cen * cen).sum(1)
+        for i in range(0, n, 1 << 18):
+            blk = xp[i:i + (1 << 18)]
+            lab[i:i + (1 << 18)] = torch.argmin(cn[None, :] - 2.0 * blk @ cen.T, dim=1)
+
+    for _ in range(3):
+        assign()
+        acc = torch.zeros(nl, d, device=device, dtype=torch.float64)
+        for i in range(0, n, 1 << 20):
+            acc.index_add_(0, lab[i:i + (1 << 20)], xp[i:i + (1 << 20)].double())
+        cnt = torch.bincount(lab, minlength=nl).double()
+        keep = cnt > 0
+        cen[keep] = (acc[keep] / cnt[keep, None]).float()
+    assign()
+    return x, xp.contiguous(), q, qp, var, cen.contiguous(), lab.to(torch.int32).contiguous()
+
+
+def me8q_leg(a, e8qlib, dev, local, stream):
+    """ME8Q index (mixed-rate) at the ME8Q workload: build time, recall@10 per
+    nprobe against an FP64 brute force over the raw vectors, batched QPS at
+    the smallest nprobe with recall >= 0.95, single-query latency, and
+    open-loop serving with k in {10, 100} and nprobe drawn from the values
+    that meet the recall bar."""
+    import torch
+
+    sp = stream.cuda_stream
+    t0 = time.perf_counter()
+    x, xp, q, qp, var, cen, lab = gen_me8q(a, dev)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    gt = ground_truth(x, q[:a.gt], 10)
+    del x
+    torch.cuda.empty_cache()
+    n, d = xp.shape
+    idx = e8qlib.Me8qIndex(d, a.me8q_avg_bits, a.seed, device=local)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    idx.build_ptr(xp.data_ptr(), n, cen.data_ptr(), cen.shape[0], lab.data_ptr(), var.data_ptr(), True, "", 0.0, sp)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    del xp
+    torch.cuda.empty_cache()
+    nb = a.batch
+    oi = torch.empty(nb, 100, dtype=torch.int32, device=dev)
+    od = torch.empty(nb, 100, dtype=torch.float32, device=dev)
+    sweep = []
+    for npb in [int(t) for t in a.me8q_nprobes.split(",") if t]:
+        ids = np.zeros((a.gt, 10), np.uint32)
+        for i in range(0, a.gt, nb):
+            b = min(nb, a.gt - i)
+            idx.search_ptr(qp[i:i + b].data_ptr(), b, 10, npb, oi.data_ptr(), od.data_ptr(), sp)
+            torch.cuda.synchronize()
+            ids[i:i + b] = oi.view(-1)[:b * 10].view(b, 10).cpu().numpy().view(np.uint32)
+        sweep.append({"nprobe": npb, "recall_at_10": round(recall_at(ids, gt, 10), 4)})
+    ok = [r for r in sweep if r["recall_at_10"] >= 0.95]
+    npb = (ok[0] if ok else sweep[-1])["nprobe"]
+    nbat = max(1, a.pool // nb)
+
+    def step(i):
+        qi = qp[(i % nbat) * nb:(i % nbat) * nb + nb]
+        return idx.search_ptr(qi.data_ptr(), nb, 10, npb, oi.data_ptr(), od.data_ptr(), sp)
+
+    for i in range(a.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    launches = 0
+    for i in range(a.steps):
+        launches += step(a.warmup + i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    qps = a.steps * nb / (ms / 1000.0)
+    # one query per call (device-resident), median of 64 calls
+    lat = []
+    for i in range(72):
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        idx.search_ptr(qp[i].data_ptr(), 1, 10, npb, oi.data_ptr(), od.data_ptr(), sp)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        if i >= 8:
+            lat.append(s0.elapsed_time(s1))
+    single_ms = statistics.median(lat)
+    # algorithmic bytes of the scan per query: codes + (coef, h2) of every
+    # probed vector, bits_per_dim * dim / 8 bytes each
+    bytes_per_vec = idx.bits_per_dim * d / 8.0
+    serving = []
+    if not a.no_serve:
+        qh = torch.empty(a.pool, d, dtype=torch.float32, pin_memory=True)
+        qh.copy_(qp.cpu())
+        qn = qh.numpy()
+        grid = [p for p in (16, 32, 64, 128, 256, 512) if p >= npb]
+        rng = np.random.default_rng(a.seed + 11)
+        # capacity of the mixed load: one ragged batch of 4,096 queries
+        kk = rng.choice([10, 100], nb).astype(np.uint32)
+        pp = rng.choice(grid, nb).astype(np.uint32)
+        idx.search_ragged(qn[:nb], kk, pp, 100)
+        c0 = time.perf_counter()
+        idx.search_ragged(qn[:nb], kk, pp, 100)
+        cap = nb / (time.perf_counter() - c0)
+        for frac in [float(f) for f in a.serve_loads.split(",") if f]:
+            st = serve_open_loop(e8qlib, idx, "batched", qn, [10, 100], grid, frac * cap, a.serve_seconds,
+                                 a.seed + 13, a.batch)
+            serving.append({"offered_qps": st["offered_qps"], "achieved_qps": round(st["qps"], 1),
+                            "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
+                            "max_ms": round(st["max_ms"], 3), "requests": st["requests"],
+                            "mean_batch_queries": round(st["mean_batch_queries"], 1)})
+        serving = {"k": [10, 100], "nprobe": grid, "mixed_batch_capacity_qps": round(cap, 1), "loads": serving}
+    out = {"workload": (f"ME8Q IVF search, {n // 1000}k x {d}-d unit vectors (spectrum i^-0.8, Haar rotation, "
+                        f"full-rank PCA), {cen.shape[0]} lists (3 Lloyd steps), avg_bits={a.me8q_avg_bits}, "
+                        f"k=10, query batch {nb}"),
+           "plan": [list(p) for p in idx.plan], "bits_per_dim": round(idx.bits_per_dim, 3),
+           "memory_bytes": idx.memory_bytes, "gen_s": round(gen_s, 2), "build_s": round(build_s, 2),
+           "recall_sweep": sweep, "nprobe": npb, "qps": round(qps, 1), "ms_per_step": round(ms / a.steps, 3),
+           "gpu_launches": int(launches), "single_query_ms": round(single_ms, 4),
+           "scan_bytes_per_vector": round(bytes_per_vec, 1),
+           "algo_gbs": round(qps * npb * (n / cen.shape[0]) * bytes_per_vec / 1e9, 1),
+           "serving": serving}
+    del idx, qp, q, cen, lab, var
+    torch.cuda.empty_cache()
     return out
 
 
@@ -444,12 +639,16 @@ def main():
     if a.path != "plain" and not a.no_serve:
         serving = []
         for frac in [float(f) for f in a.serve_loads.split(",") if f]:
-            st = serve_open_loop(e8qlib, idx, a.path, qn, a.k, a.nprobe, frac * value, a.serve_seconds,
+            st = serve_open_loop(e8qlib, idx, a.path, qn, [a.k], [a.nprobe], frac * value, a.serve_seconds,
                                  a.seed + 7, a.batch)
             serving.append({"offered_qps": st["offered_qps"], "achieved_qps": round(st["qps"], 1),
                             "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
                             "max_ms": round(st["max_ms"], 3), "requests": st["requests"],
                             "mean_batch_queries": round(st["mean_batch_queries"], 1)})
+
+    me8q = None
+    if not a.no_me8q:
+        me8q = me8q_leg(a, e8qlib, dev, local, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -482,7 +681,7 @@ def main():
         "clocks": clk.summary(), "gpu_launches": int(launches), "roofline": roofline,
         "e2e": e2e, "cpu_baseline": cpu,
         "plain_gpu_qps": None if plain_qps is None else round(plain_qps, 1),
-        "serving": serving,
+        "serving": serving, "me8q": me8q,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -279,156 +279,6 @@ class E8qIndex {
     }
 };
 
-// Captured search plan (see e8qc_plan_* in e8qc.h): one CUDA graph per
-// batch size bucket. Holds a reference to the Python index.
-class Plan {
-   public:
-    Plan(py::object index, const std::string& mode, size_t max_queries, size_t k_max, size_t nprobe_max,
-         bool autotune)
-        : index_(index), k_max_(k_max) {
-        E8qIndex& ix = index.cast<E8qIndex&>();
-        dim_ = ix.dim();
-        const int md = mode_of(mode);
-        if (md == E8QC_MODE_PLAIN) throw std::invalid_argument("plans run 'batched' or 'precision'");
-        e8qc_index* h = ix.handle("plan");
-        py::gil_scoped_release nogil;
-        check(e8qc_plan_create(h, md, max_queries, k_max, nprobe_max, autotune ? 1 : 0, &plan_));
-    }
-    ~Plan() {
-        if (plan_) e8qc_plan_destroy(plan_);
-    }
-    py::tuple run(py::handle queries, py::handle k, py::handle nprobe) {
-        auto q = ensure_nd<float>(queries, "queries", 2);
-        if (static_cast<size_t>(q.shape(1)) != dim_)
-            throw std::invalid_argument("query dimension does not match index dim");
-        const size_t nq = static_cast<size_t>(q.shape(0));
-        std::vector<uint32_t> kv(nq), nv(nq);
-        auto fill = [&](py::handle h, std::vector<uint32_t>& v, const char* name) {
-            if (py::isinstance<py::int_>(h)) {
-                std::fill(v.begin(), v.end(), h.cast<uint32_t>());
-            } else {
-                auto a = ensure_nd<uint32_t>(h, name, 1);
-                if (static_cast<size_t>(a.shape(0)) != nq)
-                    throw std::invalid_argument(std::string(name) + " must have one entry per query");
-                std::copy(a.data(), a.data() + nq, v.begin());
-            }
-        };
-        fill(k, kv, "k");
-        fill(nprobe, nv, "nprobe");
-        py::array_t<uint32_t> ids({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k_max_)});
-        py::array_t<float> dists({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k_max_)});
-        if (nq > 0) {
-            py::gil_scoped_release nogil;
-            check(e8qc_plan_run(plan_, q.data(), nq, kv.data(), nv.data(), ids.mutable_data(), dists.mutable_data(),
-                                nullptr));
-        }
-        return py::make_tuple(ids, dists);
-    }
-
-   private:
-    py::object index_;
-    size_t dim_ = 0, k_max_ = 0;
-    e8qc_plan* plan_ = nullptr;
-};
-
-// Serving loop over one index (an addition of this library; see
-// e8qc_server_* in e8qc.h). Holds a reference to the Python index so it
-// outlives the server.
-class Server {
-   public:
-    Server(py::object index, const std::string& mode, size_t max_batch, size_t max_k, size_t max_nprobe,
-           size_t memory_budget, int slots)
-        : index_(index) {
-        E8qIndex& ix = index.cast<E8qIndex&>();
-        dim_ = ix.dim();
-        e8qc_server_config c{};
-        c.mode = mode_of(mode);
-        if (c.mode == E8QC_MODE_PLAIN) throw std::invalid_argument("the server runs 'batched' or 'precision'");
-        c.max_batch_queries = max_batch;
-        c.max_k = max_k;
-        c.max_nprobe = max_nprobe;
-        c.memory_budget = memory_budget;
-        c.slots = slots;
-        e8qc_index* h = ix.handle("serve");
-        py::gil_scoped_release nogil;
-        check(e8qc_server_start(h, &c, &srv_));
-    }
-    ~Server() {
-        try {
-            stop();
-        } catch (...) {
-        }
-    }
-    uint64_t submit(py::handle queries, size_t k, size_t nprobe) {
-        if (!srv_) throw std::runtime_error("server is stopped");
-        auto q = ensure_nd<float>(queries, "queries", 2);
-        if (static_cast<size_t>(q.shape(1)) != dim_)
-            throw std::invalid_argument("query dimension does not match index dim");
-        const size_t nq = static_cast<size_t>(q.shape(0));
-        uint64_t id = 0;
-        {
-            py::gil_scoped_release nogil;
-            check(e8qc_server_submit(srv_, q.data(), nq, k, nprobe, &id));
-        }
-        shapes_[id] = {nq, k};
-        return id;
-    }
-    py::object result(uint64_t id, int timeout_ms) {
-        if (!srv_) throw std::runtime_error("server is stopped");
-        auto it = shapes_.find(id);
-        if (it == shapes_.end()) throw py::index_error("unknown or already collected request id");
-        const size_t nq = it->second.first, k = it->second.second;
-        py::array_t<uint32_t> ids({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k)});
-        py::array_t<float> dists({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k)});
-        int done = 0, rc = 0;
-        {
-            py::gil_scoped_release nogil;
-            rc = e8qc_server_poll(srv_, id, timeout_ms, ids.mutable_data(), dists.mutable_data(), &done);
-        }
-        if (done) shapes_.erase(id);
-        check(rc);
-        if (!done) return py::none();
-        return py::make_tuple(ids, dists);
-    }
-    py::dict stats(bool reset) {
-        if (!srv_) throw std::runtime_error("server is stopped");
-        e8qc_server_stats st{};
-        check(e8qc_server_get_stats(srv_, reset ? 1 : 0, &st));
-        py::dict d;
-        d["submitted"] = st.submitted;
-        d["rejected"] = st.rejected;
-        d["completed"] = st.completed;
-        d["failed"] = st.failed;
-        d["queries_completed"] = st.queries_completed;
-        d["batches"] = st.batches;
-        d["p50_ms"] = st.p50_ms;
-        d["p99_ms"] = st.p99_ms;
-        d["mean_ms"] = st.mean_ms;
-        d["max_ms"] = st.max_ms;
-        d["qps"] = st.qps;
-        d["mean_batch_queries"] = st.mean_batch_queries;
-        d["peak_batch_bytes"] = st.peak_batch_bytes;
-        return d;
-    }
-    void stop() {
-        if (!srv_) return;
-        e8qc_server* s = srv_;
-        srv_ = nullptr;
-        int rc = 0;
-        {
-            py::gil_scoped_release nogil;
-            rc = e8qc_server_stop(s);
-        }
-        check(rc);
-    }
-
-   private:
-    py::object index_;
-    size_t dim_ = 0;
-    e8qc_server* srv_ = nullptr;
-    std::unordered_map<uint64_t, std::pair<size_t, size_t>> shapes_;
-};
-
 // Me8qIndex (python_bindings/me8q_bindings.cpp:22-269 of the reference): same
 // constructor, build / search / estimate arguments, properties and errors;
 // `device` is this library's addition. save / load are not part of the
@@ -480,6 +330,41 @@ class Me8qIndex {
                                   static_cast<size_t>(c.shape(0)), ids.data(), &o, nullptr));
         }
         built_ = true;
+    }
+
+    // Device-resident build: raw CUDA pointers (e.g. torch tensor data_ptr());
+    // variance 0 = computed from the data.
+    void build_ptr(uintptr_t data, size_t n, uintptr_t centroids, size_t nlist, uintptr_t cluster_ids,
+                   uintptr_t variance, bool drop_energy, const std::string& plan_spec, double extra_budget_bits,
+                   uintptr_t stream) {
+        e8qc_me8q_build_opts o{};
+        o.variance = reinterpret_cast<const float*>(variance);
+        o.plan_spec = plan_spec.c_str();
+        o.drop_energy = drop_energy ? 1 : 0;
+        o.extra_budget_bits = extra_budget_bits;
+        if (idx_) e8qc_me8q_destroy(idx_);
+        idx_ = nullptr;
+        built_ = false;
+        check(e8qc_me8q_create(device_, dim_, avg_bits_, seed_, &idx_));
+        {
+            py::gil_scoped_release nogil;
+            check(e8qc_me8q_build(idx_, reinterpret_cast<const float*>(data), n,
+                                  reinterpret_cast<const float*>(centroids), nlist,
+                                  reinterpret_cast<const uint32_t*>(cluster_ids), &o, reinterpret_cast<void*>(stream)));
+        }
+        built_ = true;
+    }
+
+    // Device-resident search on raw CUDA pointers; returns the launch count.
+    uint64_t search_ptr(uintptr_t queries, size_t nq, size_t k, size_t nprobe, uintptr_t out_ids, uintptr_t out_dists,
+                        uintptr_t stream) {
+        require("search");
+        e8qc_stats st{};
+        py::gil_scoped_release nogil;
+        check(e8qc_me8q_search(idx_, reinterpret_cast<const float*>(queries), nq, k, nprobe,
+                               reinterpret_cast<uint32_t*>(out_ids), reinterpret_cast<float*>(out_dists), &st,
+                               reinterpret_cast<void*>(stream)));
+        return st.launches;
     }
 
     py::tuple search(py::handle queries, size_t k, size_t nprobe, size_t /*num_threads*/, bool return_stats) {
@@ -563,6 +448,33 @@ class Me8qIndex {
         return out;
     }
 
+    // Serving form: per-query k and nprobe; rows padded to k_max.
+    py::tuple search_ragged(py::handle queries, py::handle k, py::handle nprobe, size_t k_max) {
+        auto q = ensure_nd<float>(queries, "queries", 2);
+        auto ka = ensure_nd<uint32_t>(k, "k", 1);
+        auto na = ensure_nd<uint32_t>(nprobe, "nprobe", 1);
+        require("search");
+        if (static_cast<size_t>(q.shape(1)) != dim_)
+            throw std::invalid_argument("query dimension does not match index dim");
+        const size_t nq = static_cast<size_t>(q.shape(0));
+        if (static_cast<size_t>(ka.shape(0)) != nq || static_cast<size_t>(na.shape(0)) != nq)
+            throw std::invalid_argument("k and nprobe must have one entry per query");
+        py::array_t<uint32_t> ids({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k_max)});
+        py::array_t<float> dists({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k_max)});
+        {
+            py::gil_scoped_release nogil;
+            if (nq > 0)
+                check(e8qc_me8q_search_ragged(idx_, q.data(), nq, ka.data(), na.data(), k_max, ids.mutable_data(),
+                                              dists.mutable_data(), nullptr));
+        }
+        return py::make_tuple(ids, dists);
+    }
+
+    e8qc_me8q* handle(const char* what) const {
+        require(what);
+        return idx_;
+    }
+
    private:
     void require(const char* what) const {
         if (!built_ || idx_ == nullptr)
@@ -579,6 +491,175 @@ class Me8qIndex {
     int device_ = 0;
     bool built_ = false;
     e8qc_me8q* idx_ = nullptr;
+};
+
+// Captured search plan (see e8qc_plan_* in e8qc.h): one CUDA graph per
+// batch size bucket. Holds a reference to the Python index.
+class Plan {
+   public:
+    Plan(py::object index, const std::string& mode, size_t max_queries, size_t k_max, size_t nprobe_max,
+         bool autotune)
+        : index_(index), k_max_(k_max) {
+        if (py::isinstance<Me8qIndex>(index)) {
+            Me8qIndex& mx = index.cast<Me8qIndex&>();
+            dim_ = mx.dim();
+            if (!mode.empty() && mode != "batched") throw std::invalid_argument("ME8Q plans run 'batched'");
+            e8qc_me8q* h = mx.handle("plan");
+            py::gil_scoped_release nogil;
+            check(e8qc_plan_create_me8q(h, max_queries, k_max, nprobe_max, autotune ? 1 : 0, &plan_));
+            return;
+        }
+        E8qIndex& ix = index.cast<E8qIndex&>();
+        dim_ = ix.dim();
+        const int md = mode_of(mode.empty() ? std::string("precision") : mode);
+        if (md == E8QC_MODE_PLAIN) throw std::invalid_argument("plans run 'batched' or 'precision'");
+        e8qc_index* h = ix.handle("plan");
+        py::gil_scoped_release nogil;
+        check(e8qc_plan_create(h, md, max_queries, k_max, nprobe_max, autotune ? 1 : 0, &plan_));
+    }
+    ~Plan() {
+        if (plan_) e8qc_plan_destroy(plan_);
+    }
+    py::tuple run(py::handle queries, py::handle k, py::handle nprobe) {
+        auto q = ensure_nd<float>(queries, "queries", 2);
+        if (static_cast<size_t>(q.shape(1)) != dim_)
+            throw std::invalid_argument("query dimension does not match index dim");
+        const size_t nq = static_cast<size_t>(q.shape(0));
+        std::vector<uint32_t> kv(nq), nv(nq);
+        auto fill = [&](py::handle h, std::vector<uint32_t>& v, const char* name) {
+            if (py::isinstance<py::int_>(h)) {
+                std::fill(v.begin(), v.end(), h.cast<uint32_t>());
+            } else {
+                auto a = ensure_nd<uint32_t>(h, name, 1);
+                if (static_cast<size_t>(a.shape(0)) != nq)
+                    throw std::invalid_argument(std::string(name) + " must have one entry per query");
+                std::copy(a.data(), a.data() + nq, v.begin());
+            }
+        };
+        fill(k, kv, "k");
+        fill(nprobe, nv, "nprobe");
+        py::array_t<uint32_t> ids({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k_max_)});
+        py::array_t<float> dists({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k_max_)});
+        if (nq > 0) {
+            py::gil_scoped_release nogil;
+            check(e8qc_plan_run(plan_, q.data(), nq, kv.data(), nv.data(), ids.mutable_data(), dists.mutable_data(),
+                                nullptr));
+        }
+        return py::make_tuple(ids, dists);
+    }
+
+   private:
+    py::object index_;
+    size_t dim_ = 0, k_max_ = 0;
+    e8qc_plan* plan_ = nullptr;
+};
+
+// Serving loop over one index (an addition of this library; see
+// e8qc_server_* in e8qc.h). Holds a reference to the Python index so it
+// outlives the server.
+class Server {
+   public:
+    Server(py::object index, const std::string& mode, size_t max_batch, size_t max_k, size_t max_nprobe,
+           size_t memory_budget, int slots)
+        : index_(index) {
+        e8qc_server_config c{};
+        c.max_batch_queries = max_batch;
+        c.max_k = max_k;
+        c.max_nprobe = max_nprobe;
+        c.memory_budget = memory_budget;
+        c.slots = slots;
+        if (py::isinstance<Me8qIndex>(index)) {
+            Me8qIndex& mx = index.cast<Me8qIndex&>();
+            dim_ = mx.dim();
+            if (!mode.empty() && mode != "batched") throw std::invalid_argument("the ME8Q server runs 'batched'");
+            c.mode = E8QC_MODE_BATCHED;
+            e8qc_me8q* h = mx.handle("serve");
+            py::gil_scoped_release nogil;
+            check(e8qc_server_start_me8q(h, &c, &srv_));
+            return;
+        }
+        E8qIndex& ix = index.cast<E8qIndex&>();
+        dim_ = ix.dim();
+        c.mode = mode_of(mode.empty() ? std::string("precision") : mode);
+        if (c.mode == E8QC_MODE_PLAIN) throw std::invalid_argument("the server runs 'batched' or 'precision'");
+        e8qc_index* h = ix.handle("serve");
+        py::gil_scoped_release nogil;
+        check(e8qc_server_start(h, &c, &srv_));
+    }
+    ~Server() {
+        try {
+            stop();
+        } catch (...) {
+        }
+    }
+    uint64_t submit(py::handle queries, size_t k, size_t nprobe) {
+        if (!srv_) throw std::runtime_error("server is stopped");
+        auto q = ensure_nd<float>(queries, "queries", 2);
+        if (static_cast<size_t>(q.shape(1)) != dim_)
+            throw std::invalid_argument("query dimension does not match index dim");
+        const size_t nq = static_cast<size_t>(q.shape(0));
+        uint64_t id = 0;
+        {
+            py::gil_scoped_release nogil;
+            check(e8qc_server_submit(srv_, q.data(), nq, k, nprobe, &id));
+        }
+        shapes_[id] = {nq, k};
+        return id;
+    }
+    py::object result(uint64_t id, int timeout_ms) {
+        if (!srv_) throw std::runtime_error("server is stopped");
+        auto it = shapes_.find(id);
+        if (it == shapes_.end()) throw py::index_error("unknown or already collected request id");
+        const size_t nq = it->second.first, k = it->second.second;
+        py::array_t<uint32_t> ids({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k)});
+        py::array_t<float> dists({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k)});
+        int done = 0, rc = 0;
+        {
+            py::gil_scoped_release nogil;
+            rc = e8qc_server_poll(srv_, id, timeout_ms, ids.mutable_data(), dists.mutable_data(), &done);
+        }
+        if (done) shapes_.erase(id);
+        check(rc);
+        if (!done) return py::none();
+        return py::make_tuple(ids, dists);
+    }
+    py::dict stats(bool reset) {
+        if (!srv_) throw std::runtime_error("server is stopped");
+        e8qc_server_stats st{};
+        check(e8qc_server_get_stats(srv_, reset ? 1 : 0, &st));
+        py::dict d;
+        d["submitted"] = st.submitted;
+        d["rejected"] = st.rejected;
+        d["completed"] = st.completed;
+        d["failed"] = st.failed;
+        d["queries_completed"] = st.queries_completed;
+        d["batches"] = st.batches;
+        d["p50_ms"] = st.p50_ms;
+        d["p99_ms"] = st.p99_ms;
+        d["mean_ms"] = st.mean_ms;
+        d["max_ms"] = st.max_ms;
+        d["qps"] = st.qps;
+        d["mean_batch_queries"] = st.mean_batch_queries;
+        d["peak_batch_bytes"] = st.peak_batch_bytes;
+        return d;
+    }
+    void stop() {
+        if (!srv_) return;
+        e8qc_server* s = srv_;
+        srv_ = nullptr;
+        int rc = 0;
+        {
+            py::gil_scoped_release nogil;
+            rc = e8qc_server_stop(s);
+        }
+        check(rc);
+    }
+
+   private:
+    py::object index_;
+    size_t dim_ = 0;
+    e8qc_server* srv_ = nullptr;
+    std::unordered_map<uint64_t, std::pair<size_t, size_t>> shapes_;
 };
 
 }  // namespace e8qb200
@@ -636,13 +717,13 @@ PYBIND11_MODULE(_e8qlib, m) {
 
     py::class_<e8qb200::Plan>(m, "Plan")
         .def(py::init<py::object, const std::string&, size_t, size_t, size_t, bool>(), py::arg("index"),
-             py::arg("mode") = "precision", py::arg("max_queries") = 4096, py::arg("k_max") = 10,
+             py::arg("mode") = "", py::arg("max_queries") = 4096, py::arg("k_max") = 10,
              py::arg("nprobe_max") = 64, py::arg("autotune") = true)
         .def("run", &e8qb200::Plan::run, py::arg("queries"), py::arg("k"), py::arg("nprobe"));
 
     py::class_<e8qb200::Server>(m, "Server")
         .def(py::init<py::object, const std::string&, size_t, size_t, size_t, size_t, int>(), py::arg("index"),
-             py::arg("mode") = "precision", py::arg("max_batch") = 4096, py::arg("max_k") = 128,
+             py::arg("mode") = "", py::arg("max_batch") = 4096, py::arg("max_k") = 128,
              py::arg("max_nprobe") = 0, py::arg("memory_budget") = 0, py::arg("slots") = 2)
         .def("submit", &e8qb200::Server::submit, py::arg("queries"), py::arg("k"), py::arg("nprobe"))
         .def("result", &e8qb200::Server::result, py::arg("request_id"), py::arg("timeout_ms") = -1)
@@ -661,6 +742,13 @@ PYBIND11_MODULE(_e8qlib, m) {
              py::arg("num_threads") = 1, py::arg("return_stats") = false)
         .def("estimate", &e8qb200::Me8qIndex::estimate, py::arg("query"), py::arg("id"))
         .def("export_codes", &e8qb200::Me8qIndex::export_codes)
+        .def("search_ragged", &e8qb200::Me8qIndex::search_ragged, py::arg("queries"), py::arg("k"),
+             py::arg("nprobe"), py::arg("k_max"))
+        .def("build_ptr", &e8qb200::Me8qIndex::build_ptr, py::arg("data"), py::arg("n"), py::arg("centroids"),
+             py::arg("nlist"), py::arg("cluster_ids"), py::arg("variance") = 0, py::arg("drop_energy") = true,
+             py::arg("plan_spec") = "", py::arg("extra_budget_bits") = 0.0, py::arg("stream") = 0)
+        .def("search_ptr", &e8qb200::Me8qIndex::search_ptr, py::arg("queries"), py::arg("nq"), py::arg("k"),
+             py::arg("nprobe"), py::arg("out_ids"), py::arg("out_dists"), py::arg("stream") = 0)
         .def_property_readonly("dim", &e8qb200::Me8qIndex::dim)
         .def_property_readonly("avg_bits", &e8qb200::Me8qIndex::avg_bits)
         .def_property_readonly("is_built", &e8qb200::Me8qIndex::is_built)

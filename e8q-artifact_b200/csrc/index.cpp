@@ -21,6 +21,7 @@
 #include "internal.h"
 #include "scan_plain.h"
 #include "precision.h"
+#include "serve_target.h"
 #include "workspace.h"
 
 namespace e8qc {
@@ -337,89 +338,91 @@ uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, con
 }  // namespace
 
 namespace e8qc {
-// ---- serving-loop support (server.cpp) ----
+// ---- plans and the serving loop (plan.cpp, server.cpp) ----
 
-// Index facts the server needs; throws when the index is not built.
-void server_index_info(e8qc_index* x, size_t* dim, size_t* nlist, int* device) {
-    require_built(x, "serve");
-    *dim = x->dim;
-    *nlist = x->nlist;
-    *device = x->device;
-}
+namespace {
 
-// One-time preparation for a mode (the precision proxy plane), under the
-// index lock, synchronised.
-void server_prepare(e8qc_index* x, int mode) {
-    require_built(x, "serve");
-    std::lock_guard<std::mutex> lock(x->mu);
-    DeviceGuard g(x->device);
-    if (mode == E8QC_MODE_PRECISION && x->view.proxy == nullptr) {
-        x->proxy.alloc(proxy_plane_bytes(x->view, x->ntiles));
-        launch_build_proxy(x->view, static_cast<int>(x->ntiles), x->proxy.as<uint4>(), nullptr);
-        E8QC_CUDA(cudaStreamSynchronize(nullptr));
-        x->view.proxy = x->proxy.as<uint4>();
+class E8qTarget final : public SearchTarget {
+   public:
+    explicit E8qTarget(e8qc_index* x) : x_(x) {
+        require_built(x, "serve");
+        dim = x->dim;
+        nlist = x->nlist;
+        device = x->device;
     }
-}
-
-// Upper bound of the device scratch one ragged call of nq queries needs
-// (workspace buffers plus the caller's query / k / nprobe / result buffers).
-size_t search_bytes(const e8qc_index* x, int mode, size_t nq, size_t k_max, size_t np_max) {
-    const size_t np = std::min(np_max, x->nlist), nlist = x->nlist, pd = x->pd;
-    const size_t npairs = nq * np;
-    const size_t align = mode == E8QC_MODE_PRECISION ? 8 : 1;
-    const size_t pslots = npairs + (align - 1) * nlist;
-    size_t b = nq * (x->dim * 4 + pd * 4 + k_max * 8 + 8);  // queries, rotated queries, results, k/nprobe
-    b += nq * nlist * 8 + nq * 4;                             // route keys, norms
-    b += npairs * 12 + pslots * 8 + nlist * 12;               // probes, d2, positions; pair rows; list counters
-    b += (npairs / 64 + nlist + 1) * 16 + 32;                 // work items
-    if (mode == E8QC_MODE_PRECISION) {
-        const size_t rows_q = max_tiles_for(x, np) * 32;  // proxy rows one query can need
-        const size_t chunk = std::max<size_t>(1, std::min<size_t>(nq, (size_t(2) << 30) / std::max<size_t>(1, rows_q * 4)));
-        b += nq * (pd + 8) + nlist * 8;                       // int8 queries, scales, row bases
-        b += chunk * rows_q * 4;                              // proxy rows of one chunk
-        b += ((pslots + 7) / 8 * 8 + 128) * pd;               // gathered int8 query rows
-    } else {
-        b += npairs * k_max * 8;                              // per-pair partial top-k
+    void check_mode(int mode) const override {
+        if (mode != E8QC_MODE_BATCHED && mode != E8QC_MODE_PRECISION)
+            fail(E8QC_EINVAL, "plans and servers cover E8QC_MODE_BATCHED and E8QC_MODE_PRECISION");
     }
-    return b;
-}
+    // The precision proxy plane, under the index lock, synchronised.
+    void prepare(int mode) override {
+        require_built(x_, "serve");
+        std::lock_guard<std::mutex> lock(x_->mu);
+        DeviceGuard g(x_->device);
+        if (mode == E8QC_MODE_PRECISION && x_->view.proxy == nullptr) {
+            x_->proxy.alloc(proxy_plane_bytes(x_->view, x_->ntiles));
+            launch_build_proxy(x_->view, static_cast<int>(x_->ntiles), x_->proxy.as<uint4>(), nullptr);
+            E8QC_CUDA(cudaStreamSynchronize(nullptr));
+            x_->view.proxy = x_->proxy.as<uint4>();
+        }
+    }
+    // Workspace buffers plus the caller's query / k / nprobe / result buffers.
+    size_t bytes(int mode, size_t nq, size_t k_max, size_t np_max) const override {
+        const size_t np = std::min(np_max, x_->nlist), nl = x_->nlist, pd = x_->pd;
+        const size_t npairs = nq * np;
+        const size_t align = mode == E8QC_MODE_PRECISION ? 8 : 1;
+        const size_t pslots = npairs + (align - 1) * nl;
+        size_t b = nq * (x_->dim * 4 + pd * 4 + k_max * 8 + 8);  // queries, rotated queries, results, k/nprobe
+        b += nq * nl * 8 + nq * 4;                                // route keys, norms
+        b += npairs * 12 + pslots * 8 + nl * 12;                  // probes, d2, positions; pair rows; list counters
+        b += (npairs / 64 + nl + 1) * 16 + 32;                    // work items
+        if (mode == E8QC_MODE_PRECISION) {
+            const size_t rows_q = max_tiles_for(x_, np) * 32;  // proxy rows one query can need
+            const size_t chunk =
+                std::max<size_t>(1, std::min<size_t>(nq, (size_t(2) << 30) / std::max<size_t>(1, rows_q * 4)));
+            b += nq * (pd + 8) + nl * 8;            // int8 queries, scales, row bases
+            b += chunk * rows_q * 4;                // proxy rows of one chunk
+            b += ((pslots + 7) / 8 * 8 + 128) * pd;  // gathered int8 query rows
+        } else {
+            b += npairs * k_max * 8;  // per-pair partial top-k
+        }
+        return b;
+    }
+    // Kernel wait timeouts land in ws's error word. apply_tuned: take the
+    // autotuned setting of this batch shape (else ws's own setting is used,
+    // as a captured plan fixes it).
+    uint64_t enqueue(Workspace& ws, int mode, const float* q_dev, size_t nq, const uint32_t* k_dev,
+                     const uint32_t* np_dev, size_t k_max, size_t np_max, uint32_t* ids_dev, float* d_dev,
+                     cudaStream_t s, bool apply_tuned) override {
+        const size_t np = std::min(np_max, x_->nlist);
+        ws.ensure_queries(nq, x_->pd);
+        ws.ensure_err();
+        float* rq = ws.rq.as<float>();
+        if (apply_tuned) apply_tuning(x_, ws, mode, nq, np);
+        uint64_t launches = launch_rotate(x_->view, q_dev, static_cast<int>(nq), rq, s);
+        if (mode == E8QC_MODE_PRECISION)
+            launches += precision_search(x_->view, ws, rq, nq, k_dev, np_dev, k_max, np, k_max, ids_dev, d_dev,
+                                         max_tiles_for(x_, np) * 32, s);
+        else
+            launches += batched_search(x_->view, ws, rq, nq, k_dev, np_dev, k_max, np, k_max, ids_dev, d_dev,
+                                       max_tiles_for(x_, np), s);
+        return launches;
+    }
+    void autotune(Workspace& ws, int mode, size_t nq, size_t k, size_t np, cudaStream_t s, int* sched,
+                  int* stages) override {
+        const TuneResult r = autotune_run(x_, ws, mode, nq, k, np, s);
+        *sched = r.sched;
+        *stages = r.stages;
+    }
+    void stored_tuning(Workspace& ws, int mode, size_t nq, size_t np) override { apply_tuning(x_, ws, mode, nq, np); }
 
-// Enqueue a ragged batched / precision search of nq device-resident queries
-// (not rotated) on stream s with its own workspace: no host synchronisation,
-// no index lock (the index is read-only while serving). Kernel wait timeouts
-// land in ws's error word. apply_tuned: take the autotuned setting of this
-// batch shape (else ws's own setting is used, as a captured plan fixes it).
-uint64_t server_enqueue(e8qc_index* x, Workspace& ws, int mode, const float* q_dev, size_t nq,
-                        const uint32_t* k_dev, const uint32_t* np_dev, size_t k_max, size_t np_max,
-                        uint32_t* ids_dev, float* d_dev, cudaStream_t s, bool apply_tuned) {
-    const size_t np = std::min(np_max, x->nlist);
-    ws.ensure_queries(nq, x->pd);
-    ws.ensure_err();
-    float* rq = ws.rq.as<float>();
-    if (apply_tuned) apply_tuning(x, ws, mode, nq, np);
-    uint64_t launches = launch_rotate(x->view, q_dev, static_cast<int>(nq), rq, s);
-    if (mode == E8QC_MODE_PRECISION)
-        launches += precision_search(x->view, ws, rq, nq, k_dev, np_dev, k_max, np, k_max, ids_dev, d_dev,
-                                     max_tiles_for(x, np) * 32, s);
-    else
-        launches += batched_search(x->view, ws, rq, nq, k_dev, np_dev, k_max, np, k_max, ids_dev, d_dev,
-                                   max_tiles_for(x, np), s);
-    return launches;
-}
+   private:
+    e8qc_index* x_;
+};
 
-// Autotune one batch shape with a caller's workspace (plans); returns the
-// chosen schedule / stages and leaves them set in ws.
-void plan_autotune(e8qc_index* x, Workspace& ws, int mode, size_t nq, size_t k, size_t np, cudaStream_t s,
-                   int* sched, int* stages) {
-    const TuneResult r = autotune_run(x, ws, mode, nq, k, np, s);
-    *sched = r.sched;
-    *stages = r.stages;
-}
+}  // namespace
 
-// The stored tuning of a batch shape (defaults when none) into ws.
-void plan_stored_tuning(e8qc_index* x, Workspace& ws, int mode, size_t nq, size_t np) {
-    apply_tuning(x, ws, mode, nq, np);
-}
+std::shared_ptr<SearchTarget> e8q_target(e8qc_index* x) { return std::make_shared<E8qTarget>(x); }
 
 // Read-only view of a built index for the no-allocation plain search
 // (noalloc.cu). Throws like every entry point when the index is not built.

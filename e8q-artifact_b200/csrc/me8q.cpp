@@ -16,6 +16,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -23,6 +25,7 @@
 #include "e8qc.h"
 #include "internal.h"
 #include "me8q.h"
+#include "serve_target.h"
 #include "workspace.h"
 
 namespace e8qc {
@@ -192,6 +195,8 @@ struct e8qc_me8q {
     Me8qView view{};
     Workspace ws;
     std::mutex mu;
+    std::map<uint64_t, int> tuned;  // work-queue schedule per (log2 nq, log2 nprobe)
+    std::mutex tune_mu;
     size_t memory_bytes() const {
         return runs_d.bytes + chunks_d.bytes + levels.bytes + signs.bytes + cen_pad.bytes + cen_rot.bytes + cn2.bytes +
                tile_begin_d.bytes + list_len_d.bytes + list_order_d.bytes + list_of_tile_d.bytes + ids.bytes +
@@ -440,7 +445,126 @@ void build(e8qc_me8q* x, const float* data, size_t n, const float* centroids, si
     x->built = true;
 }
 
+uint64_t tune_key(size_t nq, size_t np) {
+    auto lg = [](size_t v) {
+        uint64_t l = 0;
+        while ((size_t(1) << (l + 1)) <= v) ++l;
+        return l;
+    };
+    return (lg(nq) << 8) | lg(np);
+}
+
+int stored_sched(e8qc_me8q* x, size_t nq, size_t np) {
+    std::lock_guard<std::mutex> lock(x->tune_mu);
+    auto it = x->tuned.find(tune_key(nq, np));
+    return it == x->tuned.end() ? 0 : it->second;
+}
+
+// Rotate nq device queries and run the grouped exact scan; no host
+// synchronisation (k_arr / np_arr may be NULL for uniform k / nprobe).
+uint64_t enqueue_search(e8qc_me8q* x, Workspace& ws, const float* q_dev, size_t nq, const uint32_t* k_arr,
+                        const uint32_t* np_arr, size_t k, size_t np, size_t out_stride, uint32_t* ids_d, float* d_d,
+                        cudaStream_t s) {
+    ws.ensure_queries(nq, x->pd);
+    ws.ensure_err();
+    launch_me8q_prep(q_dev, x->dim, static_cast<int>(x->dim), static_cast<int>(x->pd), nullptr, nullptr, x->view, 0,
+                     nq, ws.rq.as<float>(), nullptr, nullptr, s);
+    return 1 + static_cast<uint64_t>(me8q_grouped_search(x->view, ws, ws.rq.as<float>(), nq, k_arr, np_arr, k, np,
+                                                         out_stride, ids_d, d_d, s));
+}
+
+class Me8qTarget final : public SearchTarget {
+   public:
+    explicit Me8qTarget(e8qc_me8q* x) : x_(x) {
+        require_built(x, "serve");
+        dim = x->dim;
+        nlist = x->nlist;
+        device = x->device;
+    }
+    void check_mode(int mode) const override {
+        if (mode != E8QC_MODE_BATCHED)
+            fail(E8QC_EINVAL, "ME8Q plans and servers run E8QC_MODE_BATCHED (the grouped exact scan)");
+    }
+    void prepare(int) override {}
+    size_t bytes(int, size_t nq, size_t k_max, size_t np_max) const override {
+        const size_t np = std::min(np_max, x_->nlist), nl = x_->nlist;
+        const size_t npairs = nq * np;
+        size_t b = nq * (x_->dim * 4 + x_->pd * 4 + k_max * 8 + 8);  // queries, rotated queries, results, k/nprobe
+        b += nq * nl * 8 + nq * 4;                                    // route keys, norms
+        b += npairs * 12 + npairs * 8 + nl * 12;                      // probes, d2, positions; pair rows; counters
+        b += (npairs / 64 + nl + 1) * 16 + 32;                        // work items
+        b += npairs * k_max * 8;                                      // per-pair partial top-k
+        return b;
+    }
+    uint64_t enqueue(Workspace& ws, int, const float* q_dev, size_t nq, const uint32_t* k_dev, const uint32_t* np_dev,
+                     size_t k_max, size_t np_max, uint32_t* ids_dev, float* d_dev, cudaStream_t s,
+                     bool apply_tuned) override {
+        const size_t np = std::min(np_max, x_->nlist);
+        if (apply_tuned) ws.sched = stored_sched(x_, nq, np);
+        return enqueue_search(x_, ws, q_dev, nq, k_dev, np_dev, k_max, np, k_max, ids_dev, d_dev, s);
+    }
+    // The work-queue order (longest list first / list id order), timed on nq
+    // synthetic rotated queries (mixtures of two lists' rotated centroids).
+    void autotune(Workspace& ws, int, size_t nq, size_t k, size_t np, cudaStream_t s, int* sched,
+                  int* stages) override {
+        np = std::min(np, x_->nlist);
+        DevBuf rq, ids, d;
+        rq.alloc(nq * x_->pd * 4);
+        ids.alloc(nq * k * 4);
+        d.alloc(nq * k * 4);
+        launch_synth_queries(x_->view.base, static_cast<int>(nq), 0x5EEDull, rq.as<float>(), s);
+        ws.ensure_err();
+        cudaEvent_t e0, e1;
+        E8QC_CUDA(cudaEventCreate(&e0));
+        E8QC_CUDA(cudaEventCreate(&e1));
+        struct Ev {
+            cudaEvent_t a, b;
+            ~Ev() {
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+            }
+        } ev{e0, e1};
+        int best = 0;
+        double best_ms = 1e30;
+        for (int sc = 0; sc < 2; ++sc) {
+            ws.sched = sc;
+            auto run = [&] {
+                me8q_grouped_search(x_->view, ws, rq.as<float>(), nq, nullptr, nullptr, k, np, k, ids.as<uint32_t>(),
+                                    d.as<float>(), s);
+            };
+            run();  // warm-up: sizes buffers, sets kernel attributes
+            E8QC_CUDA(cudaEventRecord(e0, s));
+            for (int r = 0; r < 3; ++r) run();
+            E8QC_CUDA(cudaEventRecord(e1, s));
+            ws.check_error(s);
+            float ms = 0.0f;
+            E8QC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = sc;
+            }
+        }
+        ws.sched = best;
+        {
+            std::lock_guard<std::mutex> lock(x_->tune_mu);
+            x_->tuned[tune_key(nq, np)] = best;
+        }
+        *sched = best;
+        *stages = ws.stages;
+    }
+    void stored_tuning(Workspace& ws, int, size_t nq, size_t np) override {
+        ws.sched = stored_sched(x_, nq, std::min(np, x_->nlist));
+    }
+
+   private:
+    e8qc_me8q* x_;
+};
+
 }  // namespace
+
+namespace e8qc {
+std::shared_ptr<SearchTarget> me8q_target(e8qc_me8q* x) { return std::make_shared<Me8qTarget>(x); }
+}  // namespace e8qc
 
 extern "C" {
 
@@ -544,12 +668,8 @@ int e8qc_me8q_search(e8qc_me8q* x, const float* queries, size_t nq, size_t k, si
             ws.stage_d.ensure(nq * k * 4);
             d_d = ws.stage_d.as<float>();
         }
-        ws.ensure_queries(nq, x->pd);
-        ws.ensure_err();
-        launch_me8q_prep(qd, x->dim, static_cast<int>(x->dim), static_cast<int>(x->pd), nullptr, nullptr, x->view, 0, nq,
-                         ws.rq.as<float>(), nullptr, nullptr, s);
-        const int launches = 1 + me8q_grouped_search(x->view, ws, ws.rq.as<float>(), nq, nullptr, nullptr, k, np, k,
-                                                     ids_d, d_d, s);
+        ws.sched = stored_sched(x, nq, np);
+        const uint64_t launches = enqueue_search(x, ws, qd, nq, nullptr, nullptr, k, np, k, ids_d, d_d, s);
         if (!ids_dev) E8QC_CUDA(cudaMemcpyAsync(out_ids, ids_d, nq * k * 4, cudaMemcpyDeviceToHost, s));
         if (out_dists && !d_dev) E8QC_CUDA(cudaMemcpyAsync(out_dists, d_d, nq * k * 4, cudaMemcpyDeviceToHost, s));
         ws.check_error(s);
@@ -560,8 +680,60 @@ int e8qc_me8q_search(e8qc_me8q* x, const float* queries, size_t nq, size_t k, si
             E8QC_CUDA(cudaStreamSynchronize(s));
             stats->candidates = cntv[0];
             stats->survivors = cntv[0];
-            stats->launches = static_cast<uint64_t>(launches);
+            stats->launches = launches;
         }
+    });
+}
+
+int e8qc_me8q_search_ragged(e8qc_me8q* x, const float* queries, size_t nq, const uint32_t* k, const uint32_t* nprobe,
+                            size_t k_max, uint32_t* out_ids, float* out_dists, void* stream) {
+    return guarded([&] {
+        require_built(x, "search");
+        if (nq == 0) return;
+        if (!queries || !k || !nprobe || !out_ids) fail(E8QC_EINVAL, "null buffer");
+        if (k_max == 0 || k_max > static_cast<size_t>(kMaxK)) fail(E8QC_EINVAL, "k_max must be in [1, 128]");
+        if (is_device_ptr(k) || is_device_ptr(nprobe)) fail(E8QC_EINVAL, "k and nprobe must be host arrays");
+        size_t np_max = 1;
+        std::vector<uint32_t> kk(nq), nn(nq);
+        for (size_t i = 0; i < nq; ++i) {
+            if (k[i] == 0 || k[i] > k_max) fail(E8QC_EINVAL, "k must be in [1, k_max]");
+            if (nprobe[i] == 0) fail(E8QC_EINVAL, "nprobe must be positive");
+            kk[i] = k[i];
+            nn[i] = static_cast<uint32_t>(std::min<size_t>(nprobe[i], x->nlist));
+            np_max = std::max<size_t>(np_max, nn[i]);
+        }
+        std::lock_guard<std::mutex> lock(x->mu);
+        DeviceGuard g(x->device);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        Workspace& ws = x->ws;
+        const float* qd = queries;
+        if (!is_device_ptr(queries)) {
+            ws.stage_q.ensure(nq * x->dim * 4);
+            E8QC_CUDA(cudaMemcpyAsync(ws.stage_q.p, queries, nq * x->dim * 4, cudaMemcpyHostToDevice, s));
+            qd = ws.stage_q.as<float>();
+        }
+        ws.stage_k.ensure(nq * 4);
+        ws.stage_np.ensure(nq * 4);
+        E8QC_CUDA(cudaMemcpyAsync(ws.stage_k.p, kk.data(), nq * 4, cudaMemcpyHostToDevice, s));
+        E8QC_CUDA(cudaMemcpyAsync(ws.stage_np.p, nn.data(), nq * 4, cudaMemcpyHostToDevice, s));
+        const bool ids_dev = is_device_ptr(out_ids), d_dev = out_dists && is_device_ptr(out_dists);
+        uint32_t* ids_d = out_ids;
+        float* d_d = out_dists;
+        if (!ids_dev) {
+            ws.stage_ids.ensure(nq * k_max * 4);
+            ids_d = ws.stage_ids.as<uint32_t>();
+        }
+        if (!d_dev) {
+            ws.stage_d.ensure(nq * k_max * 4);
+            d_d = ws.stage_d.as<float>();
+        }
+        ws.sched = stored_sched(x, nq, np_max);
+        enqueue_search(x, ws, qd, nq, ws.stage_k.as<uint32_t>(), ws.stage_np.as<uint32_t>(), k_max, np_max, k_max,
+                       ids_d, d_d, s);
+        if (!ids_dev) E8QC_CUDA(cudaMemcpyAsync(out_ids, ids_d, nq * k_max * 4, cudaMemcpyDeviceToHost, s));
+        if (out_dists && !d_dev)
+            E8QC_CUDA(cudaMemcpyAsync(out_dists, d_d, nq * k_max * 4, cudaMemcpyDeviceToHost, s));
+        ws.check_error(s);
     });
 }
 

@@ -21,25 +21,18 @@
 
 #include "e8qc.h"
 #include "internal.h"
+#include "serve_target.h"
 #include "workspace.h"
 
 namespace e8qc {
 void set_last_error(const std::string& s);
 bool is_device_ptr(const void* p);
-void server_index_info(e8qc_index* x, size_t* dim, size_t* nlist, int* device);
-void server_prepare(e8qc_index* x, int mode);
-uint64_t server_enqueue(e8qc_index* x, Workspace& ws, int mode, const float* q_dev, size_t nq,
-                        const uint32_t* k_dev, const uint32_t* np_dev, size_t k_max, size_t np_max,
-                        uint32_t* ids_dev, float* d_dev, cudaStream_t s, bool apply_tuned);
-void plan_autotune(e8qc_index* x, Workspace& ws, int mode, size_t nq, size_t k, size_t np, cudaStream_t s,
-                   int* sched, int* stages);
-void plan_stored_tuning(e8qc_index* x, Workspace& ws, int mode, size_t nq, size_t np);
 }  // namespace e8qc
 
 using namespace e8qc;
 
 struct e8qc_plan {
-    e8qc_index* idx = nullptr;
+    std::shared_ptr<SearchTarget> target;
     int mode = 0, device = 0;
     size_t dim = 0, nlist = 0, max_q = 0, k_max = 0, np_max = 0;
     Workspace ws;
@@ -104,16 +97,18 @@ void plan_check(e8qc_plan* P, cudaStream_t s) { P->ws.check_error(s); }
 size_t plan_max_queries(const e8qc_plan* P) { return P->max_q; }
 
 // Create a plan (see e8qc_plan_create); throws on failure.
-e8qc_plan* plan_make(e8qc_index* idx, int mode, size_t max_q, size_t k_max, size_t np_max, bool autotune) {
-    if (mode != E8QC_MODE_BATCHED && mode != E8QC_MODE_PRECISION)
-        fail(E8QC_EINVAL, "plans cover E8QC_MODE_BATCHED and E8QC_MODE_PRECISION");
+e8qc_plan* plan_make(std::shared_ptr<SearchTarget> t, int mode, size_t max_q, size_t k_max, size_t np_max,
+                     bool autotune) {
+    t->check_mode(mode);
     if (max_q == 0) fail(E8QC_EINVAL, "max_queries must be positive");
     if (k_max == 0 || k_max > static_cast<size_t>(kMaxK)) fail(E8QC_EINVAL, "k_max must be in [1, 128]");
     if (np_max == 0) fail(E8QC_EINVAL, "nprobe_max must be positive");
     auto P = std::make_unique<e8qc_plan>();
-    P->idx = idx;
+    P->target = t;
     P->mode = mode;
-    server_index_info(idx, &P->dim, &P->nlist, &P->device);
+    P->dim = t->dim;
+    P->nlist = t->nlist;
+    P->device = t->device;
     P->max_q = max_q;
     P->k_max = k_max;
     P->np_max = std::min(np_max, P->nlist);
@@ -124,7 +119,7 @@ e8qc_plan* plan_make(e8qc_index* idx, int mode, size_t max_q, size_t k_max, size
         int d;
         ~Restore() { cudaSetDevice(d); }
     } restore{prev};
-    server_prepare(idx, mode);
+    t->prepare(mode);
     P->ws.device = P->device;
     E8QC_CUDA(cudaStreamCreateWithFlags(&P->cs, cudaStreamNonBlocking));
     E8QC_CUDA(cudaEventCreateWithFlags(&P->staged, cudaEventDisableTiming));
@@ -144,9 +139,9 @@ e8qc_plan* plan_make(e8qc_index* idx, int mode, size_t max_q, size_t k_max, size
     for (size_t n : sizes) {
         int sched = 0, stages = 6;
         if (autotune) {
-            plan_autotune(idx, P->ws, mode, n, k_max, P->np_max, s, &sched, &stages);
+            t->autotune(P->ws, mode, n, k_max, P->np_max, s, &sched, &stages);
         } else {
-            plan_stored_tuning(idx, P->ws, mode, n, P->np_max);
+            t->stored_tuning(P->ws, mode, n, P->np_max);
             sched = P->ws.sched;
             stages = P->ws.stages;
         }
@@ -161,8 +156,8 @@ e8qc_plan* plan_make(e8qc_index* idx, int mode, size_t max_q, size_t k_max, size
         E8QC_CUDA(cudaMemcpyAsync(P->k.p, P->hk, n * 4, cudaMemcpyHostToDevice, s));
         E8QC_CUDA(cudaMemcpyAsync(P->np.p, P->hnp, n * 4, cudaMemcpyHostToDevice, s));
         auto enqueue = [&] {
-            server_enqueue(idx, P->ws, mode, P->q.as<float>(), n, P->k.as<uint32_t>(), P->np.as<uint32_t>(), k_max,
-                           P->np_max, P->ids.as<uint32_t>(), P->d.as<float>(), s, false);
+            t->enqueue(P->ws, mode, P->q.as<float>(), n, P->k.as<uint32_t>(), P->np.as<uint32_t>(), k_max, P->np_max,
+                       P->ids.as<uint32_t>(), P->d.as<float>(), s, false);
         };
         enqueue();  // sizes the workspace, sets kernel attributes
         P->ws.check_error(s);
@@ -212,7 +207,15 @@ extern "C" int e8qc_plan_create(e8qc_index* idx, int mode, size_t max_queries, s
                                 int autotune, e8qc_plan** out) {
     return guard([&] {
         if (!idx || !out) fail(E8QC_EINVAL, "null argument");
-        *out = plan_make(idx, mode, max_queries, k_max, nprobe_max, autotune != 0);
+        *out = plan_make(e8q_target(idx), mode, max_queries, k_max, nprobe_max, autotune != 0);
+    });
+}
+
+extern "C" int e8qc_plan_create_me8q(e8qc_me8q* idx, size_t max_queries, size_t k_max, size_t nprobe_max,
+                                     int autotune, e8qc_plan** out) {
+    return guard([&] {
+        if (!idx || !out) fail(E8QC_EINVAL, "null argument");
+        *out = plan_make(me8q_target(idx), E8QC_MODE_BATCHED, max_queries, k_max, nprobe_max, autotune != 0);
     });
 }
 

@@ -31,14 +31,11 @@
 
 #include "e8qc.h"
 #include "internal.h"
+#include "serve_target.h"
 #include "workspace.h"
 
 namespace e8qc {
 void set_last_error(const std::string& s);
-void server_index_info(e8qc_index* x, size_t* dim, size_t* nlist, int* device);
-void server_prepare(e8qc_index* x, int mode);
-size_t search_bytes(const e8qc_index* x, int mode, size_t nq, size_t k_max, size_t np_max);
-e8qc_plan* plan_make(e8qc_index* idx, int mode, size_t max_q, size_t k_max, size_t np_max, bool autotune);
 void plan_enqueue(e8qc_plan* P, const float* queries, size_t nq, const uint32_t* k, const uint32_t* nprobe,
                   uint32_t* out_ids, float* out_dists, cudaStream_t s);
 void plan_check(e8qc_plan* P, cudaStream_t s);
@@ -90,7 +87,7 @@ struct Slot {
 }  // namespace
 
 struct e8qc_server {
-    e8qc_index* idx = nullptr;
+    std::shared_ptr<SearchTarget> target;
     e8qc_server_config cfg{};
     size_t dim = 0, nlist = 0;
     size_t max_admit = 0;  // largest batch the budget admits at (max_k, max_nprobe); the plans' size
@@ -160,7 +157,7 @@ void dispatcher_main(e8qc_server* S) {
         }
         S->free_slots.pop_front();
         sl.nq = nq;
-        sl.bytes = search_bytes(S->idx, S->cfg.mode, nq, S->cfg.max_k, S->cfg.max_nprobe);
+        sl.bytes = S->target->bytes(S->cfg.mode, nq, S->cfg.max_k, S->cfg.max_nprobe);
         sl.error = 0;
         sl.error_msg.clear();
         S->peak_bytes = std::max<uint64_t>(S->peak_bytes, sl.bytes);
@@ -247,59 +244,74 @@ int guard(const std::function<void()>& f) {
     }
 }
 
+e8qc_server* server_make(std::shared_ptr<SearchTarget> t, const e8qc_server_config* cfg) {
+    auto S = std::make_unique<e8qc_server>();
+    S->target = t;
+    if (cfg) S->cfg = *cfg;
+    t->check_mode(S->cfg.mode);
+    S->dim = t->dim;
+    S->nlist = t->nlist;
+    S->device = t->device;
+    if (S->cfg.max_batch_queries == 0) S->cfg.max_batch_queries = 4096;
+    if (S->cfg.max_k == 0) S->cfg.max_k = kMaxK;
+    if (S->cfg.max_k > static_cast<size_t>(kMaxK)) fail(E8QC_EINVAL, "max_k must be <= 128");
+    if (S->cfg.max_nprobe == 0 || S->cfg.max_nprobe > S->nlist) S->cfg.max_nprobe = S->nlist;
+    if (S->cfg.memory_budget == 0) S->cfg.memory_budget = size_t(4) << 30;
+    if (S->cfg.slots <= 0) S->cfg.slots = 2;
+    if (S->cfg.slots > 16) fail(E8QC_EINVAL, "at most 16 slots");
+    int prev = 0;
+    E8QC_CUDA(cudaGetDevice(&prev));
+    E8QC_CUDA(cudaSetDevice(S->device));
+    struct Restore {
+        int d;
+        ~Restore() { cudaSetDevice(d); }
+    } restore{prev};
+    t->prepare(S->cfg.mode);
+    const size_t B = S->cfg.max_batch_queries, K = S->cfg.max_k;
+    // the largest batch whose scratch at (max_k, max_nprobe) fits the budget
+    size_t nw = 1;
+    for (size_t step = B; step > 0; step >>= 1)
+        while (nw + step <= B &&
+               t->bytes(S->cfg.mode, nw + step, K, S->cfg.max_nprobe) <= S->cfg.memory_budget)
+            nw += step;
+    S->max_admit = nw;
+    for (int i = 0; i < S->cfg.slots; ++i) {
+        auto sl = std::make_unique<Slot>();
+        E8QC_CUDA(cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking));
+        E8QC_CUDA(cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming));
+        sl->hq.alloc(nw * S->dim);
+        sl->hk.alloc(nw);
+        sl->hnp.alloc(nw);
+        sl->hids.alloc(nw * K);
+        sl->hd.alloc(nw * K);
+        // captured graphs for batches of 64, 128, ... nw queries; the first
+        // slot autotunes each size, the others take the stored settings
+        sl->plan = plan_make(t, S->cfg.mode, nw, K, S->cfg.max_nprobe, i == 0);
+        S->free_slots.push_back(i);
+        S->slots.push_back(std::move(sl));
+    }
+    e8qc_server* raw = S.release();
+    raw->dispatcher = std::thread(dispatcher_main, raw);
+    raw->completer = std::thread(completer_main, raw);
+    return raw;
+}
+
 }  // namespace
 
 extern "C" int e8qc_server_start(e8qc_index* idx, const e8qc_server_config* cfg, e8qc_server** out) {
     return guard([&] {
         if (!idx || !out) fail(E8QC_EINVAL, "null argument");
-        auto S = std::make_unique<e8qc_server>();
-        S->idx = idx;
-        if (cfg) S->cfg = *cfg;
-        if (S->cfg.mode != E8QC_MODE_BATCHED && S->cfg.mode != E8QC_MODE_PRECISION)
-            fail(E8QC_EINVAL, "server mode must be E8QC_MODE_BATCHED or E8QC_MODE_PRECISION");
-        server_index_info(idx, &S->dim, &S->nlist, &S->device);
-        if (S->cfg.max_batch_queries == 0) S->cfg.max_batch_queries = 4096;
-        if (S->cfg.max_k == 0) S->cfg.max_k = kMaxK;
-        if (S->cfg.max_k > static_cast<size_t>(kMaxK)) fail(E8QC_EINVAL, "max_k must be <= 128");
-        if (S->cfg.max_nprobe == 0 || S->cfg.max_nprobe > S->nlist) S->cfg.max_nprobe = S->nlist;
-        if (S->cfg.memory_budget == 0) S->cfg.memory_budget = size_t(4) << 30;
-        if (S->cfg.slots <= 0) S->cfg.slots = 2;
-        if (S->cfg.slots > 16) fail(E8QC_EINVAL, "at most 16 slots");
-        int prev = 0;
-        E8QC_CUDA(cudaGetDevice(&prev));
-        E8QC_CUDA(cudaSetDevice(S->device));
-        struct Restore {
-            int d;
-            ~Restore() { cudaSetDevice(d); }
-        } restore{prev};
-        server_prepare(idx, S->cfg.mode);
-        const size_t B = S->cfg.max_batch_queries, K = S->cfg.max_k;
-        // the largest batch whose scratch at (max_k, max_nprobe) fits the budget
-        size_t nw = 1;
-        for (size_t step = B; step > 0; step >>= 1)
-            while (nw + step <= B &&
-                   search_bytes(idx, S->cfg.mode, nw + step, K, S->cfg.max_nprobe) <= S->cfg.memory_budget)
-                nw += step;
-        S->max_admit = nw;
-        for (int i = 0; i < S->cfg.slots; ++i) {
-            auto sl = std::make_unique<Slot>();
-            E8QC_CUDA(cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking));
-            E8QC_CUDA(cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming));
-            sl->hq.alloc(nw * S->dim);
-            sl->hk.alloc(nw);
-            sl->hnp.alloc(nw);
-            sl->hids.alloc(nw * K);
-            sl->hd.alloc(nw * K);
-            // captured graphs for batches of 64, 128, ... nw queries; the first
-            // slot autotunes each size, the others take the stored settings
-            sl->plan = plan_make(idx, S->cfg.mode, nw, K, S->cfg.max_nprobe, i == 0);
-            S->free_slots.push_back(i);
-            S->slots.push_back(std::move(sl));
-        }
-        e8qc_server* raw = S.release();
-        raw->dispatcher = std::thread(dispatcher_main, raw);
-        raw->completer = std::thread(completer_main, raw);
-        *out = raw;
+        *out = server_make(e8q_target(idx), cfg);
+    });
+}
+
+extern "C" int e8qc_server_start_me8q(e8qc_me8q* idx, const e8qc_server_config* cfg, e8qc_server** out) {
+    return guard([&] {
+        if (!idx || !out) fail(E8QC_EINVAL, "null argument");
+        e8qc_server_config c{};
+        if (cfg) c = *cfg;
+        c.mode = E8QC_MODE_BATCHED;
+        *out = server_make(me8q_target(idx), &c);
     });
 }
 

@@ -216,6 +216,12 @@ int e8qc_me8q_build(e8qc_me8q* idx, const float* data, size_t n, const float* ce
  * distances, ascending; k <= 128. Host or device pointers. */
 int e8qc_me8q_search(e8qc_me8q* idx, const float* queries, size_t nq, size_t k, size_t nprobe,
                      uint32_t* out_ids, float* out_dists, e8qc_stats* stats, void* stream);
+/* Serving form (an addition of this library): per-query k[i] <= k_max and
+ * nprobe[i] (host arrays); output rows k_max wide, padded with UINT32_MAX /
+ * +inf. */
+int e8qc_me8q_search_ragged(e8qc_me8q* idx, const float* queries, size_t nq, const uint32_t* k,
+                            const uint32_t* nprobe, size_t k_max, uint32_t* out_ids, float* out_dists,
+                            void* stream);
 /* Me8qIndex::Estimate (me8q_measure.cpp:41-66); E8QC_ERANGE for an unknown id. */
 int e8qc_me8q_estimate(e8qc_me8q* idx, const float* query, uint32_t id, float* out);
 int e8qc_me8q_info(const e8qc_me8q* idx, e8qc_me8q_meta* out);
@@ -254,6 +260,10 @@ int e8qc_e8q_autotune(e8qc_index* idx, int mode, size_t nq, size_t k, size_t npr
 typedef struct e8qc_plan e8qc_plan;
 int e8qc_plan_create(e8qc_index* idx, int mode, size_t max_queries, size_t k_max, size_t nprobe_max, int autotune,
                      e8qc_plan** out);
+/* The same over an ME8Q index: the grouped exact scan (E8QC_MODE_BATCHED);
+ * autotune picks the work-queue order per batch size. */
+int e8qc_plan_create_me8q(e8qc_me8q* idx, size_t max_queries, size_t k_max, size_t nprobe_max, int autotune,
+                          e8qc_plan** out);
 int e8qc_plan_run(e8qc_plan* plan, const float* queries, size_t nq, const uint32_t* k, const uint32_t* nprobe,
                   uint32_t* out_ids, float* out_dists, void* stream);
 int e8qc_plan_destroy(e8qc_plan* plan);
@@ -290,6 +300,9 @@ typedef struct e8qc_server_stats {
     uint64_t peak_batch_bytes;              /* largest admitted batch estimate */
 } e8qc_server_stats;
 int e8qc_server_start(e8qc_index* idx, const e8qc_server_config* cfg, e8qc_server** out);
+/* The serving loop over an ME8Q index (cfg->mode is ignored: the grouped
+ * exact scan); submit / poll / stats / stop as above. */
+int e8qc_server_start_me8q(e8qc_me8q* idx, const e8qc_server_config* cfg, e8qc_server** out);
 /* Copy nq host queries (dim floats each) into a new request; *request_id
  * identifies it. E8QC_EINVAL for bad k / nprobe, E8QC_ENOMEM when the request
  * alone exceeds the memory budget or max_batch_queries, E8QC_ESTATE after stop. */
