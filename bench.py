@@ -77,8 +77,8 @@ def parse():
     ap.add_argument("--me8q-n", type=int, default=10_000_000)
     ap.add_argument("--me8q-dim", type=int, default=768)
     ap.add_argument("--me8q-nlist", type=int, default=4096)
-    ap.add_argument("--me8q-avg-bits", type=float, default=4.0)
-    ap.add_argument("--me8q-nprobes", default="16,32,64,128")
+    ap.add_argument("--me8q-avg-bits", default="4,6", help="comma-separated avg_bits values")
+    ap.add_argument("--me8q-nprobes", default="32,64,128,256,512")
     return ap.parse_args()
 
 
@@ -379,11 +379,14 @@ def gen_me8q(a, device):
 
 
 def me8q_leg(a, e8qlib, dev, local, stream):
-    """ME8Q index (mixed-rate) at the ME8Q workload: build time, recall@10 per
-    nprobe against an FP64 brute force over the raw vectors, batched QPS at
-    the smallest nprobe with recall >= 0.95, single-query latency, and
-    open-loop serving with k in {10, 100} and nprobe drawn from the values
-    that meet the recall bar."""
+    """ME8Q index (mixed-rate) at the ME8Q workload, for each avg_bits of
+    --me8q-avg-bits: build time, recall@10 per nprobe against an FP64 brute
+    force over the raw vectors (exact grouped scan and the int8 tensor-core
+    precision mode, beside the IVF ceiling), device-resident QPS of both modes
+    at the smallest nprobe whose precision recall is >= 0.95 (else the
+    largest), single-query latency; then open-loop serving (precision mode,
+    k in {10, 100}, nprobe drawn from the values >= that nprobe) on the first
+    rate that meets the recall bar (else the last)."""
     import torch
 
     sp = stream.cuda_stream
@@ -395,93 +398,118 @@ def me8q_leg(a, e8qlib, dev, local, stream):
     del x
     torch.cuda.empty_cache()
     n, d = xp.shape
-    idx = e8qlib.Me8qIndex(d, a.me8q_avg_bits, a.seed, device=local)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    idx.build_ptr(xp.data_ptr(), n, cen.data_ptr(), cen.shape[0], lab.data_ptr(), var.data_ptr(), True, "", 0.0, sp)
-    torch.cuda.synchronize()
-    build_s = time.perf_counter() - t0
-    del xp
-    torch.cuda.empty_cache()
+    nl = cen.shape[0]
     nb = a.batch
     oi = torch.empty(nb, 100, dtype=torch.int32, device=dev)
     od = torch.empty(nb, 100, dtype=torch.float32, device=dev)
-    sweep = []
-    for npb in [int(t) for t in a.me8q_nprobes.split(",") if t]:
+    nbat = max(1, a.pool // nb)
+    gtl = lab.long()[torch.from_numpy(gt.astype(np.int64)).to(dev)]
+    qd = qp[:a.gt]
+    cd = (qd * qd).sum(1, keepdim=True) + (cen * cen).sum(1)[None, :] - 2.0 * qd @ cen.T
+
+    def recall(idx, npb, mode):
         ids = np.zeros((a.gt, 10), np.uint32)
         for i in range(0, a.gt, nb):
             b = min(nb, a.gt - i)
-            idx.search_ptr(qp[i:i + b].data_ptr(), b, 10, npb, oi.data_ptr(), od.data_ptr(), sp)
+            idx.search_ptr(qp[i:i + b].data_ptr(), b, 10, npb, oi.data_ptr(), od.data_ptr(), mode, sp)
             torch.cuda.synchronize()
             ids[i:i + b] = oi.view(-1)[:b * 10].view(b, 10).cpu().numpy().view(np.uint32)
-        sweep.append({"nprobe": npb, "recall_at_10": round(recall_at(ids, gt, 10), 4)})
-    ok = [r for r in sweep if r["recall_at_10"] >= 0.95]
-    npb = (ok[0] if ok else sweep[-1])["nprobe"]
-    nbat = max(1, a.pool // nb)
+        return recall_at(ids, gt, 10)
 
-    def step(i):
-        qi = qp[(i % nbat) * nb:(i % nbat) * nb + nb]
-        return idx.search_ptr(qi.data_ptr(), nb, 10, npb, oi.data_ptr(), od.data_ptr(), sp)
+    def qps(idx, npb, mode):
+        def step(i):
+            qi = qp[(i % nbat) * nb:(i % nbat) * nb + nb]
+            return idx.search_ptr(qi.data_ptr(), nb, 10, npb, oi.data_ptr(), od.data_ptr(), mode, sp)
 
-    for i in range(a.warmup):
-        step(i)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    launches = 0
-    for i in range(a.steps):
-        launches += step(a.warmup + i)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    qps = a.steps * nb / (ms / 1000.0)
-    # one query per call (device-resident), median of 64 calls
-    lat = []
-    for i in range(72):
-        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s0.record(stream)
-        idx.search_ptr(qp[i].data_ptr(), 1, 10, npb, oi.data_ptr(), od.data_ptr(), sp)
-        s1.record(stream)
+        for i in range(a.warmup):
+            step(i)
         torch.cuda.synchronize()
-        if i >= 8:
-            lat.append(s0.elapsed_time(s1))
-    single_ms = statistics.median(lat)
-    # algorithmic bytes of the scan per query: codes + (coef, h2) of every
-    # probed vector, bits_per_dim * dim / 8 bytes each
-    bytes_per_vec = idx.bits_per_dim * d / 8.0
-    serving = []
-    if not a.no_serve:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        launches = 0
+        for i in range(a.steps):
+            launches += step(a.warmup + i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        return a.steps * nb / (ms / 1000.0), ms / a.steps, launches
+
+    rates = []
+    serve_idx, serve_np = None, None
+    avgs = [float(t) for t in str(a.me8q_avg_bits).split(",") if t]
+    for ai, avg in enumerate(avgs):
+        idx = e8qlib.Me8qIndex(d, avg, a.seed, device=local)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        idx.build_ptr(xp.data_ptr(), n, cen.data_ptr(), nl, lab.data_ptr(), var.data_ptr(), True, "", 0.0, sp)
+        torch.cuda.synchronize()
+        build_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        idx.search_ptr(qp.data_ptr(), 1, 10, 1, oi.data_ptr(), od.data_ptr(), "precision", sp)  # proxy plane
+        torch.cuda.synchronize()
+        proxy_s = time.perf_counter() - t0
+        sweep = []
+        for npb in [int(t) for t in a.me8q_nprobes.split(",") if t]:
+            probed = torch.topk(cd, min(npb, nl), dim=1, largest=False).indices
+            ceiling = (gtl[:, :, None] == probed[:, None, :]).any(-1).float().mean().item()
+            sweep.append({"nprobe": npb, "recall_precision": round(recall(idx, npb, "precision"), 4),
+                          "recall_exact": round(recall(idx, npb, "batched"), 4), "ivf_ceiling": round(ceiling, 4)})
+        ok = [r for r in sweep if r["recall_precision"] >= 0.95]
+        npb = (ok[0] if ok else sweep[-1])["nprobe"]
+        pq, pms, pl = qps(idx, npb, "precision")
+        eq, ems, _ = qps(idx, npb, "batched")
+        lat = []
+        for i in range(72):
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            idx.search_ptr(qp[i].data_ptr(), 1, 10, npb, oi.data_ptr(), od.data_ptr(), "precision", sp)
+            s1.record(stream)
+            torch.cuda.synchronize()
+            if i >= 8:
+                lat.append(s0.elapsed_time(s1))
+        rates.append({"avg_bits": avg, "plan": [list(p) for p in idx.plan], "bits_per_dim": round(idx.bits_per_dim, 3),
+                      "memory_bytes": idx.memory_bytes, "build_s": round(build_s, 2),
+                      "proxy_build_s": round(proxy_s, 2), "recall_sweep": sweep, "nprobe": npb,
+                      "recall_at_10": [r["recall_precision"] for r in sweep if r["nprobe"] == npb][0],
+                      "qps": round(pq, 1), "ms_per_step": round(pms, 3), "gpu_launches": int(pl),
+                      "exact_qps": round(eq, 1), "exact_ms_per_step": round(ems, 3),
+                      "single_query_ms": round(statistics.median(lat), 4)})
+        if serve_idx is None and (ok or ai == len(avgs) - 1):
+            serve_idx, serve_np = idx, npb
+            rates[-1]["served"] = True
+        else:
+            del idx
+        torch.cuda.empty_cache()
+    del xp
+    torch.cuda.empty_cache()
+    serving = None
+    if not a.no_serve and serve_idx is not None:
         qh = torch.empty(a.pool, d, dtype=torch.float32, pin_memory=True)
         qh.copy_(qp.cpu())
         qn = qh.numpy()
-        grid = [p for p in (16, 32, 64, 128, 256, 512) if p >= npb]
+        grid = [p for p in (16, 32, 64, 128, 256, 512) if p >= serve_np] or [serve_np]
         rng = np.random.default_rng(a.seed + 11)
         # capacity of the mixed load: one ragged batch of 4,096 queries
         kk = rng.choice([10, 100], nb).astype(np.uint32)
         pp = rng.choice(grid, nb).astype(np.uint32)
-        idx.search_ragged(qn[:nb], kk, pp, 100)
+        serve_idx.search_ragged(qn[:nb], kk, pp, 100, mode="precision")
         c0 = time.perf_counter()
-        idx.search_ragged(qn[:nb], kk, pp, 100)
+        serve_idx.search_ragged(qn[:nb], kk, pp, 100, mode="precision")
         cap = nb / (time.perf_counter() - c0)
+        loads = []
         for frac in [float(f) for f in a.serve_loads.split(",") if f]:
-            st = serve_open_loop(e8qlib, idx, "batched", qn, [10, 100], grid, frac * cap, a.serve_seconds,
+            st = serve_open_loop(e8qlib, serve_idx, "precision", qn, [10, 100], grid, frac * cap, a.serve_seconds,
                                  a.seed + 13, a.batch)
-            serving.append({"offered_qps": st["offered_qps"], "achieved_qps": round(st["qps"], 1),
-                            "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
-                            "max_ms": round(st["max_ms"], 3), "requests": st["requests"],
-                            "mean_batch_queries": round(st["mean_batch_queries"], 1)})
-        serving = {"k": [10, 100], "nprobe": grid, "mixed_batch_capacity_qps": round(cap, 1), "loads": serving}
+            loads.append({"offered_qps": st["offered_qps"], "achieved_qps": round(st["qps"], 1),
+                          "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
+                          "max_ms": round(st["max_ms"], 3), "requests": st["requests"],
+                          "mean_batch_queries": round(st["mean_batch_queries"], 1)})
+        serving = {"mode": "precision", "k": [10, 100], "nprobe": grid, "mixed_batch_capacity_qps": round(cap, 1),
+                   "loads": loads}
     out = {"workload": (f"ME8Q IVF search, {n // 1000}k x {d}-d unit vectors (spectrum i^-0.8, Haar rotation, "
-                        f"full-rank PCA), {cen.shape[0]} lists (3 Lloyd steps), avg_bits={a.me8q_avg_bits}, "
-                        f"k=10, query batch {nb}"),
-           "plan": [list(p) for p in idx.plan], "bits_per_dim": round(idx.bits_per_dim, 3),
-           "memory_bytes": idx.memory_bytes, "gen_s": round(gen_s, 2), "build_s": round(build_s, 2),
-           "recall_sweep": sweep, "nprobe": npb, "qps": round(qps, 1), "ms_per_step": round(ms / a.steps, 3),
-           "gpu_launches": int(launches), "single_query_ms": round(single_ms, 4),
-           "scan_bytes_per_vector": round(bytes_per_vec, 1),
-           "algo_gbs": round(qps * npb * (n / cen.shape[0]) * bytes_per_vec / 1e9, 1),
-           "serving": serving}
-    del idx, qp, q, cen, lab, var
+                        f"full-rank PCA), {nl} lists (3 Lloyd steps), k=10, query batch {nb}"),
+           "gen_s": round(gen_s, 2), "rates": rates, "serving": serving}
+    del serve_idx, qp, q, cen, lab, var
     torch.cuda.empty_cache()
     return out
 
@@ -573,10 +601,13 @@ def main():
     peak = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
     kernel = {"plain": "scan_plain_kernel", "batched": "batched_scan_kernel",
               "precision": "precision_scan_kernel"}[a.path]
+    item_per_launch = prof["item_bytes"] / max(1, prof["scan_launches"])
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": None, "kernel": kernel,
                 "algo_bytes_per_launch": int(algo_per_launch),
-                "launch_us": round(t_launch * 1e6, 2), "peak_kind": pk_kind}
+                "launch_us": round(t_launch * 1e6, 2), "peak_kind": pk_kind,
+                "item_bytes_per_launch": int(item_per_launch),
+                "item_gbs": round(item_per_launch / t_launch / 1e9, 1) if t_launch > 0 else 0.0}
     if a.path == "precision":
         # the scan streams int8 proxy rows + (g1, h3) per vector of each work
         # item and writes a 4-byte proxy distance per (query, vector) pair: its

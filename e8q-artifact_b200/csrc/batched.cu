@@ -271,7 +271,7 @@ __global__ void items_kernel(const uint32_t* __restrict__ list_cnt, const uint32
             for (uint32_t t = 0; t < nit; ++t) {
                 const uint32_t idx = ibase + t;
                 if (static_cast<int>(idx) < item_cap)
-                    items[idx] = make_uint4(L, pbase + t * qt, min(qt, cnt - t * qt), 0u);
+                    items[idx] = make_uint4(L, pbase + t * qt, min(qt, cnt - t * qt), t);  // w: item index within its list
             }
         }
         __syncthreads();
@@ -363,6 +363,7 @@ __global__ void __launch_bounds__(kBT) batched_scan_kernel(
         if (tid == 0) {
             atomicAdd(cand_count, static_cast<unsigned long long>(len) * m);  // (query, vector) pairs
             atomicAdd(cand_count + 1, static_cast<unsigned long long>(len));  // vectors read
+            if (item.w == 0) atomicAdd(cand_count + 2, static_cast<unsigned long long>(len));  // once per list
         }
         for (uint32_t v0 = 0; v0 < len; v0 += kVT) {
             float acc[4][8];
@@ -566,6 +567,7 @@ __global__ void __launch_bounds__(kBT) me8q_scan_kernel(
         if (tid == 0) {
             atomicAdd(cand_count, static_cast<unsigned long long>(len) * m);
             atomicAdd(cand_count + 1, static_cast<unsigned long long>(len));
+            if (item.w == 0) atomicAdd(cand_count + 2, static_cast<unsigned long long>(len));
         }
         for (uint32_t v0 = 0; v0 < len; v0 += kVT) {
             float acc[4][8];
@@ -768,7 +770,7 @@ int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t n
     ws.b_off.ensure(static_cast<size_t>(nlist) * 4);
     ws.b_fill.ensure(static_cast<size_t>(nlist) * 4);
     ws.b_items.ensure(item_cap * 16);
-    ws.b_nitems.ensure(32);
+    ws.b_nitems.ensure(48);
     ws.b_part_d.ensure(npairs * part_width * 4);
     ws.b_part_id.ensure(npairs * part_width * 4);
     int launches = 0;
@@ -779,7 +781,7 @@ int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t n
                                         ws.b_keys.as<uint64_t>());
     ++launches;
     E8QC_CUDA(cudaMemsetAsync(ws.b_cnt.p, 0, static_cast<size_t>(nlist) * 4, s));
-    E8QC_CUDA(cudaMemsetAsync(ws.b_nitems.p, 0, 32, s));  // [0] n_items, [1] head, [2..5] pair/vector counts
+    E8QC_CUDA(cudaMemsetAsync(ws.b_nitems.p, 0, 48, s));  // [0] n_items, [1] head, [2..7] pair / vector / list-vector counts
     const size_t sel_smem = static_cast<size_t>(nlist) * 8;
     if (sel_smem > 200 * 1024) fail(E8QC_EINVAL, "batched route supports at most 25600 lists");
     {

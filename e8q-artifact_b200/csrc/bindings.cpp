@@ -54,6 +54,14 @@ int mode_of(const std::string& m) {
     throw std::invalid_argument("mode must be 'plain', 'batched' or 'precision'");
 }
 
+// ME8Q search modes: the grouped exact scan, or int8 tensor-core candidates
+// with exact rescoring.
+int me8q_mode(const std::string& m) {
+    if (m == "batched") return E8QC_MODE_BATCHED;
+    if (m == "precision") return E8QC_MODE_PRECISION;
+    throw std::invalid_argument("ME8Q modes are 'batched' and 'precision'");
+}
+
 class E8qIndex {
    public:
     E8qIndex(size_t dim, size_t nbits, uint64_t seed, int device)
@@ -224,6 +232,8 @@ class E8qIndex {
         d["algo_bytes"] = p.algo_bytes;
         d["queries"] = p.queries;
         d["list_vectors"] = p.list_vectors;
+        d["list_once"] = p.list_once;
+        d["item_bytes"] = p.item_bytes;
         return d;
     }
 
@@ -357,19 +367,22 @@ class Me8qIndex {
 
     // Device-resident search on raw CUDA pointers; returns the launch count.
     uint64_t search_ptr(uintptr_t queries, size_t nq, size_t k, size_t nprobe, uintptr_t out_ids, uintptr_t out_dists,
-                        uintptr_t stream) {
+                        const std::string& mode, uintptr_t stream) {
         require("search");
+        const int md = me8q_mode(mode);
         e8qc_stats st{};
         py::gil_scoped_release nogil;
-        check(e8qc_me8q_search(idx_, reinterpret_cast<const float*>(queries), nq, k, nprobe,
-                               reinterpret_cast<uint32_t*>(out_ids), reinterpret_cast<float*>(out_dists), &st,
-                               reinterpret_cast<void*>(stream)));
+        check(e8qc_me8q_search_mode(idx_, reinterpret_cast<const float*>(queries), nq, k, nprobe, md,
+                                    reinterpret_cast<uint32_t*>(out_ids), reinterpret_cast<float*>(out_dists), &st,
+                                    reinterpret_cast<void*>(stream)));
         return st.launches;
     }
 
-    py::tuple search(py::handle queries, size_t k, size_t nprobe, size_t /*num_threads*/, bool return_stats) {
+    py::tuple search(py::handle queries, size_t k, size_t nprobe, size_t /*num_threads*/, bool return_stats,
+                     const std::string& mode) {
         auto q = ensure_nd<float>(queries, "queries", 2);
         require("search");
+        const int md = me8q_mode(mode);
         if (static_cast<size_t>(q.shape(1)) != dim_)
             throw std::invalid_argument("query dimension does not match index dim");
         if (k == 0) throw std::invalid_argument("k must be positive");
@@ -385,8 +398,9 @@ class Me8qIndex {
         e8qc_stats st{};
         {
             py::gil_scoped_release nogil;
-            if (nq > 0) check(e8qc_me8q_search(idx_, q.data(), nq, k, nprobe, ip, dp, return_stats ? &st : nullptr,
-                                               nullptr));
+            if (nq > 0)
+                check(e8qc_me8q_search_mode(idx_, q.data(), nq, k, nprobe, md, ip, dp, return_stats ? &st : nullptr,
+                                            nullptr));
         }
         if (!return_stats) return py::make_tuple(ids, dists);
         py::dict d;
@@ -449,7 +463,9 @@ class Me8qIndex {
     }
 
     // Serving form: per-query k and nprobe; rows padded to k_max.
-    py::tuple search_ragged(py::handle queries, py::handle k, py::handle nprobe, size_t k_max) {
+    py::tuple search_ragged(py::handle queries, py::handle k, py::handle nprobe, size_t k_max,
+                            const std::string& mode) {
+        const int md = me8q_mode(mode);
         auto q = ensure_nd<float>(queries, "queries", 2);
         auto ka = ensure_nd<uint32_t>(k, "k", 1);
         auto na = ensure_nd<uint32_t>(nprobe, "nprobe", 1);
@@ -464,8 +480,8 @@ class Me8qIndex {
         {
             py::gil_scoped_release nogil;
             if (nq > 0)
-                check(e8qc_me8q_search_ragged(idx_, q.data(), nq, ka.data(), na.data(), k_max, ids.mutable_data(),
-                                              dists.mutable_data(), nullptr));
+                check(e8qc_me8q_search_ragged(idx_, q.data(), nq, ka.data(), na.data(), k_max, md,
+                                              ids.mutable_data(), dists.mutable_data(), nullptr));
         }
         return py::make_tuple(ids, dists);
     }
@@ -503,10 +519,10 @@ class Plan {
         if (py::isinstance<Me8qIndex>(index)) {
             Me8qIndex& mx = index.cast<Me8qIndex&>();
             dim_ = mx.dim();
-            if (!mode.empty() && mode != "batched") throw std::invalid_argument("ME8Q plans run 'batched'");
+            const int md = me8q_mode(mode.empty() ? std::string("batched") : mode);
             e8qc_me8q* h = mx.handle("plan");
             py::gil_scoped_release nogil;
-            check(e8qc_plan_create_me8q(h, max_queries, k_max, nprobe_max, autotune ? 1 : 0, &plan_));
+            check(e8qc_plan_create_me8q(h, md, max_queries, k_max, nprobe_max, autotune ? 1 : 0, &plan_));
             return;
         }
         E8qIndex& ix = index.cast<E8qIndex&>();
@@ -571,8 +587,7 @@ class Server {
         if (py::isinstance<Me8qIndex>(index)) {
             Me8qIndex& mx = index.cast<Me8qIndex&>();
             dim_ = mx.dim();
-            if (!mode.empty() && mode != "batched") throw std::invalid_argument("the ME8Q server runs 'batched'");
-            c.mode = E8QC_MODE_BATCHED;
+            c.mode = me8q_mode(mode.empty() ? std::string("batched") : mode);
             e8qc_me8q* h = mx.handle("serve");
             py::gil_scoped_release nogil;
             check(e8qc_server_start_me8q(h, &c, &srv_));
@@ -739,16 +754,17 @@ PYBIND11_MODULE(_e8qlib, m) {
              py::arg("num_threads") = 1, py::arg("variance") = py::none(), py::arg("drop_energy") = true,
              py::arg("prune_alpha") = 0.0F, py::arg("plan_spec") = "", py::arg("extra_budget_bits") = 0.0)
         .def("search", &e8qb200::Me8qIndex::search, py::arg("queries"), py::arg("k"), py::arg("nprobe"),
-             py::arg("num_threads") = 1, py::arg("return_stats") = false)
+             py::arg("num_threads") = 1, py::arg("return_stats") = false, py::arg("mode") = "batched")
         .def("estimate", &e8qb200::Me8qIndex::estimate, py::arg("query"), py::arg("id"))
         .def("export_codes", &e8qb200::Me8qIndex::export_codes)
         .def("search_ragged", &e8qb200::Me8qIndex::search_ragged, py::arg("queries"), py::arg("k"),
-             py::arg("nprobe"), py::arg("k_max"))
+             py::arg("nprobe"), py::arg("k_max"), py::arg("mode") = "batched")
         .def("build_ptr", &e8qb200::Me8qIndex::build_ptr, py::arg("data"), py::arg("n"), py::arg("centroids"),
              py::arg("nlist"), py::arg("cluster_ids"), py::arg("variance") = 0, py::arg("drop_energy") = true,
              py::arg("plan_spec") = "", py::arg("extra_budget_bits") = 0.0, py::arg("stream") = 0)
         .def("search_ptr", &e8qb200::Me8qIndex::search_ptr, py::arg("queries"), py::arg("nq"), py::arg("k"),
-             py::arg("nprobe"), py::arg("out_ids"), py::arg("out_dists"), py::arg("stream") = 0)
+             py::arg("nprobe"), py::arg("out_ids"), py::arg("out_dists"), py::arg("mode") = "batched",
+             py::arg("stream") = 0)
         .def_property_readonly("dim", &e8qb200::Me8qIndex::dim)
         .def_property_readonly("avg_bits", &e8qb200::Me8qIndex::avg_bits)
         .def_property_readonly("is_built", &e8qb200::Me8qIndex::is_built)

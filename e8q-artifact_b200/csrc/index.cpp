@@ -198,6 +198,9 @@ void plain_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size_
             x->prof.scan_ms += ms;
             x->prof.candidates += cand;
             x->prof.algo_bytes += cand * (static_cast<uint64_t>(x->bits) * x->pd / 8 + 8);
+            x->prof.item_bytes += cand * (static_cast<uint64_t>(x->bits) * x->pd / 8 + 8);
+            x->prof.list_vectors += cand;
+            x->prof.list_once += cand;
             x->prof.queries += 1;
         }
     }
@@ -314,8 +317,8 @@ uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, con
     else
         launches += batched_search(x->view, ws, rq, nq, k_arr, np_arr, k, np, k, ids_d, d_d, max_tiles_for(x, np), s);
     if (x->profiling) {
-        uint64_t cnt[2] = {0, 0};
-        E8QC_CUDA(cudaMemcpyAsync(cnt, ws.b_nitems.as<uint32_t>() + 2, 16, cudaMemcpyDeviceToHost, s));
+        uint64_t cnt[3] = {0, 0, 0};
+        E8QC_CUDA(cudaMemcpyAsync(cnt, ws.b_nitems.as<uint32_t>() + 2, 24, cudaMemcpyDeviceToHost, s));
         E8QC_CUDA(cudaStreamSynchronize(s));
         float ms = 0.0f;
         E8QC_CUDA(cudaEventElapsedTime(&ms, ws.scan_ev0, ws.scan_ev1));
@@ -323,13 +326,16 @@ uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, con
         x->prof.scan_ms += ms;
         x->prof.candidates += cnt[0];
         x->prof.list_vectors += cnt[1];
-        // algorithmic bytes of the scan kernel: per vector read by a work item its
-        // codes + (g1, h3) (batched), or its int8 proxy row + (g1, h3) plus 4
-        // bytes of proxy distance written per (query, vector) pair (precision)
-        if (mode == E8QC_MODE_PRECISION)
-            x->prof.algo_bytes += cnt[1] * (static_cast<uint64_t>(x->pd) + 8) + cnt[0] * 4;
-        else
-            x->prof.algo_bytes += cnt[1] * (static_cast<uint64_t>(x->bits) * x->pd / 8 + 8);
+        x->prof.list_once += cnt[2];
+        // algorithmic bytes of the scan kernel: per vector of a probed list
+        // (once per call) its codes + (g1, h3) (batched), or its int8 proxy
+        // row + (g1, h3) plus 4 bytes of proxy distance written per (query,
+        // vector) pair (precision); item_bytes counts every work item's read
+        const uint64_t per_vec = mode == E8QC_MODE_PRECISION ? static_cast<uint64_t>(x->pd) + 8
+                                                             : static_cast<uint64_t>(x->bits) * x->pd / 8 + 8;
+        const uint64_t writes = mode == E8QC_MODE_PRECISION ? cnt[0] * 4 : 0;
+        x->prof.algo_bytes += cnt[2] * per_vec + writes;
+        x->prof.item_bytes += cnt[1] * per_vec + writes;
         x->prof.queries += nq;
     }
     return static_cast<uint64_t>(launches);
@@ -378,10 +384,8 @@ class E8qTarget final : public SearchTarget {
         b += (npairs / 64 + nl + 1) * 16 + 32;                    // work items
         if (mode == E8QC_MODE_PRECISION) {
             const size_t rows_q = max_tiles_for(x_, np) * 32;  // proxy rows one query can need
-            const size_t chunk =
-                std::max<size_t>(1, std::min<size_t>(nq, (size_t(2) << 30) / std::max<size_t>(1, rows_q * 4)));
-            b += nq * (pd + 8) + nl * 8;            // int8 queries, scales, row bases
-            b += chunk * rows_q * 4;                // proxy rows of one chunk
+            b += nq * (pd + 12) + nl * 8;                      // int8 queries, scales, row bases
+            b += precision_row_scratch(nq, rows_q);            // proxy rows of one chunk
             b += ((pslots + 7) / 8 * 8 + 128) * pd;  // gathered int8 query rows
         } else {
             b += npairs * k_max * 8;  // per-pair partial top-k

@@ -25,6 +25,7 @@
 #include "e8qc.h"
 #include "internal.h"
 #include "me8q.h"
+#include "precision.h"
 #include "serve_target.h"
 #include "workspace.h"
 
@@ -192,15 +193,17 @@ struct e8qc_me8q {
     std::vector<float> cen_host;  // padded centroids (estimate)
     DevBuf runs_d, chunks_d, levels, signs, cen_pad, cen_rot, cn2, tile_begin_d, list_len_d, list_order_d,
         list_of_tile_d, ids, codes, coef, h2, hsum, list_begin_d;
+    DevBuf proxy, sigma;                 // precision mode: int8 proxy plane and per-slot scale (built on first use)
+    std::vector<uint64_t> tiles_prefix;  // prefix sums of the lists' tile counts, largest first
     Me8qView view{};
     Workspace ws;
     std::mutex mu;
-    std::map<uint64_t, int> tuned;  // work-queue schedule per (log2 nq, log2 nprobe)
+    std::map<uint64_t, std::pair<int, int>> tuned;  // (schedule, stages) per (mode, log2 nq, log2 nprobe)
     std::mutex tune_mu;
     size_t memory_bytes() const {
         return runs_d.bytes + chunks_d.bytes + levels.bytes + signs.bytes + cen_pad.bytes + cen_rot.bytes + cn2.bytes +
                tile_begin_d.bytes + list_len_d.bytes + list_order_d.bytes + list_of_tile_d.bytes + ids.bytes +
-               codes.bytes + coef.bytes + h2.bytes + hsum.bytes + list_begin_d.bytes;
+               codes.bytes + coef.bytes + h2.bytes + hsum.bytes + list_begin_d.bytes + proxy.bytes + sigma.bytes;
     }
 };
 
@@ -294,6 +297,9 @@ void fill_view(e8qc_me8q* x) {
     b.ids = x->ids.as<uint32_t>();
     b.list_order = x->list_order_d.as<uint32_t>();
     b.list_of_tile = x->list_of_tile_d.as<uint32_t>();
+    b.h3 = x->hsum.as<float>();       // precision scan epilogue: (d2 + hsum) - 2 sigma S'
+    b.g1 = x->sigma.as<const float>();
+    b.proxy = static_cast<const uint4*>(x->proxy.p);
     v.coef = x->coef.as<float>();
     v.h2 = x->h2.as<float>();
     v.hsum = x->hsum.as<float>();
@@ -361,6 +367,15 @@ void build(e8qc_me8q* x, const float* data, size_t n, const float* centroids, si
     }
     x->ntiles = x->tile_begin[nlist];
     x->nslots = x->ntiles * 32;
+    x->proxy.release();
+    x->sigma.release();
+    {
+        std::vector<uint64_t> t(nlist);
+        for (size_t c = 0; c < nlist; ++c) t[c] = x->tile_begin[c + 1] - x->tile_begin[c];
+        std::sort(t.rbegin(), t.rend());
+        x->tiles_prefix.assign(nlist + 1, 0);
+        for (size_t c = 0; c < nlist; ++c) x->tiles_prefix[c + 1] = x->tiles_prefix[c] + t[c];
+    }
     std::vector<uint32_t> slot_of_row(n), slot_ids(std::max<size_t>(1, x->nslots), 0xFFFFFFFFu), fillc(nlist, 0);
     x->ids_compact.assign(n, 0);
     for (size_t i = 0; i < n; ++i) {
@@ -445,30 +460,60 @@ void build(e8qc_me8q* x, const float* data, size_t n, const float* centroids, si
     x->built = true;
 }
 
-uint64_t tune_key(size_t nq, size_t np) {
+uint64_t tune_key(int mode, size_t nq, size_t np) {
     auto lg = [](size_t v) {
         uint64_t l = 0;
         while ((size_t(1) << (l + 1)) <= v) ++l;
         return l;
     };
-    return (lg(nq) << 8) | lg(np);
+    return (static_cast<uint64_t>(mode) << 16) | (lg(nq) << 8) | lg(np);
 }
 
-int stored_sched(e8qc_me8q* x, size_t nq, size_t np) {
+// The stored setting of a batch shape (schedule 0 and 6 stages when none) into ws.
+void apply_stored(e8qc_me8q* x, Workspace& ws, int mode, size_t nq, size_t np) {
     std::lock_guard<std::mutex> lock(x->tune_mu);
-    auto it = x->tuned.find(tune_key(nq, np));
-    return it == x->tuned.end() ? 0 : it->second;
+    auto it = x->tuned.find(tune_key(mode, nq, np));
+    ws.sched = it == x->tuned.end() ? 0 : it->second.first;
+    ws.stages = it == x->tuned.end() ? 6 : it->second.second;
 }
 
-// Rotate nq device queries and run the grouped exact scan; no host
+void check_mode(int mode) {
+    if (mode != E8QC_MODE_BATCHED && mode != E8QC_MODE_PRECISION)
+        fail(E8QC_EINVAL, "ME8Q search modes are E8QC_MODE_BATCHED and E8QC_MODE_PRECISION");
+}
+
+// The precision proxy plane, built on first use (synchronises s).
+void ensure_proxy(e8qc_me8q* x, cudaStream_t s) {
+    if (x->proxy.p) return;
+    x->proxy.alloc(proxy_plane_bytes(x->view.base, x->ntiles));
+    E8QC_CUDA(cudaMemsetAsync(x->proxy.p, 0, x->proxy.bytes, s));
+    x->sigma.alloc(std::max<size_t>(1, x->nslots) * 4);
+    fill_view(x);
+    launch_me8q_proxy(x->view, static_cast<int>(x->ntiles), static_cast<unsigned char*>(x->proxy.p),
+                      x->sigma.as<float>(), s);
+    E8QC_CUDA(cudaStreamSynchronize(s));
+}
+
+// Proxy rows one query can need: the tiles of its np largest lists.
+size_t max_rows(const e8qc_me8q* x, size_t np) {
+    return static_cast<size_t>(x->tiles_prefix[std::min(np, x->nlist)]) * 32;
+}
+
+// Rotate nq device queries and run the grouped exact scan (batched) or the
+// int8 tensor-core candidates + exact rescoring (precision); no host
 // synchronisation (k_arr / np_arr may be NULL for uniform k / nprobe).
-uint64_t enqueue_search(e8qc_me8q* x, Workspace& ws, const float* q_dev, size_t nq, const uint32_t* k_arr,
+uint64_t enqueue_search(e8qc_me8q* x, Workspace& ws, int mode, const float* q_dev, size_t nq, const uint32_t* k_arr,
                         const uint32_t* np_arr, size_t k, size_t np, size_t out_stride, uint32_t* ids_d, float* d_d,
                         cudaStream_t s) {
     ws.ensure_queries(nq, x->pd);
     ws.ensure_err();
     launch_me8q_prep(q_dev, x->dim, static_cast<int>(x->dim), static_cast<int>(x->pd), nullptr, nullptr, x->view, 0,
                      nq, ws.rq.as<float>(), nullptr, nullptr, s);
+    if (mode == E8QC_MODE_PRECISION) {
+        if (!x->view.base.proxy) fail(E8QC_ESTATE, "the ME8Q proxy plane is not built");
+        return 1 + static_cast<uint64_t>(precision_search(x->view.base, ws, ws.rq.as<float>(), nq, k_arr, np_arr, k,
+                                                          np, out_stride, ids_d, d_d, max_rows(x, np), s, &x->view));
+    }
     return 1 + static_cast<uint64_t>(me8q_grouped_search(x->view, ws, ws.rq.as<float>(), nq, k_arr, np_arr, k, np,
                                                          out_stride, ids_d, d_d, s));
 }
@@ -481,31 +526,43 @@ class Me8qTarget final : public SearchTarget {
         nlist = x->nlist;
         device = x->device;
     }
-    void check_mode(int mode) const override {
-        if (mode != E8QC_MODE_BATCHED)
-            fail(E8QC_EINVAL, "ME8Q plans and servers run E8QC_MODE_BATCHED (the grouped exact scan)");
+    void check_mode(int mode) const override { ::check_mode(mode); }
+    void prepare(int mode) override {
+        if (mode != E8QC_MODE_PRECISION) return;
+        std::lock_guard<std::mutex> lock(x_->mu);
+        DeviceGuard g(x_->device);
+        ensure_proxy(x_, nullptr);
     }
-    void prepare(int) override {}
-    size_t bytes(int, size_t nq, size_t k_max, size_t np_max) const override {
-        const size_t np = std::min(np_max, x_->nlist), nl = x_->nlist;
+    size_t bytes(int mode, size_t nq, size_t k_max, size_t np_max) const override {
+        const size_t np = std::min(np_max, x_->nlist), nl = x_->nlist, pd = x_->pd;
         const size_t npairs = nq * np;
-        size_t b = nq * (x_->dim * 4 + x_->pd * 4 + k_max * 8 + 8);  // queries, rotated queries, results, k/nprobe
-        b += nq * nl * 8 + nq * 4;                                    // route keys, norms
-        b += npairs * 12 + npairs * 8 + nl * 12;                      // probes, d2, positions; pair rows; counters
-        b += (npairs / 64 + nl + 1) * 16 + 32;                        // work items
-        b += npairs * k_max * 8;                                      // per-pair partial top-k
+        const size_t align = mode == E8QC_MODE_PRECISION ? 8 : 1;
+        const size_t pslots = npairs + (align - 1) * nl;
+        size_t b = nq * (x_->dim * 4 + pd * 4 + k_max * 8 + 8);  // queries, rotated queries, results, k/nprobe
+        b += nq * nl * 8 + nq * 4;                                // route keys, norms
+        b += npairs * 12 + pslots * 8 + nl * 12;                  // probes, d2, positions; pair rows; counters
+        b += (npairs / 64 + nl + 1) * 16 + 32;                    // work items
+        if (mode == E8QC_MODE_PRECISION) {
+            const size_t rows_q = max_rows(x_, np);
+            b += nq * (pd + 12) + nl * 8;            // int8 queries, scales, row bases
+            b += precision_row_scratch(nq, rows_q);  // proxy rows of one chunk
+            b += ((pslots + 7) / 8 * 8 + 128) * pd;  // gathered int8 query rows
+        } else {
+            b += npairs * k_max * 8;  // per-pair partial top-k
+        }
         return b;
     }
-    uint64_t enqueue(Workspace& ws, int, const float* q_dev, size_t nq, const uint32_t* k_dev, const uint32_t* np_dev,
-                     size_t k_max, size_t np_max, uint32_t* ids_dev, float* d_dev, cudaStream_t s,
-                     bool apply_tuned) override {
+    uint64_t enqueue(Workspace& ws, int mode, const float* q_dev, size_t nq, const uint32_t* k_dev,
+                     const uint32_t* np_dev, size_t k_max, size_t np_max, uint32_t* ids_dev, float* d_dev,
+                     cudaStream_t s, bool apply_tuned) override {
         const size_t np = std::min(np_max, x_->nlist);
-        if (apply_tuned) ws.sched = stored_sched(x_, nq, np);
-        return enqueue_search(x_, ws, q_dev, nq, k_dev, np_dev, k_max, np, k_max, ids_dev, d_dev, s);
+        if (apply_tuned) apply_stored(x_, ws, mode, nq, np);
+        return enqueue_search(x_, ws, mode, q_dev, nq, k_dev, np_dev, k_max, np, k_max, ids_dev, d_dev, s);
     }
-    // The work-queue order (longest list first / list id order), timed on nq
+    // The work-queue order (longest list first / list id order) and, in
+    // precision mode, the scan's ring depth (6, 4, 8 stages), timed on nq
     // synthetic rotated queries (mixtures of two lists' rotated centroids).
-    void autotune(Workspace& ws, int, size_t nq, size_t k, size_t np, cudaStream_t s, int* sched,
+    void autotune(Workspace& ws, int mode, size_t nq, size_t k, size_t np, cudaStream_t s, int* sched,
                   int* stages) override {
         np = std::min(np, x_->nlist);
         DevBuf rq, ids, d;
@@ -524,36 +581,46 @@ class Me8qTarget final : public SearchTarget {
                 cudaEventDestroy(b);
             }
         } ev{e0, e1};
-        int best = 0;
-        double best_ms = 1e30;
-        for (int sc = 0; sc < 2; ++sc) {
-            ws.sched = sc;
-            auto run = [&] {
+        auto run = [&] {
+            if (mode == E8QC_MODE_PRECISION)
+                precision_search(x_->view.base, ws, rq.as<float>(), nq, nullptr, nullptr, k, np, k,
+                                 ids.as<uint32_t>(), d.as<float>(), max_rows(x_, np), s, &x_->view);
+            else
                 me8q_grouped_search(x_->view, ws, rq.as<float>(), nq, nullptr, nullptr, k, np, k, ids.as<uint32_t>(),
                                     d.as<float>(), s);
-            };
-            run();  // warm-up: sizes buffers, sets kernel attributes
-            E8QC_CUDA(cudaEventRecord(e0, s));
-            for (int r = 0; r < 3; ++r) run();
-            E8QC_CUDA(cudaEventRecord(e1, s));
-            ws.check_error(s);
-            float ms = 0.0f;
-            E8QC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            if (ms < best_ms) {
-                best_ms = ms;
-                best = sc;
+        };
+        const int stage_opts[3] = {6, 4, 8};
+        const int nst = mode == E8QC_MODE_PRECISION ? 3 : 1;
+        std::pair<int, int> best{0, 6};
+        double best_ms = 1e30;
+        for (int sc = 0; sc < 2; ++sc) {
+            for (int si = 0; si < nst; ++si) {
+                ws.sched = sc;
+                ws.stages = stage_opts[si];
+                run();  // warm-up: sizes buffers, sets kernel attributes
+                E8QC_CUDA(cudaEventRecord(e0, s));
+                for (int r = 0; r < 3; ++r) run();
+                E8QC_CUDA(cudaEventRecord(e1, s));
+                ws.check_error(s);
+                float ms = 0.0f;
+                E8QC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = {sc, stage_opts[si]};
+                }
             }
         }
-        ws.sched = best;
+        ws.sched = best.first;
+        ws.stages = best.second;
         {
             std::lock_guard<std::mutex> lock(x_->tune_mu);
-            x_->tuned[tune_key(nq, np)] = best;
+            x_->tuned[tune_key(mode, nq, np)] = best;
         }
-        *sched = best;
-        *stages = ws.stages;
+        *sched = best.first;
+        *stages = best.second;
     }
-    void stored_tuning(Workspace& ws, int, size_t nq, size_t np) override {
-        ws.sched = stored_sched(x_, nq, std::min(np, x_->nlist));
+    void stored_tuning(Workspace& ws, int mode, size_t nq, size_t np) override {
+        apply_stored(x_, ws, mode, nq, std::min(np, x_->nlist));
     }
 
    private:
@@ -639,8 +706,14 @@ int e8qc_me8q_build(e8qc_me8q* x, const float* data, size_t n, const float* cent
 
 int e8qc_me8q_search(e8qc_me8q* x, const float* queries, size_t nq, size_t k, size_t nprobe, uint32_t* out_ids,
                      float* out_dists, e8qc_stats* stats, void* stream) {
+    return e8qc_me8q_search_mode(x, queries, nq, k, nprobe, E8QC_MODE_BATCHED, out_ids, out_dists, stats, stream);
+}
+
+int e8qc_me8q_search_mode(e8qc_me8q* x, const float* queries, size_t nq, size_t k, size_t nprobe, int mode,
+                          uint32_t* out_ids, float* out_dists, e8qc_stats* stats, void* stream) {
     return guarded([&] {
         require_built(x, "search");
+        check_mode(mode);
         if (k == 0) fail(E8QC_EINVAL, "k must be positive");
         if (k > static_cast<size_t>(kMaxK)) fail(E8QC_EINVAL, "k must be <= 128");
         if (nprobe == 0) fail(E8QC_EINVAL, "nprobe must be positive");
@@ -668,8 +741,9 @@ int e8qc_me8q_search(e8qc_me8q* x, const float* queries, size_t nq, size_t k, si
             ws.stage_d.ensure(nq * k * 4);
             d_d = ws.stage_d.as<float>();
         }
-        ws.sched = stored_sched(x, nq, np);
-        const uint64_t launches = enqueue_search(x, ws, qd, nq, nullptr, nullptr, k, np, k, ids_d, d_d, s);
+        if (mode == E8QC_MODE_PRECISION) ensure_proxy(x, s);
+        apply_stored(x, ws, mode, nq, np);
+        const uint64_t launches = enqueue_search(x, ws, mode, qd, nq, nullptr, nullptr, k, np, k, ids_d, d_d, s);
         if (!ids_dev) E8QC_CUDA(cudaMemcpyAsync(out_ids, ids_d, nq * k * 4, cudaMemcpyDeviceToHost, s));
         if (out_dists && !d_dev) E8QC_CUDA(cudaMemcpyAsync(out_dists, d_d, nq * k * 4, cudaMemcpyDeviceToHost, s));
         ws.check_error(s);
@@ -686,9 +760,10 @@ int e8qc_me8q_search(e8qc_me8q* x, const float* queries, size_t nq, size_t k, si
 }
 
 int e8qc_me8q_search_ragged(e8qc_me8q* x, const float* queries, size_t nq, const uint32_t* k, const uint32_t* nprobe,
-                            size_t k_max, uint32_t* out_ids, float* out_dists, void* stream) {
+                            size_t k_max, int mode, uint32_t* out_ids, float* out_dists, void* stream) {
     return guarded([&] {
         require_built(x, "search");
+        check_mode(mode);
         if (nq == 0) return;
         if (!queries || !k || !nprobe || !out_ids) fail(E8QC_EINVAL, "null buffer");
         if (k_max == 0 || k_max > static_cast<size_t>(kMaxK)) fail(E8QC_EINVAL, "k_max must be in [1, 128]");
@@ -727,8 +802,9 @@ int e8qc_me8q_search_ragged(e8qc_me8q* x, const float* queries, size_t nq, const
             ws.stage_d.ensure(nq * k_max * 4);
             d_d = ws.stage_d.as<float>();
         }
-        ws.sched = stored_sched(x, nq, np_max);
-        enqueue_search(x, ws, qd, nq, ws.stage_k.as<uint32_t>(), ws.stage_np.as<uint32_t>(), k_max, np_max, k_max,
+        if (mode == E8QC_MODE_PRECISION) ensure_proxy(x, s);
+        apply_stored(x, ws, mode, nq, np_max);
+        enqueue_search(x, ws, mode, qd, nq, ws.stage_k.as<uint32_t>(), ws.stage_np.as<uint32_t>(), k_max, np_max, k_max,
                        ids_d, d_d, s);
         if (!ids_dev) E8QC_CUDA(cudaMemcpyAsync(out_ids, ids_d, nq * k_max * 4, cudaMemcpyDeviceToHost, s));
         if (out_dists && !d_dev)

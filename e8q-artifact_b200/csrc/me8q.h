@@ -80,6 +80,10 @@ int launch_me8q_estimate(const Me8qView& v, const float* rq, const float* qpad, 
 int launch_me8q_decode(const Me8qView& v, int ntiles, const uint32_t* list_of_tile, const uint64_t* list_begin,
                        int pd, uint16_t* digits, uint8_t* branch, cudaStream_t s);
 
+// The int8 proxy plane of the precision scan and its per-slot scale sigma
+// (plane: proxy_plane_bytes of the view, zeroed by the caller; sigma: ntiles*32).
+int launch_me8q_proxy(const Me8qView& v, int ntiles, unsigned char* plane, float* sigma, cudaStream_t s);
+
 // Grouped (batched) exact search of nq rotated queries: route, select,
 // group by list, persistent scan, per-query merge (batched.cu).
 int me8q_grouped_search(const Me8qView& v, Workspace& ws, const float* rq, size_t nq, const uint32_t* k_arr,

@@ -13,41 +13,11 @@
 #include "device_common.cuh"
 #include "internal.h"
 #include "me8q.h"
+#include "me8q_stream.cuh"
 
 namespace e8qc {
 
 namespace {
-
-__device__ __forceinline__ uint32_t* stream_word_ptr(uint4* codes, int nch, size_t slot, int w) {
-    return reinterpret_cast<uint32_t*>(codes + ((slot >> 5) * nch + (w >> 2)) * 32 + (slot & 31)) + (w & 3);
-}
-__device__ __forceinline__ uint32_t stream_word(const uint4* codes, int nch, size_t slot, int w) {
-    return __ldg(reinterpret_cast<const uint32_t*>(codes + ((slot >> 5) * nch + (w >> 2)) * 32 + (slot & 31)) +
-                 (w & 3));
-}
-
-// Field of `width` (<= 13) bits at bit `pos` of a vector's stream.
-__device__ __forceinline__ uint32_t stream_bits(const uint4* codes, int nch, size_t slot, int word0, int pos,
-                                                int width) {
-    const int w = word0 + (pos >> 5), sh = pos & 31;
-    uint32_t v = stream_word(codes, nch, slot, w) >> sh;
-    if (sh + width > 32) v |= stream_word(codes, nch, slot, w + 1) << (32 - sh);
-    return v & ((1u << width) - 1u);
-}
-
-// Digits and branch of block j of a run (E8Q stream layout within the run).
-__device__ __forceinline__ int stream_block(const uint4* codes, int nch, size_t slot, int word0, int bits, int j,
-                                            uint32_t dg[8]) {
-    const int base = j * 8 * bits;
-    uint32_t par = 0;
-    for (int i = 0; i < 7; ++i) {
-        dg[i] = stream_bits(codes, nch, slot, word0, base + i * bits, bits);
-        par ^= dg[i];
-    }
-    const uint32_t f7 = stream_bits(codes, nch, slot, word0, base + 7 * bits, bits);
-    dg[7] = (f7 & ~1u) | (par & 1u);
-    return static_cast<int>(f7 & 1u);
-}
 
 __global__ void variance_kernel(const float* __restrict__ x, size_t n, int dim, float* __restrict__ var) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -168,7 +138,7 @@ __global__ void fits_pack_kernel(Me8qView v, const float* __restrict__ rr, const
             acc |= static_cast<unsigned long long>(f) << fill;
             fill += b;
             if (fill >= 32) {
-                *stream_word_ptr(codes, nch, slot, w++) = static_cast<uint32_t>(acc);
+                *me8q_word_ptr(codes, nch, slot, w++) = static_cast<uint32_t>(acc);
                 acc >>= 32;
                 fill -= 32;
             }
@@ -206,7 +176,7 @@ __global__ void estimate_kernel(Me8qView v, const float* __restrict__ rq, const 
         float sc = 0.0f;
         for (int j = 0; j < run.len / 8; ++j) {
             uint32_t dg[8];
-            const int br = stream_block(v.base.codes, v.base.nch, slot, run.word0, run.bits, j, dg);
+            const int br = me8q_block(v.base.codes, v.base.nch, slot, run.word0, run.bits, j, dg);
             const float* lv = lev0 + (br ? (1 << run.bits) : 0);
             for (int i = 0; i < 8; ++i) sc = __fmaf_rn(rq[run.off + j * 8 + i], lv[dg[i]], sc);
         }
@@ -230,14 +200,80 @@ __global__ void decode_kernel(Me8qView v, int ntiles, const uint32_t* __restrict
         for (int j = 0; j < run.len / 8; ++j) {
             uint32_t dg[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             int br = 0;
-            if (run.bits != 0) br = stream_block(v.base.codes, v.base.nch, slot, run.word0, run.bits, j, dg);
+            if (run.bits != 0) br = me8q_block(v.base.codes, v.base.nch, slot, run.word0, run.bits, j, dg);
             for (int i = 0; i < 8; ++i) digits[pos * pd + run.off + j * 8 + i] = static_cast<uint16_t>(dg[i]);
             branch[pos * (pd / 8) + run.off / 8 + j] = static_cast<uint8_t>(br);
         }
     }
 }
 
+// ME8Q proxy plane, the int8 operand of the precision scan (the E8Q proxy
+// plane's layout: slot s, dimension i at (s/8)*8*pd + (i/16)*128 + (s%8)*16 +
+// i%16). Per slot the decoded levels scaled by the slot's coef of their run,
+// L' = coef_s * level, are quantised with one scale per slot: p = rint(L' /
+// sigma), sigma = max|L'| / 127 (0 when every L' is 0), so sigma * p ~ L' and
+// one int8 contraction over all runs approximates sum_s coef_s * S_s. One
+// thread per slot: pass 1 finds max|L'|, pass 2 writes 16 proxies per 16-byte
+// store. Dropped runs and padding slots are zero.
+__global__ void proxy_kernel(Me8qView v, int nslots, unsigned char* __restrict__ plane, float* __restrict__ sigma) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= nslots) return;
+    const int pd = v.base.pd, nch = v.base.nch;
+    const uint32_t L = v.base.list_of_tile[slot >> 5];
+    const bool live = static_cast<uint32_t>(slot) - v.base.tile_begin[L] * 32u < v.base.list_len[L];
+    float amax = 0.0f;
+    if (live) {
+        for (int q = 0; q < v.nruns; ++q) {
+            const Me8qRun run = v.runs[q];
+            if (run.bits == 0) continue;
+            const float cf = v.coef[static_cast<size_t>(run.coded) * v.nslots + slot];
+            if (cf == 0.0f) continue;
+            const float* lev0 = v.levels + v.chunks[run.off / 64].lev;
+            for (int j = 0; j < run.len / 8; ++j) {
+                uint32_t dg[8];
+                const int br = me8q_block(v.base.codes, nch, slot, run.word0, run.bits, j, dg);
+                const float* lv = lev0 + (br ? (1 << run.bits) : 0);
+                for (int i = 0; i < 8; ++i) amax = fmaxf(amax, fabsf(__fmul_rn(cf, __ldg(lv + dg[i]))));
+            }
+        }
+    }
+    const float inv = amax > 0.0f ? 127.0f / amax : 0.0f;
+    sigma[slot] = amax > 0.0f ? amax / 127.0f : 0.0f;
+    unsigned char* dst = plane + static_cast<size_t>(slot >> 3) * 8 * pd + (slot & 7) * 16;
+    for (int q = 0; q < v.nruns; ++q) {
+        const Me8qRun run = v.runs[q];
+        const float cf = (live && run.bits != 0) ? v.coef[static_cast<size_t>(run.coded) * v.nslots + slot] : 0.0f;
+        const float* lev0 = run.bits != 0 && run.off < v.route_dim ? v.levels + v.chunks[run.off / 64].lev : v.levels;
+        for (int g = 0; g < run.len / 16; ++g) {
+            uint32_t o[4] = {0u, 0u, 0u, 0u};
+            if (cf != 0.0f) {
+                for (int h = 0; h < 2; ++h) {
+                    uint32_t dg[8];
+                    const int br = me8q_block(v.base.codes, nch, slot, run.word0, run.bits, 2 * g + h, dg);
+                    const float* lv = lev0 + (br ? (1 << run.bits) : 0);
+                    for (int i = 0; i < 8; ++i) {
+                        int p = __float2int_rn(__fmul_rn(__fmul_rn(cf, __ldg(lv + dg[i])), inv));
+                        p = p > 127 ? 127 : (p < -127 ? -127 : p);
+                        const int e = h * 8 + i;
+                        o[e >> 2] |= (static_cast<uint32_t>(p) & 0xFFu) << (8 * (e & 3));
+                    }
+                }
+            }
+            *reinterpret_cast<uint4*>(dst + static_cast<size_t>(run.off / 16 + g) * 128) =
+                make_uint4(o[0], o[1], o[2], o[3]);
+        }
+    }
+}
+
 }  // namespace
+
+int launch_me8q_proxy(const Me8qView& v, int ntiles, unsigned char* plane, float* sigma, cudaStream_t s) {
+    const int nslots = ntiles * 32;
+    if (nslots == 0) return 0;
+    proxy_kernel<<<(nslots + 127) / 128, 128, 0, s>>>(v, nslots, plane, sigma);
+    E8QC_CUDA(cudaGetLastError());
+    return 1;
+}
 
 int launch_me8q_variance(const float* x, size_t n, int dim, float* var, cudaStream_t s) {
     variance_kernel<<<(dim + 127) / 128, 128, 0, s>>>(x, n, dim, var);

@@ -211,11 +211,11 @@ extern "C" int e8qc_plan_create(e8qc_index* idx, int mode, size_t max_queries, s
     });
 }
 
-extern "C" int e8qc_plan_create_me8q(e8qc_me8q* idx, size_t max_queries, size_t k_max, size_t nprobe_max,
+extern "C" int e8qc_plan_create_me8q(e8qc_me8q* idx, int mode, size_t max_queries, size_t k_max, size_t nprobe_max,
                                      int autotune, e8qc_plan** out) {
     return guard([&] {
         if (!idx || !out) fail(E8QC_EINVAL, "null argument");
-        *out = plan_make(me8q_target(idx), E8QC_MODE_BATCHED, max_queries, k_max, nprobe_max, autotune != 0);
+        *out = plan_make(me8q_target(idx), mode, max_queries, k_max, nprobe_max, autotune != 0);
     });
 }
 

@@ -27,6 +27,7 @@
 // loads and does no decoding.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -37,6 +38,8 @@
 #include "decode_accum.cuh"
 #include "device_common.cuh"
 #include "internal.h"
+#include "me8q.h"
+#include "me8q_stream.cuh"
 #include "precision.h"
 #include "scan_plain.h"
 #include "tc.cuh"
@@ -52,12 +55,15 @@ __device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
 constexpr int kPM = 128;  // pair rows per MMA tile (M = TMEM lanes)
 constexpr int kPN = 256;  // vectors per MMA tile (N)
 constexpr int kPK = 64;   // dimensions per staged K-chunk (2 MMAs of K = 32)
-constexpr size_t kScratchBudget = size_t(2) << 30;  // proxy rows per call chunk (bytes)
+constexpr int kOrdCap = 512;  // final kernel: probes per query it orders nearest list first
+constexpr size_t kScratchBudget = size_t(8) << 30;  // proxy rows per call chunk (bytes)
 
 // Per-query int8 quantisation: q8 = rint(q * 127 / max|q|); per-query factor
 // coef / qs and sum(q8).
-__global__ void quantize_kernel(const float* __restrict__ rq, int pd, float coef, int8_t* __restrict__ q8,
-                                float* __restrict__ qscale, float* __restrict__ qsum) {
+__global__ void quantize_kernel(const float* __restrict__ rq, int pd, float coef, int with_sum,
+                                int8_t* __restrict__ q8, float* __restrict__ qscale, float* __restrict__ qsum,
+                                const float* __restrict__ pd2, const uint32_t* __restrict__ np_arr, int np_uniform,
+                                int np_max, float* __restrict__ pscale) {
     __shared__ float red[32];
     __shared__ int ired[32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
@@ -86,7 +92,13 @@ __global__ void quantize_kernel(const float* __restrict__ rq, int pd, float coef
         int s = 0;
         for (int i = 0; i < nw; ++i) s += ired[i];
         qscale[blockIdx.x] = coef / qs;
-        qsum[blockIdx.x] = static_cast<float>(s);
+        qsum[blockIdx.x] = with_sum ? static_cast<float>(s) : 0.0f;
+        // proxy distances are stored as fp16 divided by the query's largest
+        // routing distance (only their order within the query matters)
+        const int np = np_arr ? static_cast<int>(np_arr[blockIdx.x]) : np_uniform;
+        float dmax = 0.0f;
+        for (int j = 0; j < np; ++j) dmax = fmaxf(dmax, pd2[static_cast<size_t>(blockIdx.x) * np_max + j]);
+        pscale[blockIdx.x] = dmax > 0.0f ? 1.0f / dmax : 1.0f;
     }
 }
 
@@ -236,8 +248,8 @@ __global__ void __launch_bounds__(kScanThreads, 1) precision_scan_kernel(
     const uint32_t* __restrict__ pair_q,
     const float* __restrict__ pair_d2, const float* __restrict__ qscale, const float* __restrict__ qsum,
     const uint4* __restrict__ items, const uint32_t* __restrict__ n_items, uint32_t* __restrict__ head,
-    const uint32_t* __restrict__ pair_off, const unsigned long long* __restrict__ rowbase, float* __restrict__ prox,
-    unsigned long long* __restrict__ counts, uint32_t* __restrict__ err) {
+    const uint32_t* __restrict__ pair_off, const unsigned long long* __restrict__ rowbase, __half* __restrict__ prox,
+    const float* __restrict__ pscale, unsigned long long* __restrict__ counts, uint32_t* __restrict__ err) {
     extern __shared__ __align__(1024) unsigned char psm[];
     float2* ghtab = reinterpret_cast<float2*>(psm + kStages * kStageBytes);  // 4 warps x kPN
     __shared__ __align__(8) uint64_t full[kStages], empty[kStages], tfull[2], tempty[2], ifull[kRing],
@@ -371,18 +383,20 @@ __global__ void __launch_bounds__(kScanThreads, 1) precision_scan_kernel(
             const int m = static_cast<int>(item.z);
             const uint32_t len = ix.list_len[L], tile0 = ix.tile_begin[L];
             const uint32_t stride = (ix.tile_begin[L + 1] - tile0) * 32u;
-            float sc = 0.0f, sum = 0.0f, d2 = 0.0f;
-            float* row = prox;
+            float sc = 0.0f, sum = 0.0f, d2 = 0.0f, ps = 1.0f;
+            __half* row = prox;
             if (r < m) {
                 const uint32_t qq = pair_q[pbase + r];
                 sc = qscale[qq];
                 sum = qsum[qq];
+                ps = pscale[qq];
                 d2 = pair_d2[pbase + r];
                 row = prox + rowbase[L] + static_cast<unsigned long long>(pbase + r - pair_off[L]) * stride;
             }
             if (warp == 2 && lane == 0) {
                 atomicAdd(counts, static_cast<unsigned long long>(len) * m);  // (query, vector) pairs
                 atomicAdd(counts + 1, static_cast<unsigned long long>(len));  // vectors read
+                if (item.w == 0) atomicAdd(counts + 2, static_cast<unsigned long long>(len));  // once per list
             }
             // (g1, h3) of columns 4*lane.. and 128 + 4*lane.. of a tile (zero past the padded list)
             const float4* g4 = reinterpret_cast<const float4*>(ix.g1 + tile0 * 32u);
@@ -422,18 +436,25 @@ __global__ void __launch_bounds__(kScanThreads, 1) precision_scan_kernel(
                     tc::tmem_ld_wait();
                     if (r < m) {
                         // columns past len land in the row's tile padding (rows are whole tiles)
-                        float4* dst = reinterpret_cast<float4*>(row + v0 + c0);
+                        uint4* dst = reinterpret_cast<uint4*>(row + v0 + c0);
 #pragma unroll
-                        for (int q = 0; q < 8; ++q) {
-                            float o[4];
+                        for (int q = 0; q < 4; ++q) {
+                            uint32_t hw[4];
 #pragma unroll
-                            for (int e = 0; e < 4; ++e) {
-                                const float2 cg = gh[c0 + 4 * q + e];
-                                const float Sp =
-                                    sc * __fmaf_rn(2.0f, static_cast<float>(static_cast<int>(acc[4 * q + e])), sum);
-                                o[e] = __fmaf_rn(cg.x, Sp, __fadd_rn(d2, cg.y));
+                            for (int e2 = 0; e2 < 4; ++e2) {
+                                float o[2];
+#pragma unroll
+                                for (int h = 0; h < 2; ++h) {
+                                    const int e = 8 * q + 2 * e2 + h;
+                                    const float2 cg = gh[c0 + e];
+                                    const float Sp =
+                                        sc * __fmaf_rn(2.0f, static_cast<float>(static_cast<int>(acc[e])), sum);
+                                    o[h] = __fmul_rn(__fmaf_rn(cg.x, Sp, __fadd_rn(d2, cg.y)), ps);
+                                }
+                                const __half2 hv = __floats2half2_rn(o[0], o[1]);
+                                hw[e2] = *reinterpret_cast<const uint32_t*>(&hv);
                             }
-                            dst[q] = make_float4(o[0], o[1], o[2], o[3]);
+                            dst[q] = make_uint4(hw[0], hw[1], hw[2], hw[3]);
                         }
                     }
                 }
@@ -451,11 +472,44 @@ __global__ void __launch_bounds__(kScanThreads, 1) precision_scan_kernel(
     if (warp == 0) tc::tmem_dealloc(tmem, kScanCols);
 }
 
+// Exact ME8Q estimate of stored slot `slot` for a rotated query q (shared
+// memory) whose routing distance to the slot's list is d2, in the
+// reference's form (EstimateRow, src/index/me8q_search.cpp:74-95): per coded
+// run an fp32 score S_s = sum q * level accumulated in dimension order, then
+// d2 + sum_s (h2_s - 2 coef_s S_s) in fp64 (h2_s alone when coef_s is 0).
+__device__ float me8q_rescore(const Me8qView& mv, uint32_t slot, const float* q, float d2) {
+    double acc = static_cast<double>(d2);
+    const int nch = mv.base.nch;
+    for (int r = 0; r < mv.nruns; ++r) {
+        const Me8qRun run = mv.runs[r];
+        if (run.bits == 0) continue;
+        const double cf = static_cast<double>(__ldg(mv.coef + static_cast<size_t>(run.coded) * mv.nslots + slot));
+        const double hh = static_cast<double>(__ldg(mv.h2 + static_cast<size_t>(run.coded) * mv.nslots + slot));
+        if (cf == 0.0) {
+            acc += hh;
+            continue;
+        }
+        const float* lev0 = mv.levels + mv.chunks[run.off / 64].lev;
+        const int qb = 1 << run.bits;
+        float sc = 0.0f;
+        for (int j = 0; j < run.len / 8; ++j) {
+            uint32_t dg[8];
+            const int br = me8q_block(mv.base.codes, nch, slot, run.word0, run.bits, j, dg);
+            const float* lv = lev0 + (br ? qb : 0);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) sc = __fmaf_rn(q[run.off + j * 8 + i], __ldg(lv + dg[i]), sc);
+        }
+        acc += __fma_rn(-2.0 * cf, static_cast<double>(sc), hh);
+    }
+    return static_cast<float>(acc);
+}
+
 // Per query (one warp): best C proxies over the query's rows, exact rescoring
-// of those candidates, top-k by exact distance.
-template <int BITS>
+// of those candidates (E8Q estimator at BITS, or the ME8Q estimator), top-k
+// by exact distance.
+template <int BITS, bool ME8Q>
 __global__ void __launch_bounds__(128) precision_final_kernel(
-    DevIndex ix, const float* __restrict__ rq, const float* __restrict__ prox,
+    DevIndex ix, Me8qView mv, const float* __restrict__ rq, const __half* __restrict__ prox,
     const unsigned long long* __restrict__ rowbase, const uint32_t* __restrict__ pair_off,
     const uint32_t* __restrict__ pos_of, const uint32_t* __restrict__ probes, const float* __restrict__ pd2, int nq,
     const uint32_t* __restrict__ np_arr, int np_max, const uint32_t* __restrict__ k_arr, int k_uniform, int C,
@@ -468,7 +522,8 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
     float* tabrep = fsm;               // 2*Q*REP
     float* sq = tabrep + 2 * Q * REP;  // 4 warps x pd, then 4 warps x kMaxK candidate slots
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int e = tid; e < 2 * Q * REP; e += blockDim.x) tabrep[e] = ix.tab[e / REP];
+    if constexpr (!ME8Q)
+        for (int e = tid; e < 2 * Q * REP; e += blockDim.x) tabrep[e] = ix.tab[e / REP];
     const int q = blockIdx.x * 4 + warp;
     const int pd = ix.pd;
     float* myq = sq + warp * pd;
@@ -479,10 +534,31 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
     const int np = np_arr ? static_cast<int>(np_arr[q]) : np_max;
     const int kq = k_arr ? static_cast<int>(k_arr[q]) : k_uniform;
     const uint32_t* pr = probes + static_cast<size_t>(q) * np_max;
+    // Rows nearest list first (routing distance, then probe index): the best
+    // proxies mostly sit in the nearest lists, so the top-C threshold settles
+    // on the first rows and later steps pass the filter without offers. A
+    // query with more than kOrdCap probes keeps list order.
+    float* sbuf = sq + 4 * pd + 4 * kMaxK + warp * 512;  // d2 staging, then one step's values
+    uint16_t* ord = reinterpret_cast<uint16_t*>(sq + 4 * pd + 4 * kMaxK + 4 * 512) + warp * kOrdCap;
+    const bool reorder = np <= kOrdCap;
+    if (reorder) {
+        for (int i = lane; i < np; i += 32) sbuf[i] = pd2[static_cast<size_t>(q) * np_max + i];
+        __syncwarp();
+        for (int i = lane; i < np; i += 32) {
+            const float di = sbuf[i];
+            int r = 0;
+            for (int j = 0; j < np; ++j) {
+                const float dj = sbuf[j];
+                r += (dj < di) | ((dj == di) & (j < i));
+            }
+            ord[r] = static_cast<uint16_t>(i);
+        }
+        __syncwarp();
+    }
     // 1. best C proxies (slot as tie-break). Row metadata for 32 probes at a
     //    time sits in registers (lane j: probe w0 + j) and is read by shuffle;
     //    values stream 512 per step, the next step's loads in flight while
-    //    the current step is offered.
+    //    the current step is filtered.
     WarpTopK cand;
     cand.init(C);
     int w0 = -32;
@@ -495,10 +571,11 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
         m_len = 0;
         m_slot0 = 0;
         if (p < np) {
-            const uint32_t L = pr[p];
+            const int pp = reorder ? static_cast<int>(ord[p]) : p;
+            const uint32_t L = pr[pp];
             const uint32_t t0 = ix.tile_begin[L];
             const uint32_t stride = (ix.tile_begin[L + 1] - t0) * 32u;
-            const uint32_t pos = pos_of[static_cast<size_t>(q) * np_max + p];
+            const uint32_t pos = pos_of[static_cast<size_t>(q) * np_max + pp];
             m_off = rowbase[L] + static_cast<unsigned long long>(pos - pair_off[L]) * stride;
             m_len = ix.list_len[L];
             m_slot0 = t0 * 32u;
@@ -529,46 +606,69 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
         }
         return st;
     };
-    auto load_step = [&](const Step& st, float4 (&x)[4]) {
+    // a step: 512 fp16 values of the row, lane l holding columns 8l..8l+7 and
+    // 256+8l..256+8l+7 (one 16-byte load each)
+    auto load_step = [&](const Step& st, uint4 (&x)[2]) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const uint32_t va = st.v0 + 128 * j + 4 * lane;
-            x[j] = (st.p < np && va < st.len) ? __ldcs(reinterpret_cast<const float4*>(prox + st.off) + (va >> 2))
-                                              : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int j = 0; j < 2; ++j) {
+            const uint32_t va = st.v0 + 256 * j + 8 * lane;
+            x[j] = (st.p < np && va < st.len) ? __ldcs(reinterpret_cast<const uint4*>(prox + st.off) + (va >> 3))
+                                              : make_uint4(0u, 0u, 0u, 0u);
         }
     };
     load_window(0);
     Step cur = advance(-1, 0, 0);  // first non-empty row
-    float4 cx[4];
+    uint4 cx[2];
     load_step(cur, cx);
     while (cur.p < np) {
         const Step nxt = advance(cur.p, cur.v0, cur.len);
-        float4 nx[4];
+        uint4 nx[2];
         load_step(nxt, nx);
-        // fast filter: most steps hold no value that can enter the list
-        bool any = false;
+        // filter: a 16-bit mask per lane of the values that can enter the
+        // list; most steps have none once the threshold has settled.
+        // Value t of this lane is column 256*(t/8) + 8*lane + t%8.
+        float v[16];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const uint32_t va = cur.v0 + 128 * j + 4 * lane;
-            any |= (va + 0 < cur.len && !(cx[j].x > cand.thr_d)) || (va + 1 < cur.len && !(cx[j].y > cand.thr_d)) ||
-                   (va + 2 < cur.len && !(cx[j].z > cand.thr_d)) || (va + 3 < cur.len && !(cx[j].w > cand.thr_d));
+        for (int j = 0; j < 2; ++j) {
+            const uint32_t w4[4] = {cx[j].x, cx[j].y, cx[j].z, cx[j].w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w4[e]));
+                v[8 * j + 2 * e] = f.x;
+                v[8 * j + 2 * e + 1] = f.y;
+            }
         }
-        // one offer site (a rolled loop keeps the code small): value t of this
-        // lane is column v0 + 128*(t/4) + 4*lane + t%4; the 16 loaded values
-        // rotate through cx[0].x
-        const int nt = __any_sync(kFull, any) ? 16 : 0;
+        uint32_t hit = 0;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+            const uint32_t va = cur.v0 + 256 * (t >> 3) + 8 * lane + (t & 7);
+            hit |= static_cast<uint32_t>(va < cur.len && !(v[t] > cand.thr_d)) << t;
+        }
+        if (__any_sync(kFull, hit != 0)) {
+            // staged in shared memory so the offer loop indexes it
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                float4* dst = reinterpret_cast<float4*>(sbuf + 256 * j + 8 * lane);
+                dst[0] = make_float4(v[8 * j + 0], v[8 * j + 1], v[8 * j + 2], v[8 * j + 3]);
+                dst[1] = make_float4(v[8 * j + 4], v[8 * j + 5], v[8 * j + 6], v[8 * j + 7]);
+            }
+            __syncwarp();
+            // one offer per round: each lane its lowest remaining hit; offer()
+            // re-checks every value against the threshold of that moment
 #pragma unroll 1
-        for (int t = 0; t < nt; ++t) {
-            const uint32_t va = cur.v0 + 128 * (t >> 2) + 4 * lane + (t & 3);
-            cand.offer_pair(cx[0].x, cur.slot0 + va, va < cur.len);
-            cx[0].x = cx[0].y; cx[0].y = cx[0].z; cx[0].z = cx[0].w; cx[0].w = cx[1].x;
-            cx[1].x = cx[1].y; cx[1].y = cx[1].z; cx[1].z = cx[1].w; cx[1].w = cx[2].x;
-            cx[2].x = cx[2].y; cx[2].y = cx[2].z; cx[2].z = cx[2].w; cx[2].w = cx[3].x;
-            cx[3].x = cx[3].y; cx[3].y = cx[3].z; cx[3].z = cx[3].w;
+            while (__any_sync(kFull, hit != 0)) {
+                const bool has = hit != 0;
+                const int t = has ? __ffs(static_cast<int>(hit)) - 1 : 0;
+                hit &= hit - 1u;
+                const uint32_t col = 256u * static_cast<uint32_t>(t >> 3) + 8u * static_cast<uint32_t>(lane) +
+                                     static_cast<uint32_t>(t & 7);
+                cand.offer_pair(has ? sbuf[col] : inf_f(), cur.slot0 + cur.v0 + col, has);
+            }
+            __syncwarp();
         }
         cur = nxt;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) cx[j] = nx[j];
+        cx[0] = nx[0];
+        cx[1] = nx[1];
     }
     // 2. exact rescoring of candidate (s, lane); 3. top-k by exact distance.
     //    The candidates' slots go through shared memory so the loop below
@@ -595,13 +695,6 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
         uint32_t gid = 0xFFFFFFFFu;
         if (live) {
             const uint32_t tile = slot >> 5;
-            const int vl = static_cast<int>(slot & 31u);
-            const uint4* tp = ix.codes + static_cast<size_t>(tile) * ix.nch * 32;
-            float acc0 = 0.0f, acc1 = 0.0f;
-            for (int g = 0; g < ng; ++g)
-                accumulate_blocks<BITS, GBL, GCH>(tp + g * GCH * 32, vl, sq4, g * GBL, tb_addr, acc0, acc1);
-            if (tail) accumulate_blocks<BITS, 8, TCH>(tp + ng * GCH * 32, vl, sq4, ng * GBL, tb_addr, acc0, acc1);
-            const float S = __fadd_rn(acc0, acc1);
             // d2 of (query, the candidate's list): the query's probes are in list order
             const uint32_t list = ix.list_of_tile[tile];
             int lo = 0, hi = np;
@@ -611,7 +704,19 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
                 else hi = mid;
             }
             const float d2 = pd2[static_cast<size_t>(q) * np_max + lo];
-            dist = __fmaf_rn(-__fmul_rn(2.0f, __ldg(ix.g1 + slot)), S, __fadd_rn(d2, __ldg(ix.h3 + slot)));
+            if constexpr (ME8Q) {
+                dist = me8q_rescore(mv, slot, myq, d2);
+            } else {
+                const int vl = static_cast<int>(slot & 31u);
+                const uint4* tp = ix.codes + static_cast<size_t>(tile) * ix.nch * 32;
+                float acc0 = 0.0f, acc1 = 0.0f;
+                for (int g = 0; g < ng; ++g)
+                    accumulate_blocks<BITS, GBL, GCH>(tp + g * GCH * 32, vl, sq4, g * GBL, tb_addr, acc0, acc1);
+                if (tail)
+                    accumulate_blocks<BITS, 8, TCH>(tp + ng * GCH * 32, vl, sq4, ng * GBL, tb_addr, acc0, acc1);
+                const float S = __fadd_rn(acc0, acc1);
+                dist = __fmaf_rn(-__fmul_rn(2.0f, __ldg(ix.g1 + slot)), S, __fadd_rn(d2, __ldg(ix.h3 + slot)));
+            }
             gid = __ldg(ix.ids + slot);
         }
         top.offer_pair(dist, gid, live);
@@ -679,8 +784,8 @@ void launch_scan_stages(const DevIndex& ix, Workspace& ws, const CUtensorMap& ma
     precision_scan_kernel<STAGES><<<sms, kScanThreads, smem, s>>>(
         ix, map_a, map_b, ws.b_pair_q.as<uint32_t>(), ws.b_pair_d2.as<float>(), ws.p_scale.as<float>(),
         ws.p_sum.as<float>(), ws.b_items.as<uint4>(), nitems, nitems + 1, ws.b_off.as<uint32_t>(),
-        ws.p_rowbase.as<unsigned long long>(), ws.p_prox.as<float>(), reinterpret_cast<unsigned long long*>(nitems + 2),
-        ws.err.as<uint32_t>());
+        ws.p_rowbase.as<unsigned long long>(), ws.p_prox.as<__half>(), ws.p_pscale.as<float>(),
+        reinterpret_cast<unsigned long long*>(nitems + 2), ws.err.as<uint32_t>());
     E8QC_CUDA(cudaGetLastError());
     ws.mark_scan(true, s);
 }
@@ -696,22 +801,23 @@ void launch_scan(const DevIndex& ix, Workspace& ws, size_t a_rows, size_t plane_
 }
 
 // Per-query selection + exact rescoring of one chunk of queries.
-template <int BITS>
-int launch_final(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* k_arr,
-                 const uint32_t* np_arr, int k_max, int np_max, int C, int out_stride, uint32_t* out_ids,
-                 float* out_d, cudaStream_t s) {
+template <int BITS, bool ME8Q = false>
+int launch_final(const DevIndex& ix, const Me8qView& mv, Workspace& ws, const float* rq, size_t nq,
+                 const uint32_t* k_arr, const uint32_t* np_arr, int k_max, int np_max, int C, int out_stride,
+                 uint32_t* out_ids, float* out_d, cudaStream_t s) {
     int dev = 0;
     E8QC_CUDA(cudaGetDevice(&dev));
     constexpr int REP = table_rep(BITS);
-    const size_t fsmem = (static_cast<size_t>(2) * (1 << BITS) * REP + 4 * static_cast<size_t>(ix.pd) + 4 * kMaxK) * 4;
+    const size_t fsmem = (static_cast<size_t>(2) * (1 << BITS) * REP + 4 * static_cast<size_t>(ix.pd) + 4 * kMaxK +
+                          4 * 512) * 4 + 4 * kOrdCap * 2;
     static size_t fconfigured[64] = {};
     if (fsmem > 48 * 1024 && fconfigured[dev & 63] < fsmem) {
-        E8QC_CUDA(cudaFuncSetAttribute(precision_final_kernel<BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(fsmem)));
+        E8QC_CUDA(cudaFuncSetAttribute(precision_final_kernel<BITS, ME8Q>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(fsmem)));
         fconfigured[dev & 63] = fsmem;
     }
-    precision_final_kernel<BITS><<<static_cast<unsigned>((nq + 3) / 4), 128, fsmem, s>>>(
-        ix, rq, ws.p_prox.as<float>(), ws.p_rowbase.as<unsigned long long>(), ws.b_off.as<uint32_t>(),
+    precision_final_kernel<BITS, ME8Q><<<static_cast<unsigned>((nq + 3) / 4), 128, fsmem, s>>>(
+        ix, mv, rq, ws.p_prox.as<__half>(), ws.p_rowbase.as<unsigned long long>(), ws.b_off.as<uint32_t>(),
         ws.b_pos.as<uint32_t>(), ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(), static_cast<int>(nq), np_arr,
         np_max, k_arr, k_max, C, out_stride, out_ids, out_d);
     E8QC_CUDA(cudaGetLastError());
@@ -769,17 +875,26 @@ int launch_build_proxy(const DevIndex& ix, int ntiles, uint4* plane, cudaStream_
 
 int precision_candidates(int k) { return std::min(kMaxK, std::max(64, 4 * k)); }
 
+size_t precision_row_scratch(size_t nq, size_t rows_per_query) {
+    const size_t per_q = std::max<size_t>(1, rows_per_query) * sizeof(__half);
+    return std::max<size_t>(1, std::min(nq, kScratchBudget / per_q)) * per_q;
+}
+
 int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* k_arr,
                      const uint32_t* np_arr, size_t k, size_t nprobe, size_t out_stride, uint32_t* out_ids,
-                     float* out_d, size_t rows_per_query, cudaStream_t s) {
+                     float* out_d, size_t rows_per_query, cudaStream_t s, const Me8qView* me8q) {
     if (nq == 0) return 0;
     if (ix.pd % kPK != 0) fail(E8QC_EINVAL, "precision search needs the padded dimension to be a multiple of 64");
     if (ix.proxy == nullptr) fail(E8QC_ESTATE, "precision search needs the proxy plane (launch_build_proxy)");
     const int C = precision_candidates(static_cast<int>(k));
-    const int shift = ix.bits > 7 ? (1 << (ix.bits - 7)) : 1;
-    const float coef = static_cast<float>(precision_alpha(ix.bits, ix.pd) * shift / 4.0);
+    // E8Q: S' = alpha*shift/(4 qs) * (2 S8 + sum q8) from integer lattice
+    // proxies; ME8Q: S' = S8 / qs = (1/(2 qs)) * (2 S8 + 0) from the slot-
+    // scaled level proxies (the slot's sigma sits in the g1 plane, hsum in h3)
+    const int shift = !me8q && ix.bits > 7 ? (1 << (ix.bits - 7)) : 1;
+    const float coef = me8q ? 0.5f : static_cast<float>(precision_alpha(ix.bits, ix.pd) * shift / 4.0);
+    const Me8qView none{};
     // proxy rows of a chunk of queries stay within the scratch budget
-    const size_t per_q = std::max<size_t>(1, rows_per_query) * sizeof(float);
+    const size_t per_q = std::max<size_t>(1, rows_per_query) * sizeof(__half);
     const size_t chunk = std::max<size_t>(1, std::min(nq, kScratchBudget / per_q));
     ws.ensure_err();
     int launches = 0;
@@ -794,25 +909,33 @@ int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t 
         ws.p_q8.ensure(n * static_cast<size_t>(ix.pd));
         ws.p_scale.ensure(n * 4);
         ws.p_sum.ensure(n * 4);
+        ws.p_pscale.ensure(n * 4);
         ws.p_rowbase.ensure(static_cast<size_t>(ix.nlist) * 8);
         ws.p_prox.ensure(n * per_q);
         ws.p_a8.ensure(arows * ix.pd);
         rowbase_kernel<<<1, 1024, 0, s>>>(ws.b_cnt.as<uint32_t>(), ix.tile_begin, ix.nlist,
                                           ws.p_rowbase.as<unsigned long long>());
-        quantize_kernel<<<static_cast<unsigned>(n), 256, 0, s>>>(rqc, ix.pd, coef, ws.p_q8.as<int8_t>(),
-                                                                 ws.p_scale.as<float>(), ws.p_sum.as<float>());
+        quantize_kernel<<<static_cast<unsigned>(n), 256, 0, s>>>(
+            rqc, ix.pd, coef, me8q ? 0 : 1, ws.p_q8.as<int8_t>(), ws.p_scale.as<float>(), ws.p_sum.as<float>(),
+            ws.b_pd2.as<float>(), npc, static_cast<int>(nprobe), static_cast<int>(nprobe), ws.p_pscale.as<float>());
         const size_t ga = arows * (ix.pd / 16);
         gather_a8_kernel<<<static_cast<unsigned>((ga + 255) / 256), 256, 0, s>>>(
             ws.p_q8.as<int8_t>(), ws.b_pair_q.as<uint32_t>(), pslots, arows, ix.pd, ws.p_a8.as<unsigned char>());
         E8QC_CUDA(cudaGetLastError());
         launch_scan(ix, ws, arows, static_cast<size_t>(ix.ntiles) * 32 + kPN, s);
         launches += 4;
+        if (me8q) {
+            launches += launch_final<1, true>(ix, *me8q, ws, rqc, n, kc, npc, static_cast<int>(k),
+                                              static_cast<int>(nprobe), C, static_cast<int>(out_stride),
+                                              out_ids + off * out_stride, out_d + off * out_stride, s);
+            continue;
+        }
         switch (ix.bits) {
-#define E8QC_CASE(b)                                                                                          \
-    case b:                                                                                                   \
-        launches += launch_final<b>(ix, ws, rqc, n, kc, npc, static_cast<int>(k), static_cast<int>(nprobe), C, \
-                                    static_cast<int>(out_stride), out_ids + off * out_stride,                 \
-                                    out_d + off * out_stride, s);                                             \
+#define E8QC_CASE(b)                                                                                             \
+    case b:                                                                                                      \
+        launches += launch_final<b>(ix, none, ws, rqc, n, kc, npc, static_cast<int>(k), static_cast<int>(nprobe), \
+                                    C, static_cast<int>(out_stride), out_ids + off * out_stride,                 \
+                                    out_d + off * out_stride, s);                                                \
         break;
             E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
             E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)

@@ -30,8 +30,16 @@ int precision_candidates(int k);
 // rows_per_query bounds the vectors one query's probes can reach (the padded
 // slots of the nprobe longest lists): the proxy scratch of a chunk of queries
 // is sized from it, and batches whose scratch would exceed 2 GiB run in chunks.
+// me8q: the ME8Q index whose view `ix` is (its proxy plane in ix.proxy, the
+// per-slot proxy scale in ix.g1, hsum in ix.h3): slot-scaled level proxies and
+// the ME8Q estimator for rescoring. NULL for an E8Q index.
+// Device bytes of the proxy-distance rows one ragged call of nq queries
+// holds at once (it runs in chunks of queries within a fixed budget).
+size_t precision_row_scratch(size_t nq, size_t rows_per_query);
+
+struct Me8qView;
 int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* k_arr,
                      const uint32_t* np_arr, size_t k, size_t nprobe, size_t out_stride, uint32_t* out_ids,
-                     float* out_d, size_t rows_per_query, cudaStream_t s);
+                     float* out_d, size_t rows_per_query, cudaStream_t s, const Me8qView* me8q = nullptr);
 
 }  // namespace e8qc

@@ -308,10 +308,7 @@ extern "C" int e8qc_server_start(e8qc_index* idx, const e8qc_server_config* cfg,
 extern "C" int e8qc_server_start_me8q(e8qc_me8q* idx, const e8qc_server_config* cfg, e8qc_server** out) {
     return guard([&] {
         if (!idx || !out) fail(E8QC_EINVAL, "null argument");
-        e8qc_server_config c{};
-        if (cfg) c = *cfg;
-        c.mode = E8QC_MODE_BATCHED;
-        *out = server_make(me8q_target(idx), &c);
+        *out = server_make(me8q_target(idx), cfg);
     });
 }
 

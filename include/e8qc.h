@@ -139,10 +139,13 @@ typedef struct e8qc_profile {
     double scan_ms;          /* summed CUDA-event time of those launches */
     uint64_t candidates;     /* (query, vector) pairs scored */
     uint64_t algo_bytes;     /* plain: candidates * (bits*padded_dim/8 + 8), codes + g1/h3; batched:
-                                list_vectors * (bits*padded_dim/8 + 8); precision: list_vectors *
+                                list_once * (bits*padded_dim/8 + 8); precision: list_once *
                                 (padded_dim + 8) int8 proxies + g1/h3, plus 4 per candidate written */
     uint64_t queries;
-    uint64_t list_vectors;   /* vectors read from the lists (batched modes: once per work item) */
+    uint64_t list_vectors;   /* vectors read by the work items (batched modes: once per work item) */
+    uint64_t list_once;      /* vectors of the probed lists, each list counted once per call */
+    uint64_t item_bytes;     /* algo_bytes with list_vectors in place of list_once (what the work
+                                items request; repeats of a list are mostly served by L2) */
 } e8qc_profile;
 int e8qc_e8q_profile(e8qc_index* idx, int enable, e8qc_profile* out);
 /* Plain search that allocates nothing (no counterpart in the reference; an
@@ -216,11 +219,21 @@ int e8qc_me8q_build(e8qc_me8q* idx, const float* data, size_t n, const float* ce
  * distances, ascending; k <= 128. Host or device pointers. */
 int e8qc_me8q_search(e8qc_me8q* idx, const float* queries, size_t nq, size_t k, size_t nprobe,
                      uint32_t* out_ids, float* out_dists, e8qc_stats* stats, void* stream);
+/* Search with an explicit mode (an addition of this library):
+ * E8QC_MODE_BATCHED is e8qc_me8q_search (grouped exact scan, every candidate
+ * scored with the estimator); E8QC_MODE_PRECISION generates candidates on the
+ * INT8 tensor cores from an int8 plane of each vector's levels scaled by its
+ * per-run coef (one scale per vector; built on first use, padded_dim bytes
+ * per vector) and rescores each query's best max(64, 4k) (at most 128) with
+ * the reference's estimator: returned distances are exact, recall against the
+ * exact scan is measured. */
+int e8qc_me8q_search_mode(e8qc_me8q* idx, const float* queries, size_t nq, size_t k, size_t nprobe, int mode,
+                          uint32_t* out_ids, float* out_dists, e8qc_stats* stats, void* stream);
 /* Serving form (an addition of this library): per-query k[i] <= k_max and
  * nprobe[i] (host arrays); output rows k_max wide, padded with UINT32_MAX /
- * +inf. */
+ * +inf; mode as in e8qc_me8q_search_mode. */
 int e8qc_me8q_search_ragged(e8qc_me8q* idx, const float* queries, size_t nq, const uint32_t* k,
-                            const uint32_t* nprobe, size_t k_max, uint32_t* out_ids, float* out_dists,
+                            const uint32_t* nprobe, size_t k_max, int mode, uint32_t* out_ids, float* out_dists,
                             void* stream);
 /* Me8qIndex::Estimate (me8q_measure.cpp:41-66); E8QC_ERANGE for an unknown id. */
 int e8qc_me8q_estimate(e8qc_me8q* idx, const float* query, uint32_t id, float* out);
@@ -260,10 +273,9 @@ int e8qc_e8q_autotune(e8qc_index* idx, int mode, size_t nq, size_t k, size_t npr
 typedef struct e8qc_plan e8qc_plan;
 int e8qc_plan_create(e8qc_index* idx, int mode, size_t max_queries, size_t k_max, size_t nprobe_max, int autotune,
                      e8qc_plan** out);
-/* The same over an ME8Q index: the grouped exact scan (E8QC_MODE_BATCHED);
- * autotune picks the work-queue order per batch size. */
-int e8qc_plan_create_me8q(e8qc_me8q* idx, size_t max_queries, size_t k_max, size_t nprobe_max, int autotune,
-                          e8qc_plan** out);
+/* The same over an ME8Q index, mode E8QC_MODE_BATCHED or E8QC_MODE_PRECISION. */
+int e8qc_plan_create_me8q(e8qc_me8q* idx, int mode, size_t max_queries, size_t k_max, size_t nprobe_max,
+                          int autotune, e8qc_plan** out);
 int e8qc_plan_run(e8qc_plan* plan, const float* queries, size_t nq, const uint32_t* k, const uint32_t* nprobe,
                   uint32_t* out_ids, float* out_dists, void* stream);
 int e8qc_plan_destroy(e8qc_plan* plan);
@@ -300,8 +312,8 @@ typedef struct e8qc_server_stats {
     uint64_t peak_batch_bytes;              /* largest admitted batch estimate */
 } e8qc_server_stats;
 int e8qc_server_start(e8qc_index* idx, const e8qc_server_config* cfg, e8qc_server** out);
-/* The serving loop over an ME8Q index (cfg->mode is ignored: the grouped
- * exact scan); submit / poll / stats / stop as above. */
+/* The serving loop over an ME8Q index (cfg->mode E8QC_MODE_BATCHED or
+ * E8QC_MODE_PRECISION); submit / poll / stats / stop as above. */
 int e8qc_server_start_me8q(e8qc_me8q* idx, const e8qc_server_config* cfg, e8qc_server** out);
 /* Copy nq host queries (dim floats each) into a new request; *request_id
  * identifies it. E8QC_EINVAL for bad k / nprobe, E8QC_ENOMEM when the request

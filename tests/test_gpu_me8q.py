@@ -150,3 +150,25 @@ def test_me8q_gpu_all_dropped_plan(e8q, oracle_lib):
     ids, d = idx.search(q, 10, 2)
     oi, od = orc.search(q, 10, 2)
     assert np.allclose(np.sort(d, axis=1), np.sort(od, axis=1), rtol=RTOL, atol=1e-5)
+
+
+@pytest.mark.parametrize("dim,avg,spec", [(768, 4.0, ""), (320, 3.0, ""), (250, 4.0, "64:3,64:0,128:5")])
+def test_me8q_gpu_precision_mode(e8q, oracle_lib, dim, avg, spec):
+    """Int8 tensor-core candidates + exact rescoring: recall of the exact
+    top-k, and every returned distance is the reference estimator's."""
+    n, nlist, nq = 20000, 32, 64
+    x, cm, lab = det_mixture(7100 + dim, n, dim, nlist, 0.6)
+    q = det_mixture(7200 + dim, nq, dim, nlist, 0.6)[0]
+    orc, idx = _build_both(e8q, oracle_lib, x, cm, lab, avg_bits=avg, seed=9, plan_spec=spec)
+    for k, nprobe in ((10, 8), (100, 4), (1, 32)):
+        ei, ed = idx.search(q, k, nprobe)  # exact grouped scan
+        pi, pdd = idx.search(q, k, nprobe, mode="precision")
+        oi, od = orc.search(q, k, nprobe)
+        hits = sum(len(set(a.tolist()) & set(b.tolist())) for a, b in zip(pi, ei))
+        assert hits / ei.size >= 0.97, (k, nprobe, hits / ei.size)
+        for r in range(nq):
+            ref = {int(i): float(d) for i, d in zip(oi[r], od[r]) if i != 0xFFFFFFFF}
+            for i, d in zip(pi[r], pdd[r]):
+                if int(i) in ref:
+                    assert rel_err(d, ref[int(i)]) < 1e-5, (k, nprobe, r, int(i))
+        assert np.all(np.diff(pdd, axis=1) >= 0)

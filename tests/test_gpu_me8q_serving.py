@@ -56,10 +56,11 @@ def test_me8q_plan_matches_direct(e8q, index):
         ref = idx.search_ragged(qq, k, npb, 32)
         assert same(got, ref), nq
     with pytest.raises(ValueError):
-        e8q.Plan(idx, mode="precision", max_queries=64)
+        e8q.Plan(idx, mode="plain", max_queries=64)
 
 
-def test_me8q_server_matches_alone(e8q, index):
+@pytest.mark.parametrize("mode", ["batched", "precision"])
+def test_me8q_server_matches_alone(e8q, index, mode):
     idx, q = index
     rng = np.random.default_rng(3)
     reqs, off = [], 0
@@ -69,7 +70,7 @@ def test_me8q_server_matches_alone(e8q, index):
             off = 0
         reqs.append((q[off:off + m], int(rng.choice([1, 10, 100])), int(rng.integers(1, 41))))
         off += m
-    with e8q.Server(idx, max_batch=256, slots=2) as srv:
+    with e8q.Server(idx, mode=mode, max_batch=256, slots=2) as srv:
         ids = [srv.submit(qq, k, npb) for qq, k, npb in reqs]
         got = [srv.result(i, timeout_ms=60000) for i in ids]
         st = srv.stats()
@@ -77,4 +78,15 @@ def test_me8q_server_matches_alone(e8q, index):
     assert 0 < st["p50_ms"] <= st["p99_ms"]
     for (qq, k, npb), res in zip(reqs, got):
         assert res is not None
-        assert same(res, idx.search(qq, k, npb)), (k, npb)
+        assert same(res, idx.search(qq, k, npb, mode=mode)), (k, npb)
+
+
+def test_me8q_precision_plan_matches_direct(e8q, index):
+    idx, q = index
+    rng = np.random.default_rng(5)
+    plan = e8q.Plan(idx, mode="precision", max_queries=200, k_max=16, nprobe_max=24)
+    for nq in (3, 64, 200):
+        qq = q[:nq]
+        k = rng.integers(1, 17, nq).astype(np.uint32)
+        npb = rng.integers(1, 25, nq).astype(np.uint32)
+        assert same(plan.run(qq, k, npb), idx.search_ragged(qq, k, npb, 16, mode="precision")), nq
