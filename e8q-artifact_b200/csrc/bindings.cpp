@@ -234,6 +234,9 @@ class E8qIndex {
         d["list_vectors"] = p.list_vectors;
         d["list_once"] = p.list_once;
         d["item_bytes"] = p.item_bytes;
+        d["final_launches"] = p.final_launches;
+        d["final_ms"] = p.final_ms;
+        d["final_bytes"] = p.final_bytes;
         return d;
     }
 

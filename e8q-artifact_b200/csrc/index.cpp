@@ -295,13 +295,18 @@ uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, con
     if (x->profiling) {
         E8QC_CUDA(cudaEventCreate(&ws.scan_ev0));
         E8QC_CUDA(cudaEventCreate(&ws.scan_ev1));
+        if (mode == E8QC_MODE_PRECISION) {
+            E8QC_CUDA(cudaEventCreate(&ws.final_ev0));
+            E8QC_CUDA(cudaEventCreate(&ws.final_ev1));
+        }
     }
     struct Drop {
         Workspace& w;
         ~Drop() {
-            if (w.scan_ev0) cudaEventDestroy(w.scan_ev0);
-            if (w.scan_ev1) cudaEventDestroy(w.scan_ev1);
-            w.scan_ev0 = w.scan_ev1 = nullptr;
+            for (cudaEvent_t* e : {&w.scan_ev0, &w.scan_ev1, &w.final_ev0, &w.final_ev1}) {
+                if (*e) cudaEventDestroy(*e);
+                *e = nullptr;
+            }
         }
     } drop{ws};
     int launches = 0;
@@ -333,10 +338,21 @@ uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, con
         // vector) pair (precision); item_bytes counts every work item's read
         const uint64_t per_vec = mode == E8QC_MODE_PRECISION ? static_cast<uint64_t>(x->pd) + 8
                                                              : static_cast<uint64_t>(x->bits) * x->pd / 8 + 8;
-        const uint64_t writes = mode == E8QC_MODE_PRECISION ? cnt[0] * 4 : 0;
+        const uint64_t writes = mode == E8QC_MODE_PRECISION ? cnt[0] * 2 : 0;  // fp16 proxy distances
         x->prof.algo_bytes += cnt[2] * per_vec + writes;
         x->prof.item_bytes += cnt[1] * per_vec + writes;
         x->prof.queries += nq;
+        if (mode == E8QC_MODE_PRECISION) {
+            // select + rescore: every proxy distance read once, then per query
+            // C candidates' codes + (g1, h3) + id
+            float fms = 0.0f;
+            E8QC_CUDA(cudaEventElapsedTime(&fms, ws.final_ev0, ws.final_ev1));
+            x->prof.final_launches += 1;
+            x->prof.final_ms += fms;
+            x->prof.final_bytes += cnt[0] * 2 + static_cast<uint64_t>(nq) *
+                                                    static_cast<uint64_t>(precision_candidates(static_cast<int>(k))) *
+                                                    (static_cast<uint64_t>(x->bits) * x->pd / 8 + 12);
+        }
     }
     return static_cast<uint64_t>(launches);
 }

@@ -56,6 +56,7 @@ constexpr int kPM = 128;  // pair rows per MMA tile (M = TMEM lanes)
 constexpr int kPN = 256;  // vectors per MMA tile (N)
 constexpr int kPK = 64;   // dimensions per staged K-chunk (2 MMAs of K = 32)
 constexpr int kOrdCap = 512;  // final kernel: probes per query it orders nearest list first
+constexpr size_t kFinalWideRows = 131072;  // final kernel: 4 warps per query from this many proxy rows
 constexpr size_t kScratchBudget = size_t(8) << 30;  // proxy rows per call chunk (bytes)
 
 // Per-query int8 quantisation: q8 = rint(q * 127 / max|q|); per-query factor
@@ -504,73 +505,93 @@ __device__ float me8q_rescore(const Me8qView& mv, uint32_t slot, const float* q,
     return static_cast<float>(acc);
 }
 
-// Per query (one warp): best C proxies over the query's rows, exact rescoring
-// of those candidates (E8Q estimator at BITS, or the ME8Q estimator), top-k
-// by exact distance.
-template <int BITS, bool ME8Q>
+// Per query (FW warps of a 4-warp block; 4/FW queries per block): best C
+// proxies over the query's rows, exact rescoring of those candidates (E8Q
+// estimator at BITS, or the ME8Q estimator), top-k by exact distance. FW = 4
+// for queries with many rows (long per-query chains), 1 otherwise (more
+// queries resident per SM).
+//
+// Rows are visited nearest list first (routing distance, then probe index):
+// the best proxies mostly sit in the nearest lists, so the thresholds settle
+// on the first rows and later steps pass the filter without offers (a query
+// with more than kOrdCap probes keeps list order). Warp w of a query streams
+// the rows of probes w, w + FW, ... keeping its own top-C; the query's warps
+// publish their C-th best in shared memory and each filters with the
+// smallest of them (a value above another warp's C-th best has C better
+// values and cannot be in the query's top C). The query's first warp merges
+// the FW lists; its warps rescore the C candidates and the first warp keeps
+// the top k.
+template <int BITS, bool ME8Q, int FW>
 __global__ void __launch_bounds__(128) precision_final_kernel(
     DevIndex ix, Me8qView mv, const float* __restrict__ rq, const __half* __restrict__ prox,
     const unsigned long long* __restrict__ rowbase, const uint32_t* __restrict__ pair_off,
     const uint32_t* __restrict__ pos_of, const uint32_t* __restrict__ probes, const float* __restrict__ pd2, int nq,
     const uint32_t* __restrict__ np_arr, int np_max, const uint32_t* __restrict__ k_arr, int k_uniform, int C,
     int out_stride, uint32_t* __restrict__ out_ids, float* __restrict__ out_d) {
+    static_assert(FW == 1 || FW == 2 || FW == 4, "warps per query");
+    constexpr int QPB = 4 / FW;  // queries per block
     constexpr int Q = 1 << BITS;
     constexpr int REP = table_rep(BITS);
     constexpr int GBL = group_blocks(BITS), GCH = group_chunks(BITS);
     constexpr int TCH = (64 * BITS + 127) / 128;
     extern __shared__ __align__(16) float fsm[];
-    float* tabrep = fsm;               // 2*Q*REP
-    float* sq = tabrep + 2 * Q * REP;  // 4 warps x pd, then 4 warps x kMaxK candidate slots
+    const int pd = ix.pd;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int qi = warp / FW, wq = warp % FW;  // query slot in the block, warp within the query
+    float* tabrep = fsm;                                           // 2*Q*REP (E8Q)
+    float* myq = tabrep + (ME8Q ? 0 : 2 * Q * REP) + qi * pd;      // the query's rotated query
+    float* sbufs = tabrep + (ME8Q ? 0 : 2 * Q * REP) + QPB * pd;   // 4 warps x 512
+    float* cd = sbufs + 4 * 512;                                   // 4 warps x kMaxK candidate distances
+    uint32_t* ci = reinterpret_cast<uint32_t*>(cd + 4 * kMaxK);    // 4 warps x kMaxK slots / ids
+    uint16_t* ord = reinterpret_cast<uint16_t*>(ci + 4 * kMaxK) + qi * kOrdCap;
+    __shared__ float s_thr[4];
+    const int q = blockIdx.x * QPB + qi;
+    const bool qvalid = q < nq;
     if constexpr (!ME8Q)
         for (int e = tid; e < 2 * Q * REP; e += blockDim.x) tabrep[e] = ix.tab[e / REP];
-    const int q = blockIdx.x * 4 + warp;
-    const int pd = ix.pd;
-    float* myq = sq + warp * pd;
-    if (q < nq)
-        for (int i = lane; i < pd; i += 32) myq[i] = rq[static_cast<size_t>(q) * pd + i];
-    __syncthreads();
-    if (q >= nq) return;
-    const int np = np_arr ? static_cast<int>(np_arr[q]) : np_max;
-    const int kq = k_arr ? static_cast<int>(k_arr[q]) : k_uniform;
-    const uint32_t* pr = probes + static_cast<size_t>(q) * np_max;
-    // Rows nearest list first (routing distance, then probe index): the best
-    // proxies mostly sit in the nearest lists, so the top-C threshold settles
-    // on the first rows and later steps pass the filter without offers. A
-    // query with more than kOrdCap probes keeps list order.
-    float* sbuf = sq + 4 * pd + 4 * kMaxK + warp * 512;  // d2 staging, then one step's values
-    uint16_t* ord = reinterpret_cast<uint16_t*>(sq + 4 * pd + 4 * kMaxK + 4 * 512) + warp * kOrdCap;
+    if (qvalid)
+        for (int i = wq * 32 + lane; i < pd; i += FW * 32) myq[i] = rq[static_cast<size_t>(q) * pd + i];
+    const int np = qvalid ? (np_arr ? static_cast<int>(np_arr[q]) : np_max) : 0;
+    const int kq = qvalid ? (k_arr ? static_cast<int>(k_arr[q]) : k_uniform) : 0;
+    const uint32_t* pr = probes + static_cast<size_t>(qvalid ? q : 0) * np_max;
     const bool reorder = np <= kOrdCap;
-    if (reorder) {
-        for (int i = lane; i < np; i += 32) sbuf[i] = pd2[static_cast<size_t>(q) * np_max + i];
-        __syncwarp();
-        for (int i = lane; i < np; i += 32) {
-            const float di = sbuf[i];
+    float* qstage = sbufs + qi * FW * 512;  // FW*512 >= kOrdCap floats: the query's d2 staging
+    if (reorder)
+        for (int i = wq * 32 + lane; i < np; i += FW * 32) qstage[i] = pd2[static_cast<size_t>(q) * np_max + i];
+    __syncthreads();
+    if (reorder)
+        for (int i = wq * 32 + lane; i < np; i += FW * 32) {
+            const float di = qstage[i];
             int r = 0;
             for (int j = 0; j < np; ++j) {
-                const float dj = sbuf[j];
+                const float dj = qstage[j];
                 r += (dj < di) | ((dj == di) & (j < i));
             }
             ord[r] = static_cast<uint16_t>(i);
         }
-        __syncwarp();
-    }
-    // 1. best C proxies (slot as tie-break). Row metadata for 32 probes at a
-    //    time sits in registers (lane j: probe w0 + j) and is read by shuffle;
-    //    values stream 512 per step, the next step's loads in flight while
-    //    the current step is filtered.
+    if (tid < 4) s_thr[tid] = inf_f();
+    __syncthreads();
+    volatile float* vthr = s_thr + qi * FW;
+    float* sbuf = sbufs + warp * 512;
+
+    // 1. best C proxies of this warp's rows (slot as tie-break). Row metadata
+    //    for 32 of the warp's probes at a time sits in registers (lane j: the
+    //    warp's probe w0 + j) and is read by shuffle; values stream 512 per
+    //    step, two steps in flight ahead of the one being filtered.
+    const int npw = np > wq ? (np - wq + FW - 1) / FW : 0;
     WarpTopK cand;
     cand.init(C);
     int w0 = -32;
-    unsigned long long m_off = 0;  // this lane's row: float offset into prox
+    unsigned long long m_off = 0;  // this lane's row: element offset into prox
     uint32_t m_len = 0, m_slot0 = 0;
     auto load_window = [&](int base) {
         w0 = base;
-        const int p = base + lane;
+        const int i = base + lane;
         m_off = 0;
         m_len = 0;
         m_slot0 = 0;
-        if (p < np) {
+        if (i < npw) {
+            const int p = wq + FW * i;
             const int pp = reorder ? static_cast<int>(ord[p]) : p;
             const uint32_t L = pr[pp];
             const uint32_t t0 = ix.tile_begin[L];
@@ -586,20 +607,20 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
         uint32_t v0, len, slot0;
         unsigned long long off;
     };
-    // the step after (p, v0 + 512), skipping empty rows; p == np when done
+    // the step after (p, v0 + 512), skipping empty rows; p >= npw when done
     auto advance = [&](int p, uint32_t v0, uint32_t len) {
         Step st{p, v0 + 512, len, 0, 0};
         if (st.v0 >= len) {
             st.p = p + 1;
             st.v0 = 0;
             for (;; ++st.p) {
-                if (st.p >= np) break;
+                if (st.p >= npw) break;
                 if (st.p >= w0 + 32) load_window(w0 + 32);
                 const uint32_t l = __shfl_sync(kFull, m_len, st.p - w0);
                 if (l > 0) break;
             }
         }
-        if (st.p < np) {
+        if (st.p < npw) {
             st.len = __shfl_sync(kFull, m_len, st.p - w0);
             st.slot0 = __shfl_sync(kFull, m_slot0, st.p - w0);
             st.off = __shfl_sync(kFull, m_off, st.p - w0);
@@ -612,21 +633,28 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
             const uint32_t va = st.v0 + 256 * j + 8 * lane;
-            x[j] = (st.p < np && va < st.len) ? __ldcs(reinterpret_cast<const uint4*>(prox + st.off) + (va >> 3))
-                                              : make_uint4(0u, 0u, 0u, 0u);
+            x[j] = (st.p < npw && va < st.len) ? __ldcs(reinterpret_cast<const uint4*>(prox + st.off) + (va >> 3))
+                                               : make_uint4(0u, 0u, 0u, 0u);
         }
     };
     load_window(0);
     Step cur = advance(-1, 0, 0);  // first non-empty row
     uint4 cx[2];
     load_step(cur, cx);
-    while (cur.p < np) {
-        const Step nxt = advance(cur.p, cur.v0, cur.len);
-        uint4 nx[2];
-        load_step(nxt, nx);
+    Step nxt = advance(cur.p, cur.v0, cur.len);
+    uint4 nx[2];
+    load_step(nxt, nx);
+    while (cur.p < npw) {
+        const Step nn = advance(nxt.p, nxt.v0, nxt.len);
+        uint4 nnx[2];
+        load_step(nn, nnx);
         // filter: a 16-bit mask per lane of the values that can enter the
-        // list; most steps have none once the threshold has settled.
-        // Value t of this lane is column 256*(t/8) + 8*lane + t%8.
+        // query's top C; value t of this lane is column 256*(t/8) + 8*lane + t%8
+        float filt = cand.thr_d;
+        if constexpr (FW > 1) {
+#pragma unroll
+            for (int w2 = 0; w2 < FW; ++w2) filt = fminf(filt, vthr[w2]);
+        }
         float v[16];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
@@ -642,7 +670,7 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
 #pragma unroll
         for (int t = 0; t < 16; ++t) {
             const uint32_t va = cur.v0 + 256 * (t >> 3) + 8 * lane + (t & 7);
-            hit |= static_cast<uint32_t>(va < cur.len && !(v[t] > cand.thr_d)) << t;
+            hit |= static_cast<uint32_t>(va < cur.len && !(v[t] > filt)) << t;
         }
         if (__any_sync(kFull, hit != 0)) {
             // staged in shared memory so the offer loop indexes it
@@ -654,7 +682,7 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
             }
             __syncwarp();
             // one offer per round: each lane its lowest remaining hit; offer()
-            // re-checks every value against the threshold of that moment
+            // re-checks every value against the warp's threshold of that moment
 #pragma unroll 1
             while (__any_sync(kFull, hit != 0)) {
                 const bool has = hit != 0;
@@ -665,36 +693,46 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
                 cand.offer_pair(has ? sbuf[col] : inf_f(), cur.slot0 + cur.v0 + col, has);
             }
             __syncwarp();
+            if constexpr (FW > 1)
+                if (lane == 0) vthr[wq] = cand.thr_d;
         }
         cur = nxt;
         cx[0] = nx[0];
         cx[1] = nx[1];
+        nxt = nn;
+        nx[0] = nnx[0];
+        nx[1] = nnx[1];
     }
-    // 2. exact rescoring of candidate (s, lane); 3. top-k by exact distance.
-    //    The candidates' slots go through shared memory so the loop below
-    //    stays rolled (one offer site).
-    uint32_t* cslots = reinterpret_cast<uint32_t*>(sq + 4 * pd) + warp * kMaxK;
-    {
-#pragma unroll
-        for (int s2 = 0; s2 < 4; ++s2)
-            if (s2 * 32 < C) cslots[s2 * 32 + lane] = cand.id[s2];
-        __syncwarp();
+    // 2. the query's first warp merges its warps' lists into the query's top C
+    float* qcd = cd + qi * FW * kMaxK;
+    uint32_t* qci = ci + qi * FW * kMaxK;
+    if constexpr (FW > 1) {
+        cand.store(cd + warp * kMaxK, ci + warp * kMaxK, C);
+        __syncthreads();
+        if (wq == 0) {
+            for (int w2 = 1; w2 < FW; ++w2)
+                for (int s2 = 0; s2 * 32 < C; ++s2) {
+                    const int j = s2 * 32 + lane;
+                    const bool in = j < C && qci[w2 * kMaxK + j] != 0xFFFFFFFFu;
+                    cand.offer_pair(in ? qcd[w2 * kMaxK + j] : inf_f(), in ? qci[w2 * kMaxK + j] : 0xFFFFFFFFu, in);
+                }
+            cand.store(qcd, qci, C);
+        }
+    } else {
+        cand.store(qcd, qci, C);
     }
-    WarpTopK top;
-    top.init(kq);
-    const uint32_t tb_addr = static_cast<uint32_t>(__cvta_generic_to_shared(tabrep)) + (lane % REP) * 4u;
-    const float4* sq4 = reinterpret_cast<const float4*>(myq);
-    const int ng = (pd / 8) / GBL;
-    const bool tail = ((pd / 8) % GBL) != 0;
-#pragma unroll 1
-    for (int s = 0; s < 4; ++s) {
-        if (s * 32 >= C) break;
-        const uint32_t slot = cslots[s * 32 + lane];
-        const bool live = s * 32 + lane < C && slot != 0xFFFFFFFFu;
+    __syncthreads();
+    // 3. exact rescoring: the query's warp wq takes candidates wq*32 + lane,
+    //    + FW*32, ...; each lane writes its candidate's (distance, id) over its
+    //    (proxy, slot) entry
+    for (int j = wq * 32 + lane; j - lane < C; j += FW * 32) {
+        const uint32_t slot = j < C ? qci[j] : 0xFFFFFFFFu;
+        const bool live = slot != 0xFFFFFFFFu;
+        const uint32_t tile = live ? slot >> 5 : 0u;
         float dist = inf_f();
         uint32_t gid = 0xFFFFFFFFu;
+        float d2 = 0.0f;
         if (live) {
-            const uint32_t tile = slot >> 5;
             // d2 of (query, the candidate's list): the query's probes are in list order
             const uint32_t list = ix.list_of_tile[tile];
             int lo = 0, hi = np;
@@ -703,10 +741,16 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
                 if (pr[mid] <= list) lo = mid;
                 else hi = mid;
             }
-            const float d2 = pd2[static_cast<size_t>(q) * np_max + lo];
-            if constexpr (ME8Q) {
-                dist = me8q_rescore(mv, slot, myq, d2);
-            } else {
+            d2 = pd2[static_cast<size_t>(q) * np_max + lo];
+        }
+        if constexpr (ME8Q) {
+            if (live) dist = me8q_rescore(mv, slot, myq, d2);
+        } else {
+            const uint32_t tb_addr = static_cast<uint32_t>(__cvta_generic_to_shared(tabrep)) + (lane % REP) * 4u;
+            const float4* sq4 = reinterpret_cast<const float4*>(myq);
+            const int ng = (pd / 8) / GBL;
+            const bool tail = ((pd / 8) % GBL) != 0;
+            if (live) {
                 const int vl = static_cast<int>(slot & 31u);
                 const uint4* tp = ix.codes + static_cast<size_t>(tile) * ix.nch * 32;
                 float acc0 = 0.0f, acc1 = 0.0f;
@@ -717,17 +761,31 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
                 const float S = __fadd_rn(acc0, acc1);
                 dist = __fmaf_rn(-__fmul_rn(2.0f, __ldg(ix.g1 + slot)), S, __fadd_rn(d2, __ldg(ix.h3 + slot)));
             }
-            gid = __ldg(ix.ids + slot);
         }
-        top.offer_pair(dist, gid, live);
+        if (live) gid = __ldg(ix.ids + slot);
+        if (j < C) {
+            qcd[j] = dist;
+            qci[j] = gid;
+        }
     }
+    __syncthreads();
+    // 4. top k by exact distance
+    if (wq == 0 && qvalid) {
+        WarpTopK top;
+        top.init(kq);
+        for (int s2 = 0; s2 * 32 < C; ++s2) {
+            const int j = s2 * 32 + lane;
+            const bool in = j < C && qci[j] != 0xFFFFFFFFu;
+            top.offer_pair(in ? qcd[j] : inf_f(), in ? qci[j] : 0xFFFFFFFFu, in);
+        }
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        const int j = s * 32 + lane;
-        if (j < out_stride) {
-            const bool in = j < kq;
-            out_d[static_cast<size_t>(q) * out_stride + j] = in ? top.d[s] : inf_f();
-            out_ids[static_cast<size_t>(q) * out_stride + j] = in ? top.id[s] : 0xFFFFFFFFu;
+        for (int s3 = 0; s3 < 4; ++s3) {
+            const int j = s3 * 32 + lane;
+            if (j < out_stride) {
+                const bool in = j < kq;
+                out_d[static_cast<size_t>(q) * out_stride + j] = in ? top.d[s3] : inf_f();
+                out_ids[static_cast<size_t>(q) * out_stride + j] = in ? top.id[s3] : 0xFFFFFFFFu;
+            }
         }
     }
 }
@@ -801,27 +859,40 @@ void launch_scan(const DevIndex& ix, Workspace& ws, size_t a_rows, size_t plane_
 }
 
 // Per-query selection + exact rescoring of one chunk of queries.
-template <int BITS, bool ME8Q = false>
-int launch_final(const DevIndex& ix, const Me8qView& mv, Workspace& ws, const float* rq, size_t nq,
-                 const uint32_t* k_arr, const uint32_t* np_arr, int k_max, int np_max, int C, int out_stride,
-                 uint32_t* out_ids, float* out_d, cudaStream_t s) {
+template <int BITS, bool ME8Q, int FW>
+int launch_final_fw(const DevIndex& ix, const Me8qView& mv, Workspace& ws, const float* rq, size_t nq,
+                    const uint32_t* k_arr, const uint32_t* np_arr, int k_max, int np_max, int C, int out_stride,
+                    uint32_t* out_ids, float* out_d, cudaStream_t s) {
     int dev = 0;
     E8QC_CUDA(cudaGetDevice(&dev));
     constexpr int REP = table_rep(BITS);
-    const size_t fsmem = (static_cast<size_t>(2) * (1 << BITS) * REP + 4 * static_cast<size_t>(ix.pd) + 4 * kMaxK +
-                          4 * 512) * 4 + 4 * kOrdCap * 2;
+    constexpr int QPB = 4 / FW;
+    const size_t fsmem = ((ME8Q ? 0 : static_cast<size_t>(2) * (1 << BITS) * REP) +
+                          static_cast<size_t>(QPB) * ix.pd + 4 * 512 + 4 * kMaxK * 2) * 4 +
+                         static_cast<size_t>(QPB) * kOrdCap * 2;
     static size_t fconfigured[64] = {};
     if (fsmem > 48 * 1024 && fconfigured[dev & 63] < fsmem) {
-        E8QC_CUDA(cudaFuncSetAttribute(precision_final_kernel<BITS, ME8Q>,
+        E8QC_CUDA(cudaFuncSetAttribute(precision_final_kernel<BITS, ME8Q, FW>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(fsmem)));
         fconfigured[dev & 63] = fsmem;
     }
-    precision_final_kernel<BITS, ME8Q><<<static_cast<unsigned>((nq + 3) / 4), 128, fsmem, s>>>(
+    precision_final_kernel<BITS, ME8Q, FW><<<static_cast<unsigned>((nq + QPB - 1) / QPB), 128, fsmem, s>>>(
         ix, mv, rq, ws.p_prox.as<__half>(), ws.p_rowbase.as<unsigned long long>(), ws.b_off.as<uint32_t>(),
         ws.b_pos.as<uint32_t>(), ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(), static_cast<int>(nq), np_arr,
         np_max, k_arr, k_max, C, out_stride, out_ids, out_d);
     E8QC_CUDA(cudaGetLastError());
     return 1;
+}
+
+template <int BITS, bool ME8Q = false>
+int launch_final(const DevIndex& ix, const Me8qView& mv, Workspace& ws, const float* rq, size_t nq,
+                 const uint32_t* k_arr, const uint32_t* np_arr, int k_max, int np_max, int C, int out_stride,
+                 uint32_t* out_ids, float* out_d, size_t rows_per_query, cudaStream_t s) {
+    if (rows_per_query >= kFinalWideRows)
+        return launch_final_fw<BITS, ME8Q, 4>(ix, mv, ws, rq, nq, k_arr, np_arr, k_max, np_max, C, out_stride,
+                                              out_ids, out_d, s);
+    return launch_final_fw<BITS, ME8Q, 1>(ix, mv, ws, rq, nq, k_arr, np_arr, k_max, np_max, C, out_stride, out_ids,
+                                          out_d, s);
 }
 
 template <int BITS>
@@ -924,10 +995,13 @@ int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t 
         E8QC_CUDA(cudaGetLastError());
         launch_scan(ix, ws, arows, static_cast<size_t>(ix.ntiles) * 32 + kPN, s);
         launches += 4;
+        ws.mark_final(false, s);
         if (me8q) {
             launches += launch_final<1, true>(ix, *me8q, ws, rqc, n, kc, npc, static_cast<int>(k),
                                               static_cast<int>(nprobe), C, static_cast<int>(out_stride),
-                                              out_ids + off * out_stride, out_d + off * out_stride, s);
+                                              out_ids + off * out_stride, out_d + off * out_stride, rows_per_query,
+                                              s);
+            ws.mark_final(true, s);
             continue;
         }
         switch (ix.bits) {
@@ -935,7 +1009,7 @@ int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t 
     case b:                                                                                                      \
         launches += launch_final<b>(ix, none, ws, rqc, n, kc, npc, static_cast<int>(k), static_cast<int>(nprobe), \
                                     C, static_cast<int>(out_stride), out_ids + off * out_stride,                 \
-                                    out_d + off * out_stride, s);                                                \
+                                    out_d + off * out_stride, rows_per_query, s);                                \
         break;
             E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
             E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
@@ -943,6 +1017,7 @@ int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t 
 #undef E8QC_CASE
             default: fail(E8QC_EINVAL, "bits out of range");
         }
+        ws.mark_final(true, s);
     }
     return launches;
 }

@@ -76,6 +76,12 @@ struct Workspace {
         cudaEvent_t e = end ? scan_ev1 : scan_ev0;
         if (e) E8QC_CUDA(cudaEventRecord(e, s));
     }
+    // the same around the precision path's select + rescore kernel
+    cudaEvent_t final_ev0 = nullptr, final_ev1 = nullptr;
+    void mark_final(bool end, cudaStream_t s) {
+        cudaEvent_t e = end ? final_ev1 : final_ev0;
+        if (e) E8QC_CUDA(cudaEventRecord(e, s));
+    }
 
     ~Workspace() {
         if (err_host) cudaFreeHost(err_host);

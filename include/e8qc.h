@@ -140,12 +140,16 @@ typedef struct e8qc_profile {
     uint64_t candidates;     /* (query, vector) pairs scored */
     uint64_t algo_bytes;     /* plain: candidates * (bits*padded_dim/8 + 8), codes + g1/h3; batched:
                                 list_once * (bits*padded_dim/8 + 8); precision: list_once *
-                                (padded_dim + 8) int8 proxies + g1/h3, plus 4 per candidate written */
+                                (padded_dim + 8) int8 proxies + g1/h3, plus 2 per candidate written */
     uint64_t queries;
     uint64_t list_vectors;   /* vectors read by the work items (batched modes: once per work item) */
     uint64_t list_once;      /* vectors of the probed lists, each list counted once per call */
     uint64_t item_bytes;     /* algo_bytes with list_vectors in place of list_once (what the work
                                 items request; repeats of a list are mostly served by L2) */
+    uint64_t final_launches; /* precision mode: select + rescore kernel launches timed */
+    double final_ms;         /* their summed CUDA-event time */
+    uint64_t final_bytes;    /* their algorithmic bytes: 2 per proxy distance read + per query
+                                C * (bits*padded_dim/8 + 12) for the rescored candidates */
 } e8qc_profile;
 int e8qc_e8q_profile(e8qc_index* idx, int enable, e8qc_profile* out);
 /* Plain search that allocates nothing (no counterpart in the reference; an
