@@ -315,6 +315,7 @@ uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, con
         x->proxy.alloc(proxy_plane_bytes(x->view, x->ntiles));
         launches += launch_build_proxy(x->view, static_cast<int>(x->ntiles), x->proxy.as<uint4>(), s);
         x->view.proxy = x->proxy.as<uint4>();
+        x->view.proxy_scale = precision_proxy_step(x->view.bits, x->view.pd);
     }
     if (mode == E8QC_MODE_PRECISION)
         launches += precision_search(x->view, ws, rq, nq, k_arr, np_arr, k, np, k, ids_d, d_d,
@@ -386,6 +387,7 @@ class E8qTarget final : public SearchTarget {
             launch_build_proxy(x_->view, static_cast<int>(x_->ntiles), x_->proxy.as<uint4>(), nullptr);
             E8QC_CUDA(cudaStreamSynchronize(nullptr));
             x_->view.proxy = x_->proxy.as<uint4>();
+            x_->view.proxy_scale = precision_proxy_step(x_->view.bits, x_->view.pd);
         }
     }
     // Workspace buffers plus the caller's query / k / nprobe / result buffers.
@@ -899,6 +901,7 @@ int e8qc_e8q_autotune(e8qc_index* x, int mode, size_t nq, size_t k, size_t nprob
             x->proxy.alloc(proxy_plane_bytes(x->view, x->ntiles));
             launch_build_proxy(x->view, static_cast<int>(x->ntiles), x->proxy.as<uint4>(), s);
             x->view.proxy = x->proxy.as<uint4>();
+            x->view.proxy_scale = precision_proxy_step(x->view.bits, x->view.pd);
         }
         const TuneResult r = autotune_run(x, x->ws, mode, nq, k, nprobe, s);
         if (out) *out = e8qc_tuning{r.sched, r.stages, r.best_ms, r.default_ms};

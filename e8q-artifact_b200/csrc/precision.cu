@@ -1,24 +1,25 @@
 // Precision search path: INT8 tensor-core candidate generation + exact
 // rescoring.
 //
-// The lattice code of a vector is a small integer point: coordinate i of a
-// block is t_i + eta with t_i the signed digit and eta = 1/4 + br/2, so
-// 2*(t + eta) = (2t + br) + 1/2. p = (2t + br) >> max(0, bits - 7) is an exact
-// int8 for rates <= 7 and keeps the top 8 bits above. The query is quantised
-// to int8 with a per-query scale qs, S8 = sum_i q8_i * p_i runs on tcgen05
-// kind::i8 with int32 accumulation in TMEM, and since the level tables are
-// close to linear in t + eta near the centre,
-//   S ~ S' = alpha * shift / (4 qs) * (2 S8 + sum(q8)),   shift = 2^max(0, bits-7)
-// (alpha: a weighted least-squares fit of table against t + eta). The proxy
-// distance D' = (d2 + h3) - 2*g1*S' of every (query, vector) pair is written
-// to a scratch row per (query, list) pair in HBM (4 bytes per pair: far less
-// than the codes the pair stands for); a per-query kernel then selects the
-// query's best C proxies over all its rows, rescores those C candidates with
-// the exact estimator of the plain scan (src/simd/e8q_search_generic.cpp:58-66;
-// same table and per-block FMA chain, blocks summed in order into two
-// alternating accumulators) and keeps the top-k. A rescored distance depends
-// only on (query, vector), so results do not depend on what else is in the
-// batch.
+// Every coordinate of a stored vector is one entry of a small level table
+// (table[br][digit] = level / sqrt(Dpad), 2 x 2^bits values). The proxy of a
+// coordinate is that entry quantised to int8 with one step for the whole
+// table, p = rint(table / step), step = max|table| / 127 (an int8 lookup per
+// digit, so each vector's proxy row is its level sequence to 8 bits). The
+// query is quantised to int8 with a per-query scale qs, S8 = sum_i q8_i * p_i
+// runs on tcgen05 kind::i8 with int32 accumulation in TMEM, and
+//   S ~ S' = step * S8 / qs.
+// The proxy distance D' = (d2 + h3) - 2*g1*S' of every (query, vector) pair
+// is written, scaled per query, as fp16 to a scratch row per (query, list)
+// pair in HBM (2 bytes per pair: far less than the codes the pair stands
+// for); a per-query kernel then selects the query's best C proxies over all
+// its rows, rescores those C candidates with the exact estimator of the plain
+// scan (src/simd/e8q_search_generic.cpp:58-66; same table and per-block FMA
+// chain, blocks summed in order into two alternating accumulators) and keeps
+// the top-k. A rescored distance depends only on (query, vector), so results
+// do not depend on what else is in the batch. An ME8Q index uses the same
+// scan with each vector's coef-scaled levels quantised per vector
+// (me8q_kernels.cu) and the ME8Q estimator for rescoring.
 //
 // The proxies of every vector are decoded once into an int8 "proxy plane"
 // stored in the MMA operand layout (built on the first precision search), and
@@ -57,6 +58,12 @@ constexpr int kPN = 256;  // vectors per MMA tile (N)
 constexpr int kPK = 64;   // dimensions per staged K-chunk (2 MMAs of K = 32)
 constexpr int kOrdCap = 512;  // final kernel: probes per query it orders nearest list first
 constexpr size_t kFinalWideRows = 131072;  // final kernel: 4 warps per query from this many proxy rows
+
+// Proxy candidates rescored per query, from the query's own k (so a query's
+// result does not depend on the k of the others in its batch).
+__host__ __device__ constexpr int candidates_for(int k) {
+    return (3 * k > 32 ? 3 * k : 32) < kMaxK ? (3 * k > 32 ? 3 * k : 32) : kMaxK;
+}
 constexpr size_t kScratchBudget = size_t(8) << 30;  // proxy rows per call chunk (bytes)
 
 // Per-query int8 quantisation: q8 = rint(q * 127 / max|q|); per-query factor
@@ -144,17 +151,17 @@ __global__ void rowbase_kernel(const uint32_t* __restrict__ list_cnt, const uint
     }
 }
 
-// Proxy integers of one block (8 dims) as 8 packed int8.
+// Proxies of one block (8 dims) as 8 packed int8: the quantised table entry
+// of each digit (lut: 2 x 2^BITS int8, branch-major).
 template <int BITS>
-__device__ __forceinline__ uint2 block_proxy(const uint32_t* w, int base) {
-    constexpr int SH = BITS > 7 ? BITS - 7 : 0;
+__device__ __forceinline__ uint2 block_proxy(const uint32_t* w, int base, const int8_t* __restrict__ lut) {
     uint32_t dg[8];
     const int br = decode_block<BITS>(w, base, dg);
+    const int8_t* t = lut + (br ? (1 << BITS) : 0);
     uint32_t lo = 0, hi = 0;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        const int t = static_cast<int>(dg[i]) - ((dg[i] >> (BITS - 1)) ? (1 << BITS) : 0);
-        const uint32_t p = static_cast<uint32_t>((2 * t + br) >> SH) & 0xFFu;  // arithmetic shift: floor
+        const uint32_t p = static_cast<uint32_t>(static_cast<uint8_t>(__ldg(t + dg[i])));
         if (i < 4) lo |= p << (8 * i);
         else hi |= p << (8 * (i - 4));
     }
@@ -169,7 +176,8 @@ __device__ __forceinline__ uint2 block_proxy(const uint32_t* w, int base) {
 // decoded into 64 proxies (four 16-byte stores; 8 consecutive slots fill 128
 // contiguous bytes).
 template <int BITS>
-__global__ void __launch_bounds__(256) build_proxy_kernel(DevIndex ix, int nslots, unsigned char* __restrict__ plane) {
+__global__ void __launch_bounds__(256) build_proxy_kernel(DevIndex ix, int nslots, const int8_t* __restrict__ lut,
+                                                          unsigned char* __restrict__ plane) {
     constexpr int NW = 2 * BITS;
     const int slot = blockIdx.x * 256 + threadIdx.x;
     const int kc = blockIdx.y;
@@ -188,7 +196,7 @@ __global__ void __launch_bounds__(256) build_proxy_kernel(DevIndex ix, int nslot
     uint32_t o[16];
 #pragma unroll
     for (int blk = 0; blk < 8; ++blk) {
-        const uint2 pr = block_proxy<BITS>(w, blk * 8 * BITS);
+        const uint2 pr = block_proxy<BITS>(w, blk * 8 * BITS, lut);
         o[2 * blk] = pr.x;
         o[2 * blk + 1] = pr.y;
     }
@@ -553,6 +561,7 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
         for (int i = wq * 32 + lane; i < pd; i += FW * 32) myq[i] = rq[static_cast<size_t>(q) * pd + i];
     const int np = qvalid ? (np_arr ? static_cast<int>(np_arr[q]) : np_max) : 0;
     const int kq = qvalid ? (k_arr ? static_cast<int>(k_arr[q]) : k_uniform) : 0;
+    C = candidates_for(kq);  // the query's own candidate count (uniform within the query's warps)
     const uint32_t* pr = probes + static_cast<size_t>(qvalid ? q : 0) * np_max;
     const bool reorder = np <= kOrdCap;
     float* qstage = sbufs + qi * FW * 512;  // FW*512 >= kOrdCap floats: the query's d2 staging
@@ -896,32 +905,42 @@ int launch_final(const DevIndex& ix, const Me8qView& mv, Workspace& ws, const fl
 }
 
 template <int BITS>
-int launch_build_proxy_bits(const DevIndex& ix, int ntiles, uint4* plane, cudaStream_t s) {
+int launch_build_proxy_bits(const DevIndex& ix, int ntiles, const int8_t* lut, uint4* plane, cudaStream_t s) {
     const int nslots = ntiles * 32;
     dim3 g(static_cast<unsigned>((nslots + 255) / 256), static_cast<unsigned>(ix.pd / kPK));
-    build_proxy_kernel<BITS><<<g, 256, 0, s>>>(ix, nslots, reinterpret_cast<unsigned char*>(plane));
+    build_proxy_kernel<BITS><<<g, 256, 0, s>>>(ix, nslots, lut, reinterpret_cast<unsigned char*>(plane));
     E8QC_CUDA(cudaGetLastError());
     return 1;
 }
 
 }  // namespace
 
-double precision_alpha(int bits, int pd) {
+// The level table as the device holds it (fp32 level / sqrt(Dpad)), its
+// int8 step and the quantised table (branch-major).
+std::vector<int8_t> proxy_table(int bits, int pd, float* step) {
     const int q = 1 << bits;
-    const double s = fixed_scale(bits);
-    double sxy = 0.0, sxx = 0.0;
+    std::vector<float> tab(2 * static_cast<size_t>(q));
+    float amax = 0.0f;
     for (int br = 0; br < 2; ++br) {
         const std::vector<double> lev = branch_levels(bits, br);
         for (int d = 0; d < q; ++d) {
-            const int t = d >= q / 2 ? d - q : d;
-            const double x = t + 0.25 + 0.5 * br;
-            const double y = lev[d] / std::sqrt(static_cast<double>(pd));
-            const double w = std::exp(-lev[d] * lev[d] / (2.0 * s * s));
-            sxy += w * x * y;
-            sxx += w * x * x;
+            tab[br * q + d] = static_cast<float>(lev[d] / std::sqrt(static_cast<double>(pd)));
+            amax = std::max(amax, std::fabs(tab[br * q + d]));
         }
     }
-    return sxx > 0.0 ? sxy / sxx : 0.0;
+    *step = amax > 0.0f ? amax / 127.0f : 1.0f;
+    std::vector<int8_t> lut(tab.size());
+    for (size_t e = 0; e < tab.size(); ++e) {
+        const long v = std::lrint(static_cast<double>(tab[e]) / static_cast<double>(*step));
+        lut[e] = static_cast<int8_t>(std::max(-127L, std::min(127L, v)));
+    }
+    return lut;
+}
+
+float precision_proxy_step(int bits, int pd) {
+    float step = 1.0f;
+    proxy_table(bits, pd, &step);
+    return step;
 }
 
 size_t proxy_plane_bytes(const DevIndex& ix, size_t ntiles) {
@@ -930,21 +949,28 @@ size_t proxy_plane_bytes(const DevIndex& ix, size_t ntiles) {
 
 int launch_build_proxy(const DevIndex& ix, int ntiles, uint4* plane, cudaStream_t s) {
     if (ix.pd % kPK != 0) fail(E8QC_EINVAL, "precision search needs the padded dimension to be a multiple of 64");
+    if (ix.bits < 1 || ix.bits > 13) fail(E8QC_EINVAL, "bits out of range");
     // the slots past the last tile are read by the last MMA tile: zero them
     E8QC_CUDA(cudaMemsetAsync(plane, 0, proxy_plane_bytes(ix, ntiles), s));
+    float step = 1.0f;
+    const std::vector<int8_t> lut_h = proxy_table(ix.bits, ix.pd, &step);
+    DevBuf lut;  // one-time build: freed after the kernel below has run
+    lut.upload(lut_h.data(), lut_h.size(), s);
+    int launches = 0;
     switch (ix.bits) {
 #define E8QC_CASE(b) \
-    case b: return 1 + launch_build_proxy_bits<b>(ix, ntiles, plane, s);
+    case b: launches = 1 + launch_build_proxy_bits<b>(ix, ntiles, lut.as<int8_t>(), plane, s); break;
         E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
         E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
         E8QC_CASE(13)
 #undef E8QC_CASE
         default: fail(E8QC_EINVAL, "bits out of range");
     }
-    return 0;
+    E8QC_CUDA(cudaStreamSynchronize(s));
+    return launches;
 }
 
-int precision_candidates(int k) { return std::min(kMaxK, std::max(64, 4 * k)); }
+int precision_candidates(int k) { return candidates_for(k); }
 
 size_t precision_row_scratch(size_t nq, size_t rows_per_query) {
     const size_t per_q = std::max<size_t>(1, rows_per_query) * sizeof(__half);
@@ -958,11 +984,10 @@ int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t 
     if (ix.pd % kPK != 0) fail(E8QC_EINVAL, "precision search needs the padded dimension to be a multiple of 64");
     if (ix.proxy == nullptr) fail(E8QC_ESTATE, "precision search needs the proxy plane (launch_build_proxy)");
     const int C = precision_candidates(static_cast<int>(k));
-    // E8Q: S' = alpha*shift/(4 qs) * (2 S8 + sum q8) from integer lattice
-    // proxies; ME8Q: S' = S8 / qs = (1/(2 qs)) * (2 S8 + 0) from the slot-
-    // scaled level proxies (the slot's sigma sits in the g1 plane, hsum in h3)
-    const int shift = !me8q && ix.bits > 7 ? (1 << (ix.bits - 7)) : 1;
-    const float coef = me8q ? 0.5f : static_cast<float>(precision_alpha(ix.bits, ix.pd) * shift / 4.0);
+    // the epilogue forms S' = (coef / qs) * (2 S8 + 0): E8Q coef = step / 2
+    // (one table step for every vector); ME8Q coef = 1/2 with the slot's own
+    // step in the g1 plane (hsum in h3)
+    const float coef = me8q ? 0.5f : 0.5f * ix.proxy_scale;
     const Me8qView none{};
     // proxy rows of a chunk of queries stay within the scratch budget
     const size_t per_q = std::max<size_t>(1, rows_per_query) * sizeof(__half);
@@ -987,7 +1012,7 @@ int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t 
         rowbase_kernel<<<1, 1024, 0, s>>>(ws.b_cnt.as<uint32_t>(), ix.tile_begin, ix.nlist,
                                           ws.p_rowbase.as<unsigned long long>());
         quantize_kernel<<<static_cast<unsigned>(n), 256, 0, s>>>(
-            rqc, ix.pd, coef, me8q ? 0 : 1, ws.p_q8.as<int8_t>(), ws.p_scale.as<float>(), ws.p_sum.as<float>(),
+            rqc, ix.pd, coef, 0, ws.p_q8.as<int8_t>(), ws.p_scale.as<float>(), ws.p_sum.as<float>(),
             ws.b_pd2.as<float>(), npc, static_cast<int>(nprobe), static_cast<int>(nprobe), ws.p_pscale.as<float>());
         const size_t ga = arows * (ix.pd / 16);
         gather_a8_kernel<<<static_cast<unsigned>((ga + 255) / 256), 256, 0, s>>>(

@@ -11,10 +11,9 @@
 
 namespace e8qc {
 
-// Slope of the weighted least-squares line level/sqrt(pd) ~ alpha * (t + eta)
-// over both branches (weights: the N(0, s^2) density at each level, s the
-// rate's encoding scale).
-double precision_alpha(int bits, int pd);
+// The int8 step of the E8Q proxy plane for `bits` at padded dimension pd
+// (set as DevIndex::proxy_scale once the plane is built).
+float precision_proxy_step(int bits, int pd);
 
 // Bytes of the int8 proxy plane: the padded slots (plus one MMA tile of 256
 // slots read past the last list) x pd.
