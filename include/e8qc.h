@@ -47,8 +47,9 @@ extern "C" {
 #define E8QC_MODE_BATCHED 1
 /* PRECISION (an addition of this library, no counterpart in the reference):
  * batch grouped by list as in BATCHED, but candidates are generated on the
- * INT8 tensor cores from an integer proxy of the codes and int8 queries; each
- * query's best max(64, 4k) (at most 128) proxy candidates are then rescored
+ * INT8 tensor cores from an int8 plane of every vector's levels (built on the
+ * first precision search, padded_dim bytes per vector) and int8 queries; each
+ * query's best max(32, 3k) (at most 128) proxy candidates are then rescored
  * with the exact estimator. Distances returned are exact; recall against the
  * exact scan is measured, not guaranteed. */
 #define E8QC_MODE_PRECISION 2
@@ -228,7 +229,7 @@ int e8qc_me8q_search(e8qc_me8q* idx, const float* queries, size_t nq, size_t k, 
  * scored with the estimator); E8QC_MODE_PRECISION generates candidates on the
  * INT8 tensor cores from an int8 plane of each vector's levels scaled by its
  * per-run coef (one scale per vector; built on first use, padded_dim bytes
- * per vector) and rescores each query's best max(64, 4k) (at most 128) with
+ * per vector) and rescores each query's best max(32, 3k) (at most 128) with
  * the reference's estimator: returned distances are exact, recall against the
  * exact scan is measured. */
 int e8qc_me8q_search_mode(e8qc_me8q* idx, const float* queries, size_t nq, size_t k, size_t nprobe, int mode,
