@@ -291,7 +291,8 @@ def cpu_baseline(a, x_host, cm_host, lab_host, q_host, gt, steps=None, warmup=No
     cores = os.cpu_count() or 1
     t0 = time.perf_counter()
     ref = E.E8qIndex(a.dim, a.nbits, a.seed)
-    ref.build(x_host, cm_host, lab_host.astype(np.uint32), num_threads=cores)
+    with QuietStdout():
+        ref.build(x_host, cm_host, lab_host.astype(np.uint32), num_threads=cores)
     build_s = time.perf_counter() - t0
     out = {"cores": cores, "build_s": round(build_s, 2)}
     sample = min(2048, q_host.shape[0])
@@ -311,6 +312,61 @@ def cpu_baseline(a, x_host, cm_host, lab_host, q_host, gt, steps=None, warmup=No
     ref.set_disable_prune(False)
     out["ref"] = ref
     return out
+
+
+class QuietStdout:
+    """Route file descriptor 1 to /dev/null (the reference's builds print
+    progress lines; the bench's stdout carries one JSON line)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
+def me8q_cpu_baseline(xp_host, cen_host, lab_host, var_host, q_host, avg_bits, nprobe, full_n, nlist,
+                      sample_n=500_000, nq=256):
+    """The reference's own Me8qIndex on this host, all cores, on a bounded
+    sample: the first sample_n vectors of the ME8Q workload (same lists,
+    centroids and variance), its production search at nprobe over nq queries.
+    The search rate in scored vectors per second is scaled to the full-size
+    query (nprobe lists of full_n / nlist vectors)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    E = O.ref_module()
+    if E is None:
+        return None
+    cores = os.cpu_count() or 1
+    xs = np.ascontiguousarray(xp_host[:sample_n])
+    ls = np.ascontiguousarray(lab_host[:sample_n]).astype(np.uint32)
+    t0 = time.perf_counter()
+    ref = E.Me8qIndex(xs.shape[1], float(avg_bits), 0)
+    with QuietStdout():
+        ref.build(xs, cen_host, ls, num_threads=cores, variance=var_host)
+    build_s = time.perf_counter() - t0
+    qs = np.ascontiguousarray(q_host[:nq])
+    ref.search(qs[:16], 10, nprobe, cores)
+    t0 = time.perf_counter()
+    ref.search(qs, 10, nprobe, cores)
+    sec = time.perf_counter() - t0
+    per_list = sample_n / nlist
+    vec_rate = nq * nprobe * per_list / sec
+    return {"value": round(vec_rate / (nprobe * full_n / nlist), 1), "unit": "QPS", "cores": cores,
+            "kind": "reference",
+            "sample": (f"reference Me8qIndex(avg_bits={avg_bits}) built on the first {sample_n} vectors of this "
+                       f"workload ({cores} threads, {build_s:.1f} s), production search of {nq} queries at "
+                       f"nprobe {nprobe}: {vec_rate / 1e6:.1f}M scored vectors/s, scaled to a full-size query of "
+                       f"{nprobe} x {full_n // nlist} vectors"),
+            "sample_qps": round(nq / sec, 1), "build_s": round(build_s, 2)}
 
 
 def gen_me8q(a, device):
@@ -480,6 +536,7 @@ def me8q_leg(a, e8qlib, dev, local, stream):
         else:
             del idx
         torch.cuda.empty_cache()
+    xp_host = None if a.no_cpu_baseline else xp[:500_000].cpu().numpy()
     del xp
     torch.cuda.empty_cache()
     serving = None
@@ -506,9 +563,15 @@ def me8q_leg(a, e8qlib, dev, local, stream):
                           "mean_batch_queries": round(st["mean_batch_queries"], 1)})
         serving = {"mode": "precision", "k": [10, 100], "nprobe": grid, "mixed_batch_capacity_qps": round(cap, 1),
                    "loads": loads}
+    cpu = None
+    solo = int(os.environ.get("RANK", "0")) == 0 and int(os.environ.get("WORLD_SIZE", "1")) == 1
+    if xp_host is not None and solo and serve_np is not None:
+        served = [r for r in rates if r.get("served")][0]
+        cpu = me8q_cpu_baseline(xp_host, cen.cpu().numpy(), lab.cpu().numpy(), var.cpu().numpy(),
+                                qp[:a.gt].cpu().numpy(), served["avg_bits"], serve_np, n, nl)
     out = {"workload": (f"ME8Q IVF search, {n // 1000}k x {d}-d unit vectors (spectrum i^-0.8, Haar rotation, "
                         f"full-rank PCA), {nl} lists (3 Lloyd steps), k=10, query batch {nb}"),
-           "gen_s": round(gen_s, 2), "rates": rates, "serving": serving}
+           "gen_s": round(gen_s, 2), "rates": rates, "serving": serving, "cpu_baseline": cpu}
     del serve_idx, qp, q, cen, lab, var
     torch.cuda.empty_cache()
     return out
