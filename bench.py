@@ -819,7 +819,7 @@ def run_reference(a, rank, world, dist):
         return
     ref = cb.pop("ref")
     cores = cb["cores"]
-    nb = 1024
+    nb = a.batch  # the same query batch as the measured arm
     nbat = max(1, a.pool // nb)
     for i in range(a.warmup):
         ref.search(qh[(i % nbat) * nb:(i % nbat + 1) * nb], a.k, a.nprobe, cores)
