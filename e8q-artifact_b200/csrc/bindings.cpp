@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <limits>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <unordered_map>
@@ -289,6 +290,25 @@ class E8qIndex {
     e8qc_index* handle(const char* what) const {
         require(what);
         return idx_;
+    }
+
+    // E8qIndex.load (e8q_bindings.cpp:258-268): a reference-written index file.
+    static std::unique_ptr<E8qIndex> load(const std::string& path, int device) {
+        e8qc_index* h = nullptr;
+        {
+            py::gil_scoped_release nogil;
+            check(e8qc_e8q_load(device, path.c_str(), &h));
+        }
+        e8qc_info in{};
+        const int rc = e8qc_e8q_info(h, &in);
+        if (rc != E8QC_OK) {
+            e8qc_e8q_destroy(h);
+            check(rc);
+        }
+        auto out = std::make_unique<E8qIndex>(static_cast<size_t>(in.dim), static_cast<size_t>(in.nbits), 0, device);
+        out->idx_ = h;
+        out->built_ = true;
+        return out;
     }
 };
 
@@ -794,6 +814,7 @@ PYBIND11_MODULE(_e8qlib, m) {
         .def("search_ragged", &E8qIndex::search_ragged, py::arg("queries"), py::arg("k"),
              py::arg("nprobe"), py::arg("k_max"), py::arg("mode") = "batched")
         .def("estimate", &E8qIndex::estimate, py::arg("query"), py::arg("id"))
+        .def_static("load", &E8qIndex::load, py::arg("path"), py::arg("device") = 0)
         .def("autotune", &E8qIndex::autotune, py::arg("mode"), py::arg("nq"), py::arg("k"), py::arg("nprobe"))
         .def("set_disable_prune", &E8qIndex::set_disable_prune, py::arg("on"))
         .def("set_prune_alpha", &E8qIndex::set_prune_alpha, py::arg("alpha"))

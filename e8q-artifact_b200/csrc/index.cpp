@@ -20,6 +20,7 @@
 #include "e8qc.h"
 #include "internal.h"
 #include "scan_plain.h"
+#include "io_e8ax.h"
 #include "precision.h"
 #include "serve_target.h"
 #include "workspace.h"
@@ -532,6 +533,123 @@ int e8qc_rotate(int device, size_t dim, uint64_t seed, const float* src, size_t 
     });
 }
 
+}  // extern "C"
+
+namespace {
+
+// The device view of an index whose buffers are in place (build, load); a new
+// layout invalidates the precision plane.
+void set_view(e8qc_index* x) {
+    DevIndex& v = x->view;
+    v.dim = static_cast<int>(x->dim);
+    v.pd = static_cast<int>(x->pd);
+    v.B = x->B;
+    v.bits = x->bits;
+    v.nlist = static_cast<int>(x->nlist);
+    v.nch = x->nch;
+    v.ntiles = static_cast<int>(x->ntiles);
+    v.signs = x->signs.as<uint8_t>();
+    v.mean_rot = x->mean_rot.as<float>();
+    v.cen = x->cen.as<float>();
+    v.cn2 = x->cn2.as<float>();
+    v.tile_begin = x->tile_begin_d.as<uint32_t>();
+    v.list_len = x->list_len_d.as<uint32_t>();
+    v.codes = static_cast<const uint4*>(x->codes.p);
+    v.g1 = x->g1.as<float>();
+    v.h3 = x->h3.as<float>();
+    v.ids = x->ids.as<uint32_t>();
+    v.tab = x->tab.as<float>();
+    v.list_order = x->list_order.as<uint32_t>();
+    v.list_of_tile = x->list_of_tile.as<uint32_t>();
+    x->proxy.release();
+    v.proxy = nullptr;
+}
+
+// The host list layout and the small device tables every index carries:
+// tiles, list lengths, tile -> list, work-queue orders and the level table.
+void install_lists(e8qc_index* x, const std::vector<uint64_t>& counts, cudaStream_t s) {
+    const size_t nlist = x->nlist;
+    x->list_begin.assign(nlist + 1, 0);
+    x->tile_begin.assign(nlist + 1, 0);
+    for (size_t c = 0; c < nlist; ++c) {
+        x->list_begin[c + 1] = x->list_begin[c] + counts[c];
+        x->tile_begin[c + 1] = x->tile_begin[c] + static_cast<uint32_t>((counts[c] + 31) / 32);
+    }
+    x->ntiles = x->tile_begin[nlist];
+    std::vector<uint32_t> t(nlist), list_len(nlist), list_of_tile(std::max<size_t>(1, x->ntiles), 0);
+    for (size_t c = 0; c < nlist; ++c) {
+        t[c] = x->tile_begin[c + 1] - x->tile_begin[c];
+        list_len[c] = static_cast<uint32_t>(counts[c]);
+        for (uint32_t tl = x->tile_begin[c]; tl < x->tile_begin[c + 1]; ++tl) list_of_tile[tl] = static_cast<uint32_t>(c);
+    }
+    std::sort(t.begin(), t.end(), std::greater<uint32_t>());
+    x->sorted_tiles_prefix.assign(nlist + 1, 0);
+    for (size_t c = 0; c < nlist; ++c) x->sorted_tiles_prefix[c + 1] = x->sorted_tiles_prefix[c] + t[c];
+    x->tile_begin_d.upload(x->tile_begin.data(), x->tile_begin.size() * 4, s);
+    x->list_len_d.upload(list_len.data(), list_len.size() * 4, s);
+    x->list_of_tile.upload(list_of_tile.data(), list_of_tile.size() * 4, s);
+    x->list_begin_d.upload(x->list_begin.data(), x->list_begin.size() * 8, s);
+    std::vector<uint32_t> order(2 * nlist);
+    for (size_t c = 0; c < nlist; ++c) order[c] = order[nlist + c] = static_cast<uint32_t>(c);
+    std::stable_sort(order.begin(), order.begin() + nlist, [&](uint32_t a, uint32_t b) { return counts[a] > counts[b]; });
+    x->list_order.upload(order.data(), order.size() * 4, s);
+    const int q = 1 << x->bits;
+    std::vector<float> tab(2 * static_cast<size_t>(q));
+    const double rd = std::sqrt(static_cast<double>(x->pd));
+    for (int br = 0; br < 2; ++br) {
+        const std::vector<double> lev = branch_levels(x->bits, br);
+        for (int d = 0; d < q; ++d) tab[br * q + d] = static_cast<float>(lev[d] / rd);
+    }
+    x->tab.upload(tab.data(), tab.size() * 4, s);
+}
+
+size_t sign_bytes(size_t dim) { return rotator_signs(dim, 0).size(); }
+
+}  // namespace
+
+extern "C" {
+
+int e8qc_e8q_load(int device, const char* path, e8qc_index** out) {
+    return guarded([&] {
+        if (out == nullptr) fail(E8QC_EINVAL, "null output");
+        *out = nullptr;
+        int ndev = 0;
+        E8QC_CUDA(cudaGetDeviceCount(&ndev));
+        if (device < 0 || device >= ndev) fail(E8QC_EINVAL, "no such CUDA device");
+        E8axParts p = read_e8ax(path, sign_bytes);
+        auto x = std::make_unique<e8qc_index>();
+        x->device = device;
+        x->dim = p.dim;
+        x->pd = p.pd;
+        x->bits = p.bits;
+        x->seed = 0;
+        x->B = static_cast<int>(p.pd / 8);
+        x->nch = p.nch;
+        x->ws.device = device;
+        x->n = p.n;
+        x->nlist = p.nlist;
+        x->prune_alpha = p.prune_alpha;
+        DeviceGuard g(device);
+        cudaStream_t s = nullptr;
+        std::vector<uint64_t> counts(p.nlist);
+        for (size_t c = 0; c < p.nlist; ++c) counts[c] = p.list_begin[c + 1] - p.list_begin[c];
+        install_lists(x.get(), counts, s);
+        x->ids_compact = std::move(p.ids_compact);
+        x->signs.upload(p.signs.data(), p.signs.size(), s);
+        x->mean_rot.upload(p.mean_rot.data(), p.mean_rot.size() * 4, s);
+        x->cen.upload(p.cen_rot.data(), p.cen_rot.size() * 4, s);
+        x->cn2.upload(p.cn2.data(), p.cn2.size() * 4, s);
+        x->codes.upload(p.codes.data(), p.codes.size() * sizeof(uint4), s);
+        x->g1.upload(p.g1.data(), p.g1.size() * 4, s);
+        x->h3.upload(p.h3.data(), p.h3.size() * 4, s);
+        x->ids.upload(p.slot_ids.data(), p.slot_ids.size() * 4, s);
+        set_view(x.get());
+        E8QC_CUDA(cudaStreamSynchronize(s));
+        x->built = true;
+        *out = x.release();
+    });
+}
+
 int e8qc_e8q_create(int device, size_t dim, int nbits, uint64_t seed, e8qc_index** out) {
     return guarded([&] {
         if (out == nullptr) fail(E8QC_EINVAL, "null output");
@@ -669,29 +787,8 @@ int e8qc_e8q_build(e8qc_index* x, const float* data, size_t n, const float* cent
         launch_centroids(x->signs.as<uint8_t>(), static_cast<int>(dim), static_cast<int>(pd), cen_raw,
                          static_cast<int>(nlist), x->mean_rot.as<float>(), x->cen.as<float>(),
                          x->cn2.as<float>(), s);
+        set_view(x);
         DevIndex& v = x->view;
-        v.dim = static_cast<int>(dim);
-        v.pd = static_cast<int>(pd);
-        v.B = x->B;
-        v.bits = x->bits;
-        v.nlist = static_cast<int>(nlist);
-        v.nch = x->nch;
-        v.ntiles = static_cast<int>(x->ntiles);
-        v.signs = x->signs.as<uint8_t>();
-        v.mean_rot = x->mean_rot.as<float>();
-        v.cen = x->cen.as<float>();
-        v.cn2 = x->cn2.as<float>();
-        v.tile_begin = x->tile_begin_d.as<uint32_t>();
-        v.list_len = x->list_len_d.as<uint32_t>();
-        v.codes = static_cast<const uint4*>(x->codes.p);
-        v.g1 = x->g1.as<float>();
-        v.h3 = x->h3.as<float>();
-        v.ids = x->ids.as<uint32_t>();
-        v.tab = x->tab.as<float>();
-        v.list_order = x->list_order.as<uint32_t>();
-        v.list_of_tile = x->list_of_tile.as<uint32_t>();
-        x->proxy.release();  // a rebuild invalidates the precision plane
-        v.proxy = nullptr;
         const DevEncTables& et = enc_tables_device(x->device, x->bits);
         BuildEncodeArgs a{};
         a.base = data_d;

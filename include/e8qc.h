@@ -175,6 +175,13 @@ int e8qc_e8q_search_plain_noalloc(e8qc_index* idx, const float* queries, size_t 
  * n: multiple of 16 in [16, 256]; k: multiple of 32 in [32, 256]. */
 int e8qc_tc_i8_gemm(int device, const int8_t* A, const int8_t* B, int n, int k, int reps, int grid,
                     int32_t* C, float* ms);
+/* E8qIndex::Load (src/index/e8q_io.cpp:86-211): open an index file the
+ * reference wrote with E8qIndex::Save (E8AX layout, optional build-options
+ * trailer) straight into a device index on `device`. Codes, g1/h3, ids,
+ * rotator, rotated mean and centroids come from the file (nothing is
+ * re-encoded); the file's pruning headers are not needed by the device scans.
+ * E8QC_EIO for an unreadable, foreign, truncated or inconsistent file. */
+int e8qc_e8q_load(int device, const char* path, e8qc_index** out);
 /* Copy the global ids, cluster-major (n entries), to a host buffer. */
 int e8qc_e8q_get_ids(const e8qc_index* idx, uint32_t* out);
 /* Export the per-vector lattice codes (cluster-major, the order of

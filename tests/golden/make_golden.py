@@ -48,6 +48,26 @@ ME8Q_CASES = [
 ]
 
 
+# reference-written E8AX index files, kept whole, for the loader's tests
+E8AX_FILES = ["d96_b4", "d100_b1", "d128_b9"]
+
+
+def write_e8ax_fixtures() -> None:
+    """Build the E8AX_FILES cases of INDEX_CASES with the reference and keep
+    its saved index files (tests/golden/index_<name>.e8ax): the same builds
+    whose parsed contents and search results are in index_<name>.npz."""
+    import oracle as O
+
+    E = O.ref_module()
+    for name, dim, bits, n, nlist, seed, sigma, nq, k, nprobe in INDEX_CASES:
+        if name not in E8AX_FILES:
+            continue
+        x, cm, lab = det_mixture(seed, n, dim, nlist, sigma)
+        idx = E.E8qIndex(dim, bits, seed)
+        idx.build(x, cm, lab, num_threads=4)
+        idx.save(os.path.join(HERE, f"index_{name}.e8ax"))
+
+
 def main() -> None:
     R = O.ref_lib()
     E = O.ref_module()
@@ -154,8 +174,12 @@ def main() -> None:
             sigma=np.float64(sigma), plan_spec=np.array(spec), plan=np.array(P["plan"], np.int64),
             ids=P["ids"], list_begin=P["list_begin"], digits=P["digits"], branch=P["branch"], coef=P["coef"],
             h2=P["h2"], search_ids=ids, search_dists=dists, est_ids=est_ids, est=est)
+    write_e8ax_fixtures()
     print("golden fixtures written to", HERE)
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "e8ax":
+        write_e8ax_fixtures()  # only the E8AX files
+    else:
+        main()
