@@ -514,6 +514,27 @@ class Me8qIndex {
         return idx_;
     }
 
+    // Me8qIndex.load (me8q_bindings.cpp:227-235): a reference-written index file.
+    static std::unique_ptr<Me8qIndex> load(const std::string& path, int device) {
+        e8qc_me8q* h = nullptr;
+        {
+            py::gil_scoped_release nogil;
+            check(e8qc_me8q_load(device, path.c_str(), &h));
+        }
+        e8qc_me8q_meta in{};
+        const int rc = e8qc_me8q_info(h, &in);
+        if (rc != E8QC_OK) {
+            e8qc_me8q_destroy(h);
+            check(rc);
+        }
+        // as the reference's load: avg_bits reports the stored rate (bits_per_dim)
+        const float avg = in.bits_per_dim > 0.0 ? static_cast<float>(in.bits_per_dim) : in.avg_bits;
+        auto out = std::make_unique<Me8qIndex>(static_cast<size_t>(in.dim), avg, 0, device);
+        out->idx_ = h;
+        out->built_ = true;
+        return out;
+    }
+
    private:
     void require(const char* what) const {
         if (!built_ || idx_ == nullptr)
@@ -779,6 +800,7 @@ PYBIND11_MODULE(_e8qlib, m) {
         .def("search", &e8qb200::Me8qIndex::search, py::arg("queries"), py::arg("k"), py::arg("nprobe"),
              py::arg("num_threads") = 1, py::arg("return_stats") = false, py::arg("mode") = "batched")
         .def("estimate", &e8qb200::Me8qIndex::estimate, py::arg("query"), py::arg("id"))
+        .def_static("load", &e8qb200::Me8qIndex::load, py::arg("path"), py::arg("device") = 0)
         .def("export_codes", &e8qb200::Me8qIndex::export_codes)
         .def("search_ragged", &e8qb200::Me8qIndex::search_ragged, py::arg("queries"), py::arg("k"),
              py::arg("nprobe"), py::arg("k_max"), py::arg("mode") = "batched")

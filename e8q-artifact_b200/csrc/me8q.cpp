@@ -14,6 +14,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdlib>
+#include <cstdio>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -314,6 +315,75 @@ void fill_view(e8qc_me8q* x) {
     v.nslots = x->nslots;
 }
 
+// Lists of cnt[c] vectors in 32-vector tiles: offsets, tiles, work-queue
+// orders (longest first, then list id), the tile -> list map; uploads them.
+// A new layout drops the precision plane.
+void setup_lists(e8qc_me8q* x, const std::vector<uint32_t>& cnt, cudaStream_t s) {
+    const size_t nlist = x->nlist;
+    x->list_begin.assign(nlist + 1, 0);
+    x->tile_begin.assign(nlist + 1, 0);
+    for (size_t c = 0; c < nlist; ++c) {
+        x->list_begin[c + 1] = x->list_begin[c] + cnt[c];
+        x->tile_begin[c + 1] = x->tile_begin[c] + (cnt[c] + 31) / 32;
+    }
+    x->ntiles = x->tile_begin[nlist];
+    x->nslots = x->ntiles * 32;
+    x->proxy.release();
+    x->sigma.release();
+    {
+        std::vector<uint64_t> t(nlist);
+        for (size_t c = 0; c < nlist; ++c) t[c] = x->tile_begin[c + 1] - x->tile_begin[c];
+        std::sort(t.rbegin(), t.rend());
+        x->tiles_prefix.assign(nlist + 1, 0);
+        for (size_t c = 0; c < nlist; ++c) x->tiles_prefix[c + 1] = x->tiles_prefix[c] + t[c];
+    }
+    std::vector<uint32_t> list_len(nlist), list_of_tile(std::max<size_t>(1, x->ntiles), 0), order(2 * nlist);
+    for (size_t c = 0; c < nlist; ++c) {
+        list_len[c] = cnt[c];
+        for (uint32_t t = x->tile_begin[c]; t < x->tile_begin[c + 1]; ++t) list_of_tile[t] = static_cast<uint32_t>(c);
+        order[c] = order[nlist + c] = static_cast<uint32_t>(c);
+    }
+    std::stable_sort(order.begin(), order.begin() + nlist, [&](uint32_t a, uint32_t b) { return cnt[a] > cnt[b]; });
+    x->tile_begin_d.upload(x->tile_begin.data(), x->tile_begin.size() * 4, s);
+    x->list_len_d.upload(list_len.data(), nlist * 4, s);
+    x->list_order_d.upload(order.data(), order.size() * 4, s);
+    x->list_of_tile_d.upload(list_of_tile.data(), list_of_tile.size() * 4, s);
+    x->list_begin_d.upload(x->list_begin.data(), x->list_begin.size() * 8, s);
+}
+
+// Zeroed code / factor storage for the layout, and the centroids: padded
+// (nlist x pd) -> per-run rotated on the device -> ||.||^2 in fp64 on the host
+// (include/e8qlib/index/ivf_common.hpp:43-54). Leaves the view filled.
+void setup_storage(e8qc_me8q* x, std::vector<float> cen_padded, cudaStream_t s) {
+    const size_t nlist = x->nlist, pd = x->pd;
+    x->cen_host = std::move(cen_padded);
+    x->cen_pad.upload(x->cen_host.data(), x->cen_host.size() * 4, s);
+    x->cen_rot.alloc(nlist * pd * 4);
+    x->codes.alloc(std::max<size_t>(1, x->ntiles) * x->nch * 32 * 16);
+    E8QC_CUDA(cudaMemsetAsync(x->codes.p, 0, x->codes.bytes, s));
+    const size_t nc = std::max(1, x->ncoded);
+    x->coef.alloc(nc * std::max<size_t>(1, x->nslots) * 4);
+    x->h2.alloc(nc * std::max<size_t>(1, x->nslots) * 4);
+    x->hsum.alloc(std::max<size_t>(1, x->nslots) * 4);
+    E8QC_CUDA(cudaMemsetAsync(x->coef.p, 0, x->coef.bytes, s));
+    E8QC_CUDA(cudaMemsetAsync(x->h2.p, 0, x->h2.bytes, s));
+    x->cn2.alloc(nlist * 4);
+    fill_view(x);
+    launch_me8q_prep(x->cen_pad.as<float>(), pd, static_cast<int>(pd), static_cast<int>(pd), nullptr, nullptr, x->view,
+                     0, nlist, x->cen_rot.as<float>(), nullptr, nullptr, s);
+    std::vector<float> cr(nlist * pd), n2(nlist);
+    E8QC_CUDA(cudaMemcpyAsync(cr.data(), x->cen_rot.p, cr.size() * 4, cudaMemcpyDeviceToHost, s));
+    E8QC_CUDA(cudaStreamSynchronize(s));
+    for (size_t c = 0; c < nlist; ++c) {
+        double acc = 0.0;
+        for (size_t d = 0; d < pd; ++d)
+            acc = std::fma(static_cast<double>(cr[c * pd + d]), static_cast<double>(cr[c * pd + d]), acc);
+        n2[c] = static_cast<float>(acc);
+    }
+    E8QC_CUDA(cudaMemcpyAsync(x->cn2.p, n2.data(), nlist * 4, cudaMemcpyHostToDevice, s));
+    E8QC_CUDA(cudaStreamSynchronize(s));
+}
+
 void build(e8qc_me8q* x, const float* data, size_t n, const float* centroids, size_t nlist, const uint32_t* cluster_ids,
            const e8qc_me8q_build_opts* o, cudaStream_t s) {
     const size_t dim = x->dim, pd = x->pd;
@@ -359,23 +429,7 @@ void build(e8qc_me8q* x, const float* data, size_t n, const float* centroids, si
     x->nlist = nlist;
     std::vector<uint32_t> cnt(nlist, 0);
     for (size_t i = 0; i < n; ++i) ++cnt[cid[i]];
-    x->list_begin.assign(nlist + 1, 0);
-    x->tile_begin.assign(nlist + 1, 0);
-    for (size_t c = 0; c < nlist; ++c) {
-        x->list_begin[c + 1] = x->list_begin[c] + cnt[c];
-        x->tile_begin[c + 1] = x->tile_begin[c] + (cnt[c] + 31) / 32;
-    }
-    x->ntiles = x->tile_begin[nlist];
-    x->nslots = x->ntiles * 32;
-    x->proxy.release();
-    x->sigma.release();
-    {
-        std::vector<uint64_t> t(nlist);
-        for (size_t c = 0; c < nlist; ++c) t[c] = x->tile_begin[c + 1] - x->tile_begin[c];
-        std::sort(t.rbegin(), t.rend());
-        x->tiles_prefix.assign(nlist + 1, 0);
-        for (size_t c = 0; c < nlist; ++c) x->tiles_prefix[c + 1] = x->tiles_prefix[c] + t[c];
-    }
+    setup_lists(x, cnt, s);
     std::vector<uint32_t> slot_of_row(n), slot_ids(std::max<size_t>(1, x->nslots), 0xFFFFFFFFu), fillc(nlist, 0);
     x->ids_compact.assign(n, 0);
     for (size_t i = 0; i < n; ++i) {
@@ -386,48 +440,13 @@ void build(e8qc_me8q* x, const float* data, size_t n, const float* centroids, si
         x->ids_compact[x->list_begin[c] + local] = static_cast<uint32_t>(i);
     }
     x->inv_pos.clear();
-    std::vector<uint32_t> list_len(nlist), list_of_tile(std::max<size_t>(1, x->ntiles), 0), order(2 * nlist);
-    for (size_t c = 0; c < nlist; ++c) {
-        list_len[c] = cnt[c];
-        for (uint32_t t = x->tile_begin[c]; t < x->tile_begin[c + 1]; ++t) list_of_tile[t] = static_cast<uint32_t>(c);
-        order[c] = order[nlist + c] = static_cast<uint32_t>(c);
-    }
-    std::stable_sort(order.begin(), order.begin() + nlist, [&](uint32_t a, uint32_t b) { return cnt[a] > cnt[b]; });
-    x->tile_begin_d.upload(x->tile_begin.data(), x->tile_begin.size() * 4, s);
-    x->list_len_d.upload(list_len.data(), nlist * 4, s);
-    x->list_order_d.upload(order.data(), order.size() * 4, s);
-    x->list_of_tile_d.upload(list_of_tile.data(), list_of_tile.size() * 4, s);
     x->ids.upload(slot_ids.data(), slot_ids.size() * 4, s);
-    x->list_begin_d.upload(x->list_begin.data(), x->list_begin.size() * 8, s);
-    // ---- centroids: padded, per-run rotated, ||.||^2 (ivf_common.hpp:43-54) ----
-    x->cen_host.assign(nlist * pd, 0.0f);
-    for (size_t c = 0; c < nlist; ++c) std::memcpy(&x->cen_host[c * pd], &cen[c * dim], dim * 4);
-    x->cen_pad.upload(x->cen_host.data(), x->cen_host.size() * 4, s);
-    x->cen_rot.alloc(nlist * pd * 4);
-    x->codes.alloc(std::max<size_t>(1, x->ntiles) * x->nch * 32 * 16);
-    E8QC_CUDA(cudaMemsetAsync(x->codes.p, 0, x->codes.bytes, s));
-    const size_t nc = std::max(1, x->ncoded);
-    x->coef.alloc(nc * std::max<size_t>(1, x->nslots) * 4);
-    x->h2.alloc(nc * std::max<size_t>(1, x->nslots) * 4);
-    x->hsum.alloc(std::max<size_t>(1, x->nslots) * 4);
-    E8QC_CUDA(cudaMemsetAsync(x->coef.p, 0, x->coef.bytes, s));
-    E8QC_CUDA(cudaMemsetAsync(x->h2.p, 0, x->h2.bytes, s));
-    x->cn2.alloc(nlist * 4);
-    fill_view(x);
-    launch_me8q_prep(x->cen_pad.as<float>(), pd, static_cast<int>(pd), static_cast<int>(pd), nullptr, nullptr, x->view,
-                     0, nlist, x->cen_rot.as<float>(), nullptr, nullptr, s);
     {
-        std::vector<float> cr(nlist * pd), n2(nlist);
-        E8QC_CUDA(cudaMemcpyAsync(cr.data(), x->cen_rot.p, cr.size() * 4, cudaMemcpyDeviceToHost, s));
-        E8QC_CUDA(cudaStreamSynchronize(s));
-        for (size_t c = 0; c < nlist; ++c) {
-            double acc = 0.0;
-            for (size_t d = 0; d < pd; ++d) acc = std::fma(static_cast<double>(cr[c * pd + d]), static_cast<double>(cr[c * pd + d]), acc);
-            n2[c] = static_cast<float>(acc);
-        }
-        E8QC_CUDA(cudaMemcpyAsync(x->cn2.p, n2.data(), nlist * 4, cudaMemcpyHostToDevice, s));
-        E8QC_CUDA(cudaStreamSynchronize(s));
+        std::vector<float> padded(nlist * pd, 0.0f);
+        for (size_t c = 0; c < nlist; ++c) std::memcpy(&padded[c * pd], &cen[c * dim], dim * 4);
+        setup_storage(x, std::move(padded), s);
     }
+    const size_t nc = std::max(1, x->ncoded);
     // ---- encode in chunks of rows ----
     DevBuf cid_d, slot_d, rr, norm2, drop, dg, br;
     cid_d.upload(cid.data(), n * 4, s);
@@ -454,6 +473,172 @@ void build(e8qc_me8q* x, const float* data, size_t n, const float* centroids, si
                               drop.as<double>(), cid_d.as<uint32_t>(), x->cen_rot.as<float>(), static_cast<int>(pd), r0, m,
                               slot_d.as<uint32_t>(), drop_energy, static_cast<uint4*>(x->codes.p), x->coef.as<float>(),
                               x->h2.as<float>(), s);
+    }
+    launch_me8q_hsum(x->view, x->hsum.as<float>(), s);
+    E8QC_CUDA(cudaStreamSynchronize(s));
+    x->built = true;
+}
+
+// Reader of the reference's ME8Q index file (ME8QIDXX; Me8qIndex::Save /
+// Load, src/index/me8q_io.cpp:29-175): header (n, dim, padded dim, lists,
+// bytes per vector), avg_bits and the option flags, the plan, the padded
+// centroids, cluster-major ids, list and byte offsets, the rows, the rotator
+// seed and each coded run's rotator signs. A row is the (coef, h2) pair of
+// every coded run, then the runs' blocks of b bytes each: digits 0..6 at b
+// bits, digit 7 without its parity bit at b - 1 bits, the branch in the top
+// bit (src/quantization/me8q_codec.cpp:109-129). The rows are unpacked and
+// repacked into this library's streams; nothing is re-encoded.
+void load_me8q_file(e8qc_me8q* x, const char* path, cudaStream_t s) {
+    if (path == nullptr) fail(E8QC_EINVAL, "null path");
+    std::vector<uint8_t> buf;
+    {
+        std::unique_ptr<std::FILE, int (*)(std::FILE*)> f(std::fopen(path, "rb"), &std::fclose);
+        if (!f) fail(E8QC_EIO, std::string("Me8qIndex::Load: cannot read ") + path);
+        if (std::fseek(f.get(), 0, SEEK_END) != 0) fail(E8QC_EIO, "cannot size the index file");
+        const long sz = std::ftell(f.get());
+        if (sz < 0) fail(E8QC_EIO, "cannot size the index file");
+        std::rewind(f.get());
+        buf.resize(static_cast<size_t>(sz));
+        if (sz > 0 && std::fread(buf.data(), 1, buf.size(), f.get()) != buf.size())
+            fail(E8QC_EIO, "short read while loading index");
+    }
+    size_t off = 0;
+    auto take = [&](size_t bytes, const char* what) {
+        if (bytes > buf.size() - off) fail(E8QC_EIO, std::string("Me8qIndex::Load: short read (") + what + ")");
+        const uint8_t* p = buf.data() + off;
+        off += bytes;
+        return p;
+    };
+    auto u64 = [&](const char* what) {
+        uint64_t v;
+        std::memcpy(&v, take(8, what), 8);
+        return v;
+    };
+    if (std::memcmp(take(8, "magic"), "ME8QIDXX", 8) != 0) fail(E8QC_EIO, std::string("Me8qIndex::Load: bad magic ") + path);
+    const uint64_t n = u64("header"), dim = u64("header"), pd = u64("header"), nlist = u64("header");
+    u64("header");  // bytes per vector: recomputed from the plan
+    float avg = 0.0f;
+    std::memcpy(&avg, take(4, "avg_bits"), 4);
+    int32_t flags[4];
+    std::memcpy(flags, take(16, "flags"), 16);
+    if (dim == 0 || dim > 16384 || pd != (dim + 63) / 64 * 64 || nlist == 0 || n > 0xFFFFFFFEull)
+        fail(E8QC_EIO, "Me8qIndex::Load: corrupt header");
+    if (dim != x->dim) fail(E8QC_EINVAL, "index file dimension does not match the index");
+    const uint64_t nplan = u64("plan");
+    if (nplan == 0 || nplan > 256) fail(E8QC_EIO, "Me8qIndex::Load: corrupt plan");
+    Plan plan;
+    size_t covered = 0;
+    for (uint64_t i = 0; i < nplan; ++i) {
+        const uint64_t len = u64("plan");
+        int32_t bits = 0;
+        std::memcpy(&bits, take(4, "plan"), 4);
+        if (len == 0 || len % kSegDim != 0 || bits < 0 || bits > kMaxBitsMe8q) fail(E8QC_EIO, "Me8qIndex::Load: corrupt plan");
+        plan.emplace_back(static_cast<size_t>(len), bits);
+        covered += static_cast<size_t>(len);
+    }
+    if (covered != pd) fail(E8QC_EIO, "Me8qIndex::Load: plan does not cover the padded dimension");
+    if (nlist > (buf.size() - off) / (pd * 4)) fail(E8QC_EIO, "Me8qIndex::Load: short read (centroids)");
+    std::vector<float> cen(nlist * pd);
+    std::memcpy(cen.data(), take(cen.size() * 4, "centroids"), cen.size() * 4);
+    if (n > (buf.size() - off) / 4) fail(E8QC_EIO, "Me8qIndex::Load: short read (ids)");
+    std::vector<uint32_t> ids(n);
+    if (n) std::memcpy(ids.data(), take(n * 4, "ids"), n * 4);
+    std::vector<uint64_t> lb(nlist + 1), bb(nlist + 1);
+    std::memcpy(lb.data(), take(lb.size() * 8, "list_begin"), lb.size() * 8);
+    std::memcpy(bb.data(), take(bb.size() * 8, "byte_begin"), bb.size() * 8);
+    // per-row stride from the plan (coef, h2 per coded run + b bytes per block)
+    size_t nseg = 0, stride = 0;
+    for (const auto& seg : plan)
+        if (seg.second) {
+            ++nseg;
+            stride += seg.first / 8 * static_cast<size_t>(seg.second);
+        }
+    stride += nseg * 8;
+    if (lb[0] != 0 || lb[nlist] != n || bb[0] != 0) fail(E8QC_EIO, "Me8qIndex::Load: offsets inconsistent");
+    for (uint64_t c = 0; c < nlist; ++c)
+        if (lb[c + 1] < lb[c] || bb[c + 1] - bb[c] != (lb[c + 1] - lb[c]) * stride)
+            fail(E8QC_EIO, "Me8qIndex::Load: offsets inconsistent");
+    const uint8_t* rows = take(bb[nlist], "codes");
+    const uint64_t rot_seed = u64("rot_seed");
+    const uint64_t n_rot = u64("rotator count");
+    if (n_rot != nseg) fail(E8QC_EIO, "Me8qIndex::Load: rotator count mismatch");
+    std::vector<uint8_t> file_signs;
+    for (uint64_t r = 0; r < n_rot; ++r) {
+        const uint64_t bytes = u64("rot_bytes");
+        const uint8_t* p = take(bytes, "rotator");
+        file_signs.insert(file_signs.end(), p, p + bytes);
+    }
+    // index state: plan, runs and rotators (the file's signs), lists, storage
+    x->avg_bits = avg;
+    x->seed = rot_seed;
+    x->plan = plan;
+    layout_plan(x, rot_seed, s);
+    {
+        size_t want = 0;
+        for (const auto& run : x->runs)
+            if (run.bits) want += rotator_signs(static_cast<size_t>(run.len), 0).size();
+        if (want != file_signs.size()) fail(E8QC_EIO, "Me8qIndex::Load: rotator payload size mismatch");
+        if (!file_signs.empty()) x->signs.upload(file_signs.data(), file_signs.size(), s);
+    }
+    x->n = n;
+    x->nlist = nlist;
+    std::vector<uint32_t> cnt(nlist);
+    for (uint64_t c = 0; c < nlist; ++c) cnt[c] = static_cast<uint32_t>(lb[c + 1] - lb[c]);
+    setup_lists(x, cnt, s);
+    std::vector<uint32_t> slot_ids(std::max<size_t>(1, x->nslots), 0xFFFFFFFFu);
+    for (uint64_t c = 0; c < nlist; ++c)
+        for (uint64_t r = lb[c]; r < lb[c + 1]; ++r) slot_ids[x->tile_begin[c] * 32 + (r - lb[c])] = ids[r];
+    x->ids_compact = ids;
+    x->inv_pos.clear();
+    x->ids.upload(slot_ids.data(), slot_ids.size() * 4, s);
+    setup_storage(x, std::move(cen), s);
+    // rows -> streams and factor planes
+    const size_t nc = static_cast<size_t>(std::max(1, x->ncoded));
+    std::vector<uint4> codes(std::max<size_t>(1, x->ntiles) * x->nch * 32, uint4{0u, 0u, 0u, 0u});
+    std::vector<float> coef(nc * std::max<size_t>(1, x->nslots), 0.0f), h2(coef.size(), 0.0f);
+    std::vector<uint32_t> w(static_cast<size_t>(x->nch) * 4 + 1);
+    for (uint64_t c = 0; c < nlist; ++c)
+        for (uint64_t r = 0; r < lb[c + 1] - lb[c]; ++r) {
+            const uint8_t* row = rows + bb[c] + r * stride;
+            const size_t slot = static_cast<size_t>(x->tile_begin[c]) * 32 + r;
+            for (size_t q = 0; q < nseg; ++q) {
+                std::memcpy(&coef[q * x->nslots + slot], row + 8 * q, 4);
+                std::memcpy(&h2[q * x->nslots + slot], row + 8 * q + 4, 4);
+            }
+            std::fill(w.begin(), w.end(), 0u);
+            const uint8_t* cur = row + nseg * 8;
+            for (const auto& run : x->runs) {
+                if (run.bits == 0) continue;
+                const int b = run.bits;
+                for (int blk = 0; blk < run.len / 8; ++blk, cur += b) {
+                    auto bit_at = [&](int pos) { return static_cast<uint32_t>((cur[pos >> 3] >> (pos & 7)) & 1u); };
+                    auto get = [&](int pos, int width) {
+                        uint32_t v = 0;
+                        for (int t = 0; t < width; ++t) v |= bit_at(pos + t) << t;
+                        return v;
+                    };
+                    const size_t base = static_cast<size_t>(run.word0) * 32 + static_cast<size_t>(blk) * 8 * b;
+                    for (int i = 0; i < 7; ++i) {
+                        const uint32_t d = get(b * i, b);
+                        const size_t pos = base + static_cast<size_t>(i) * b;
+                        w[pos >> 5] |= d << (pos & 31);
+                        if ((pos & 31) + b > 32) w[(pos >> 5) + 1] |= d >> (32 - (pos & 31));
+                    }
+                    // digit 7 field: its bits 1..b-1 and the branch in bit 0
+                    const uint32_t f7 = (get(b * 7, b - 1) << 1) | bit_at(8 * b - 1);
+                    const size_t pos = base + static_cast<size_t>(7) * b;
+                    w[pos >> 5] |= f7 << (pos & 31);
+                    if ((pos & 31) + b > 32) w[(pos >> 5) + 1] |= f7 >> (32 - (pos & 31));
+                }
+            }
+            const size_t tile = slot >> 5, l = slot & 31;
+            for (int ch = 0; ch < x->nch; ++ch)
+                codes[(tile * x->nch + ch) * 32 + l] = uint4{w[4 * ch], w[4 * ch + 1], w[4 * ch + 2], w[4 * ch + 3]};
+        }
+    E8QC_CUDA(cudaMemcpyAsync(x->codes.p, codes.data(), codes.size() * sizeof(uint4), cudaMemcpyHostToDevice, s));
+    if (x->ncoded > 0) {
+        E8QC_CUDA(cudaMemcpyAsync(x->coef.p, coef.data(), coef.size() * 4, cudaMemcpyHostToDevice, s));
+        E8QC_CUDA(cudaMemcpyAsync(x->h2.p, h2.data(), h2.size() * 4, cudaMemcpyHostToDevice, s));
     }
     launch_me8q_hsum(x->view, x->hsum.as<float>(), s);
     E8QC_CUDA(cudaStreamSynchronize(s));
@@ -701,6 +886,35 @@ int e8qc_me8q_build(e8qc_me8q* x, const float* data, size_t n, const float* cent
         DeviceGuard g(x->device);
         x->built = false;
         build(x, data, n, centroids, nlist, cluster_ids, opts, static_cast<cudaStream_t>(stream));
+    });
+}
+
+int e8qc_me8q_load(int device, const char* path, e8qc_me8q** out) {
+    return guarded([&] {
+        if (!out) fail(E8QC_EINVAL, "null output");
+        *out = nullptr;
+        if (!path) fail(E8QC_EINVAL, "null path");
+        // the dimension comes from the file header (offset 16, after magic and n)
+        uint64_t dim = 0;
+        {
+            std::unique_ptr<std::FILE, int (*)(std::FILE*)> f(std::fopen(path, "rb"), &std::fclose);
+            if (!f) fail(E8QC_EIO, std::string("Me8qIndex::Load: cannot read ") + path);
+            unsigned char head[24];
+            if (std::fread(head, 1, 24, f.get()) != 24) fail(E8QC_EIO, "Me8qIndex::Load: short read (header)");
+            if (std::memcmp(head, "ME8QIDXX", 8) != 0) fail(E8QC_EIO, std::string("Me8qIndex::Load: bad magic ") + path);
+            std::memcpy(&dim, head + 16, 8);
+        }
+        if (dim == 0 || dim > 16384) fail(E8QC_EIO, "Me8qIndex::Load: corrupt header");
+        e8qc_me8q* x = nullptr;
+        const int rc = e8qc_me8q_create(device, static_cast<size_t>(dim), 4.0f, 0, &x);
+        if (rc != E8QC_OK) fail(rc, std::string(e8qc_last_error()));
+        std::unique_ptr<e8qc_me8q, int (*)(e8qc_me8q*)> hold(x, &e8qc_me8q_destroy);
+        {
+            std::lock_guard<std::mutex> lock(x->mu);
+            DeviceGuard g(x->device);
+            load_me8q_file(x, path, nullptr);
+        }
+        *out = hold.release();
     });
 }
 

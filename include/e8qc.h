@@ -247,6 +247,12 @@ int e8qc_me8q_search_mode(e8qc_me8q* idx, const float* queries, size_t nq, size_
 int e8qc_me8q_search_ragged(e8qc_me8q* idx, const float* queries, size_t nq, const uint32_t* k,
                             const uint32_t* nprobe, size_t k_max, int mode, uint32_t* out_ids, float* out_dists,
                             void* stream);
+/* Me8qIndex::Load (src/index/me8q_io.cpp:67-175): open an index file the
+ * reference wrote with Me8qIndex::Save (ME8QIDXX) straight into a device index
+ * on `device`: plan, rotator signs, centroids, ids, rows (codes, coef, h2) come
+ * from the file, nothing is re-encoded. E8QC_EIO for an unreadable, foreign,
+ * truncated or inconsistent file. */
+int e8qc_me8q_load(int device, const char* path, e8qc_me8q** out);
 /* Me8qIndex::Estimate (me8q_measure.cpp:41-66); E8QC_ERANGE for an unknown id. */
 int e8qc_me8q_estimate(e8qc_me8q* idx, const float* query, uint32_t id, float* out);
 int e8qc_me8q_info(const e8qc_me8q* idx, e8qc_me8q_meta* out);

@@ -52,6 +52,26 @@ ME8Q_CASES = [
 E8AX_FILES = ["d96_b4", "d100_b1", "d128_b9"]
 
 
+# reference-written ME8QIDXX index files, kept whole, for the ME8Q loader's tests
+ME8Q_FILES = ["me8q_d200_spec", "me8q_d150_a3"]
+
+
+def write_me8q_fixtures() -> None:
+    """Build the ME8Q_FILES cases of ME8Q_CASES with the reference (one thread,
+    as the parsed fixtures) and keep its saved index files
+    (tests/golden/<name>.me8q)."""
+    import oracle as O
+
+    E = O.ref_module()
+    for name, dim, avg, seed, spec, n, nlist, sigma, nq, k, nprobe in ME8Q_CASES:
+        if name not in ME8Q_FILES:
+            continue
+        x, cm, lab = det_mixture(seed + 5000 + dim, n, dim, nlist, sigma)
+        idx = E.Me8qIndex(dim, avg, seed)
+        idx.build(x, cm, lab, num_threads=1, plan_spec=spec, prune_alpha=1e-9)
+        idx.save(os.path.join(HERE, f"{name}.me8q"))
+
+
 def write_e8ax_fixtures() -> None:
     """Build the E8AX_FILES cases of INDEX_CASES with the reference and keep
     its saved index files (tests/golden/index_<name>.e8ax): the same builds
@@ -175,11 +195,14 @@ def main() -> None:
             ids=P["ids"], list_begin=P["list_begin"], digits=P["digits"], branch=P["branch"], coef=P["coef"],
             h2=P["h2"], search_ids=ids, search_dists=dists, est_ids=est_ids, est=est)
     write_e8ax_fixtures()
+    write_me8q_fixtures()
     print("golden fixtures written to", HERE)
 
 
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "e8ax":
         write_e8ax_fixtures()  # only the E8AX files
+    elif len(sys.argv) > 1 and sys.argv[1] == "me8q":
+        write_me8q_fixtures()  # only the ME8QIDXX files
     else:
         main()

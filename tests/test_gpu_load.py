@@ -1,9 +1,11 @@
-"""E8qIndex.load on index files written by the reference itself
-(tests/golden/index_<name>.e8ax, made by tests/golden/make_golden.py from the
-same builds as index_<name>.npz): the loaded device index holds the reference's
-codes, g1, h3 and ids bit for bit, and its searches and estimates agree with
-the reference's own results. Rates 4, 1 and 9 cover the three split-decode
-forms (b = 1 keeps the whole code in the scan byte; b >= 9 fields pass 64 bits)."""
+"""E8qIndex.load and Me8qIndex.load on index files written by the reference
+itself (tests/golden/index_<name>.e8ax and <name>.me8q, made by
+tests/golden/make_golden.py from the same builds as the .npz fixtures): the
+loaded device index holds the reference's codes and factors and ids bit for
+bit, and its searches and estimates agree with the reference's own results.
+E8Q rates 4, 1 and 9 cover the three split-decode forms (b = 1 keeps the whole
+code in the scan byte; b >= 9 fields pass 64 bits); the ME8Q files cover a
+manual plan with a dropped run and a DP plan."""
 import os
 
 import numpy as np
@@ -81,3 +83,45 @@ def test_load_errors(e8q, tmp_path):
     cut.write_bytes(raw[: len(raw) // 2])
     with pytest.raises(RuntimeError, match="short read"):
         e8q.E8qIndex.load(str(cut))
+
+
+ME8Q_CASES = ["me8q_d200_spec", "me8q_d150_a3"]
+
+
+@pytest.mark.parametrize("name", ME8Q_CASES)
+def test_me8q_load_reference_file(e8q, name):
+    """Me8qIndex.load on a file the reference wrote: plan, ids, every segment
+    code and (coef, h2) bit for bit, estimates and the plain search as the
+    reference's own (the same build as me8q_<name>.npz)."""
+    G = load_golden(name + ".npz")
+    dim, seed, n, nlist, nq, k, nprobe = (int(v) for v in G["params"])
+    m = e8q.Me8qIndex.load(os.path.join(ROOT, "tests", "golden", f"{name}.me8q"))
+    assert m.is_built and m.dim == dim and m.n == n and m.num_clusters == nlist
+    assert [list(p) for p in m.plan] == [list(p) for p in G["plan"]]
+    assert m.avg_bits == pytest.approx(m.bits_per_dim)
+    ids, dg, br, cf, h2 = m.export_codes()
+    assert np.array_equal(ids, G["ids"])
+    assert np.array_equal(dg, G["digits"]) and np.array_equal(br, G["branch"])
+    assert np.array_equal(cf.view(np.uint32), G["coef"].view(np.uint32))
+    assert np.array_equal(h2.view(np.uint32), G["h2"].view(np.uint32))
+    q = det_mixture(seed + 6000 + dim, nq, dim, nlist, float(G["sigma"]))[0]
+    est = np.array([[m.estimate(q[i], int(g)) for g in G["est_ids"]] for i in range(nq)], np.float32)
+    assert rel_err(est, G["est"]).max() < 1e-6
+    got_ids, got_d = m.search(q, k, nprobe)
+    assert_topk_parity(got_ids, got_d, G["search_ids"], G["search_dists"])
+    p_ids, p_d = m.search(q, k, nprobe, mode="precision")
+    assert p_ids.shape == got_ids.shape and np.all(np.diff(p_d, axis=1) >= 0)
+
+
+def test_me8q_load_errors(e8q, tmp_path):
+    with pytest.raises(RuntimeError, match="cannot read"):
+        e8q.Me8qIndex.load(str(tmp_path / "missing.me8q"))
+    bad = tmp_path / "foreign.bin"
+    bad.write_bytes(b"\x00" * 64)
+    with pytest.raises(RuntimeError, match="bad magic"):
+        e8q.Me8qIndex.load(str(bad))
+    raw = open(os.path.join(ROOT, "tests", "golden", "me8q_d150_a3.me8q"), "rb").read()
+    cut = tmp_path / "truncated.me8q"
+    cut.write_bytes(raw[: len(raw) // 2])
+    with pytest.raises(RuntimeError, match="short read"):
+        e8q.Me8qIndex.load(str(cut))
