@@ -514,6 +514,13 @@ class Me8qIndex {
         return idx_;
     }
 
+    // Me8qIndex.save (me8q_bindings.cpp:220-225): a file the reference loads.
+    void save(const std::string& path) {
+        require("save");
+        py::gil_scoped_release nogil;
+        check(e8qc_me8q_save(idx_, path.c_str()));
+    }
+
     // Me8qIndex.load (me8q_bindings.cpp:227-235): a reference-written index file.
     static std::unique_ptr<Me8qIndex> load(const std::string& path, int device) {
         e8qc_me8q* h = nullptr;
@@ -801,6 +808,7 @@ PYBIND11_MODULE(_e8qlib, m) {
              py::arg("num_threads") = 1, py::arg("return_stats") = false, py::arg("mode") = "batched")
         .def("estimate", &e8qb200::Me8qIndex::estimate, py::arg("query"), py::arg("id"))
         .def_static("load", &e8qb200::Me8qIndex::load, py::arg("path"), py::arg("device") = 0)
+        .def("save", &e8qb200::Me8qIndex::save, py::arg("path"))
         .def("export_codes", &e8qb200::Me8qIndex::export_codes)
         .def("search_ragged", &e8qb200::Me8qIndex::search_ragged, py::arg("queries"), py::arg("k"),
              py::arg("nprobe"), py::arg("k_max"), py::arg("mode") = "batched")

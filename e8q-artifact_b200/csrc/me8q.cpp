@@ -182,6 +182,12 @@ struct e8qc_me8q {
     size_t dim = 0, pd = 0;
     float avg_bits = 4.0F;
     uint64_t seed = 0;
+    // what an ME8QIDXX file records besides the data (Me8qIndex::Save)
+    uint64_t rot_seed = 0;   // the effective rotator seed of the plan's runs
+    int max_bits = 13;
+    bool drop_energy = true;
+    float prune_alpha = 0.0F;
+    std::vector<uint8_t> signs_host;  // the coded runs' rotator signs, in plan order
     bool built = false;
     size_t n = 0, nlist = 0, ntiles = 0, nslots = 0;
     int nch = 0, ncoded = 0, route_dim = 0;
@@ -269,6 +275,8 @@ void layout_plan(e8qc_me8q* x, uint64_t rot_seed, cudaStream_t s) {
     x->bytes_per_vector = static_cast<size_t>(coded) * 8;
     for (const auto& seg : x->plan)
         if (seg.second) x->bytes_per_vector += seg.first / 8 * static_cast<size_t>(seg.second);
+    x->rot_seed = rot_seed;
+    x->signs_host = sg_all;
     if (lev_all.empty()) lev_all.push_back(0.0f);
     if (sg_all.empty()) sg_all.push_back(0);
     x->runs_d.upload(x->runs.data(), x->runs.size() * sizeof(Me8qRun), s);
@@ -459,6 +467,9 @@ void build(e8qc_me8q* x, const float* data, size_t n, const float* centroids, si
     br.alloc(chunk * (pd / 8));
     const int dev = x->device;
     const bool drop_energy = o ? o->drop_energy != 0 : true;
+    x->max_bits = max_bits;
+    x->drop_energy = drop_energy;
+    x->prune_alpha = o ? o->prune_alpha : 0.0F;
     for (size_t r0 = 0; r0 < n; r0 += chunk) {
         const size_t m = std::min(chunk, n - r0);
         launch_me8q_prep(xd, dim, static_cast<int>(dim), static_cast<int>(pd), x->cen_pad.as<float>(),
@@ -571,6 +582,9 @@ void load_me8q_file(e8qc_me8q* x, const char* path, cudaStream_t s) {
     // index state: plan, runs and rotators (the file's signs), lists, storage
     x->avg_bits = avg;
     x->seed = rot_seed;
+    x->max_bits = flags[1];
+    x->drop_energy = flags[2] != 0;
+    std::memcpy(&x->prune_alpha, &flags[3], 4);
     x->plan = plan;
     layout_plan(x, rot_seed, s);
     {
@@ -579,6 +593,7 @@ void load_me8q_file(e8qc_me8q* x, const char* path, cudaStream_t s) {
             if (run.bits) want += rotator_signs(static_cast<size_t>(run.len), 0).size();
         if (want != file_signs.size()) fail(E8QC_EIO, "Me8qIndex::Load: rotator payload size mismatch");
         if (!file_signs.empty()) x->signs.upload(file_signs.data(), file_signs.size(), s);
+        x->signs_host = file_signs;
     }
     x->n = n;
     x->nlist = nlist;
@@ -643,6 +658,103 @@ void load_me8q_file(e8qc_me8q* x, const char* path, cudaStream_t s) {
     launch_me8q_hsum(x->view, x->hsum.as<float>(), s);
     E8QC_CUDA(cudaStreamSynchronize(s));
     x->built = true;
+}
+
+// Writer of the reference's ME8QIDXX layout (Me8qIndex::Save,
+// src/index/me8q_io.cpp:29-65), from the device index: digits and branch of
+// every slot come back through the decode kernel, (coef, h2) from the factor
+// planes, and each row is packed as the reference packs it (PackSegment /
+// PackBlock, src/quantization/me8q_codec.cpp:109-151: per block of a coded
+// run, digits 0..6 at b bits, digit 7 without its parity bit at b - 1 bits,
+// the branch in the block's top bit). The reference loads such a file.
+void save_me8q_file(e8qc_me8q* x, const char* path, cudaStream_t s) {
+    if (path == nullptr) fail(E8QC_EINVAL, "null path");
+    const size_t n = x->n, pd = x->pd, nlist = x->nlist, B = pd / 8;
+    std::vector<uint16_t> dg(n * pd);
+    std::vector<uint8_t> br(n * B);
+    {
+        DevBuf dd, bb;
+        dd.alloc(std::max<size_t>(1, n * pd * 2));
+        bb.alloc(std::max<size_t>(1, n * B));
+        launch_me8q_decode(x->view, static_cast<int>(x->ntiles), x->list_of_tile_d.as<uint32_t>(),
+                           x->list_begin_d.as<uint64_t>(), static_cast<int>(pd), dd.as<uint16_t>(), bb.as<uint8_t>(), s);
+        E8QC_CUDA(cudaMemcpyAsync(dg.data(), dd.p, n * pd * 2, cudaMemcpyDeviceToHost, s));
+        E8QC_CUDA(cudaMemcpyAsync(br.data(), bb.p, n * B, cudaMemcpyDeviceToHost, s));
+        E8QC_CUDA(cudaStreamSynchronize(s));
+    }
+    const size_t nc = static_cast<size_t>(x->ncoded);
+    std::vector<float> cf(nc * x->nslots), hh(nc * x->nslots);
+    if (nc) {
+        E8QC_CUDA(cudaMemcpy(cf.data(), x->coef.p, cf.size() * 4, cudaMemcpyDeviceToHost));
+        E8QC_CUDA(cudaMemcpy(hh.data(), x->h2.p, hh.size() * 4, cudaMemcpyDeviceToHost));
+    }
+    const size_t stride = x->bytes_per_vector;
+    std::vector<uint8_t> rows(n * stride, 0);
+    for (size_t c = 0; c < nlist; ++c)
+        for (uint64_t pos = x->list_begin[c]; pos < x->list_begin[c + 1]; ++pos) {
+            const size_t slot = static_cast<size_t>(x->tile_begin[c]) * 32 + (pos - x->list_begin[c]);
+            uint8_t* row = rows.data() + pos * stride;
+            for (size_t q = 0; q < nc; ++q) {
+                std::memcpy(row + 8 * q, &cf[q * x->nslots + slot], 4);
+                std::memcpy(row + 8 * q + 4, &hh[q * x->nslots + slot], 4);
+            }
+            uint8_t* cur = row + 8 * nc;
+            for (const auto& run : x->runs) {
+                if (run.bits == 0) continue;
+                const int b = run.bits;
+                for (int blk = 0; blk < run.len / 8; ++blk, cur += b) {
+                    auto put = [&](int at, int width, uint32_t v) {
+                        for (int t = 0; t < width; ++t)
+                            if ((v >> t) & 1u) cur[(at + t) >> 3] |= static_cast<uint8_t>(1u << ((at + t) & 7));
+                    };
+                    const uint16_t* d = dg.data() + pos * pd + run.off + blk * 8;
+                    for (int i = 0; i < 7; ++i) put(b * i, b, d[i]);
+                    put(b * 7, b - 1, static_cast<uint32_t>(d[7]) >> 1);
+                    put(8 * b - 1, 1, br[pos * B + run.off / 8 + blk]);
+                }
+            }
+        }
+    std::unique_ptr<std::FILE, int (*)(std::FILE*)> f(std::fopen(path, "wb"), &std::fclose);
+    if (!f) fail(E8QC_EIO, std::string("Me8qIndex::Save: cannot write ") + path);
+    bool ok = true;
+    auto wr = [&](const void* p, size_t bytes) {
+        if (bytes && std::fwrite(p, 1, bytes, f.get()) != bytes) ok = false;
+    };
+    wr("ME8QIDXX", 8);
+    const uint64_t hdr[5] = {n, x->dim, pd, nlist, stride};
+    wr(hdr, sizeof(hdr));
+    wr(&x->avg_bits, 4);
+    int32_t flags[4] = {0, x->max_bits, x->drop_energy ? 1 : 0, 0};
+    std::memcpy(&flags[3], &x->prune_alpha, 4);
+    wr(flags, sizeof(flags));
+    const uint64_t nplan = x->plan.size();
+    wr(&nplan, 8);
+    for (const auto& seg : x->plan) {
+        const uint64_t len = seg.first;
+        const int32_t bits = seg.second;
+        wr(&len, 8);
+        wr(&bits, 4);
+    }
+    wr(x->cen_host.data(), x->cen_host.size() * 4);
+    wr(x->ids_compact.data(), n * 4);
+    wr(x->list_begin.data(), (nlist + 1) * 8);
+    std::vector<uint64_t> byte_begin(nlist + 1);
+    for (size_t c = 0; c <= nlist; ++c) byte_begin[c] = x->list_begin[c] * stride;
+    wr(byte_begin.data(), byte_begin.size() * 8);
+    wr(rows.data(), rows.size());
+    wr(&x->rot_seed, 8);
+    const uint64_t n_rot = nc;
+    wr(&n_rot, 8);
+    size_t so = 0;
+    for (const auto& run : x->runs) {
+        if (run.bits == 0) continue;
+        const uint64_t bytes = rotator_signs(static_cast<size_t>(run.len), 0).size();
+        if (so + bytes > x->signs_host.size()) fail(E8QC_ESTATE, "rotator signs missing");
+        wr(&bytes, 8);
+        wr(x->signs_host.data() + so, bytes);
+        so += bytes;
+    }
+    if (!ok) fail(E8QC_EIO, std::string("Me8qIndex::Save: write failed ") + path);
 }
 
 uint64_t tune_key(int mode, size_t nq, size_t np) {
@@ -915,6 +1027,15 @@ int e8qc_me8q_load(int device, const char* path, e8qc_me8q** out) {
             load_me8q_file(x, path, nullptr);
         }
         *out = hold.release();
+    });
+}
+
+int e8qc_me8q_save(e8qc_me8q* x, const char* path) {
+    return guarded([&] {
+        require_built(x, "save");
+        std::lock_guard<std::mutex> lock(x->mu);
+        DeviceGuard g(x->device);
+        save_me8q_file(x, path, nullptr);
     });
 }
 

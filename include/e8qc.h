@@ -253,6 +253,11 @@ int e8qc_me8q_search_ragged(e8qc_me8q* idx, const float* queries, size_t nq, con
  * from the file, nothing is re-encoded. E8QC_EIO for an unreadable, foreign,
  * truncated or inconsistent file. */
 int e8qc_me8q_load(int device, const char* path, e8qc_me8q** out);
+/* Me8qIndex::Save (src/index/me8q_io.cpp:29-65): write the index as an
+ * ME8QIDXX file the reference's Me8qIndex::Load reads (plan, padded
+ * centroids, ids, offsets, rows packed as the reference packs them, rotator
+ * seed and signs). E8QC_EIO when the file cannot be written. */
+int e8qc_me8q_save(e8qc_me8q* idx, const char* path);
 /* Me8qIndex::Estimate (me8q_measure.cpp:41-66); E8QC_ERANGE for an unknown id. */
 int e8qc_me8q_estimate(e8qc_me8q* idx, const float* query, uint32_t id, float* out);
 int e8qc_me8q_info(const e8qc_me8q* idx, e8qc_me8q_meta* out);

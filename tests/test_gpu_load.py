@@ -125,3 +125,32 @@ def test_me8q_load_errors(e8q, tmp_path):
     cut.write_bytes(raw[: len(raw) // 2])
     with pytest.raises(RuntimeError, match="short read"):
         e8q.Me8qIndex.load(str(cut))
+
+
+def test_me8q_save_round_trip_and_reference_load(e8q, oracle_lib, tmp_path):
+    """Me8qIndex.save writes what the reference reads: the file parses to the
+    reference's own fixture (the same build), loads back on the GPU bit for
+    bit, and the reference's Me8qIndex.load accepts it and searches like the
+    GPU index."""
+    name = "me8q_d200_spec"
+    G = load_golden(name + ".npz")
+    dim, seed, n, nlist, nq, k, nprobe = (int(v) for v in G["params"])
+    x, cm, lab = det_mixture(seed + 5000 + dim, n, dim, nlist, float(G["sigma"]))
+    q = det_mixture(seed + 6000 + dim, nq, dim, nlist, float(G["sigma"]))[0]
+    m = e8q.Me8qIndex(dim, float(G["avg_bits"]), seed)
+    m.build(x, cm, lab, plan_spec=str(G["plan_spec"]), prune_alpha=1e-9)
+    path = str(tmp_path / "gpu.me8q")
+    m.save(path)
+    P = oracle_lib.parse_me8q(path)
+    for key in ("ids", "digits", "branch", "coef", "h2"):
+        assert np.array_equal(np.asarray(P[key]).view(np.uint8), np.asarray(G[key]).view(np.uint8)), key
+    back = e8q.Me8qIndex.load(path)
+    for a, b in zip(m.export_codes(), back.export_codes()):
+        assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(b).view(np.uint8))
+    assert_topk_parity(*back.search(q, k, nprobe), G["search_ids"], G["search_dists"])
+    E = oracle_lib.ref_module()  # the reference compiled into oracle/_ref, present wherever it was built
+    if E is not None:
+        ref = E.Me8qIndex.load(path)
+        rid, rd = ref.search(q, k, nprobe, 1)
+        gid, gd = m.search(q, k, nprobe)
+        assert_topk_parity(gid, gd, rid, rd)
