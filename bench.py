@@ -671,6 +671,12 @@ def main():
                 "launch_us": round(t_launch * 1e6, 2), "peak_kind": pk_kind,
                 "item_bytes_per_launch": int(item_per_launch),
                 "item_gbs": round(item_per_launch / t_launch / 1e9, 1) if t_launch > 0 else 0.0}
+    step_breakdown = None
+    if a.path == "precision" and prof.get("final_launches"):
+        nl_ = max(1, prof["final_launches"])
+        step_breakdown = {"route_group_ms": round(prof["prep_ms"] / nl_, 4),
+                          "scan_ms": round(prof["scan_ms"] / max(1, prof["scan_launches"]), 4),
+                          "select_rescore_ms": round(prof["final_ms"] / nl_, 4)}
     if a.path == "precision" and prof.get("final_launches"):
         # the select + rescore kernel: every fp16 proxy distance read once, C
         # exact rescores per query; reported as the roofline when it takes
@@ -791,7 +797,7 @@ def main():
         "clocks": clk.summary(), "gpu_launches": int(launches), "roofline": roofline,
         "e2e": e2e, "cpu_baseline": cpu,
         "plain_gpu_qps": None if plain_qps is None else round(plain_qps, 1),
-        "serving": serving, "me8q": me8q,
+        "serving": serving, "me8q": me8q, "step_breakdown": step_breakdown,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)

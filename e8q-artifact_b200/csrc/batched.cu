@@ -58,51 +58,94 @@ __global__ void qn2_kernel(const float* __restrict__ rq, int pd, float* __restri
     }
 }
 
-// Route GEMM: 64 queries x 64 centroids per CTA, 4x4 fp64 accumulators per
-// thread, 32-dim chunks of both operands staged in shared memory.
-__global__ void __launch_bounds__(256) route_gemm_kernel(const float* __restrict__ rq, int nq,
-                                                         const float* __restrict__ cen,
-                                                         const float* __restrict__ cn2, int nlist, int pd,
-                                                         const float* __restrict__ qn2,
-                                                         uint64_t* __restrict__ keys) {
-    __shared__ float As[32][65];
-    __shared__ float Bs[32][65];
+// Route GEMM: 128 queries x 64 centroids per CTA of 128 threads, 8 x 8 fp64
+// accumulators per thread (queries ty*4+i and 64+ty*4+i, centroids tx*4+j and
+// 32+tx*4+j). 16-dim chunks of both operands are converted to fp64 once, when
+// they are staged (transposed) in shared memory; the next chunk is fetched into
+// registers while the current one is multiplied. Every (query, list) dot is one
+// fp64 FMA chain over the dimensions in order (products of two floats are exact
+// in fp64), so the result does not depend on the tiling.
+constexpr int kRouteBQ = 128, kRouteBC = 64, kRouteBK = 16;
+__global__ void __launch_bounds__(128, 2) route_gemm_kernel(const float* __restrict__ rq, int nq,
+                                                            const float* __restrict__ cen,
+                                                            const float* __restrict__ cn2, int nlist, int pd,
+                                                            const float* __restrict__ qn2,
+                                                            uint64_t* __restrict__ keys) {
+    __shared__ __align__(16) double As[kRouteBK][kRouteBQ + 2];
+    __shared__ __align__(16) double Bs[kRouteBK][kRouteBC + 2];
     const int tid = threadIdx.x;
-    const int q0 = blockIdx.y * 64, c0 = blockIdx.x * 64;
-    const int tq = tid >> 4, tc = tid & 15;
-    double acc[4][4] = {};
-    for (int k0 = 0; k0 < pd; k0 += 32) {
-        for (int e = tid; e < 64 * 32; e += 256) {
-            const int r = e >> 5, kk = e & 31;
-            const int qi = q0 + r, ci = c0 + r;
-            As[kk][r] = qi < nq ? rq[static_cast<size_t>(qi) * pd + k0 + kk] : 0.0f;
-            Bs[kk][r] = ci < nlist ? cen[static_cast<size_t>(ci) * pd + k0 + kk] : 0.0f;
+    const int q0 = blockIdx.y * kRouteBQ, c0 = blockIdx.x * kRouteBC;
+    const int ty = tid >> 3, tx = tid & 7;
+    // staging: A chunk = 128 rows x 4 float4 (4 per thread), B = 64 x 4 (2 per thread)
+    float4 ra[4], rb[2];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const int e = tid + h * 128, r = e >> 2, k4 = (e & 3) * 4;
+            ra[h] = q0 + r < nq ? *reinterpret_cast<const float4*>(rq + static_cast<size_t>(q0 + r) * pd + k0 + k4)
+                                : make_float4(0.f, 0.f, 0.f, 0.f);
         }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int e = tid + h * 128, r = e >> 2, k4 = (e & 3) * 4;
+            rb[h] = c0 + r < nlist ? *reinterpret_cast<const float4*>(cen + static_cast<size_t>(c0 + r) * pd + k0 + k4)
+                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    };
+    auto stage = [&]() {
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const int e = tid + h * 128, r = e >> 2, k4 = (e & 3) * 4;
+            As[k4 + 0][r] = ra[h].x;
+            As[k4 + 1][r] = ra[h].y;
+            As[k4 + 2][r] = ra[h].z;
+            As[k4 + 3][r] = ra[h].w;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int e = tid + h * 128, r = e >> 2, k4 = (e & 3) * 4;
+            Bs[k4 + 0][r] = rb[h].x;
+            Bs[k4 + 1][r] = rb[h].y;
+            Bs[k4 + 2][r] = rb[h].z;
+            Bs[k4 + 3][r] = rb[h].w;
+        }
+    };
+    double acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    fetch(0);
+    for (int k0 = 0; k0 < pd; k0 += kRouteBK) {
+        stage();
         __syncthreads();
-#pragma unroll 8
-        for (int kk = 0; kk < 32; ++kk) {
-            double a[4], b[4];
+        if (k0 + kRouteBK < pd) fetch(k0 + kRouteBK);
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                a[i] = static_cast<double>(As[kk][tq * 4 + i]);
-                b[i] = static_cast<double>(Bs[kk][tc * 4 + i]);
-            }
+        for (int kk = 0; kk < kRouteBK; ++kk) {
+            double a[8], b[8];
+            const double2* ar = reinterpret_cast<const double2*>(&As[kk][0]);
+            const double2* br = reinterpret_cast<const double2*>(&Bs[kk][0]);
+            const double2 a0 = ar[ty * 2], a1 = ar[ty * 2 + 1], a2 = ar[32 + ty * 2], a3 = ar[32 + ty * 2 + 1];
+            const double2 b0 = br[tx * 2], b1 = br[tx * 2 + 1], b2 = br[16 + tx * 2], b3 = br[16 + tx * 2 + 1];
+            a[0] = a0.x, a[1] = a0.y, a[2] = a1.x, a[3] = a1.y, a[4] = a2.x, a[5] = a2.y, a[6] = a3.x, a[7] = a3.y;
+            b[0] = b0.x, b[1] = b0.y, b[2] = b1.x, b[3] = b1.y, b[4] = b2.x, b[5] = b2.y, b[6] = b3.x, b[7] = b3.y;
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < 8; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+                for (int j = 0; j < 8; ++j) acc[i][j] = __fma_rn(a[i], b[j], acc[i][j]);
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int qi = q0 + tq * 4 + i;
+    for (int i = 0; i < 8; ++i) {
+        const int qi = q0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
         if (qi >= nq) continue;
+        const float qq = qn2[qi];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int ci = c0 + tc * 4 + j;
+        for (int j = 0; j < 8; ++j) {
+            const int ci = c0 + (j < 4 ? tx * 4 + j : 32 + tx * 4 + (j - 4));
             if (ci >= nlist) continue;
-            float d2 = __fmaf_rn(-2.0f, static_cast<float>(acc[i][j]), __fadd_rn(qn2[qi], cn2[ci]));
+            float d2 = __fmaf_rn(-2.0f, static_cast<float>(acc[i][j]), __fadd_rn(qq, cn2[ci]));
             if (d2 < 0.0f) d2 = 0.0f;
             keys[static_cast<size_t>(qi) * nlist + ci] =
                 (static_cast<uint64_t>(__float_as_uint(d2)) << 32) | static_cast<uint32_t>(ci);
@@ -776,8 +819,9 @@ int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t n
     int launches = 0;
     qn2_kernel<<<static_cast<unsigned>(nq), 256, 0, s>>>(rq, ix.pd, ws.b_qn2.as<float>());
     ++launches;
-    dim3 g((nlist + 63) / 64, static_cast<unsigned>((nq + 63) / 64));
-    route_gemm_kernel<<<g, 256, 0, s>>>(rq, static_cast<int>(nq), ix.cen, ix.cn2, nlist, ix.pd, ws.b_qn2.as<float>(),
+    if (ix.pd % kRouteBK != 0) fail(E8QC_EINVAL, "batched route needs the padded dimension to be a multiple of 16");
+    dim3 g((nlist + kRouteBC - 1) / kRouteBC, static_cast<unsigned>((nq + kRouteBQ - 1) / kRouteBQ));
+    route_gemm_kernel<<<g, 128, 0, s>>>(rq, static_cast<int>(nq), ix.cen, ix.cn2, nlist, ix.pd, ws.b_qn2.as<float>(),
                                         ws.b_keys.as<uint64_t>());
     ++launches;
     E8QC_CUDA(cudaMemsetAsync(ws.b_cnt.p, 0, static_cast<size_t>(nlist) * 4, s));

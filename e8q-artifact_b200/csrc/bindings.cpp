@@ -238,6 +238,7 @@ class E8qIndex {
         d["final_launches"] = p.final_launches;
         d["final_ms"] = p.final_ms;
         d["final_bytes"] = p.final_bytes;
+        d["prep_ms"] = p.prep_ms;
         return d;
     }
 

@@ -299,12 +299,14 @@ uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, con
         if (mode == E8QC_MODE_PRECISION) {
             E8QC_CUDA(cudaEventCreate(&ws.final_ev0));
             E8QC_CUDA(cudaEventCreate(&ws.final_ev1));
+            E8QC_CUDA(cudaEventCreate(&ws.prep_ev0));
+            E8QC_CUDA(cudaEventCreate(&ws.prep_ev1));
         }
     }
     struct Drop {
         Workspace& w;
         ~Drop() {
-            for (cudaEvent_t* e : {&w.scan_ev0, &w.scan_ev1, &w.final_ev0, &w.final_ev1}) {
+            for (cudaEvent_t* e : {&w.scan_ev0, &w.scan_ev1, &w.final_ev0, &w.final_ev1, &w.prep_ev0, &w.prep_ev1}) {
                 if (*e) cudaEventDestroy(*e);
                 *e = nullptr;
             }
@@ -351,6 +353,9 @@ uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, con
             E8QC_CUDA(cudaEventElapsedTime(&fms, ws.final_ev0, ws.final_ev1));
             x->prof.final_launches += 1;
             x->prof.final_ms += fms;
+            float pms = 0.0f;
+            E8QC_CUDA(cudaEventElapsedTime(&pms, ws.prep_ev0, ws.prep_ev1));
+            x->prof.prep_ms += pms;
             x->prof.final_bytes += cnt[0] * 2 + static_cast<uint64_t>(nq) *
                                                     static_cast<uint64_t>(precision_candidates(static_cast<int>(k))) *
                                                     (static_cast<uint64_t>(x->bits) * x->pd / 8 + 12);

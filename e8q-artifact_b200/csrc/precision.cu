@@ -999,7 +999,9 @@ int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t 
         const float* rqc = rq + off * ix.pd;
         const uint32_t* kc = k_arr ? k_arr + off : nullptr;
         const uint32_t* npc = np_arr ? np_arr + off : nullptr;
+        ws.mark_prep(false, s);
         launches += batched_prepare(ix, ws, rqc, n, npc, nprobe, 0, kPM, 8, s);
+        ws.mark_prep(true, s);
         const size_t pslots = n * nprobe + static_cast<size_t>(7) * ix.nlist;
         const size_t arows = (pslots + 7) / 8 * 8 + kPM;  // an item reads up to 128 rows from its start
         ws.p_q8.ensure(n * static_cast<size_t>(ix.pd));

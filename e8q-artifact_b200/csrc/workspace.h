@@ -78,6 +78,12 @@ struct Workspace {
     }
     // the same around the precision path's select + rescore kernel
     cudaEvent_t final_ev0 = nullptr, final_ev1 = nullptr;
+    // and around the routing + grouping stage (route GEMM, select, items, scatter)
+    cudaEvent_t prep_ev0 = nullptr, prep_ev1 = nullptr;
+    void mark_prep(bool end, cudaStream_t s) {
+        cudaEvent_t e = end ? prep_ev1 : prep_ev0;
+        if (e) E8QC_CUDA(cudaEventRecord(e, s));
+    }
     void mark_final(bool end, cudaStream_t s) {
         cudaEvent_t e = end ? final_ev1 : final_ev0;
         if (e) E8QC_CUDA(cudaEventRecord(e, s));

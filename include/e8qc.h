@@ -151,6 +151,8 @@ typedef struct e8qc_profile {
     double final_ms;         /* their summed CUDA-event time */
     uint64_t final_bytes;    /* their algorithmic bytes: 2 per proxy distance read + per query
                                 C * (bits*padded_dim/8 + 12) for the rescored candidates */
+    double prep_ms;          /* precision mode: routing + grouping (route GEMM, probe select,
+                                work items, pair scatter), summed CUDA-event time */
 } e8qc_profile;
 int e8qc_e8q_profile(e8qc_index* idx, int enable, e8qc_profile* out);
 /* Plain search that allocates nothing (no counterpart in the reference; an
