@@ -56,6 +56,122 @@ __global__ void rotate_queries_kernel(const float* __restrict__ q, int dim, int 
         out[row * pd + i] = subtract ? __fsub_rn(sx[i], subtract[i]) : sx[i];
 }
 
+// Register form of the same rotation for padded_dim <= 1024: one warp per
+// row, lane l holding elements j*32 + l (j < NJ = padded_dim / 32) in
+// registers. Butterfly stages with h < 32 exchange values between lanes
+// (shfl_xor h), stages with h >= 32 pair registers j and j + h/32 of a lane;
+// the stages, their order and every rounding are those of rotate_rows_smem
+// (sign flip over the whole row, FHT of size td at offset 0 or
+// padded_dim - td alternately, scale by fac, Kac half-swap when td <
+// padded_dim, final 0.25 when padded), so the two forms agree bit for bit.
+template <int NJ, int J0, int TJ>
+__device__ __forceinline__ void fht_scale_regs(float (&v)[NJ], int lane, float fac) {
+#pragma unroll
+    for (int h = 1; h < 32; h <<= 1) {
+        const bool lower = (lane & h) == 0;
+#pragma unroll
+        for (int j = J0; j < J0 + TJ; ++j) {
+            const float o = __shfl_xor_sync(kFull, v[j], h);
+            v[j] = lower ? __fadd_rn(v[j], o) : __fsub_rn(o, v[j]);
+        }
+    }
+#pragma unroll
+    for (int H = 1; H < TJ; H <<= 1) {
+#pragma unroll
+        for (int j = J0; j < J0 + TJ; ++j) {
+            if (((j - J0) & H) == 0) {
+                const float a0 = v[j], a1 = v[j + H];
+                v[j] = __fadd_rn(a0, a1);
+                v[j + H] = __fsub_rn(a0, a1);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = J0; j < J0 + TJ; ++j) v[j] = __fmul_rn(v[j], fac);
+}
+
+constexpr int kRotWarps = 4;  // rows per CTA of the register form
+
+template <int NJ, int TJ>
+__global__ void __launch_bounds__(kRotWarps * 32) rotate_rows_warp_kernel(
+    const float* __restrict__ q, int dim, int n, float fac, const uint8_t* __restrict__ signs,
+    const float* __restrict__ subtract, float* __restrict__ out) {
+    constexpr int PD = NJ * 32;
+    constexpr bool kPadded = TJ != NJ;
+    const int lane = threadIdx.x & 31;
+    const size_t row = static_cast<size_t>(blockIdx.x) * kRotWarps + (threadIdx.x >> 5);
+    if (row >= static_cast<size_t>(n)) return;
+    float v[NJ];
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+        const int i = j * 32 + lane;
+        v[j] = i < dim ? q[row * dim + i] : 0.0f;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        // sign bit of element j*32 + l = bit l of the round's little-endian word j
+        const uint32_t* sw = reinterpret_cast<const uint32_t*>(signs + r * (PD / 8));
+#pragma unroll
+        for (int j = 0; j < NJ; ++j)
+            if ((__ldg(sw + j) >> lane) & 1u) v[j] = -v[j];
+        if (!kPadded || (r & 1) == 0)
+            fht_scale_regs<NJ, 0, TJ>(v, lane, fac);
+        else
+            fht_scale_regs<NJ, NJ - TJ, TJ>(v, lane, fac);
+        if (kPadded) {
+#pragma unroll
+            for (int j = 0; j < NJ / 2; ++j) {
+                const float a0 = v[j], a1 = v[j + NJ / 2];
+                v[j] = __fadd_rn(a0, a1);
+                v[j + NJ / 2] = __fsub_rn(a0, a1);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+        const int i = j * 32 + lane;
+        const float x = kPadded ? __fmul_rn(v[j], 0.25f) : v[j];
+        out[row * PD + i] = subtract ? __fsub_rn(x, subtract[i]) : x;
+    }
+}
+
+constexpr int largest_pow2_le(int x) { return x >= 2 ? 2 * largest_pow2_le(x / 2) : 1; }
+
+template <int NJ>
+bool launch_rotate_warp_nj(int tj, const float* q, int dim, int n, float fac, const uint8_t* signs,
+                           const float* subtract, float* out, cudaStream_t s) {
+    constexpr int P = largest_pow2_le(NJ);
+    const unsigned grid = static_cast<unsigned>((n + kRotWarps - 1) / kRotWarps);
+    if (tj == P)
+        rotate_rows_warp_kernel<NJ, P><<<grid, kRotWarps * 32, 0, s>>>(q, dim, n, fac, signs, subtract, out);
+    else if (P >= 2 && tj == P / 2)
+        rotate_rows_warp_kernel<NJ, (P >= 2 ? P / 2 : 1)><<<grid, kRotWarps * 32, 0, s>>>(q, dim, n, fac, signs,
+                                                                                         subtract, out);
+    else
+        return false;
+    return true;
+}
+
+// Register-form rotation when it applies (padded_dim <= 1024, td >= 32,
+// 4-byte aligned sign rounds); false leaves the row to the shared-memory form.
+bool launch_rotate_warp(int dim, int pd, int td, const float* q, int n, float fac, const uint8_t* signs,
+                        const float* subtract, float* out, cudaStream_t s) {
+    if (n <= 0 || pd % 64 != 0 || pd > 1024 || td < 32 || (reinterpret_cast<uintptr_t>(signs) & 3u) != 0)
+        return false;
+    const int tj = td / 32;
+    switch (pd / 32) {
+#define E8QC_ROT_CASE(NJ) \
+    case NJ:              \
+        return launch_rotate_warp_nj<NJ>(tj, q, dim, n, fac, signs, subtract, out, s);
+        E8QC_ROT_CASE(2) E8QC_ROT_CASE(4) E8QC_ROT_CASE(6) E8QC_ROT_CASE(8) E8QC_ROT_CASE(10) E8QC_ROT_CASE(12)
+        E8QC_ROT_CASE(14) E8QC_ROT_CASE(16) E8QC_ROT_CASE(18) E8QC_ROT_CASE(20) E8QC_ROT_CASE(22)
+        E8QC_ROT_CASE(24) E8QC_ROT_CASE(26) E8QC_ROT_CASE(28) E8QC_ROT_CASE(30) E8QC_ROT_CASE(32)
+#undef E8QC_ROT_CASE
+        default:
+            return false;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Top-nprobe lists of one query by 64-bit key (float bits of d2 << 32 | cid),
 // src/index/ivf_route.cpp:9-27 + src/simd/kernels.hpp:13-21. Keys are unique,
@@ -286,8 +402,9 @@ int launch_rotate(const DevIndex& ix, const float* q, int nq, float* out, cudaSt
     int td = 1;
     while ((td << 1) <= ix.dim) td <<= 1;
     const float fac = 1.0f / sqrtf(static_cast<float>(td));
-    rotate_queries_kernel<<<nq, 256, ix.pd * sizeof(float), s>>>(q, ix.dim, ix.pd, td, fac,
-                                                                 ix.signs, ix.mean_rot, out);
+    if (!launch_rotate_warp(ix.dim, ix.pd, td, q, nq, fac, ix.signs, ix.mean_rot, out, s))
+        rotate_queries_kernel<<<nq, 256, ix.pd * sizeof(float), s>>>(q, ix.dim, ix.pd, td, fac,
+                                                                     ix.signs, ix.mean_rot, out);
     E8QC_CUDA(cudaGetLastError());
     return 1;
 }
@@ -297,8 +414,9 @@ int launch_rotate_raw(const uint8_t* signs, int dim, int pd, const float* src, i
     int td = 1;
     while ((td << 1) <= dim) td <<= 1;
     const float fac = 1.0f / sqrtf(static_cast<float>(td));
-    rotate_queries_kernel<<<n, 256, pd * sizeof(float), s>>>(src, dim, pd, td, fac, signs,
-                                                             subtract, dst);
+    if (!launch_rotate_warp(dim, pd, td, src, n, fac, signs, subtract, dst, s))
+        rotate_queries_kernel<<<n, 256, pd * sizeof(float), s>>>(src, dim, pd, td, fac, signs,
+                                                                 subtract, dst);
     E8QC_CUDA(cudaGetLastError());
     return 1;
 }

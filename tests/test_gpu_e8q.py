@@ -58,6 +58,20 @@ def test_gpu_rotation_bit_exact(e8q):
         assert np.array_equal(y.view(np.uint32), g[f"rot_{dim}_{seed}"].view(np.uint32)), dim
 
 
+def test_gpu_rotation_every_width(e8q, oracle_lib):
+    """Every padded width of the register-form rotation (64..1024, both FHT
+    sizes a width admits) and the shared-memory form around it (dim < 32,
+    padded_dim > 1024) agree with the oracle bit for bit."""
+    dims = [20, 31, 32, 33, 63, 64, 96, 128, 129, 192, 193, 256, 300, 384, 420, 449, 512, 520, 640, 700,
+            768, 800, 896, 930, 960, 961, 1000, 1023, 1024, 1100, 2000]
+    for dim in dims:
+        seed = dim % 7
+        x = det_normal(7000 + dim, (9, dim))
+        y = e8q.rotate(x, dim, seed)
+        o = oracle_lib.rotate(x, dim, oracle_lib.rotator_signs(dim, seed))
+        assert np.array_equal(y.view(np.uint32), o.view(np.uint32)), dim
+
+
 @pytest.mark.parametrize("name", INDEX_CASES)
 def test_gpu_build_matches_reference_index(e8q, name):
     """Codes, ids and the (g1, h3) fit of a GPU-built index equal the
