@@ -82,15 +82,17 @@ struct BlockRun {
 };
 
 // Decode + accumulate NBLK consecutive blocks whose NCH chunks start at
-// `sbuf` (chunk-row major, 32 lanes per row); query blocks start at `qblk`.
-template <int BITS, int NBLK, int NCH>
+// `sbuf` (chunk c of the vector at sbuf[c * STRIDE + lane]: STRIDE 32 for
+// chunk-row-major tiles, 1 with lane 0 for one vector's contiguous chunks);
+// query blocks start at `qblk`.
+template <int BITS, int NBLK, int NCH, int STRIDE = 32>
 __device__ __forceinline__ void accumulate_blocks(const uint4* __restrict__ sbuf, int lane,
                                                   const float4* __restrict__ sq4, int qblk, uint32_t tb_addr,
                                                   float& acc0, float& acc1) {
     uint32_t w[4 * NCH + 1];
 #pragma unroll
     for (int c = 0; c < NCH; ++c) {
-        const uint4 v = sbuf[c * 32 + lane];
+        const uint4 v = sbuf[c * STRIDE + lane];
         w[4 * c] = v.x;
         w[4 * c + 1] = v.y;
         w[4 * c + 2] = v.z;

@@ -99,7 +99,8 @@ struct e8qc_index {
 
     DevBuf signs, mean_rot, cen, cn2, tile_begin_d, list_len_d, codes, g1, h3, ids, tab,
         list_of_tile, list_begin_d, list_order;
-    DevBuf proxy;  // int8 proxy plane of the precision mode, built on its first search
+    DevBuf proxy;   // int8 proxy plane of the precision mode, built on its first search
+    DevBuf vcodes;  // the codes slot-major, for the precision mode's rescoring (built with the plane)
     // autotuned (schedule, stages) per (mode, log2 batch size, log2 nprobe)
     std::mutex tune_mu;
     std::map<uint64_t, std::pair<int, int>> tuned;
@@ -111,9 +112,28 @@ struct e8qc_index {
     size_t memory_bytes() const {
         return signs.bytes + mean_rot.bytes + cen.bytes + cn2.bytes + tile_begin_d.bytes +
                list_len_d.bytes + codes.bytes + g1.bytes + h3.bytes + ids.bytes + tab.bytes +
-               list_of_tile.bytes + list_begin_d.bytes + list_order.bytes + proxy.bytes;
+               list_of_tile.bytes + list_begin_d.bytes + list_order.bytes + proxy.bytes + vcodes.bytes;
     }
 };
+
+namespace {
+
+// The precision mode's device planes (int8 proxies, slot-major codes), built
+// on first use; returns the kernels launched.
+int ensure_precision_planes(e8qc_index* x, cudaStream_t s) {
+    if (x->view.proxy != nullptr) return 0;
+    int launches = 0;
+    x->vcodes.alloc(vcodes_bytes(x->view, x->ntiles));
+    launches += launch_vcodes(x->view, static_cast<int>(x->ntiles), x->vcodes.as<uint4>(), s);
+    x->proxy.alloc(proxy_plane_bytes(x->view, x->ntiles));
+    launches += launch_build_proxy(x->view, static_cast<int>(x->ntiles), x->proxy.as<uint4>(), s);
+    x->view.vcodes = x->vcodes.as<uint4>();
+    x->view.proxy = x->proxy.as<uint4>();
+    x->view.proxy_scale = precision_proxy_step(x->view.bits, x->view.pd);
+    return launches;
+}
+
+}  // namespace
 
 namespace {
 
@@ -314,12 +334,7 @@ uint64_t grouped_search(e8qc_index* x, int mode, const float* rq, size_t nq, con
     } drop{ws};
     int launches = 0;
     apply_tuning(x, ws, mode, nq, np);
-    if (mode == E8QC_MODE_PRECISION && x->view.proxy == nullptr) {
-        x->proxy.alloc(proxy_plane_bytes(x->view, x->ntiles));
-        launches += launch_build_proxy(x->view, static_cast<int>(x->ntiles), x->proxy.as<uint4>(), s);
-        x->view.proxy = x->proxy.as<uint4>();
-        x->view.proxy_scale = precision_proxy_step(x->view.bits, x->view.pd);
-    }
+    if (mode == E8QC_MODE_PRECISION) launches += ensure_precision_planes(x, s);
     if (mode == E8QC_MODE_PRECISION)
         launches += precision_search(x->view, ws, rq, nq, k_arr, np_arr, k, np, k, ids_d, d_d,
                                      max_tiles_for(x, np) * 32, s);
@@ -389,11 +404,8 @@ class E8qTarget final : public SearchTarget {
         std::lock_guard<std::mutex> lock(x_->mu);
         DeviceGuard g(x_->device);
         if (mode == E8QC_MODE_PRECISION && x_->view.proxy == nullptr) {
-            x_->proxy.alloc(proxy_plane_bytes(x_->view, x_->ntiles));
-            launch_build_proxy(x_->view, static_cast<int>(x_->ntiles), x_->proxy.as<uint4>(), nullptr);
+            ensure_precision_planes(x_, nullptr);
             E8QC_CUDA(cudaStreamSynchronize(nullptr));
-            x_->view.proxy = x_->proxy.as<uint4>();
-            x_->view.proxy_scale = precision_proxy_step(x_->view.bits, x_->view.pd);
         }
     }
     // Workspace buffers plus the caller's query / k / nprobe / result buffers.
@@ -567,7 +579,9 @@ void set_view(e8qc_index* x) {
     v.list_order = x->list_order.as<uint32_t>();
     v.list_of_tile = x->list_of_tile.as<uint32_t>();
     x->proxy.release();
+    x->vcodes.release();
     v.proxy = nullptr;
+    v.vcodes = nullptr;
 }
 
 // The host list layout and the small device tables every index carries:
@@ -999,12 +1013,7 @@ int e8qc_e8q_autotune(e8qc_index* x, int mode, size_t nq, size_t k, size_t nprob
         std::lock_guard<std::mutex> lock(x->mu);
         DeviceGuard g(x->device);
         cudaStream_t s = nullptr;
-        if (mode == E8QC_MODE_PRECISION && x->view.proxy == nullptr) {
-            x->proxy.alloc(proxy_plane_bytes(x->view, x->ntiles));
-            launch_build_proxy(x->view, static_cast<int>(x->ntiles), x->proxy.as<uint4>(), s);
-            x->view.proxy = x->proxy.as<uint4>();
-            x->view.proxy_scale = precision_proxy_step(x->view.bits, x->view.pd);
-        }
+        if (mode == E8QC_MODE_PRECISION) ensure_precision_planes(x, s);
         const TuneResult r = autotune_run(x, x->ws, mode, nq, k, nprobe, s);
         if (out) *out = e8qc_tuning{r.sched, r.stages, r.best_ms, r.default_ms};
     });

@@ -103,6 +103,7 @@ struct DevIndex {
     const uint32_t* list_of_tile;  // ntiles: the list each tile belongs to
     const uint4* proxy;            // precision mode's int8 proxy plane, or NULL until built
     float proxy_scale;             // E8Q: the plane's level step (proxy * step ~ table level)
+    const uint4* vcodes;           // precision mode: the codes slot-major (nch chunks per slot), or NULL
 };
 
 inline int code_chunks(int pd, int bits) { return (pd / 8 * 8 * bits + 127) / 128; }

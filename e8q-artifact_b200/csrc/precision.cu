@@ -168,6 +168,19 @@ __device__ __forceinline__ uint2 block_proxy(const uint32_t* w, int base, const 
     return make_uint2(lo, hi);
 }
 
+// Slot-major copy of the codes for the exact rescoring of scattered
+// candidates: out[slot * nch + c] = chunk c of the slot (tile-major source:
+// chunk c of lane l of tile t at codes[(t * nch + c) * 32 + l]). One thread
+// per output chunk (coalesced writes).
+__global__ void vcodes_kernel(const uint4* __restrict__ codes, size_t nslots, int nch, uint4* __restrict__ out) {
+    const size_t total = nslots * static_cast<size_t>(nch);
+    for (size_t e = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; e < total;
+         e += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const size_t slot = e / nch, c = e - slot * nch;
+        out[e] = codes[((slot >> 5) * nch + c) * 32 + (slot & 31)];
+    }
+}
+
 // Proxy plane: slot s, dimension i at byte (s/8)*8*pd + (i/16)*128 + (s%8)*16
 // + i%16 -- 8-slot row groups of 16-byte core-matrix rows, the K-major
 // no-swizzle operand layout of tcgen05, so the 64-dimension K-chunk kc of a
@@ -760,13 +773,14 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
             const int ng = (pd / 8) / GBL;
             const bool tail = ((pd / 8) % GBL) != 0;
             if (live) {
-                const int vl = static_cast<int>(slot & 31u);
-                const uint4* tp = ix.codes + static_cast<size_t>(tile) * ix.nch * 32;
+                // the candidate's own contiguous codes (slot-major copy): a
+                // lane's 16-byte reads walk one vector, not 512-byte strides
+                const uint4* vp = ix.vcodes + static_cast<size_t>(slot) * ix.nch;
                 float acc0 = 0.0f, acc1 = 0.0f;
                 for (int g = 0; g < ng; ++g)
-                    accumulate_blocks<BITS, GBL, GCH>(tp + g * GCH * 32, vl, sq4, g * GBL, tb_addr, acc0, acc1);
+                    accumulate_blocks<BITS, GBL, GCH, 1>(vp + g * GCH, 0, sq4, g * GBL, tb_addr, acc0, acc1);
                 if (tail)
-                    accumulate_blocks<BITS, 8, TCH>(tp + ng * GCH * 32, vl, sq4, ng * GBL, tb_addr, acc0, acc1);
+                    accumulate_blocks<BITS, 8, TCH, 1>(vp + ng * GCH, 0, sq4, ng * GBL, tb_addr, acc0, acc1);
                 const float S = __fadd_rn(acc0, acc1);
                 dist = __fmaf_rn(-__fmul_rn(2.0f, __ldg(ix.g1 + slot)), S, __fadd_rn(d2, __ldg(ix.h3 + slot)));
             }
@@ -970,6 +984,20 @@ int launch_build_proxy(const DevIndex& ix, int ntiles, uint4* plane, cudaStream_
     return launches;
 }
 
+size_t vcodes_bytes(const DevIndex& ix, size_t ntiles) {
+    return ntiles * 32 * static_cast<size_t>(ix.nch) * sizeof(uint4);
+}
+
+int launch_vcodes(const DevIndex& ix, int ntiles, uint4* out, cudaStream_t s) {
+    const size_t nslots = static_cast<size_t>(ntiles) * 32;
+    if (nslots == 0) return 0;
+    const size_t total = nslots * ix.nch;
+    const unsigned grid = static_cast<unsigned>(std::min<size_t>((total + 255) / 256, 148 * 16));
+    vcodes_kernel<<<grid, 256, 0, s>>>(ix.codes, nslots, ix.nch, out);
+    E8QC_CUDA(cudaGetLastError());
+    return 1;
+}
+
 int precision_candidates(int k) { return candidates_for(k); }
 
 size_t precision_row_scratch(size_t nq, size_t rows_per_query) {
@@ -983,6 +1011,8 @@ int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t 
     if (nq == 0) return 0;
     if (ix.pd % kPK != 0) fail(E8QC_EINVAL, "precision search needs the padded dimension to be a multiple of 64");
     if (ix.proxy == nullptr) fail(E8QC_ESTATE, "precision search needs the proxy plane (launch_build_proxy)");
+    if (me8q == nullptr && ix.vcodes == nullptr)
+        fail(E8QC_ESTATE, "precision search needs the slot-major codes (launch_vcodes)");
     const int C = precision_candidates(static_cast<int>(k));
     // the epilogue forms S' = (coef / qs) * (2 S8 + 0): E8Q coef = step / 2
     // (one table step for every vector); ME8Q coef = 1/2 with the slot's own

@@ -22,6 +22,11 @@ size_t proxy_plane_bytes(const DevIndex& ix, size_t ntiles);
 // Decode every slot's code into the proxy plane (layout in precision.cu).
 int launch_build_proxy(const DevIndex& ix, int ntiles, uint4* plane, cudaStream_t s);
 
+// Slot-major copy of an E8Q index's codes (each slot's nch chunks
+// contiguous), read by the exact rescoring of the precision mode.
+size_t vcodes_bytes(const DevIndex& ix, size_t ntiles);
+int launch_vcodes(const DevIndex& ix, int ntiles, uint4* out, cudaStream_t s);
+
 // Candidates kept per query for exact rescoring at a given k.
 int precision_candidates(int k);
 
