@@ -102,4 +102,21 @@ __device__ __forceinline__ void accumulate_blocks(const uint4* __restrict__ sbuf
     BlockRun<BITS, NBLK, 0>::run(w, tb_addr, sq4, qblk, acc0, acc1);
 }
 
+// Decode + accumulate NBLK consecutive blocks from NCH chunks held in
+// registers (the same words accumulate_blocks reads from memory).
+template <int BITS, int NBLK, int NCH>
+__device__ __forceinline__ void accumulate_regs(const uint4 (&v)[NCH], const float4* __restrict__ sq4, int qblk,
+                                                uint32_t tb_addr, float& acc0, float& acc1) {
+    uint32_t w[4 * NCH + 1];
+#pragma unroll
+    for (int c = 0; c < NCH; ++c) {
+        w[4 * c] = v[c].x;
+        w[4 * c + 1] = v[c].y;
+        w[4 * c + 2] = v[c].z;
+        w[4 * c + 3] = v[c].w;
+    }
+    w[4 * NCH] = 0;
+    BlockRun<BITS, NBLK, 0>::run(w, tb_addr, sq4, qblk, acc0, acc1);
+}
+
 }  // namespace e8qc

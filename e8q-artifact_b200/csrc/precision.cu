@@ -526,11 +526,10 @@ __device__ float me8q_rescore(const Me8qView& mv, uint32_t slot, const float* q,
     return static_cast<float>(acc);
 }
 
-// Per query (FW warps of a 4-warp block; 4/FW queries per block): best C
-// proxies over the query's rows, exact rescoring of those candidates (E8Q
-// estimator at BITS, or the ME8Q estimator), top-k by exact distance. FW = 4
-// for queries with many rows (long per-query chains), 1 otherwise (more
-// queries resident per SM).
+// Per query (FW warps of a 4-warp block; 4/FW queries per block): the best
+// C proxies over the query's rows, written as candidate slots for the
+// rescoring kernel. FW = 4 for queries with many rows (long per-query
+// chains), 1 otherwise.
 //
 // Rows are visited nearest list first (routing distance, then probe index):
 // the best proxies mostly sit in the nearest lists, so the thresholds settle
@@ -540,41 +539,29 @@ __device__ float me8q_rescore(const Me8qView& mv, uint32_t slot, const float* q,
 // publish their C-th best in shared memory and each filters with the
 // smallest of them (a value above another warp's C-th best has C better
 // values and cannot be in the query's top C). The query's first warp merges
-// the FW lists; its warps rescore the C candidates and the first warp keeps
-// the top k.
-template <int BITS, bool ME8Q, int FW>
-__global__ void __launch_bounds__(128) precision_final_kernel(
-    DevIndex ix, Me8qView mv, const float* __restrict__ rq, const __half* __restrict__ prox,
-    const unsigned long long* __restrict__ rowbase, const uint32_t* __restrict__ pair_off,
-    const uint32_t* __restrict__ pos_of, const uint32_t* __restrict__ probes, const float* __restrict__ pd2, int nq,
-    const uint32_t* __restrict__ np_arr, int np_max, const uint32_t* __restrict__ k_arr, int k_uniform, int C,
-    int out_stride, uint32_t* __restrict__ out_ids, float* __restrict__ out_d) {
+// the FW lists. The kernel holds no level table or query, so many warps stay
+// resident to keep the row reads in flight.
+template <int FW>
+__global__ void __launch_bounds__(128, 8) precision_select_kernel(
+    DevIndex ix, const __half* __restrict__ prox, const unsigned long long* __restrict__ rowbase,
+    const uint32_t* __restrict__ pair_off, const uint32_t* __restrict__ pos_of, const uint32_t* __restrict__ probes,
+    const float* __restrict__ pd2, int nq, const uint32_t* __restrict__ np_arr, int np_max,
+    const uint32_t* __restrict__ k_arr, int k_uniform, uint32_t* __restrict__ cand_out) {
     static_assert(FW == 1 || FW == 2 || FW == 4, "warps per query");
     constexpr int QPB = 4 / FW;  // queries per block
-    constexpr int Q = 1 << BITS;
-    constexpr int REP = table_rep(BITS);
-    constexpr int GBL = group_blocks(BITS), GCH = group_chunks(BITS);
-    constexpr int TCH = (64 * BITS + 127) / 128;
-    extern __shared__ __align__(16) float fsm[];
-    const int pd = ix.pd;
+    __shared__ __align__(16) float sbufs[4 * 512];        // per warp: one step of values; the query's d2 staging
+    __shared__ float cd[(FW > 1 ? 4 : 1) * kMaxK];      // per warp: candidate proxies (merge of FW lists)
+    __shared__ uint32_t ci[(FW > 1 ? 4 : 1) * kMaxK];   // per warp: candidate slots
+    __shared__ uint16_t ords[QPB * kOrdCap];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int qi = warp / FW, wq = warp % FW;  // query slot in the block, warp within the query
-    float* tabrep = fsm;                                           // 2*Q*REP (E8Q)
-    float* myq = tabrep + (ME8Q ? 0 : 2 * Q * REP) + qi * pd;      // the query's rotated query
-    float* sbufs = tabrep + (ME8Q ? 0 : 2 * Q * REP) + QPB * pd;   // 4 warps x 512
-    float* cd = sbufs + 4 * 512;                                   // 4 warps x kMaxK candidate distances
-    uint32_t* ci = reinterpret_cast<uint32_t*>(cd + 4 * kMaxK);    // 4 warps x kMaxK slots / ids
-    uint16_t* ord = reinterpret_cast<uint16_t*>(ci + 4 * kMaxK) + qi * kOrdCap;
+    uint16_t* ord = ords + qi * kOrdCap;
     __shared__ float s_thr[4];
     const int q = blockIdx.x * QPB + qi;
     const bool qvalid = q < nq;
-    if constexpr (!ME8Q)
-        for (int e = tid; e < 2 * Q * REP; e += blockDim.x) tabrep[e] = ix.tab[e / REP];
-    if (qvalid)
-        for (int i = wq * 32 + lane; i < pd; i += FW * 32) myq[i] = rq[static_cast<size_t>(q) * pd + i];
     const int np = qvalid ? (np_arr ? static_cast<int>(np_arr[q]) : np_max) : 0;
     const int kq = qvalid ? (k_arr ? static_cast<int>(k_arr[q]) : k_uniform) : 0;
-    C = candidates_for(kq);  // the query's own candidate count (uniform within the query's warps)
+    const int C = candidates_for(kq);  // the query's own candidate count (uniform within the query's warps)
     const uint32_t* pr = probes + static_cast<size_t>(qvalid ? q : 0) * np_max;
     const bool reorder = np <= kOrdCap;
     float* qstage = sbufs + qi * FW * 512;  // FW*512 >= kOrdCap floats: the query's d2 staging
@@ -726,9 +713,10 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
         nx[1] = nnx[1];
     }
     // 2. the query's first warp merges its warps' lists into the query's top C
-    float* qcd = cd + qi * FW * kMaxK;
-    uint32_t* qci = ci + qi * FW * kMaxK;
+    //    and writes the candidate slots (C of them, padding UINT32_MAX)
     if constexpr (FW > 1) {
+        const float* qcd = cd + qi * FW * kMaxK;
+        const uint32_t* qci = ci + qi * FW * kMaxK;
         cand.store(cd + warp * kMaxK, ci + warp * kMaxK, C);
         __syncthreads();
         if (wq == 0) {
@@ -738,62 +726,142 @@ __global__ void __launch_bounds__(128) precision_final_kernel(
                     const bool in = j < C && qci[w2 * kMaxK + j] != 0xFFFFFFFFu;
                     cand.offer_pair(in ? qcd[w2 * kMaxK + j] : inf_f(), in ? qci[w2 * kMaxK + j] : 0xFFFFFFFFu, in);
                 }
-            cand.store(qcd, qci, C);
         }
-    } else {
-        cand.store(qcd, qci, C);
+    }
+    if (wq == 0 && qvalid) {
+#pragma unroll
+        for (int s2 = 0; s2 < 4; ++s2) {
+            const int j = s2 * 32 + lane;
+            if (j < C) cand_out[static_cast<size_t>(q) * kMaxK + j] = cand.id[s2];
+        }
+    }
+}
+
+// Routing distance of (query, the list holding `slot`): the query's probes
+// (np of them, in list order) are binary-searched for the slot's list.
+__device__ __forceinline__ float rescore_d2(const DevIndex& ix, const uint32_t* __restrict__ pr, int np,
+                                            const float* __restrict__ qpd2, uint32_t slot) {
+    const uint32_t list = __ldg(ix.list_of_tile + (slot >> 5));
+    int lo = 0, hi = np;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (pr[mid] <= list) lo = mid;
+        else hi = mid;
+    }
+    return qpd2[lo];
+}
+
+// Exact rescoring of each query's C candidates (E8Q estimator at BITS, or
+// the ME8Q estimator) and the top k by exact distance. Four queries per
+// 4-warp block; the (query, 32-candidate chunk) units of the block are dealt
+// over its warps, then warp w keeps the top k of query w.
+template <int BITS, bool ME8Q>
+__global__ void __launch_bounds__(128) precision_rescore_kernel(
+    DevIndex ix, Me8qView mv, const float* __restrict__ rq, const uint32_t* __restrict__ cand,
+    const uint32_t* __restrict__ probes, const float* __restrict__ pd2, int nq, const uint32_t* __restrict__ np_arr,
+    int np_max, const uint32_t* __restrict__ k_arr, int k_uniform, int out_stride, uint32_t* __restrict__ out_ids,
+    float* __restrict__ out_d) {
+    constexpr int Q = 1 << BITS;
+    constexpr int REP = table_rep(BITS);
+    constexpr int GBL = group_blocks(BITS), GCH = group_chunks(BITS);
+    constexpr int TCH = (64 * BITS + 127) / 128;
+    extern __shared__ __align__(16) float fsm[];
+    const int pd = ix.pd;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float* tabrep = fsm;                                        // 2*Q*REP (E8Q)
+    float* myqs = tabrep + (ME8Q ? 0 : 2 * Q * REP);            // 4 rotated queries
+    float* cd = myqs + 4 * pd;                                  // 4 queries x kMaxK exact distances
+    uint32_t* ci = reinterpret_cast<uint32_t*>(cd + 4 * kMaxK);  // 4 queries x kMaxK slots, then ids
+    const int q0 = blockIdx.x * 4;
+    if constexpr (!ME8Q)
+        for (int e = tid; e < 2 * Q * REP; e += blockDim.x) tabrep[e] = ix.tab[e / REP];
+    int nunit[4], Cq[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const int q = q0 + t;
+        Cq[t] = q < nq ? candidates_for(k_arr ? static_cast<int>(k_arr[q]) : k_uniform) : 0;
+        nunit[t] = (Cq[t] + 31) / 32;
+    }
+    for (int e = tid; e < 4 * pd; e += blockDim.x) {
+        const int t = e / pd, i = e - t * pd;
+        myqs[e] = q0 + t < nq ? rq[static_cast<size_t>(q0 + t) * pd + i] : 0.0f;
+    }
+    for (int e = tid; e < 4 * kMaxK; e += blockDim.x) {
+        const int t = e / kMaxK, j = e - t * kMaxK;
+        ci[e] = j < Cq[t] ? cand[static_cast<size_t>(q0 + t) * kMaxK + j] : 0xFFFFFFFFu;
     }
     __syncthreads();
-    // 3. exact rescoring: the query's warp wq takes candidates wq*32 + lane,
-    //    + FW*32, ...; each lane writes its candidate's (distance, id) over its
-    //    (proxy, slot) entry
-    for (int j = wq * 32 + lane; j - lane < C; j += FW * 32) {
-        const uint32_t slot = j < C ? qci[j] : 0xFFFFFFFFu;
+    // 3. exact rescoring: unit u = (query t, candidates 32c..32c+31); each lane
+    //    writes its candidate's (distance, id) over its slot entry
+    const int total = nunit[0] + nunit[1] + nunit[2] + nunit[3];
+    for (int u = warp; u < total; u += 4) {
+        int t = 0, c = u;
+        while (c >= nunit[t]) c -= nunit[t++];
+        const int q = q0 + t;
+        const int np = np_arr ? static_cast<int>(np_arr[q]) : np_max;
+        const uint32_t* pr = probes + static_cast<size_t>(q) * np_max;
+        const float* myq = myqs + t * pd;
+        const int j = c * 32 + lane;
+        const uint32_t slot = j < Cq[t] ? ci[t * kMaxK + j] : 0xFFFFFFFFu;
         const bool live = slot != 0xFFFFFFFFu;
-        const uint32_t tile = live ? slot >> 5 : 0u;
         float dist = inf_f();
         uint32_t gid = 0xFFFFFFFFu;
-        float d2 = 0.0f;
-        if (live) {
-            // d2 of (query, the candidate's list): the query's probes are in list order
-            const uint32_t list = ix.list_of_tile[tile];
-            int lo = 0, hi = np;
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (pr[mid] <= list) lo = mid;
-                else hi = mid;
-            }
-            d2 = pd2[static_cast<size_t>(q) * np_max + lo];
-        }
         if constexpr (ME8Q) {
-            if (live) dist = me8q_rescore(mv, slot, myq, d2);
-        } else {
-            const uint32_t tb_addr = static_cast<uint32_t>(__cvta_generic_to_shared(tabrep)) + (lane % REP) * 4u;
-            const float4* sq4 = reinterpret_cast<const float4*>(myq);
+            if (live) {
+                const float d2 = rescore_d2(ix, pr, np, pd2 + static_cast<size_t>(q) * np_max, slot);
+                dist = me8q_rescore(mv, slot, myq, d2);
+            }
+        } else if (live) {
+            // The candidate's codes (slot-major copy, contiguous) stream
+            // through a ring of PF prefetched groups; the factors and id are
+            // loaded and the routing distance searched while they are in flight.
+            constexpr int PF = GCH >= 12 ? 1 : (12 / GCH >= 3 ? 3 : 12 / GCH);
+            const uint4* vp = ix.vcodes + static_cast<size_t>(slot) * ix.nch;
             const int ng = (pd / 8) / GBL;
             const bool tail = ((pd / 8) % GBL) != 0;
-            if (live) {
-                // the candidate's own contiguous codes (slot-major copy): a
-                // lane's 16-byte reads walk one vector, not 512-byte strides
-                const uint4* vp = ix.vcodes + static_cast<size_t>(slot) * ix.nch;
-                float acc0 = 0.0f, acc1 = 0.0f;
-                for (int g = 0; g < ng; ++g)
-                    accumulate_blocks<BITS, GBL, GCH, 1>(vp + g * GCH, 0, sq4, g * GBL, tb_addr, acc0, acc1);
-                if (tail)
-                    accumulate_blocks<BITS, 8, TCH, 1>(vp + ng * GCH, 0, sq4, ng * GBL, tb_addr, acc0, acc1);
-                const float S = __fadd_rn(acc0, acc1);
-                dist = __fmaf_rn(-__fmul_rn(2.0f, __ldg(ix.g1 + slot)), S, __fadd_rn(d2, __ldg(ix.h3 + slot)));
+            uint4 ring[PF][GCH];
+#pragma unroll
+            for (int r = 0; r < PF; ++r)
+                if (r < ng)
+#pragma unroll
+                    for (int c = 0; c < GCH; ++c) ring[r][c] = __ldg(vp + r * GCH + c);
+            const float g1 = __ldg(ix.g1 + slot), h3 = __ldg(ix.h3 + slot);
+            gid = __ldg(ix.ids + slot);
+            const float d2 = rescore_d2(ix, pr, np, pd2 + static_cast<size_t>(q) * np_max, slot);
+            const uint32_t tb_addr = static_cast<uint32_t>(__cvta_generic_to_shared(tabrep)) + (lane % REP) * 4u;
+            const float4* sq4 = reinterpret_cast<const float4*>(myq);
+            float acc0 = 0.0f, acc1 = 0.0f;
+            for (int g = 0; g < ng; ++g) {
+                uint4 cur[GCH];
+#pragma unroll
+                for (int c = 0; c < GCH; ++c) cur[c] = ring[0][c];
+#pragma unroll
+                for (int r = 0; r + 1 < PF; ++r)
+#pragma unroll
+                    for (int c = 0; c < GCH; ++c) ring[r][c] = ring[r + 1][c];
+                if (g + PF < ng)
+#pragma unroll
+                    for (int c = 0; c < GCH; ++c) ring[PF - 1][c] = __ldg(vp + (g + PF) * GCH + c);
+                accumulate_regs<BITS, GBL, GCH>(cur, sq4, g * GBL, tb_addr, acc0, acc1);
             }
+            if (tail) accumulate_blocks<BITS, 8, TCH, 1>(vp + ng * GCH, 0, sq4, ng * GBL, tb_addr, acc0, acc1);
+            const float S = __fadd_rn(acc0, acc1);
+            dist = __fmaf_rn(-__fmul_rn(2.0f, g1), S, __fadd_rn(d2, h3));
         }
-        if (live) gid = __ldg(ix.ids + slot);
-        if (j < C) {
-            qcd[j] = dist;
-            qci[j] = gid;
+        if (live && ME8Q) gid = __ldg(ix.ids + slot);
+        if (j < Cq[t]) {
+            cd[t * kMaxK + j] = dist;
+            ci[t * kMaxK + j] = gid;
         }
     }
     __syncthreads();
-    // 4. top k by exact distance
-    if (wq == 0 && qvalid) {
+    // 4. top k by exact distance: warp w, query q0 + w
+    const int q = q0 + warp;
+    if (q < nq) {
+        const int kq = k_arr ? static_cast<int>(k_arr[q]) : k_uniform;
+        const int C = Cq[warp];
+        const float* qcd = cd + warp * kMaxK;
+        const uint32_t* qci = ci + warp * kMaxK;
         WarpTopK top;
         top.init(kq);
         for (int s2 = 0; s2 * 32 < C; ++s2) {
@@ -882,40 +950,43 @@ void launch_scan(const DevIndex& ix, Workspace& ws, size_t a_rows, size_t plane_
 }
 
 // Per-query selection + exact rescoring of one chunk of queries.
-template <int BITS, bool ME8Q, int FW>
-int launch_final_fw(const DevIndex& ix, const Me8qView& mv, Workspace& ws, const float* rq, size_t nq,
-                    const uint32_t* k_arr, const uint32_t* np_arr, int k_max, int np_max, int C, int out_stride,
-                    uint32_t* out_ids, float* out_d, cudaStream_t s) {
-    int dev = 0;
-    E8QC_CUDA(cudaGetDevice(&dev));
-    constexpr int REP = table_rep(BITS);
+template <int FW>
+int launch_select_fw(const DevIndex& ix, Workspace& ws, size_t nq, const uint32_t* k_arr, const uint32_t* np_arr,
+                     int k_max, int np_max, cudaStream_t s) {
     constexpr int QPB = 4 / FW;
-    const size_t fsmem = ((ME8Q ? 0 : static_cast<size_t>(2) * (1 << BITS) * REP) +
-                          static_cast<size_t>(QPB) * ix.pd + 4 * 512 + 4 * kMaxK * 2) * 4 +
-                         static_cast<size_t>(QPB) * kOrdCap * 2;
-    static size_t fconfigured[64] = {};
-    if (fsmem > 48 * 1024 && fconfigured[dev & 63] < fsmem) {
-        E8QC_CUDA(cudaFuncSetAttribute(precision_final_kernel<BITS, ME8Q, FW>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(fsmem)));
-        fconfigured[dev & 63] = fsmem;
-    }
-    precision_final_kernel<BITS, ME8Q, FW><<<static_cast<unsigned>((nq + QPB - 1) / QPB), 128, fsmem, s>>>(
-        ix, mv, rq, ws.p_prox.as<__half>(), ws.p_rowbase.as<unsigned long long>(), ws.b_off.as<uint32_t>(),
+    precision_select_kernel<FW><<<static_cast<unsigned>((nq + QPB - 1) / QPB), 128, 0, s>>>(
+        ix, ws.p_prox.as<__half>(), ws.p_rowbase.as<unsigned long long>(), ws.b_off.as<uint32_t>(),
         ws.b_pos.as<uint32_t>(), ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(), static_cast<int>(nq), np_arr,
-        np_max, k_arr, k_max, C, out_stride, out_ids, out_d);
+        np_max, k_arr, k_max, ws.p_cand.as<uint32_t>());
     E8QC_CUDA(cudaGetLastError());
     return 1;
 }
 
+// Candidate selection (4 warps per query from kFinalWideRows proxy rows per
+// query, else one) and then the exact rescoring.
 template <int BITS, bool ME8Q = false>
 int launch_final(const DevIndex& ix, const Me8qView& mv, Workspace& ws, const float* rq, size_t nq,
-                 const uint32_t* k_arr, const uint32_t* np_arr, int k_max, int np_max, int C, int out_stride,
+                 const uint32_t* k_arr, const uint32_t* np_arr, int k_max, int np_max, int out_stride,
                  uint32_t* out_ids, float* out_d, size_t rows_per_query, cudaStream_t s) {
-    if (rows_per_query >= kFinalWideRows)
-        return launch_final_fw<BITS, ME8Q, 4>(ix, mv, ws, rq, nq, k_arr, np_arr, k_max, np_max, C, out_stride,
-                                              out_ids, out_d, s);
-    return launch_final_fw<BITS, ME8Q, 1>(ix, mv, ws, rq, nq, k_arr, np_arr, k_max, np_max, C, out_stride, out_ids,
-                                          out_d, s);
+    int launches = rows_per_query >= kFinalWideRows
+                       ? launch_select_fw<4>(ix, ws, nq, k_arr, np_arr, k_max, np_max, s)
+                       : launch_select_fw<1>(ix, ws, nq, k_arr, np_arr, k_max, np_max, s);
+    int dev = 0;
+    E8QC_CUDA(cudaGetDevice(&dev));
+    constexpr int REP = table_rep(BITS);
+    const size_t fsmem =
+        ((ME8Q ? 0 : static_cast<size_t>(2) * (1 << BITS) * REP) + static_cast<size_t>(4) * ix.pd + 4 * kMaxK * 2) * 4;
+    static size_t fconfigured[64] = {};
+    if (fsmem > 48 * 1024 && fconfigured[dev & 63] < fsmem) {
+        E8QC_CUDA(cudaFuncSetAttribute(precision_rescore_kernel<BITS, ME8Q>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(fsmem)));
+        fconfigured[dev & 63] = fsmem;
+    }
+    precision_rescore_kernel<BITS, ME8Q><<<static_cast<unsigned>((nq + 3) / 4), 128, fsmem, s>>>(
+        ix, mv, rq, ws.p_cand.as<uint32_t>(), ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(), static_cast<int>(nq),
+        np_arr, np_max, k_arr, k_max, out_stride, out_ids, out_d);
+    E8QC_CUDA(cudaGetLastError());
+    return launches + 1;
 }
 
 template <int BITS>
@@ -1002,7 +1073,8 @@ int precision_candidates(int k) { return candidates_for(k); }
 
 size_t precision_row_scratch(size_t nq, size_t rows_per_query) {
     const size_t per_q = std::max<size_t>(1, rows_per_query) * sizeof(__half);
-    return std::max<size_t>(1, std::min(nq, kScratchBudget / per_q)) * per_q;
+    const size_t chunk = std::max<size_t>(1, std::min(nq, kScratchBudget / per_q));
+    return chunk * (per_q + static_cast<size_t>(kMaxK) * 4);  // proxy rows + candidate slots
 }
 
 int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* k_arr,
@@ -1013,7 +1085,6 @@ int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t 
     if (ix.proxy == nullptr) fail(E8QC_ESTATE, "precision search needs the proxy plane (launch_build_proxy)");
     if (me8q == nullptr && ix.vcodes == nullptr)
         fail(E8QC_ESTATE, "precision search needs the slot-major codes (launch_vcodes)");
-    const int C = precision_candidates(static_cast<int>(k));
     // the epilogue forms S' = (coef / qs) * (2 S8 + 0): E8Q coef = step / 2
     // (one table step for every vector); ME8Q coef = 1/2 with the slot's own
     // step in the g1 plane (hsum in h3)
@@ -1040,6 +1111,7 @@ int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t 
         ws.p_pscale.ensure(n * 4);
         ws.p_rowbase.ensure(static_cast<size_t>(ix.nlist) * 8);
         ws.p_prox.ensure(n * per_q);
+        ws.p_cand.ensure(n * static_cast<size_t>(kMaxK) * 4);
         ws.p_a8.ensure(arows * ix.pd);
         rowbase_kernel<<<1, 1024, 0, s>>>(ws.b_cnt.as<uint32_t>(), ix.tile_begin, ix.nlist,
                                           ws.p_rowbase.as<unsigned long long>());
@@ -1055,7 +1127,7 @@ int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t 
         ws.mark_final(false, s);
         if (me8q) {
             launches += launch_final<1, true>(ix, *me8q, ws, rqc, n, kc, npc, static_cast<int>(k),
-                                              static_cast<int>(nprobe), C, static_cast<int>(out_stride),
+                                              static_cast<int>(nprobe), static_cast<int>(out_stride),
                                               out_ids + off * out_stride, out_d + off * out_stride, rows_per_query,
                                               s);
             ws.mark_final(true, s);
@@ -1065,7 +1137,7 @@ int precision_search(const DevIndex& ix, Workspace& ws, const float* rq, size_t 
 #define E8QC_CASE(b)                                                                                             \
     case b:                                                                                                      \
         launches += launch_final<b>(ix, none, ws, rqc, n, kc, npc, static_cast<int>(k), static_cast<int>(nprobe), \
-                                    C, static_cast<int>(out_stride), out_ids + off * out_stride,                 \
+                                    static_cast<int>(out_stride), out_ids + off * out_stride,                    \
                                     out_d + off * out_stride, rows_per_query, s);                                \
         break;
             E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)

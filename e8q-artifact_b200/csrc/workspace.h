@@ -63,7 +63,7 @@ struct Workspace {
         b_nitems, b_part_d, b_part_id;
     // precision path: int8 queries, per-query scale and sum, per-list row
     // bases, the proxy-distance rows and the gathered int8 query rows
-    DevBuf p_q8, p_scale, p_sum, p_rowbase, p_prox, p_a8, p_pscale;
+    DevBuf p_q8, p_scale, p_sum, p_rowbase, p_prox, p_a8, p_pscale, p_cand;
     // tuning of the grouped paths (chosen by the autotuner): work-queue order
     // (0: longest list first, 1: list id order) and the precision scan's
     // shared-memory ring depth (4, 6 or 8 K-chunk stages)
