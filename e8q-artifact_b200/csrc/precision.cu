@@ -526,6 +526,9 @@ __device__ float me8q_rescore(const Me8qView& mv, uint32_t slot, const float* q,
     return static_cast<float>(acc);
 }
 
+constexpr uint32_t kHalfInf2 = 0x7C007C00u;  // two fp16 +inf
+__device__ __forceinline__ __half2 u32_as_half2(uint32_t w) { return *reinterpret_cast<const __half2*>(&w); }
+
 // Per query (FW warps of a 4-warp block; 4/FW queries per block): the best
 // C proxies over the query's rows, written as candidate slots for the
 // rescoring kernel. FW = 4 for queries with many rows (long per-query
@@ -643,7 +646,7 @@ __global__ void __launch_bounds__(128, 8) precision_select_kernel(
         for (int j = 0; j < 2; ++j) {
             const uint32_t va = st.v0 + 256 * j + 8 * lane;
             x[j] = (st.p < npw && va < st.len) ? __ldcs(reinterpret_cast<const uint4*>(prox + st.off) + (va >> 3))
-                                               : make_uint4(0u, 0u, 0u, 0u);
+                                               : make_uint4(kHalfInf2, kHalfInf2, kHalfInf2, kHalfInf2);
         }
     };
     load_window(0);
@@ -663,6 +666,22 @@ __global__ void __launch_bounds__(128, 8) precision_select_kernel(
         if constexpr (FW > 1) {
 #pragma unroll
             for (int w2 = 0; w2 < FW; ++w2) filt = fminf(filt, vthr[w2]);
+        }
+        // quick test first: can any of the lane's 16 values pass? (for a half
+        // v and a float f, v > f exactly when v > f rounded down to a half)
+        __half2 mn = __hmin2(__hmin2(__hmin2(u32_as_half2(cx[0].x), u32_as_half2(cx[0].y)),
+                                     __hmin2(u32_as_half2(cx[0].z), u32_as_half2(cx[0].w))),
+                             __hmin2(__hmin2(u32_as_half2(cx[1].x), u32_as_half2(cx[1].y)),
+                                     __hmin2(u32_as_half2(cx[1].z), u32_as_half2(cx[1].w))));
+        const bool maybe = __hle2_mask(mn, __half2half2(__float2half_rd(filt))) != 0u;
+        if (!__any_sync(kFull, maybe)) {
+            cur = nxt;
+            cx[0] = nx[0];
+            cx[1] = nx[1];
+            nxt = nn;
+            nx[0] = nnx[0];
+            nx[1] = nnx[1];
+            continue;
         }
         float v[16];
 #pragma unroll
