@@ -23,6 +23,7 @@
 #include "device_common.cuh"
 #include "internal.h"
 #include "me8q.h"
+#include "route_tc.h"
 #include "workspace.h"
 
 namespace e8qc {
@@ -793,6 +794,9 @@ size_t batched_scan_smem(const DevIndex& ix, int k_max) {
     return (static_cast<size_t>(2) * kKC * kQT + 2 * kKC * kVT + 2 * (1 << ix.bits) + 2 * kQT * k_max) * 4;
 }
 
+int group_pairs(const DevIndex& ix, Workspace& ws, size_t nq, const uint32_t* np_arr, int np_max, size_t pslots,
+                size_t item_cap, int qt, int align, cudaStream_t s);
+
 int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* np_arr,
                     size_t nprobe, size_t part_width, int qt, int align, cudaStream_t s) {
     const int nlist = ix.nlist;
@@ -819,13 +823,17 @@ int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t n
     int launches = 0;
     qn2_kernel<<<static_cast<unsigned>(nq), 256, 0, s>>>(rq, ix.pd, ws.b_qn2.as<float>());
     ++launches;
+    E8QC_CUDA(cudaMemsetAsync(ws.b_cnt.p, 0, static_cast<size_t>(nlist) * 4, s));
+    E8QC_CUDA(cudaMemsetAsync(ws.b_nitems.p, 0, 48, s));  // [0] n_items, [1] head, [2..7] pair / vector / list-vector counts
+    if (ws.route_tc && route_tc_applies(ix, nq)) {
+        launches += route_tc(ix, ws, rq, nq, np_arr, np_max, s);
+        return launches + group_pairs(ix, ws, nq, np_arr, np_max, pslots, item_cap, qt, align, s);
+    }
     if (ix.pd % kRouteBK != 0) fail(E8QC_EINVAL, "batched route needs the padded dimension to be a multiple of 16");
     dim3 g((nlist + kRouteBC - 1) / kRouteBC, static_cast<unsigned>((nq + kRouteBQ - 1) / kRouteBQ));
     route_gemm_kernel<<<g, 128, 0, s>>>(rq, static_cast<int>(nq), ix.cen, ix.cn2, nlist, ix.pd, ws.b_qn2.as<float>(),
                                         ws.b_keys.as<uint64_t>());
     ++launches;
-    E8QC_CUDA(cudaMemsetAsync(ws.b_cnt.p, 0, static_cast<size_t>(nlist) * 4, s));
-    E8QC_CUDA(cudaMemsetAsync(ws.b_nitems.p, 0, 48, s));  // [0] n_items, [1] head, [2..7] pair / vector / list-vector counts
     const size_t sel_smem = static_cast<size_t>(nlist) * 8;
     if (sel_smem > 200 * 1024) fail(E8QC_EINVAL, "batched route supports at most 25600 lists");
     {
@@ -843,6 +851,16 @@ int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t n
         ws.b_keys.as<uint64_t>(), nlist, np_arr, np_max, np_max, ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(),
         ws.b_cnt.as<uint32_t>());
     ++launches;
+    return launches + group_pairs(ix, ws, nq, np_arr, np_max, pslots, item_cap, qt, align, s);
+}
+
+// Work items and the (query, list) pair arrays from the probes and per-list
+// pair counts of a routed batch.
+int group_pairs(const DevIndex& ix, Workspace& ws, size_t nq, const uint32_t* np_arr, int np_max, size_t pslots,
+                size_t item_cap, int qt, int align, cudaStream_t s) {
+    const int nlist = ix.nlist;
+    const size_t npairs = nq * static_cast<size_t>(np_max);
+    int launches = 0;
     uint32_t* nitems = ws.b_nitems.as<uint32_t>();
     items_kernel<<<1, 1024, 0, s>>>(ws.b_cnt.as<uint32_t>(), ix.list_order + (ws.sched ? nlist : 0), nlist,
                                     ws.b_off.as<uint32_t>(),

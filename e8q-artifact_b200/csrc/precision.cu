@@ -904,6 +904,8 @@ constexpr size_t scan_smem(int stages) {
     return static_cast<size_t>(stages) * kStageBytes + static_cast<size_t>(4) * kPN * 8;
 }
 
+}  // namespace
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against the driver library).
 PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
@@ -932,6 +934,8 @@ CUtensorMap plane_map(const void* base, size_t row_groups, int pd, uint32_t box_
     if (r != CUDA_SUCCESS) fail(E8QC_ECUDA, "cuTensorMapEncodeTiled failed");
     return m;
 }
+
+namespace {
 
 template <int STAGES>
 void launch_scan_stages(const DevIndex& ix, Workspace& ws, const CUtensorMap& map_a, const CUtensorMap& map_b,

@@ -2,6 +2,7 @@
 // followed by exact rescoring of each query's candidates.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stddef.h>
 #include <stdint.h>
@@ -26,6 +27,12 @@ int launch_build_proxy(const DevIndex& ix, int ntiles, uint4* plane, cudaStream_
 // contiguous), read by the exact rescoring of the precision mode.
 size_t vcodes_bytes(const DevIndex& ix, size_t ntiles);
 int launch_vcodes(const DevIndex& ix, int ntiles, uint4* out, cudaStream_t s);
+
+// A row-group int8 plane (8-row groups of 16-byte core-matrix rows, K-major:
+// row r, byte k at (r/8)*8*pd + (k/16)*128 + (r%8)*16 + k%16) as a 2D tensor
+// map over row groups (8*pd bytes each, seen as 2*pd u32) whose box is
+// box_rows row groups x 512 bytes (one 64-byte K-chunk of each row).
+CUtensorMap plane_map(const void* base, size_t row_groups, int pd, uint32_t box_rows);
 
 // Candidates kept per query for exact rescoring at a given k.
 int precision_candidates(int k);

@@ -64,11 +64,16 @@ struct Workspace {
     // precision path: int8 queries, per-query scale and sum, per-list row
     // bases, the proxy-distance rows and the gathered int8 query rows
     DevBuf p_q8, p_scale, p_sum, p_rowbase, p_prox, p_a8, p_pscale, p_cand;
+    // tensor-core routing: int8 slice planes and per-row scale / norms of the
+    // queries and the centroids
+    DevBuf r_qplane, r_cplane, r_qmeta, r_cmeta, r_cand, r_ncand, r_units, r_ckeys;
     // tuning of the grouped paths (chosen by the autotuner): work-queue order
     // (0: longest list first, 1: list id order) and the precision scan's
     // shared-memory ring depth (4, 6 or 8 K-chunk stages)
     int sched = 0;
     int stages = 6;
+    // batch routing on the int8 tensor cores (route_tc) where it applies
+    bool route_tc = true;
     // optional CUDA events around the batched / precision scan kernel (set by
     // the caller while profiling; recorded on the launch stream)
     cudaEvent_t scan_ev0 = nullptr, scan_ev1 = nullptr;
