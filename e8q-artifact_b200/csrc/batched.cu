@@ -154,34 +154,18 @@ __global__ void __launch_bounds__(128, 2) route_gemm_kernel(const float* __restr
     }
 }
 
-// Per-query top-nprobe: one CTA per query, keys staged in shared memory,
-// 8-pass MSB radix select of the nprobe-th key, compaction in cid order.
-__global__ void select_kernel(const uint64_t* __restrict__ keys, int nlist, const uint32_t* __restrict__ np_arr,
-                              int np_uniform, int np_max, uint32_t* __restrict__ probes,
-                              float* __restrict__ pd2, uint32_t* __restrict__ list_cnt) {
-    extern __shared__ unsigned long long skeys[];
-    __shared__ int hist[256];
-    __shared__ unsigned long long s_prefix;
-    __shared__ int s_want;
-    __shared__ int sm32[32];
+// The want-th smallest of n 32-bit values in shared memory by MSB radix
+// select with 8-bit digits (four passes); every thread of the block gets it.
+// hist: 256 ints; sm: 2 ints.
+__device__ uint32_t block_select32(const uint32_t* v, int n, int want, int* hist, int* sm) {
     const int tid = threadIdx.x, nt = blockDim.x;
-    const int q = blockIdx.x;
-    const int nprobe = np_arr ? static_cast<int>(np_arr[q]) : np_uniform;
-    const unsigned long long* kq = reinterpret_cast<const unsigned long long*>(keys) + static_cast<size_t>(q) * nlist;
-    for (int c = tid; c < nlist; c += nt) skeys[c] = kq[c];
-    if (tid == 0) {
-        s_prefix = 0;
-        s_want = nprobe;
-    }
-    unsigned long long mask = 0;
-    __syncthreads();
-    for (int shift = 56; shift >= 0; shift -= 8) {
+    uint32_t prefix = 0, mask = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
         for (int i = tid; i < 256; i += nt) hist[i] = 0;
         __syncthreads();
-        const unsigned long long prefix = s_prefix;
-        for (int c = tid; c < nlist; c += nt) {
-            const unsigned long long key = skeys[c];
-            if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1);
+        for (int c = tid; c < n; c += nt) {
+            const uint32_t x = v[c];
+            if ((x & mask) == prefix) atomicAdd(&hist[(x >> shift) & 255u], 1);
         }
         __syncthreads();
         if (tid < 32) {
@@ -198,7 +182,6 @@ __global__ void select_kernel(const uint64_t* __restrict__ keys, int nlist, cons
                 if (tid >= o) incl += y;
             }
             const int excl = incl - tot;
-            const int want = s_want;
             const unsigned hit = __ballot_sync(kFull, excl < want && incl >= want);
             const int owner = __ffs(hit) - 1;
             if (tid == owner) {
@@ -211,49 +194,173 @@ __global__ void select_kernel(const uint64_t* __restrict__ keys, int nlist, cons
                     }
                     cum += cnt[j];
                 }
-                s_prefix = prefix | (static_cast<unsigned long long>(tid * 8 + sel) << shift);
-                s_want = want - cum;
+                sm[0] = tid * 8 + sel;
+                sm[1] = want - cum;
             }
         }
-        mask |= 0xFFull << shift;
+        __syncthreads();
+        prefix |= static_cast<uint32_t>(sm[0]) << shift;
+        mask |= 0xFFu << shift;
+        want = sm[1];
         __syncthreads();
     }
-    const unsigned long long kth = s_prefix;
-    int base = 0;
-    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    return prefix;
+}
+
+// d2 bits of (query row qr, list c) by route_gemm_kernel's sequential fp64
+// chain, computed by a whole warp: per 32-dimension block each lane loads
+// one element of both rows (coalesced, the next block in flight) and every
+// lane runs the same chain on the shuffled values.
+__device__ uint32_t warp_exact_d2(const float* __restrict__ qr, const float* __restrict__ cen, int pd, float qq,
+                                  float cc, int c) {
+    const int lane = threadIdx.x & 31;
+    const float* cr = cen + static_cast<size_t>(c) * pd;
+    float qv = qr[lane], cv = cr[lane];
+    double acc = 0.0;
+    for (int k = 0; k < pd; k += 32) {
+        const float nq = k + 32 < pd ? qr[k + 32 + lane] : 0.0f;
+        const float nc = k + 32 < pd ? cr[k + 32 + lane] : 0.0f;
+#pragma unroll
+        for (int l = 0; l < 32; ++l)
+            acc = __fma_rn(static_cast<double>(__shfl_sync(kFull, qv, l)), static_cast<double>(__shfl_sync(kFull, cv, l)),
+                           acc);
+        qv = nq;
+        cv = nc;
+    }
+    float d2 = __fmaf_rn(-2.0f, static_cast<float>(acc), __fadd_rn(qq, cc));
+    if (d2 < 0.0f) d2 = 0.0f;
+    return __float_as_uint(d2);
+}
+
+// Per-query top-nprobe: one CTA per query. A key is exact, or (from the
+// tensor-core route) an interval: the low word's bit 31 set, the high word a
+// lower bound of the list's d2 bits and ub[q * nlist + c] an upper bound. The
+// nprobe-th smallest upper bound U bounds the true nprobe-th d2; interval
+// lists whose lower bound is at most U get their exact key (the fp64 chain),
+// the rest keep their lower bound (above U, never selected). Then the
+// nprobe-th smallest d2 T (11-bit radix select), and the lists with d2 < T
+// plus the first ones in list order with d2 == T -- the nprobe smallest
+// 64-bit keys -- are written in list order with their d2.
+__global__ void select_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ ub, int nlist,
+                              const uint32_t* __restrict__ np_arr, int np_uniform, int np_max,
+                              const float* __restrict__ rq, const float* __restrict__ cen, int pd,
+                              const float* __restrict__ qn2, const float* __restrict__ cn2,
+                              uint32_t* __restrict__ probes, float* __restrict__ pd2,
+                              uint32_t* __restrict__ list_cnt) {
+    extern __shared__ uint32_t shi[];  // nlist d2 words, then nlist interval lower bounds
+    uint32_t* slb = shi + nlist;
+    __shared__ int hist[256];
+    __shared__ int sm[34];
+    __shared__ int s_any, s_nres;
+    __shared__ int s_res[256];  // interval lists to resolve (more are resolved in further rounds)
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    const int q = blockIdx.x;
+    const int want = min(np_arr ? static_cast<int>(np_arr[q]) : np_uniform, nlist);
+    const unsigned long long* kq = reinterpret_cast<const unsigned long long*>(keys) + static_cast<size_t>(q) * nlist;
+    if (tid == 0) s_any = 0;
+    __syncthreads();
+    bool any = false;
+    for (int c = tid; c < nlist; c += nt) {
+        const unsigned long long key = kq[c];
+        if (key & 0x80000000ull) {
+            slb[c] = static_cast<uint32_t>(key >> 32);
+            shi[c] = ub[static_cast<size_t>(q) * nlist + c];
+            any = true;
+        } else {
+            slb[c] = 0xFFFFFFFFu;  // exact
+            shi[c] = static_cast<uint32_t>(key >> 32);
+        }
+    }
+    if (any) s_any = 1;
+    __syncthreads();
+    if (s_any) {
+        const uint32_t U = block_select32(shi, nlist, want, hist, sm);
+        const float* qr = rq + static_cast<size_t>(q) * pd;
+        // interval lists that could be selected get their exact d2 (one warp
+        // each); the others keep their lower bound, above U
+        for (int c0 = 0; c0 < nlist; c0 += 256) {
+            if (tid == 0) s_nres = 0;
+            __syncthreads();
+            for (int c = c0 + tid; c < min(nlist, c0 + 256); c += nt) {
+                if (slb[c] == 0xFFFFFFFFu) continue;
+                if (slb[c] <= U) s_res[atomicAdd(&s_nres, 1)] = c;
+                else shi[c] = slb[c];
+            }
+            __syncthreads();
+            for (int i = warp; i < s_nres; i += nw) {
+                const int c = s_res[i];
+                const uint32_t d = warp_exact_d2(qr, cen, pd, qn2[q], cn2[c], c);
+                if (lane == 0) shi[c] = d;
+            }
+            __syncthreads();
+        }
+    }
+    const uint32_t T = block_select32(shi, nlist, want, hist, sm);
+    // lists below T, then ties at T in list order, up to want
+    int below = 0;
     for (int c0 = 0; c0 < nlist; c0 += nt) {
         const int c = c0 + tid;
-        const unsigned long long key = c < nlist ? skeys[c] : ~0ull;
-        const int flag = (c < nlist && key <= kth) ? 1 : 0;
-        // block exclusive scan of flag
-        int x = flag;
+        const int f = (c < nlist && shi[c] < T) ? 1 : 0;
+        below += __syncthreads_count(f);
+    }
+    int base = 0, ties = 0;
+    const int room = want - below;  // ties taken
+    for (int c0 = 0; c0 < nlist; c0 += nt) {
+        const int c = c0 + tid;
+        const uint32_t h = c < nlist ? shi[c] : 0xFFFFFFFFu;
+        const int tie = (c < nlist && h == T) ? 1 : 0;
+        // block exclusive scans of (tie) and of (selected)
+        int x = tie;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(kFull, x, o);
             if (lane >= o) x += y;
         }
-        if (lane == 31) sm32[warp] = x;
+        if (lane == 31) sm[warp] = x;
         __syncthreads();
         if (warp == 0) {
-            int s = lane < nw ? sm32[lane] : 0;
+            int v = lane < nw ? sm[lane] : 0;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(kFull, s, o);
-                if (lane >= o) s += y;
+                const int y = __shfl_up_sync(kFull, v, o);
+                if (lane >= o) v += y;
             }
-            sm32[lane] = s;
+            sm[lane] = v;
         }
         __syncthreads();
-        const int pos = base + (warp > 0 ? sm32[warp - 1] : 0) + x - flag;
-        const int tot = sm32[nw - 1];
+        const int tie_rank = ties + (warp > 0 ? sm[warp - 1] : 0) + x - tie;
+        const int tie_tot = sm[nw - 1];
+        __syncthreads();
+        const int flag = (c < nlist && (h < T || (tie && tie_rank < room))) ? 1 : 0;
+        x = flag;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) sm[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int v = lane < nw ? sm[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(kFull, v, o);
+                if (lane >= o) v += y;
+            }
+            sm[lane] = v;
+        }
+        __syncthreads();
+        const int pos = base + (warp > 0 ? sm[warp - 1] : 0) + x - flag;
+        const int tot = sm[nw - 1];
+        __syncthreads();
         if (flag) {
             const size_t o = static_cast<size_t>(q) * np_max + pos;
             probes[o] = static_cast<uint32_t>(c);
-            pd2[o] = __uint_as_float(static_cast<uint32_t>(key >> 32));
+            pd2[o] = __uint_as_float(h);
             atomicAdd(&list_cnt[c], 1u);
         }
         base += tot;
-        __syncthreads();
+        ties += tie_tot;
     }
 }
 
@@ -826,15 +933,16 @@ int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t n
     E8QC_CUDA(cudaMemsetAsync(ws.b_cnt.p, 0, static_cast<size_t>(nlist) * 4, s));
     E8QC_CUDA(cudaMemsetAsync(ws.b_nitems.p, 0, 48, s));  // [0] n_items, [1] head, [2..7] pair / vector / list-vector counts
     if (ws.route_tc && route_tc_applies(ix, nq)) {
-        launches += route_tc(ix, ws, rq, nq, np_arr, np_max, s);
-        return launches + group_pairs(ix, ws, nq, np_arr, np_max, pslots, item_cap, qt, align, s);
+        launches += route_tc_keys(ix, ws, rq, nq, s);
+    } else {
+        if (ix.pd % kRouteBK != 0)
+            fail(E8QC_EINVAL, "batched route needs the padded dimension to be a multiple of 16");
+        dim3 g((nlist + kRouteBC - 1) / kRouteBC, static_cast<unsigned>((nq + kRouteBQ - 1) / kRouteBQ));
+        route_gemm_kernel<<<g, 128, 0, s>>>(rq, static_cast<int>(nq), ix.cen, ix.cn2, nlist, ix.pd,
+                                            ws.b_qn2.as<float>(), ws.b_keys.as<uint64_t>());
+        ++launches;
     }
-    if (ix.pd % kRouteBK != 0) fail(E8QC_EINVAL, "batched route needs the padded dimension to be a multiple of 16");
-    dim3 g((nlist + kRouteBC - 1) / kRouteBC, static_cast<unsigned>((nq + kRouteBQ - 1) / kRouteBQ));
-    route_gemm_kernel<<<g, 128, 0, s>>>(rq, static_cast<int>(nq), ix.cen, ix.cn2, nlist, ix.pd, ws.b_qn2.as<float>(),
-                                        ws.b_keys.as<uint64_t>());
-    ++launches;
-    const size_t sel_smem = static_cast<size_t>(nlist) * 8;
+    const size_t sel_smem = static_cast<size_t>(nlist) * 8;  // d2 words + interval lower bounds
     if (sel_smem > 200 * 1024) fail(E8QC_EINVAL, "batched route supports at most 25600 lists");
     {
         // raised once per device (also keeps the call out of captured sequences)
@@ -848,8 +956,8 @@ int batched_prepare(const DevIndex& ix, Workspace& ws, const float* rq, size_t n
         }
     }
     select_kernel<<<static_cast<unsigned>(nq), 256, sel_smem, s>>>(
-        ws.b_keys.as<uint64_t>(), nlist, np_arr, np_max, np_max, ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(),
-        ws.b_cnt.as<uint32_t>());
+        ws.b_keys.as<uint64_t>(), ws.r_ub.as<uint32_t>(), nlist, np_arr, np_max, np_max, rq, ix.cen, ix.pd,
+        ws.b_qn2.as<float>(), ix.cn2, ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(), ws.b_cnt.as<uint32_t>());
     ++launches;
     return launches + group_pairs(ix, ws, nq, np_arr, np_max, pslots, item_cap, qt, align, s);
 }

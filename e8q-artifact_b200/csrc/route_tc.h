@@ -1,4 +1,4 @@
-// Batch routing on the int8 tensor cores with exact fp64 keys (route_tc.cu).
+// Batch routing keys on the int8 tensor cores (route_tc.cu).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -10,20 +10,20 @@
 
 namespace e8qc {
 
-// Batches from this many queries route through route_tc (below it the fp64
-// route GEMM is as fast).
+// Batches from this many queries compute their routing keys with
+// route_tc_keys (below it the fp64 route GEMM is as fast).
 constexpr size_t kRouteTcMinQueries = 256;
 
-// Whether route_tc serves this index and batch size (at most 4096 lists and a
-// padded dimension of at most 4096).
+// Whether route_tc_keys serves this index and batch size (at most 25600
+// lists, padded dimension at most 4096).
 bool route_tc_applies(const DevIndex& ix, size_t nq);
 
-// Probes of nq rotated queries: probes / pd2 ([nq x np_max], list order) and
-// the per-list pair counts in ws.b_cnt (zeroed by the caller), bit-identical
-// to the fp64 route GEMM + select. Needs ws.b_qn2 (the queries' squared
-// norms), uses ws.b_keys as the (query, list) interval matrix. Returns the
-// kernels launched.
-int route_tc(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, const uint32_t* np_arr, int np_max,
-             cudaStream_t s);
+// The (query, list) key matrix of nq rotated queries in ws.b_keys, equal to
+// the fp64 route GEMM's except where the tensor-core bound cannot settle a
+// key: there the key holds a lower bound of the d2 bits with bit 31 of its low
+// word set and ws.r_ub an upper bound (select_kernel resolves those that
+// matter). Needs ws.b_qn2 (the queries' squared norms). Returns the kernels
+// launched.
+int route_tc_keys(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq, cudaStream_t s);
 
 }  // namespace e8qc

@@ -66,7 +66,7 @@ struct Workspace {
     DevBuf p_q8, p_scale, p_sum, p_rowbase, p_prox, p_a8, p_pscale, p_cand;
     // tensor-core routing: int8 slice planes and per-row scale / norms of the
     // queries and the centroids
-    DevBuf r_qplane, r_cplane, r_qmeta, r_cmeta, r_cand, r_ncand, r_units, r_ckeys;
+    DevBuf r_qplane, r_cplane, r_qmeta, r_cmeta, r_ub;
     // tuning of the grouped paths (chosen by the autotuner): work-queue order
     // (0: longest list first, 1: list id order) and the precision scan's
     // shared-memory ring depth (4, 6 or 8 K-chunk stages)
