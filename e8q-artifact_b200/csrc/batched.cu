@@ -238,7 +238,8 @@ __device__ uint32_t warp_exact_d2(const float* __restrict__ qr, const float* __r
 // nprobe-th smallest upper bound U bounds the true nprobe-th d2; interval
 // lists whose lower bound is at most U get their exact key (the fp64 chain),
 // the rest keep their lower bound (above U, never selected). Then the
-// nprobe-th smallest d2 T (11-bit radix select), and the lists with d2 < T
+// nprobe-th smallest d2 T (U itself when nothing was resolved; 8-bit radix
+// select), and the lists with d2 < T
 // plus the first ones in list order with d2 == T -- the nprobe smallest
 // 64-bit keys -- are written in list order with their d2.
 __global__ void select_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ ub, int nlist,
@@ -273,8 +274,11 @@ __global__ void select_kernel(const uint64_t* __restrict__ keys, const uint32_t*
     }
     if (any) s_any = 1;
     __syncthreads();
+    uint32_t T = 0;
+    bool have_T = false;
     if (s_any) {
         const uint32_t U = block_select32(shi, nlist, want, hist, sm);
+        int resolved = 0;
         const float* qr = rq + static_cast<size_t>(q) * pd;
         // interval lists that could be selected get their exact d2 (one warp
         // each); the others keep their lower bound, above U
@@ -287,6 +291,7 @@ __global__ void select_kernel(const uint64_t* __restrict__ keys, const uint32_t*
                 else shi[c] = slb[c];
             }
             __syncthreads();
+            resolved += s_nres;
             for (int i = warp; i < s_nres; i += nw) {
                 const int c = s_res[i];
                 const uint32_t d = warp_exact_d2(qr, cen, pd, qn2[q], cn2[c], c);
@@ -294,8 +299,14 @@ __global__ void select_kernel(const uint64_t* __restrict__ keys, const uint32_t*
             }
             __syncthreads();
         }
+        // nothing resolved: every interval list now sits above U, which stays
+        // the want-th smallest value
+        if (resolved == 0) {
+            T = U;
+            have_T = true;
+        }
     }
-    const uint32_t T = block_select32(shi, nlist, want, hist, sm);
+    if (!have_T) T = block_select32(shi, nlist, want, hist, sm);
     // lists below T, then ties at T in list order, up to want
     int below = 0;
     for (int c0 = 0; c0 < nlist; c0 += nt) {

@@ -921,12 +921,13 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
 }
 
 // A row-group plane (rows of 8 * pd bytes, seen as 2 * pd u32) as a 2D tensor
-// map whose box is box_rows row groups x 512 bytes (one K-chunk).
-CUtensorMap plane_map(const void* base, size_t row_groups, int pd, uint32_t box_rows) {
+// map whose box is box_rows row groups x box_u32 u32 (512 bytes: one 64-byte
+// K-chunk of each of the 8 rows).
+CUtensorMap plane_map(const void* base, size_t row_groups, int pd, uint32_t box_rows, uint32_t box_u32) {
     CUtensorMap m;
     const cuuint64_t dims[2] = {static_cast<cuuint64_t>(2 * pd), static_cast<cuuint64_t>(row_groups)};
     const cuuint64_t strides[1] = {static_cast<cuuint64_t>(8) * pd};
-    const cuuint32_t box[2] = {128u, box_rows};
+    const cuuint32_t box[2] = {box_u32, box_rows};
     const cuuint32_t estr[2] = {1u, 1u};
     const CUresult r = encode_tiled()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<void*>(base), dims, strides,
                                       box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

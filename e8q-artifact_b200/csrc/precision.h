@@ -31,8 +31,9 @@ int launch_vcodes(const DevIndex& ix, int ntiles, uint4* out, cudaStream_t s);
 // A row-group int8 plane (8-row groups of 16-byte core-matrix rows, K-major:
 // row r, byte k at (r/8)*8*pd + (k/16)*128 + (r%8)*16 + k%16) as a 2D tensor
 // map over row groups (8*pd bytes each, seen as 2*pd u32) whose box is
-// box_rows row groups x 512 bytes (one 64-byte K-chunk of each row).
-CUtensorMap plane_map(const void* base, size_t row_groups, int pd, uint32_t box_rows);
+// box_rows row groups x box_u32 u32 (128 u32: one 64-byte K-chunk of each row;
+// 64 u32: a 32-byte one).
+CUtensorMap plane_map(const void* base, size_t row_groups, int pd, uint32_t box_rows, uint32_t box_u32 = 128);
 
 // Candidates kept per query for exact rescoring at a given k.
 int precision_candidates(int k);

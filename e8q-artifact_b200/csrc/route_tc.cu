@@ -5,14 +5,14 @@
 //
 // 1. Slicing (route_slice_kernel): each row x (a rotated query or centroid)
 //    is scaled by 127 / 2^e, 2^e > max|x| (exact in fp64: a 24-bit by 7-bit
-//    product), and split exactly into six int8 slices,
-//      X = sum_t Q_t 128^-t + rho,  |Q_0| <= 127, |Q_t| <= 64, |rho_i| <= 2^-36,
+//    product), and split exactly into seven int8 slices,
+//      X = sum_t Q_t 128^-t + rho,  |Q_0| <= 127, |Q_t| <= 64, |rho_i| <= 2^-43,
 //    with the row's N = sum_{t>=1} |Q_t| and |X - rho| (rounded up).
 // 2. Keys (route_tc_kernel): tcgen05 kind::i8 products of the slices with
-//    exact int32 accumulation, the 21 with t + u <= 5 summed by weight w =
-//    t + u into six TMEM accumulators. The epilogue forms the dot in fp64 and
-//    a rigorous bound on |dot - (the reference's fp64 dot)|: the dropped
-//    products (all have t, u >= 1, so at most 2^-42 N_q N_c), the residuals
+//    exact int32 accumulation, the 28 with t + u <= 6 summed by weight w =
+//    t + u into seven TMEM accumulators. The epilogue forms the dot in fp64
+//    and a rigorous bound on |dot - (the reference's fp64 dot)|: the dropped
+//    products (all have t, u >= 1, so at most 2^-49 N_q N_c), the residuals
 //    (Cauchy-Schwarz), the fp64 combination, and the reference's own
 //    sequential fp64 rounding (n 2^-53 |q||c|, taken twice). When both ends of
 //    that interval round to the same float F, float(dot) is F and the key is
@@ -39,16 +39,16 @@ namespace e8qc {
 
 namespace {
 
-constexpr int kSl = 6;                                 // int8 slices per row
+constexpr int kSl = 7;                                 // int8 slices per row
 constexpr int kRM = 128;                               // queries per tile (TMEM lanes)
 constexpr int kRN = 64;                                // lists per tile
-constexpr int kRK = 64;                                // K bytes per chunk
-constexpr int kASlab = kRM * kRK;                      // 8 KB: one query slice of one chunk
-constexpr int kBSlab = kRN * kRK;                      // 4 KB: one list slice of one chunk
-constexpr int kRStageBytes = kSl * (kASlab + kBSlab);  // 72 KB
-constexpr int kRStages = 3;
+constexpr int kRK = 32;                                // K bytes per chunk (one MMA)
+constexpr int kASlab = kRM * kRK;                      // 4 KB: one query slice of one chunk
+constexpr int kBSlab = kRN * kRK;                      // 2 KB: one list slice of one chunk
+constexpr int kRStageBytes = kSl * (kASlab + kBSlab);  // 42 KB
+constexpr int kRStages = 5;
 constexpr int kRThreads = 192;
-constexpr uint32_t kRCols = 512;  // 6 accumulators x 64 columns, rounded to a power of two
+constexpr uint32_t kRCols = 512;  // 7 accumulators x 64 columns, rounded to a power of two
 constexpr int kRouteTcMaxLists = 25600;
 constexpr int kRouteTcMaxDim = 4096;
 
@@ -93,7 +93,7 @@ __global__ void route_slice_kernel(const float* __restrict__ src, int n, int row
                 for (int t = 0; t < kSl; ++t) {
                     const double qt = rint(rr);      // |qt| <= 127 (t = 0), <= 64 after
                     rr = (rr - qt) * 128.0;          // exact
-                    xh += qt * ldexp(1.0, -7 * t);  // exact: 42 significant bits at most
+                    xh += qt * ldexp(1.0, -7 * t);  // exact: 49 significant bits at most
                     nt[t] = __fma_rn(qt, qt, nt[t]);
                     w[t][b] |= static_cast<uint32_t>(static_cast<uint8_t>(static_cast<int8_t>(qt))) << (8 * k);
                 }
@@ -124,9 +124,9 @@ __global__ void route_slice_kernel(const float* __restrict__ src, int n, int row
     }
 }
 
-// One 128-query x 64-list tile per CTA. Warp 0 loads the twelve slices of
-// each 64-byte K-chunk by TMA into a kRStages ring, one thread of warp 1
-// issues the 21 kind::i8 MMAs per 32 bytes of K, warps 2-5 read the six
+// One 128-query x 64-list tile per CTA. Warp 0 loads the fourteen slices of
+// each 32-byte K-chunk by TMA into a kRStages ring, one thread of warp 1
+// issues the chunk's 28 kind::i8 MMAs, warps 2-5 read the seven
 // accumulators (thread = query row) and write the keys. Waits are bounded; a
 // timeout sets the error word.
 __global__ void __launch_bounds__(kRThreads, 1) route_tc_kernel(
@@ -182,11 +182,11 @@ __global__ void __launch_bounds__(kRThreads, 1) route_tc_kernel(
             if (lane == 0) {
                 unsigned char* base = rsm + st * kRStageBytes;
                 mbar_arrive_expect_tx(&full[st], kRStageBytes);
-                // 16 (queries) / 8 (lists) row groups x 512 bytes (128 u32 at x = kc * 128) per slice
+                // 16 (queries) / 8 (lists) row groups x 8 * kRK bytes (2 * kRK u32 at x = kc * 2 * kRK)
 #pragma unroll
                 for (int t = 0; t < kSl; ++t) {
-                    tma_load_2d(base + t * kASlab, &map_q, kc * 128, (t * qrows_pad + q0) >> 3, &full[st]);
-                    tma_load_2d(base + kSl * kASlab + t * kBSlab, &map_c, kc * 128, (t * crows_pad + c0) >> 3,
+                    tma_load_2d(base + t * kASlab, &map_q, kc * 2 * kRK, (t * qrows_pad + q0) >> 3, &full[st]);
+                    tma_load_2d(base + kSl * kASlab + t * kBSlab, &map_c, kc * 2 * kRK, (t * crows_pad + c0) >> 3,
                                 &full[st]);
                 }
             }
@@ -241,20 +241,16 @@ __global__ void __launch_bounds__(kRThreads, 1) route_tc_kernel(
         const double n = static_cast<double>(pd), rn = sqrt(n);
         if (mbar_wait_or_abort(&tfull, 0u, &s_abort)) {
             tc::fence_after_sync();
-            for (int cb = 0; cb < kRN; cb += 16) {
-                uint32_t acc[kSl][16];
+            for (int cb = 0; cb < kRN; cb += 8) {
+                uint32_t acc[kSl][8];
 #pragma unroll
                 for (int w = 0; w < kSl; ++w)
-#pragma unroll
-                    for (int jj = 0; jj < 2; ++jj) {
-                        uint32_t(&part)[8] = *reinterpret_cast<uint32_t(*)[8]>(acc[w] + 8 * jj);
-                        tc::tmem_ld8(tmem + ((static_cast<uint32_t>(q4) * 32u) << 16) + w * kRN + cb + 8 * jj, part);
-                    }
+                    tc::tmem_ld8(tmem + ((static_cast<uint32_t>(q4) * 32u) << 16) + w * kRN + cb, acc[w]);
                 tc::tmem_ld_wait();
                 if (q >= nq) continue;
                 unsigned long long* krow = keys + static_cast<size_t>(q) * nlist + c0 + cb;
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
+                for (int j = 0; j < 8; ++j) {
                     const int c = c0 + cb + j;
                     if (c >= nlist) continue;
                     double S = 0.0;
@@ -264,8 +260,8 @@ __global__ void __launch_bounds__(kRThreads, 1) route_tc_kernel(
                     const double sc = static_cast<double>(qm.x) * s_cs[cb + j];
                     const double dot = S * sc;
                     // |sum x y - S| over the scaled rows: dropped products + residuals
-                    const double E = 0x1p-42 * static_cast<double>(qm.y) * s_cN[cb + j] +
-                                     0x1p-36 * rn * (static_cast<double>(qm.z) + s_cX[cb + j]) + n * 0x1p-72;
+                    const double E = 0x1p-49 * static_cast<double>(qm.y) * s_cN[cb + j] +
+                                     0x1p-43 * rn * (static_cast<double>(qm.z) + s_cX[cb + j]) + n * 0x1p-86;
                     const double er =
                         E * sc * (1.0 + 0x1p-40) + fabs(dot) * 0x1p-48 + n * 0x1p-52 * qr * s_cr[cb + j];
                     const float s2 = __fadd_rn(qqf, s_cn2[cb + j]);
@@ -316,8 +312,8 @@ int route_tc_keys(const DevIndex& ix, Workspace& ws, const float* rq, size_t nq,
     route_slice_kernel<<<static_cast<unsigned>(crows / 8), 256, 0, s>>>(ix.cen, nlist, crows, pd,
                                                                          ws.r_cplane.as<int8_t>(),
                                                                          ws.r_cmeta.as<float4>());
-    const CUtensorMap map_q = plane_map(ws.r_qplane.p, static_cast<size_t>(kSl) * qrows / 8, pd, kRM / 8);
-    const CUtensorMap map_c = plane_map(ws.r_cplane.p, static_cast<size_t>(kSl) * crows / 8, pd, kRN / 8);
+    const CUtensorMap map_q = plane_map(ws.r_qplane.p, static_cast<size_t>(kSl) * qrows / 8, pd, kRM / 8, 2 * kRK);
+    const CUtensorMap map_c = plane_map(ws.r_cplane.p, static_cast<size_t>(kSl) * crows / 8, pd, kRN / 8, 2 * kRK);
     int dev = 0;
     E8QC_CUDA(cudaGetDevice(&dev));
     const size_t gsmem = static_cast<size_t>(kRStages) * kRStageBytes;
