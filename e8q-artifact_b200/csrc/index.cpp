@@ -855,8 +855,9 @@ int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, si
         if (!d_dev) { tds.ensure(nq * k * 4); d_d = tds.as<float>(); }
         x->ws.ensure_queries(nq, x->pd);
         float* rq = x->ws.rq.as<float>();
+        uint64_t launches = 0;
         if (stats) E8QC_CUDA(cudaEventRecord(ev[0], s));
-        uint64_t launches = launch_rotate(x->view, qd, static_cast<int>(nq), rq, s);
+        launches += launch_rotate(x->view, qd, static_cast<int>(nq), rq, s);
         if (stats) E8QC_CUDA(cudaEventRecord(ev[1], s));
         if (mode == E8QC_MODE_PLAIN) {
             plain_search(x, rq, nq, k, np, ids_d, d_d, stats, s);

@@ -57,7 +57,8 @@ constexpr int kPM = 128;  // pair rows per MMA tile (M = TMEM lanes)
 constexpr int kPN = 256;  // vectors per MMA tile (N)
 constexpr int kPK = 64;   // dimensions per staged K-chunk (2 MMAs of K = 32)
 constexpr int kOrdCap = 512;  // final kernel: probes per query it orders nearest list first
-constexpr size_t kFinalWideRows = 131072;  // final kernel: 4 warps per query from this many proxy rows
+constexpr size_t kFinalWideRows = 131072;  // select kernel: 4 warps per query from this many proxy rows
+constexpr size_t kFinalWideBatch = 2048;   // ... and for batches below this size (too few queries to fill the GPU)
 
 // Proxy candidates rescored per query, from the query's own k (so a query's
 // result does not depend on the k of the others in its batch).
@@ -987,12 +988,13 @@ int launch_select_fw(const DevIndex& ix, Workspace& ws, size_t nq, const uint32_
 }
 
 // Candidate selection (4 warps per query from kFinalWideRows proxy rows per
-// query, else one) and then the exact rescoring.
+// query or below kFinalWideBatch queries, else one) and then the exact
+// rescoring.
 template <int BITS, bool ME8Q = false>
 int launch_final(const DevIndex& ix, const Me8qView& mv, Workspace& ws, const float* rq, size_t nq,
                  const uint32_t* k_arr, const uint32_t* np_arr, int k_max, int np_max, int out_stride,
                  uint32_t* out_ids, float* out_d, size_t rows_per_query, cudaStream_t s) {
-    int launches = rows_per_query >= kFinalWideRows
+    int launches = (rows_per_query >= kFinalWideRows || nq < kFinalWideBatch)
                        ? launch_select_fw<4>(ix, ws, nq, k_arr, np_arr, k_max, np_max, s)
                        : launch_select_fw<1>(ix, ws, nq, k_arr, np_arr, k_max, np_max, s);
     int dev = 0;

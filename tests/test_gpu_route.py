@@ -68,3 +68,24 @@ def test_tc_route_me8q(e8q):
         sids, sd = split_search(m, q, ks, nps, 16, mode)
         assert np.array_equal(ids, sids), mode
         assert np.array_equal(d.view(np.uint32), sd.view(np.uint32)), mode
+
+
+def test_host_and_device_queries_agree(e8q):
+    """A 4,100-query batch searched from host memory (staged by the library)
+    and from device memory returns the same ids and distances."""
+    import torch
+
+    dim, nlist = 128, 32
+    x, cm, lab = det_mixture(91, 3000, dim, nlist, 0.5)
+    idx = e8q.E8qIndex(dim, 5, 2)
+    idx.build(x, cm, lab)
+    q = det_mixture(92, 4100, dim, nlist, 0.5)[0]
+    qd = torch.from_numpy(q).cuda()
+    for mode in ("batched", "precision"):
+        ids, d = idx.search(q, 10, 8, mode=mode)
+        oi = torch.empty(len(q), 10, dtype=torch.int32, device="cuda")
+        od = torch.empty(len(q), 10, dtype=torch.float32, device="cuda")
+        idx.search_ptr(qd.data_ptr(), len(q), 10, 8, oi.data_ptr(), od.data_ptr(), mode=mode)
+        torch.cuda.synchronize()
+        assert np.array_equal(ids.view(np.int32), oi.cpu().numpy()), mode
+        assert np.array_equal(d.view(np.uint32), od.cpu().numpy().view(np.uint32)), mode
