@@ -111,3 +111,16 @@ def test_precision_small_and_degenerate(e8q, oracle_lib):
     check_exact_distances(orc, q, ids, d)
     one_ids, one_d = idx.search(q[:1], 40, 1, mode="precision")
     assert np.array_equal(one_ids[0], ids[0])
+
+
+def test_precision_batch_size_independent(e8q):
+    """Large batches (one warp per query in the candidate select) and small
+    ones (four warps per query) give bit-identical results."""
+    x, cm, lab = det_mixture(55, 4000, 128, 24, 0.5)
+    idx = e8q.E8qIndex(128, 6, 3)
+    idx.build(x, cm, lab)
+    q = det_mixture(56, 2100, 128, 24, 0.5)[0]
+    ids, d = idx.search(q, 10, 6, mode="precision")
+    parts = [idx.search(q[i:i + 700], 10, 6, mode="precision") for i in range(0, 2100, 700)]
+    assert np.array_equal(ids, np.concatenate([p[0] for p in parts]))
+    assert np.array_equal(d.view(np.uint32), np.concatenate([p[1] for p in parts]).view(np.uint32))
