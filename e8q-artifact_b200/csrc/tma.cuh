@@ -98,18 +98,29 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// Poll `phase` of `bar` (non-blocking tests, a short sleep between tests once
-// the first few fail), giving up after about max_ms of device time, or as soon
+// Potentially blocking test of the phase with parity `phase`: the thread is
+// suspended until the phase completes or a hardware time limit passes (true
+// once it completed).
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t phase) {
+    uint32_t ok = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for `phase` of `bar` (suspending tests, which wake as soon as the
+// phase completes), giving up after about max_ms of device time, or as soon
 // as *abort (when given) is set by another role of the CTA; a timeout sets
 // *abort. Returns false when it gave up.
 __device__ __forceinline__ bool mbar_wait_poll(uint64_t* bar, uint32_t phase, volatile int* abort, uint32_t max_ms) {
-    for (int i = 0; i < 32; ++i)
-        if (mbar_test(bar, phase)) return true;
+    if (mbar_try(bar, phase)) return true;
     const uint64_t t0 = global_ns();
     const uint64_t limit = static_cast<uint64_t>(max_ms) * 1000000ull;
     for (uint32_t i = 0; i < (1u << 30); ++i) {
-        if (mbar_test(bar, phase)) return true;
-        __nanosleep(32);
+        if (mbar_try(bar, phase)) return true;
         if ((i & 15u) == 15u) {
             if (abort && *abort) return false;
             if (global_ns() - t0 > limit) break;
