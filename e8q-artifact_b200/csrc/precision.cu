@@ -775,7 +775,7 @@ __device__ __forceinline__ float rescore_d2(const DevIndex& ix, const uint32_t* 
 // the ME8Q estimator) and the top k by exact distance. Four queries per
 // 4-warp block; the (query, 32-candidate chunk) units of the block are dealt
 // over its warps, then warp w keeps the top k of query w.
-template <int BITS, bool ME8Q>
+template <int BITS, bool ME8Q, int QPB>
 __global__ void __launch_bounds__(128) precision_rescore_kernel(
     DevIndex ix, Me8qView mv, const float* __restrict__ rq, const uint32_t* __restrict__ cand,
     const uint32_t* __restrict__ probes, const float* __restrict__ pd2, int nq, const uint32_t* __restrict__ np_arr,
@@ -789,31 +789,33 @@ __global__ void __launch_bounds__(128) precision_rescore_kernel(
     const int pd = ix.pd;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float* tabrep = fsm;                                        // 2*Q*REP (E8Q)
-    float* myqs = tabrep + (ME8Q ? 0 : 2 * Q * REP);            // 4 rotated queries
-    float* cd = myqs + 4 * pd;                                  // 4 queries x kMaxK exact distances
-    uint32_t* ci = reinterpret_cast<uint32_t*>(cd + 4 * kMaxK);  // 4 queries x kMaxK slots, then ids
-    const int q0 = blockIdx.x * 4;
+    float* myqs = tabrep + (ME8Q ? 0 : 2 * Q * REP);              // QPB rotated queries
+    float* cd = myqs + QPB * pd;                                  // QPB queries x kMaxK exact distances
+    uint32_t* ci = reinterpret_cast<uint32_t*>(cd + QPB * kMaxK);  // QPB queries x kMaxK slots, then ids
+    const int q0 = blockIdx.x * QPB;
     if constexpr (!ME8Q)
         for (int e = tid; e < 2 * Q * REP; e += blockDim.x) tabrep[e] = ix.tab[e / REP];
-    int nunit[4], Cq[4];
+    int nunit[QPB], Cq[QPB];
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
+    for (int t = 0; t < QPB; ++t) {
         const int q = q0 + t;
         Cq[t] = q < nq ? candidates_for(k_arr ? static_cast<int>(k_arr[q]) : k_uniform) : 0;
         nunit[t] = (Cq[t] + 31) / 32;
     }
-    for (int e = tid; e < 4 * pd; e += blockDim.x) {
+    for (int e = tid; e < QPB * pd; e += blockDim.x) {
         const int t = e / pd, i = e - t * pd;
         myqs[e] = q0 + t < nq ? rq[static_cast<size_t>(q0 + t) * pd + i] : 0.0f;
     }
-    for (int e = tid; e < 4 * kMaxK; e += blockDim.x) {
+    for (int e = tid; e < QPB * kMaxK; e += blockDim.x) {
         const int t = e / kMaxK, j = e - t * kMaxK;
         ci[e] = j < Cq[t] ? cand[static_cast<size_t>(q0 + t) * kMaxK + j] : 0xFFFFFFFFu;
     }
     __syncthreads();
     // 3. exact rescoring: unit u = (query t, candidates 32c..32c+31); each lane
     //    writes its candidate's (distance, id) over its slot entry
-    const int total = nunit[0] + nunit[1] + nunit[2] + nunit[3];
+    int total = 0;
+#pragma unroll
+    for (int t = 0; t < QPB; ++t) total += nunit[t];
     for (int u = warp; u < total; u += 4) {
         int t = 0, c = u;
         while (c >= nunit[t]) c -= nunit[t++];
@@ -875,11 +877,14 @@ __global__ void __launch_bounds__(128) precision_rescore_kernel(
         }
     }
     __syncthreads();
-    // 4. top k by exact distance: warp w, query q0 + w
+    // 4. top k by exact distance: warp w < QPB, query q0 + w
     const int q = q0 + warp;
-    if (q < nq) {
+    if (warp < QPB && q < nq) {
         const int kq = k_arr ? static_cast<int>(k_arr[q]) : k_uniform;
-        const int C = Cq[warp];
+        int C = 0;
+#pragma unroll
+        for (int t = 0; t < QPB; ++t)
+            if (t == warp) C = Cq[t];
         const float* qcd = cd + warp * kMaxK;
         const uint32_t* qci = ci + warp * kMaxK;
         WarpTopK top;
@@ -1000,17 +1005,32 @@ int launch_final(const DevIndex& ix, const Me8qView& mv, Workspace& ws, const fl
     int dev = 0;
     E8QC_CUDA(cudaGetDevice(&dev));
     constexpr int REP = table_rep(BITS);
-    const size_t fsmem =
-        ((ME8Q ? 0 : static_cast<size_t>(2) * (1 << BITS) * REP) + static_cast<size_t>(4) * ix.pd + 4 * kMaxK * 2) * 4;
-    static size_t fconfigured[64] = {};
-    if (fsmem > 48 * 1024 && fconfigured[dev & 63] < fsmem) {
-        E8QC_CUDA(cudaFuncSetAttribute(precision_rescore_kernel<BITS, ME8Q>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(fsmem)));
-        fconfigured[dev & 63] = fsmem;
+    // four queries per block when each has one unit of 32 candidates, else one
+    // (its up to four units spread over the block's warps)
+    const bool one = precision_candidates(k_max) > 32;
+    const int qpb = one ? 1 : 4;
+    const size_t fsmem = ((ME8Q ? 0 : static_cast<size_t>(2) * (1 << BITS) * REP) +
+                          static_cast<size_t>(qpb) * ix.pd + static_cast<size_t>(qpb) * kMaxK * 2) *
+                         4;
+    static size_t fconfigured[2][64] = {};
+    if (fsmem > 48 * 1024 && fconfigured[one][dev & 63] < fsmem) {
+        if (one)
+            E8QC_CUDA(cudaFuncSetAttribute(precision_rescore_kernel<BITS, ME8Q, 1>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(fsmem)));
+        else
+            E8QC_CUDA(cudaFuncSetAttribute(precision_rescore_kernel<BITS, ME8Q, 4>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(fsmem)));
+        fconfigured[one][dev & 63] = fsmem;
     }
-    precision_rescore_kernel<BITS, ME8Q><<<static_cast<unsigned>((nq + 3) / 4), 128, fsmem, s>>>(
-        ix, mv, rq, ws.p_cand.as<uint32_t>(), ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(), static_cast<int>(nq),
-        np_arr, np_max, k_arr, k_max, out_stride, out_ids, out_d);
+    const unsigned grid = static_cast<unsigned>((nq + qpb - 1) / qpb);
+    if (one)
+        precision_rescore_kernel<BITS, ME8Q, 1><<<grid, 128, fsmem, s>>>(
+            ix, mv, rq, ws.p_cand.as<uint32_t>(), ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(),
+            static_cast<int>(nq), np_arr, np_max, k_arr, k_max, out_stride, out_ids, out_d);
+    else
+        precision_rescore_kernel<BITS, ME8Q, 4><<<grid, 128, fsmem, s>>>(
+            ix, mv, rq, ws.p_cand.as<uint32_t>(), ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(),
+            static_cast<int>(nq), np_arr, np_max, k_arr, k_max, out_stride, out_ids, out_d);
     E8QC_CUDA(cudaGetLastError());
     return launches + 1;
 }
