@@ -684,7 +684,8 @@ def main():
         f_bytes = prof["final_bytes"] / prof["final_launches"]
         f_t = prof["final_ms"] / prof["final_launches"] / 1000.0
         f_ach = f_bytes / f_t / 1e9 if f_t > 0 else 0.0
-        final = {"kernel": "precision_final_kernel", "achieved": round(f_ach, 1), "frac": round(f_ach / peak, 4),
+        final = {"kernel": "precision_select_kernel + precision_rescore_kernel", "achieved": round(f_ach, 1),
+                 "frac": round(f_ach / peak, 4),
                  "algo_bytes_per_launch": int(f_bytes), "launch_us": round(f_t * 1e6, 2)}
         scan_part = {k2: roofline[k2] for k2 in ("kernel", "achieved", "frac", "algo_bytes_per_launch", "launch_us")}
         if f_t > t_launch:
