@@ -65,6 +65,10 @@ std::vector<uint8_t> rotator_signs(size_t dim, uint64_t seed) {
     return s;
 }
 
+// Grouped-mode searches from this many queries whose shape repeats the
+// previous call's replay a captured graph of that shape.
+constexpr size_t kGraphMinQueries = 1024;
+
 // Input staging: device pointers pass through, host data is copied to a
 // temporary device buffer on the call's stream.
 template <class T>
@@ -114,6 +118,18 @@ struct e8qc_index {
                list_len_d.bytes + codes.bytes + g1.bytes + h3.bytes + ids.bytes + tab.bytes +
                list_of_tile.bytes + list_begin_d.bytes + list_order.bytes + proxy.bytes + vcodes.bytes;
     }
+    // A captured graph of the last repeated batch shape of the grouped modes
+    // (search calls from kGraphMinQueries queries whose mode, size, k and
+    // nprobe equal the previous call's): later calls of that shape replay it.
+    // Declared last, so it is released before the buffers it points into.
+    struct GraphKey {
+        int mode = -1;
+        size_t nq = 0, k = 0, np = 0;
+        bool operator==(const GraphKey& o) const { return mode == o.mode && nq == o.nq && k == o.k && np == o.np; }
+    };
+    std::mutex gmu;
+    GraphKey glast, gkey;
+    std::shared_ptr<e8qc_plan> gplan;
 };
 
 namespace {
@@ -557,6 +573,13 @@ namespace {
 // The device view of an index whose buffers are in place (build, load); a new
 // layout invalidates the precision plane.
 void set_view(e8qc_index* x) {
+    {
+        // a captured graph points into the old view's buffers
+        std::lock_guard<std::mutex> gl(x->gmu);
+        x->gplan.reset();
+        x->glast = e8qc_index::GraphKey{};
+        x->gkey = e8qc_index::GraphKey{};
+    }
     DevIndex& v = x->view;
     v.dim = static_cast<int>(x->dim);
     v.pd = static_cast<int>(x->pd);
@@ -833,10 +856,39 @@ int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, si
             fail(E8QC_EINVAL, "unknown search mode");
         if (nq == 0) return;
         if (!queries || !out_ids) fail(E8QC_EINVAL, "null buffer");
+        // a repeated large batch shape of a grouped mode replays a captured graph
+        std::shared_ptr<e8qc_plan> plan;
+        if (mode != E8QC_MODE_PLAIN && nq >= kGraphMinQueries && !stats && !x->profiling) {
+            const e8qc_index::GraphKey key{mode, nq, k, std::min(nprobe, x->nlist)};
+            bool create = false;
+            {
+                std::lock_guard<std::mutex> gl(x->gmu);
+                if (x->gplan && x->gkey == key) plan = x->gplan;
+                else if (x->glast == key) create = true;
+                else x->glast = key;
+            }
+            if (create) {
+                try {
+                    plan = std::shared_ptr<e8qc_plan>(plan_make(e8q_target(x), mode, nq, k, key.np, false, true),
+                                                      plan_free);
+                    std::lock_guard<std::mutex> gl(x->gmu);
+                    x->gplan = plan;
+                    x->gkey = key;
+                } catch (const Error&) {
+                    plan.reset();  // e.g. no memory for a second workspace: the direct path below
+                }
+            }
+        }
         std::lock_guard<std::mutex> lock(x->mu);
         DeviceGuard g(x->device);
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         const size_t np = std::min(nprobe, x->nlist);
+        if (plan) {
+            const std::vector<uint32_t> kh(nq, static_cast<uint32_t>(k)), nph(nq, static_cast<uint32_t>(np));
+            plan_enqueue(plan.get(), queries, nq, kh.data(), nph.data(), out_ids, out_dists, s);
+            plan_check(plan.get(), s);
+            return;
+        }
         if (stats) std::memset(stats, 0, sizeof(*stats));
         cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
         if (stats)

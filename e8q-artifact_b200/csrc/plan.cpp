@@ -47,6 +47,7 @@ struct e8qc_plan {
         int sched, stages;
     };
     std::vector<Graph> graphs;  // ascending nq
+    uint64_t kernels = 0;       // launched by one run of the largest graph
     ~e8qc_plan() {
         for (auto& g : graphs)
             if (g.exec) cudaGraphExecDestroy(g.exec);
@@ -96,9 +97,22 @@ void plan_check(e8qc_plan* P, cudaStream_t s) { P->ws.check_error(s); }
 
 size_t plan_max_queries(const e8qc_plan* P) { return P->max_q; }
 
+uint64_t plan_kernels(const e8qc_plan* P) { return P->kernels; }
+
+void plan_free(e8qc_plan* P) {
+    if (!P) return;
+    int prev = 0;
+    const bool have_prev = cudaGetDevice(&prev) == cudaSuccess;
+    cudaSetDevice(P->device);
+    cudaStreamSynchronize(P->cs);
+    cudaEventSynchronize(P->staged);
+    delete P;
+    if (have_prev) cudaSetDevice(prev);
+}
+
 // Create a plan (see e8qc_plan_create); throws on failure.
 e8qc_plan* plan_make(std::shared_ptr<SearchTarget> t, int mode, size_t max_q, size_t k_max, size_t np_max,
-                     bool autotune) {
+                     bool autotune, bool exact_size) {
     t->check_mode(mode);
     if (max_q == 0) fail(E8QC_EINVAL, "max_queries must be positive");
     if (k_max == 0 || k_max > static_cast<size_t>(kMaxK)) fail(E8QC_EINVAL, "k_max must be in [1, 128]");
@@ -132,7 +146,8 @@ e8qc_plan* plan_make(std::shared_ptr<SearchTarget> t, int mode, size_t max_q, si
     P->ids.alloc(max_q * k_max * 4);
     P->d.alloc(max_q * k_max * 4);
     std::vector<size_t> sizes;
-    for (size_t n = 64; n < max_q; n <<= 1) sizes.push_back(n);
+    if (!exact_size)
+        for (size_t n = 64; n < max_q; n <<= 1) sizes.push_back(n);
     sizes.push_back(max_q);
     std::sort(sizes.rbegin(), sizes.rend());
     cudaStream_t s = P->cs;
@@ -156,8 +171,10 @@ e8qc_plan* plan_make(std::shared_ptr<SearchTarget> t, int mode, size_t max_q, si
         E8QC_CUDA(cudaMemcpyAsync(P->k.p, P->hk, n * 4, cudaMemcpyHostToDevice, s));
         E8QC_CUDA(cudaMemcpyAsync(P->np.p, P->hnp, n * 4, cudaMemcpyHostToDevice, s));
         auto enqueue = [&] {
-            t->enqueue(P->ws, mode, P->q.as<float>(), n, P->k.as<uint32_t>(), P->np.as<uint32_t>(), k_max, P->np_max,
-                       P->ids.as<uint32_t>(), P->d.as<float>(), s, false);
+            const uint64_t kn = t->enqueue(P->ws, mode, P->q.as<float>(), n, P->k.as<uint32_t>(),
+                                           P->np.as<uint32_t>(), k_max, P->np_max, P->ids.as<uint32_t>(),
+                                           P->d.as<float>(), s, false);
+            if (n == max_q) P->kernels = kn;
         };
         enqueue();  // sizes the workspace, sets kernel attributes
         P->ws.check_error(s);

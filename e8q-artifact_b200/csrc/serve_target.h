@@ -43,8 +43,17 @@ struct SearchTarget {
 std::shared_ptr<SearchTarget> e8q_target(e8qc_index* x);
 std::shared_ptr<SearchTarget> me8q_target(e8qc_me8q* x);
 
-// Captured plan over a target (plan.cpp).
+// Captured plan over a target (plan.cpp): graphs for batch sizes 64, 128, ...
+// up to max_q, or (exact_size) for max_q alone.
 e8qc_plan* plan_make(std::shared_ptr<SearchTarget> t, int mode, size_t max_q, size_t k_max, size_t np_max,
-                     bool autotune);
+                     bool autotune, bool exact_size = false);
+// Enqueue one batch on s (k / nprobe: host arrays of nq entries; queries and
+// outputs host or device), then synchronise and report a kernel timeout.
+void plan_enqueue(e8qc_plan* P, const float* queries, size_t nq, const uint32_t* k, const uint32_t* nprobe,
+                  uint32_t* out_ids, float* out_dists, cudaStream_t s);
+void plan_check(e8qc_plan* P, cudaStream_t s);
+// Kernels one run of the plan's largest graph launches.
+uint64_t plan_kernels(const e8qc_plan* P);
+void plan_free(e8qc_plan* P);
 
 }  // namespace e8qc

@@ -69,3 +69,32 @@ def test_autotune_keeps_results(e8q, index):
     assert same(idx.search(q[:150], 10, 12, mode="batched"), idx.search(q[:150], 10, 12, mode="batched"))
     with pytest.raises(ValueError):
         idx.autotune("plain", 10, 10, 4)
+
+
+def test_search_replays_graph_of_repeated_shape(e8q):
+    """search() calls of a repeated shape (1,024+ queries, grouped modes)
+    replay a captured graph: the results equal the direct path's (a ragged
+    call with the same uniform k / nprobe), for new query contents, and after
+    a rebuild of the index."""
+    from gen import det_mixture
+
+    dim, nlist = 128, 24
+    x, cm, lab = det_mixture(61, 3000, dim, nlist, 0.5)
+    idx = e8q.E8qIndex(dim, 5, 1)
+    idx.build(x, cm, lab)
+    n = 1100
+    ks = np.full(n, 10, np.uint32)
+    nps = np.full(n, 6, np.uint32)
+    for mode in ("precision", "batched"):
+        for seed in (62, 63, 64, 65):  # direct, capture, replay, replay
+            q = det_mixture(seed, n, dim, nlist, 0.5)[0]
+            ids, d = idx.search(q, 10, 6, mode=mode)
+            rids, rd = idx.search_ragged(q, ks, nps, 10, mode=mode)
+            assert np.array_equal(ids, rids) and np.array_equal(d.view(np.uint32), rd.view(np.uint32)), (mode, seed)
+    x2, cm2, lab2 = det_mixture(66, 3000, dim, nlist, 0.5)
+    idx.build(x2, cm2, lab2)
+    for seed in (67, 68, 69):
+        q = det_mixture(seed, n, dim, nlist, 0.5)[0]
+        ids, d = idx.search(q, 10, 6, mode="batched")
+        rids, rd = idx.search_ragged(q, ks, nps, 10, mode="batched")
+        assert np.array_equal(ids, rids) and np.array_equal(d.view(np.uint32), rd.view(np.uint32)), seed
