@@ -858,7 +858,7 @@ int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, si
         if (!queries || !out_ids) fail(E8QC_EINVAL, "null buffer");
         // a repeated large batch shape of a grouped mode replays a captured graph
         std::shared_ptr<e8qc_plan> plan;
-        if (mode != E8QC_MODE_PLAIN && nq >= kGraphMinQueries && !stats && !x->profiling) {
+        if (mode != E8QC_MODE_PLAIN && nq >= kGraphMinQueries && !x->profiling) {
             const e8qc_index::GraphKey key{mode, nq, k, std::min(nprobe, x->nlist)};
             bool create = false;
             {
@@ -885,8 +885,24 @@ int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, si
         const size_t np = std::min(nprobe, x->nlist);
         if (plan) {
             const std::vector<uint32_t> kh(nq, static_cast<uint32_t>(k)), nph(nq, static_cast<uint32_t>(np));
+            cudaEvent_t ge[2] = {nullptr, nullptr};
+            if (stats) {
+                std::memset(stats, 0, sizeof(*stats));
+                for (auto& e : ge) E8QC_CUDA(cudaEventCreate(&e));
+                E8QC_CUDA(cudaEventRecord(ge[0], s));
+            }
             plan_enqueue(plan.get(), queries, nq, kh.data(), nph.data(), out_ids, out_dists, s);
+            if (stats) E8QC_CUDA(cudaEventRecord(ge[1], s));
             plan_check(plan.get(), s);
+            if (stats) {
+                // a replayed graph reports its whole device time (with the
+                // staging copies) as scan_us
+                float t = 0;
+                E8QC_CUDA(cudaEventElapsedTime(&t, ge[0], ge[1]));
+                stats->scan_us = t * 1000.0;
+                stats->launches = plan_kernels(plan.get());
+                for (auto& e : ge) cudaEventDestroy(e);
+            }
             return;
         }
         if (stats) std::memset(stats, 0, sizeof(*stats));
