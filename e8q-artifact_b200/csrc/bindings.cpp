@@ -293,6 +293,13 @@ class E8qIndex {
         return idx_;
     }
 
+    // E8qIndex.save (e8q_bindings.cpp:258-263): a file the reference's load reads.
+    void save(const std::string& path) const {
+        require("save");
+        py::gil_scoped_release nogil;
+        check(e8qc_e8q_save(idx_, path.c_str()));
+    }
+
     // E8qIndex.load (e8q_bindings.cpp:258-268): a reference-written index file.
     static std::unique_ptr<E8qIndex> load(const std::string& path, int device) {
         e8qc_index* h = nullptr;
@@ -846,6 +853,7 @@ PYBIND11_MODULE(_e8qlib, m) {
              py::arg("nprobe"), py::arg("k_max"), py::arg("mode") = "batched")
         .def("estimate", &E8qIndex::estimate, py::arg("query"), py::arg("id"))
         .def_static("load", &E8qIndex::load, py::arg("path"), py::arg("device") = 0)
+        .def("save", &E8qIndex::save, py::arg("path"))
         .def("autotune", &E8qIndex::autotune, py::arg("mode"), py::arg("nq"), py::arg("k"), py::arg("nprobe"))
         .def("set_disable_prune", &E8qIndex::set_disable_prune, py::arg("on"))
         .def("set_prune_alpha", &E8qIndex::set_prune_alpha, py::arg("alpha"))

@@ -305,19 +305,29 @@ __global__ void __launch_bounds__(kBuildThreads) build_encode_kernel(
     if (tid < rb) {
         const int r = tid;
         const size_t slot = static_cast<size_t>(tile) * 32 + lane0 + r;
-        float g1f = 0.0f, h3f = 0.0f;
+        float g1f = 0.0f, h3f = 0.0f, obf = 0.0f, owf = 0.0f, opf = 0.0f;
         const double rn2 = rn2s[r];
         const double rn = sqrt(rn2);
         if (rows[r] != 0xFFFFFFFFu && !(rn < 1e-20)) {
             double dot_ue = 0.0, n2_e = 0.0, dot_ce = 0.0;
+            // scan-basis projections (e8q_build.cpp:338-377): w is the class
+            // mean of each digit's top bit, none for dim 7 at b = 1
+            double dot_ew = 0.0, dot_uw = 0.0, n2_w = 0.0, dot_cw = 0.0;
             for (int blk = 0; blk < B; ++blk) {
                 const double* lv = et.levels[brs[r * B + blk]];
                 for (int kk = 0; kk < 8; ++kk) {
                     const int idx = blk * 8 + kk;
-                    const double ve = lv[dig[(r * B + blk) * 8 + kk]] * a.inv_level_scale;
-                    dot_ue = __fma_rn(static_cast<double>(X[r * ld + idx]), ve, dot_ue);
-                    dot_ce = __fma_rn(static_cast<double>(C[idx]), ve, dot_ce);
+                    const int digit = dig[(r * B + blk) * 8 + kk];
+                    const double ve = lv[digit] * a.inv_level_scale;
+                    const double wc = (bits == 1 && kk == 7) ? 0.0 : a.w_cls[digit >> (bits - 1)];
+                    const double u = static_cast<double>(X[r * ld + idx]), cc = static_cast<double>(C[idx]);
+                    dot_ue = __fma_rn(u, ve, dot_ue);
+                    dot_ce = __fma_rn(cc, ve, dot_ce);
                     n2_e = __fma_rn(ve, ve, n2_e);
+                    dot_ew = __fma_rn(ve, wc, dot_ew);
+                    dot_uw = __fma_rn(u, wc, dot_uw);
+                    n2_w = __fma_rn(wc, wc, n2_w);
+                    dot_cw = __fma_rn(cc, wc, dot_cw);
                 }
             }
             if (n2_e > 1e-30 && dot_ue > 1e-12) {
@@ -326,9 +336,37 @@ __global__ void __launch_bounds__(kBuildThreads) build_encode_kernel(
                 g1f = static_cast<float>(g1);
                 h3f = static_cast<float>(h3);
             }
+            // orthogonal-projection bank inputs (e8q_build.cpp:414-445), with
+            // the reference build's fused multiply-adds spelled out
+            const double g1v = static_cast<double>(g1f);
+            const double sqrt_dm1 = sqrt(static_cast<double>(ix.dim > 1 ? ix.dim - 1 : 1));
+            const double n2_w_safe = n2_w < 1e-30 ? 1e-30 : n2_w;
+            const double uw_eps = 1e-12 * sqrt(n2_w_safe);
+            double w_use, perp_use;
+            if (fabs(dot_uw) > uw_eps) {
+                const double wx = 2.0 * rn / dot_uw;
+                const double a1 = 4.0 * g1v * g1v, b1 = wx * wx, c1 = 4.0 * g1v * wx;
+                const double rx2 = __fma_rn(-c1, dot_ew, __fma_rn(a1, n2_e, b1 * n2_w));
+                w_use = wx;
+                perp_use = sqrt(0.0 < rx2 ? rx2 : 0.0) / sqrt_dm1;
+            } else {
+                const double gamma = dot_ew / n2_w_safe;
+                const double t = __fma_rn(-(gamma * gamma), n2_w, n2_e);
+                const double vp2 = t < 0.0 ? 0.0 : t;
+                w_use = 2.0 * g1v * gamma;
+                perp_use = 2.0 * g1v * sqrt(vp2) / sqrt_dm1;
+            }
+            owf = static_cast<float>(w_use);
+            obf = static_cast<float>(__fma_rn(w_use, dot_cw, rn2));
+            opf = static_cast<float>(perp_use);
         }
         g1o[slot] = g1f;
         h3o[slot] = h3f;
+        if (a.ortho) {
+            a.ortho[slot * 3 + 0] = obf;
+            a.ortho[slot * 3 + 1] = owf;
+            a.ortho[slot * 3 + 2] = opf;
+        }
     }
     // write the tile's chunks: chunk c of lane l at [tile][c][l]
     for (int e = tid; e < rb * nch; e += nt) {

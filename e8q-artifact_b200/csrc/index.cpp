@@ -103,6 +103,8 @@ struct e8qc_index {
 
     DevBuf signs, mean_rot, cen, cn2, tile_begin_d, list_len_d, codes, g1, h3, ids, tab,
         list_of_tile, list_begin_d, list_order;
+    DevBuf ortho;   // built indexes: per slot the scan-bank inputs (base, weight, perp), for saving
+    std::vector<uint8_t> banks;  // loaded indexes: the file's 128-byte scan-bank headers, for saving
     DevBuf proxy;   // int8 proxy plane of the precision mode, built on its first search
     DevBuf vcodes;  // the codes slot-major, for the precision mode's rescoring (built with the plane)
     // autotuned (schedule, stages) per (mode, log2 batch size, log2 nprobe)
@@ -116,7 +118,8 @@ struct e8qc_index {
     size_t memory_bytes() const {
         return signs.bytes + mean_rot.bytes + cen.bytes + cn2.bytes + tile_begin_d.bytes +
                list_len_d.bytes + codes.bytes + g1.bytes + h3.bytes + ids.bytes + tab.bytes +
-               list_of_tile.bytes + list_begin_d.bytes + list_order.bytes + proxy.bytes + vcodes.bytes;
+               list_of_tile.bytes + list_begin_d.bytes + list_order.bytes + proxy.bytes + vcodes.bytes +
+               ortho.bytes + banks.size();
     }
     // A captured graph of the last repeated batch shape of the grouped modes
     // (search calls from kGraphMinQueries queries whose mode, size, k and
@@ -647,6 +650,22 @@ void install_lists(e8qc_index* x, const std::vector<uint64_t>& counts, cudaStrea
 
 size_t sign_bytes(size_t dim) { return rotator_signs(dim, 0).size(); }
 
+// Branch-averaged level mean of each top-bit class (ScanClassMeans,
+// src/quantization/e8q_codec.cpp:511-524): the basis the reference's scan
+// banks price each digit at.
+void scan_class_means(int bits, double w_cls[2]) {
+    const std::vector<double> l0 = branch_levels(bits, 0), l1 = branch_levels(bits, 1);
+    const int cvals = 1 << (bits - 1);
+    for (int t2 = 0; t2 < 2; ++t2) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int lo = 0; lo < cvals; ++lo) {
+            s0 += l0[static_cast<size_t>((t2 << (bits - 1)) | lo)];
+            s1 += l1[static_cast<size_t>((t2 << (bits - 1)) | lo)];
+        }
+        w_cls[t2] = 0.5 * (s0 / cvals + s1 / cvals);
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -685,6 +704,7 @@ int e8qc_e8q_load(int device, const char* path, e8qc_index** out) {
         x->g1.upload(p.g1.data(), p.g1.size() * 4, s);
         x->h3.upload(p.h3.data(), p.h3.size() * 4, s);
         x->ids.upload(p.slot_ids.data(), p.slot_ids.size() * 4, s);
+        x->banks = std::move(p.banks);
         set_view(x.get());
         E8QC_CUDA(cudaStreamSynchronize(s));
         x->built = true;
@@ -821,6 +841,8 @@ int e8qc_e8q_build(e8qc_index* x, const float* data, size_t n, const float* cent
         x->codes.alloc(x->ntiles * static_cast<size_t>(x->nch) * 32 * 16);
         x->g1.alloc(x->ntiles * 32 * sizeof(float));
         x->h3.alloc(x->ntiles * 32 * sizeof(float));
+        x->ortho.alloc(x->ntiles * 32 * 3 * sizeof(float));
+        x->banks.clear();
         E8QC_CUDA(cudaMemsetAsync(x->codes.p, 0, x->codes.bytes, s));
         // mean -> rotated mean -> centroids
         launch_mean(data_d, n, static_cast<int>(dim), mu.as<float>(), s);
@@ -839,6 +861,8 @@ int e8qc_e8q_build(e8qc_index* x, const float* data, size_t n, const float* cent
         a.ntiles = static_cast<int>(x->ntiles);
         a.srd = fixed_scale(x->bits) * std::sqrt(static_cast<double>(pd));
         a.inv_level_scale = 1.0 / std::sqrt(static_cast<double>(pd));
+        scan_class_means(x->bits, a.w_cls);
+        a.ortho = x->ortho.as<float>();
         launch_build_encode(v, et, a, static_cast<uint4*>(x->codes.p), x->g1.as<float>(), x->h3.as<float>(), s);
         E8QC_CUDA(cudaStreamSynchronize(s));
         x->built = true;
@@ -1107,6 +1131,75 @@ int e8qc_e8q_get_ids(const e8qc_index* x, uint32_t* out) {
         require_built(x, "get_ids");
         if (!out) fail(E8QC_EINVAL, "null output");
         std::memcpy(out, x->ids_compact.data(), x->n * 4);
+    });
+}
+
+int e8qc_e8q_save(const e8qc_index* xc, const char* path) {
+    return guarded([&] {
+        require_built(xc, "save");
+        if (path == nullptr) fail(E8QC_EINVAL, "null path");
+        e8qc_index* x = const_cast<e8qc_index*>(xc);
+        std::lock_guard<std::mutex> lock(x->mu);
+        DeviceGuard g(x->device);
+        cudaStream_t s = nullptr;
+        const size_t n = x->n, B = static_cast<size_t>(x->B), pd = x->pd, nlist = x->nlist;
+        if (x->ortho.bytes == 0 && x->banks.empty()) fail(E8QC_ESTATE, "index holds no scan banks to save");
+        // codes in compact order, then the per-slot arrays mapped to it
+        std::vector<uint16_t> digits(n * B * 8);
+        std::vector<uint8_t> branch(n * B);
+        {
+            DevBuf dd, bd;
+            dd.alloc(std::max<size_t>(1, n * B * 8 * 2));
+            bd.alloc(std::max<size_t>(1, n * B));
+            launch_decode(x->view, static_cast<int>(x->ntiles), x->list_of_tile.as<uint32_t>(),
+                          x->list_begin_d.as<uint64_t>(), dd.as<uint16_t>(), bd.as<uint8_t>(), s);
+            E8QC_CUDA(cudaStreamSynchronize(s));
+            if (n) {
+                E8QC_CUDA(cudaMemcpy(digits.data(), dd.p, n * B * 8 * 2, cudaMemcpyDeviceToHost));
+                E8QC_CUDA(cudaMemcpy(branch.data(), bd.p, n * B, cudaMemcpyDeviceToHost));
+            }
+        }
+        const size_t slots = x->ntiles * 32;
+        std::vector<float> g1s(slots), h3s(slots), os(x->ortho.bytes ? slots * 3 : 0);
+        E8QC_CUDA(cudaMemcpy(g1s.data(), x->g1.p, slots * 4, cudaMemcpyDeviceToHost));
+        E8QC_CUDA(cudaMemcpy(h3s.data(), x->h3.p, slots * 4, cudaMemcpyDeviceToHost));
+        if (!os.empty()) E8QC_CUDA(cudaMemcpy(os.data(), x->ortho.p, slots * 12, cudaMemcpyDeviceToHost));
+        std::vector<float> g1(n), h3(n), ortho(os.empty() ? 0 : n * 3);
+        for (size_t c = 0; c < nlist; ++c)
+            for (uint64_t p = x->list_begin[c]; p < x->list_begin[c + 1]; ++p) {
+                const size_t slot = static_cast<size_t>(x->tile_begin[c]) * 32 + (p - x->list_begin[c]);
+                g1[p] = g1s[slot];
+                h3[p] = h3s[slot];
+                if (!os.empty())
+                    for (int t = 0; t < 3; ++t) ortho[p * 3 + t] = os[slot * 3 + t];
+            }
+        std::vector<uint8_t> signs(sign_bytes(x->dim));
+        std::vector<float> mean_rot(pd), cen(nlist * pd), cn2(nlist);
+        E8QC_CUDA(cudaMemcpy(signs.data(), x->signs.p, signs.size(), cudaMemcpyDeviceToHost));
+        E8QC_CUDA(cudaMemcpy(mean_rot.data(), x->mean_rot.p, pd * 4, cudaMemcpyDeviceToHost));
+        E8QC_CUDA(cudaMemcpy(cen.data(), x->cen.p, nlist * pd * 4, cudaMemcpyDeviceToHost));
+        E8QC_CUDA(cudaMemcpy(cn2.data(), x->cn2.p, nlist * 4, cudaMemcpyDeviceToHost));
+        E8axSave w;
+        w.n = n;
+        w.dim = x->dim;
+        w.nlist = nlist;
+        w.pd = pd;
+        w.bits = x->bits;
+        w.prune_alpha = x->prune_alpha > 0.0f ? x->prune_alpha : 1.0f;
+        w.signs = signs.data();
+        w.sign_bytes = signs.size();
+        w.mean_rot = mean_rot.data();
+        w.cen_rot = cen.data();
+        w.cn2 = cn2.data();
+        w.list_begin = x->list_begin.data();
+        w.ids = x->ids_compact.data();
+        w.digits = digits.data();
+        w.branch = branch.data();
+        w.g1 = g1.data();
+        w.h3 = h3.data();
+        w.ortho = ortho.empty() ? nullptr : ortho.data();
+        w.banks = ortho.empty() ? x->banks.data() : nullptr;
+        write_e8ax(path, w);
     });
 }
 

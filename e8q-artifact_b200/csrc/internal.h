@@ -151,6 +151,8 @@ struct BuildEncodeArgs {
     int ntiles;
     double srd;              // FixedScale(bits) * sqrt(pd)
     double inv_level_scale;  // 1/sqrt(pd)
+    double w_cls[2];         // branch-averaged level mean of each top-bit class (the scan basis)
+    float* ortho;            // ntiles*32*3: per slot the scan-bank inputs (base, weight, perp), or NULL
 };
 int launch_build_encode(const DevIndex& ix, const DevEncTables& et, const BuildEncodeArgs& a,
                         uint4* codes, float* g1, float* h3, cudaStream_t s);

@@ -25,7 +25,32 @@ struct E8axParts {
     std::vector<uint32_t> slot_ids;      // ntiles * 32 (UINT32_MAX on padding)
     std::vector<float> g1, h3;           // ntiles * 32
     std::vector<uint4> codes;            // ntiles * nch * 32: chunk c of lane l at [tile][c][l]
+    std::vector<uint8_t> banks;          // the 128-byte scan-bank header of every 32-vector batch, file order
 };
+
+// Everything an E8AX file holds, in compact (cluster-major) vector order.
+struct E8axSave {
+    size_t n = 0, dim = 0, nlist = 0, pd = 0;
+    int bits = 0;
+    float prune_alpha = 1.0f;        // written to the build-options trailer
+    const uint8_t* signs = nullptr;  // rotator sign bytes
+    size_t sign_bytes = 0;
+    const float* mean_rot = nullptr;     // pd
+    const float* cen_rot = nullptr;      // nlist x pd
+    const float* cn2 = nullptr;          // nlist
+    const uint64_t* list_begin = nullptr;  // nlist + 1
+    const uint32_t* ids = nullptr;       // n global ids
+    const uint16_t* digits = nullptr;    // n x B x 8
+    const uint8_t* branch = nullptr;     // n x B
+    const float* g1 = nullptr;           // n
+    const float* h3 = nullptr;           // n
+    const float* ortho = nullptr;        // n x 3 (bank inputs base, weight, perp), or NULL when
+    const uint8_t* banks = nullptr;      // ... the headers are given as they were read
+};
+
+// Write an E8AX file the reference's E8qIndex::Load reads (E8qIndex::Save,
+// src/index/e8q_io.cpp:35-84). Throws Error(E8QC_EIO) on a write failure.
+void write_e8ax(const char* path, const E8axSave& w);
 
 // Throws Error(E8QC_EIO) for an unreadable, foreign or inconsistent file.
 // sign_bytes_for_dim: the rotator's sign-byte count for a dimension.

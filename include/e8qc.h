@@ -189,6 +189,10 @@ int e8qc_tc_i8_gemm(int device, const int8_t* A, const int8_t* B, int n, int k, 
  * re-encoded); the file's pruning headers are not needed by the device scans.
  * E8QC_EIO for an unreadable, foreign, truncated or inconsistent file. */
 int e8qc_e8q_load(int device, const char* path, e8qc_index** out);
+/* Save as an E8AX file the reference's E8qIndex::Load reads (E8qIndex::Save,
+   src/index/e8q_io.cpp:35-84): a built index writes the scan banks from its
+   build, a loaded one the banks it read. */
+int e8qc_e8q_save(const e8qc_index* idx, const char* path);
 /* Copy the global ids, cluster-major (n entries), to a host buffer. */
 int e8qc_e8q_get_ids(const e8qc_index* idx, uint32_t* out);
 /* Export the per-vector lattice codes (cluster-major, the order of
