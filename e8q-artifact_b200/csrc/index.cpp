@@ -65,8 +65,8 @@ std::vector<uint8_t> rotator_signs(size_t dim, uint64_t seed) {
     return s;
 }
 
-// Grouped-mode searches from this many queries whose shape repeats the
-// previous call's replay a captured graph of that shape.
+// Grouped-mode searches of host-resident queries from this many queries whose
+// shape repeats the previous call's replay a captured graph of that shape.
 constexpr size_t kGraphMinQueries = 1024;
 
 // Input staging: device pointers pass through, host data is copied to a
@@ -882,7 +882,9 @@ int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, si
         if (!queries || !out_ids) fail(E8QC_EINVAL, "null buffer");
         // a repeated large batch shape of a grouped mode replays a captured graph
         std::shared_ptr<e8qc_plan> plan;
-        if (mode != E8QC_MODE_PLAIN && nq >= kGraphMinQueries && !x->profiling) {
+        // (host-resident queries only: device-resident ones would add a copy
+        // into the plan's staging, and the direct path keeps the GPU as busy)
+        if (mode != E8QC_MODE_PLAIN && nq >= kGraphMinQueries && !x->profiling && !is_device_ptr(queries)) {
             const e8qc_index::GraphKey key{mode, nq, k, std::min(nprobe, x->nlist)};
             bool create = false;
             {

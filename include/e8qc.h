@@ -70,8 +70,9 @@ typedef struct e8qc_stats {
     double refine_us;
     uint64_t launches;   /* kernels this library launched for the call */
 } e8qc_stats;
-/* A grouped-mode search of 1,024 or more queries whose mode, size, k and
-   nprobe repeat the previous call's replays a captured graph of that shape
+/* A grouped-mode search of 1,024 or more host-resident queries whose mode,
+   size, k and nprobe repeat the previous call's replays a captured graph of
+   that shape
    (the index then holds a second workspace for it, released when the shape
    changes or the index is rebuilt); its stats carry the graph's kernel count
    and its whole device time, staging copies included, as scan_us. */
