@@ -381,7 +381,6 @@ __global__ void items_kernel(const uint32_t* __restrict__ list_cnt, const uint32
                              int nlist, uint32_t* __restrict__ pair_off, uint32_t* __restrict__ fill,
                              uint4* __restrict__ items, uint32_t* __restrict__ n_items, int item_cap, uint32_t qt,
                              uint32_t align) {
-    __shared__ int sm32[32];
     __shared__ uint32_t s_pairs, s_items;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     if (tid == 0) {
@@ -443,7 +442,6 @@ __global__ void items_kernel(const uint32_t* __restrict__ list_cnt, const uint32
         }
         __syncthreads();
     }
-    (void)sm32;
     if (tid == 0) *n_items = min(s_items, static_cast<uint32_t>(item_cap));
 }
 

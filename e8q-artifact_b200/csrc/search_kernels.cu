@@ -13,8 +13,6 @@ namespace e8qc {
 
 namespace {
 
-__device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
-
 // Block-wide exclusive scan of one int per thread (blockDim <= 1024).
 __device__ int block_exclusive_scan(int v, int* total, int* sm32) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
