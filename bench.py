@@ -183,8 +183,10 @@ class Clocks:
     def __init__(self, dev):
         self.dev = dev
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out"))
-                                 else ".", f".clocks_{os.getpid()}_{dev}.csv")
+        import tempfile
+
+        fd, self.path = tempfile.mkstemp(prefix=f"e8q_clocks_{dev}_", suffix=".csv")
+        os.close(fd)
 
     def __enter__(self):
         try:

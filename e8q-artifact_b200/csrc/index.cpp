@@ -54,6 +54,21 @@ bool is_device_ptr(const void* p) {
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// Device memory of `device` itself (or managed memory, reachable from every
+// device): a buffer on another GPU would be dereferenced through a peer
+// mapping that may not exist.
+bool is_device_ptr_on(const void* p, int device) {
+    if (p == nullptr) return false;
+    cudaPointerAttributes a{};
+    const cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == device;
+}
+
 std::vector<uint8_t> rotator_signs(size_t dim, uint64_t seed) {
     // FhtKac4Rotator(dim, seed) (src/utils/rotator.cpp:13-28): one byte per
     // draw of mt19937_64; a uniform [0, 255] draw from a full 64-bit engine
@@ -485,14 +500,20 @@ std::shared_ptr<SearchTarget> e8q_target(e8qc_index* x) { return std::make_share
 
 // Read-only view of a built index for the no-allocation plain search
 // (noalloc.cu). Throws like every entry point when the index is not built.
-void plain_context(e8qc_index* x, size_t nprobe, DevIndex* view, int* device, size_t* nlist, size_t* dim,
-                   size_t* max_tiles) {
+// The returned lock holds the index mutex: the caller keeps it until its
+// kernels have finished, so a concurrent build or load cannot free or replace
+// the buffers the view points at.
+std::unique_lock<std::mutex> plain_context(e8qc_index* x, size_t nprobe, DevIndex* view, int* device,
+                                           size_t* nlist, size_t* dim, size_t* max_tiles) {
+    if (x == nullptr) fail(E8QC_EINVAL, "null index");
+    std::unique_lock<std::mutex> lock(x->mu);
     require_built(x, "search");
     *view = x->view;
     *device = x->device;
     *nlist = x->nlist;
     *dim = x->dim;
     *max_tiles = max_tiles_for(x, nprobe);
+    return lock;
 }
 }  // namespace e8qc
 
@@ -906,6 +927,13 @@ int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, si
             }
         }
         std::lock_guard<std::mutex> lock(x->mu);
+        if (plan) {
+            // a build or load between the lookup above and taking the index
+            // mutex resets the cached plan (its graph points at freed
+            // buffers): replay only the plan that is still current
+            std::lock_guard<std::mutex> gl(x->gmu);
+            if (x->gplan != plan) plan.reset();
+        }
         DeviceGuard g(x->device);
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         const size_t np = std::min(nprobe, x->nlist);

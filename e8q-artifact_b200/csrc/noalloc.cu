@@ -19,8 +19,10 @@
 // before any stream capture. Every call reuses the same array and it keeps
 // the last call's contents: the counters the kernels rely on are cleared at
 // the start of each call, and calls whose GPU work overlaps (two host
-// threads, or two streams) race on the array and must be serialised by the
-// caller.
+// threads with different indexes, or two streams) race on the array and must
+// be serialised by the caller. A call holds its index's mutex until its
+// kernels have finished (it waits for its stream before returning), so a
+// build or load of the same index cannot replace the buffers it reads.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -33,9 +35,9 @@
 namespace e8qc {
 
 // Index internals the entry point needs (index.cpp).
-void plain_context(e8qc_index* x, size_t nprobe, DevIndex* view, int* device, size_t* nlist, size_t* dim,
-                   size_t* max_tiles);
-bool is_device_ptr(const void* p);
+std::unique_lock<std::mutex> plain_context(e8qc_index* x, size_t nprobe, DevIndex* view, int* device,
+                                           size_t* nlist, size_t* dim, size_t* max_tiles);
+bool is_device_ptr_on(const void* p, int device);
 void set_last_error(const std::string& s);
 
 namespace {
@@ -88,7 +90,9 @@ extern "C" int e8qc_e8q_search_plain_noalloc(e8qc_index* idx, const float* queri
         DevIndex view{};
         int device = 0;
         size_t nlist = 0, dim = 0, max_tiles = 0;
-        plain_context(idx, nprobe, &view, &device, &nlist, &dim, &max_tiles);
+        // held until the kernels below have finished
+        const std::unique_lock<std::mutex> index_lock =
+            plain_context(idx, nprobe, &view, &device, &nlist, &dim, &max_tiles);
         if (nq == 0) return E8QC_OK;
         if (nlist > kNaMaxLists)
             fail(E8QC_EINVAL, "no-alloc search supports at most 65536 lists (the scratch array's size)");
@@ -101,8 +105,9 @@ extern "C" int e8qc_e8q_search_plain_noalloc(e8qc_index* idx, const float* queri
             int d;
             ~Restore() { cudaSetDevice(d); }
         } restore{prev};
-        if (!is_device_ptr(queries) || !is_device_ptr(out_ids) || !is_device_ptr(out_dists))
-            fail(E8QC_EINVAL, "no-alloc search needs device pointers for queries, ids and dists");
+        if (!is_device_ptr_on(queries, device) || !is_device_ptr_on(out_ids, device) ||
+            !is_device_ptr_on(out_dists, device))
+            fail(E8QC_EINVAL, "no-alloc search needs device pointers for queries, ids and dists, on the index's device");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
         NaScratch* sc = scratch_for(device);
         const size_t np = nprobe < nlist ? nprobe : nlist;
@@ -122,10 +127,9 @@ extern "C" int e8qc_e8q_search_plain_noalloc(e8qc_index* idx, const float* queri
             launch_scan_plain(view, sc->rq, rw, static_cast<int>(np), static_cast<int>(k), sw, geo, out_ids + i * k,
                               out_dists + i * k, s);
         }
-        uint32_t err = 0;
-        E8QC_CUDA(cudaMemcpyAsync(&err, &sc->words[3], sizeof(err), cudaMemcpyDeviceToHost, s));
+        // results are complete when the call returns (and the index mutex
+        // may be released): wait for the stream
         E8QC_CUDA(cudaStreamSynchronize(s));
-        if (err != 0) fail(E8QC_ETIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
         return E8QC_OK;
     } catch (const Error& e) {
         set_last_error(e.msg);

@@ -169,11 +169,13 @@ int e8qc_e8q_profile(e8qc_index* idx, int enable, e8qc_profile* out);
  * budget. Same kernels and results as e8qc_e8q_search(..., E8QC_MODE_PLAIN),
  * but the scratch is a fixed 2.4 MB static device array per device (held
  * until the process exits) and queries (nq*dim), out_ids and out_dists
- * (nq*k) must be DEVICE pointers. Limits: nlist <= 65536, padded_dim <= 4096;
- * larger indexes return E8QC_EINVAL. The first call on a device resolves the
- * array's address (make it before any stream capture). All calls share the
- * array: calls whose GPU work overlaps race and must be serialised by the
- * caller. Returns after the results are in out_ids / out_dists. */
+ * (nq*k) must be DEVICE pointers on the index's device (else E8QC_EINVAL).
+ * Limits: nlist <= 65536, padded_dim <= 4096; larger indexes return
+ * E8QC_EINVAL. The first call on a device resolves the array's address (make
+ * it before any stream capture). All calls share the array: calls whose GPU
+ * work overlaps race and must be serialised by the caller. The call holds the
+ * index's mutex and waits for `stream` before returning, so the results are
+ * in out_ids / out_dists when it returns. */
 int e8qc_e8q_search_plain_noalloc(e8qc_index* idx, const float* queries, size_t nq, size_t k,
                                   size_t nprobe, uint32_t* out_ids, float* out_dists, void* stream);
 /* INT8 tensor-core self-test / throughput probe (no reference counterpart):
