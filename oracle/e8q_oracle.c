@@ -672,6 +672,10 @@ orc_e8q_index* orc_e8q_build(const float* base, const float* centroids,
     x->branch = (uint8_t*)calloc(n * (size_t)B, 1);
     x->g1 = (float*)calloc(n, sizeof(float));
     x->h3 = (float*)calloc(n, sizeof(float));
+    x->ortho = (float*)calloc(n * 3, sizeof(float));
+    double w_cls[2];
+    orc_scan_class_means(bits, w_cls);
+    const double sqrt_dm1 = sqrt((double)(dim > 1 ? dim - 1 : 1));
     const double s_vec = orc_fixed_scale(bits);
     const double inv_level_scale = 1.0 / sqrt((double)pd);
     const double* lev[2] = {levels_of(bits, 0), levels_of(bits, 1)};
@@ -701,14 +705,23 @@ orc_e8q_index* orc_e8q_build(const float* base, const float* centroids,
             uint16_t* dg = x->digits + pos * (size_t)B * 8;
             uint8_t* br = x->branch + pos * (size_t)B;
             orc_encode(unit, 1, (int)pd, bits, s_vec, dg, br);
+            /* scan-basis projections: w is the branch-averaged class mean of
+             * each digit's top bit, none for dim 7 at b = 1 (:338-377) */
             double dot_ue = 0.0, n2_e = 0.0, dot_ce = 0.0;
+            double dot_ew = 0.0, dot_uw = 0.0, n2_w = 0.0, dot_cw = 0.0;
             for (int blk = 0; blk < B; ++blk) {
                 for (int k = 0; k < 8; ++k) {
-                    const double ve = lev[br[blk]][dg[blk * 8 + k]] * inv_level_scale;
+                    const int digit = dg[blk * 8 + k];
+                    const double ve = lev[br[blk]][digit] * inv_level_scale;
+                    const double wc = (bits == 1 && k == 7) ? 0.0 : w_cls[digit >> (bits - 1)];
                     const size_t idx = (size_t)blk * 8 + (size_t)k;
                     dot_ue = fma((double)unit[idx], ve, dot_ue);
                     dot_ce = fma((double)rc[idx], ve, dot_ce);
                     n2_e = fma(ve, ve, n2_e);
+                    dot_ew = fma(ve, wc, dot_ew);
+                    dot_uw = fma((double)unit[idx], wc, dot_uw);
+                    n2_w = fma(wc, wc, n2_w);
+                    dot_cw = fma((double)rc[idx], wc, dot_cw);
                 }
             }
             double g1 = 0.0, h3 = 0.0;
@@ -718,6 +731,32 @@ orc_e8q_index* orc_e8q_build(const float* base, const float* centroids,
             }
             x->g1[pos] = (float)g1;
             x->h3[pos] = (float)h3;
+            /* zero-parallel-residual bank inputs (:405-445) with the fused
+             * multiply-adds the reference's GCC build forms: rx2 as
+             * fnma(c1, <e,w>, fma(a1, |e|^2, b1*|w|^2)), vp2 and base as one
+             * fma each */
+            {
+                const double g1v = (double)x->g1[pos];
+                const double n2_w_safe = n2_w < 1e-30 ? 1e-30 : n2_w;
+                const double uw_eps = 1e-12 * sqrt(n2_w_safe);
+                double w_use, perp_use;
+                if (fabs(dot_uw) > uw_eps) {
+                    const double wx = 2.0 * rn / dot_uw;
+                    const double a1 = 4.0 * g1v * g1v, b1 = wx * wx, c1 = 4.0 * g1v * wx;
+                    const double rx2 = fma(-c1, dot_ew, fma(a1, n2_e, b1 * n2_w));
+                    w_use = wx;
+                    perp_use = sqrt(0.0 < rx2 ? rx2 : 0.0) / sqrt_dm1;
+                } else {
+                    const double gamma = dot_ew / n2_w_safe;
+                    const double t = fma(-(gamma * gamma), n2_w, n2_e);
+                    const double vp2 = t < 0.0 ? 0.0 : t;
+                    w_use = 2.0 * g1v * gamma;
+                    perp_use = 2.0 * g1v * sqrt(vp2) / sqrt_dm1;
+                }
+                x->ortho[pos * 3 + 0] = (float)fma(w_use, dot_cw, rn2);
+                x->ortho[pos * 3 + 1] = (float)w_use;
+                x->ortho[pos * 3 + 2] = (float)perp_use;
+            }
         }
         free(rot_x);
         free(unit);
@@ -730,7 +769,7 @@ void orc_e8q_free(orc_e8q_index* x) {
     if (!x) return;
     free(x->signs); free(x->mean_rot); free(x->centroid_rot); free(x->cn2);
     free(x->list_begin); free(x->ids); free(x->digits); free(x->branch);
-    free(x->g1); free(x->h3); free(x->tab);
+    free(x->g1); free(x->h3); free(x->tab); free(x->ortho);
     free(x);
 }
 
@@ -901,4 +940,360 @@ void orc_e8q_search(const orc_e8q_index* x, const float* queries, size_t nq, siz
         }
         free(rq); free(probes); free(pd2); free(hd); free(hi);
     }
+}
+
+/* ------------------------------------------------------------------------
+ * Pruned production path: PrepareQuery (src/index/e8q_search.cpp:20-73),
+ * ScanClusterAvx512 (src/simd/e8q_search_avx512.cpp:552-751), CollectLanes
+ * and OrthoBatchHeader (src/index/e8q_scan_common.hpp:86-156),
+ * FlushSurvivors / RefineRowsAvx512 (e8q_search.cpp:182-207,
+ * e8q_search_avx512.cpp:118-347), WriteOrthoBanks (e8q_build.cpp:31-80).
+ * Scalar expressions that the reference's GCC build contracts into fused
+ * multiply-adds are spelled with fmaf(); the vector intrinsics' fmadd /
+ * fnmadd are fmaf() by definition.
+ * ---------------------------------------------------------------------- */
+
+double orc_phi_inv(double p) {
+    if (p <= 0.0) return -8.0;
+    if (p >= 1.0) return 8.0;
+    const double t = p < 1.0 - p ? p : 1.0 - p;
+    double x = sqrt(-2.0 * log(t));
+    if (p < 0.5) x = -x;
+    for (int it = 0; it < 12; ++it) {
+        const double phi = 0.3989422804014327 * exp(-0.5 * x * x);
+        const double Phi = 0.5 * (1.0 + erf(x * 0.7071067811865476));
+        x -= (Phi - p) / phi;
+    }
+    return x;
+}
+
+float orc_ortho_quantile(double alpha, size_t k_eff) {
+    double tail = alpha / (double)(k_eff > 1 ? k_eff : 1);
+    if (tail > 0.49) tail = 0.49;
+    const double z = orc_phi_inv(1.0 - tail);
+    return (float)(z > 1.0 ? z : 1.0);
+}
+
+static int clamp_u8(int v) { return v < 0 ? 0 : (v > 255 ? 255 : v); }
+
+void orc_ortho_header(const float* base, const float* weight, const float* perp, size_t cnt,
+                      uint8_t* hdr) {
+    float bmin = 0.0F, bmax = 0.0F, wmin = 0.0F, wmax = 0.0F, pmin = 0.0F, pmax = 0.0F;
+    if (cnt > 0) {
+        bmin = bmax = base[0];
+        wmin = wmax = weight[0];
+        pmin = pmax = perp[0];
+        for (size_t i = 1; i < cnt; ++i) {
+            if (base[i] < bmin) bmin = base[i];
+            if (base[i] > bmax) bmax = base[i];
+            if (weight[i] < wmin) wmin = weight[i];
+            if (weight[i] > wmax) wmax = weight[i];
+            if (perp[i] < pmin) pmin = perp[i];
+            if (perp[i] > pmax) pmax = perp[i];
+        }
+    }
+    const float wamax = fabsf(wmin) > fabsf(wmax) ? fabsf(wmin) : fabsf(wmax);
+    const float bsc = bmax > bmin ? (bmax - bmin) / 255.0F : 1.0F;
+    const float wsc = wmax > wmin ? (wmax - wmin) / 255.0F : 1.0F;
+    const float psc = pmax > pmin ? (pmax - pmin) / 255.0F : 1.0F;
+    memset(hdr, 0, 128);
+    for (size_t i = 0; i < cnt; ++i) {
+        hdr[i] = (uint8_t)clamp_u8((int)((base[i] - bmin) / bsc));          /* truncation */
+        hdr[32 + i] = (uint8_t)clamp_u8((int)lroundf((weight[i] - wmin) / wsc)); /* nearest */
+        hdr[64 + i] = (uint8_t)clamp_u8((int)ceilf((perp[i] - pmin) / psc));   /* up */
+    }
+    const float sc[7] = {bmin, bsc, wmin, wsc, pmin, psc, wamax};
+    memcpy(hdr + 96, sc, sizeof(sc));
+}
+
+size_t orc_e8q_banks(const orc_e8q_index* x, uint8_t* out) {
+    size_t nb = 0;
+    float ob[32], ow[32], op[32];
+    for (size_t c = 0; c < x->nlist; ++c) {
+        const uint64_t lo = x->list_begin[c], hi = x->list_begin[c + 1];
+        for (uint64_t b0 = lo; b0 < hi; b0 += 32, ++nb) {
+            if (!out) continue;
+            const size_t cnt = (size_t)(hi - b0 < 32 ? hi - b0 : 32);
+            for (size_t i = 0; i < cnt; ++i) {
+                ob[i] = x->ortho[(b0 + i) * 3 + 0];
+                ow[i] = x->ortho[(b0 + i) * 3 + 1];
+                op[i] = x->ortho[(b0 + i) * 3 + 2];
+            }
+            orc_ortho_header(ob, ow, op, cnt, out + nb * 128);
+        }
+    }
+    return nb;
+}
+
+uint8_t orc_e8q_rowa(const orc_e8q_index* x, size_t pos, int blk) {
+    return orc_pack_coarse(x->digits + (pos * (size_t)x->blocks + (size_t)blk) * 8,
+                           x->branch[pos * (size_t)x->blocks + (size_t)blk], x->bits);
+}
+
+void orc_e8q_prepare_lut(int bits, int blocks, const float* rq, uint8_t* lut, float* scal) {
+    /* gate_mid_: InitBitTables, src/index/e8q_io.cpp:213-228 */
+    double w_cls[2], mid[16];
+    orc_scan_class_means(bits, w_cls);
+    for (int d = 0; d < 8; ++d) {
+        mid[2 * d] = (bits == 1 && d == 7) ? 0.0 : w_cls[0];
+        mid[2 * d + 1] = (bits == 1 && d == 7) ? 0.0 : w_cls[1];
+    }
+    float* cf = (float*)malloc(sizeof(float) * (size_t)blocks * 32);
+    float hc = 0.0F;
+    for (int blk = 0; blk < blocks; ++blk) {
+        const float* qb = rq + (size_t)blk * 8;
+        float* A = cf + (size_t)blk * 32; /* prices the low nibble: digits 4..7 */
+        float* Bt = A + 16;               /* the high nibble: digits 0..3 */
+        for (int v = 0; v < 16; ++v) {
+            double av = 0.0, bv = 0.0;
+            for (int h = 0; h < 4; ++h) {
+                const int bit = (v >> (3 - h)) & 1;
+                av = fma((double)qb[4 + h], mid[2 * (4 + h) + bit], av);
+                bv = fma((double)qb[h], mid[2 * h + bit], bv);
+            }
+            A[v] = (float)av;
+            Bt[v] = (float)bv;
+        }
+    }
+    for (size_t i = 0; i < (size_t)blocks * 32; ++i)
+        if (fabsf(cf[i]) > hc) hc = fabsf(cf[i]);
+    const float delta = hc > 0.0F ? 2.0F * hc / 255.0F : 1.0F;
+    const float qinv = 1.0F / delta, qoff = hc / delta;
+    /* QuantizeU8Avx512: cvtps_epi32 (round to nearest even) of
+     * fmadd(x, qinv, qoff), then unsigned saturation to u8 */
+    for (size_t i = 0; i < (size_t)blocks * 32; ++i) {
+        const int v = (int)nearbyintf(fmaf(cf[i], qinv, qoff));
+        const uint32_t u = (uint32_t)v;
+        lut[i] = (uint8_t)(u > 255u ? 255u : u);
+    }
+    free(cf);
+    const float sqrt_blocks = sqrtf((float)blocks);
+    scal[0] = delta;
+    scal[1] = -hc * (float)(2 * blocks);
+    scal[2] = 2.0F * sqrt_blocks * delta; /* LutErrClt */
+    scal[3] = (float)blocks * fmaf(255.0F, delta, 2.0F * hc);
+    (void)bits;
+}
+
+int32_t orc_e8q_coarse(const orc_e8q_index* x, size_t pos, const uint8_t* lut) {
+    int32_t acc = 0;
+    for (int blk = 0; blk < x->blocks; ++blk) {
+        const uint8_t h = pos == (size_t)-1 ? 0 : orc_e8q_rowa(x, pos, blk);
+        acc += lut[blk * 32 + (h & 0xF)] + lut[blk * 32 + 16 + (h >> 4)];
+    }
+    return acc;
+}
+
+float orc_e8q_refine_score(const orc_e8q_index* x, size_t pos, const float* rq) {
+    const uint16_t* dg = x->digits + pos * (size_t)x->blocks * 8;
+    const uint8_t* br = x->branch + pos * (size_t)x->blocks;
+    float acc[8] = {0}, acc2[8] = {0};
+    for (int blk = 0; blk < x->blocks; ++blk) {
+        const float* tab = x->tab + (size_t)br[blk] * (size_t)x->tab_stride;
+        float* dst = (blk & 1) ? acc2 : acc;
+        for (int d = 0; d < 8; ++d) dst[d] = fmaf(tab[dg[blk * 8 + d]], rq[blk * 8 + d], dst[d]);
+    }
+    float t[8], s4[4];
+    for (int d = 0; d < 8; ++d) t[d] = acc[d] + acc2[d];
+    for (int i = 0; i < 4; ++i) s4[i] = t[i] + t[i + 4];
+    const float s2a = s4[0] + s4[2], s2b = s4[1] + s4[3];
+    return s2a + s2b;
+}
+
+typedef struct {
+    size_t pos;
+    float g1, h3; /* h3 = d2 + h3 of the row */
+} orc_row;
+
+typedef struct {
+    float* hd;
+    uint32_t* hi;
+    size_t k, cnt;
+} orc_heap;
+
+/* InsertHeap: src/index/e8q_search.cpp:135-180 */
+static void heap_insert(orc_heap* h, float dist, uint32_t id) {
+    if (h->cnt < h->k) {
+        size_t i = h->cnt++;
+        h->hd[i] = dist;
+        h->hi[i] = id;
+        while (i > 0) {
+            const size_t par = (i - 1) / 2;
+            if (!better(h->hd[par], h->hi[par], h->hd[i], h->hi[i])) break;
+            float td = h->hd[i]; h->hd[i] = h->hd[par]; h->hd[par] = td;
+            uint32_t ti = h->hi[i]; h->hi[i] = h->hi[par]; h->hi[par] = ti;
+            i = par;
+        }
+        return;
+    }
+    if (!better(dist, id, h->hd[0], h->hi[0])) return;
+    h->hd[0] = dist;
+    h->hi[0] = id;
+    size_t i = 0;
+    for (;;) {
+        const size_t l = 2 * i + 1, r = l + 1;
+        size_t lg = i;
+        if (l < h->k && better(h->hd[lg], h->hi[lg], h->hd[l], h->hi[l])) lg = l;
+        if (r < h->k && better(h->hd[lg], h->hi[lg], h->hd[r], h->hi[r])) lg = r;
+        if (lg == i) break;
+        float td = h->hd[i]; h->hd[i] = h->hd[lg]; h->hd[lg] = td;
+        uint32_t ti = h->hi[i]; h->hi[i] = h->hi[lg]; h->hi[lg] = ti;
+        i = lg;
+    }
+}
+
+static float heap_limit(const orc_heap* h) { return h->cnt == h->k ? h->hd[0] : INFINITY; }
+
+static void flush_rows(const orc_e8q_index* x, orc_row* rows, size_t* n, const float* rq,
+                       orc_heap* h) {
+    for (size_t j = 0; j < *n; ++j) {
+        const float s = orc_e8q_refine_score(x, rows[j].pos, rq);
+        heap_insert(h, fmaf(-(2.0F * rows[j].g1), s, rows[j].h3), x->ids[rows[j].pos]);
+    }
+    *n = 0;
+}
+
+void orc_e8q_search_pruned(const orc_e8q_index* x, const uint8_t* banks_in, float alpha,
+                           int disable_prune, const float* queries, size_t nq, size_t k,
+                           size_t nprobe, uint32_t* out_ids, float* out_dists, uint64_t* cand_out,
+                           uint64_t* surv_out, int threads) {
+    const size_t nbatches = orc_e8q_banks(x, NULL);
+    uint8_t* own = NULL;
+    const uint8_t* banks = banks_in;
+    if (!banks) {
+        own = (uint8_t*)malloc(nbatches * 128 + 1);
+        orc_e8q_banks(x, own);
+        banks = own;
+    }
+    /* first batch of each list */
+    size_t* bfirst = (size_t*)malloc(sizeof(size_t) * (x->nlist + 1));
+    bfirst[0] = 0;
+    for (size_t c = 0; c < x->nlist; ++c)
+        bfirst[c + 1] = bfirst[c] + (size_t)((x->list_begin[c + 1] - x->list_begin[c] + 31) / 32);
+    const size_t k_eff = 4 * k > 32 ? 4 * k : 32;
+    const float z = orc_ortho_quantile((double)alpha, k_eff);
+    const int B = x->blocks;
+#pragma omp parallel num_threads(threads > 0 ? threads : 1)
+    {
+        float* rq = (float*)malloc(sizeof(float) * x->padded_dim);
+        uint32_t* probes = (uint32_t*)malloc(sizeof(uint32_t) * x->nlist);
+        float* pd2 = (float*)malloc(sizeof(float) * x->nlist);
+        uint8_t* lut = (uint8_t*)malloc((size_t)B * 32);
+        orc_heap h;
+        h.hd = (float*)malloc(sizeof(float) * (k + 1));
+        h.hi = (uint32_t*)malloc(sizeof(uint32_t) * (k + 1));
+        h.k = k;
+        orc_row rows[32];
+#pragma omp for schedule(dynamic, 1)
+        for (long long qi = 0; qi < (long long)nq; ++qi) {
+            float scal[4];
+            orc_e8q_prepare_query(x, queries + (size_t)qi * x->dim, rq);
+            orc_e8q_prepare_lut(x->bits, B, rq, lut, scal);
+            const float delta_c = scal[0], base_c = scal[1], lut_err = scal[2], score_max = scal[3];
+            const size_t take = nprobe < x->nlist ? nprobe : x->nlist;
+            orc_e8q_route(x, rq, take, probes, pd2);
+            const int32_t pad_acc = orc_e8q_coarse(x, (size_t)-1, lut);
+            h.cnt = 0;
+            size_t nst = 0;
+            uint64_t cand = 0, surv = 0;
+            for (size_t p = 0; p < take; ++p) {
+                const size_t c = probes[p];
+                const float d2 = pd2[p];
+                const uint64_t lo = x->list_begin[c], cnt = x->list_begin[c + 1] - lo;
+                if (cnt == 0) continue;
+                const float sqrt_d2 = sqrtf(d2 > 0.0F ? d2 : 0.0F);
+                for (uint64_t off = 0; off < cnt; off += 32) {
+                    const size_t n_logic = (size_t)(cnt - off < 32 ? cnt - off : 32);
+                    const uint8_t* bp = banks + (bfirst[c] + (size_t)(off / 32)) * 128;
+                    int32_t accC[32];
+                    for (size_t t = 0; t < 32; ++t)
+                        accC[t] = t < n_logic ? orc_e8q_coarse(x, (size_t)(lo + off + t), lut) : pad_acc;
+                    cand += n_logic;
+                    const float distk0 = heap_limit(&h);
+                    const float r_horizon =
+                        (distk0 < d2) ? sqrtf(distk0 > 0.0F ? distk0 : 0.0F) : sqrt_d2;
+                    float sc[7];
+                    memcpy(sc, bp + 96, sizeof(sc));
+                    const float base_min = sc[0], base_scale = sc[1], wmin = sc[2], wscale = sc[3];
+                    const float perp_min = sc[4], perp_scale = sc[5];
+                    const float pad_w_lut = lut_err;
+                    const float pad_w_round = 0.5F * wscale * (score_max + lut_err);
+                    if (!disable_prune && distk0 < INFINITY) {
+                        /* whole-batch skip (:611-635) */
+                        const float w_amax = sc[6];
+                        const float pad_add = fmaf(w_amax, pad_w_lut, pad_w_round);
+                        const float perp_amax = fmaf(255.0F, perp_scale, perp_min);
+                        int32_t mx = accC[0], mn = accC[0];
+                        for (int t = 1; t < 32; ++t) {
+                            if (accC[t] > mx) mx = accC[t];
+                            if (accC[t] < mn) mn = accC[t];
+                        }
+                        const float s_hi = fmaf((float)mx, delta_c, base_c);
+                        const float s_lo = fmaf((float)mn, delta_c, base_c);
+                        const float s_absmax = fabsf(s_hi) > fabsf(s_lo) ? fabsf(s_hi) : fabsf(s_lo);
+                        const float lb = fmaf(-(z * r_horizon), perp_amax,
+                                              fmaf(-w_amax, s_absmax, (d2 + base_min) - pad_add));
+                        if (lb >= distk0) continue;
+                    }
+                    /* per-lane bound (:636-676) */
+                    float dlo[32];
+                    const float bmin_d2 = (base_min + d2) - pad_w_round;
+                    const float slack = z * r_horizon;
+                    for (int t = 0; t < 32; ++t) {
+                        const float scv = fmaf((float)accC[t], delta_c, base_c);
+                        const float base_term = fmaf((float)bp[t], base_scale, bmin_d2);
+                        const float weight = fmaf((float)bp[32 + t], wscale, wmin);
+                        const float perp = fmaf((float)bp[64 + t], perp_scale, perp_min);
+                        const float dc = fmaf(-weight, scv, base_term);
+                        dlo[t] = fmaf(-slack, perp, fmaf(-fabsf(weight), pad_w_lut, dc));
+                    }
+                    uint32_t mask = 0;
+                    if (disable_prune) {
+                        mask = 0xFFFFFFFFu;
+                    } else {
+                        for (int t = 0; t < 32; ++t)
+                            if (dlo[t] < distk0) mask |= 1u << t;
+                    }
+                    if (n_logic < 32) mask &= (1u << n_logic) - 1u;
+                    /* CollectLanes (e8q_scan_common.hpp:86-113) */
+                    while (mask) {
+                        const int lane = __builtin_ctz(mask);
+                        mask &= mask - 1;
+                        if (!disable_prune && !(dlo[lane] < heap_limit(&h))) continue;
+                        if (nst >= 32) flush_rows(x, rows, &nst, rq, &h);
+                        ++surv;
+                        const size_t pos = (size_t)(lo + off) + (size_t)lane;
+                        rows[nst].pos = pos;
+                        rows[nst].g1 = x->g1[pos];
+                        rows[nst].h3 = d2 + x->h3[pos];
+                        ++nst;
+                    }
+                }
+                flush_rows(x, rows, &nst, rq, &h);
+            }
+            flush_rows(x, rows, &nst, rq, &h);
+            /* ExtractTopK: src/index/e8q_search.cpp:295-318 */
+            uint32_t* oid = out_ids + (size_t)qi * k;
+            float* od = out_dists + (size_t)qi * k;
+            for (size_t j = 0; j < k; ++j) {
+                if (j < h.cnt) {
+                    size_t bi = j;
+                    for (size_t t = j + 1; t < h.cnt; ++t)
+                        if (better(h.hd[t], h.hi[t], h.hd[bi], h.hi[bi])) bi = t;
+                    float td = h.hd[j]; h.hd[j] = h.hd[bi]; h.hd[bi] = td;
+                    uint32_t ti = h.hi[j]; h.hi[j] = h.hi[bi]; h.hi[bi] = ti;
+                    oid[j] = h.hi[j];
+                    od[j] = h.hd[j];
+                } else {
+                    oid[j] = 0xFFFFFFFFu;
+                    od[j] = INFINITY;
+                }
+            }
+            if (cand_out) cand_out[qi] = cand;
+            if (surv_out) surv_out[qi] = surv;
+        }
+        free(rq); free(probes); free(pd2); free(lut); free(h.hd); free(h.hi);
+    }
+    free(bfirst);
+    free(own);
 }

@@ -72,6 +72,7 @@ typedef struct orc_e8q_index {
     float* h3;             /* n */
     float* tab;            /* 2*stride refine tables */
     int tab_stride;
+    float* ortho;          /* n*3 scan-bank inputs per row: base, weight, perp */
 } orc_e8q_index;
 
 /* Restates E8qIndex::Build for everything the plain search reads. */
@@ -93,6 +94,46 @@ void orc_e8q_route(const orc_e8q_index* idx, const float* rot_q, size_t nprobe,
  * UINT32_MAX / +inf. threads: OpenMP threads over queries. */
 void orc_e8q_search(const orc_e8q_index* idx, const float* queries, size_t nq, size_t k,
                     size_t nprobe, uint32_t* out_ids, float* out_dists, int threads);
+
+/* ---- pruned production path -------------------------------------------
+ * The reference's shipped search: a coarse pass prices one rowA byte per
+ * block against a u8 LUT, a zero-parallel-residual lower bound dlo rejects
+ * rows that cannot beat the current k-th distance, and the survivors are
+ * refined exactly. */
+
+/* PhiInv (Newton on Phi) and OrthoQuantile: src/index/e8q_internal.hpp:75-107. */
+double orc_phi_inv(double p);
+float orc_ortho_quantile(double alpha, size_t k_eff);
+/* One 128-byte batch header from its rows' bank inputs (WriteOrthoBanks,
+ * src/index/e8q_build.cpp:31-80). */
+void orc_ortho_header(const float* base, const float* weight, const float* perp, size_t cnt,
+                      uint8_t* hdr);
+/* Headers of every 32-row batch, lists in order (128 B each); returns the
+ * batch count (out may be NULL to count). */
+size_t orc_e8q_banks(const orc_e8q_index* idx, uint8_t* out);
+/* rowA byte of cluster-major row `pos`, block blk (PackCoarseRow). */
+uint8_t orc_e8q_rowa(const orc_e8q_index* idx, size_t pos, int blk);
+/* PrepareQuery (src/index/e8q_search.cpp:20-73): the u8 coarse LUT, 32 bytes
+ * per block ([0,16) prices the low nibble = digits 4..7, [16,32) the high
+ * nibble = digits 0..3) and scal = {delta_c, base_c, lut_err, score_max}. */
+void orc_e8q_prepare_lut(int bits, int blocks, const float* rot_q, uint8_t* lut, float* scal);
+/* Coarse sum of the row's rowA bytes against the LUT (AccumulateCoarseHi,
+ * src/simd/scan_kernels_generic.cpp:12-35); pos == (size_t)-1 prices an
+ * all-zero padding row. */
+int32_t orc_e8q_coarse(const orc_e8q_index* idx, size_t pos, const uint8_t* lut);
+/* The refine arithmetic of the shipped search (RefineRowsAvx512,
+ * src/simd/e8q_search_avx512.cpp:118-347): eight fp32 dimension lanes, even
+ * and odd blocks in separate fused chains, then HsumPs. */
+float orc_e8q_refine_score(const orc_e8q_index* idx, size_t pos, const float* rot_q);
+/* The shipped sequential search (E8qIndex::Search, e8q_search.cpp:215-293,
+ * with ScanClusterAvx512 and CollectLanes): lists in probe order, batches of
+ * 32 in order, survivors refined every 32 staged rows and at the end of each
+ * list. banks: the 128-byte headers (orc_e8q_banks order), NULL for this
+ * oracle's own. cand/surv (may be NULL): per query rows scanned / refined. */
+void orc_e8q_search_pruned(const orc_e8q_index* idx, const uint8_t* banks, float alpha,
+                           int disable_prune, const float* queries, size_t nq, size_t k,
+                           size_t nprobe, uint32_t* out_ids, float* out_dists, uint64_t* cand,
+                           uint64_t* surv, int threads);
 
 #ifdef __cplusplus
 }

@@ -71,6 +71,20 @@ def lib() -> C.CDLL:
         L.orc_e8q_route.argtypes = [C.c_void_p, _f32p, C.c_size_t, _u32p, _f32p]
         L.orc_e8q_search.argtypes = [C.c_void_p, _f32p, C.c_size_t, C.c_size_t, C.c_size_t,
                                      _u32p, _f32p, C.c_int]
+        L.orc_phi_inv.argtypes = [C.c_double]
+        L.orc_phi_inv.restype = C.c_double
+        L.orc_ortho_quantile.argtypes = [C.c_double, C.c_size_t]
+        L.orc_ortho_quantile.restype = C.c_float
+        L.orc_e8q_banks.argtypes = [C.c_void_p, C.c_void_p]
+        L.orc_e8q_banks.restype = C.c_size_t
+        L.orc_e8q_prepare_lut.argtypes = [C.c_int, C.c_int, _f32p, _u8p, _f32p]
+        L.orc_e8q_coarse.argtypes = [C.c_void_p, C.c_size_t, _u8p]
+        L.orc_e8q_coarse.restype = C.c_int32
+        L.orc_e8q_refine_score.argtypes = [C.c_void_p, C.c_size_t, _f32p]
+        L.orc_e8q_refine_score.restype = C.c_float
+        L.orc_e8q_search_pruned.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_int, _f32p,
+                                            C.c_size_t, C.c_size_t, C.c_size_t, _u32p, _f32p,
+                                            C.c_void_p, C.c_void_p, C.c_int]
         L.orc_me8q_variance.argtypes = [_f32p, C.c_size_t, C.c_size_t, C.c_size_t, _f32p]
         L.orc_me8q_allocate.argtypes = [_f32p, C.c_size_t, C.c_float, C.c_int, C.c_double,
                                         C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
@@ -269,6 +283,47 @@ class OracleE8qIndex:
         lib().orc_e8q_search(self._p, queries, nq, k, nprobe, ids, dists, threads)
         return ids, dists
 
+    def banks(self):
+        """The 128-byte scan-bank header of every 32-row batch, lists in
+        order: (nbatches, 128) uint8."""
+        nb = lib().orc_e8q_banks(self._p, None)
+        out = np.zeros((nb, 128), np.uint8)
+        lib().orc_e8q_banks(self._p, out.ctypes.data)
+        return out
+
+    def prepare_lut(self, rot_q):
+        """PrepareQuery's u8 LUT (blocks x 32) and (delta, base, lut_err, score_max)."""
+        lut = np.zeros((self.blocks, 32), np.uint8)
+        scal = np.zeros(4, np.float32)
+        lib().orc_e8q_prepare_lut(self.bits, self.blocks, np.ascontiguousarray(rot_q, np.float32), lut, scal)
+        return lut, scal
+
+    def prepare_query(self, q):
+        rq = np.zeros(self.pd, np.float32)
+        lib().orc_e8q_prepare_query(self._p, np.ascontiguousarray(q, np.float32), rq)
+        return rq
+
+    def coarse(self, pos, lut):
+        return int(lib().orc_e8q_coarse(self._p, pos, np.ascontiguousarray(lut)))
+
+    def refine_score(self, pos, rot_q):
+        return float(lib().orc_e8q_refine_score(self._p, pos, np.ascontiguousarray(rot_q, np.float32)))
+
+    def search_pruned(self, queries, k, nprobe, alpha=1.0, disable_prune=False, banks=None, threads=8):
+        """The reference's shipped sequential pruned search; returns ids,
+        dists and per-query (candidates, survivors)."""
+        queries = np.ascontiguousarray(np.atleast_2d(queries), np.float32)
+        nq = queries.shape[0]
+        ids = np.zeros((nq, k), np.uint32)
+        dists = np.zeros((nq, k), np.float32)
+        cand = np.zeros(nq, np.uint64)
+        surv = np.zeros(nq, np.uint64)
+        bk = None if banks is None else np.ascontiguousarray(banks, np.uint8)
+        lib().orc_e8q_search_pruned(self._p, None if bk is None else bk.ctypes.data, alpha,
+                                    1 if disable_prune else 0, queries, nq, k, nprobe, ids, dists,
+                                    cand.ctypes.data, surv.ctypes.data, threads)
+        return ids, dists, cand, surv
+
 
 # ---- the reference's on-disk E8Q index (E8AX), read as test input ----------
 
@@ -317,6 +372,7 @@ def parse_e8ax(path: str) -> dict:
     stride = B * c if bits >= 2 else 0
     ref_batch = (stride * 32 + 256 + 63) & ~63
     rowa = np.zeros((n, B), np.uint8)
+    banks = []
     refine = np.zeros((n, max(stride, 1)), np.uint8)
     g1 = np.zeros(n, np.float32)
     h3 = np.zeros(n, np.float32)
@@ -326,6 +382,7 @@ def parse_e8ax(path: str) -> dict:
         for b0 in range(0, cnt, 32):
             m = min(32, cnt - b0)
             rec = int(arena_begin[cl]) + (b0 // 32) * batch_bytes + 128
+            banks.append(arena[rec - 128:rec])
             plane = arena[rec:rec + B * 32].reshape(B, 32)
             rrec = int(ref_begin[cl]) + (b0 // 32) * ref_batch
             base = int(lb[cl]) + b0
@@ -351,7 +408,7 @@ def parse_e8ax(path: str) -> dict:
             digits[i, b] = dbuf
             branch[i, b] = brv.value
     out.update(rowa=rowa, refine=refine[:, :stride], g1=g1, h3=h3, digits=digits,
-               branch=branch)
+               branch=branch, banks=np.array(banks, np.uint8).reshape(-1, 128))
     return out
 
 

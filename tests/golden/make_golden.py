@@ -7,7 +7,8 @@ integer-derived floats), outputs come from the reference's own code:
     BuildRefineTables, PackCoarseRow/PackRefineBlock, FhtKac4Rotator
   * oracle/_ref/e8qlib_ref    - the reference's pybind11 module: E8qIndex
     build / save (E8AX, parsed for codes, g1, h3, ids) / plain search
-    (set_disable_prune(True)) / estimate.
+    (set_disable_prune(True)) / estimate / production pruned search with its
+    per-query stats.
 
 Usage: python tests/golden/make_golden.py
 """
@@ -50,6 +51,49 @@ ME8Q_CASES = [
 
 # reference-written E8AX index files, kept whole, for the loader's tests
 E8AX_FILES = ["d96_b4", "d100_b1", "d128_b9"]
+
+
+# the reference's shipped pruned search, query by query with its stats:
+# (name, dim, bits, n, nlist, seed, sigma, nq, k, nprobe, alpha)
+PRUNED_CASES = [
+    ("d96_b4", 96, 4, 1500, 8, 11, 0.5, 20, 10, 3, 1.0),
+    ("d100_b1", 100, 1, 800, 4, 12, 0.5, 12, 10, 2, 1.0),
+    ("d128_b9", 128, 9, 600, 4, 13, 0.5, 12, 16, 4, 1.0),
+    ("d960_b6", 960, 6, 3000, 8, 14, 0.4, 16, 10, 3, 1.0),
+    ("d64_b2_k128", 64, 2, 2000, 6, 15, 0.5, 12, 128, 5, 1.0),
+    ("d200_b5_a001", 200, 5, 4000, 16, 16, 0.5, 16, 10, 6, 0.01),
+]
+
+
+def write_pruned_fixtures() -> None:
+    """The reference's production (pruned) search on PRUNED_CASES, one call
+    per query with return_stats so each query's candidate and survivor counts
+    are kept (tests/golden/pruned_<name>.npz), plus its scan-bank headers."""
+    import oracle as O
+
+    E = O.ref_module()
+    for name, dim, bits, n, nlist, seed, sigma, nq, k, nprobe, alpha in PRUNED_CASES:
+        x, cm, lab = det_mixture(seed, n, dim, nlist, sigma)
+        q = det_mixture(seed + 1000, nq, dim, nlist, sigma)[0]
+        idx = E.E8qIndex(dim, bits, seed)
+        idx.build(x, cm, lab, num_threads=4, prune_alpha=alpha)
+        with tempfile.TemporaryDirectory() as d:
+            p = os.path.join(d, "i.e8ax")
+            idx.save(p)
+            P = O.parse_e8ax(p)
+        ids, dists, cand, surv = [], [], [], []
+        for i in range(nq):
+            a, b, st = idx.search(q[i:i + 1], k, nprobe, 1, True)
+            ids.append(a[0])
+            dists.append(b[0])
+            cand.append(st["candidates"])
+            surv.append(st["survivors"])
+        np.savez_compressed(
+            os.path.join(HERE, f"pruned_{name}.npz"),
+            params=np.array([dim, bits, n, nlist, seed, nq, k, nprobe], np.int64),
+            sigma=np.float64(sigma), alpha=np.float32(alpha), banks=P["banks"],
+            search_ids=np.array(ids, np.uint32), search_dists=np.array(dists, np.float32),
+            candidates=np.array(cand, np.uint64), survivors=np.array(surv, np.uint64))
 
 
 # reference-written ME8QIDXX index files, kept whole, for the ME8Q loader's tests
@@ -196,6 +240,7 @@ def main() -> None:
             h2=P["h2"], search_ids=ids, search_dists=dists, est_ids=est_ids, est=est)
     write_e8ax_fixtures()
     write_me8q_fixtures()
+    write_pruned_fixtures()
     print("golden fixtures written to", HERE)
 
 
@@ -204,5 +249,7 @@ if __name__ == "__main__":
         write_e8ax_fixtures()  # only the E8AX files
     elif len(sys.argv) > 1 and sys.argv[1] == "me8q":
         write_me8q_fixtures()  # only the ME8QIDXX files
+    elif len(sys.argv) > 1 and sys.argv[1] == "pruned":
+        write_pruned_fixtures()  # only the pruned-search fixtures
     else:
         main()
