@@ -177,6 +177,71 @@ def recall_at(ids, gt, k=10):
     return hit / (gt.shape[0] * k)
 
 
+def host_cpu():
+    """Threads the CPU baseline uses and what they are: one per physical core
+    available to this process (logical CPUs in the affinity mask divided by
+    the hardware threads per core), the logical count and the CPU model."""
+    logical = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        import psutil
+
+        per_core = max(1, (psutil.cpu_count(logical=True) or 1) // max(1, psutil.cpu_count(logical=False) or 1))
+    except Exception:
+        per_core = 1
+    model = None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"cores": max(1, logical // per_core), "logical_cpus": logical, "threads_per_core": per_core,
+            "cpu_model": model}
+
+
+def time_rounds(fn, nq, warmup=3, min_rounds=9, min_s=0.4, max_s=30.0):
+    """QPS of fn() (nq queries per call) with the reference protocol's timing
+    (experiments/protocol.py:559-597): `warmup` untimed calls, then rounds
+    until at least min_rounds rounds and min_s seconds; median QPS with p25 and
+    p75. max_s bounds the host time of slow arms (at least 3 rounds)."""
+    for _ in range(warmup):
+        fn()
+    qps = []
+    t_start = time.perf_counter()
+    while len(qps) < min_rounds or time.perf_counter() - t_start < min_s:
+        t0 = time.perf_counter()
+        fn()
+        qps.append(nq / (time.perf_counter() - t0))
+        if time.perf_counter() - t_start > max_s and len(qps) >= 3:
+            break
+    qps.sort()
+    return {"qps": statistics.median(qps), "p25": float(np.percentile(qps, 25)),
+            "p75": float(np.percentile(qps, 75)), "rounds": len(qps)}
+
+
+def relerr(x, q, ids, dists, k):
+    """SAQ relative distance error |D_hat - Delta| / Delta over the returned
+    top-k (experiments/protocol.py:525-556, p99 as in :941-966): D_hat is the
+    distance the search returned for an id, Delta the exact squared L2 from the
+    raw vectors in FP64. Returns (mean, p99, max)."""
+    import torch
+
+    idt = torch.from_numpy(ids[:, :k].astype(np.int64)).to(x.device)
+    dt = torch.from_numpy(np.ascontiguousarray(dists[:, :k])).to(x.device).double()
+    ok = (idt >= 0) & (idt < x.shape[0]) & torch.isfinite(dt)
+    errs = []
+    for i in range(0, idt.shape[0], 128):
+        ii = idt[i:i + 128].clamp(0, x.shape[0] - 1)
+        delta = ((q[i:i + 128, None, :].double() - x[ii].double()) ** 2).sum(-1)
+        m = ok[i:i + 128] & (delta > 1e-12)
+        errs.append(((dt[i:i + 128] - delta).abs() / delta)[m])
+    e = torch.cat(errs).cpu().numpy()
+    if e.size == 0:
+        return -1.0, -1.0, -1.0
+    return float(e.mean()), float(np.percentile(e, 99)), float(e.max())
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
@@ -232,6 +297,28 @@ class Clocks:
         reasons = sorted({names[i] for r in busy for i, v in enumerate(r[2]) if v.lower() == "active"})
         return {"sm_mhz": statistics.median(r[0] for r in busy), "sm_max_mhz": max(r[1] for r in rows),
                 "reasons": reasons, "samples": len(busy)}
+
+
+def plain_roofline(prof, a, peak, pk_kind):
+    """The plain scan kernel (one query per launch) against HBM: algorithmic
+    bytes per launch = (nbits * Dpad / 8 + 8) per candidate (codes, g1, h3);
+    its CUDA-event time per launch; beside it the whole per-query chain
+    (routing launch + scan launch) with the route sweep's nlist * Dpad * 4
+    bytes added."""
+    n = max(1, prof["scan_launches"])
+    t = prof["scan_ms"] / n / 1000.0
+    b = prof["algo_bytes"] / n
+    pd = (a.dim + 63) // 64 * 64
+    rb = a.nlist * pd * 4 + a.nlist * 4
+    tr = prof["prep_ms"] / n / 1000.0
+    ach = b / t / 1e9 if t > 0 else 0.0
+    chain = (b + rb) / (t + tr) / 1e9 if t + tr > 0 else 0.0
+    return {"kernel": "scan_plain_kernel", "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
+            "unit": "GB/s", "frac": round(ach / peak, 4), "peak_kind": pk_kind,
+            "algo_bytes_per_launch": int(b), "launch_us": round(t * 1e6, 2),
+            "candidates_per_query": int(prof["candidates"] / n),
+            "route_kernel_us": round(tr * 1e6, 2), "route_bytes": int(rb),
+            "chain_gbs": round(chain, 1), "chain_frac": round(chain / peak, 4)}
 
 
 def serve_open_loop(e8qlib, idx, mode, qn, ks, nprobes, rate_qps, seconds, seed, max_batch):
@@ -290,27 +377,26 @@ def cpu_baseline(a, x_host, cm_host, lab_host, q_host, gt, steps=None, warmup=No
     E = O.ref_module()
     if E is None:
         return None
-    cores = os.cpu_count() or 1
+    hc = host_cpu()
+    cores = hc["cores"]
     t0 = time.perf_counter()
     ref = E.E8qIndex(a.dim, a.nbits, a.seed)
     with QuietStdout():
         ref.build(x_host, cm_host, lab_host.astype(np.uint32), num_threads=cores)
     build_s = time.perf_counter() - t0
-    out = {"cores": cores, "build_s": round(build_s, 2)}
+    out = dict(hc, build_s=round(build_s, 2))
     sample = min(2048, q_host.shape[0])
     qs = q_host[:sample]
-    ref.search(qs[:64], a.k, a.nprobe, cores)
-    t0 = time.perf_counter()
     ids, _ = ref.search(qs, a.k, a.nprobe, cores)
-    pruned_qps = sample / (time.perf_counter() - t0)
-    out["pruned_qps"] = pruned_qps
     out["pruned_recall"] = recall_at(ids[:gt.shape[0]], gt[:min(sample, gt.shape[0])], a.k)
+    out["pruned"] = time_rounds(lambda: ref.search(qs, a.k, a.nprobe, cores), sample)
+    out["pruned_qps"] = out["pruned"]["qps"]
     ref.set_disable_prune(True)
-    ps = min(512, sample)
-    t0 = time.perf_counter()
+    ps = min(256, sample)
     ids_p, _ = ref.search(qs[:ps], a.k, a.nprobe, cores)
-    out["plain_qps"] = ps / (time.perf_counter() - t0)
     out["plain_recall"] = recall_at(ids_p, gt[:ps], a.k)
+    out["plain"] = time_rounds(lambda: ref.search(qs[:ps], a.k, a.nprobe, cores), ps, warmup=1, max_s=12.0)
+    out["plain_qps"] = out["plain"]["qps"]
     ref.set_disable_prune(False)
     out["ref"] = ref
     return out
@@ -347,7 +433,7 @@ def me8q_cpu_baseline(xp_host, cen_host, lab_host, var_host, q_host, avg_bits, n
     E = O.ref_module()
     if E is None:
         return None
-    cores = os.cpu_count() or 1
+    cores = host_cpu()["cores"]
     xs = np.ascontiguousarray(xp_host[:sample_n])
     ls = np.ascontiguousarray(lab_host[:sample_n]).astype(np.uint32)
     t0 = time.perf_counter()
@@ -621,15 +707,18 @@ def main():
         return idx.search_ptr(qi.data_ptr(), b, a.k, a.nprobe, out_ids.data_ptr(), out_d.data_ptr(),
                               mode, sp)
 
-    # recall of the measured path on the ground-truth queries
+    # recall and distance error of the measured path on the ground-truth queries
     rec_ids = np.zeros((a.gt, a.k), np.uint32)
+    rec_d = np.zeros((a.gt, a.k), np.float32)
     for i in range(0, a.gt, nb):
         b = min(nb, a.gt - i)
         idx.search_ptr(q[i:i + b].data_ptr(), b, a.k, a.nprobe, out_ids.data_ptr(), out_d.data_ptr(),
                        a.path, sp)
         torch.cuda.synchronize()
         rec_ids[i:i + b] = out_ids[:b].cpu().numpy().view(np.uint32)
+        rec_d[i:i + b] = out_d[:b].cpu().numpy()
     recall = recall_at(rec_ids, gt, a.k)
+    err_mean, err_p99, err_max = relerr(x, q[:a.gt], rec_ids, rec_d, a.k)
 
     for i in range(a.warmup):
         step(i, a.path)
@@ -673,6 +762,8 @@ def main():
                 "launch_us": round(t_launch * 1e6, 2), "peak_kind": pk_kind,
                 "item_bytes_per_launch": int(item_per_launch),
                 "item_gbs": round(item_per_launch / t_launch / 1e9, 1) if t_launch > 0 else 0.0}
+    if a.path == "plain":
+        roofline["plain_scan"] = plain_roofline(prof, a, peak, pk_kind)
     step_breakdown = None
     if a.path == "precision" and prof.get("final_launches"):
         nl_ = max(1, prof["final_launches"])
@@ -736,6 +827,20 @@ def main():
            "h2d_bytes_per_step": nb * a.dim * 4, "d2h_bytes_per_step": nb * a.k * 8,
            "host_wall_qps": round(total_q / (e2e_wall_ms / 1000.0), 1)}
 
+    # the plain one-query-per-launch scan's own roofline (the streaming scan):
+    # events around each routing and scan launch of 128 single queries
+    if a.path != "plain":
+        pq = 128
+        pi = torch.empty(pq, a.k, dtype=torch.int32, device=dev)
+        pdd = torch.empty(pq, a.k, dtype=torch.float32, device=dev)
+        idx.search_ptr(q.data_ptr(), 16, a.k, a.nprobe, pi.data_ptr(), pdd.data_ptr(), "plain", sp)
+        torch.cuda.synchronize()
+        idx.profile_start()
+        idx.search_ptr(q[pq:2 * pq].data_ptr(), pq, a.k, a.nprobe, pi.data_ptr(), pdd.data_ptr(), "plain", sp)
+        torch.cuda.synchronize()
+        pp = idx.profile_stop()
+        roofline["plain_scan"] = plain_roofline(pp, a, peak, pk_kind)
+
     # the plain one-query-per-launch GPU scan on the same index (the drop-in
     # path the batched modes are compared against), a short device-resident run
     plain_qps = None
@@ -778,8 +883,11 @@ def main():
             cpu = {"value": round(cb["pruned_qps"], 1), "unit": "QPS", "cores": cb["cores"],
                    "kind": "reference",
                    "sample": (f"2048 queries of this workload through the reference E8qIndex.search "
-                              f"(production pruned path, {cb['cores']} threads); plain scan "
-                              f"(set_disable_prune) {cb['plain_qps']:.1f} QPS on 512 queries"),
+                              f"(production pruned path, {cb['cores']} threads = physical cores), median of "
+                              f"{cb['pruned']['rounds']} rounds after 3 warm-up passes; plain scan "
+                              f"(set_disable_prune) on 256 queries"),
+                   "p25": round(cb["pruned"]["p25"], 1), "p75": round(cb["pruned"]["p75"], 1),
+                   "logical_cpus": cb["logical_cpus"], "cpu_model": cb["cpu_model"],
                    "recall_at_10": round(cb["pruned_recall"], 4),
                    "plain_qps": round(cb["plain_qps"], 1), "plain_recall_at_10": round(cb["plain_recall"], 4),
                    "build_s": cb["build_s"]}
@@ -795,8 +903,15 @@ def main():
         "config": {"workload": workload_name(a), "n": a.n, "dim": a.dim, "nlist": a.nlist,
                    "nbits": a.nbits, "k": a.k, "nprobe": a.nprobe, "query_batch": nb,
                    "path": a.path, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (codes %.0f MB > 126 MB)" % (idx.memory_bytes / 1e6)},
+                   "l2": "inputs larger than L2 (codes %.0f MB > 126 MB)" % (idx.memory_bytes / 1e6),
+                   "recall_at_10": round(recall, 4),
+                   "relerr_mean": round(err_mean, 6), "relerr_p99": round(err_p99, 6),
+                   "relerr_max": round(err_max, 6),
+                   "plain_gpu_qps": None if plain_qps is None else round(plain_qps, 1),
+                   "plain_scan_frac": roofline.get("plain_scan", {}).get("frac")},
         "recall_at_10": round(recall, 4), "build_s": round(build_s, 2),
+        "relerr": {"mean": round(err_mean, 6), "p99": round(err_p99, 6), "max": round(err_max, 6),
+                   "definition": "|D_hat - Delta| / Delta over the returned top-k, Delta = FP64 exact"},
         "clocks": clk.summary(), "gpu_launches": int(launches), "roofline": roofline,
         "e2e": e2e, "cpu_baseline": cpu,
         "plain_gpu_qps": None if plain_qps is None else round(plain_qps, 1),
@@ -842,12 +957,16 @@ def run_reference(a, rank, world, dist):
             "value": round(value, 1), "unit": "QPS", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": round(sec * 1000 / a.steps, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32", "data": "synthetic (same seeded mixture)",
-            "config": {"workload": workload_name(a) + " (reference CPU, production pruned search)",
+            "config": {"workload": workload_name(a),
                        "n": a.n, "dim": a.dim, "nlist": a.nlist, "nbits": a.nbits, "k": a.k,
-                       "nprobe": a.nprobe, "query_batch": nb},
+                       "nprobe": a.nprobe, "query_batch": nb,
+                       "arm": "reference CPU, production pruned search",
+                       "recall_at_10": round(cb["pruned_recall"], 4)},
             "recall_at_10": round(cb["pruned_recall"], 4),
             "cpu_baseline": {"value": round(value, 1), "unit": "QPS", "cores": cores, "kind": "reference",
-                             "sample": f"{nb} queries per step, {cores} threads, reference E8qIndex.search"},
+                             "logical_cpus": cb["logical_cpus"], "cpu_model": cb["cpu_model"],
+                             "sample": (f"{nb} queries per step, {cores} threads (physical cores), "
+                                        f"reference E8qIndex.search")},
             "e2e": {"value": round(value, 1), "unit": "QPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "plain_qps": round(cb["plain_qps"], 1), "build_s": cb["build_s"]}
     print(json.dumps(line), flush=True)

@@ -52,7 +52,8 @@ int mode_of(const std::string& m) {
     if (m == "plain") return E8QC_MODE_PLAIN;
     if (m == "batched") return E8QC_MODE_BATCHED;
     if (m == "precision") return E8QC_MODE_PRECISION;
-    throw std::invalid_argument("mode must be 'plain', 'batched' or 'precision'");
+    if (m == "pruned") return E8QC_MODE_PRUNED;
+    throw std::invalid_argument("mode must be 'auto', 'plain', 'pruned', 'batched' or 'precision'");
 }
 
 // ME8Q search modes: the grouped exact scan, or int8 tensor-core candidates
@@ -115,7 +116,7 @@ class E8qIndex {
         if (k == 0) throw std::invalid_argument("k must be positive");
         if (k > E8QC_MAX_K) throw std::invalid_argument("k must be <= " + std::to_string(E8QC_MAX_K));
         if (nprobe == 0) throw std::invalid_argument("nprobe must be positive");
-        const int md = mode_of(mode);
+        const int md = search_mode(mode);
         const size_t nq = static_cast<size_t>(q.shape(0));
         py::array_t<uint32_t> ids({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k)});
         py::array_t<float> dists({static_cast<py::ssize_t>(nq), static_cast<py::ssize_t>(k)});
@@ -137,7 +138,7 @@ class E8qIndex {
     uint64_t search_ptr(uintptr_t queries, size_t nq, size_t k, size_t nprobe, uintptr_t out_ids,
                         uintptr_t out_dists, const std::string& mode, uintptr_t stream) {
         require("search");
-        const int md = mode_of(mode);
+        const int md = search_mode(mode);
         e8qc_stats st{};
         py::gil_scoped_release nogil;
         check(e8qc_e8q_search(idx_, reinterpret_cast<const float*>(queries), nq, k, nprobe, md,
@@ -177,6 +178,23 @@ class E8qIndex {
             throw std::invalid_argument("query dimension does not match index dim");
         float out = 0.0f;
         check(e8qc_e8q_estimate(idx_, q.data(), id, &out));
+        return out;
+    }
+
+    // "auto" is the reference's search: the pruned production path, or the
+    // plain scan of every candidate after set_disable_prune(True).
+    int search_mode(const std::string& mode) const {
+        if (mode != "auto") return mode_of(mode);
+        e8qc_info inf{};
+        check(e8qc_e8q_info(idx_, &inf));
+        return inf.disable_prune ? E8QC_MODE_PLAIN : E8QC_MODE_PRUNED;
+    }
+
+    // Thresholds of the last pruned search's first nq queries.
+    py::array_t<float> pruned_thresholds(size_t nq) {
+        require("pruned_thresholds");
+        py::array_t<float> out(static_cast<py::ssize_t>(nq));
+        check(e8qc_e8q_pruned_thresholds(idx_, out.mutable_data(), nq));
         return out;
     }
 
@@ -845,9 +863,10 @@ PYBIND11_MODULE(_e8qlib, m) {
              py::arg("nlist"), py::arg("cluster_ids"), py::arg("prune_alpha") = 0.0F,
              py::arg("stream") = 0)
         .def("search", &E8qIndex::search, py::arg("queries"), py::arg("k"), py::arg("nprobe"),
-             py::arg("num_threads") = 1, py::arg("return_stats") = false, py::arg("mode") = "plain")
+             py::arg("num_threads") = 1, py::arg("return_stats") = false, py::arg("mode") = "auto")
+        .def("pruned_thresholds", &E8qIndex::pruned_thresholds, py::arg("nq"))
         .def("search_ptr", &E8qIndex::search_ptr, py::arg("queries"), py::arg("nq"), py::arg("k"),
-             py::arg("nprobe"), py::arg("out_ids"), py::arg("out_dists"), py::arg("mode") = "plain",
+             py::arg("nprobe"), py::arg("out_ids"), py::arg("out_dists"), py::arg("mode") = "auto",
              py::arg("stream") = 0)
         .def("search_ragged", &E8qIndex::search_ragged, py::arg("queries"), py::arg("k"),
              py::arg("nprobe"), py::arg("k_max"), py::arg("mode") = "batched")

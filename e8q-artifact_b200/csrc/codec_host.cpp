@@ -86,6 +86,28 @@ double fixed_scale(int bits) {
     return sched[std::min(std::max(bits, 1), kMaxBits)];
 }
 
+// Newton on Phi from the asymptotic start, 12 steps (std::erf / std::exp /
+// std::log, the functions the reference calls): src/index/e8q_internal.hpp:75-97.
+double phi_inv(double p) {
+    if (p <= 0.0) return -8.0;
+    if (p >= 1.0) return 8.0;
+    const double t = std::min(p, 1.0 - p);
+    double x = std::sqrt(-2.0 * std::log(t));
+    if (p < 0.5) x = -x;
+    for (int it = 0; it < 12; ++it) {
+        const double phi = 0.3989422804014327 * std::exp(-0.5 * x * x);
+        const double Phi = 0.5 * (1.0 + std::erf(x * 0.7071067811865476));
+        x -= (Phi - p) / phi;
+    }
+    return x;
+}
+
+// src/index/e8q_internal.hpp:99-107.
+float ortho_quantile(double alpha, size_t k_eff) {
+    const double tail = std::min(alpha / static_cast<double>(std::max<size_t>(k_eff, 1)), 0.49);
+    return static_cast<float>(std::max(phi_inv(1.0 - tail), 1.0));
+}
+
 namespace {
 
 // Bounded-bin index (src/quantization/e8q_codec.cpp:70-123): bins no wider

@@ -22,6 +22,7 @@
 #include "scan_plain.h"
 #include "io_e8ax.h"
 #include "precision.h"
+#include "pruned.h"
 #include "serve_target.h"
 #include "workspace.h"
 
@@ -120,6 +121,8 @@ struct e8qc_index {
         list_of_tile, list_begin_d, list_order;
     DevBuf ortho;   // built indexes: per slot the scan-bank inputs (base, weight, perp), for saving
     std::vector<uint8_t> banks;  // loaded indexes: the file's 128-byte scan-bank headers, for saving
+    DevBuf rowa;     // pruned mode: the coarse plane (rowA bytes per vector), built on its first search
+    DevBuf banks_d;  // pruned mode: the 128-byte scan-bank header of every tile
     DevBuf proxy;   // int8 proxy plane of the precision mode, built on its first search
     DevBuf vcodes;  // the codes slot-major, for the precision mode's rescoring (built with the plane)
     // autotuned (schedule, stages) per (mode, log2 batch size, log2 nprobe)
@@ -134,7 +137,7 @@ struct e8qc_index {
         return signs.bytes + mean_rot.bytes + cen.bytes + cn2.bytes + tile_begin_d.bytes +
                list_len_d.bytes + codes.bytes + g1.bytes + h3.bytes + ids.bytes + tab.bytes +
                list_of_tile.bytes + list_begin_d.bytes + list_order.bytes + proxy.bytes + vcodes.bytes +
-               ortho.bytes + banks.size();
+               ortho.bytes + banks.size() + rowa.bytes + banks_d.bytes;
     }
     // A captured graph of the last repeated batch shape of the grouped modes
     // (search calls from kGraphMinQueries queries whose mode, size, k and
@@ -214,7 +217,7 @@ void plain_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size_
     ws.ensure_route(x->nlist);
     // grid: one CTA per SM (the kernel fills an SM's shared memory), fewer
     // when the largest possible probe set has fewer tiles than that
-    const ScanGeo geo = plain_scan_geo(x->view, 1536);
+    const ScanGeo geo = plain_scan_geo(x->view);
     const size_t max_tiles = max_tiles_for(x, nprobe);
     int sms = 148;
     E8QC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device));
@@ -228,15 +231,17 @@ void plain_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size_
                 ws.err.as<uint32_t>(), grid};
 
     uint64_t launches = 0;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEvent_t er = nullptr, e0 = nullptr, e1 = nullptr;
     std::vector<uint32_t> probes;
     if (x->profiling) {
+        E8QC_CUDA(cudaEventCreate(&er));
         E8QC_CUDA(cudaEventCreate(&e0));
         E8QC_CUDA(cudaEventCreate(&e1));
         probes.resize(nprobe);
     }
     for (size_t i = 0; i < nq; ++i) {
         const float* rq = rq_all + i * x->pd;
+        if (x->profiling) E8QC_CUDA(cudaEventRecord(er, s));
         launches += launch_route_one(x->view, rq, static_cast<int>(nprobe), rw, s);
         if (x->profiling) E8QC_CUDA(cudaEventRecord(e0, s));
         launches += launch_scan_plain(x->view, rq, rw, static_cast<int>(nprobe), static_cast<int>(k), sw,
@@ -245,8 +250,10 @@ void plain_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size_
             E8QC_CUDA(cudaEventRecord(e1, s));
             E8QC_CUDA(cudaMemcpyAsync(probes.data(), rw.probes, nprobe * 4, cudaMemcpyDeviceToHost, s));
             E8QC_CUDA(cudaStreamSynchronize(s));
-            float ms = 0.0f;
+            float ms = 0.0f, rms = 0.0f;
             E8QC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            E8QC_CUDA(cudaEventElapsedTime(&rms, er, e0));
+            x->prof.prep_ms += rms;  // the routing launch of this query
             uint64_t cand = 0;
             for (uint32_t c : probes) cand += x->list_begin[c + 1] - x->list_begin[c];
             x->prof.scan_launches += 1;
@@ -259,9 +266,112 @@ void plain_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size_
             x->prof.queries += 1;
         }
     }
+    if (er) cudaEventDestroy(er);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (st) st->launches += launches;
+}
+
+void scan_class_means(int bits, double w_cls[2]);
+
+// The pruned mode's device planes: the coarse plane (derived from the codes)
+// and the scan-bank headers of every tile -- a loaded index's headers as its
+// file holds them, a built index's quantised from its bank inputs (the
+// reference's WriteOrthoBanks, which its saved files carry). Built on first
+// use; returns the kernels launched.
+int ensure_pruned_planes(e8qc_index* x, cudaStream_t s) {
+    if (x->rowa.p != nullptr) return 0;
+    int launches = 0;
+    std::vector<uint8_t> hdr(x->ntiles * 128, 0);
+    if (!x->banks.empty()) {
+        if (x->banks.size() != hdr.size()) fail(E8QC_ESTATE, "scan-bank headers do not match the tiles");
+        std::memcpy(hdr.data(), x->banks.data(), hdr.size());
+    } else if (x->ortho.bytes != 0) {
+        std::vector<float> os(x->ntiles * 32 * 3);
+        E8QC_CUDA(cudaMemcpyAsync(os.data(), x->ortho.p, os.size() * 4, cudaMemcpyDeviceToHost, s));
+        E8QC_CUDA(cudaStreamSynchronize(s));
+        float ob[32], ow[32], op[32];
+        for (size_t c = 0; c < x->nlist; ++c) {
+            const uint64_t len = x->list_begin[c + 1] - x->list_begin[c];
+            for (uint32_t t = x->tile_begin[c]; t < x->tile_begin[c + 1]; ++t) {
+                const uint64_t lo = static_cast<uint64_t>(t - x->tile_begin[c]) * 32;
+                const size_t cnt = static_cast<size_t>(std::min<uint64_t>(32, len - lo));
+                for (size_t v = 0; v < cnt; ++v) {
+                    ob[v] = os[(t * 32 + v) * 3 + 0];
+                    ow[v] = os[(t * 32 + v) * 3 + 1];
+                    op[v] = os[(t * 32 + v) * 3 + 2];
+                }
+                ortho_banks(ob, ow, op, cnt, hdr.data() + static_cast<size_t>(t) * 128);
+            }
+        }
+    } else {
+        fail(E8QC_ESTATE, "index holds no scan banks for the pruned search");
+    }
+    x->banks_d.upload(hdr.data(), hdr.size(), s);
+    DevBuf rowa;
+    rowa.alloc(x->ntiles * static_cast<size_t>(rowa_chunks(x->B)) * 32 * 16);
+    launches += launch_build_rowa(x->view, static_cast<int>(x->ntiles), rowa.as<uint4>(), s);
+    E8QC_CUDA(cudaStreamSynchronize(s));
+    std::swap(x->rowa.p, rowa.p);
+    std::swap(x->rowa.bytes, rowa.bytes);
+    return launches;
+}
+
+// The reference's production search, one query per launch sequence (route,
+// then one cooperative pruned kernel): pruned.cu.
+void pruned_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size_t nprobe, uint32_t* ids_d,
+                   float* d_d, e8qc_stats* st, cudaStream_t s) {
+    Workspace& ws = x->ws;
+    ws.ensure_route(x->nlist);
+    uint64_t launches = static_cast<uint64_t>(ensure_pruned_planes(x, s));
+    const size_t max_tiles = max_tiles_for(x, nprobe);
+    int sms = 148;
+    E8QC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device));
+    int grid = static_cast<int>(std::max<size_t>(1, std::min<size_t>(max_tiles, static_cast<size_t>(sms))));
+    const int per_cta = static_cast<int>((max_tiles + static_cast<size_t>(grid) - 1) / static_cast<size_t>(grid));
+    const int stash = std::min(per_cta, pruned_stash_cap(x->view));
+    grid = std::min(grid, pruned_max_grid(x->view, stash));
+    if (grid < 1) fail(E8QC_EINVAL, "the pruned search does not fit this device");
+    ws.ensure_scan(static_cast<size_t>(grid));
+    ws.ensure_pruned(static_cast<size_t>(grid), nq);
+    RouteWork rw{ws.keys.as<uint64_t>(), ws.probes.as<uint32_t>(), ws.probe_d2.as<float>(),
+                 ws.tile_off.as<uint32_t>(), ws.route_counter.as<uint32_t>(), ws.total_tiles.as<uint32_t>()};
+    ScanWork sw{ws.part_d.as<float>(), ws.part_id.as<uint32_t>(), ws.scan_counter.as<uint32_t>(),
+                ws.err.as<uint32_t>(), grid};
+    double w_cls[2];
+    scan_class_means(x->bits, w_cls);
+    PrunedWork pw{};
+    pw.seed_dc = ws.pr_dc.as<float>();
+    pw.seed_key = ws.pr_key.as<uint32_t>();
+    pw.counters = ws.pr_counters.as<uint32_t>();
+    pw.stats = ws.pr_stats.as<unsigned long long>();
+    pw.err = ws.err.as<uint32_t>();
+    pw.banks = x->banks_d.as<uint8_t>();
+    pw.rowa = x->rowa.as<uint4>();
+    pw.nrc = rowa_chunks(x->B);
+    pw.z = ortho_quantile(static_cast<double>(x->prune_alpha), std::max<size_t>(4 * k, 32));
+    pw.w_cls0 = w_cls[0];
+    pw.w_cls1 = w_cls[1];
+    pw.disable_prune = x->disable_prune ? 1 : 0;
+    pw.stash_tiles = stash;
+    E8QC_CUDA(cudaMemsetAsync(ws.pr_counters.p, 0, 8, s));
+    E8QC_CUDA(cudaMemsetAsync(ws.pr_stats.p, 0, 16, s));
+    for (size_t i = 0; i < nq; ++i) {
+        const float* rq = rq_all + i * x->pd;
+        launches += launch_route_one(x->view, rq, static_cast<int>(nprobe), rw, s);
+        pw.thr = ws.pr_thr.as<float>() + i;
+        launches += launch_pruned(x->view, rq, rw, static_cast<int>(nprobe), static_cast<int>(k), sw, pw,
+                                  ids_d + i * k, d_d + i * k, s);
+    }
+    ws.pr_last_nq = nq;
+    if (st) {
+        unsigned long long cs[2] = {0, 0};
+        E8QC_CUDA(cudaMemcpyAsync(cs, ws.pr_stats.p, 16, cudaMemcpyDeviceToHost, s));
+        E8QC_CUDA(cudaStreamSynchronize(s));
+        st->candidates += cs[0];
+        st->survivors += cs[1];
+        st->launches += launches;
+    }
 }
 
 // ---- autotuning of the grouped paths ----
@@ -627,6 +737,8 @@ void set_view(e8qc_index* x) {
     v.list_of_tile = x->list_of_tile.as<uint32_t>();
     x->proxy.release();
     x->vcodes.release();
+    x->rowa.release();
+    x->banks_d.release();
     v.proxy = nullptr;
     v.vcodes = nullptr;
 }
@@ -897,7 +1009,8 @@ int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, si
         if (k == 0) fail(E8QC_EINVAL, "k must be positive");
         if (k > static_cast<size_t>(kMaxK)) fail(E8QC_EINVAL, "k must be <= 128");
         if (nprobe == 0) fail(E8QC_EINVAL, "nprobe must be positive");
-        if (mode != E8QC_MODE_PLAIN && mode != E8QC_MODE_BATCHED && mode != E8QC_MODE_PRECISION)
+        if (mode != E8QC_MODE_PLAIN && mode != E8QC_MODE_BATCHED && mode != E8QC_MODE_PRECISION &&
+            mode != E8QC_MODE_PRUNED)
             fail(E8QC_EINVAL, "unknown search mode");
         if (nq == 0) return;
         if (!queries || !out_ids) fail(E8QC_EINVAL, "null buffer");
@@ -905,7 +1018,8 @@ int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, si
         std::shared_ptr<e8qc_plan> plan;
         // (host-resident queries only: device-resident ones would add a copy
         // into the plan's staging, and the direct path keeps the GPU as busy)
-        if (mode != E8QC_MODE_PLAIN && nq >= kGraphMinQueries && !x->profiling && !is_device_ptr(queries)) {
+        if (mode != E8QC_MODE_PLAIN && mode != E8QC_MODE_PRUNED && nq >= kGraphMinQueries && !x->profiling &&
+            !is_device_ptr(queries)) {
             const e8qc_index::GraphKey key{mode, nq, k, std::min(nprobe, x->nlist)};
             bool create = false;
             {
@@ -983,6 +1097,8 @@ int e8qc_e8q_search(e8qc_index* x, const float* queries, size_t nq, size_t k, si
         if (stats) E8QC_CUDA(cudaEventRecord(ev[1], s));
         if (mode == E8QC_MODE_PLAIN) {
             plain_search(x, rq, nq, k, np, ids_d, d_d, stats, s);
+        } else if (mode == E8QC_MODE_PRUNED) {
+            pruned_search(x, rq, nq, k, np, ids_d, d_d, stats, s);
         } else {
             launches += grouped_search(x, mode, rq, nq, nullptr, nullptr, k, np, ids_d, d_d, s);
         }
@@ -1107,6 +1223,18 @@ int e8qc_e8q_set_prune_alpha(e8qc_index* x, float alpha) {
         require_built(x, "set_prune_alpha");
         if (!(alpha > 0.0f)) fail(E8QC_EINVAL, "prune_alpha must be positive");
         x->prune_alpha = alpha;
+    });
+}
+
+int e8qc_e8q_pruned_thresholds(e8qc_index* x, float* out, size_t nq) {
+    return guarded([&] {
+        require_built(x, "pruned_thresholds");
+        if (out == nullptr && nq > 0) fail(E8QC_EINVAL, "null buffer");
+        std::lock_guard<std::mutex> lock(x->mu);
+        if (nq > x->ws.pr_last_nq) fail(E8QC_EINVAL, "more thresholds asked for than the last pruned search had queries");
+        if (nq == 0) return;
+        DeviceGuard g(x->device);
+        E8QC_CUDA(cudaMemcpy(out, x->ws.pr_thr.p, nq * 4, cudaMemcpyDeviceToHost));
     });
 }
 

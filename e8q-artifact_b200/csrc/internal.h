@@ -31,6 +31,11 @@ void cuda_check(cudaError_t e, const char* what);
 double inv_normal_cdf(double p);
 std::vector<double> branch_levels(int bits, int branch);
 double fixed_scale(int bits);
+// PhiInv by Newton steps on Phi, and the per-query concentration quantile
+// lambda = max(1, PhiInv(1 - min(alpha / k_eff, 0.49)))
+// (src/index/e8q_internal.hpp:75-107).
+double phi_inv(double p);
+float ortho_quantile(double alpha, size_t k_eff);
 constexpr double kSigmaC = 1.1180339887498949;
 
 // Sorted level table with the bounded-bin insertion index

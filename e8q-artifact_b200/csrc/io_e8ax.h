@@ -28,6 +28,10 @@ struct E8axParts {
     std::vector<uint8_t> banks;          // the 128-byte scan-bank header of every 32-vector batch, file order
 };
 
+// The 128-byte scan-bank header of one 32-vector batch from its vectors'
+// bank inputs (WriteOrthoBanks, src/index/e8q_build.cpp:31-80).
+void ortho_banks(const float* base, const float* weight, const float* perp, size_t cnt, uint8_t* hdr);
+
 // Everything an E8AX file holds, in compact (cluster-major) vector order.
 struct E8axSave {
     size_t n = 0, dim = 0, nlist = 0, pd = 0;

@@ -120,7 +120,7 @@ extern "C" int e8qc_e8q_search_plain_noalloc(e8qc_index* idx, const float* queri
         E8QC_CUDA(cudaMemsetAsync(sc->words, 0, sizeof(sc->words), s));
         RouteWork rw{sc->keys, sc->probes, sc->probe_d2, sc->tile_off, &sc->words[0], &sc->words[2]};
         ScanWork sw{sc->part_d, sc->part_id, &sc->words[1], &sc->words[3], grid};
-        const ScanGeo geo = plain_scan_geo(view, 1536);
+        const ScanGeo geo = plain_scan_geo(view);
         for (size_t i = 0; i < nq; ++i) {
             launch_rotate(view, queries + i * dim, 1, sc->rq, s);
             launch_route_one(view, sc->rq, static_cast<int>(np), rw, s);

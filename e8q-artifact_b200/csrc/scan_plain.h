@@ -13,19 +13,19 @@ __host__ __device__ constexpr int table_rep(int bits) {
     return (8192 >> (bits + 1)) >= 32 ? 32 : ((8192 >> (bits + 1)) >= 1 ? (8192 >> (bits + 1)) : 1);
 }
 
-// A tile (32 vectors) is streamed in segments of U whole chunk-groups; odd
-// rates whose block count leaves half a group end with a tail segment.
+// Launch geometry of the plain scan: warps per CTA, vectors per lane of a
+// work unit (1 or 2), tiles per batch and the dynamic shared memory (query,
+// tile offsets, the batch's unit partial sums, merge buffers; the level table
+// copies too for the rates that do not fit the static table).
 struct ScanGeo {
-    int ng;         // full groups per vector
-    int tail;       // 1 when a half-group (8 blocks) follows
-    int U;          // groups per segment
-    int nseg;       // segments per tile
-    int seg_bytes;  // bytes of one ring stage (128-aligned)
-    int warps;      // warps per CTA (shared-memory budget)
+    int warps;
+    int v;
+    int tb_tiles;
+    size_t smem;
 };
 
-ScanGeo plain_scan_geo(const DevIndex& ix, size_t max_seg_bytes);
-size_t scan_smem_bytes(const DevIndex& ix, const ScanGeo& geo);
+ScanGeo plain_scan_geo(const DevIndex& ix);
+size_t scan_smem_bytes(const DevIndex& ix, int tb_tiles);
 int launch_scan_plain(const DevIndex& ix, const float* rq, const RouteWork& rw, int nprobe, int k,
                       const ScanWork& sw, const ScanGeo& geo, uint32_t* out_ids, float* out_d, cudaStream_t s);
 

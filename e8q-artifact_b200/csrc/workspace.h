@@ -67,6 +67,10 @@ struct Workspace {
     // tensor-core routing: int8 slice planes and per-row scale / norms of the
     // queries and the centroids
     DevBuf r_qplane, r_cplane, r_qmeta, r_cmeta, r_ub;
+    // pruned path: per-CTA best coarse estimates and keys, the grid-barrier
+    // and finish counters, candidate/survivor counts, per-query thresholds
+    DevBuf pr_dc, pr_key, pr_counters, pr_stats, pr_thr;
+    size_t pr_grid_cap = 0, pr_thr_cap = 0, pr_last_nq = 0;
     // tuning of the grouped paths (chosen by the autotuner): work-queue order
     // (0: longest list first, 1: list id order) and the precision scan's
     // shared-memory ring depth (4, 6 or 8 K-chunk stages)
@@ -131,6 +135,23 @@ struct Workspace {
         total_tiles.alloc(4);
         E8QC_CUDA(cudaMemset(route_counter.p, 0, 4));
         route_cap = nlist;
+    }
+    void ensure_pruned(size_t grid, size_t nq) {
+        ensure_err();
+        if (grid > pr_grid_cap) {
+            pr_dc.alloc(grid * kMaxK * 4);
+            pr_key.alloc(grid * kMaxK * 4);
+            pr_grid_cap = grid;
+        }
+        if (!pr_counters.p) {
+            pr_counters.alloc(8);
+            E8QC_CUDA(cudaMemset(pr_counters.p, 0, 8));
+            pr_stats.alloc(16);
+        }
+        if (nq > pr_thr_cap) {
+            pr_thr.alloc(nq * 4);
+            pr_thr_cap = nq;
+        }
     }
     void ensure_scan(size_t grid) {
         ensure_err();

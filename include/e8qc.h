@@ -53,6 +53,17 @@ extern "C" {
  * with the exact estimator. Distances returned are exact; recall against the
  * exact scan is measured, not guaranteed. */
 #define E8QC_MODE_PRECISION 2
+/* PRUNED is the reference's production search (E8qIndex::Search with its
+ * coarse gate, src/index/e8q_search.cpp:215-293): a coarse pass prices one
+ * rowA byte per 8-dim block against the query's u8 LUT (PrepareQuery), the
+ * zero-parallel-residual bound of the scan banks rejects vectors that cannot
+ * beat the threshold, and the survivors are scored exactly. The threshold is
+ * the k-th exact distance among the query's k best coarse estimates (fixed
+ * per query rather than the reference's running heap); the bound, its LUT and
+ * banks and prune_alpha are the reference's. With set_disable_prune every
+ * candidate is scored (the reference's plain scan). stats: candidates scanned
+ * and survivors refined. */
+#define E8QC_MODE_PRUNED 3
 
 /* Maximum top-k (include/e8qlib/index/e8q.hpp:44 kMaxK). */
 #define E8QC_MAX_K 128
@@ -76,6 +87,13 @@ typedef struct e8qc_stats {
    (the index then holds a second workspace for it, released when the shape
    changes or the index is rebuilt); its stats carry the graph's kernel count
    and its whole device time, staging copies included, as scan_us. */
+
+/* The pruning threshold of each query of the last E8QC_MODE_PRUNED search on
+ * this index (its first nq queries; +inf where pruning was off or fewer than
+ * k candidates existed): the k-th exact distance among the query's k best
+ * coarse estimates. No reference counterpart (the reference's threshold is
+ * its running heap); for checking the bound. */
+int e8qc_e8q_pruned_thresholds(e8qc_index* idx, float* out, size_t nq);
 
 typedef struct e8qc_info {
     uint64_t dim, padded_dim, n, nlist, memory_bytes;
@@ -158,7 +176,8 @@ typedef struct e8qc_profile {
     uint64_t final_bytes;    /* their algorithmic bytes: 2 per proxy distance read + per query
                                 C * (bits*padded_dim/8 + 12) for the rescored candidates */
     double prep_ms;          /* precision mode: routing + grouping (route GEMM, probe select,
-                                work items, pair scatter), summed CUDA-event time */
+                                work items, pair scatter); plain mode: the per-query routing
+                                launches; summed CUDA-event time */
 } e8qc_profile;
 int e8qc_e8q_profile(e8qc_index* idx, int enable, e8qc_profile* out);
 /* Plain search that allocates nothing (no counterpart in the reference; an

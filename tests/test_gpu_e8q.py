@@ -98,7 +98,7 @@ def test_gpu_plain_search_matches_reference(e8q, name):
     q = det_mixture(seed + 1000, nq, dim, nlist, float(g["sigma"]))[0]
     idx = e8q.E8qIndex(dim, bits, seed)
     idx.build(x, cm, lab)
-    ids, dists = idx.search(q, k, nprobe)
+    ids, dists = idx.search(q, k, nprobe, mode="plain")
     assert ids.dtype == np.uint32 and dists.dtype == np.float32 and ids.shape == (nq, k)
     assert_topk_parity(ids, dists, g["search_ids"], g["search_dists"])
     est = np.array([[idx.estimate(q[i], int(gid)) for gid in g["est_ids"][i]] for i in range(nq)],
@@ -116,7 +116,7 @@ def test_gpu_plain_search_vs_oracle(e8q, oracle_lib, dim, bits, nlist, nprobe, k
     idx = e8q.E8qIndex(dim, bits, 5)
     idx.build(x, cm, lab)
     orc = oracle_lib.OracleE8qIndex(x, cm, lab, bits, seed=5, threads=4)
-    ids, dists = idx.search(q, k, nprobe)
+    ids, dists = idx.search(q, k, nprobe, mode="plain")
     rids, rd = orc.search(q, k, nprobe, threads=4)
     assert_topk_parity(ids, dists, rids, rd)
 
@@ -136,12 +136,13 @@ def test_gpu_edge_cases(e8q, oracle_lib):
     orc = oracle_lib.OracleE8qIndex(x, cm, lab, bits, seed=1)
     q = det_normal(5, (9, dim))
     for k, nprobe in [(1, 1), (128, 100), (10, 8), (50, 1)]:
-        ids, d = idx.search(q, k, nprobe)
+        ids, d = idx.search(q, k, nprobe, mode="plain")
         rids, rd = orc.search(q, k, nprobe)
         assert_topk_parity(ids, d, rids, rd)
     # fewer candidates than k: padding
-    ids, d = idx.search(q[:2], 128, 1)
-    assert np.all(ids[np.isinf(d)] == 0xFFFFFFFF)
+    for mode in ("plain", "pruned"):
+        ids, d = idx.search(q[:2], 128, 1, mode=mode)
+        assert np.all(ids[np.isinf(d)] == 0xFFFFFFFF)
     assert idx.estimate(x[40], 40) == pytest.approx(orc.estimate(x[40], 40), rel=1e-4, abs=1e-4)
 
 

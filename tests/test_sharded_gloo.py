@@ -84,3 +84,33 @@ def test_two_rank_gloo_matches_single_index(oracle_lib):
         s.bind(("127.0.0.1", 0))
         port = s.getsockname()[1]
     mp.spawn(_worker, args=(2, port, x, cm, lab, q, k, nprobe, ref_ids, ref_d), nprocs=2, join=True)
+
+
+def test_vectorised_merges_agree():
+    """The host merge (numpy) and the device merge (torch, here on CPU
+    tensors) give the same rows: (distance, id) order, -0 == +0, negative
+    distances, padding last."""
+    import torch
+
+    from e8qlib.sharded import merge_topk_torch
+
+    rng = np.random.default_rng(4)
+    nq, m, k = 9, 3, 7
+    parts_i, parts_d = [], []
+    for r in range(m):
+        d = np.sort(rng.choice(np.array([-1.5, -0.0, 0.0, 0.25, 1.0, 2.0, np.inf], np.float32), (nq, k)), axis=1)
+        i = rng.permutation(10_000)[:nq * k].reshape(nq, k).astype(np.uint32) + np.uint32(r * 10_000)
+        i[np.isinf(d)] = UMAX
+        parts_i.append(i)
+        parts_d.append(d.astype(np.float32))
+    hi, hd = merge_topk(parts_i, parts_d, k)
+    ti = torch.from_numpy(np.concatenate(parts_i, 1).view(np.int32))
+    td = torch.from_numpy(np.concatenate(parts_d, 1))
+    di, dd = merge_topk_torch(ti, td, k)
+    assert np.array_equal(di.numpy().view(np.uint32), hi)
+    assert np.array_equal(dd.numpy(), hd + np.float32(0.0))
+    # reference order by a plain sort of (distance, id) pairs
+    for q in range(nq):
+        pairs = sorted(zip((np.concatenate(parts_d, 1)[q] + np.float32(0)).tolist(),
+                           np.concatenate(parts_i, 1)[q].tolist()))[:k]
+        assert [p[1] for p in pairs] == hi[q].tolist()
