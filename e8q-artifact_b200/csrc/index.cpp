@@ -215,18 +215,22 @@ void plain_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size_
                   uint32_t* ids_d, float* d_d, e8qc_stats* st, cudaStream_t s) {
     Workspace& ws = x->ws;
     ws.ensure_route(x->nlist);
-    // grid: one CTA per SM (the kernel fills an SM's shared memory), fewer
-    // when the largest possible probe set has fewer tiles than that
-    const ScanGeo geo = plain_scan_geo(x->view);
+    // grid: one CTA per SM (the kernel fills an SM's registers and shared
+    // memory) but one, fewer when the largest possible probe set has fewer
+    // tiles than that. The scan starts while the routing kernel's last CTA
+    // still selects the probes; that CTA's SM is the one left out, so no scan
+    // CTA waits for it.
     const size_t max_tiles = max_tiles_for(x, nprobe);
     int sms = 148;
     E8QC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device));
-    int grid = static_cast<int>(std::min<size_t>(max_tiles, static_cast<size_t>(sms)));
+    int grid = static_cast<int>(std::min<size_t>(max_tiles, static_cast<size_t>(std::max(1, sms - 1))));
     grid = std::max(grid, 1);
+    const ScanGeo geo =
+        plain_scan_geo(x->view, (max_tiles + static_cast<size_t>(grid) - 1) / static_cast<size_t>(grid));
     ws.ensure_scan(static_cast<size_t>(grid));
     RouteWork rw{ws.keys.as<uint64_t>(), ws.probes.as<uint32_t>(), ws.probe_d2.as<float>(),
                  ws.tile_off.as<uint32_t>(), ws.route_counter.as<uint32_t>(),
-                 ws.total_tiles.as<uint32_t>()};
+                 ws.total_tiles.as<uint32_t>(), ws.probe_info.as<uint2>()};
     ScanWork sw{ws.part_d.as<float>(), ws.part_id.as<uint32_t>(), ws.scan_counter.as<uint32_t>(),
                 ws.err.as<uint32_t>(), grid};
 
@@ -335,7 +339,8 @@ void pruned_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size
     ws.ensure_scan(static_cast<size_t>(grid));
     ws.ensure_pruned(static_cast<size_t>(grid), nq);
     RouteWork rw{ws.keys.as<uint64_t>(), ws.probes.as<uint32_t>(), ws.probe_d2.as<float>(),
-                 ws.tile_off.as<uint32_t>(), ws.route_counter.as<uint32_t>(), ws.total_tiles.as<uint32_t>()};
+                 ws.tile_off.as<uint32_t>(), ws.route_counter.as<uint32_t>(), ws.total_tiles.as<uint32_t>(),
+                 ws.probe_info.as<uint2>()};
     ScanWork sw{ws.part_d.as<float>(), ws.part_id.as<uint32_t>(), ws.scan_counter.as<uint32_t>(),
                 ws.err.as<uint32_t>(), grid};
     double w_cls[2];

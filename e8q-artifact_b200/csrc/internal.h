@@ -131,6 +131,7 @@ struct RouteWork {
     uint32_t* tile_off;    // nlist+1 exclusive prefix of probed tiles
     uint32_t* counter;     // last-CTA-done counter (self-resetting)
     uint32_t* total_tiles; // 1
+    uint2* probe_info;     // nlist: (first tile, vectors) of the p-th probed list
 };
 // One query: d2 to every centroid, then (last CTA) the nprobe nearest lists
 // and the prefix of their tile counts.

@@ -11,7 +11,7 @@
 // and the caller passes device buffers for the queries and the results, so
 // nothing is staged either.
 //
-// The array is a fixed 2.4 MB per device that loads the library and stays
+// The array is a fixed 3.0 MB per device that loads the library and stays
 // allocated until the process exits. Its size sets the limits checked on every
 // call: at most kNaMaxLists lists and kNaMaxPd padded dimensions. The first
 // call on a device looks up the array's device address
@@ -51,6 +51,7 @@ struct NaScratch {
     uint32_t probes[kNaMaxLists];
     float probe_d2[kNaMaxLists];
     uint32_t tile_off[kNaMaxLists + 1];
+    uint2 probe_info[kNaMaxLists];
     float rq[kNaMaxPd];
     float part_d[kNaMaxGrid * kMaxK];
     uint32_t part_id[kNaMaxGrid * kMaxK];
@@ -113,14 +114,16 @@ extern "C" int e8qc_e8q_search_plain_noalloc(e8qc_index* idx, const float* queri
         const size_t np = nprobe < nlist ? nprobe : nlist;
         int sms = 148;
         E8QC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-        int grid = static_cast<int>(max_tiles < static_cast<size_t>(sms) ? max_tiles : static_cast<size_t>(sms));
+        // one CTA per SM but one (the routing kernel's last CTA keeps its SM)
+        const size_t cap = static_cast<size_t>(sms > 1 ? sms - 1 : 1);
+        int grid = static_cast<int>(max_tiles < cap ? max_tiles : cap);
         if (grid < 1) grid = 1;
         if (grid > kNaMaxGrid) grid = kNaMaxGrid;
         // counters and the error word must start at zero on every call
         E8QC_CUDA(cudaMemsetAsync(sc->words, 0, sizeof(sc->words), s));
-        RouteWork rw{sc->keys, sc->probes, sc->probe_d2, sc->tile_off, &sc->words[0], &sc->words[2]};
+        RouteWork rw{sc->keys, sc->probes, sc->probe_d2, sc->tile_off, &sc->words[0], &sc->words[2], sc->probe_info};
         ScanWork sw{sc->part_d, sc->part_id, &sc->words[1], &sc->words[3], grid};
-        const ScanGeo geo = plain_scan_geo(view);
+        const ScanGeo geo = plain_scan_geo(view, (max_tiles + static_cast<size_t>(grid) - 1) / static_cast<size_t>(grid));
         for (size_t i = 0; i < nq; ++i) {
             launch_rotate(view, queries + i * dim, 1, sc->rq, s);
             launch_route_one(view, sc->rq, static_cast<int>(np), rw, s);

@@ -10,6 +10,7 @@
 #include "device_common.cuh"
 #include "internal.h"
 #include "scan_plain.h"
+#include "tma.cuh"
 
 namespace e8qc {
 namespace scan1 {
@@ -19,10 +20,6 @@ __device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
 constexpr int kWarps = 16;      // warps per CTA; one CTA per SM
 constexpr int kToffCap = 1024;  // tile offsets cached in shared memory
 constexpr int kSelCap = 256;    // survivors ranked by counting
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
 
 // Streaming 16-byte load: read-only, no L1 allocation (each byte is used once
 // per query).
@@ -98,19 +95,24 @@ __device__ __forceinline__ int find_probe(const uint32_t* off, int nprobe, uint3
     return lo;
 }
 
-// The k best of `nlists` sorted lists of k entries each (list L at [L*k,
-// L*k+k), padding (+inf, UINT32_MAX) at its end), written ascending to
-// od / oi (shared or global), padded when fewer exist. Threshold filter +
-// rank counting (see the file comment); returns false, having written
-// nothing, when more than kSelCap entries survive the threshold. Block-wide;
-// the caller synchronises before reusing ld / lid / sv_*.
-__device__ inline bool block_select(const float* ld, const uint32_t* lid, int nlists, int k, float* sv_d, uint32_t* sv_id,
-                             float* od, uint32_t* oi) {
-    __shared__ float s_td;
-    __shared__ uint32_t s_ti;
-    __shared__ int s_n;
+// The sharper of two upper bounds of the k-th best entry of `nlists`
+// sorted lists of k entries each (list L at [L*k, L*k+k)): the best of the
+// lists' k-th entries (that list holds k entries at or below it) and, with
+// at least k lists, the k-th best of the lists' first entries (k lists each
+// hold one). Block-wide (all threads call; the result is in every thread).
+__device__ inline void lists_threshold(const float* ld, const uint32_t* lid, int nlists, int k, float& td_out,
+                                       uint32_t& ti_out) {
+    __shared__ float s_td, s_t2d;
+    __shared__ uint32_t s_ti, s_t2i;
     const int tid = threadIdx.x, lane = tid & 31, nt = blockDim.x;
-    if (tid < 32) {
+    const int warp = tid >> 5, nw = nt >> 5;
+    if (tid == 0) {
+        s_t2d = inf_f();
+        s_t2i = 0xFFFFFFFFu;
+    }
+    __syncthreads();
+    // warp 0: the best of the lists' k-th entries
+    if (warp == 0) {
         float td = inf_f();
         uint32_t ti = 0xFFFFFFFFu;
         for (int L = lane; L < nlists; L += 32) {
@@ -127,12 +129,86 @@ __device__ inline bool block_select(const float* ld, const uint32_t* lid, int nl
         if (lane == 0) {
             s_td = td;
             s_ti = ti;
-            s_n = 0;
+        }
+    }
+    // the other warps (all, with one warp): the head whose rank among the
+    // heads is k - 1 (real heads are unique; padding heads only matter when
+    // fewer than k are real). Each warp holds all heads in registers (lane l:
+    // heads l, l + 32, ...) and ranks four of its share per step, each with a
+    // warp reduction of the lanes' counts.
+    constexpr int kHpl = 8;  // heads per lane: up to 256 lists
+    const int w0 = nw > 1 ? 1 : 0, nr = nw - w0;
+    if (nlists >= k && warp >= w0) {
+        if (nlists <= 32 * kHpl) {
+            float hd[kHpl];
+            uint32_t hi[kHpl];
+#pragma unroll
+            for (int m = 0; m < kHpl; ++m) {
+                const int L = lane + 32 * m;
+                hd[m] = L < nlists ? ld[L * k] : inf_f();
+                hi[m] = L < nlists ? lid[L * k] : 0xFFFFFFFFu;
+            }
+            for (int L0 = warp - w0; L0 < nlists; L0 += 4 * nr) {
+                int c[4] = {0, 0, 0, 0};
+                float d[4];
+                uint32_t i[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int L = L0 + u * nr;
+                    d[u] = L < nlists ? ld[L * k] : inf_f();
+                    i[u] = L < nlists ? lid[L * k] : 0xFFFFFFFFu;
+                }
+#pragma unroll
+                for (int m = 0; m < kHpl; ++m)
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) c[u] += better(hd[m], hi[m], d[u], i[u]) ? 1 : 0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int r = __reduce_add_sync(kFull, c[u]);
+                    if (lane == 0 && i[u] != 0xFFFFFFFFu && r == k - 1) {
+                        s_t2d = d[u];  // a single warp can reach this
+                        s_t2i = i[u];
+                    }
+                }
+            }
+        } else {
+            for (int L = tid - 32 * w0; L < nlists; L += 32 * nr) {
+                const float d = ld[L * k];
+                const uint32_t i = lid[L * k];
+                if (i == 0xFFFFFFFFu) continue;
+                int r = 0;
+#pragma unroll 8
+                for (int M = 0; M < nlists; ++M) r += better(ld[M * k], lid[M * k], d, i) ? 1 : 0;
+                if (r == k - 1) {
+                    s_t2d = d;  // a single thread can reach this
+                    s_t2i = i;
+                }
+            }
         }
     }
     __syncthreads();
-    const float td = s_td;
-    const uint32_t ti = s_ti;
+    td_out = s_td;
+    ti_out = s_ti;
+    if (better(s_t2d, s_t2i, td_out, ti_out)) {
+        td_out = s_t2d;
+        ti_out = s_t2i;
+    }
+}
+
+// The k best of `nlists` sorted lists of k entries each (list L at [L*k,
+// L*k+k), padding (+inf, UINT32_MAX) at its end), written ascending to
+// od / oi (shared or global), padded when fewer exist. Threshold filter +
+// rank counting (see the file comment); returns false, having written
+// nothing, when more than kSelCap entries survive the threshold. Block-wide;
+// the caller synchronises before reusing ld / lid / sv_*.
+__device__ inline bool block_select(const float* ld, const uint32_t* lid, int nlists, int k, float* sv_d, uint32_t* sv_id,
+                             float* od, uint32_t* oi) {
+    __shared__ int s_n;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    float td;
+    uint32_t ti;
+    if (tid == 0) s_n = 0;
+    lists_threshold(ld, lid, nlists, k, td, ti);
     const int total = nlists * k;
     for (int e = tid; e < total; e += nt) {
         const uint32_t i = lid[e];
@@ -152,6 +228,7 @@ __device__ inline bool block_select(const float* ld, const uint32_t* lid, int nl
         const float d = sv_d[s];
         const uint32_t i = sv_id[s];
         int r = 0;
+#pragma unroll 8
         for (int j = 0; j < S; ++j) r += better(sv_d[j], sv_id[j], d, i) ? 1 : 0;
         if (r < k) {
             od[r] = d;
@@ -215,6 +292,7 @@ __device__ inline bool block_select_g(const float* ld, const uint32_t* lid, int 
         const float d = sv_d[s];
         const uint32_t i = sv_id[s];
         int r = 0;
+#pragma unroll 8
         for (int j = 0; j < S; ++j) r += better(sv_d[j], sv_id[j], d, i) ? 1 : 0;
         if (r < k) {
             od[r] = d;

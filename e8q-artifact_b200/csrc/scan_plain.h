@@ -24,8 +24,9 @@ struct ScanGeo {
     size_t smem;
 };
 
-ScanGeo plain_scan_geo(const DevIndex& ix);
-size_t scan_smem_bytes(const DevIndex& ix, int tb_tiles);
+// max_tiles_per_cta: the most tiles any CTA of the launch can get.
+ScanGeo plain_scan_geo(const DevIndex& ix, size_t max_tiles_per_cta);
+size_t scan_smem_bytes(const DevIndex& ix, int tb_tiles, int v);
 int launch_scan_plain(const DevIndex& ix, const float* rq, const RouteWork& rw, int nprobe, int k,
                       const ScanWork& sw, const ScanGeo& geo, uint32_t* out_ids, float* out_d, cudaStream_t s);
 

@@ -8,6 +8,7 @@
 
 #include "device_common.cuh"
 #include "internal.h"
+#include "tma.cuh"
 
 namespace e8qc {
 
@@ -36,6 +37,35 @@ __device__ int block_exclusive_scan(int v, int* total, int* sm32) {
     __syncthreads();
     const int before = (warp > 0 ? sm32[warp - 1] : 0) + x - v;
     *total = sm32[nw - 1];
+    __syncthreads();
+    return before;
+}
+
+// The same over 64-bit values (two packed 32-bit counts whose sums stay
+// below 2^32 add without carries).
+__device__ unsigned long long block_exclusive_scan64(unsigned long long v, unsigned long long* total,
+                                                     unsigned long long* sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    unsigned long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sm[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned long long t = lane < nw ? sm[lane] : 0ull;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(kFull, t, o);
+            if (lane >= o) t += y;
+        }
+        sm[lane] = t;
+    }
+    __syncthreads();
+    const unsigned long long before = (warp > 0 ? sm[warp - 1] : 0ull) + x - v;
+    *total = sm[nw - 1];
     __syncthreads();
     return before;
 }
@@ -173,9 +203,258 @@ bool launch_rotate_warp(int dim, int pd, int td, const float* q, int n, float fa
 // ---------------------------------------------------------------------------
 // Top-nprobe lists of one query by 64-bit key (float bits of d2 << 32 | cid),
 // src/index/ivf_route.cpp:9-27 + src/simd/kernels.hpp:13-21. Keys are unique,
-// so an 8-pass MSB radix select finds the nprobe-th key exactly; the selected
-// lists are compacted in cid order (the plain scan's result does not depend
-// on probe order) with their tile-count prefix.
+// so an MSB radix select finds the nprobe-th key exactly; the selected lists
+// are compacted in cid order (the plain scan's result does not depend on
+// probe order) with their first tile and length, and the tile-count prefix.
+//
+// select_probes_reg: up to kRegKeys keys per thread, held in registers (thread
+// t holds keys [t * kpt, t * kpt + kpt), kpt = ceil(nlist / blockDim)); the
+// lists' first tiles and lengths are staged in shared memory (stb: nlist + 1,
+// slen: nlist) beside them, and compaction and tile prefix are one block
+// scan of each thread's (selected lists, their tiles). The nprobe-th key is
+// found by one bucket pass: 256 buckets over [min d2, max d2] (a monotone map
+// of d2, so every key of a lower bucket is smaller than every key of a
+// higher one); the keys of the bucket holding the nprobe-th are gathered and
+// ranked by counting. When that bucket holds more than kBucketCap keys (d2
+// values piled up, or not finite) an MSB radix select over the registers
+// takes over: each 8-bit pass histograms the keys that still match the
+// prefix with one shared atomic per distinct bin per warp (lanes with equal
+// bins found by __match_any_sync); the cid half of a key is below 2^16, so
+// its two top bytes need no pass.
+constexpr int kRegKeys = 16;
+constexpr int kBucketCap = 256;
+
+// Warp 0 finds the bin holding the s_want-th key of the histogram and
+// narrows the prefix (shared by both selects).
+__device__ __forceinline__ void radix_pick(const int* hist, uint64_t prefix, int shift, uint64_t* s_prefix,
+                                           int* s_want) {
+    const int lane = threadIdx.x;
+    int cnt[8], tot = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        cnt[j] = hist[lane * 8 + j];
+        tot += cnt[j];
+    }
+    int incl = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int excl = incl - tot;
+    const int want = *s_want;
+    const unsigned hit = __ballot_sync(kFull, excl < want && incl >= want);
+    const int owner = __ffs(hit) - 1;
+    if (lane == owner) {
+        int cum = excl, sel = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            if (cum + cnt[j] >= want) {
+                sel = j;
+                break;
+            }
+            cum += cnt[j];
+        }
+        *s_prefix = prefix | (static_cast<uint64_t>(lane * 8 + sel) << shift);
+        *s_want = want - cum;
+    }
+}
+
+__device__ void select_probes_reg(const DevIndex& ix, const uint64_t* gkeys, int nprobe, const RouteWork& w,
+                                  uint32_t* stb, uint32_t* slen) {
+    __shared__ int hist[256];
+    __shared__ uint64_t s_prefix;
+    __shared__ int s_want;
+    __shared__ uint32_t s_lo[32], s_hi[32];
+    __shared__ int s_bucket, s_nb, s_nc;
+    __shared__ bool s_done;
+    __shared__ unsigned long long s_cand[kBucketCap];
+    __shared__ unsigned long long sm64[32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x, nw = nt >> 5;
+    const int nlist = ix.nlist;
+    const int kpt = (nlist + nt - 1) / nt;  // keys per thread (<= kRegKeys)
+    nprobe = nprobe < nlist ? nprobe : nlist;
+    unsigned long long key[kRegKeys];
+    uint32_t lo = 0xFFFFFFFFu, hi = 0u;  // d2 bits (non-negative floats order as integers)
+#pragma unroll
+    for (int j = 0; j < kRegKeys; ++j) {
+        const int c = tid * kpt + j;
+        key[j] = (j < kpt && c < nlist) ? __ldcg(reinterpret_cast<const unsigned long long*>(gkeys) + c) : ~0ull;
+        if (j < kpt && c < nlist) {
+            const uint32_t b = static_cast<uint32_t>(key[j] >> 32);
+            lo = min(lo, b);
+            hi = max(hi, b);
+        }
+    }
+    for (int c = tid; c < nlist; c += nt) {
+        stb[c] = ix.tile_begin[c];
+        slen[c] = ix.list_len[c];
+    }
+    for (int i = tid; i < 256; i += nt) hist[i] = 0;
+    lo = __reduce_min_sync(kFull, lo);
+    hi = __reduce_max_sync(kFull, hi);
+    if (lane == 0) {
+        s_lo[warp] = lo;
+        s_hi[warp] = hi;
+    }
+    if (tid == 0) {
+        stb[nlist] = ix.tile_begin[nlist];
+        s_prefix = 0;
+        s_want = nprobe;
+        s_nc = 0;
+        s_done = false;
+    }
+    __syncthreads();
+    if (tid < 32) {
+        lo = lane < nw ? s_lo[lane] : 0xFFFFFFFFu;
+        hi = lane < nw ? s_hi[lane] : 0u;
+        lo = __reduce_min_sync(kFull, lo);
+        hi = __reduce_max_sync(kFull, hi);
+        if (lane == 0) {
+            s_lo[0] = lo;
+            s_hi[0] = hi;
+        }
+    }
+    __syncthreads();
+    lo = s_lo[0];
+    hi = s_hi[0];
+    const float flo = __uint_as_float(lo), fhi = __uint_as_float(hi);
+    // d2 is finite and >= 0 when hi < +inf; scale 0 (one bucket) when all equal
+    const bool finite = hi < 0x7F800000u;
+    const float span = __fsub_rn(fhi, flo);
+    const float scale = (finite && span > 1.0e-30f && span < 3.0e38f) ? __fdiv_rn(256.0f, span) : 0.0f;
+    auto bucket = [&](unsigned long long kk) {
+        const float d = __uint_as_float(static_cast<uint32_t>(kk >> 32));
+        const int b = static_cast<int>(__fmul_rn(__fsub_rn(d, flo), scale));
+        return b < 255 ? b : 255;
+    };
+    if (finite) {
+#pragma unroll
+        for (int j = 0; j < kRegKeys; ++j) {
+            if (j >= kpt) break;  // uniform over the block
+            if (tid * kpt + j < nlist) atomicAdd(&hist[bucket(key[j])], 1);
+        }
+    }
+    __syncthreads();
+    if (finite && tid < 32) {
+        // the bucket holding the nprobe-th key
+        int cnt[8], tot = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            cnt[j] = hist[lane * 8 + j];
+            tot += cnt[j];
+        }
+        int incl = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int excl = incl - tot;
+        const unsigned hitm = __ballot_sync(kFull, excl < nprobe && incl >= nprobe);
+        if (lane == __ffs(hitm) - 1) {
+            int cum = excl, sel = 0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (cum + cnt[j] >= nprobe) {
+                    sel = j;
+                    break;
+                }
+                cum += cnt[j];
+            }
+            s_bucket = lane * 8 + sel;
+            s_want = nprobe - cum;
+            s_nb = cnt[sel];
+        }
+    }
+    __syncthreads();
+    if (finite && s_nb <= kBucketCap) {
+        const int bs = s_bucket;
+#pragma unroll
+        for (int j = 0; j < kRegKeys; ++j) {
+            if (j >= kpt) break;
+            if (tid * kpt + j < nlist && bucket(key[j]) == bs) s_cand[atomicAdd(&s_nc, 1)] = key[j];
+        }
+        __syncthreads();
+        // the want-th smallest of the bucket's keys, by rank counting
+        const int nb = s_nc, want = s_want;
+        for (int i = tid; i < nb; i += nt) {
+            const unsigned long long x = s_cand[i];
+            int r = 0;
+#pragma unroll 8
+            for (int m = 0; m < nb; ++m) r += s_cand[m] < x ? 1 : 0;
+            if (r == want - 1) {
+                s_prefix = x;  // keys are unique: one thread
+                s_done = true;
+            }
+        }
+        __syncthreads();
+    }
+    const bool bucket_done = s_done;
+    if (!bucket_done && tid == 0) {
+        s_prefix = 0;
+        s_want = nprobe;
+    }
+    uint64_t mask = 0;
+    for (int shift = 56; shift >= 0 && !bucket_done; shift -= 8) {
+        if (shift == 24 || shift == 16) {  // cid bits 16..31: zero in every key
+            mask |= 0xFFull << shift;
+            continue;
+        }
+        for (int i = tid; i < 256; i += nt) hist[i] = 0;
+        __syncthreads();
+        const uint64_t prefix = s_prefix;
+#pragma unroll
+        for (int j = 0; j < kRegKeys; ++j) {
+            if (j >= kpt) break;  // uniform over the block
+            const int c = tid * kpt + j;
+            const bool in = c < nlist && (key[j] & mask) == prefix;
+            // lanes outside the prefix get a bin of their own (>= 256)
+            const uint32_t bin = in ? static_cast<uint32_t>((key[j] >> shift) & 255u) : 256u + lane;
+            const unsigned m = __match_any_sync(kFull, bin);
+            if (in && lane == __ffs(m) - 1) atomicAdd(&hist[bin], __popc(m));
+        }
+        __syncthreads();
+        if (tid < 32) radix_pick(hist, prefix, shift, &s_prefix, &s_want);
+        mask |= 0xFFull << shift;
+        __syncthreads();
+    }
+    const uint64_t kth = s_prefix;
+    // compact keys <= kth in cid order, with their tile offsets: one scan of
+    // (lists, tiles) per thread, then each thread writes its lists in order
+    uint32_t cnt = 0, tiles = 0;
+#pragma unroll
+    for (int j = 0; j < kRegKeys; ++j) {
+        const int c = tid * kpt + j;
+        if (j < kpt && c < nlist && key[j] <= kth) {
+            ++cnt;
+            tiles += stb[c + 1] - stb[c];
+        }
+    }
+    unsigned long long tot;
+    const unsigned long long before =
+        block_exclusive_scan64((static_cast<unsigned long long>(cnt) << 32) | tiles, &tot, sm64);
+    uint32_t pos = static_cast<uint32_t>(before >> 32), toff = static_cast<uint32_t>(before);
+#pragma unroll
+    for (int j = 0; j < kRegKeys; ++j) {
+        const int c = tid * kpt + j;
+        if (j < kpt && c < nlist && key[j] <= kth) {
+            w.probes[pos] = static_cast<uint32_t>(c);
+            w.probe_d2[pos] = __uint_as_float(static_cast<uint32_t>(key[j] >> 32));
+            w.probe_info[pos] = make_uint2(stb[c], slen[c]);
+            w.tile_off[pos] = toff;
+            ++pos;
+            toff += stb[c + 1] - stb[c];
+        }
+    }
+    if (tid == 0) {
+        w.tile_off[nprobe] = static_cast<uint32_t>(tot);
+        *w.total_tiles = static_cast<uint32_t>(tot);
+    }
+}
+
+// select_probes: any nlist; keys in shared memory when they fit (skeys),
+// else read through L2 on every pass (8 passes).
 __device__ void select_probes(const DevIndex& ix, const uint64_t* gkeys, int nprobe,
                               const RouteWork& w, unsigned long long* skeys) {
     __shared__ int hist[256];
@@ -184,7 +463,7 @@ __device__ void select_probes(const DevIndex& ix, const uint64_t* gkeys, int npr
     __shared__ int sm32[32];
     const int tid = threadIdx.x, nt = blockDim.x;
     const int nlist = ix.nlist;
-    // keys in shared memory when they fit (one coalesced pass), else L2
+    nprobe = nprobe < nlist ? nprobe : nlist;
     const unsigned long long* keys = reinterpret_cast<const unsigned long long*>(gkeys);
     if (skeys != nullptr) {
         for (int c = tid; c < nlist; c += nt) skeys[c] = __ldcg(keys + c);
@@ -205,35 +484,7 @@ __device__ void select_probes(const DevIndex& ix, const uint64_t* gkeys, int npr
             if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1);
         }
         __syncthreads();
-        if (tid < 32) {
-            // each lane owns 8 consecutive bins
-            int cnt[8], tot = 0;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                cnt[j] = hist[tid * 8 + j];
-                tot += cnt[j];
-            }
-            int incl = tot;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(kFull, incl, o);
-                if (tid >= o) incl += y;
-            }
-            const int excl = incl - tot;
-            const int want = s_want;
-            const unsigned hit = __ballot_sync(kFull, excl < want && incl >= want);
-            const int owner = __ffs(hit) - 1;
-            if (tid == owner) {
-                int cum = excl, sel = 0;
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    if (cum + cnt[j] >= want) { sel = j; break; }
-                    cum += cnt[j];
-                }
-                s_prefix = prefix | (static_cast<uint64_t>(tid * 8 + sel) << shift);
-                s_want = want - cum;
-            }
-        }
+        if (tid < 32) radix_pick(hist, prefix, shift, &s_prefix, &s_want);
         mask |= 0xFFull << shift;
         __syncthreads();
     }
@@ -254,14 +505,16 @@ __device__ void select_probes(const DevIndex& ix, const uint64_t* gkeys, int npr
         base += tot;
     }
     __syncthreads();
-    // tile prefix of the probed lists
+    // tile prefix, first tile and length of the probed lists
     int tbase = 0;
     for (int p0 = 0; p0 < nprobe; p0 += nt) {
         const int p = p0 + tid;
         int t = 0;
         if (p < nprobe) {
             const uint32_t c = __ldcg(w.probes + p);
-            t = static_cast<int>(ix.tile_begin[c + 1] - ix.tile_begin[c]);
+            const uint32_t tb = ix.tile_begin[c];
+            t = static_cast<int>(ix.tile_begin[c + 1] - tb);
+            w.probe_info[p] = make_uint2(tb, ix.list_len[c]);
         }
         int tot;
         const int pos = tbase + block_exclusive_scan(t, &tot, sm32);
@@ -284,6 +537,8 @@ __global__ void route_one_kernel(DevIndex ix, const float* __restrict__ rq, int 
     __shared__ float s_qn2;
     __shared__ bool s_last;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    // the scan launched after this one may start its own setup now
+    launch_dependents();
     const int pd = ix.pd;
     double part = 0.0;
     for (int i = tid; i < pd; i += blockDim.x) {
@@ -342,11 +597,18 @@ __global__ void route_one_kernel(DevIndex ix, const float* __restrict__ rq, int 
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    // the dynamic shared buffer (query, then free) holds the keys if they fit
-    unsigned long long* skeys =
-        (static_cast<size_t>(ix.nlist) * 8 <= s_dyn_bytes) ? reinterpret_cast<unsigned long long*>(sq) : nullptr;
+    // the dynamic shared buffer (query, then free): the lists' first tiles
+    // and lengths for the register select, else the keys if they fit
+    const int nl = ix.nlist;
     __syncthreads();
-    select_probes(ix, w.keys, nprobe, w, skeys);
+    if (nl <= kRegKeys * static_cast<int>(blockDim.x) && static_cast<size_t>(2 * nl + 8) * 4 <= s_dyn_bytes) {
+        uint32_t* stb = reinterpret_cast<uint32_t*>(sq);
+        select_probes_reg(ix, w.keys, nprobe, w, stb, stb + nl + 4);
+    } else {
+        unsigned long long* skeys =
+            (static_cast<size_t>(nl) * 8 <= s_dyn_bytes) ? reinterpret_cast<unsigned long long*>(sq) : nullptr;
+        select_probes(ix, w.keys, nprobe, w, skeys);
+    }
     if (tid == 0) *w.counter = 0;
 }
 
@@ -425,7 +687,12 @@ int launch_route_one(const DevIndex& ix, const float* rq, int nprobe, const Rout
     int grid = (ix.nlist + warps - 1) / warps;  // one centroid per warp
     grid = grid < 1 ? 1 : (grid > 1184 ? 1184 : grid);
     // dynamic shared memory: the query, reused by the last CTA for the keys
-    size_t dyn = std::max<size_t>(ix.pd * sizeof(float), std::min<size_t>(ix.nlist * 8, 64 * 1024));
+    // (up to 8 * 256 lists: their first tiles and lengths; more: the keys,
+    // up to 64 KB of them)
+    const size_t lists_bytes = ix.nlist <= static_cast<size_t>(kRegKeys) * warps * 32
+                                   ? (2 * static_cast<size_t>(ix.nlist) + 8) * 4
+                                   : std::min<size_t>(ix.nlist * 8, 64 * 1024);
+    size_t dyn = std::max<size_t>(ix.pd * sizeof(float), lists_bytes);
     if (dyn > 48 * 1024) {
         static size_t configured[64] = {};
         int dev = 0;

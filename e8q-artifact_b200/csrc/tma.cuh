@@ -76,6 +76,20 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// Invalidate an mbarrier whose phases are all complete, so its shared
+// memory can be reused for plain data.
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialisation may start while the previous kernel in the stream is still
+// running; grid_dependency_wait() blocks until that kernel has completed and
+// its memory is visible (a no-op for an ordinary launch), and
+// launch_dependents() lets the next such kernel start early.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Plain arrival (count 1) on `bar`.
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");

@@ -52,7 +52,7 @@ struct Workspace {
     DevBuf stage_q, stage_k, stage_np, stage_ids, stage_d;
     size_t rq_cap = 0;
     // plain path
-    DevBuf keys, probes, probe_d2, tile_off, route_counter, total_tiles;
+    DevBuf keys, probes, probe_d2, tile_off, probe_info, route_counter, total_tiles;
     size_t route_cap = 0;
     DevBuf part_d, part_id, scan_counter;
     size_t scan_cap = 0;
@@ -131,6 +131,7 @@ struct Workspace {
         probes.alloc(nlist * 4);
         probe_d2.alloc(nlist * 4);
         tile_off.alloc((nlist + 1) * 4);
+        probe_info.alloc(nlist * 8);
         route_counter.alloc(4);
         total_tiles.alloc(4);
         E8QC_CUDA(cudaMemset(route_counter.p, 0, 4));

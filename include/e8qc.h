@@ -186,7 +186,7 @@ int e8qc_e8q_profile(e8qc_index* idx, int enable, e8qc_profile* out);
  * caching allocator, a request handler that must not stall other streams
  * (cudaFree synchronises the device), a JNI/cgo host with a fixed memory
  * budget. Same kernels and results as e8qc_e8q_search(..., E8QC_MODE_PLAIN),
- * but the scratch is a fixed 2.4 MB static device array per device (held
+ * but the scratch is a fixed 3.0 MB static device array per device (held
  * until the process exits) and queries (nq*dim), out_ids and out_dists
  * (nq*k) must be DEVICE pointers on the index's device (else E8QC_EINVAL).
  * Limits: nlist <= 65536, padded_dim <= 4096; larger indexes return
