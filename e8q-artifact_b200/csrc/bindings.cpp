@@ -198,6 +198,13 @@ class E8qIndex {
         return out;
     }
 
+    // Fault injection (no reference counterpart): the next `searches` plain
+    // searches give up a bounded device wait and raise (E8QC_ETIMEOUT).
+    void debug_inject_wait_timeout(int searches, uint32_t wait_ms) {
+        require("debug_inject_wait_timeout");
+        check(e8qc_e8q_debug_inject_wait_timeout(idx_, searches, wait_ms));
+    }
+
     void set_disable_prune(bool on) {
         require("set_disable_prune");
         check(e8qc_e8q_set_disable_prune(idx_, on ? 1 : 0));
@@ -653,9 +660,10 @@ class Plan {
 class Server {
    public:
     Server(py::object index, const std::string& mode, size_t max_batch, size_t max_k, size_t max_nprobe,
-           size_t memory_budget, int slots)
+           size_t memory_budget, int slots, int request_timeout_ms)
         : index_(index) {
         e8qc_server_config c{};
+        c.request_timeout_ms = request_timeout_ms;
         c.max_batch_queries = max_batch;
         c.max_k = max_k;
         c.max_nprobe = max_nprobe;
@@ -715,6 +723,14 @@ class Server {
         if (!done) return py::none();
         return py::make_tuple(ids, dists);
     }
+    // Cancel a request (e8qc_server_cancel): its result() then raises unless
+    // it had already completed.
+    void cancel(uint64_t id) {
+        if (!srv_) throw std::runtime_error("server is stopped");
+        const int rc = e8qc_server_cancel(srv_, id);
+        if (rc == E8QC_ERANGE) throw py::index_error(e8qc_last_error());
+        check(rc);
+    }
     py::dict stats(bool reset) {
         if (!srv_) throw std::runtime_error("server is stopped");
         e8qc_server_stats st{};
@@ -733,6 +749,8 @@ class Server {
         d["qps"] = st.qps;
         d["mean_batch_queries"] = st.mean_batch_queries;
         d["peak_batch_bytes"] = st.peak_batch_bytes;
+        d["canceled"] = st.canceled;
+        d["expired"] = st.expired;
         return d;
     }
     void stop() {
@@ -760,6 +778,9 @@ PYBIND11_MODULE(_e8qlib, m) {
     using e8qb200::E8qIndex;
     m.doc() = "E8Q IVF search on B200 (sm_100a): the e8qlib Python API over libe8qcuda.so";
     m.def("version", [] { return e8qc_version(); });
+    // Fault injection (no reference counterpart): the next `count` checked
+    // host allocations fail (index creation, server request intake).
+    m.def("debug_fail_host_allocs", [](int count) { e8qb200::check(e8qc_debug_fail_host_allocs(count)); }, py::arg("count"));
     m.def("branch_levels", [](int bits, int branch) {
         py::array_t<double> out(static_cast<py::ssize_t>(1) << std::max(1, std::min(bits, 13)));
         e8qb200::check(e8qc_branch_levels(bits, branch, out.mutable_data()));
@@ -814,9 +835,11 @@ PYBIND11_MODULE(_e8qlib, m) {
         .def("run", &e8qb200::Plan::run, py::arg("queries"), py::arg("k"), py::arg("nprobe"));
 
     py::class_<e8qb200::Server>(m, "Server")
-        .def(py::init<py::object, const std::string&, size_t, size_t, size_t, size_t, int>(), py::arg("index"),
-             py::arg("mode") = "", py::arg("max_batch") = 4096, py::arg("max_k") = 128,
-             py::arg("max_nprobe") = 0, py::arg("memory_budget") = 0, py::arg("slots") = 2)
+        .def(py::init<py::object, const std::string&, size_t, size_t, size_t, size_t, int, int>(),
+             py::arg("index"), py::arg("mode") = "", py::arg("max_batch") = 4096, py::arg("max_k") = 128,
+             py::arg("max_nprobe") = 0, py::arg("memory_budget") = 0, py::arg("slots") = 2,
+             py::arg("request_timeout_ms") = 0)
+        .def("cancel", &e8qb200::Server::cancel, py::arg("request_id"))
         .def("submit", &e8qb200::Server::submit, py::arg("queries"), py::arg("k"), py::arg("nprobe"))
         .def("result", &e8qb200::Server::result, py::arg("request_id"), py::arg("timeout_ms") = -1)
         .def("stats", &e8qb200::Server::stats, py::arg("reset") = false)
@@ -875,6 +898,8 @@ PYBIND11_MODULE(_e8qlib, m) {
         .def("save", &E8qIndex::save, py::arg("path"))
         .def("autotune", &E8qIndex::autotune, py::arg("mode"), py::arg("nq"), py::arg("k"), py::arg("nprobe"))
         .def("set_disable_prune", &E8qIndex::set_disable_prune, py::arg("on"))
+        .def("debug_inject_wait_timeout", &E8qIndex::debug_inject_wait_timeout, py::arg("searches"),
+             py::arg("wait_ms") = 50)
         .def("set_prune_alpha", &E8qIndex::set_prune_alpha, py::arg("alpha"))
         .def("export_codes", &E8qIndex::export_codes)
         .def("profile_start", &E8qIndex::profile_start)

@@ -12,6 +12,7 @@
 #include <limits>
 #include <map>
 #include <memory>
+#include <atomic>
 #include <mutex>
 #include <random>
 #include <string>
@@ -33,6 +34,15 @@ thread_local std::string g_last_error;
 }
 
 void fail(int code, const std::string& msg) { throw Error{code, msg}; }
+
+namespace {
+std::atomic<int> g_fail_host_allocs{0};  // injected host-allocation failures left
+}  // namespace
+
+void host_alloc_point() {
+    for (int left = g_fail_host_allocs.load(); left > 0;)
+        if (g_fail_host_allocs.compare_exchange_weak(left, left - 1)) throw std::bad_alloc();
+}
 
 void cuda_check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) {
@@ -132,6 +142,10 @@ struct e8qc_index {
     Workspace ws;
     bool profiling = false;
     e8qc_profile prof{};
+    // fault injection (e8qc_e8q_debug_inject_wait_timeout): plain searches
+    // left whose scan waits on a barrier nothing completes, and the bound
+    std::atomic<int> inject_waits{0};
+    std::atomic<uint32_t> inject_wait_ms{0};
 
     size_t memory_bytes() const {
         return signs.bytes + mean_rot.bytes + cen.bytes + cn2.bytes + tile_begin_d.bytes +
@@ -248,6 +262,12 @@ void plain_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size_
         if (x->profiling) E8QC_CUDA(cudaEventRecord(er, s));
         launches += launch_route_one(x->view, rq, static_cast<int>(nprobe), rw, s);
         if (x->profiling) E8QC_CUDA(cudaEventRecord(e0, s));
+        sw.stuck_ms = 0;
+        for (int left = x->inject_waits.load(); left > 0;)
+            if (x->inject_waits.compare_exchange_weak(left, left - 1)) {
+                sw.stuck_ms = x->inject_wait_ms.load();
+                break;
+            }
         launches += launch_scan_plain(x->view, rq, rw, static_cast<int>(nprobe), static_cast<int>(k), sw,
                                       geo, ids_d + i * k, d_d + i * k, s);
         if (x->profiling) {
@@ -856,6 +876,7 @@ int e8qc_e8q_create(int device, size_t dim, int nbits, uint64_t seed, e8qc_index
         *out = nullptr;
         if (dim == 0) fail(E8QC_EINVAL, "dim must be positive");
         if (nbits < 1 || nbits > kMaxBits) fail(E8QC_EINVAL, "nbits must be in [1, 13]");
+        host_alloc_point();
         int ndev = 0;
         E8QC_CUDA(cudaGetDeviceCount(&ndev));
         if (device < 0 || device >= ndev) fail(E8QC_EINVAL, "no such CUDA device");
@@ -869,6 +890,23 @@ int e8qc_e8q_create(int device, size_t dim, int nbits, uint64_t seed, e8qc_index
         x->nch = code_chunks(static_cast<int>(x->pd), nbits);
         x->ws.device = device;
         *out = x.release();
+    });
+}
+
+int e8qc_debug_fail_host_allocs(int count) {
+    return guarded([&] {
+        if (count < 0) fail(E8QC_EINVAL, "count must be >= 0");
+        g_fail_host_allocs.store(count);
+    });
+}
+
+int e8qc_e8q_debug_inject_wait_timeout(e8qc_index* x, int searches, uint32_t wait_ms) {
+    return guarded([&] {
+        if (x == nullptr) fail(E8QC_EINVAL, "null index");
+        if (searches < 0) fail(E8QC_EINVAL, "searches must be >= 0");
+        if (searches > 0 && (wait_ms < 1 || wait_ms > 10000)) fail(E8QC_EINVAL, "wait_ms must be in [1, 10000]");
+        x->inject_wait_ms.store(wait_ms);
+        x->inject_waits.store(searches);
     });
 }
 

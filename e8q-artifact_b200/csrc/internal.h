@@ -22,6 +22,9 @@ struct Error {
     std::string msg;
 };
 [[noreturn]] void fail(int code, const std::string& msg);
+// A checked host-allocation point: throws std::bad_alloc while injected
+// failures (e8qc_debug_fail_host_allocs) remain, consuming one.
+void host_alloc_point();
 void cuda_check(cudaError_t e, const char* what);
 #define E8QC_CUDA(x) ::e8qc::cuda_check((x), #x)
 
@@ -144,6 +147,7 @@ struct ScanWork {
     uint32_t* counter;  // self-resetting
     uint32_t* err;      // device error word (bounded waits that gave up)
     int grid;
+    uint32_t stuck_ms = 0;  // test hook: CTA 0 waits this long on a barrier nothing completes
 };
 
 // Build kernels.

@@ -967,6 +967,7 @@ int e8qc_me8q_create(int device, size_t dim, float avg_bits, uint64_t seed, e8qc
         if (dim == 0) fail(E8QC_EINVAL, "dim must be positive");
         if (dim > 16384) fail(E8QC_EINVAL, "dim must be <= 16384");
         if (!(avg_bits > 0.0F)) fail(E8QC_EINVAL, "avg_bits must be positive");
+        host_alloc_point();
         int ndev = 0;
         E8QC_CUDA(cudaGetDeviceCount(&ndev));
         if (device < 0 || device >= ndev) fail(E8QC_EINVAL, "no such CUDA device");

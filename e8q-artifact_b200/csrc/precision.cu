@@ -61,9 +61,11 @@ constexpr size_t kFinalWideRows = 131072;  // select kernel: 4 warps per query f
 constexpr size_t kFinalWideBatch = 2048;   // ... and for batches below this size (too few queries to fill the GPU)
 
 // Proxy candidates rescored per query, from the query's own k (so a query's
-// result does not depend on the k of the others in its batch).
+// result does not depend on the k of the others in its batch): the top 4k
+// (at least 32) by proxy distance, up to the 128 a warp's list holds (k <= 32
+// gets its full 4k).
 __host__ __device__ constexpr int candidates_for(int k) {
-    return (3 * k > 32 ? 3 * k : 32) < kMaxK ? (3 * k > 32 ? 3 * k : 32) : kMaxK;
+    return (4 * k > 32 ? 4 * k : 32) < kMaxK ? (4 * k > 32 ? 4 * k : 32) : kMaxK;
 }
 constexpr size_t kScratchBudget = size_t(8) << 30;  // proxy rows per call chunk (bytes)
 

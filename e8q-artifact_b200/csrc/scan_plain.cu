@@ -135,8 +135,8 @@ __host__ __device__ constexpr int ring_depth(int bits, int v) {
 __host__ __device__ constexpr bool static_tab_b(int bits) { return 2 * (1 << bits) * table_rep(bits) <= kStaticTab; }
 
 // Byte offsets of the kernel's dynamic shared memory (host and device agree
-// through this one function): the warps' unit rings, their mbarriers and the
-// batch barrier; the batch's g1 / h3 / ids rows (bulk-copy destinations,
+// through this one function): the warps' unit rings, their mbarriers, the
+// batch barrier and the test-hook barrier; the batch's g1 / h3 / ids rows (bulk-copy destinations,
 // 128-byte aligned); [level table copies when not static]; query; tile
 // offsets; the batch's tiles; unit partial sums; per-warp lists; survivors.
 struct PlainCarve {
@@ -148,7 +148,7 @@ __host__ __device__ inline PlainCarve plain_carve(int bits, int v, int pd, int n
     const int ring = ring_depth(bits, v);
     size_t o = static_cast<size_t>(kWarps) * ring * v * sch * 512;
     c.bars = o;
-    o += static_cast<size_t>(kWarps * ring + 1) * 8;
+    o += static_cast<size_t>(kWarps * ring + 2) * 8;
     o = (o + 127) & ~static_cast<size_t>(127);
     c.meta = o;
     o += static_cast<size_t>(tb + 1) * 32 * 4 * 3;
@@ -193,6 +193,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) scan_plain_kernel(
     unsigned char* ring = smem;
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + cv.bars);  // kWarps*kRing ring slots, then the batch's
     uint64_t* bbar = bars + kWarps * kRing;
+    uint64_t* sbar = bbar + 1;  // the test hook's barrier (nothing completes it)
     float* s_g1 = reinterpret_cast<float*>(smem + cv.meta);  // (tb_tiles + 1) * 32 each
     float* s_h3 = s_g1 + (tb_tiles + 1) * 32;
     uint32_t* s_ids = reinterpret_cast<uint32_t*>(s_h3 + (tb_tiles + 1) * 32);
@@ -212,8 +213,15 @@ __global__ void __launch_bounds__(kWarps * 32, 1) scan_plain_kernel(
     // ---- setup that does not read the routing launch's results: with a
     // programmatic launch it overlaps the routing kernel's tail
     if (tid == 0) {
-        for (int b = 0; b < kWarps * kRing + 1; ++b) mbar_init(bars + b, 1);
+        for (int b = 0; b < kWarps * kRing + 2; ++b) mbar_init(bars + b, 1);
         fence_barrier_init();
+        if (sw.stuck_ms != 0 && blockIdx.x == 0) {
+            // test hook: a wait on a barrier nothing completes, bounded like
+            // every wait here; giving up is recorded as a wait timeout, then
+            // the phase is completed so the barrier can be invalidated
+            if (!mbar_wait_bounded(sbar, 0u, sw.stuck_ms)) atomicOr(sw.err, kErrWaitTimeout);
+            mbar_arrive(sbar);
+        }
     }
     for (int i = tid; i < pd; i += nt) sq[i] = rq[i];
     // one load per table entry, then its per-lane copies
@@ -369,7 +377,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) scan_plain_kernel(
 
     // the rings are idle: their barriers give the space back to plain data
     if (tid == 0)
-        for (int b = 0; b < kWarps * kRing + 1; ++b) mbar_inval(bars + b);
+        for (int b = 0; b < kWarps * kRing + 2; ++b) mbar_inval(bars + b);
     // CTA reduction of the warps' lists
     top.store(sm_d + warp * k, sm_id + warp * k, k);
     __syncthreads();

@@ -52,8 +52,9 @@ struct Request {
     std::vector<float> q;
     std::vector<uint32_t> ids;
     std::vector<float> d;
-    int status = 1;  // 1 pending / running, 0 done, < 0 failed
-    Clock::time_point t_submit, t_done;
+    int status = 1;  // 1 pending / running, 0 done, < 0 failed (E8QC_ECANCELED, E8QC_ETIMEOUT, ...)
+    bool canceled = false;  // canceled while its batch ran: its rows are discarded
+    Clock::time_point t_submit, t_done, deadline;
 };
 
 template <class T>
@@ -103,7 +104,7 @@ struct e8qc_server {
     std::thread dispatcher, completer;
     // stats
     uint64_t submitted = 0, rejected = 0, completed = 0, failed = 0, queries_done = 0, batches = 0,
-             batch_queries = 0, peak_bytes = 0;
+             batch_queries = 0, peak_bytes = 0, canceled = 0, expired = 0;
     std::vector<double> lat_ms;
     Clock::time_point first_submit{}, last_done{};
     bool any_submit = false;
@@ -137,7 +138,29 @@ void dispatcher_main(e8qc_server* S) {
     cudaSetDevice(S->device);
     std::unique_lock<std::mutex> lk(S->mu);
     for (;;) {
-        S->cv_dispatch.wait(lk, [&] { return S->stopping || (!S->free_slots.empty() && !S->pending.empty()); });
+        auto ready = [&] { return S->stopping || (!S->free_slots.empty() && !S->pending.empty()); };
+        if (S->cfg.request_timeout_ms > 0 && !S->pending.empty()) {
+            // wake for the earliest deadline too (the queue is in submit
+            // order, so the front's is the earliest)
+            S->cv_dispatch.wait_until(lk, S->pending.front()->deadline, ready);
+        } else {
+            S->cv_dispatch.wait(lk, ready);
+        }
+        if (S->cfg.request_timeout_ms > 0) {
+            const Clock::time_point now = Clock::now();
+            bool any = false;
+            while (!S->pending.empty() && S->pending.front()->deadline <= now) {
+                auto r = S->pending.front();
+                S->pending.pop_front();
+                r->status = E8QC_ETIMEOUT;
+                r->t_done = now;
+                ++S->expired;
+                ++S->failed;
+                any = true;
+            }
+            if (any) S->cv_done.notify_all();
+        }
+        if (!S->stopping && (S->free_slots.empty() || S->pending.empty())) continue;
         if (S->stopping) {
             S->dispatcher_done = true;
             S->cv_complete.notify_all();
@@ -208,8 +231,10 @@ void completer_main(e8qc_server* S) {
         lk.lock();
         for (auto& r : sl.reqs) {
             r->t_done = now;
-            r->status = st;
-            if (st == 0) {
+            r->status = (st == 0 && r->canceled) ? E8QC_ECANCELED : st;
+            if (r->status == E8QC_ECANCELED) {
+                ++S->canceled;
+            } else if (st == 0) {
                 ++S->completed;
                 S->queries_done += r->nq;
                 S->lat_ms.push_back(std::chrono::duration<double, std::milli>(now - r->t_submit).count());
@@ -259,6 +284,7 @@ e8qc_server* server_make(std::shared_ptr<SearchTarget> t, const e8qc_server_conf
     if (S->cfg.memory_budget == 0) S->cfg.memory_budget = size_t(4) << 30;
     if (S->cfg.slots <= 0) S->cfg.slots = 2;
     if (S->cfg.slots > 16) fail(E8QC_EINVAL, "at most 16 slots");
+    if (S->cfg.request_timeout_ms < 0) fail(E8QC_EINVAL, "request_timeout_ms must be >= 0");
     int prev = 0;
     E8QC_CUDA(cudaGetDevice(&prev));
     E8QC_CUDA(cudaSetDevice(S->device));
@@ -328,12 +354,14 @@ extern "C" int e8qc_server_submit(e8qc_server* S, const float* queries, size_t n
                 fail(E8QC_ENOMEM, "request exceeds the server's batch size or memory budget");
             }
         }
+        host_alloc_point();
         auto r = std::make_shared<Request>();
         r->nq = nq;
         r->k = k;
         r->nprobe = nprobe;
         r->q.assign(queries, queries + nq * S->dim);
         r->t_submit = Clock::now();
+        r->deadline = r->t_submit + std::chrono::milliseconds(S->cfg.request_timeout_ms);
         std::lock_guard<std::mutex> lk(S->mu);
         if (S->stopping) fail(E8QC_ESTATE, "server is stopping");
         r->id = S->next_id++;
@@ -373,8 +401,32 @@ extern "C" int e8qc_server_poll(e8qc_server* S, uint64_t id, int timeout_ms, uin
         }
     });
     if (rc != E8QC_OK) return rc;
-    if (req_status != E8QC_OK) set_last_error("the batch that carried this request failed");
+    if (req_status == E8QC_ECANCELED) set_last_error("the request was canceled");
+    else if (req_status == E8QC_ETIMEOUT) set_last_error("the request expired before a batch slot took it (request_timeout_ms)");
+    else if (req_status == E8QC_ESTATE) set_last_error("the server stopped before the request ran");
+    else if (req_status != E8QC_OK) set_last_error("the batch that carried this request failed");
     return req_status;
+}
+
+extern "C" int e8qc_server_cancel(e8qc_server* S, uint64_t id) {
+    return guard([&] {
+        if (!S) fail(E8QC_EINVAL, "null argument");
+        std::lock_guard<std::mutex> lk(S->mu);
+        auto it = S->live.find(id);
+        if (it == S->live.end()) fail(E8QC_ERANGE, "unknown or already collected request id");
+        const std::shared_ptr<Request>& r = it->second;
+        if (r->status != 1) return;  // complete: it keeps its results
+        auto pit = std::find(S->pending.begin(), S->pending.end(), r);
+        if (pit != S->pending.end()) {
+            S->pending.erase(pit);
+            r->status = E8QC_ECANCELED;
+            r->t_done = Clock::now();
+            ++S->canceled;
+            S->cv_done.notify_all();
+        } else {
+            r->canceled = true;  // in a batch on the device: resolved when it ends
+        }
+    });
 }
 
 extern "C" int e8qc_server_get_stats(e8qc_server* S, int reset, e8qc_server_stats* out) {
@@ -389,6 +441,8 @@ extern "C" int e8qc_server_get_stats(e8qc_server* S, int reset, e8qc_server_stat
         st.queries_completed = S->queries_done;
         st.batches = S->batches;
         st.peak_batch_bytes = S->peak_bytes;
+        st.canceled = S->canceled;
+        st.expired = S->expired;
         st.mean_batch_queries = S->batches ? static_cast<double>(S->batch_queries) / S->batches : 0.0;
         if (!S->lat_ms.empty()) {
             std::vector<double> v = S->lat_ms;
@@ -412,6 +466,7 @@ extern "C" int e8qc_server_get_stats(e8qc_server* S, int reset, e8qc_server_stat
         if (reset) {
             S->submitted = S->rejected = S->completed = S->failed = S->queries_done = S->batches = 0;
             S->batch_queries = S->peak_bytes = 0;
+            S->canceled = S->expired = 0;
             S->lat_ms.clear();
             S->any_submit = false;
         }

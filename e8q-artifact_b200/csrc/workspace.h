@@ -116,7 +116,7 @@ struct Workspace {
         if (*err_host != 0) {
             E8QC_CUDA(cudaMemsetAsync(err.p, 0, 4, s));
             E8QC_CUDA(cudaStreamSynchronize(s));
-            fail(E8QC_ETIMEOUT, "a bounded device wait gave up (bulk copy did not complete)");
+            fail(E8QC_ETIMEOUT, "a bounded device wait gave up (a bulk copy or barrier did not complete in time)");
         }
     }
     void ensure_queries(size_t nq, size_t pd) {

@@ -36,7 +36,8 @@ extern "C" {
 #define E8QC_ENOMEM -4   /* device or host allocation failed */
 #define E8QC_ERANGE -5   /* unknown id: std::out_of_range / invalid_argument */
 #define E8QC_EIO -6      /* file I/O or format error */
-#define E8QC_ETIMEOUT -7 /* a bounded device wait gave up */
+#define E8QC_ETIMEOUT -7 /* a bounded device wait gave up, or a served request expired */
+#define E8QC_ECANCELED -8 /* a served request was canceled (e8qc_server_cancel) */
 
 /* Search modes. PLAIN is the drop-in: one query per launch sequence
  * (rotate -> route -> streaming scan -> top-k), every candidate of every probed
@@ -49,7 +50,7 @@ extern "C" {
  * batch grouped by list as in BATCHED, but candidates are generated on the
  * INT8 tensor cores from an int8 plane of every vector's levels (built on the
  * first precision search, padded_dim bytes per vector) and int8 queries; each
- * query's best max(32, 3k) (at most 128) proxy candidates are then rescored
+ * query's best max(32, 4k) (at most 128) proxy candidates are then rescored
  * with the exact estimator. Distances returned are exact; recall against the
  * exact scan is measured, not guaranteed. */
 #define E8QC_MODE_PRECISION 2
@@ -269,7 +270,7 @@ int e8qc_me8q_search(e8qc_me8q* idx, const float* queries, size_t nq, size_t k, 
  * scored with the estimator); E8QC_MODE_PRECISION generates candidates on the
  * INT8 tensor cores from an int8 plane of each vector's levels scaled by its
  * per-run coef (one scale per vector; built on first use, padded_dim bytes
- * per vector) and rescores each query's best max(32, 3k) (at most 128) with
+ * per vector) and rescores each query's best max(32, 4k) (at most 128) with
  * the reference's estimator: returned distances are exact, recall against the
  * exact scan is measured. */
 int e8qc_me8q_search_mode(e8qc_me8q* idx, const float* queries, size_t nq, size_t k, size_t nprobe, int mode,
@@ -359,6 +360,8 @@ typedef struct e8qc_server_config {
     size_t max_nprobe;        /* largest nprobe a request may ask for (0 = nlist) */
     size_t memory_budget;     /* device scratch bytes one batch may use (0 = 4 GiB) */
     int slots;                /* batches in flight (0 = 2) */
+    int request_timeout_ms;   /* a request not admitted to a batch within this many ms of its
+                                 submit fails with E8QC_ETIMEOUT (0 = no limit) */
 } e8qc_server_config;
 typedef struct e8qc_server_stats {
     uint64_t submitted, rejected, completed, failed, queries_completed, batches;
@@ -366,6 +369,7 @@ typedef struct e8qc_server_stats {
     double qps;                             /* queries completed / (last completion - first submit) */
     double mean_batch_queries;
     uint64_t peak_batch_bytes;              /* largest admitted batch estimate */
+    uint64_t canceled, expired;             /* requests canceled / expired before admission */
 } e8qc_server_stats;
 int e8qc_server_start(e8qc_index* idx, const e8qc_server_config* cfg, e8qc_server** out);
 /* The serving loop over an ME8Q index (cfg->mode E8QC_MODE_BATCHED or
@@ -383,11 +387,34 @@ int e8qc_server_submit(e8qc_server* srv, const float* queries, size_t nq, size_t
  * timeout. E8QC_ERANGE for an unknown or already collected id. */
 int e8qc_server_poll(e8qc_server* srv, uint64_t request_id, int timeout_ms, uint32_t* out_ids, float* out_dists,
                      int* done);
+/* Cancel a request. One still waiting for admission leaves the queue and
+ * completes at once with E8QC_ECANCELED; one already in a batch on the device
+ * completes with E8QC_ECANCELED when its batch ends (its rows are discarded);
+ * one already complete keeps its results. The request is still collected with
+ * e8qc_server_poll. E8QC_ERANGE for an unknown or already collected id. */
+int e8qc_server_cancel(e8qc_server* srv, uint64_t request_id);
 /* Counters and latency percentiles; reset = 1 clears them after the read. */
 int e8qc_server_get_stats(e8qc_server* srv, int reset, e8qc_server_stats* out);
 /* Stop accepting requests, finish the batches in flight, fail the requests
  * still pending (E8QC_ESTATE), join the threads and free the server. */
 int e8qc_server_stop(e8qc_server* srv);
+
+/* ---- Fault injection for callers' error paths (no reference counterpart) ----
+ * Failures these calls provoke are made on the host or by a bounded device
+ * wait; none of them faults, traps or hangs the GPU. */
+/* The next `count` host allocations at the library's checked points --
+ * creating an index (e8qc_e8q_create, e8qc_me8q_create) and taking in a
+ * served request (e8qc_server_submit) -- fail as if the host were out of
+ * memory: the call returns E8QC_ENOMEM and changes nothing. Process-wide;
+ * count 0 clears it. */
+int e8qc_debug_fail_host_allocs(int count);
+/* The next `searches` plain searches of this index make their scan kernel
+ * wait, bounded by wait_ms (1..10000), on a device barrier that nothing
+ * completes -- the path a bulk copy that never lands would take. The wait
+ * gives up, the kernel records it in the index's device error word, and the
+ * search returns E8QC_ETIMEOUT; the index stays usable and later searches run
+ * normally. searches 0 clears it. */
+int e8qc_e8q_debug_inject_wait_timeout(e8qc_index* idx, int searches, uint32_t wait_ms);
 
 #ifdef __cplusplus
 }
