@@ -79,6 +79,12 @@ def parse():
     ap.add_argument("--me8q-nlist", type=int, default=4096)
     ap.add_argument("--me8q-avg-bits", default="4,6", help="comma-separated avg_bits values")
     ap.add_argument("--me8q-nprobes", default="32,64,128,256,512")
+    ap.add_argument("--me8q-lloyd", type=int, default=3, help="Lloyd steps refining the ME8Q lists")
+    ap.add_argument("--spectrum", type=float, default=0.5, help="per-dimension variance lambda_i ~ i^-spectrum")
+    ap.add_argument("--sigma", type=float, default=0.4, help="within-component standard deviation")
+    ap.add_argument("--sweep", action="store_true",
+                    help="instead of the bench line: nbits x nprobe grid, batch sizes and the 100k x 128 "
+                         "config, one JSON line")
     return ap.parse_args()
 
 
@@ -113,7 +119,7 @@ def int8_peak(device):
 
 def workload_name(a):
     return (f"E8Q IVF search, {a.n // 1000}k x {a.dim}-d Gaussian mixture ({a.nlist} lists, "
-            f"lambda_i ~ i^-0.5), nbits={a.nbits}, k={a.k}, nprobe={a.nprobe}, "
+            f"sigma {a.sigma}, lambda_i ~ i^-{a.spectrum}), nbits={a.nbits}, k={a.k}, nprobe={a.nprobe}, "
             f"query batch {a.batch}")
 
 
@@ -123,7 +129,7 @@ def gen_data(a, device, rank):
 
     g = torch.Generator(device=device)
     g.manual_seed(1000 + a.seed)
-    lam = torch.arange(1, a.dim + 1, device=device, dtype=torch.float64) ** -0.5
+    lam = torch.arange(1, a.dim + 1, device=device, dtype=torch.float64) ** -getattr(a, "spectrum", 0.5)
     lam = lam / lam.mean()
     s = lam.sqrt().float()
     cen = torch.randn(a.nlist, a.dim, generator=g, device=device) * s
@@ -132,7 +138,7 @@ def gen_data(a, device, rank):
     step = 1 << 18
     for i in range(0, a.n, step):
         j = min(a.n, i + step)
-        x[i:j] = cen[lab[i:j]] + 0.4 * torch.randn(j - i, a.dim, generator=g, device=device) * s
+        x[i:j] = cen[lab[i:j]] + getattr(a, "sigma", 0.4) * torch.randn(j - i, a.dim, generator=g, device=device) * s
     cm = torch.zeros(a.nlist, a.dim, device=device, dtype=torch.float64)
     cm.index_add_(0, lab, x.double())
     cnt = torch.bincount(lab, minlength=a.nlist).clamp_min(1).double()
@@ -140,7 +146,7 @@ def gen_data(a, device, rank):
     gq = torch.Generator(device=device)
     gq.manual_seed(2000 + a.seed + 7919 * rank)
     lq = torch.randint(0, a.nlist, (a.pool,), generator=gq, device=device)
-    q = cen[lq] + 0.4 * torch.randn(a.pool, a.dim, generator=gq, device=device) * s
+    q = cen[lq] + getattr(a, "sigma", 0.4) * torch.randn(a.pool, a.dim, generator=gq, device=device) * s
     return x.contiguous(), cm.contiguous(), lab.to(torch.int32).contiguous(), q.contiguous()
 
 
@@ -461,7 +467,8 @@ def gen_me8q(a, device):
     """ME8Q workload on `device`: z ~ N(0, diag(i^-0.8)), x = normalise(R z)
     with a seeded Haar rotation R (QR of a Gaussian); full-rank PCA (fp64
     covariance + eigh) gives the base, queries and per-dimension variance the
-    index is built on; lists from 4,096 seeded rows refined by 3 Lloyd steps.
+    index is built on; lists from 4,096 seeded rows refined by --me8q-lloyd
+    Lloyd steps.
     Returns (x_raw, base_pca, q_raw, q_pca, variance, centroids, labels)."""
     import torch
 
@@ -500,7 +507,7 @@ def gen_me8q(a, device):
     for i in range(0, n, 1 << 20):
         xp[i:i + (1 << 20)] = (x[i:i + (1 << 20)] - meanf) @ V
     qp = ((q - meanf) @ V).contiguous()
-    # lists: seeded rows, 3 Lloyd steps, final assignment
+    # lists: seeded rows, Lloyd steps, final assignment
     cen = xp[torch.randperm(n, generator=g, device=device)[:nl]].clone()
     lab = torch.empty(n, dtype=torch.int64, device=device)
 
@@ -510,7 +517,7 @@ def gen_me8q(a, device):
             blk = xp[i:i + (1 << 18)]
             lab[i:i + (1 << 18)] = torch.argmin(cn[None, :] - 2.0 * blk @ cen.T, dim=1)
 
-    for _ in range(3):
+    for _ in range(getattr(a, "me8q_lloyd", 3)):
         assign()
         acc = torch.zeros(nl, d, device=device, dtype=torch.float64)
         for i in range(0, n, 1 << 20):
@@ -658,15 +665,129 @@ def me8q_leg(a, e8qlib, dev, local, stream):
         cpu = me8q_cpu_baseline(xp_host, cen.cpu().numpy(), lab.cpu().numpy(), var.cpu().numpy(),
                                 qp[:a.gt].cpu().numpy(), served["avg_bits"], serve_np, n, nl)
     out = {"workload": (f"ME8Q IVF search, {n // 1000}k x {d}-d unit vectors (spectrum i^-0.8, Haar rotation, "
-                        f"full-rank PCA), {nl} lists (3 Lloyd steps), k=10, query batch {nb}"),
+                        f"full-rank PCA), {nl} lists ({a.me8q_lloyd} Lloyd steps), k=10, query batch {nb}"),
            "gen_s": round(gen_s, 2), "rates": rates, "serving": serving, "cpu_baseline": cpu}
     del serve_idx, qp, q, cen, lab, var
     torch.cuda.empty_cache()
     return out
 
 
+def run_sweep(a):
+    """--sweep: the configurations beside the headline, each measured the way
+    the bench line is (device-resident CUDA-event timing after warm-up):
+      * the 1M x 960 mixture at nbits {2, 4, 6} x nprobe {16, 64, 256}:
+        recall@10 of the plain and precision paths against FP64 ground truth,
+        plain (one query per launch), pruned (one query per launch), batched
+        and precision (batch 4096) QPS, and the plain scan's HBM fraction;
+      * nbits 6, nprobe 64: the batched and precision paths at query batches
+        1 ... 4096;
+      * the 100k x 128 mixture of 256 lists (sigma 0.5, flat spectrum, nbits 4,
+        nprobe 16): the same paths, and the reference's CPU search on this
+        host's cores.
+    One JSON line."""
+    import copy
+
+    import torch
+
+    import e8qlib
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    pk, pk_kind = peaks()
+    peak = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
+
+    def ev_time(fn, reps):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def measure(b, idx, q, gt, nprobe, batches=(4096,), with_plain=True):
+        row = {"nbits": b.nbits, "nprobe": nprobe}
+        ng = gt.shape[0]
+        qn = q[:ng].cpu().numpy()
+        ids, _ = idx.search(qn, b.k, nprobe, mode="plain")
+        row["recall_plain"] = round(recall_at(ids, gt, b.k), 4)
+        ids, _ = idx.search(qn, b.k, nprobe, mode="precision")
+        row["recall_precision"] = round(recall_at(ids, gt, b.k), 4)
+        ids, _ = idx.search(qn, b.k, nprobe, mode="pruned")
+        row["recall_pruned"] = round(recall_at(ids, gt, b.k), 4)
+        nmax = max(max(batches), 256)
+        oi = torch.empty(nmax, b.k, dtype=torch.int32, device=dev)
+        od = torch.empty(nmax, b.k, dtype=torch.float32, device=dev)
+        if with_plain:
+            for mode in ("plain", "pruned"):
+                ms = ev_time(lambda: idx.search_ptr(q.data_ptr(), 256, b.k, nprobe, oi.data_ptr(), od.data_ptr(),
+                                                    mode, sp), 2)
+                row[mode + "_qps"] = round(256 / (ms / 1000.0), 1)
+            idx.profile_start()
+            idx.search_ptr(q[256:].data_ptr(), 64, b.k, nprobe, oi.data_ptr(), od.data_ptr(), "plain", sp)
+            torch.cuda.synchronize()
+            pr = plain_roofline(idx.profile_stop(), b, peak, pk_kind)
+            row["plain_scan_frac"] = pr["frac"]
+            row["plain_scan_us"] = pr["launch_us"]
+        for mode in ("batched", "precision"):
+            for nb in batches:
+                reps = 5 if nb >= 256 else 20
+                ms = ev_time(lambda: idx.search_ptr(q.data_ptr(), nb, b.k, nprobe, oi.data_ptr(), od.data_ptr(),
+                                                    mode, sp), reps)
+                key = f"{mode}_qps" if len(batches) == 1 else f"{mode}_qps_b{nb}"
+                row[key] = round(nb / (ms / 1000.0), 1)
+        return row
+
+    out = {"sweep": "1M x 960 mixture (sigma 0.4, lambda_i ~ i^-0.5), k=10", "grid": [], "batch_sweep": None,
+           "config1": None, "peak_hbm_gbs": peak, "peak_kind": pk_kind}
+    b = copy.copy(a)
+    b.n, b.dim, b.nlist, b.k, b.pool = 1_000_000, 960, 1024, 10, 4096
+    b.spectrum, b.sigma = 0.5, 0.4
+    x, cm, lab, q = gen_data(b, dev, 0)
+    gt = ground_truth(x, q[:500], b.k)
+    for nbits in (2, 4, 6):
+        b.nbits = nbits
+        idx = e8qlib.E8qIndex(b.dim, nbits, b.seed, device=0)
+        idx.build_ptr(x.data_ptr(), b.n, cm.data_ptr(), b.nlist, lab.data_ptr(), 0.0, sp)
+        torch.cuda.synchronize()
+        for nprobe in (16, 64, 256):
+            out["grid"].append(measure(b, idx, q, gt, nprobe))
+        if nbits == 6:
+            out["batch_sweep"] = measure(b, idx, q, gt, 64, batches=(1, 16, 64, 256, 1024, 4096), with_plain=False)
+        del idx
+        torch.cuda.empty_cache()
+    del x, cm, lab, q
+    torch.cuda.empty_cache()
+
+    # 100k x 128, 256 lists, sigma 0.5, flat spectrum
+    c = copy.copy(a)
+    c.n, c.dim, c.nlist, c.k, c.nbits, c.pool, c.seed = 100_000, 128, 256, 10, 4, 4096, 0
+    c.spectrum, c.sigma, c.nprobe = 0.0, 0.5, 16
+    x, cm, lab, q = gen_data(c, dev, 0)
+    gt = ground_truth(x, q[:1000], c.k)
+    idx = e8qlib.E8qIndex(c.dim, c.nbits, c.seed, device=0)
+    idx.build_ptr(x.data_ptr(), c.n, cm.data_ptr(), c.nlist, lab.data_ptr(), 0.0, sp)
+    torch.cuda.synchronize()
+    row = measure(c, idx, q, gt, 16, batches=(1024,))
+    row["workload"] = workload_name(c)
+    cb = cpu_baseline(c, x.cpu().numpy(), cm.cpu().numpy(), lab.cpu().numpy(), q.cpu().numpy(), gt)
+    if cb is not None:
+        row["cpu_reference"] = {"pruned_qps": round(cb["pruned_qps"], 1), "plain_qps": round(cb["plain_qps"], 1),
+                                "recall_pruned": round(cb["pruned_recall"], 4), "cores": cb["cores"],
+                                "cpu_model": cb["cpu_model"]}
+    out["config1"] = row
+    print(json.dumps(out), flush=True)
+
+
 def main():
     a = parse()
+    if a.sweep:
+        return run_sweep(a)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -198,6 +198,33 @@ class E8qIndex {
         return out;
     }
 
+    // E8qIndex.probe_bound_w (e8q_bindings.cpp:182-233): the bound's
+    // normalised discrepancy per (query, stored vector) pair, on the GPU.
+    py::array_t<double> probe_bound_w(py::handle queries, py::handle base_rows, py::handle qidx, py::handle ids,
+                                      size_t /*num_threads*/) {
+        if (!built_ || idx_ == nullptr)
+            throw std::runtime_error("E8qIndex must be built or loaded before probe_bound_w");
+        auto q = ensure_nd<float>(queries, "queries", 2);
+        auto b = ensure_nd<float>(base_rows, "base_rows", 2);
+        auto qi = ensure_nd<uint32_t>(qidx, "qidx", 1);
+        auto ii = ensure_nd<uint32_t>(ids, "ids", 1);
+        if (static_cast<size_t>(q.shape(1)) != dim_)
+            throw std::invalid_argument("queries dimension does not match index dim");
+        if (static_cast<size_t>(b.shape(1)) != dim_)
+            throw std::invalid_argument("base_rows dimension does not match index dim");
+        const size_t m = static_cast<size_t>(ii.shape(0));
+        if (static_cast<size_t>(qi.shape(0)) != m || static_cast<size_t>(b.shape(0)) != m)
+            throw std::invalid_argument("qidx, ids and base_rows must have the same length");
+        py::array_t<double> out(static_cast<py::ssize_t>(m));
+        const size_t nq = static_cast<size_t>(q.shape(0));
+        {
+            py::gil_scoped_release nogil;
+            check(e8qc_e8q_probe_bound_w(idx_, q.data(), nq, b.data(), qi.data(), ii.data(), m,
+                                         out.mutable_data()));
+        }
+        return out;
+    }
+
     // Fault injection (no reference counterpart): the next `searches` plain
     // searches give up a bounded device wait and raise (E8QC_ETIMEOUT).
     void debug_inject_wait_timeout(int searches, uint32_t wait_ms) {
@@ -898,6 +925,8 @@ PYBIND11_MODULE(_e8qlib, m) {
         .def("save", &E8qIndex::save, py::arg("path"))
         .def("autotune", &E8qIndex::autotune, py::arg("mode"), py::arg("nq"), py::arg("k"), py::arg("nprobe"))
         .def("set_disable_prune", &E8qIndex::set_disable_prune, py::arg("on"))
+        .def("probe_bound_w", &E8qIndex::probe_bound_w, py::arg("queries"), py::arg("base"), py::arg("qidx"),
+             py::arg("ids"), py::arg("num_threads") = 1)
         .def("debug_inject_wait_timeout", &E8qIndex::debug_inject_wait_timeout, py::arg("searches"),
              py::arg("wait_ms") = 50)
         .def("set_prune_alpha", &E8qIndex::set_prune_alpha, py::arg("alpha"))

@@ -1254,6 +1254,74 @@ int e8qc_e8q_estimate(e8qc_index* x, const float* query, uint32_t id, float* out
     });
 }
 
+int e8qc_e8q_probe_bound_w(e8qc_index* x, const float* queries, size_t nq, const float* base_rows,
+                           const uint32_t* qidx, const uint32_t* ids, size_t m, double* out) {
+    return guarded([&] {
+        require_built(x, "probe_bound_w");
+        if (m == 0) return;
+        if (!queries || !base_rows || !qidx || !ids || !out) fail(E8QC_EINVAL, "null buffer");
+        std::lock_guard<std::mutex> lock(x->mu);
+        if (x->inv_pos.size() != x->n) {
+            x->inv_pos.assign(x->n, 0xFFFFFFFFu);
+            for (size_t i = 0; i < x->n; ++i) x->inv_pos[x->ids_compact[i]] = static_cast<uint32_t>(i);
+        }
+        DeviceGuard g(x->device);
+        cudaStream_t s = nullptr;
+        // per pair: the stored vector's slot and list (UINT32_MAX: NaN, as the
+        // reference's binding for a query or id out of range)
+        std::vector<uint32_t> qi(m), ids_h(m), slot(m, 0xFFFFFFFFu), list(m, 0);
+        E8QC_CUDA(cudaMemcpy(qi.data(), qidx, m * 4, cudaMemcpyDefault));
+        E8QC_CUDA(cudaMemcpy(ids_h.data(), ids, m * 4, cudaMemcpyDefault));
+        for (size_t i = 0; i < m; ++i) {
+            const uint32_t id = ids_h[i];
+            if (qi[i] >= nq || id >= x->n || x->inv_pos[id] == 0xFFFFFFFFu) {
+                qi[i] = 0;
+                continue;
+            }
+            const uint64_t pos = x->inv_pos[id];
+            const size_t c = static_cast<size_t>(
+                std::upper_bound(x->list_begin.begin() + 1, x->list_begin.end(), pos) - x->list_begin.begin() - 1);
+            slot[i] = x->tile_begin[c] * 32 + static_cast<uint32_t>(pos - x->list_begin[c]);
+            list[i] = static_cast<uint32_t>(c);
+        }
+        // levels / sqrt(Dpad) of both branches and the scan basis (class means,
+        // zero for dim 7 at 1 bit), in double
+        const int q = 1 << x->bits;
+        const double rd = std::sqrt(static_cast<double>(x->pd));
+        std::vector<double> tabs(2 * static_cast<size_t>(q) + 16);
+        for (int br = 0; br < 2; ++br) {
+            const std::vector<double> lev = branch_levels(x->bits, br);
+            for (int d = 0; d < q; ++d) tabs[static_cast<size_t>(br) * q + d] = lev[d] / rd;
+        }
+        double w_cls[2];
+        scan_class_means(x->bits, w_cls);
+        for (int d = 0; d < 8; ++d) {
+            tabs[2 * q + 2 * d] = (x->bits == 1 && d == 7) ? 0.0 : w_cls[0];
+            tabs[2 * q + 2 * d + 1] = (x->bits == 1 && d == 7) ? 0.0 : w_cls[1];
+        }
+        DevBuf tq, tb, rqd, rxd, meta, tabd, outd;
+        const float* qd = stage_in(queries, nq * x->dim, tq, s);
+        const float* bd = stage_in(base_rows, m * x->dim, tb, s);
+        rqd.alloc(std::max<size_t>(nq, 1) * x->pd * 4);
+        rxd.alloc(m * x->pd * 4);
+        if (nq > 0) launch_rotate(x->view, qd, static_cast<int>(nq), rqd.as<float>(), s);
+        launch_rotate(x->view, bd, static_cast<int>(m), rxd.as<float>(), s);
+        meta.alloc(m * 12);
+        uint32_t* md = meta.as<uint32_t>();
+        E8QC_CUDA(cudaMemcpyAsync(md, qi.data(), m * 4, cudaMemcpyHostToDevice, s));
+        E8QC_CUDA(cudaMemcpyAsync(md + m, slot.data(), m * 4, cudaMemcpyHostToDevice, s));
+        E8QC_CUDA(cudaMemcpyAsync(md + 2 * m, list.data(), m * 4, cudaMemcpyHostToDevice, s));
+        tabd.alloc(tabs.size() * 8);
+        E8QC_CUDA(cudaMemcpyAsync(tabd.p, tabs.data(), tabs.size() * 8, cudaMemcpyHostToDevice, s));
+        outd.alloc(m * 8);
+        launch_probe_bound(x->view, rqd.as<float>(), rxd.as<float>(), md, md + m, md + 2 * m, tabd.as<double>(),
+                           tabd.as<double>() + 2 * q, static_cast<int>(m), static_cast<int>(x->dim),
+                           outd.as<double>(), s);
+        E8QC_CUDA(cudaMemcpyAsync(out, outd.p, m * 8, cudaMemcpyDefault, s));
+        E8QC_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
 int e8qc_e8q_set_disable_prune(e8qc_index* x, int on) {
     return guarded([&] {
         require_built(x, "set_disable_prune");

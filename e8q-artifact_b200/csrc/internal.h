@@ -178,6 +178,11 @@ int launch_me8q_encode(const DevEncTables& et, const float* rr, int pd, const do
 int launch_decode(const DevIndex& ix, int ntiles, const uint32_t* list_of_tile,
                   const uint64_t* list_begin, uint16_t* digits, uint8_t* branch, cudaStream_t s);
 // Estimate one stored vector at tile slot `slot` of list `list`.
+// ProbeBoundW of m (query, stored vector) pairs (rotated, centred queries rq
+// and base rows rx; slot_of UINT32_MAX marks an invalid pair -> NaN).
+int launch_probe_bound(const DevIndex& ix, const float* rq, const float* rx, const uint32_t* qsel,
+                       const uint32_t* slot_of, const uint32_t* list_of, const double* dlev, const double* mid, int m,
+                       int dim, double* out, cudaStream_t s);
 int launch_estimate(const DevIndex& ix, const float* rq, int list, uint32_t slot, float* out,
                     cudaStream_t s);
 

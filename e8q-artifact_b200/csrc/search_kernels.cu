@@ -656,6 +656,125 @@ __global__ void estimate_kernel(DevIndex ix, const float* __restrict__ rq, int l
     *out = __fmaf_rn(-__fmul_rn(2.0f, ix.g1[s]), S, __fadd_rn(d2, ix.h3[s]));
 }
 
+// ProbeBoundW (src/index/e8q_oracle.cpp:103-218), one warp per (query,
+// stored vector) pair, every term in fp64: the rotated, centred query and the
+// vector's raw row against the list centroid (d2, the residual's norm and
+// direction), the exact reconstruction (levels / sqrt(Dpad)) and the scan
+// basis (class means, `mid`: 2 per digit position) of the stored code, and the
+// normalised discrepancy of the zero-parallel-residual bound. The digits are
+// those the reference's 8-bit split decoder returns (e8q_scan.cpp:34-60 as
+// called there): at 1 bit digit 7 reads the branch and the branch reads 0; at
+// 9 bits and up each digit keeps its low 8 bits. Sums run per lane, then a
+// warp reduction (the reference sums in dimension order: results agree to
+// ~1e-12 relative).
+template <int BITS>
+__global__ void probe_bound_kernel(DevIndex ix, const float* __restrict__ rq, const float* __restrict__ rx,
+                                   const uint32_t* __restrict__ qsel, const uint32_t* __restrict__ slot_of,
+                                   const uint32_t* __restrict__ list_of, const double* __restrict__ dlev,
+                                   const double* __restrict__ mid, int m, int dim, double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int pair = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (pair >= m) return;
+    const double qnan = __longlong_as_double(0x7ff8000000000000ll);
+    const uint32_t slot = slot_of[pair];
+    if (slot == 0xFFFFFFFFu) {
+        if (lane == 0) out[pair] = qnan;
+        return;
+    }
+    const int pd = ix.pd;
+    const float* cc = ix.cen + static_cast<size_t>(list_of[pair]) * pd;
+    const float* q = rq + static_cast<size_t>(qsel[pair]) * pd;
+    const float* xr = rx + static_cast<size_t>(pair) * pd;
+    auto wsum = [](double v) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+        return v;
+    };
+    double d2 = 0.0, rn2 = 0.0;
+    for (int d = lane; d < pd; d += 32) {
+        const double a = static_cast<double>(q[d]) - static_cast<double>(cc[d]);
+        const double b = static_cast<double>(xr[d]) - static_cast<double>(cc[d]);
+        d2 += a * a;
+        rn2 += b * b;
+    }
+    d2 = wsum(d2);
+    rn2 = wsum(rn2);
+    const double rn = sqrt(rn2);
+    if (!(rn > 0.0)) {
+        if (lane == 0) out[pair] = qnan;
+        return;
+    }
+    constexpr int Q = 1 << BITS;
+    const uint4* tile = ix.codes + static_cast<size_t>(slot / 32) * ix.nch * 32;
+    const int vl = static_cast<int>(slot % 32);
+    double dot_ue = 0, n2_e = 0, dot_ce = 0, dot_ew = 0, dot_uw = 0, n2_w = 0, dot_cw = 0, s_exact = 0,
+           s_coarse = 0;
+    for (int blk = lane; blk < ix.B; blk += 32) {
+        const int off = blk * 8 * BITS;
+        uint32_t words[5];
+        for (int j = 0; j < 5; ++j) {
+            const int wi = (off >> 5) + j;
+            const int c = wi >> 2;
+            if (c < ix.nch) {
+                const uint4 v = tile[c * 32 + vl];
+                const uint32_t arr[4] = {v.x, v.y, v.z, v.w};
+                words[j] = arr[wi & 3];
+            } else {
+                words[j] = 0;
+            }
+        }
+        uint32_t dg[8];
+        int br = decode_block<BITS>(words, off & 31, dg);
+        if (BITS == 1) {
+            dg[7] = static_cast<uint32_t>(br);
+            br = 0;
+        } else if (BITS >= 9) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) dg[k] &= 0xFFu;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int idx = blk * 8 + k;
+            const double ve = dlev[br * Q + static_cast<int>(dg[k])];
+            const double wc = mid[2 * k + static_cast<int>(dg[k] >> (BITS - 1))];
+            const double c0 = static_cast<double>(cc[idx]);
+            const double u = (static_cast<double>(xr[idx]) - c0) / rn;
+            dot_ue += u * ve;
+            n2_e += ve * ve;
+            dot_ce += c0 * ve;
+            dot_ew += ve * wc;
+            dot_uw += u * wc;
+            n2_w += wc * wc;
+            dot_cw += c0 * wc;
+            s_exact += static_cast<double>(q[idx]) * ve;
+            s_coarse += static_cast<double>(q[idx]) * wc;
+        }
+    }
+    dot_ue = wsum(dot_ue);
+    n2_e = wsum(n2_e);
+    dot_ce = wsum(dot_ce);
+    dot_ew = wsum(dot_ew);
+    dot_uw = wsum(dot_uw);
+    n2_w = wsum(n2_w);
+    dot_cw = wsum(dot_cw);
+    s_exact = wsum(s_exact);
+    s_coarse = wsum(s_coarse);
+    if (lane != 0) return;
+    double r = qnan;
+    if (fabs(dot_ue) > 0.0 && fabs(dot_uw) > 0.0) {
+        const double g1 = rn / dot_ue;
+        const double h3 = rn2 + 2.0 * g1 * dot_ce;
+        const double d_full = d2 + h3 - 2.0 * g1 * s_exact;
+        const double w_x = 2.0 * rn / dot_uw;
+        const double d_coarse = d2 + rn2 + w_x * dot_cw - w_x * s_coarse;
+        const double rx2 = 4.0 * g1 * g1 * n2_e + w_x * w_x * n2_w - 4.0 * g1 * w_x * dot_ew;
+        const double omega = sqrt(rx2 > 0.0 ? rx2 : 0.0) / sqrt(static_cast<double>(dim > 1 ? dim - 1 : 1));
+        const double r_q = sqrt(d2 > 0.0 ? d2 : 0.0);
+        if (omega > 0.0 && r_q > 0.0) r = (d_coarse - d_full) / (r_q * omega);
+    }
+    out[pair] = r;
+}
+
 }  // namespace
 
 int launch_rotate(const DevIndex& ix, const float* q, int nq, float* out, cudaStream_t s) {
@@ -726,6 +845,26 @@ __global__ void synth_queries_kernel(const float* __restrict__ cen, int nlist, i
 
 int launch_synth_queries(const DevIndex& ix, int nq, unsigned long long seed, float* out, cudaStream_t s) {
     synth_queries_kernel<<<nq, 256, 0, s>>>(ix.cen, ix.nlist, ix.pd, seed, out);
+    E8QC_CUDA(cudaGetLastError());
+    return 1;
+}
+
+int launch_probe_bound(const DevIndex& ix, const float* rq, const float* rx, const uint32_t* qsel,
+                       const uint32_t* slot_of, const uint32_t* list_of, const double* dlev, const double* mid, int m,
+                       int dim, double* out, cudaStream_t s) {
+    if (m <= 0) return 0;
+    const int grid = (m + 7) / 8;
+    switch (ix.bits) {
+#define E8QC_CASE(b)                                                                                              \
+    case b:                                                                                                       \
+        probe_bound_kernel<b><<<grid, 256, 0, s>>>(ix, rq, rx, qsel, slot_of, list_of, dlev, mid, m, dim, out); \
+        break;
+        E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
+        E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
+        E8QC_CASE(13)
+#undef E8QC_CASE
+        default: fail(E8QC_EINVAL, "bits out of range");
+    }
     E8QC_CUDA(cudaGetLastError());
     return 1;
 }

@@ -50,7 +50,7 @@ extern "C" {
  * batch grouped by list as in BATCHED, but candidates are generated on the
  * INT8 tensor cores from an int8 plane of every vector's levels (built on the
  * first precision search, padded_dim bytes per vector) and int8 queries; each
- * query's best max(32, 4k) (at most 128) proxy candidates are then rescored
+ * query's best max(32, 3k) (at most 128) proxy candidates are then rescored
  * with the exact estimator. Distances returned are exact; recall against the
  * exact scan is measured, not guaranteed. */
 #define E8QC_MODE_PRECISION 2
@@ -270,7 +270,7 @@ int e8qc_me8q_search(e8qc_me8q* idx, const float* queries, size_t nq, size_t k, 
  * scored with the estimator); E8QC_MODE_PRECISION generates candidates on the
  * INT8 tensor cores from an int8 plane of each vector's levels scaled by its
  * per-run coef (one scale per vector; built on first use, padded_dim bytes
- * per vector) and rescores each query's best max(32, 4k) (at most 128) with
+ * per vector) and rescores each query's best max(32, 3k) (at most 128) with
  * the reference's estimator: returned distances are exact, recall against the
  * exact scan is measured. */
 int e8qc_me8q_search_mode(e8qc_me8q* idx, const float* queries, size_t nq, size_t k, size_t nprobe, int mode,
@@ -398,6 +398,16 @@ int e8qc_server_get_stats(e8qc_server* srv, int reset, e8qc_server_stats* out);
 /* Stop accepting requests, finish the batches in flight, fail the requests
  * still pending (E8QC_ESTATE), join the threads and free the server. */
 int e8qc_server_stop(e8qc_server* srv);
+
+/* E8qIndex.probe_bound_w (python_bindings/e8q_bindings.cpp:182-233;
+ * E8qIndex::ProbeBoundW, src/index/e8q_oracle.cpp:103-218): for m pairs, pair i
+ * = query queries[qidx[i]] (nq x dim) against the stored vector ids[i] whose
+ * raw build row is base_rows[i] (m x dim): the zero-parallel-residual bound's
+ * normalised discrepancy (d_coarse^2 - d^2) / (r_q * Omega), every term in
+ * double from the stored code, into out[m]. NaN where qidx[i] >= nq, the id
+ * is not in the index, or the pair is degenerate. Host or device buffers. */
+int e8qc_e8q_probe_bound_w(e8qc_index* idx, const float* queries, size_t nq, const float* base_rows,
+                           const uint32_t* qidx, const uint32_t* ids, size_t m, double* out);
 
 /* ---- Fault injection for callers' error paths (no reference counterpart) ----
  * Failures these calls provoke are made on the host or by a bounded device

@@ -1454,3 +1454,105 @@ void orc_e8q_search_pruned_at(const orc_e8q_index* x, const uint8_t* banks_in, f
     free(bfirst);
     free(own);
 }
+
+/* ProbeBoundW: src/index/e8q_oracle.cpp:103-218. Query and base row are
+ * rotated and centred like the build's rows; the exact reconstruction uses
+ * the double level tables / sqrt(Dpad) and the scan basis the class means of
+ * InitBitTables (src/index/e8q_io.cpp:213-228: zero for dim 7 at 1 bit).
+ * The reference decodes each block with the 8-bit-digit split decoder
+ * (e8q_oracle.cpp:177-184 calls DecodeSplitBlockLane with uint8_t digits,
+ * src/index/e8q_scan.cpp:34-60), and this restates what that returns from the
+ * stored digits: at 2..8 bits the real digits and branch; at 1 bit the refine
+ * field is empty, so digit 7 is the rowA byte's bit 0 (the branch) and the
+ * branch reads 0; at 9 bits the digits keep their low 8 bits (the top bit
+ * falls out of the uint8_t). Above 9 bits the reference's decoder copies more
+ * than its 8-byte staging integer holds; the same low-8-bit rule is used. */
+static void probe_digits(int bits, const uint16_t* real, int branch, int* dg, int* br) {
+    for (int k = 0; k < 8; ++k) dg[k] = real[k];
+    *br = branch;
+    if (bits == 1) {
+        dg[7] = branch;
+        *br = 0;
+    } else if (bits >= 9) {
+        for (int k = 0; k < 8; ++k) dg[k] &= 0xFF;
+    }
+}
+
+double orc_e8q_probe_bound_w(const orc_e8q_index* x, const float* q, const float* base_row, uint32_t id) {
+    size_t pos = (size_t)-1;
+    for (size_t i = 0; i < x->n; ++i)
+        if (x->ids[i] == id) { pos = i; break; }
+    if (pos == (size_t)-1) return NAN;
+    const size_t c = list_of(x, pos);
+    const size_t pd = x->padded_dim;
+    const float* cc = x->centroid_rot + c * pd;
+    float* rq = (float*)malloc(sizeof(float) * pd);
+    float* rx = (float*)malloc(sizeof(float) * pd);
+    double* unit = (double*)malloc(sizeof(double) * pd);
+    orc_e8q_prepare_query(x, q, rq);
+    orc_e8q_prepare_query(x, base_row, rx);
+    double d2 = 0.0, rn2 = 0.0;
+    for (size_t d = 0; d < pd; ++d) {
+        const double qr = (double)rq[d] - (double)cc[d];
+        const double xr = (double)rx[d] - (double)cc[d];
+        d2 += qr * qr;
+        rn2 += xr * xr;
+        unit[d] = xr;
+    }
+    const double rn = sqrt(rn2);
+    double out = NAN;
+    if (rn > 0.0) {
+        for (size_t d = 0; d < pd; ++d) unit[d] /= rn;
+        const int bits = x->bits, qn = 1 << bits;
+        double* lev = (double*)malloc(sizeof(double) * 2 * (size_t)qn);
+        orc_branch_levels(bits, 0, lev);
+        orc_branch_levels(bits, 1, lev + qn);
+        double w_cls[2], mid[16];
+        orc_scan_class_means(bits, w_cls);
+        for (int d = 0; d < 8; ++d) {
+            mid[2 * d] = (bits == 1 && d == 7) ? 0.0 : w_cls[0];
+            mid[2 * d + 1] = (bits == 1 && d == 7) ? 0.0 : w_cls[1];
+        }
+        const double rd = sqrt((double)pd);
+        double dot_ue = 0, n2_e = 0, dot_ce = 0, dot_ew = 0, dot_uw = 0, n2_w = 0, dot_cw = 0, s_exact = 0,
+               s_coarse = 0;
+        const uint16_t* dg = x->digits + pos * (size_t)x->blocks * 8;
+        const uint8_t* br = x->branch + pos * (size_t)x->blocks;
+        for (int blk = 0; blk < x->blocks; ++blk) {
+            int pdg[8], pbr = 0;
+            probe_digits(bits, dg + (size_t)blk * 8, br[blk], pdg, &pbr);
+            for (int k = 0; k < 8; ++k) {
+                const size_t idx = (size_t)blk * 8 + (size_t)k;
+                const int g = pdg[k];
+                const double ve = lev[(size_t)pbr * (size_t)qn + (size_t)g] / rd;
+                const double wc = mid[2 * k + (g >> (bits - 1))];
+                dot_ue += unit[idx] * ve;
+                n2_e += ve * ve;
+                dot_ce += (double)cc[idx] * ve;
+                dot_ew += ve * wc;
+                dot_uw += unit[idx] * wc;
+                n2_w += wc * wc;
+                dot_cw += (double)cc[idx] * wc;
+                s_exact += (double)rq[idx] * ve;
+                s_coarse += (double)rq[idx] * wc;
+            }
+        }
+        free(lev);
+        if (fabs(dot_ue) > 0.0 && fabs(dot_uw) > 0.0) {
+            const double g1 = rn / dot_ue;
+            const double h3 = rn2 + 2.0 * g1 * dot_ce;
+            const double d_full = d2 + h3 - 2.0 * g1 * s_exact;
+            const double w_x = 2.0 * rn / dot_uw;
+            const double d_coarse = d2 + rn2 + w_x * dot_cw - w_x * s_coarse;
+            const double rx2 = 4.0 * g1 * g1 * n2_e + w_x * w_x * n2_w - 4.0 * g1 * w_x * dot_ew;
+            const double sqrt_dm1 = sqrt((double)(x->dim > 1 ? x->dim - 1 : 1));
+            const double omega = sqrt(rx2 > 0.0 ? rx2 : 0.0) / sqrt_dm1;
+            const double r_q = sqrt(d2 > 0.0 ? d2 : 0.0);
+            if (omega > 0.0 && r_q > 0.0) out = (d_coarse - d_full) / (r_q * omega);
+        }
+    }
+    free(rq);
+    free(rx);
+    free(unit);
+    return out;
+}

@@ -147,6 +147,13 @@ void orc_e8q_search_pruned_at(const orc_e8q_index* idx, const uint8_t* banks, fl
                               size_t nprobe, const float* thr, uint32_t* out_ids, float* out_dists,
                               uint64_t* cand, uint64_t* surv, int threads);
 
+/* ProbeBoundW (src/index/e8q_oracle.cpp:103-218): for the stored vector `id`
+ * whose raw build input is base_row, the normalised discrepancy
+ * (d_coarse^2 - d^2) / (r_q * Omega) of the zero-parallel-residual bound,
+ * every term recomputed in double from the stored codes; NaN for a
+ * degenerate pair or an id not in the index. */
+double orc_e8q_probe_bound_w(const orc_e8q_index* idx, const float* query, const float* base_row, uint32_t id);
+
 #ifdef __cplusplus
 }
 #endif

@@ -68,6 +68,8 @@ def lib() -> C.CDLL:
         L.orc_e8q_exact_score.restype = C.c_float
         L.orc_e8q_estimate.argtypes = [C.c_void_p, _f32p, C.c_uint32]
         L.orc_e8q_estimate.restype = C.c_float
+        L.orc_e8q_probe_bound_w.argtypes = [C.c_void_p, _f32p, _f32p, C.c_uint32]
+        L.orc_e8q_probe_bound_w.restype = C.c_double
         L.orc_e8q_route.argtypes = [C.c_void_p, _f32p, C.c_size_t, _u32p, _f32p]
         L.orc_e8q_search.argtypes = [C.c_void_p, _f32p, C.c_size_t, C.c_size_t, C.c_size_t,
                                      _u32p, _f32p, C.c_int]
@@ -270,6 +272,18 @@ class OracleE8qIndex:
 
     def estimate(self, q, gid):
         return lib().orc_e8q_estimate(self._p, np.ascontiguousarray(q, np.float32), gid)
+
+    def probe_bound_w(self, queries, base_rows, qidx, ids):
+        """ProbeBoundW per pair i: queries[qidx[i]] against the stored vector
+        ids[i] whose raw input is base_rows[i]; NaN where qidx or the id is out
+        of range (as the reference's binding)."""
+        queries = np.ascontiguousarray(np.atleast_2d(queries), np.float32)
+        base_rows = np.ascontiguousarray(np.atleast_2d(base_rows), np.float32)
+        out = np.full(len(ids), np.nan)
+        for i, (qi, gid) in enumerate(zip(qidx, ids)):
+            if qi < queries.shape[0] and gid < self.n:
+                out[i] = lib().orc_e8q_probe_bound_w(self._p, queries[qi], base_rows[i], int(gid))
+        return out
 
     def route(self, rot_q, nprobe):
         take = min(nprobe, self.nlist)

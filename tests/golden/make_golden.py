@@ -96,6 +96,35 @@ def write_pruned_fixtures() -> None:
             candidates=np.array(cand, np.uint64), survivors=np.array(surv, np.uint64))
 
 
+# (name, dim, bits, n, nlist, seed, sigma, nq, pairs)
+PROBE_CASES = [
+    ("d96_b4", 96, 4, 3000, 20, 31, 0.5, 8, 64),
+    ("d100_b1", 100, 1, 2000, 16, 32, 0.5, 6, 48),
+    ("d200_b9", 200, 9, 2500, 24, 33, 0.45, 5, 40),
+]
+
+
+def write_probe_fixtures() -> None:
+    """The reference's E8qIndex.probe_bound_w on PROBE_CASES: pair i probes
+    stored vector ids[i] (its raw row as base) with query qidx[i]
+    (tests/golden/probe_bound_<name>.npz)."""
+    import oracle as O
+
+    E = O.ref_module()
+    for name, dim, bits, n, nlist, seed, sigma, nq, pairs in PROBE_CASES:
+        x, cm, lab = det_mixture(seed, n, dim, nlist, sigma)
+        q = det_mixture(seed + 1000, nq, dim, nlist, sigma)[0]
+        idx = E.E8qIndex(dim, bits, seed)
+        idx.build(x, cm, lab, num_threads=4)
+        rng = np.random.default_rng(seed)
+        ids = rng.choice(n, pairs, replace=False).astype(np.uint32)
+        qidx = rng.integers(0, nq, pairs).astype(np.uint32)
+        out = idx.probe_bound_w(q, x[ids], qidx, ids)
+        np.savez_compressed(os.path.join(HERE, f"probe_bound_{name}.npz"),
+                            params=np.array([dim, bits, n, nlist, seed, nq], np.int64), sigma=np.float64(sigma),
+                            ids=ids, qidx=qidx, out=np.asarray(out, np.float64))
+
+
 # reference-written ME8QIDXX index files, kept whole, for the ME8Q loader's tests
 ME8Q_FILES = ["me8q_d200_spec", "me8q_d150_a3"]
 
@@ -249,6 +278,8 @@ if __name__ == "__main__":
         write_e8ax_fixtures()  # only the E8AX files
     elif len(sys.argv) > 1 and sys.argv[1] == "me8q":
         write_me8q_fixtures()  # only the ME8QIDXX files
+    elif len(sys.argv) > 1 and sys.argv[1] == "probe":
+        write_probe_fixtures()
     elif len(sys.argv) > 1 and sys.argv[1] == "pruned":
         write_pruned_fixtures()  # only the pruned-search fixtures
     else:

@@ -11,7 +11,7 @@ from parity import RTOL, rel_err
 pytestmark = pytest.mark.gpu
 
 # Recall@k of precision mode against the exact scan on these synthetic
-# mixtures; the proxy keeps min(128, max(32, 4k)) candidates per query.
+# mixtures; the proxy keeps min(128, max(32, 3k)) candidates per query.
 RECALL_FLOOR = 0.97
 
 

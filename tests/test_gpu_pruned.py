@@ -130,3 +130,32 @@ def test_pruned_vs_oracle_bound_larger(e8q, oracle_lib, dim, bits, nlist, nprobe
     oi, od, oc, osv = orc.search_pruned_at(q, k, nprobe, thr=thr)
     assert np.array_equal(surv, osv)
     assert_topk_parity(ids, d, oi, od)
+
+
+PROBES = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "probe_bound_*.npz")))
+
+
+@pytest.mark.parametrize("path", PROBES, ids=lambda p: os.path.basename(p)[12:-4])
+def test_probe_bound_w_matches_reference(e8q, oracle_lib, path):
+    """E8qIndex.probe_bound_w on the GPU: the reference's values (its
+    probe_bound_w on the same build, rates 1, 4 and 9) within 1e-9 relative,
+    the oracle's too; NaN for a query index or an id out of range."""
+    g = np.load(path)
+    dim, bits, n, nlist, seed, nq = (int(v) for v in g["params"])
+    x, cm, lab = det_mixture(seed, n, dim, nlist, float(g["sigma"]))
+    q = det_mixture(seed + 1000, nq, dim, nlist, float(g["sigma"]))[0]
+    idx = e8q.E8qIndex(dim, bits, seed)
+    idx.build(x, cm, lab)
+    got = idx.probe_bound_w(q, x[g["ids"]], g["qidx"], g["ids"])
+    ref = g["out"]
+    assert got.dtype == np.float64
+    assert np.array_equal(np.isnan(got), np.isnan(ref))
+    fin = ~np.isnan(ref)
+    assert np.all(np.abs(got[fin] - ref[fin]) <= 1e-9 * np.maximum(np.abs(ref[fin]), 1e-3))
+    orc = oracle_lib.OracleE8qIndex(x, cm, lab, bits, seed=seed, threads=8)
+    o = orc.probe_bound_w(q, x[g["ids"][:8]], g["qidx"][:8], g["ids"][:8])
+    assert np.allclose(got[:8], o, rtol=1e-9, atol=1e-12, equal_nan=True)
+    bad = idx.probe_bound_w(q, x[:2], np.array([nq, 0], np.uint32), np.array([0, n + 5], np.uint32))
+    assert np.all(np.isnan(bad))
+    with pytest.raises(ValueError):
+        idx.probe_bound_w(q, x[:3], np.zeros(2, np.uint32), np.zeros(2, np.uint32))

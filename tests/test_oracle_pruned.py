@@ -54,3 +54,23 @@ def test_ortho_quantile_values(oracle_lib):
     assert abs(L.orc_phi_inv(0.975) - 1.959963984540054) < 1e-12
     assert abs(L.orc_ortho_quantile(1.0, 40) - 1.959964) < 1e-6
     assert L.orc_ortho_quantile(1.0, 1) == 1.0  # tail capped at 0.49 -> PhiInv(0.51) < 1
+
+
+PROBES = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "probe_bound_*.npz")))
+
+
+@pytest.mark.parametrize("path", PROBES, ids=lambda p: os.path.basename(p)[12:-4])
+def test_oracle_probe_bound_w_matches_reference(oracle_lib, path):
+    """ProbeBoundW: the bound's normalised discrepancy per (query, stored
+    vector) pair, every term in double; the reference's values (its
+    probe_bound_w, at rates 1, 4 and 9) within 1e-9 relative."""
+    g = np.load(path)
+    dim, bits, n, nlist, seed, nq = (int(v) for v in g["params"])
+    x, cm, lab = det_mixture(seed, n, dim, nlist, float(g["sigma"]))
+    q = det_mixture(seed + 1000, nq, dim, nlist, float(g["sigma"]))[0]
+    orc = oracle_lib.OracleE8qIndex(x, cm, lab, bits, seed=seed, threads=8)
+    got = orc.probe_bound_w(q, x[g["ids"]], g["qidx"], g["ids"])
+    ref = g["out"]
+    assert np.array_equal(np.isnan(got), np.isnan(ref))
+    fin = ~np.isnan(ref)
+    assert np.all(np.abs(got[fin] - ref[fin]) <= 1e-9 * np.maximum(np.abs(ref[fin]), 1e-3))
