@@ -165,10 +165,10 @@ __device__ __forceinline__ TileRef resolve_tile(const DevIndex& ix, const RouteW
                                                 int nprobe, uint32_t t) {
     TileRef r;
     r.p = find_probe(off, nprobe, t);
-    const uint32_t list = __ldcg(rw.probes + r.p);
+    const uint2 info = __ldcg(rw.probe_info + r.p);  // (first tile, vectors) of the probed list
     const uint32_t local = t - off[r.p];
-    r.gt = __ldg(ix.tile_begin + list) + local;
-    r.nvalid = min(32u, __ldg(ix.list_len + list) - local * 32u);
+    r.gt = info.x + local;
+    r.nvalid = min(32u, info.y - local * 32u);
     r.d2 = __ldcg(rw.probe_d2 + r.p);
     return r;
 }
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) pruned_kernel(DevIndex ix, con
     float* sm_d = reinterpret_cast<float*>(soff + kToffCap + 4);                    // kWarps*kMaxK
     uint32_t* sm_id = reinterpret_cast<uint32_t*>(sm_d + kWarps * kMaxK);
     float* sv_d = reinterpret_cast<float*>(sm_id + kWarps * kMaxK);                // kSelCap
-    uint32_t* sv_id = reinterpret_cast<uint32_t*>(sv_d + kSelCap);
+    uint32_t* sv_id = reinterpret_cast<uint32_t*>(sv_d + kSelCapWide);
     float* seed_dc = reinterpret_cast<float*>(sv_id + kSelCap);                    // kMaxK
     uint32_t* seed_key = reinterpret_cast<uint32_t*>(seed_dc + kMaxK);
     float* seed_d = reinterpret_cast<float*>(seed_key + kMaxK);
@@ -206,6 +206,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) pruned_kernel(DevIndex ix, con
     __shared__ float s_T;
     __shared__ int s_ok;
     __shared__ bool s_last;
+    __shared__ unsigned long long s_stats[2];  // the CTA's candidates and survivors
 
     // ---- prologue: query (padded units), level table copies, tile offsets, LUT
     for (int i = tid; i < ix.pd; i += nt) {
@@ -216,7 +217,10 @@ __global__ void __launch_bounds__(kWarps * 32, 1) pruned_kernel(DevIndex ix, con
     const bool off_in_smem = nprobe <= kToffCap;
     if (off_in_smem)
         for (int i = tid; i <= nprobe; i += nt) soff[i] = __ldcg(rw.tile_off + i);
-    if (tid == 0) s_hc = 0u;
+    if (tid == 0) {
+        s_hc = 0u;
+        s_stats[0] = s_stats[1] = 0ull;
+    }
     __syncthreads();
     // LUT entry e = blk*32 + v: v < 16 prices the low nibble (digits 4..7),
     // v >= 16 the high nibble (digits 0..3); fp64 sums in the reference's order
@@ -286,7 +290,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) pruned_kernel(DevIndex ix, con
     {
         float* cd = pw.seed_dc + static_cast<size_t>(blockIdx.x) * kMaxK;
         uint32_t* ck = pw.seed_key + static_cast<size_t>(blockIdx.x) * kMaxK;
-        if (!block_select(sm_d, sm_id, kWarps, ns, sv_d, sv_id, cd, ck)) {
+        if (!block_select(sm_d, sm_id, kWarps, ns, sv_d, sv_id, cd, ck, kSelCapWide)) {
             __syncthreads();
             block_sort_select(sm_d, sm_id, kWarps, ns, cd, ck);
         }
@@ -316,7 +320,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) pruned_kernel(DevIndex ix, con
     {
         const int Gi = static_cast<int>(Gd);
         __syncthreads();
-        if (!block_select_g(pw.seed_dc, pw.seed_key, Gi, kMaxK, ns, sv_d, sv_id, seed_dc, seed_key)) {
+        if (!block_select_g(pw.seed_dc, pw.seed_key, Gi, kMaxK, ns, sv_d, sv_id, seed_dc, seed_key, kSelCapWide)) {
             __syncthreads();
             top.init(ns);
             for (int e0 = warp * 32; e0 < Gi * ns; e0 += nt) {
@@ -333,7 +337,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) pruned_kernel(DevIndex ix, con
             }
             top.store(sm_d + warp * ns, sm_id + warp * ns, ns);
             __syncthreads();
-            if (!block_select(sm_d, sm_id, kWarps, ns, sv_d, sv_id, seed_dc, seed_key)) {
+            if (!block_select(sm_d, sm_id, kWarps, ns, sv_d, sv_id, seed_dc, seed_key, kSelCapWide)) {
                 __syncthreads();
                 block_sort_select(sm_d, sm_id, kWarps, ns, seed_dc, seed_key);
             }
@@ -426,17 +430,23 @@ __global__ void __launch_bounds__(kWarps * 32, 1) pruned_kernel(DevIndex ix, con
             top.offer_pair(okj ? seed_d[s] : inf_f(), okj ? seed_id[s] : 0xFFFFFFFFu, okj);
         }
     }
+    // counters: per CTA in shared memory, then one global add each (thousands
+    // of same-address global atomics from every warp serialise in L2)
     if (lane == 0) {
-        atomicAdd(pw.stats + 0, cand_w);
-        atomicAdd(pw.stats + 1, surv_w);
+        atomicAdd(&s_stats[0], cand_w);
+        atomicAdd(&s_stats[1], surv_w);
     }
 
     // ---- phase 4: CTA reduction, then the last CTA reduces the CTAs' lists
     top.store(sm_d + warp * k, sm_id + warp * k, k);
     __syncthreads();
+    if (tid == 0) {
+        atomicAdd(pw.stats + 0, s_stats[0]);
+        atomicAdd(pw.stats + 1, s_stats[1]);
+    }
     float* cta_d = sw.part_d + static_cast<size_t>(blockIdx.x) * kMaxK;
     uint32_t* cta_id = sw.part_id + static_cast<size_t>(blockIdx.x) * kMaxK;
-    if (!block_select(sm_d, sm_id, kWarps, k, sv_d, sv_id, cta_d, cta_id)) {
+    if (!block_select(sm_d, sm_id, kWarps, k, sv_d, sv_id, cta_d, cta_id, kSelCapWide)) {
         __syncthreads();
         block_sort_select(sm_d, sm_id, kWarps, k, cta_d, cta_id);
     }
@@ -447,7 +457,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) pruned_kernel(DevIndex ix, con
     if (!s_last) return;
     __threadfence();
     const int Gi = static_cast<int>(Gd);
-    if (!block_select_g(sw.part_d, sw.part_id, Gi, kMaxK, k, sv_d, sv_id, out_d, out_ids)) {
+    if (!block_select_g(sw.part_d, sw.part_id, Gi, kMaxK, k, sv_d, sv_id, out_d, out_ids, kSelCapWide)) {
         __syncthreads();
         top.init(k);
         for (int e0 = warp * 32; e0 < Gi * k; e0 += nt) {
@@ -464,7 +474,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1) pruned_kernel(DevIndex ix, con
         }
         top.store(sm_d + warp * k, sm_id + warp * k, k);
         __syncthreads();
-        if (!block_select(sm_d, sm_id, kWarps, k, sv_d, sv_id, out_d, out_ids)) {
+        if (!block_select(sm_d, sm_id, kWarps, k, sv_d, sv_id, out_d, out_ids, kSelCapWide)) {
             __syncthreads();
             block_sort_select(sm_d, sm_id, kWarps, k, out_d, out_ids);
         }
@@ -547,7 +557,7 @@ size_t pruned_smem_bytes(const DevIndex& ix, int stash_tiles) {
     b += static_cast<size_t>(stash_tiles) * 64 * 4;
     b += static_cast<size_t>(kToffCap + 4) * 4;
     b += static_cast<size_t>(kWarps) * kMaxK * 8;
-    b += static_cast<size_t>(kSelCap) * 8;
+    b += static_cast<size_t>(kSelCapWide) * 8;
     b += static_cast<size_t>(kMaxK) * 16;
     return b;
 }

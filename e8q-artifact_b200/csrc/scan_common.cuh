@@ -19,7 +19,8 @@ __device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
 
 constexpr int kWarps = 16;      // warps per CTA; one CTA per SM
 constexpr int kToffCap = 1024;  // tile offsets cached in shared memory
-constexpr int kSelCap = 256;    // survivors ranked by counting
+constexpr int kSelCap = 256;      // survivors of a threshold select (counted or sorted)
+constexpr int kSelCapWide = 1024;  // the same for the pruned search's seed selects
 
 // Streaming 16-byte load: read-only, no L1 allocation (each byte is used once
 // per query).
@@ -95,13 +96,32 @@ __device__ __forceinline__ int find_probe(const uint32_t* off, int nprobe, uint3
     return lo;
 }
 
-// The sharper of two upper bounds of the k-th best entry of `nlists`
-// sorted lists of k entries each (list L at [L*k, L*k+k)): the best of the
-// lists' k-th entries (that list holds k entries at or below it) and, with
-// at least k lists, the k-th best of the lists' first entries (k lists each
-// hold one). Block-wide (all threads call; the result is in every thread).
-__device__ inline void lists_threshold(const float* ld, const uint32_t* lid, int nlists, int k, float& td_out,
-                                       uint32_t& ti_out) {
+// Entry j of list L: shared memory, or global memory written by other CTAs
+// (read through L2).
+template <bool G>
+__device__ __forceinline__ float lst_d(const float* ld, size_t e) {
+    if constexpr (G) return __ldcg(ld + e);
+    else return ld[e];
+}
+template <bool G>
+__device__ __forceinline__ uint32_t lst_i(const uint32_t* lid, size_t e) {
+    if constexpr (G) return __ldcg(lid + e);
+    else return lid[e];
+}
+
+// The sharper of two upper bounds of the k-th best entry of `nlists` sorted
+// lists of k entries each (list L's entries at [L*stride, L*stride + k)):
+// the best of the lists' k-th entries (that list holds k entries at or below
+// it), and T_m = the need-th best of the lists' m-th entries, m = ceil(k /
+// nlists), need = ceil(k / m) <= nlists (`need` lists each hold m entries at
+// or below it: need * m >= k; with nlists >= k this is the k-th best head).
+// Warp 0 forms the first; the other warps the second, each holding the lists'
+// m-th entries in registers (lane l: lists l, l + 32, ...) and ranking four of
+// its share per step with a warp reduction. Block-wide (all threads call; the
+// result is in every thread).
+template <bool G>
+__device__ inline void lists_threshold_t(const float* ld, const uint32_t* lid, int nlists, int stride, int k,
+                                         float& td_out, uint32_t& ti_out) {
     __shared__ float s_td, s_t2d;
     __shared__ uint32_t s_ti, s_t2i;
     const int tid = threadIdx.x, lane = tid & 31, nt = blockDim.x;
@@ -111,13 +131,14 @@ __device__ inline void lists_threshold(const float* ld, const uint32_t* lid, int
         s_t2i = 0xFFFFFFFFu;
     }
     __syncthreads();
-    // warp 0: the best of the lists' k-th entries
     if (warp == 0) {
         float td = inf_f();
         uint32_t ti = 0xFFFFFFFFu;
+#pragma unroll 8
         for (int L = lane; L < nlists; L += 32) {
-            const float d = ld[L * k + k - 1];
-            const uint32_t i = lid[L * k + k - 1];
+            const size_t e = static_cast<size_t>(L) * stride + k - 1;
+            const float d = lst_d<G>(ld, e);
+            const uint32_t i = lst_i<G>(lid, e);
             if (better(d, i, td, ti)) { td = d; ti = i; }
         }
 #pragma unroll
@@ -131,57 +152,43 @@ __device__ inline void lists_threshold(const float* ld, const uint32_t* lid, int
             s_ti = ti;
         }
     }
-    // the other warps (all, with one warp): the head whose rank among the
-    // heads is k - 1 (real heads are unique; padding heads only matter when
-    // fewer than k are real). Each warp holds all heads in registers (lane l:
-    // heads l, l + 32, ...) and ranks four of its share per step, each with a
-    // warp reduction of the lanes' counts.
-    constexpr int kHpl = 8;  // heads per lane: up to 256 lists
+    constexpr int kHpl = 8;  // entries per lane: up to 256 lists
+    const int m = nlists > 0 ? (k + nlists - 1) / nlists : 1;
+    const int need = (k + m - 1) / m;
     const int w0 = nw > 1 ? 1 : 0, nr = nw - w0;
-    if (nlists >= k && warp >= w0) {
-        if (nlists <= 32 * kHpl) {
-            float hd[kHpl];
-            uint32_t hi[kHpl];
+    if (nlists > 0 && nlists <= 32 * kHpl && warp >= w0) {
+        float hd[kHpl];
+        uint32_t hi[kHpl];
 #pragma unroll
-            for (int m = 0; m < kHpl; ++m) {
-                const int L = lane + 32 * m;
-                hd[m] = L < nlists ? ld[L * k] : inf_f();
-                hi[m] = L < nlists ? lid[L * k] : 0xFFFFFFFFu;
+        for (int u = 0; u < kHpl; ++u) {
+            const int L = lane + 32 * u;
+            const size_t e = static_cast<size_t>(L) * stride + m - 1;
+            hd[u] = L < nlists ? lst_d<G>(ld, e) : inf_f();
+            hi[u] = L < nlists ? lst_i<G>(lid, e) : 0xFFFFFFFFu;
+        }
+        for (int L0 = warp - w0; L0 < nlists; L0 += 4 * nr) {
+            int c[4] = {0, 0, 0, 0};
+            float d[4];
+            uint32_t i[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int L = L0 + u * nr;
+                const size_t e = static_cast<size_t>(L) * stride + m - 1;
+                d[u] = L < nlists ? lst_d<G>(ld, e) : inf_f();
+                i[u] = L < nlists ? lst_i<G>(lid, e) : 0xFFFFFFFFu;
             }
-            for (int L0 = warp - w0; L0 < nlists; L0 += 4 * nr) {
-                int c[4] = {0, 0, 0, 0};
-                float d[4];
-                uint32_t i[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int L = L0 + u * nr;
-                    d[u] = L < nlists ? ld[L * k] : inf_f();
-                    i[u] = L < nlists ? lid[L * k] : 0xFFFFFFFFu;
-                }
+            for (int u2 = 0; u2 < kHpl; ++u2)
 #pragma unroll
-                for (int m = 0; m < kHpl; ++m)
+                for (int u = 0; u < 4; ++u) c[u] += better(hd[u2], hi[u2], d[u], i[u]) ? 1 : 0;
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) c[u] += better(hd[m], hi[m], d[u], i[u]) ? 1 : 0;
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int r = __reduce_add_sync(kFull, c[u]);
-                    if (lane == 0 && i[u] != 0xFFFFFFFFu && r == k - 1) {
-                        s_t2d = d[u];  // a single warp can reach this
-                        s_t2i = i[u];
-                    }
-                }
-            }
-        } else {
-            for (int L = tid - 32 * w0; L < nlists; L += 32 * nr) {
-                const float d = ld[L * k];
-                const uint32_t i = lid[L * k];
-                if (i == 0xFFFFFFFFu) continue;
-                int r = 0;
-#pragma unroll 8
-                for (int M = 0; M < nlists; ++M) r += better(ld[M * k], lid[M * k], d, i) ? 1 : 0;
-                if (r == k - 1) {
-                    s_t2d = d;  // a single thread can reach this
-                    s_t2i = i;
+            for (int u = 0; u < 4; ++u) {
+                const int r = __reduce_add_sync(kFull, c[u]);
+                // real entries are unique; padding only matters when fewer
+                // than `need` lists hold m real entries
+                if (lane == 0 && i[u] != 0xFFFFFFFFu && r == need - 1) {
+                    s_t2d = d[u];  // a single warp can reach this
+                    s_t2i = i[u];
                 }
             }
         }
@@ -195,116 +202,120 @@ __device__ inline void lists_threshold(const float* ld, const uint32_t* lid, int
     }
 }
 
-// The k best of `nlists` sorted lists of k entries each (list L at [L*k,
-// L*k+k), padding (+inf, UINT32_MAX) at its end), written ascending to
-// od / oi (shared or global), padded when fewer exist. Threshold filter +
-// rank counting (see the file comment); returns false, having written
-// nothing, when more than kSelCap entries survive the threshold. Block-wide;
-// the caller synchronises before reusing ld / lid / sv_*.
-__device__ inline bool block_select(const float* ld, const uint32_t* lid, int nlists, int k, float* sv_d, uint32_t* sv_id,
-                             float* od, uint32_t* oi) {
-    __shared__ int s_n;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    float td;
-    uint32_t ti;
-    if (tid == 0) s_n = 0;
-    lists_threshold(ld, lid, nlists, k, td, ti);
+__device__ inline void lists_threshold(const float* ld, const uint32_t* lid, int nlists, int k, float& td_out,
+                                       uint32_t& ti_out) {
+    lists_threshold_t<false>(ld, lid, nlists, k, k, td_out, ti_out);
+}
+
+// The entries at or below the threshold (td, ti), compacted into sv_* with
+// one shared atomic per warp and step (lanes' slots from a ballot), then the
+// k best of them written ascending to od / oi: ranked by counting when few
+// survive, else sorted (a block bitonic sort of at most `cap` entries).
+// False, having written nothing, when more than `cap` (sv_*'s size) survive.
+template <bool G>
+__device__ inline bool filter_select(const float* ld, const uint32_t* lid, int nlists, int stride, int k, float td,
+                                     uint32_t ti, int* s_n, float* sv_d, uint32_t* sv_id, float* od, uint32_t* oi,
+                                     int cap) {
+    const int tid = threadIdx.x, lane = tid & 31, nt = blockDim.x;
     const int total = nlists * k;
-    for (int e = tid; e < total; e += nt) {
-        const uint32_t i = lid[e];
-        if (i == 0xFFFFFFFFu) continue;
-        const float d = ld[e];
-        if (better(td, ti, d, i)) continue;  // worse than the threshold
-        const int pos = atomicAdd(&s_n, 1);
-        if (pos < kSelCap) {
-            sv_d[pos] = d;
-            sv_id[pos] = i;
+    // eight entries per thread per round, loaded before any is filtered (one
+    // memory latency per round when the lists are in global memory)
+    constexpr int kPer = 8;
+    for (int b0 = 0; b0 < total; b0 += kPer * nt) {  // the same trip count in every thread
+        float d[kPer];
+        uint32_t i[kPer];
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int e = b0 + u * nt + tid;
+            d[u] = 0.0f;
+            i[u] = 0xFFFFFFFFu;
+            if (e < total) {
+                const int L = e / k, j = e - L * k;
+                const size_t a = static_cast<size_t>(L) * stride + j;
+                i[u] = lst_i<G>(lid, a);
+                d[u] = lst_d<G>(ld, a);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const bool keep = i[u] != 0xFFFFFFFFu && !better(td, ti, d[u], i[u]);  // not worse than the threshold
+            const unsigned m = __ballot_sync(kFull, keep);
+            int wb = 0;
+            if (lane == 0 && m != 0u) wb = atomicAdd(s_n, __popc(m));
+            wb = __shfl_sync(kFull, wb, 0);
+            if (keep) {
+                const int pos = wb + __popc(m & ((1u << lane) - 1u));
+                if (pos < cap) {
+                    sv_d[pos] = d[u];
+                    sv_id[pos] = i[u];
+                }
+            }
         }
     }
     __syncthreads();
-    const int S = s_n;
-    if (S > kSelCap) return false;
-    for (int s = tid; s < S; s += nt) {
-        const float d = sv_d[s];
-        const uint32_t i = sv_id[s];
-        int r = 0;
+    const int S = *s_n;
+    if (S > cap) return false;
+    if (S <= 64) {
+        for (int s = tid; s < S; s += nt) {
+            const float d = sv_d[s];
+            const uint32_t i = sv_id[s];
+            int r = 0;
 #pragma unroll 8
-        for (int j = 0; j < S; ++j) r += better(sv_d[j], sv_id[j], d, i) ? 1 : 0;
-        if (r < k) {
-            od[r] = d;
-            oi[r] = i;
+            for (int j = 0; j < S; ++j) r += better(sv_d[j], sv_id[j], d, i) ? 1 : 0;
+            if (r < k) {
+                od[r] = d;
+                oi[r] = i;
+            }
         }
+        for (int r = S + tid; r < k; r += nt) {
+            od[r] = inf_f();
+            oi[r] = 0xFFFFFFFFu;
+        }
+        return true;
     }
-    for (int r = S + tid; r < k; r += nt) {
-        od[r] = inf_f();
-        oi[r] = 0xFFFFFFFFu;
+    const int pn = next_pow2(S);
+    for (int e = S + tid; e < pn; e += nt) {
+        sv_d[e] = inf_f();
+        sv_id[e] = 0xFFFFFFFFu;
+    }
+    __syncthreads();
+    block_bitonic_sort(sv_d, sv_id, pn);
+    for (int r = tid; r < k; r += nt) {
+        od[r] = r < S ? sv_d[r] : inf_f();
+        oi[r] = r < S ? sv_id[r] : 0xFFFFFFFFu;
     }
     return true;
+}
+
+// The k best of `nlists` sorted lists of k entries each (list L at [L*k,
+// L*k+k), padding (+inf, UINT32_MAX) at its end), written ascending to
+// od / oi (shared or global), padded when fewer exist. Threshold filter +
+// rank counting or a survivors' sort (see the file comment); returns false,
+// having written nothing, when more than kSelCap entries survive the
+// threshold. Block-wide; the caller synchronises before reusing ld / lid /
+// sv_*.
+__device__ inline bool block_select(const float* ld, const uint32_t* lid, int nlists, int k, float* sv_d, uint32_t* sv_id,
+                             float* od, uint32_t* oi, int cap = kSelCap) {
+    __shared__ int s_n;
+    if (threadIdx.x == 0) s_n = 0;
+    float td;
+    uint32_t ti;
+    lists_threshold(ld, lid, nlists, k, td, ti);
+    return filter_select<false>(ld, lid, nlists, k, k, td, ti, &s_n, sv_d, sv_id, od, oi, cap);
 }
 
 // block_select over lists that other CTAs wrote to global memory (read
 // through L2): list L's entries at [L*stride, L*stride + k).
 __device__ inline bool block_select_g(const float* ld, const uint32_t* lid, int nlists, int stride, int k,
-                                      float* sv_d, uint32_t* sv_id, float* od, uint32_t* oi) {
-    __shared__ float s_td;
-    __shared__ uint32_t s_ti;
+                                      float* sv_d, uint32_t* sv_id, float* od, uint32_t* oi, int cap = kSelCap) {
     __shared__ int s_n;
-    const int tid = threadIdx.x, lane = tid & 31, nt = blockDim.x;
-    if (tid < 32) {
-        float td = inf_f();
-        uint32_t ti = 0xFFFFFFFFu;
-        for (int L = lane; L < nlists; L += 32) {
-            const float d = __ldcg(ld + static_cast<size_t>(L) * stride + k - 1);
-            const uint32_t i = __ldcg(lid + static_cast<size_t>(L) * stride + k - 1);
-            if (better(d, i, td, ti)) { td = d; ti = i; }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const float d = __shfl_xor_sync(kFull, td, o);
-            const uint32_t i = __shfl_xor_sync(kFull, ti, o);
-            if (better(d, i, td, ti)) { td = d; ti = i; }
-        }
-        if (lane == 0) {
-            s_td = td;
-            s_ti = ti;
-            s_n = 0;
-        }
-    }
-    __syncthreads();
-    const float td = s_td;
-    const uint32_t ti = s_ti;
-    for (int e = tid; e < nlists * k; e += nt) {
-        const int L = e / k, j = e - L * k;
-        const uint32_t i = __ldcg(lid + static_cast<size_t>(L) * stride + j);
-        if (i == 0xFFFFFFFFu) continue;
-        const float d = __ldcg(ld + static_cast<size_t>(L) * stride + j);
-        if (better(td, ti, d, i)) continue;
-        const int pos = atomicAdd(&s_n, 1);
-        if (pos < kSelCap) {
-            sv_d[pos] = d;
-            sv_id[pos] = i;
-        }
-    }
-    __syncthreads();
-    const int S = s_n;
-    if (S > kSelCap) return false;
-    for (int s = tid; s < S; s += nt) {
-        const float d = sv_d[s];
-        const uint32_t i = sv_id[s];
-        int r = 0;
-#pragma unroll 8
-        for (int j = 0; j < S; ++j) r += better(sv_d[j], sv_id[j], d, i) ? 1 : 0;
-        if (r < k) {
-            od[r] = d;
-            oi[r] = i;
-        }
-    }
-    for (int r = S + tid; r < k; r += nt) {
-        od[r] = inf_f();
-        oi[r] = 0xFFFFFFFFu;
-    }
-    return true;
+    if (threadIdx.x == 0) s_n = 0;
+    float td;
+    uint32_t ti;
+    lists_threshold_t<true>(ld, lid, nlists, stride, k, td, ti);
+    return filter_select<true>(ld, lid, nlists, stride, k, td, ti, &s_n, sv_d, sv_id, od, oi, cap);
 }
+
 
 // Bitonic fallback of block_select: sort all nlists*k entries in place
 // (sd / si hold at least next_pow2(nlists*k) entries) and copy the first k.
