@@ -683,7 +683,9 @@ def run_sweep(a):
         1 ... 4096;
       * the 100k x 128 mixture of 256 lists (sigma 0.5, flat spectrum, nbits 4,
         nprobe 16): the same paths, and the reference's CPU search on this
-        host's cores.
+        host's cores;
+      * 1M x 768, nbits 4, nprobe 64: the batched and precision paths at
+        query batches 256 ... 8192.
     One JSON line."""
     import copy
 
@@ -744,7 +746,7 @@ def run_sweep(a):
         return row
 
     out = {"sweep": "1M x 960 mixture (sigma 0.4, lambda_i ~ i^-0.5), k=10", "grid": [], "batch_sweep": None,
-           "config1": None, "peak_hbm_gbs": peak, "peak_kind": pk_kind}
+           "config1": None, "config4": None, "peak_hbm_gbs": peak, "peak_kind": pk_kind}
     b = copy.copy(a)
     b.n, b.dim, b.nlist, b.k, b.pool = 1_000_000, 960, 1024, 10, 4096
     b.spectrum, b.sigma = 0.5, 0.4
@@ -781,6 +783,21 @@ def run_sweep(a):
                                 "recall_pruned": round(cb["pruned_recall"], 4), "cores": cb["cores"],
                                 "cpu_model": cb["cpu_model"]}
     out["config1"] = row
+    del idx, x, cm, lab, q
+    torch.cuda.empty_cache()
+
+    # 1M x 768, nbits 4: the precision path at query batches 256 ... 8192
+    d4 = copy.copy(a)
+    d4.n, d4.dim, d4.nlist, d4.k, d4.nbits, d4.pool, d4.seed = 1_000_000, 768, 1024, 10, 4, 8192, 0
+    d4.spectrum, d4.sigma, d4.nprobe = 0.5, 0.4, 64
+    x, cm, lab, q = gen_data(d4, dev, 0)
+    gt = ground_truth(x, q[:500], d4.k)
+    idx = e8qlib.E8qIndex(d4.dim, d4.nbits, d4.seed, device=0)
+    idx.build_ptr(x.data_ptr(), d4.n, cm.data_ptr(), d4.nlist, lab.data_ptr(), 0.0, sp)
+    torch.cuda.synchronize()
+    row = measure(d4, idx, q, gt, 64, batches=(256, 1024, 4096, 8192), with_plain=False)
+    row["workload"] = workload_name(d4)
+    out["config4"] = row
     print(json.dumps(out), flush=True)
 
 

@@ -218,10 +218,26 @@ __device__ inline bool filter_select(const float* ld, const uint32_t* lid, int n
                                      int cap) {
     const int tid = threadIdx.x, lane = tid & 31, nt = blockDim.x;
     const int total = nlists * k;
-    // eight entries per thread per round, loaded before any is filtered (one
-    // memory latency per round when the lists are in global memory)
+    if constexpr (!G) {
+        // lists in shared memory: one pass, a shared atomic per survivor
+        // (few survive the bounds; the short loop keeps the merge's code
+        // small)
+        for (int e = tid; e < total; e += nt) {
+            const uint32_t i = lid[e];
+            if (i == 0xFFFFFFFFu) continue;
+            const float d = ld[e];
+            if (better(td, ti, d, i)) continue;  // worse than the threshold
+            const int pos = atomicAdd(s_n, 1);
+            if (pos < cap) {
+                sv_d[pos] = d;
+                sv_id[pos] = i;
+            }
+        }
+    }
+    // lists in global memory: eight entries per thread per round, loaded
+    // before any is filtered (one memory latency per round)
     constexpr int kPer = 8;
-    for (int b0 = 0; b0 < total; b0 += kPer * nt) {  // the same trip count in every thread
+    for (int b0 = 0; G && b0 < total; b0 += kPer * nt) {  // the same trip count in every thread
         float d[kPer];
         uint32_t i[kPer];
 #pragma unroll
@@ -236,19 +252,32 @@ __device__ inline bool filter_select(const float* ld, const uint32_t* lid, int n
                 d[u] = lst_d<G>(ld, a);
             }
         }
+        // the round's masks first (independent votes), then one shared
+        // atomic per warp and round, only when something survives
+        unsigned mk[kPer];
+        bool keep[kPer];
+        int tot = 0;
 #pragma unroll
         for (int u = 0; u < kPer; ++u) {
-            const bool keep = i[u] != 0xFFFFFFFFu && !better(td, ti, d[u], i[u]);  // not worse than the threshold
-            const unsigned m = __ballot_sync(kFull, keep);
+            keep[u] = i[u] != 0xFFFFFFFFu && !better(td, ti, d[u], i[u]);  // not worse than the threshold
+            mk[u] = __ballot_sync(kFull, keep[u]);
+            tot += __popc(mk[u]);
+        }
+        if (tot != 0) {  // warp-uniform
             int wb = 0;
-            if (lane == 0 && m != 0u) wb = atomicAdd(s_n, __popc(m));
+            if (lane == 0) wb = atomicAdd(s_n, tot);
             wb = __shfl_sync(kFull, wb, 0);
-            if (keep) {
-                const int pos = wb + __popc(m & ((1u << lane) - 1u));
-                if (pos < cap) {
-                    sv_d[pos] = d[u];
-                    sv_id[pos] = i[u];
+            const unsigned below = (1u << lane) - 1u;
+#pragma unroll
+            for (int u = 0; u < kPer; ++u) {
+                if (keep[u]) {
+                    const int pos = wb + __popc(mk[u] & below);
+                    if (pos < cap) {
+                        sv_d[pos] = d[u];
+                        sv_id[pos] = i[u];
+                    }
                 }
+                wb += __popc(mk[u]);
             }
         }
     }
