@@ -21,12 +21,16 @@ stands in for the public corpora (no network).
   roofline: the dominant scan kernel's algorithmic bytes per launch over its
            CUDA-event time against the measured HBM copy bandwidth -- for the
            precision scan: int8 proxy row + g1/h3 per vector of each work item
-           plus 4 bytes of proxy distance written per (query, vector) pair;
+           plus 2 bytes of fp16 proxy distance written per (query, vector) pair;
            beside it the int8 tensor ops against an int8 MMA rate measured in
            the run with the library's tcgen05 probe.
   plain_gpu_qps: the plain one-query-per-launch GPU scan on the same index.
   serving: open-loop Poisson load through e8qlib.Server (U{1..64} queries per
-           request) at fractions of `value`: achieved QPS, p50/p99/max ms.
+           request) at fractions of `value`: achieved QPS, p50/p99/max ms;
+           the loads with the headline k and nprobe, then one of uneven
+           requests (k in {10, 100}, nprobe in {16, 32, 64} drawn per request).
+  --sweep: the nbits x nprobe grid, query-batch sweeps and the other E8Q
+           configurations instead of the bench line (see run_sweep).
   cpu_baseline: the reference's own CPU search (compiled from its sources into
            oracle/_ref), all host cores, a bounded sample of the same workload.
 
@@ -1006,7 +1010,17 @@ def main():
             serving.append({"offered_qps": st["offered_qps"], "achieved_qps": round(st["qps"], 1),
                             "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
                             "max_ms": round(st["max_ms"], 3), "requests": st["requests"],
-                            "mean_batch_queries": round(st["mean_batch_queries"], 1)})
+                            "mean_batch_queries": round(st["mean_batch_queries"], 1),
+                            "k": [a.k], "nprobe": [a.nprobe]})
+        # uneven requests: k and nprobe drawn per request
+        mix_k, mix_np = [a.k, 100], sorted({16, 32, a.nprobe})
+        frac = float([f for f in a.serve_loads.split(",") if f][0])
+        st = serve_open_loop(e8qlib, idx, a.path, qn, mix_k, mix_np, frac * value, a.serve_seconds, a.seed + 11,
+                             a.batch)
+        serving.append({"offered_qps": st["offered_qps"], "achieved_qps": round(st["qps"], 1),
+                        "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3),
+                        "max_ms": round(st["max_ms"], 3), "requests": st["requests"],
+                        "mean_batch_queries": round(st["mean_batch_queries"], 1), "k": mix_k, "nprobe": mix_np})
 
     me8q = None
     if not a.no_me8q:
