@@ -316,6 +316,10 @@ __device__ inline bool filter_select(const float* ld, const uint32_t* lid, int n
     return true;
 }
 
+// The selects below are not inlined: a kernel calls them at several sites,
+// once each per launch, and one shared copy of their code stays warm in the
+// instruction cache where inlined copies would each be fetched cold.
+//
 // The k best of `nlists` sorted lists of k entries each (list L at [L*k,
 // L*k+k), padding (+inf, UINT32_MAX) at its end), written ascending to
 // od / oi (shared or global), padded when fewer exist. Threshold filter +
@@ -323,7 +327,7 @@ __device__ inline bool filter_select(const float* ld, const uint32_t* lid, int n
 // having written nothing, when more than kSelCap entries survive the
 // threshold. Block-wide; the caller synchronises before reusing ld / lid /
 // sv_*.
-__device__ inline bool block_select(const float* ld, const uint32_t* lid, int nlists, int k, float* sv_d, uint32_t* sv_id,
+static __device__ __noinline__ bool block_select(const float* ld, const uint32_t* lid, int nlists, int k, float* sv_d, uint32_t* sv_id,
                              float* od, uint32_t* oi, int cap = kSelCap) {
     __shared__ int s_n;
     if (threadIdx.x == 0) s_n = 0;
@@ -335,7 +339,7 @@ __device__ inline bool block_select(const float* ld, const uint32_t* lid, int nl
 
 // block_select over lists that other CTAs wrote to global memory (read
 // through L2): list L's entries at [L*stride, L*stride + k).
-__device__ inline bool block_select_g(const float* ld, const uint32_t* lid, int nlists, int stride, int k,
+static __device__ __noinline__ bool block_select_g(const float* ld, const uint32_t* lid, int nlists, int stride, int k,
                                       float* sv_d, uint32_t* sv_id, float* od, uint32_t* oi, int cap = kSelCap) {
     __shared__ int s_n;
     if (threadIdx.x == 0) s_n = 0;
@@ -348,7 +352,7 @@ __device__ inline bool block_select_g(const float* ld, const uint32_t* lid, int 
 
 // Bitonic fallback of block_select: sort all nlists*k entries in place
 // (sd / si hold at least next_pow2(nlists*k) entries) and copy the first k.
-__device__ inline void block_sort_select(float* sd, uint32_t* si, int nlists, int k, float* od, uint32_t* oi) {
+static __device__ __noinline__ void block_sort_select(float* sd, uint32_t* si, int nlists, int k, float* od, uint32_t* oi) {
     const int n = nlists * k, pn = next_pow2(n);
     for (int i = n + threadIdx.x; i < pn; i += blockDim.x) {
         sd[i] = inf_f();
