@@ -40,6 +40,14 @@ void orc_me8q_ids(const orc_me8q_index* x, uint32_t* out);
 float orc_me8q_estimate(const orc_me8q_index* x, const float* query, uint32_t id);
 void orc_me8q_search(const orc_me8q_index* x, const float* queries, size_t nq, size_t k, size_t nprobe,
                      uint32_t* out_ids, float* out_dists, int threads);
+/* The reference's production search (SearchIVFFast*, src/index/me8q_fast.cpp:
+ * 37-1090, src/simd/me8q_prune_avx512.cpp:9-92): FastScan coarse plane,
+ * zero-parallel-residual bound and run cascade against the live heap; alpha
+ * is the build's prune_alpha. cand / surv (may be NULL): per query the scanned
+ * candidates and the rows pushed to the heap. */
+void orc_me8q_search_pruned(const orc_me8q_index* x, const float* queries, size_t nq, size_t k, size_t nprobe,
+                            float alpha, uint32_t* out_ids, float* out_dists, uint64_t* cand, uint64_t* surv,
+                            int threads);
 
 #ifdef __cplusplus
 }

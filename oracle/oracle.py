@@ -107,6 +107,9 @@ def lib() -> C.CDLL:
         L.orc_me8q_estimate.restype = C.c_float
         L.orc_me8q_search.argtypes = [C.c_void_p, _f32p, C.c_size_t, C.c_size_t, C.c_size_t,
                                       _u32p, _f32p, C.c_int]
+        _u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+        L.orc_me8q_search_pruned.argtypes = [C.c_void_p, _f32p, C.c_size_t, C.c_size_t, C.c_size_t, C.c_float,
+                                             _u32p, _f32p, _u64p, _u64p, C.c_int]
         _lib = L
     return _lib
 
@@ -489,7 +492,9 @@ def parse_plan_spec(spec: str, pd: int):
 
 
 class OracleMe8qIndex:
-    """The restated ME8Q index (plain SearchIVF path) as a Python object."""
+    """The restated ME8Q index as a Python object: the plain SearchIVF path
+    (search) and the reference's production FastScan cascade
+    (search_pruned)."""
 
     def __init__(self, data, centroids, cluster_ids, avg_bits=4.0, seed=0, variance=None, drop_energy=True,
                  plan_spec="", extra_budget_bits=0.0, max_bits=13, threads=8):
@@ -540,6 +545,18 @@ class OracleMe8qIndex:
         dists = np.zeros((nq, k), np.float32)
         lib().orc_me8q_search(self._p, queries, nq, k, nprobe, ids, dists, threads)
         return ids, dists
+
+    def search_pruned(self, queries, k, nprobe, alpha=1.0, threads=8):
+        """(ids, dists, candidates, survivors) of the production search; alpha
+        is the build's prune_alpha (1 when not positive)."""
+        queries = np.ascontiguousarray(np.atleast_2d(queries), np.float32)
+        nq = queries.shape[0]
+        ids = np.zeros((nq, k), np.uint32)
+        dists = np.zeros((nq, k), np.float32)
+        cand = np.zeros(nq, np.uint64)
+        surv = np.zeros(nq, np.uint64)
+        lib().orc_me8q_search_pruned(self._p, queries, nq, k, nprobe, alpha, ids, dists, cand, surv, threads)
+        return ids, dists, cand, surv
 
 
 def parse_me8q(path: str) -> dict:

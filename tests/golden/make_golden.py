@@ -8,7 +8,8 @@ integer-derived floats), outputs come from the reference's own code:
   * oracle/_ref/e8qlib_ref    - the reference's pybind11 module: E8qIndex
     build / save (E8AX, parsed for codes, g1, h3, ids) / plain search
     (set_disable_prune(True)) / estimate / production pruned search with its
-    per-query stats.
+    per-query stats; Me8qIndex build / save / search (prune_alpha 1e-9: the
+    plain scan) and its production FastScan search with per-query stats.
 
 Usage: python tests/golden/make_golden.py
 """
@@ -123,6 +124,45 @@ def write_probe_fixtures() -> None:
         np.savez_compressed(os.path.join(HERE, f"probe_bound_{name}.npz"),
                             params=np.array([dim, bits, n, nlist, seed, nq], np.int64), sigma=np.float64(sigma),
                             ids=ids, qidx=qidx, out=np.asarray(out, np.float64))
+
+
+# the reference's production ME8Q search (FastScan cascade), query by query
+# with its stats: (name, dim, avg_bits, seed, plan_spec, n, nlist, sigma, nq,
+# k, nprobe, prune_alpha)
+ME8Q_PRUNED_CASES = [
+    ("d200_a4", 200, 4.0, 7, "", 3000, 12, 0.5, 24, 10, 5, 0.0),
+    ("d200_spec", 200, 4.0, 0, "64:6,64:4,64:3,64:0", 3000, 12, 0.5, 24, 10, 5, 0.0),
+    ("d96_a6_k20", 96, 6.0, 11, "", 2500, 8, 0.5, 24, 20, 3, 0.0),
+    ("d150_a3_a001", 150, 3.0, 0, "", 4000, 10, 0.5, 24, 16, 4, 0.01),
+    ("d64_a1", 64, 1.0, 3, "", 2000, 6, 0.5, 16, 10, 3, 0.0),
+]
+
+
+def write_me8q_pruned_fixtures() -> None:
+    """The reference's Me8qIndex.search (its only search: the FastScan
+    cascade) on ME8Q_PRUNED_CASES, one call per query with return_stats
+    (tests/golden/me8q_pruned_<name>.npz)."""
+    import oracle as O
+
+    E = O.ref_module()
+    for name, dim, avg, seed, spec, n, nlist, sigma, nq, k, nprobe, alpha in ME8Q_PRUNED_CASES:
+        x, cm, lab = det_mixture(seed + 5000 + dim, n, dim, nlist, sigma)
+        q = det_mixture(seed + 6000 + dim, nq, dim, nlist, sigma)[0]
+        idx = E.Me8qIndex(dim, avg, seed)
+        idx.build(x, cm, lab, num_threads=1, plan_spec=spec, prune_alpha=alpha)
+        ids, dists, cand, surv = [], [], [], []
+        for i in range(nq):
+            a, b, st = idx.search(q[i:i + 1], k, nprobe, 1, True)
+            ids.append(a[0])
+            dists.append(b[0])
+            cand.append(st["candidates"])
+            surv.append(st["survivors"])
+        np.savez_compressed(
+            os.path.join(HERE, f"me8q_pruned_{name}.npz"),
+            params=np.array([dim, seed, n, nlist, nq, k, nprobe], np.int64), avg_bits=np.float64(avg),
+            sigma=np.float64(sigma), plan_spec=np.array(spec), alpha=np.float32(alpha),
+            search_ids=np.array(ids, np.uint32), search_dists=np.array(dists, np.float32),
+            candidates=np.array(cand, np.uint64), survivors=np.array(surv, np.uint64))
 
 
 # reference-written ME8QIDXX index files, kept whole, for the ME8Q loader's tests
@@ -270,6 +310,7 @@ def main() -> None:
     write_e8ax_fixtures()
     write_me8q_fixtures()
     write_pruned_fixtures()
+    write_me8q_pruned_fixtures()
     print("golden fixtures written to", HERE)
 
 
@@ -282,5 +323,7 @@ if __name__ == "__main__":
         write_probe_fixtures()
     elif len(sys.argv) > 1 and sys.argv[1] == "pruned":
         write_pruned_fixtures()  # only the pruned-search fixtures
+    elif len(sys.argv) > 1 and sys.argv[1] == "me8q_pruned":
+        write_me8q_pruned_fixtures()  # only the ME8Q production-search fixtures
     else:
         main()

@@ -47,3 +47,25 @@ def test_me8q_plan_edges(oracle_lib):
         O.parse_plan_spec("64:3", 128)
     with pytest.raises(ValueError):
         O.parse_plan_spec("60:3,68:0", 128)
+
+
+PRUNED_CASES = ["d200_a4", "d200_spec", "d96_a6_k20", "d150_a3_a001", "d64_a1"]
+
+
+@pytest.mark.parametrize("name", PRUNED_CASES)
+def test_me8q_pruned_oracle_matches_reference(oracle_lib, name):
+    """The restated FastScan cascade (orc_me8q_search_pruned) against the
+    reference's own Me8qIndex.search: every row, its distances, and each
+    query's scanned candidates and survivors."""
+    G = load_golden(f"me8q_pruned_{name}.npz")
+    dim, seed, n, nlist, nq, k, nprobe = (int(v) for v in G["params"])
+    avg, sigma, spec, alpha = float(G["avg_bits"]), float(G["sigma"]), str(G["plan_spec"]), float(G["alpha"])
+    x, cm, lab = det_mixture(seed + 5000 + dim, n, dim, nlist, sigma)
+    q = det_mixture(seed + 6000 + dim, nq, dim, nlist, sigma)[0]
+    orc = oracle_lib.OracleMe8qIndex(x, cm, lab, avg_bits=avg, seed=seed, plan_spec=spec, threads=4)
+    ids, d, cand, surv = orc.search_pruned(q, k, nprobe, alpha=alpha, threads=4)
+    assert np.array_equal(ids, G["search_ids"])
+    assert rel_err(d, G["search_dists"]).max() < 1e-6
+    assert np.array_equal(cand, G["candidates"]) and np.array_equal(surv, G["survivors"])
+    # the cascade prunes: most scanned rows never reach the heap
+    assert surv.sum() < 0.2 * cand.sum()
