@@ -5,8 +5,9 @@ Produces, next to the package sources (so they travel with the tree):
   e8qlib/_e8qlib<ext>             pybind11 module over the C ABI
 
 Every .cu file is compiled for sm_100a only
-(-gencode arch=compute_100a,code=sm_100a). build_kernels.cu and me8q_kernels.cu
-additionally use --fmad=false (bit-exact encoder and ME8Q fits). Host C++ uses -ffp-contract=off. Objects
+(-gencode arch=compute_100a,code=sm_100a). build_kernels.cu, me8q_kernels.cu and
+me8q_fast.cu additionally use --fmad=false (bit-exact encoder, ME8Q fits and
+the pruned search's bound arithmetic). Host C++ uses -ffp-contract=off. Objects
 are rebuilt when a source or header is newer than its object.
 
 Usage: python e8q-artifact_b200/build.py [-j N] [--force]
@@ -35,7 +36,7 @@ EXT = os.path.join(PKG, "_e8qlib" + sysconfig.get_config_var("EXT_SUFFIX"))
 
 CU_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INC, "-I" + CSRC,
             "--expt-relaxed-constexpr", "-diag-suppress", "940"]
-PER_FILE = {"build_kernels.cu": ["--fmad=false"], "me8q_kernels.cu": ["--fmad=false"]}
+PER_FILE = {"build_kernels.cu": ["--fmad=false"], "me8q_kernels.cu": ["--fmad=false"], "me8q_fast.cu": ["--fmad=false"]}
 CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", "-Wextra",
              "-I" + INC, "-I" + CSRC, "-I" + os.path.join(CUDA, "include")]
 

@@ -59,9 +59,10 @@ int mode_of(const std::string& m) {
 // ME8Q search modes: the grouped exact scan, or int8 tensor-core candidates
 // with exact rescoring.
 int me8q_mode(const std::string& m) {
+    if (m == "pruned") return E8QC_MODE_PRUNED;
     if (m == "batched") return E8QC_MODE_BATCHED;
     if (m == "precision") return E8QC_MODE_PRECISION;
-    throw std::invalid_argument("ME8Q modes are 'batched' and 'precision'");
+    throw std::invalid_argument("ME8Q modes are 'pruned', 'batched' and 'precision'");
 }
 
 class E8qIndex {
@@ -881,7 +882,7 @@ PYBIND11_MODULE(_e8qlib, m) {
              py::arg("num_threads") = 1, py::arg("variance") = py::none(), py::arg("drop_energy") = true,
              py::arg("prune_alpha") = 0.0F, py::arg("plan_spec") = "", py::arg("extra_budget_bits") = 0.0)
         .def("search", &e8qb200::Me8qIndex::search, py::arg("queries"), py::arg("k"), py::arg("nprobe"),
-             py::arg("num_threads") = 1, py::arg("return_stats") = false, py::arg("mode") = "batched")
+             py::arg("num_threads") = 1, py::arg("return_stats") = false, py::arg("mode") = "pruned")
         .def("estimate", &e8qb200::Me8qIndex::estimate, py::arg("query"), py::arg("id"))
         .def_static("load", &e8qb200::Me8qIndex::load, py::arg("path"), py::arg("device") = 0)
         .def("save", &e8qb200::Me8qIndex::save, py::arg("path"))

@@ -201,6 +201,9 @@ struct e8qc_me8q {
     DevBuf runs_d, chunks_d, levels, signs, cen_pad, cen_rot, cn2, tile_begin_d, list_len_d, list_order_d,
         list_of_tile_d, ids, codes, coef, h2, hsum, list_begin_d;
     DevBuf proxy, sigma;                 // precision mode: int8 proxy plane and per-slot scale (built on first use)
+    // pruned mode: the fast layout (me8q_fast.cu), built on first use
+    DevBuf f_runs, f_plane, f_gain, f_vpc, f_bank, f_scl, f_rcn2;
+    Me8qFast fast{};
     std::vector<uint64_t> tiles_prefix;  // prefix sums of the lists' tile counts, largest first
     Me8qView view{};
     Workspace ws;
@@ -210,7 +213,8 @@ struct e8qc_me8q {
     size_t memory_bytes() const {
         return runs_d.bytes + chunks_d.bytes + levels.bytes + signs.bytes + cen_pad.bytes + cen_rot.bytes + cn2.bytes +
                tile_begin_d.bytes + list_len_d.bytes + list_order_d.bytes + list_of_tile_d.bytes + ids.bytes +
-               codes.bytes + coef.bytes + h2.bytes + hsum.bytes + list_begin_d.bytes + proxy.bytes + sigma.bytes;
+               codes.bytes + coef.bytes + h2.bytes + hsum.bytes + list_begin_d.bytes + proxy.bytes + sigma.bytes +
+               f_runs.bytes + f_plane.bytes + f_gain.bytes + f_vpc.bytes + f_bank.bytes + f_scl.bytes + f_rcn2.bytes;
     }
 };
 
@@ -338,6 +342,8 @@ void setup_lists(e8qc_me8q* x, const std::vector<uint32_t>& cnt, cudaStream_t s)
     x->nslots = x->ntiles * 32;
     x->proxy.release();
     x->sigma.release();
+    x->f_plane.release();
+    x->fast = Me8qFast{};
     {
         std::vector<uint64_t> t(nlist);
         for (size_t c = 0; c < nlist; ++c) t[c] = x->tile_begin[c + 1] - x->tile_begin[c];
@@ -779,6 +785,79 @@ void check_mode(int mode) {
         fail(E8QC_EINVAL, "ME8Q search modes are E8QC_MODE_BATCHED and E8QC_MODE_PRECISION");
 }
 
+// The direct search also takes E8QC_MODE_PRUNED (the reference's production
+// search; uniform k and nprobe).
+void check_search_mode(int mode) {
+    if (mode != E8QC_MODE_PRUNED) check_mode(mode);
+}
+
+// The pruned search's fast layout, built on first use (synchronises s):
+// plane, fits and banks from the code streams (me8q_fast.cu).
+void ensure_fast(e8qc_me8q* x, cudaStream_t s) {
+    if (x->f_plane.p) return;
+    std::vector<Me8qFastRun> fr;
+    int blk0 = 0;
+    std::vector<float> lev_host;
+    for (const auto& r : x->runs) {
+        if (r.bits == 0) continue;
+        Me8qFastRun f{};
+        f.off = r.off;
+        f.len = r.len;
+        f.bits = r.bits;
+        f.word0 = r.word0;
+        f.blk0 = blk0;
+        blk0 += r.len / 8;
+        // ClassModelOf (me8q_codec.cpp:235-262): pbar[c] = mean of the float
+        // levels of both branches whose top bit is c, summed in fp64
+        const int q = 1 << r.bits, half = q >> 1;
+        double sums[2] = {0.0, 0.0};
+        for (int c = 0; c < 2; ++c)
+            for (int br = 0; br < 2; ++br) {
+                const std::vector<double> lv = branch_levels(r.bits, br);
+                for (int d = c * half; d < (c + 1) * half; ++d) sums[c] += static_cast<double>(static_cast<float>(lv[d]));
+            }
+        f.p0 = static_cast<float>(sums[0] / static_cast<double>(2 * half));
+        f.p1 = static_cast<float>(sums[1] / static_cast<double>(2 * half));
+        fr.push_back(f);
+    }
+    // level-table offsets as the code streams' chunks hold them
+    for (auto& f : fr)
+        for (const auto& c : x->chunks)
+            if (c.bits == f.bits) {
+                f.lev = c.lev;
+                break;
+            }
+    Me8qFast& F = x->fast;
+    F = Me8qFast{};
+    F.nrun = static_cast<int>(fr.size());
+    F.cols = blk0;
+    F.colw = (blk0 + 3) / 4;
+    if (F.nrun > kFastMaxRuns || F.cols > kFastMaxCols)
+        fail(E8QC_EINVAL, "the ME8Q pruned search supports at most 512 coded blocks and 16 coded runs");
+    const size_t nr = std::max<size_t>(1, fr.size());
+    if (fr.empty()) fr.push_back(Me8qFastRun{});
+    x->f_runs.upload(fr.data(), fr.size() * sizeof(Me8qFastRun), s);
+    x->f_plane.alloc(std::max<size_t>(1, x->ntiles * static_cast<size_t>(F.colw) * 32 * 4));
+    x->f_gain.alloc(nr * std::max<size_t>(1, x->nslots) * 4);
+    x->f_vpc.alloc(nr * std::max<size_t>(1, x->nslots) * 4);
+    x->f_bank.alloc(std::max<size_t>(1, x->ntiles) * nr * 96);
+    x->f_scl.alloc(std::max<size_t>(1, x->ntiles) * nr * 32);
+    x->f_rcn2.alloc(std::max<size_t>(1, x->nlist) * nr * 8);
+    F.runs = x->f_runs.as<Me8qFastRun>();
+    F.plane = x->f_plane.as<uint32_t>();
+    F.gain = x->f_gain.as<float>();
+    F.vpc = x->f_vpc.as<float>();
+    F.bank = x->f_bank.as<uint8_t>();
+    F.scl = x->f_scl.as<float>();
+    F.rc_n2 = x->f_rcn2.as<double>();
+    DevBuf perp;
+    perp.alloc(nr * std::max<size_t>(1, x->nslots) * 4);
+    fill_view(x);
+    launch_me8q_fast_build(x->view, F, x->f_plane.as<uint32_t>(), x->f_gain.as<float>(), x->f_vpc.as<float>(),
+                           perp.as<float>(), x->f_bank.as<uint8_t>(), x->f_scl.as<float>(), x->f_rcn2.as<double>(), s);
+    E8QC_CUDA(cudaStreamSynchronize(s));
+}
+
 // The precision proxy plane, built on first use (synchronises s).
 void ensure_proxy(e8qc_me8q* x, cudaStream_t s) {
     if (x->proxy.p) return;
@@ -806,6 +885,15 @@ uint64_t enqueue_search(e8qc_me8q* x, Workspace& ws, int mode, const float* q_de
     ws.ensure_err();
     launch_me8q_prep(q_dev, x->dim, static_cast<int>(x->dim), static_cast<int>(x->pd), nullptr, nullptr, x->view, 0,
                      nq, ws.rq.as<float>(), nullptr, nullptr, s);
+    if (mode == E8QC_MODE_PRUNED) {
+        if (!x->f_plane.p) fail(E8QC_ESTATE, "the ME8Q fast layout is not built");
+        if (k_arr || np_arr) fail(E8QC_EINVAL, "the ME8Q pruned search takes a uniform k and nprobe");
+        const float alpha = x->prune_alpha > 0.0F ? x->prune_alpha : 1.0F;
+        const float lambda = ortho_quantile(static_cast<double>(alpha), std::max<size_t>(4 * k, 32));
+        if (x->fast.nrun == 0) fail(E8QC_EINVAL, "the ME8Q pruned search needs at least one coded run");
+        return 1 + static_cast<uint64_t>(me8q_pruned_search(x->view, x->fast, ws, ws.rq.as<float>(), nq, k, np,
+                                                            lambda, out_stride, ids_d, d_d, s));
+    }
     if (mode == E8QC_MODE_PRECISION) {
         if (!x->view.base.proxy) fail(E8QC_ESTATE, "the ME8Q proxy plane is not built");
         return 1 + static_cast<uint64_t>(precision_search(x->view.base, ws, ws.rq.as<float>(), nq, k_arr, np_arr, k,
@@ -1049,7 +1137,7 @@ int e8qc_me8q_search_mode(e8qc_me8q* x, const float* queries, size_t nq, size_t 
                           uint32_t* out_ids, float* out_dists, e8qc_stats* stats, void* stream) {
     return guarded([&] {
         require_built(x, "search");
-        check_mode(mode);
+        check_search_mode(mode);
         if (k == 0) fail(E8QC_EINVAL, "k must be positive");
         if (k > static_cast<size_t>(kMaxK)) fail(E8QC_EINVAL, "k must be <= 128");
         if (nprobe == 0) fail(E8QC_EINVAL, "nprobe must be positive");
@@ -1078,6 +1166,7 @@ int e8qc_me8q_search_mode(e8qc_me8q* x, const float* queries, size_t nq, size_t 
             d_d = ws.stage_d.as<float>();
         }
         if (mode == E8QC_MODE_PRECISION) ensure_proxy(x, s);
+        if (mode == E8QC_MODE_PRUNED) ensure_fast(x, s);
         apply_stored(x, ws, mode, nq, np);
         const uint64_t launches = enqueue_search(x, ws, mode, qd, nq, nullptr, nullptr, k, np, k, ids_d, d_d, s);
         if (!ids_dev) E8QC_CUDA(cudaMemcpyAsync(out_ids, ids_d, nq * k * 4, cudaMemcpyDeviceToHost, s));
@@ -1086,10 +1175,15 @@ int e8qc_me8q_search_mode(e8qc_me8q* x, const float* queries, size_t nq, size_t 
         if (stats) {
             std::memset(stats, 0, sizeof(*stats));
             uint64_t cntv[2] = {0, 0};
-            E8QC_CUDA(cudaMemcpyAsync(cntv, ws.b_nitems.as<uint32_t>() + 2, 16, cudaMemcpyDeviceToHost, s));
+            if (mode == E8QC_MODE_PRUNED) {
+                E8QC_CUDA(cudaMemcpyAsync(cntv, ws.f_counts.p, 16, cudaMemcpyDeviceToHost, s));
+            } else {
+                E8QC_CUDA(cudaMemcpyAsync(cntv, ws.b_nitems.as<uint32_t>() + 2, 16, cudaMemcpyDeviceToHost, s));
+                cntv[1] = cntv[0];
+            }
             E8QC_CUDA(cudaStreamSynchronize(s));
             stats->candidates = cntv[0];
-            stats->survivors = cntv[0];
+            stats->survivors = cntv[1];
             stats->launches = launches;
         }
     });

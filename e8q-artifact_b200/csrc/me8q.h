@@ -50,6 +50,40 @@ struct Me8qView {
     size_t nslots;
 };
 
+// The fast layout of the production (pruned) search, me8q_fast.cu.
+constexpr int kFastMaxRuns = 16;   // coded runs
+constexpr int kFastMaxCols = 512;  // coded 8-dim blocks (4,096 coded dims)
+
+// A coded run as the pruned search sees it: dims [off, off + len) at bits
+// per digit, its first stream word and level-table offset, its first plane
+// column, and the scan basis pbar[0], pbar[1] of its rate (ClassModelOf,
+// src/quantization/me8q_codec.cpp:235-262).
+struct Me8qFastRun {
+    int off, len, bits, word0, lev, blk0;
+    float p0, p1;
+};
+
+struct Me8qFast {
+    int nrun, cols, colw;    // coded runs, plane columns, plane words per lane (ceil(cols / 4))
+    const Me8qFastRun* runs;  // nrun
+    const uint32_t* plane;    // ntiles x colw x 32 words
+    const float* gain;        // nrun x nslots
+    const float* vpc;         // nrun x nslots
+    const uint8_t* bank;      // ntiles x nrun x 96: base[32], weight[32], perp[32]
+    const float* scl;         // ntiles x nrun x 8: (min, step) of base, weight, perp
+    const double* rc_n2;      // nlist x nrun: ||centroid slice of the run||^2
+};
+
+// Builds the fast layout of a built index (perp: nrun x nslots scratch).
+int launch_me8q_fast_build(const Me8qView& v, const Me8qFast& f, uint32_t* plane, float* gain, float* vpc,
+                           float* perp, uint8_t* bank, float* scl, double* rc_n2, cudaStream_t s);
+
+// The production search of nq rotated queries (uniform k and nprobe):
+// route, per-query select, per-query LUT, the cascade (one warp per query).
+int me8q_pruned_search(const Me8qView& v, const Me8qFast& f, Workspace& ws, const float* rq, size_t nq, size_t k,
+                       size_t nprobe, float lambda, size_t out_stride, uint32_t* out_ids, float* out_d,
+                       cudaStream_t s);
+
 // Per-dimension variance (float mean row by row, fp64 spread; one thread
 // per dimension so the sums follow the reference's order).
 int launch_me8q_variance(const float* x, size_t n, int dim, float* var, cudaStream_t s);

@@ -70,6 +70,9 @@ struct Workspace {
     // pruned path: per-CTA best coarse estimates and keys, the grid-barrier
     // and finish counters, candidate/survivor counts, per-query thresholds
     DevBuf pr_dc, pr_key, pr_counters, pr_stats, pr_thr;
+    // ME8Q pruned path: per-query u8 LUTs, per-run scalars, LUT steps,
+    // thresholds, and the candidate / survivor counts
+    DevBuf f_lut, f_qrun, f_delta, f_thr, f_counts;
     size_t pr_grid_cap = 0, pr_thr_cap = 0, pr_last_nq = 0;
     // tuning of the grouped paths (chosen by the autotuner): work-queue order
     // (0: longest list first, 1: list id order) and the precision scan's

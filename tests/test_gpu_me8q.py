@@ -51,7 +51,7 @@ def test_me8q_gpu_matches_reference_fixtures(e8q, name):
     _assert_codes_equal(idx, G["ids"], G["digits"], G["branch"], G["coef"], G["h2"])
     est = np.array([[idx.estimate(q[i], int(g)) for g in G["est_ids"]] for i in range(nq)], np.float32)
     assert rel_err(est, G["est"]).max() < 1e-6
-    ids, d = idx.search(q, k, nprobe)
+    ids, d = idx.search(q, k, nprobe, mode="batched")
     assert_topk_parity(ids, d, G["search_ids"], G["search_dists"], rtol=RTOL)
 
 
@@ -89,7 +89,7 @@ def test_me8q_gpu_matches_oracle(e8q, oracle_lib, dim, avg, seed, kw):
         a, b = idx.estimate(q[0], gid), orc.estimate(q[0], gid)
         assert rel_err(a, b) < 1e-6, gid
     for k, nprobe in ((10, 4), (64, 24), (128, 2)):
-        ids, d = idx.search(q, k, nprobe)
+        ids, d = idx.search(q, k, nprobe, mode="batched")
         oi, od = orc.search(q, k, nprobe)
         assert_topk_parity(ids, d, oi, od, rtol=RTOL)
 
@@ -111,7 +111,7 @@ def test_me8q_gpu_given_variance_and_ragged_lists(e8q, oracle_lib):
     assert [tuple(p) for p in idx.plan] == [tuple(p) for p in orc.plan]
     _assert_codes_equal(idx, orc.ids, *_oracle_codes(orc))
     for k, nprobe in ((10, 3), (128, 2), (5, 1000)):
-        ids, d = idx.search(q, k, nprobe)
+        ids, d = idx.search(q, k, nprobe, mode="batched")
         oi, od = orc.search(q, k, nprobe)
         assert_topk_parity(ids, d, oi, od, rtol=RTOL)
     empty_ids, empty_d = idx.search(np.zeros((0, dim), np.float32), 10, 4)
@@ -147,7 +147,7 @@ def test_me8q_gpu_all_dropped_plan(e8q, oracle_lib):
     assert idx.plan == [(128, 0)]
     assert idx.bits_per_dim == 0.0
     assert rel_err(idx.estimate(q[0], 3), orc.estimate(q[0], 3)) < 1e-6
-    ids, d = idx.search(q, 10, 2)
+    ids, d = idx.search(q, 10, 2, mode="batched")
     oi, od = orc.search(q, 10, 2)
     assert np.allclose(np.sort(d, axis=1), np.sort(od, axis=1), rtol=RTOL, atol=1e-5)
 
@@ -161,7 +161,7 @@ def test_me8q_gpu_precision_mode(e8q, oracle_lib, dim, avg, spec):
     q = det_mixture(7200 + dim, nq, dim, nlist, 0.6)[0]
     orc, idx = _build_both(e8q, oracle_lib, x, cm, lab, avg_bits=avg, seed=9, plan_spec=spec)
     for k, nprobe in ((10, 8), (100, 4), (1, 32)):
-        ei, ed = idx.search(q, k, nprobe)  # exact grouped scan
+        ei, ed = idx.search(q, k, nprobe, mode="batched")  # exact grouped scan
         pi, pdd = idx.search(q, k, nprobe, mode="precision")
         oi, od = orc.search(q, k, nprobe)
         hits = sum(len(set(a.tolist()) & set(b.tolist())) for a, b in zip(pi, ei))

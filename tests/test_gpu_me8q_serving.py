@@ -38,7 +38,7 @@ def test_me8q_search_ragged_matches_uniform(e8q, index):
     npb = rng.integers(1, 41, len(q)).astype(np.uint32)
     ids, d = idx.search_ragged(q, k, npb, 64)
     for i in range(0, len(q), 37):
-        ai, ad = idx.search(q[i:i + 1], int(k[i]), int(npb[i]))
+        ai, ad = idx.search(q[i:i + 1], int(k[i]), int(npb[i]), mode="batched")
         assert np.array_equal(ids[i, :k[i]], ai[0]) and np.array_equal(d[i, :k[i]].view(np.uint32),
                                                                        ad[0].view(np.uint32)), i
         assert np.all(ids[i, k[i]:] == 0xFFFFFFFF) and np.all(np.isinf(d[i, k[i]:]))

@@ -38,7 +38,7 @@ def _worker(rank, world, port, kind, nbits, x, cm, lab, q, k, nprobe, var, ref_i
             ids, d = sh.search(q, k, nprobe, mode="plain")
         else:
             sh.build(x, cm, lab, variance=var)
-            ids, d = sh.search(q, k, nprobe)
+            ids, d = sh.search(q, k, nprobe, mode="batched")
         assert np.nonzero(sh.owner == rank)[0].size > 0
         assert_topk_parity(ids, d, ref_ids, ref_d)
     finally:
@@ -68,7 +68,7 @@ def test_two_rank_me8q_cuda_shards_match_single_index():
     var = x.astype(np.float64).var(axis=0).astype(np.float32)
     single = e8qlib.Me8qIndex(dim, 4.0, 3, device=0)
     single.build(x, cm, lab, variance=var)
-    ref_ids, ref_d = single.search(q, k, nprobe)
+    ref_ids, ref_d = single.search(q, k, nprobe, mode="batched")
     del single
     mp.spawn(_worker, args=(2, _port(), "me8q", 4.0, x, cm, lab, q, k, nprobe, var, ref_ids, ref_d), nprocs=2,
              join=True)
