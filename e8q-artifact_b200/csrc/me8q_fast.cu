@@ -355,12 +355,131 @@ struct WarpHeap {
 
 // Per-warp shared memory of the cascade kernel (sizes in bytes).
 // The u8 LUT first (16-byte aligned), then fp64 sqrt(d2_r) and the group's
-// s_c and t (4 members), then acc, s_c and t per (run, lane); a multiple of
-// 16 bytes so every warp's slice stays aligned.
+// s_c and t (4 members), the group's (coef, h2, gain, vpc) per (member,
+// run), then acc, s_c and t per (run, lane), then two tile
+// stages (the tile's plane words, then per run its 96 bank bytes and 8
+// scales); a multiple of 16 bytes so every warp's slice stays aligned.
+__host__ __device__ inline size_t cascade_stage_words(int cols, int nrun) {
+    return static_cast<size_t>((cols + 3) / 4) * 32 + static_cast<size_t>(nrun) * 32;
+}
 __host__ __device__ inline size_t cascade_warp_bytes(int cols, int nrun) {
     const size_t b = static_cast<size_t>(cols) * 32 + static_cast<size_t>(nrun) * 8 * (1 + 8) +
-                     static_cast<size_t>(nrun) * 32 * 4 * 3;
+                     static_cast<size_t>(nrun) * 4 * 4 * 4 + 128 + static_cast<size_t>(nrun) * 32 * 4 * 3 +
+                     2 * cascade_stage_words(cols, nrun) * 4;
     return (b + 15) / 16 * 16;
+}
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Stage tile `tile` (plane words, banks and scales) into one of the warp's
+// two buffers, asynchronously (one commit group per tile).
+__device__ __forceinline__ void stage_tile(const Me8qFast& f, size_t tile, uint32_t* dst) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t* src = f.plane + tile * f.colw * 32;
+    for (int w = 0; w < f.colw; ++w) cp_async4(dst + w * 32 + lane, src + w * 32 + lane);
+    uint32_t* bd = dst + f.colw * 32;
+    for (int r = 0; r < f.nrun; ++r) {
+        const uint32_t* bs = lane < 24 ? reinterpret_cast<const uint32_t*>(f.bank + (tile * f.nrun + r) * 96) + lane
+                                       : reinterpret_cast<const uint32_t*>(f.scl + (tile * f.nrun + r) * 8) + (lane - 24);
+        cp_async4(bd + r * 32 + lane, bs);
+    }
+    cp_async_commit();
+}
+
+// flush4 (me8q_fast.cpp:830-960) for a group of bn <= 4 members: the runs
+// in the order of the group's mean t^2 per block (largest first, ties in
+// run order), each run's exact score replacing its coarse term, death once
+// the remaining slack cannot bring a member under dk. Writes the members'
+// distances to dist and returns the mask of the dead. Out of line: one copy
+// of this rarely-run code keeps the scan loop's instruction stream small.
+static __device__ __noinline__ unsigned flush_group(const Me8qView& v, const Me8qFast& f, const float* qv, size_t tile,
+                                                    int bn, double d2, float lambda, double dk, const int* g_ln,
+                                                    const double* g_pq, const double* g_sc, const double* g_tr,
+                                                    float* g_fac, double* dist) {
+    const int lane = threadIdx.x & 31;
+    const int nr = f.nrun;
+    // the group's factors, one load per (member, run)
+    for (int i = lane; i < bn * nr; i += 32) {
+        const int j = i / nr, r = i - j * nr;
+        const size_t o = static_cast<size_t>(r) * v.nslots + tile * 32 + g_ln[j];
+        float* fo = g_fac + (j * nr + r) * 4;
+        fo[0] = __ldg(v.coef + o);
+        fo[1] = __ldg(v.h2 + o);
+        fo[2] = __ldg(f.gain + o);
+        fo[3] = __ldg(f.vpc + o);
+    }
+    __syncwarp();
+    int order[kFastMaxRuns];
+    double mean[kFastMaxRuns];
+    for (int r = 0; r < nr; ++r) {
+        order[r] = r;
+        double a = 0.0;
+        for (int j = 0; j < bn; ++j) a = fma(g_tr[j * nr + r], g_tr[j * nr + r], a);
+        const int nb = f.runs[r].len / 8;
+        mean[r] = __ddiv_rn(a, static_cast<double>(nb > 1 ? nb : 1));
+    }
+    for (int a = 1; a < nr; ++a)
+        for (int z = a; z > 0 && mean[order[z]] > mean[order[z - 1]]; --z) {
+            const int t = order[z];
+            order[z] = order[z - 1];
+            order[z - 1] = t;
+        }
+    double dj[4], rem[4];
+    unsigned dead = 0;
+    for (int j = 0; j < 4; ++j) {
+        rem[j] = j < bn ? g_pq[2 * j] : 0.0;
+        dj[j] = d2;
+        if (j >= bn) {
+            dead |= 1u << j;
+            continue;
+        }
+        if (nr == 1) {
+            dj[j] = __dadd_rn(d2, static_cast<double>(g_fac[j * 4 + 1]));
+        } else {
+            double dcc = d2;
+            for (int r = 0; r < nr; ++r) {
+                const float* fo = g_fac + (j * nr + r) * 4;
+                dcc = __dadd_rn(dcc, fma(-(2.0 * static_cast<double>(fo[0])),
+                                         fma(static_cast<double>(fo[2]), g_sc[j * nr + r], static_cast<double>(fo[3])),
+                                         static_cast<double>(fo[1])));
+            }
+            dj[j] = dcc;
+        }
+    }
+    for (int oi = 0; oi < nr; ++oi) {
+        const int r = order[oi];
+        const Me8qFastRun run = f.runs[r];
+#pragma unroll 1
+        for (int j = 0; j < bn; ++j) {
+            if ((dead >> j) & 1u) continue;
+            const float* fo = g_fac + (j * nr + r) * 4;
+            const double coef = static_cast<double>(fo[0]);
+            const double s_ex = static_cast<double>(run_score_warp(v, run, tile * 32 + g_ln[j], qv));
+            if (nr == 1) {
+                dj[j] = fma(-(2.0 * coef), s_ex, dj[j]);
+            } else {
+                const double u = fma(static_cast<double>(fo[2]), g_sc[j * nr + r], static_cast<double>(fo[3]));
+                dj[j] = fma(2.0 * coef, __dsub_rn(u, s_ex), dj[j]);
+            }
+            const double t = g_tr[j * nr + r];
+            rem[j] = fma(-t, t, rem[j]);
+            if (__dsub_rn(fma(-static_cast<double>(lambda), sqrt(rem[j] > 0.0 ? rem[j] : 0.0), dj[j]),
+                          g_pq[2 * j + 1]) >= dk)
+                dead |= 1u << j;
+        }
+    }
+    if (lane == 0)
+        for (int j = 0; j < bn; ++j) dist[j] = dj[j];
+    __syncwarp();
+    return dead;
 }
 
 // One warp per query: the reference's ScanPreRouted (me8q_fast.cpp:548-1090)
@@ -371,7 +490,7 @@ __host__ __device__ inline size_t cascade_warp_bytes(int cols, int nrun) {
 // the tail lanes), groups of 4 through the run cascade (flush4) and into the
 // heap. Coarse accumulators and the filter run lane-parallel, run scores
 // warp-cooperatively; everything else is warp-uniform.
-__global__ void __launch_bounds__(kFastWarps * 32) me8q_cascade_kernel(
+__global__ void __launch_bounds__(kFastWarps * 32, 2) me8q_cascade_kernel(
     Me8qView v, Me8qFast f, const float* __restrict__ rq, const uint8_t* __restrict__ lut8,
     const double* __restrict__ qrun, const float* __restrict__ qdelta, const uint32_t* __restrict__ probes,
     const float* __restrict__ pd2, int nq, int np, int k, float lambda, int out_stride, uint32_t* __restrict__ out_ids,
@@ -387,9 +506,15 @@ __global__ void __launch_bounds__(kFastWarps * 32) me8q_cascade_kernel(
     double* s_sd2 = reinterpret_cast<double*>(base + lut_bytes);     // nr
     double* g_sc = s_sd2 + nr;                                       // 4 x nr
     double* g_tr = g_sc + 4 * nr;                                    // 4 x nr
-    int* s_acc = reinterpret_cast<int*>(g_tr + 4 * nr);              // nr x 32
+    double* g_pq = g_tr + 4 * nr;                                    // 4 x (pool, qadd)
+    double* g_dist = g_pq + 8;                                       // 4 flushed distances
+    int* g_ln = reinterpret_cast<int*>(g_dist + 4);                  // 4 member lanes (+ pad)
+    float* g_fac = reinterpret_cast<float*>(g_ln + 8);               // 4 x nr x 4
+    int* s_acc = reinterpret_cast<int*>(g_fac + 16 * nr);            // nr x 32
     float* s_sc = reinterpret_cast<float*>(s_acc + nr * 32);         // nr x 32
     float* s_tr = s_sc + nr * 32;                                    // nr x 32
+    uint32_t* stg = reinterpret_cast<uint32_t*>(s_tr + nr * 32);     // 2 tile stages
+    const int stg_words = static_cast<int>(cascade_stage_words(cols, nr));
     {
         const uint4* src = reinterpret_cast<const uint4*>(lut8 + static_cast<size_t>(q) * lut_bytes);
         uint4* dst = reinterpret_cast<uint4*>(lut);
@@ -437,28 +562,44 @@ __global__ void __launch_bounds__(kFastWarps * 32) me8q_cascade_kernel(
             if (lane == 0) s_sd2[r] = sqrt(d2r > 0.0 ? d2r : 0.0);
         }
         __syncwarp();
+        stage_tile(f, tile0, stg);
         for (uint32_t i0 = 0; i0 < len; i0 += 32) {
             const int m = static_cast<int>(min(32u, len - i0));
             const size_t tile = tile0 + (i0 >> 5);
             const int covered = m >= 16 ? (m / 16) * 16 : 0;
             const float distk0 = heap.distk();
             const float sdk = distk0 < inf_f() ? sqrtf(fmaxf(distk0, 0.0f)) : inf_f();
+            // the next tile streams in while this one is scored
+            const int buf = static_cast<int>((i0 >> 5) & 1u);
+            if (i0 + 32 < len) {
+                stage_tile(f, tile + 1, stg + (buf ^ 1) * stg_words);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncwarp();
+            const uint32_t* stp = stg + buf * stg_words;
+            const uint8_t* stb = reinterpret_cast<const uint8_t*>(stp + f.colw * 32);  // per run 128 B
             // coarse accumulators (AccumulateCoarseHi) and the fp32 filter
-            const uint32_t* pw = f.plane + tile * f.colw * 32 + lane;
+            const uint32_t* pw = stp + lane;
             float dc = d2f, pool = 0.0f, qa = 0.0f, wpad = 0.0f;
             for (int r = 0; r < nr; ++r) {
                 const Me8qFastRun run = f.runs[r];
+                // a run covers whole plane words (its length is a multiple
+                // of 64 dims): one word = 4 columns = 8 LUT entries
                 int acc = 0;
-                uint32_t word = 0;
-                for (int col = run.blk0; col < run.blk0 + run.len / 8; ++col) {
-                    if (col == run.blk0 || (col & 3) == 0) word = __ldg(pw + (col >> 2) * 32);
-                    const uint32_t b = (word >> ((col & 3) * 8)) & 0xFFu;
-                    acc += lut[col * 32 + (b & 15u)] + lut[col * 32 + 16 + (b >> 4)];
+#pragma unroll 4
+                for (int w = run.blk0 >> 2; w < (run.blk0 + run.len / 8) >> 2; ++w) {
+                    const uint32_t word = pw[w * 32];
+                    const uint8_t* lc = lut + w * 128;
+                    acc += lc[word & 15u] + lc[16 + ((word >> 4) & 15u)] + lc[32 + ((word >> 8) & 15u)] +
+                           lc[48 + ((word >> 12) & 15u)] + lc[64 + ((word >> 16) & 15u)] +
+                           lc[80 + ((word >> 20) & 15u)] + lc[96 + ((word >> 24) & 15u)] + lc[112 + (word >> 28)];
                 }
                 s_acc[r * 32 + lane] = acc;
                 const double* qr = qr0 + r * 4;
-                const float* sc = f.scl + (tile * nr + r) * 8;
-                const uint8_t* bp = f.bank + (tile * nr + r) * 96;
+                const uint8_t* bp = stb + r * 128;
+                const float* sc = reinterpret_cast<const float*>(bp + 96);
                 const float sd2 = static_cast<float>(s_sd2[r]);
                 const float rh = sdk < sd2 ? sdk : sd2;
                 const float wp = static_cast<float>(0.5 * static_cast<double>(sc[3]) * (qr[3] + qr[2]));
@@ -478,158 +619,104 @@ __global__ void __launch_bounds__(kFastWarps * 32) me8q_cascade_kernel(
             const float lane_qa = __fadd_rn(qa, wpad);
             const float slack = fmaf(lambda, sqrtf(pool), lane_qa);
             const bool filtered = lane < covered && __fsub_rn(dc, slack) >= distk0;
-            unsigned kmask = __ballot_sync(kFull, lane < m && !filtered);
+            const bool cand = lane < m && !filtered;
+            // The reference then walks the kept lanes in order, testing each
+            // against the heap's k-th distance at its turn; that distance only
+            // changes when a group of 4 is flushed, so the test values are
+            // taken lane-parallel and re-taken after each flush. A filter
+            // lane's value does not depend on the heap.
+            const double val_f = lane < covered
+                                     ? __dsub_rn(static_cast<double>(dc),
+                                                 fma(static_cast<double>(lambda), sqrt(static_cast<double>(pool)),
+                                                     static_cast<double>(lane_qa)))
+                                     : 0.0;
             __syncwarp();
             n_cand += static_cast<unsigned long long>(m);
             int bn = 0;
-            int g_lane[4];
-            double g_pool[4], g_qadd[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                g_lane[j] = 0;
-                g_pool[j] = 0.0;
-                g_qadd[j] = 0.0;
-            }
+            int pos = -1;  // the last lane taken in order
             for (;;) {
-                const bool have = kmask != 0;
-                if (have) {
-                const int l = __ffs(kmask) - 1;
-                kmask &= kmask - 1;
                 const float dkf = heap.distk();
                 const double distk = static_cast<double>(dkf);
-                double dc_q, pool2, qadd;
-                if (l < covered) {
-                    dc_q = static_cast<double>(__shfl_sync(kFull, dc, l));
-                    pool2 = static_cast<double>(__shfl_sync(kFull, pool, l));
-                    qadd = static_cast<double>(__shfl_sync(kFull, lane_qa, l));
-                    if (lane < nr) {
-                        g_sc[bn * nr + lane] = static_cast<double>(s_sc[lane * 32 + l]);
-                        g_tr[bn * nr + lane] = static_cast<double>(s_tr[lane * 32 + l]);
-                    }
-                } else {
-                    // the scalar twin (me8q_fast.cpp:1000-1040), fp64, in run order
-                    dc_q = d2;
-                    pool2 = 0.0;
-                    qadd = 0.0;
-                    const double sk = dkf < inf_f() ? sqrt(distk > 0.0 ? distk : 0.0) : static_cast<double>(inf_f());
+                const double sk = dkf < inf_f() ? sqrt(distk > 0.0 ? distk : 0.0) : static_cast<double>(inf_f());
+                // the scalar twin of the tail lanes (me8q_fast.cpp:1000-1040) at this k-th distance
+                double val = val_f, t_pool = 0.0, t_qadd = 0.0;
+                if (cand && lane >= covered && lane > pos) {
+                    double dc_q = d2;
                     for (int r = 0; r < nr; ++r) {
                         const double* qr = qr0 + r * 4;
                         const float* sc = f.scl + (tile * nr + r) * 8;
                         const uint8_t* bp = f.bank + (tile * nr + r) * 96;
                         const double s_cr =
-                            fma(static_cast<double>(delta), static_cast<double>(s_acc[r * 32 + l]), qr[1]);
-                        const double base_q = fma(static_cast<double>(bp[l]), static_cast<double>(sc[1]),
+                            fma(static_cast<double>(delta), static_cast<double>(s_acc[r * 32 + lane]), qr[1]);
+                        const double base_q = fma(static_cast<double>(bp[lane]), static_cast<double>(sc[1]),
                                                   static_cast<double>(sc[0]));
-                        const double weight_q = fma(static_cast<double>(bp[32 + l]), static_cast<double>(sc[3]),
+                        const double weight_q = fma(static_cast<double>(bp[32 + lane]), static_cast<double>(sc[3]),
                                                     static_cast<double>(sc[2]));
-                        const double perp_q = fma(static_cast<double>(bp[64 + l]), static_cast<double>(sc[5]),
+                        const double perp_q = fma(static_cast<double>(bp[64 + lane]), static_cast<double>(sc[5]),
                                                   static_cast<double>(sc[4]));
                         dc_q = __dadd_rn(dc_q, fma(-weight_q, s_cr, base_q));
                         const double rh = sk < s_sd2[r] ? sk : s_sd2[r];
                         const double tr = __dmul_rn(perp_q, rh);
-                        pool2 = fma(tr, tr, pool2);
-                        qadd = fma(fabs(weight_q), qr[2], qadd);
-                        qadd = fma(0.5 * static_cast<double>(sc[3]), __dadd_rn(qr[3], qr[2]), qadd);
-                        if (lane == 0) {
-                            g_sc[bn * nr + r] = s_cr;
-                            g_tr[bn * nr + r] = tr;
+                        t_pool = fma(tr, tr, t_pool);
+                        t_qadd = fma(fabs(weight_q), qr[2], t_qadd);
+                        t_qadd = fma(0.5 * static_cast<double>(sc[3]), __dadd_rn(qr[3], qr[2]), t_qadd);
+                    }
+                    val = __dsub_rn(dc_q, fma(static_cast<double>(lambda), sqrt(t_pool), t_qadd));
+                }
+                unsigned pass = __ballot_sync(kFull, cand && lane > pos && !(val >= distk));
+                bool full = false;
+                while (pass) {
+                    const int l = __ffs(pass) - 1;
+                    pass &= pass - 1;
+                    pos = l;
+                    double pool2, qadd;
+                    if (l < covered) {
+                        pool2 = static_cast<double>(__shfl_sync(kFull, pool, l));
+                        qadd = static_cast<double>(__shfl_sync(kFull, lane_qa, l));
+                        if (lane < nr) {
+                            g_sc[bn * nr + lane] = static_cast<double>(s_sc[lane * 32 + l]);
+                            g_tr[bn * nr + lane] = static_cast<double>(s_tr[lane * 32 + l]);
                         }
+                    } else {
+                        pool2 = __shfl_sync(kFull, t_pool, l);
+                        qadd = __shfl_sync(kFull, t_qadd, l);
+                        if (lane < nr) {
+                            const int r = lane;
+                            const double* qr = qr0 + r * 4;
+                            const float* sc = f.scl + (tile * nr + r) * 8;
+                            const uint8_t* bp = f.bank + (tile * nr + r) * 96;
+                            g_sc[bn * nr + r] =
+                                fma(static_cast<double>(delta), static_cast<double>(s_acc[r * 32 + l]), qr[1]);
+                            const double perp_q = fma(static_cast<double>(bp[64 + l]), static_cast<double>(sc[5]),
+                                                      static_cast<double>(sc[4]));
+                            g_tr[bn * nr + r] = __dmul_rn(perp_q, sk < s_sd2[r] ? sk : s_sd2[r]);
+                        }
+                    }
+                    if (lane == 0) {
+                        g_ln[bn] = l;
+                        g_pq[2 * bn] = pool2;
+                        g_pq[2 * bn + 1] = qadd;
+                    }
+                    ++bn;
+                    if (bn == 4) {
+                        full = true;
+                        break;
                     }
                 }
                 __syncwarp();
-                if (!(__dsub_rn(dc_q, fma(static_cast<double>(lambda), sqrt(pool2), qadd)) >= distk)) {
-#pragma unroll
-                    for (int j = 0; j < 4; ++j)
-                        if (j == bn) {
-                            g_lane[j] = l;
-                            g_pool[j] = pool2;
-                            g_qadd[j] = qadd;
-                        }
-                    ++bn;
-                }
-                }
-                // a full group, or the batch's last partial one
-                if (bn < 4 && (have || bn == 0)) {
-                    if (!have) break;
-                    continue;
-                }
-                // flush4 (me8q_fast.cpp:830-960): runs by the group's mean t^2
-                // per block, largest first (ties in run order)
-                int order[kFastMaxRuns];
-                double mean[kFastMaxRuns];
-                for (int r = 0; r < nr; ++r) {
-                    order[r] = r;
-                    double a = 0.0;
-                    for (int j = 0; j < bn; ++j) a = fma(g_tr[j * nr + r], g_tr[j * nr + r], a);
-                    const int nb = f.runs[r].len / 8;
-                    mean[r] = __ddiv_rn(a, static_cast<double>(nb > 1 ? nb : 1));
-                }
-                for (int a = 1; a < nr; ++a)
-                    for (int z = a; z > 0 && mean[order[z]] > mean[order[z - 1]]; --z) {
-                        const int t = order[z];
-                        order[z] = order[z - 1];
-                        order[z - 1] = t;
-                    }
-                double dist[4], rem[4];
-                bool died[4];
-                const double dk = static_cast<double>(heap.distk());
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    died[j] = j >= bn;
-                    rem[j] = g_pool[j];
-                    dist[j] = d2;
-                    if (j < bn) {
-                        const size_t slot = tile * 32 + g_lane[j];
-                        if (nr == 1) {
-                            dist[j] = __dadd_rn(d2, static_cast<double>(__ldg(v.h2 + slot)));
-                        } else {
-                            double dcc = d2;
-                            for (int r = 0; r < nr; ++r) {
-                                const size_t o = static_cast<size_t>(r) * v.nslots + slot;
-                                const double coef = static_cast<double>(__ldg(v.coef + o));
-                                const double h2 = static_cast<double>(__ldg(v.h2 + o));
-                                dcc = __dadd_rn(dcc, fma(-(2.0 * coef),
-                                                         fma(static_cast<double>(__ldg(f.gain + o)), g_sc[j * nr + r],
-                                                             static_cast<double>(__ldg(f.vpc + o))),
-                                                         h2));
-                            }
-                            dist[j] = dcc;
-                        }
-                    }
-                }
-                for (int oi = 0; oi < nr; ++oi) {
-                    const int r = order[oi];
-                    const Me8qFastRun run = f.runs[r];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        if (died[j]) continue;
-                        const size_t slot = tile * 32 + g_lane[j];
-                        const size_t o = static_cast<size_t>(r) * v.nslots + slot;
-                        const double coef = static_cast<double>(__ldg(v.coef + o));
-                        const double s_ex = static_cast<double>(run_score_warp(v, run, slot, qv));
-                        if (nr == 1) {
-                            dist[j] = fma(-(2.0 * coef), s_ex, dist[j]);
-                        } else {
-                            const double u = fma(static_cast<double>(__ldg(f.gain + o)), g_sc[j * nr + r],
-                                                 static_cast<double>(__ldg(f.vpc + o)));
-                            dist[j] = fma(2.0 * coef, __dsub_rn(u, s_ex), dist[j]);
-                        }
-                        const double t = g_tr[j * nr + r];
-                        rem[j] = fma(-t, t, rem[j]);
-                        if (__dsub_rn(fma(-static_cast<double>(lambda), sqrt(rem[j] > 0.0 ? rem[j] : 0.0), dist[j]),
-                                      g_qadd[j]) >= dk)
-                            died[j] = true;
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    if (died[j]) continue;
+                const bool last = !full;  // every passing lane taken: the batch's last group
+                if (bn == 0) break;
+                const unsigned dmask = flush_group(v, f, qv, tile, bn, d2, lambda,
+                                                   static_cast<double>(heap.distk()), g_ln, g_pq, g_sc, g_tr, g_fac,
+                                                   g_dist);
+                for (int j = 0; j < bn; ++j) {
+                    if ((dmask >> j) & 1u) continue;
                     ++n_surv;
-                    heap.push(static_cast<float>(dist[j]), __ldg(v.base.ids + tile * 32 + g_lane[j]));
+                    heap.push(static_cast<float>(g_dist[j]), __ldg(v.base.ids + tile * 32 + g_ln[j]));
                 }
                 bn = 0;
                 __syncwarp();
-                if (!have) break;
+                if (last) break;
             }
         }
     }
