@@ -538,7 +538,8 @@ def me8q_leg(a, e8qlib, dev, local, stream):
     --me8q-avg-bits: build time, recall@10 per nprobe against an FP64 brute
     force over the raw vectors (exact grouped scan and the int8 tensor-core
     precision mode, beside the IVF ceiling), device-resident QPS of both modes
-    at the smallest nprobe whose precision recall is >= 0.95 (else the
+    and of the reference's production FastScan cascade (pruned mode, with its
+    recall) at the smallest nprobe whose precision recall is >= 0.95 (else the
     largest), single-query latency; then open-loop serving (precision mode,
     k in {10, 100}, nprobe drawn from the values >= that nprobe) on the first
     rate that meets the recall bar (else the last)."""
@@ -613,6 +614,9 @@ def me8q_leg(a, e8qlib, dev, local, stream):
         npb = (ok[0] if ok else sweep[-1])["nprobe"]
         pq, pms, pl = qps(idx, npb, "precision")
         eq, ems, _ = qps(idx, npb, "batched")
+        # the reference's own search (its FastScan cascade, Me8qIndex.search's default)
+        rec_pruned = recall(idx, npb, "pruned")
+        prq, prms, _ = qps(idx, npb, "pruned")
         lat = []
         for i in range(72):
             s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -628,6 +632,8 @@ def me8q_leg(a, e8qlib, dev, local, stream):
                       "recall_at_10": [r["recall_precision"] for r in sweep if r["nprobe"] == npb][0],
                       "qps": round(pq, 1), "ms_per_step": round(pms, 3), "gpu_launches": int(pl),
                       "exact_qps": round(eq, 1), "exact_ms_per_step": round(ems, 3),
+                      "pruned_qps": round(prq, 1), "pruned_ms_per_step": round(prms, 3),
+                      "recall_pruned": round(rec_pruned, 4),
                       "single_query_ms": round(statistics.median(lat), 4)})
         if serve_idx is None and (ok or ai == len(avgs) - 1):
             serve_idx, serve_np = idx, npb

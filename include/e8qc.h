@@ -63,7 +63,8 @@ extern "C" {
  * per query rather than the reference's running heap); the bound, its LUT and
  * banks and prune_alpha are the reference's. With set_disable_prune every
  * candidate is scored (the reference's plain scan). stats: candidates scanned
- * and survivors refined. */
+ * and survivors refined. On an ME8Q index (e8qc_me8q_search_mode) the mode
+ * replays the reference's FastScan cascade in its own order instead. */
 #define E8QC_MODE_PRUNED 3
 
 /* Maximum top-k (include/e8qlib/index/e8q.hpp:44 kMaxK). */
@@ -266,6 +267,14 @@ int e8qc_me8q_build(e8qc_me8q* idx, const float* data, size_t n, const float* ce
 int e8qc_me8q_search(e8qc_me8q* idx, const float* queries, size_t nq, size_t k, size_t nprobe,
                      uint32_t* out_ids, float* out_dists, e8qc_stats* stats, void* stream);
 /* Search with an explicit mode (an addition of this library):
+ * E8QC_MODE_PRUNED is the reference's production search, the one its Python
+ * Me8qIndex.search runs (SearchIVFFast / SearchIVFFastBatch,
+ * src/index/me8q_fast.cpp:37-1090, python_bindings/me8q_bindings.cpp:97-160):
+ * FastScan coarse plane, zero-parallel-residual bound with the build's
+ * prune_alpha, run cascade against the running heap -- its prune decisions
+ * in its own order, so its rows (the fast layout is built on first use,
+ * about 1.4 B per coded block and 13 B per run per vector; uniform k and
+ * nprobe; at most 16 coded runs and 512 coded blocks);
  * E8QC_MODE_BATCHED is e8qc_me8q_search (grouped exact scan, every candidate
  * scored with the estimator); E8QC_MODE_PRECISION generates candidates on the
  * INT8 tensor cores from an int8 plane of each vector's levels scaled by its
