@@ -273,14 +273,14 @@ __global__ void me8q_lut_kernel(Me8qFast f, const float* __restrict__ rq, int pd
 // src/simd/me8q_score_generic.cpp:100-126): sum over the run's dims of
 // q * level, a chain per block, the lanes splitting the blocks; returns the
 // warp total.
-__device__ __forceinline__ float run_score_warp(const Me8qView& v, const Me8qFastRun& run, size_t slot,
-                                                const float* qv) {
+__device__ __forceinline__ float run_score_warp(const uint4* codes, int nch, const float* levels,
+                                                const Me8qFastRun& run, size_t slot, const float* qv) {
     const int lane = threadIdx.x & 31;
-    const float* lev0 = v.levels + run.lev;
+    const float* lev0 = levels + run.lev;
     float acc = 0.0f;
     for (int j = lane; j < run.len / 8; j += 32) {
         uint32_t dg[8];
-        const int br = me8q_block(v.base.codes, v.base.nch, slot, run.word0, run.bits, j, dg);
+        const int br = me8q_block(codes, nch, slot, run.word0, run.bits, j, dg);
         const float* lev = lev0 + br * (1 << run.bits);
         const float* qb = qv + run.off + j * 8;
         float b = 0.0f;
@@ -354,7 +354,8 @@ struct WarpHeap {
 };
 
 // Per-warp shared memory of the cascade kernel (sizes in bytes).
-// The u8 LUT first (16-byte aligned), then fp64 sqrt(d2_r) and the group's
+// The u8 LUT first (16-byte aligned), then fp64 sqrt(d2_r), the query's
+// per-run scalars and the group's
 // s_c and t (4 members), the group's (coef, h2, gain, vpc) per (member,
 // run), then acc, s_c and t per (run, lane), then two tile
 // stages (the tile's plane words, then per run its 96 bank bytes and 8
@@ -363,7 +364,7 @@ __host__ __device__ inline size_t cascade_stage_words(int cols, int nrun) {
     return static_cast<size_t>((cols + 3) / 4) * 32 + static_cast<size_t>(nrun) * 32;
 }
 __host__ __device__ inline size_t cascade_warp_bytes(int cols, int nrun) {
-    const size_t b = static_cast<size_t>(cols) * 32 + static_cast<size_t>(nrun) * 8 * (1 + 8) +
+    const size_t b = static_cast<size_t>(cols) * 32 + static_cast<size_t>(nrun) * 8 * (1 + 4 + 8) +
                      static_cast<size_t>(nrun) * 4 * 4 * 4 + 128 + static_cast<size_t>(nrun) * 32 * 4 * 3 +
                      2 * cascade_stage_words(cols, nrun) * 4;
     return (b + 15) / 16 * 16;
@@ -400,21 +401,29 @@ __device__ __forceinline__ void stage_tile(const Me8qFast& f, size_t tile, uint3
 // the remaining slack cannot bring a member under dk. Writes the members'
 // distances to dist and returns the mask of the dead. Out of line: one copy
 // of this rarely-run code keeps the scan loop's instruction stream small.
-static __device__ __noinline__ unsigned flush_group(const Me8qView& v, const Me8qFast& f, const float* qv, size_t tile,
-                                                    int bn, double d2, float lambda, double dk, const int* g_ln,
-                                                    const double* g_pq, const double* g_sc, const double* g_tr,
-                                                    float* g_fac, double* dist) {
+struct FlushArgs {
+    const uint4* codes;
+    const float *coef, *h2, *gain, *vpc, *levels;
+    const Me8qFastRun* runs;  // the CTA's shared copy
+    size_t nslots;
+    int nch, nr;
+};
+
+static __device__ __noinline__ unsigned flush_group(const FlushArgs fa, const float* qv, size_t tile, int bn, double d2,
+                                                    float lambda, double dk, const int* g_ln, const double* g_pq,
+                                                    const double* g_sc, const double* g_tr, float* g_fac,
+                                                    double* dist) {
     const int lane = threadIdx.x & 31;
-    const int nr = f.nrun;
+    const int nr = fa.nr;
     // the group's factors, one load per (member, run)
     for (int i = lane; i < bn * nr; i += 32) {
         const int j = i / nr, r = i - j * nr;
-        const size_t o = static_cast<size_t>(r) * v.nslots + tile * 32 + g_ln[j];
+        const size_t o = static_cast<size_t>(r) * fa.nslots + tile * 32 + g_ln[j];
         float* fo = g_fac + (j * nr + r) * 4;
-        fo[0] = __ldg(v.coef + o);
-        fo[1] = __ldg(v.h2 + o);
-        fo[2] = __ldg(f.gain + o);
-        fo[3] = __ldg(f.vpc + o);
+        fo[0] = __ldg(fa.coef + o);
+        fo[1] = __ldg(fa.h2 + o);
+        fo[2] = __ldg(fa.gain + o);
+        fo[3] = __ldg(fa.vpc + o);
     }
     __syncwarp();
     int order[kFastMaxRuns];
@@ -423,7 +432,7 @@ static __device__ __noinline__ unsigned flush_group(const Me8qView& v, const Me8
         order[r] = r;
         double a = 0.0;
         for (int j = 0; j < bn; ++j) a = fma(g_tr[j * nr + r], g_tr[j * nr + r], a);
-        const int nb = f.runs[r].len / 8;
+        const int nb = fa.runs[r].len / 8;
         mean[r] = __ddiv_rn(a, static_cast<double>(nb > 1 ? nb : 1));
     }
     for (int a = 1; a < nr; ++a)
@@ -456,13 +465,13 @@ static __device__ __noinline__ unsigned flush_group(const Me8qView& v, const Me8
     }
     for (int oi = 0; oi < nr; ++oi) {
         const int r = order[oi];
-        const Me8qFastRun run = f.runs[r];
+        const Me8qFastRun run = fa.runs[r];
 #pragma unroll 1
         for (int j = 0; j < bn; ++j) {
             if ((dead >> j) & 1u) continue;
             const float* fo = g_fac + (j * nr + r) * 4;
             const double coef = static_cast<double>(fo[0]);
-            const double s_ex = static_cast<double>(run_score_warp(v, run, tile * 32 + g_ln[j], qv));
+            const double s_ex = static_cast<double>(run_score_warp(fa.codes, fa.nch, fa.levels, run, tile * 32 + g_ln[j], qv));
             if (nr == 1) {
                 dj[j] = fma(-(2.0 * coef), s_ex, dj[j]);
             } else {
@@ -496,15 +505,20 @@ __global__ void __launch_bounds__(kFastWarps * 32, 2) me8q_cascade_kernel(
     const float* __restrict__ pd2, int nq, int np, int k, float lambda, int out_stride, uint32_t* __restrict__ out_ids,
     float* __restrict__ out_d, unsigned long long* __restrict__ counts) {
     extern __shared__ __align__(16) uint8_t fsm[];
+    __shared__ Me8qFastRun s_runs[kFastMaxRuns];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x < f.nrun) s_runs[threadIdx.x] = f.runs[threadIdx.x];
+    __syncthreads();
     const int q = blockIdx.x * kFastWarps + warp;
-    if (q >= nq) return;  // warp-uniform; the kernel has no block barrier
+    if (q >= nq) return;  // warp-uniform; no block barrier follows
     const int nr = f.nrun, cols = f.cols;
+    const FlushArgs fa{v.base.codes, v.coef, v.h2, f.gain, f.vpc, v.levels, s_runs, v.nslots, v.base.nch, nr};
     uint8_t* base = fsm + static_cast<size_t>(warp) * cascade_warp_bytes(cols, nr);
     const int lut_bytes = cols * 32;
     uint8_t* lut = base;                                             // cols x 32
     double* s_sd2 = reinterpret_cast<double*>(base + lut_bytes);     // nr
-    double* g_sc = s_sd2 + nr;                                       // 4 x nr
+    double* s_qr = s_sd2 + nr;                                       // nr x {qn2, lut_min_x, qerr, score_max}
+    double* g_sc = s_qr + 4 * nr;                                    // 4 x nr
     double* g_tr = g_sc + 4 * nr;                                    // 4 x nr
     double* g_pq = g_tr + 4 * nr;                                    // 4 x (pool, qadd)
     double* g_dist = g_pq + 8;                                       // 4 flushed distances
@@ -522,7 +536,9 @@ __global__ void __launch_bounds__(kFastWarps * 32, 2) me8q_cascade_kernel(
     }
     __syncwarp();
     const float* qv = rq + static_cast<size_t>(q) * v.base.pd;
-    const double* qr0 = qrun + static_cast<size_t>(q) * nr * 4;  // per run {qn2, lut_min_x, qerr, score_max}
+    for (int i = lane; i < 4 * nr; i += 32) s_qr[i] = qrun[static_cast<size_t>(q) * nr * 4 + i];
+    __syncwarp();
+    const double* qr0 = s_qr;  // per run {qn2, lut_min_x, qerr, score_max}
     const float delta = qdelta[q];
     const uint32_t* pr = probes + static_cast<size_t>(q) * np;
     const float* pdq = pd2 + static_cast<size_t>(q) * np;
@@ -551,7 +567,7 @@ __global__ void __launch_bounds__(kFastWarps * 32, 2) me8q_cascade_kernel(
         if (len == 0) continue;
         // sqrt(d2_r) per run (fp64; the dot split over the lanes)
         for (int r = 0; r < nr; ++r) {
-            const Me8qFastRun run = f.runs[r];
+            const Me8qFastRun run = s_runs[r];
             const float* rc = v.base.cen + static_cast<size_t>(L) * v.base.pd + run.off;
             double dot = 0.0;
             for (int t = lane; t < run.len; t += 32)
@@ -584,7 +600,7 @@ __global__ void __launch_bounds__(kFastWarps * 32, 2) me8q_cascade_kernel(
             const uint32_t* pw = stp + lane;
             float dc = d2f, pool = 0.0f, qa = 0.0f, wpad = 0.0f;
             for (int r = 0; r < nr; ++r) {
-                const Me8qFastRun run = f.runs[r];
+                const Me8qFastRun run = s_runs[r];
                 // a run covers whole plane words (its length is a multiple
                 // of 64 dims): one word = 4 columns = 8 LUT entries
                 int acc = 0;
@@ -706,7 +722,7 @@ __global__ void __launch_bounds__(kFastWarps * 32, 2) me8q_cascade_kernel(
                 __syncwarp();
                 const bool last = !full;  // every passing lane taken: the batch's last group
                 if (bn == 0) break;
-                const unsigned dmask = flush_group(v, f, qv, tile, bn, d2, lambda,
+                const unsigned dmask = flush_group(fa, qv, tile, bn, d2, lambda,
                                                    static_cast<double>(heap.distk()), g_ln, g_pq, g_sc, g_tr, g_fac,
                                                    g_dist);
                 for (int j = 0; j < bn; ++j) {
