@@ -306,32 +306,18 @@ void scan_class_means(int bits, double w_cls[2]);
 int ensure_pruned_planes(e8qc_index* x, cudaStream_t s) {
     if (x->rowa.p != nullptr) return 0;
     int launches = 0;
-    std::vector<uint8_t> hdr(x->ntiles * 128, 0);
     if (!x->banks.empty()) {
-        if (x->banks.size() != hdr.size()) fail(E8QC_ESTATE, "scan-bank headers do not match the tiles");
-        std::memcpy(hdr.data(), x->banks.data(), hdr.size());
+        // a loaded file's headers, as read
+        if (x->banks.size() != x->ntiles * 128) fail(E8QC_ESTATE, "scan-bank headers do not match the tiles");
+        x->banks_d.upload(x->banks.data(), x->banks.size(), s);
     } else if (x->ortho.bytes != 0) {
-        std::vector<float> os(x->ntiles * 32 * 3);
-        E8QC_CUDA(cudaMemcpyAsync(os.data(), x->ortho.p, os.size() * 4, cudaMemcpyDeviceToHost, s));
-        E8QC_CUDA(cudaStreamSynchronize(s));
-        float ob[32], ow[32], op[32];
-        for (size_t c = 0; c < x->nlist; ++c) {
-            const uint64_t len = x->list_begin[c + 1] - x->list_begin[c];
-            for (uint32_t t = x->tile_begin[c]; t < x->tile_begin[c + 1]; ++t) {
-                const uint64_t lo = static_cast<uint64_t>(t - x->tile_begin[c]) * 32;
-                const size_t cnt = static_cast<size_t>(std::min<uint64_t>(32, len - lo));
-                for (size_t v = 0; v < cnt; ++v) {
-                    ob[v] = os[(t * 32 + v) * 3 + 0];
-                    ow[v] = os[(t * 32 + v) * 3 + 1];
-                    op[v] = os[(t * 32 + v) * 3 + 2];
-                }
-                ortho_banks(ob, ow, op, cnt, hdr.data() + static_cast<size_t>(t) * 128);
-            }
-        }
+        // a build's per-slot bank inputs, quantised on the device
+        x->banks_d.alloc(std::max<size_t>(1, x->ntiles * 128));
+        launches += launch_ortho_banks(x->ortho.as<float>(), x->ids.as<uint32_t>(), static_cast<int>(x->ntiles),
+                                       x->banks_d.as<uint8_t>(), s);
     } else {
         fail(E8QC_ESTATE, "index holds no scan banks for the pruned search");
     }
-    x->banks_d.upload(hdr.data(), hdr.size(), s);
     DevBuf rowa;
     rowa.alloc(x->ntiles * static_cast<size_t>(rowa_chunks(x->B)) * 32 * 16);
     launches += launch_build_rowa(x->view, static_cast<int>(x->ntiles), rowa.as<uint4>(), s);

@@ -604,6 +604,64 @@ int pruned_max_grid(const DevIndex& ix, int stash_tiles) {
     return per_sm * sms;
 }
 
+namespace {
+
+// WriteOrthoBanks (src/index/e8q_build.cpp:33-80) per tile, one warp: the
+// live lanes' (base, weight, perp) quantised to u8 over their range (base
+// floor, weight nearest, perp ceil) and the 128-byte header: three banks of
+// 32 bytes, then min and step of each and max |weight|.
+__global__ void ortho_bank_kernel(const float* __restrict__ ortho, const uint32_t* __restrict__ ids, int ntiles,
+                                  uint8_t* __restrict__ hdr) {
+    const int w = static_cast<int>((static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (w >= ntiles) return;
+    const size_t slot = static_cast<size_t>(w) * 32 + lane;
+    const bool live = ids[slot] != 0xFFFFFFFFu;
+    float val[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) val[c] = live ? ortho[slot * 3 + c] : 0.0f;
+    float mn[3], sc[3], mx[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float lo = live ? val[c] : __int_as_float(0x7f800000), hi = live ? val[c] : __int_as_float(0xff800000);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = fminf(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+            hi = fmaxf(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, o));
+        }
+        mn[c] = lo;
+        mx[c] = hi;
+        sc[c] = hi > lo ? __fdiv_rn(__fsub_rn(hi, lo), 255.0f) : 1.0f;
+    }
+    uint8_t* h = hdr + static_cast<size_t>(w) * 128;
+    int q0 = 0, q1 = 0, q2 = 0;
+    if (live) {
+        q0 = static_cast<int>(__fdiv_rn(__fsub_rn(val[0], mn[0]), sc[0]));
+        q1 = static_cast<int>(roundf(__fdiv_rn(__fsub_rn(val[1], mn[1]), sc[1])));
+        q2 = static_cast<int>(ceilf(__fdiv_rn(__fsub_rn(val[2], mn[2]), sc[2])));
+    }
+    h[lane] = static_cast<uint8_t>(min(max(q0, 0), 255));
+    h[32 + lane] = static_cast<uint8_t>(min(max(q1, 0), 255));
+    h[64 + lane] = static_cast<uint8_t>(min(max(q2, 0), 255));
+    // scales: bmin, bstep, wmin, wstep, pmin, pstep, max |w|, then zero
+    const float out[8] = {mn[0], sc[0], mn[1], sc[1], mn[2], sc[2], fmaxf(fabsf(mn[1]), fabsf(mx[1])), 0.0f};
+    float o8 = out[0];
+#pragma unroll
+    for (int i = 1; i < 8; ++i)
+        if (lane == i) o8 = out[i];
+    if (lane < 8) reinterpret_cast<float*>(h + 96)[lane] = o8;
+}
+
+}  // namespace
+
+int launch_ortho_banks(const float* ortho, const uint32_t* ids, int ntiles, uint8_t* hdr, cudaStream_t s) {
+    if (ntiles == 0) return 0;
+    ortho_bank_kernel<<<static_cast<unsigned>((static_cast<size_t>(ntiles) * 32 + 255) / 256), 256, 0, s>>>(
+        ortho, ids, ntiles, hdr);
+    E8QC_CUDA(cudaGetLastError());
+    return 1;
+}
+
 int launch_build_rowa(const DevIndex& ix, int ntiles, uint4* rowa, cudaStream_t s) {
     const int nrc = rowa_chunks(ix.B);
     const size_t total = static_cast<size_t>(ntiles) * nrc * 32;

@@ -44,5 +44,8 @@ int launch_pruned(const DevIndex& ix, const float* rq, const RouteWork& rw, int 
 // The coarse plane of every tile from the codes (rowA byte of block b = the
 // top bit of each stored digit field, digit i at bit 7 - i).
 int launch_build_rowa(const DevIndex& ix, int ntiles, uint4* rowa, cudaStream_t s);
+// The 128-byte scan-bank header of every tile from the build's per-slot
+// (base, weight, perp) (ortho: ntiles*32*3 floats; padding lanes by ids).
+int launch_ortho_banks(const float* ortho, const uint32_t* ids, int ntiles, uint8_t* hdr, cudaStream_t s);
 
 }  // namespace e8qc
