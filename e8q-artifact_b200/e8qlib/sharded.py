@@ -17,6 +17,12 @@ residual to the list centroid does not depend on that mean, so sharded
 distances match a single index's up to float rounding. ME8Q: the bit plan
 follows the per-dimension variance, so every rank must build with the same
 ``variance`` (the whole data's); ``ShardedIndex.build`` passes it through.
+The merge equals one index's result for the exact modes (``mode="batched"``
+or ``"plain"``). The pruned modes (both engines' default, as in the
+reference) prune against each rank's own running top-k, so a sharded pruned
+search can keep rows a single index's cascade would have cut, and the
+reverse where the bound fails; pass ``mode="batched"`` for the single index's
+exact rows.
 
 The per-rank engine is any object with ``build(data, centroids, cluster_ids,
 **kw)`` and ``search(queries, k, nprobe, **kw) -> (ids, dists)``; by default an
