@@ -327,35 +327,23 @@ int ensure_pruned_planes(e8qc_index* x, cudaStream_t s) {
     return launches;
 }
 
-// The reference's production search, one query per launch sequence (route,
-// then one cooperative pruned kernel): pruned.cu.
+// The reference's production search for a batch: the batched route, then
+// per-query u8 LUTs and one warp per query replaying the reference's scan
+// with its running heap (pruned.cu, launch_pruned_batch).
 void pruned_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size_t nprobe, uint32_t* ids_d,
                    float* d_d, e8qc_stats* st, cudaStream_t s) {
     Workspace& ws = x->ws;
-    ws.ensure_route(x->nlist);
     uint64_t launches = static_cast<uint64_t>(ensure_pruned_planes(x, s));
-    const size_t max_tiles = max_tiles_for(x, nprobe);
-    int sms = 148;
-    E8QC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, x->device));
-    int grid = static_cast<int>(std::max<size_t>(1, std::min<size_t>(max_tiles, static_cast<size_t>(sms))));
-    const int per_cta = static_cast<int>((max_tiles + static_cast<size_t>(grid) - 1) / static_cast<size_t>(grid));
-    const int stash = std::min(per_cta, pruned_stash_cap(x->view));
-    grid = std::min(grid, pruned_max_grid(x->view, stash));
-    if (grid < 1) fail(E8QC_EINVAL, "the pruned search does not fit this device");
-    ws.ensure_scan(static_cast<size_t>(grid));
-    ws.ensure_pruned(static_cast<size_t>(grid), nq);
-    RouteWork rw{ws.keys.as<uint64_t>(), ws.probes.as<uint32_t>(), ws.probe_d2.as<float>(),
-                 ws.tile_off.as<uint32_t>(), ws.route_counter.as<uint32_t>(), ws.total_tiles.as<uint32_t>(),
-                 ws.probe_info.as<uint2>()};
-    ScanWork sw{ws.part_d.as<float>(), ws.part_id.as<uint32_t>(), ws.scan_counter.as<uint32_t>(),
-                ws.err.as<uint32_t>(), grid};
+    // route + per-query probes (the batched route; its pair grouping is unused)
+    launches += static_cast<uint64_t>(batched_prepare(x->view, ws, rq_all, nq, nullptr, nprobe, 1, 64, 1, s));
+    ws.ensure_pruned(1, nq);
+    ws.f_lut.ensure(nq * static_cast<size_t>(x->B) * 32);
+    ws.f_qrun.ensure(nq * 16);
     double w_cls[2];
     scan_class_means(x->bits, w_cls);
     PrunedWork pw{};
-    pw.seed_dc = ws.pr_dc.as<float>();
-    pw.seed_key = ws.pr_key.as<uint32_t>();
-    pw.counters = ws.pr_counters.as<uint32_t>();
     pw.stats = ws.pr_stats.as<unsigned long long>();
+    pw.thr = ws.pr_thr.as<float>();
     pw.err = ws.err.as<uint32_t>();
     pw.banks = x->banks_d.as<uint8_t>();
     pw.rowa = x->rowa.as<uint4>();
@@ -364,16 +352,11 @@ void pruned_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size
     pw.w_cls0 = w_cls[0];
     pw.w_cls1 = w_cls[1];
     pw.disable_prune = x->disable_prune ? 1 : 0;
-    pw.stash_tiles = stash;
-    E8QC_CUDA(cudaMemsetAsync(ws.pr_counters.p, 0, 8, s));
     E8QC_CUDA(cudaMemsetAsync(ws.pr_stats.p, 0, 16, s));
-    for (size_t i = 0; i < nq; ++i) {
-        const float* rq = rq_all + i * x->pd;
-        launches += launch_route_one(x->view, rq, static_cast<int>(nprobe), rw, s);
-        pw.thr = ws.pr_thr.as<float>() + i;
-        launches += launch_pruned(x->view, rq, rw, static_cast<int>(nprobe), static_cast<int>(k), sw, pw,
-                                  ids_d + i * k, d_d + i * k, s);
-    }
+    launches += static_cast<uint64_t>(launch_pruned_batch(
+        x->view, rq_all, ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(), static_cast<int>(nq),
+        static_cast<int>(nprobe), static_cast<int>(k), pw, ws.f_lut.as<uint8_t>(), ws.f_qrun.as<float>(), ids_d, d_d,
+        s));
     ws.pr_last_nq = nq;
     if (st) {
         unsigned long long cs[2] = {0, 0};

@@ -109,6 +109,7 @@ __device__ __forceinline__ float exact_half(const uint4* __restrict__ src, bool 
 // operations, in its order: src/simd/e8q_search_avx512.cpp:636-676).
 struct Coarse {
     float dc, P, perp;
+    int acc;  // the u8 LUT sum
 };
 
 __device__ __forceinline__ Coarse coarse_lane(const uint4* __restrict__ rowa, int nrc, int B, const uint8_t* lut,
@@ -147,6 +148,7 @@ __device__ __forceinline__ Coarse coarse_lane(const uint4* __restrict__ rowa, in
     const float base_term = __fmaf_rn(bq, bsc, bmin_d2);
     const float weight = __fmaf_rn(wq, wsc, wmin);
     Coarse r;
+    r.acc = acc;
     r.perp = __fmaf_rn(pq, psc, pmin);
     r.dc = __fmaf_rn(-weight, scv, base_term);
     r.P = __fmaf_rn(-fabsf(weight), lut_err, r.dc);
@@ -602,6 +604,279 @@ int pruned_max_grid(const DevIndex& ix, int stash_tiles) {
     E8QC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     E8QC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kWarps * 32, smem));
     return per_sm * sms;
+}
+
+namespace {
+
+// ---- batched form: one warp per query, the reference's order ---------------
+
+constexpr int kCWarps = 8;  // queries (warps) per CTA of the cascade kernel
+
+// Per query (one CTA): the u8 LUT (B*32 bytes: entry blk*32 + v, v < 16 the
+// low nibble, v >= 16 the high one) and its scalars {delta, base, lut_err,
+// score_max} (PrepareQuery, src/index/e8q_search.cpp:20-73; the arithmetic of
+// the one-query kernel's prologue).
+__global__ void pruned_lut_kernel(const float* __restrict__ rq, int pd, int B, int bits, double w0, double w1,
+                                  uint8_t* __restrict__ lut8, float* __restrict__ scal) {
+    __shared__ unsigned s_hc;
+    const int q = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+    const float* qv = rq + static_cast<size_t>(q) * pd;
+    auto cf_of = [&](int e) -> float {
+        const int blk = e >> 5, v = e & 15, hi = (e >> 4) & 1;
+        const float* qb = qv + blk * 8 + (hi ? 0 : 4);
+        double acc = 0.0;
+#pragma unroll
+        for (int h = 0; h < 4; ++h) {
+            const int bit = (v >> (3 - h)) & 1;
+            const int dim = hi ? h : 4 + h;
+            const double m = (bits == 1 && dim == 7) ? 0.0 : (bit ? w1 : w0);
+            acc = __fma_rn(static_cast<double>(__ldg(qb + h)), m, acc);
+        }
+        return __double2float_rn(acc);
+    };
+    if (tid == 0) s_hc = 0u;
+    __syncthreads();
+    unsigned mx = 0u;
+    for (int e = tid; e < B * 32; e += nt) mx = max(mx, __float_as_uint(fabsf(cf_of(e))));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+    if ((tid & 31) == 0) atomicMax(&s_hc, mx);
+    __syncthreads();
+    const float hc = __uint_as_float(s_hc);
+    const float delta = hc > 0.0f ? __fdiv_rn(__fmul_rn(2.0f, hc), 255.0f) : 1.0f;
+    const float qinv = __fdiv_rn(1.0f, delta), qoff = __fdiv_rn(hc, delta);
+    uint8_t* out = lut8 + static_cast<size_t>(q) * B * 32;
+    for (int e = tid; e < B * 32; e += nt) {
+        const unsigned u = static_cast<unsigned>(__float2int_rn(__fmaf_rn(cf_of(e), qinv, qoff)));
+        out[e] = static_cast<uint8_t>(u > 255u ? 255u : u);
+    }
+    if (tid == 0) {
+        float* sc = scal + static_cast<size_t>(q) * 4;
+        sc[0] = delta;
+        sc[1] = __fmul_rn(-hc, static_cast<float>(2 * B));
+        sc[2] = __fmul_rn(__fmul_rn(2.0f, __fsqrt_rn(static_cast<float>(B))), delta);
+        sc[3] = __fmul_rn(static_cast<float>(B), __fmaf_rn(255.0f, delta, __fmul_rn(2.0f, hc)));
+    }
+}
+
+// Per-warp shared memory of the cascade kernel: the query in padded units,
+// its u8 LUT, the staged rows (slot, g1, d2 + h3) and their distances.
+template <int BITS>
+__host__ __device__ inline size_t cascade_warp_bytes(int pd, int B) {
+    using G = StepGeo<BITS>;
+    const int nunits = B / G::SBLK + ((B % G::SBLK) != 0 ? 1 : 0);
+    const size_t b = static_cast<size_t>(nunits) * qstep_floats<BITS>() * 4 + ((static_cast<size_t>(B) * 32 + 15) & ~static_cast<size_t>(15)) +
+                     32 * 16;
+    (void)pd;
+    return (b + 15) / 16 * 16;
+}
+
+// One warp per query: ScanCluster (src/simd/e8q_search_avx512.cpp:552-751)
+// over the probes in (d2, list) order with the running heap -- the
+// whole-batch skip, the per-lane bound against the heap's k-th distance at
+// the batch start, CollectLanes (e8q_scan_common.hpp:86-113: each kept lane
+// re-tested against the current k-th, survivors staged, 32 at most, refined
+// and inserted when the stage is full and at the end of every list). The
+// heap's k-th distance changes only at a flush, so the re-test is a ballot
+// taken again after each one. The heap is the warp's top-k in the (distance,
+// id) order, the reference heap's order.
+template <int BITS>
+__global__ void __launch_bounds__(kCWarps * 32, 1) pruned_cascade_kernel(
+    DevIndex ix, const float* __restrict__ rq_all, const uint8_t* __restrict__ lut8, const float* __restrict__ scal_all,
+    const uint32_t* __restrict__ probes, const float* __restrict__ pd2, int nq, int np, int k, PrunedWork pw,
+    uint32_t* __restrict__ out_ids, float* __restrict__ out_d, float* __restrict__ thr_out,
+    unsigned long long* __restrict__ stats) {
+    using G = StepGeo<BITS>;
+    constexpr int Q = 1 << BITS, REP = table_rep(BITS), SBLK = G::SBLK, QS = qstep_floats<BITS>();
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int B = ix.B;
+    const int nsteps = B / SBLK;
+    const bool tail = (B % SBLK) != 0;
+    const int nunits = nsteps + (tail ? 1 : 0);
+    float* tabrep = reinterpret_cast<float*>(smem);  // 2*Q*REP, the CTA's
+    for (int e = tid; e < 2 * Q * REP; e += blockDim.x) tabrep[e] = ix.tab[e / REP];
+    __syncthreads();
+    const int q = blockIdx.x * kCWarps + warp;
+    if (q >= nq) return;  // warp-uniform; no block barrier follows
+    unsigned char* wb = smem + static_cast<size_t>(2 * Q * REP) * 4 +
+                        static_cast<size_t>(warp) * cascade_warp_bytes<BITS>(ix.pd, B);
+    float* sq = reinterpret_cast<float*>(wb);                                        // nunits*QS
+    uint8_t* lut = reinterpret_cast<uint8_t*>(sq + nunits * QS);                     // B*32
+    uint32_t* st_slot = reinterpret_cast<uint32_t*>(lut + ((B * 32 + 15) & ~15));   // 32
+    float* st_g1 = reinterpret_cast<float*>(st_slot + 32);                           // 32
+    float* st_h3 = st_g1 + 32;                                                       // 32
+    float* st_d = st_h3 + 32;                                                        // 32
+    const float* rq = rq_all + static_cast<size_t>(q) * ix.pd;
+    for (int i = lane; i < ix.pd; i += 32) {
+        const int u = i / (SBLK * 8), r = i - u * (SBLK * 8);
+        sq[u * QS + r] = rq[i];
+    }
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(lut8 + static_cast<size_t>(q) * B * 32);
+        uint4* dst = reinterpret_cast<uint4*>(lut);
+        for (int e = lane; e < B * 2; e += 32) dst[e] = src[e];
+    }
+    float scal[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) scal[i] = scal_all[static_cast<size_t>(q) * 4 + i];
+    __syncwarp();
+    const uint32_t tb_addr = smem_addr(tabrep) + static_cast<uint32_t>(lane % REP) * 4u;
+    const float lut_err = scal[2], score_max = scal[3], delta_c = scal[0], base_c = scal[1];
+    const uint32_t* pr = probes + static_cast<size_t>(q) * np;
+    const float* pdq = pd2 + static_cast<size_t>(q) * np;
+    WarpTopK top;
+    top.init(k);
+    int nst = 0;
+    unsigned long long n_cand = 0, n_surv = 0;
+    // refine the staged rows (a half-warp per row) and insert them
+    auto flush = [&]() {
+        for (int j0 = 0; j0 < nst; j0 += 2) {
+            const int j = j0 + (lane >> 4);
+            const bool act = j < nst;
+            const uint32_t slot = act ? st_slot[j] : 0u;
+            const float S = exact_half<BITS>(ix.codes + static_cast<size_t>(slot >> 5) * ix.nch * 32 + (slot & 31u),
+                                             act, nsteps, tail, sq, tb_addr);
+            if (act && (lane & 15) == 0) st_d[j] = __fmaf_rn(-__fmul_rn(2.0f, st_g1[j]), S, st_h3[j]);
+        }
+        __syncwarp();
+        const bool in = lane < nst;
+        const float dl = in ? st_d[lane] : inf_f();
+        top.offer(dl, in, [&] { return __ldg(ix.ids + st_slot[lane]); });
+        nst = 0;
+        __syncwarp();
+    };
+    unsigned long long last = 0;
+    for (int it = 0; it < np; ++it) {
+        unsigned long long best = ~0ull;
+        for (int p = lane; p < np; p += 32) {
+            const unsigned long long key = (static_cast<unsigned long long>(__float_as_uint(pdq[p])) << 32) | pr[p];
+            if ((it == 0 || key > last) && key < best) best = key;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long v = __shfl_xor_sync(kFull, best, o);
+            if (v < best) best = v;
+        }
+        if (best == ~0ull) break;
+        last = best;
+        const uint32_t L = static_cast<uint32_t>(best & 0xFFFFFFFFull);
+        const float d2 = __uint_as_float(static_cast<uint32_t>(best >> 32));
+        const uint32_t len = ix.list_len[L], tile0 = ix.tile_begin[L];
+        if (len == 0) continue;
+        const float sqrt_d2 = __fsqrt_rn(d2 > 0.0f ? d2 : 0.0f);
+        for (uint32_t i0 = 0; i0 < len; i0 += 32) {
+            const uint32_t n_logic = min(32u, len - i0);
+            const uint32_t gt = tile0 + (i0 >> 5);
+            const uint8_t* hdr = pw.banks + static_cast<size_t>(gt) * 128;
+            const Coarse cr = coarse_lane(pw.rowa + static_cast<size_t>(gt) * pw.nrc * 32, pw.nrc, B, lut, hdr, d2,
+                                          scal);
+            n_cand += n_logic;
+            const float distk0 = top.thr_d;
+            const float r_h = distk0 < d2 ? __fsqrt_rn(distk0 > 0.0f ? distk0 : 0.0f) : sqrt_d2;
+            const float slack = __fmul_rn(pw.z, r_h);
+            if (!pw.disable_prune && distk0 < inf_f()) {
+                // the whole-batch skip (e8q_search_avx512.cpp:611-635): padding
+                // lanes price the zero rowA bytes, as the reference's do
+                const float* sc = reinterpret_cast<const float*>(hdr + 96);
+                const float bmin = __ldg(sc + 0), wsc = __ldg(sc + 3), pmin = __ldg(sc + 4), psc = __ldg(sc + 5);
+                const float wamax = __ldg(sc + 6);
+                const float pad_w_round = __fmul_rn(__fmul_rn(0.5f, wsc), __fadd_rn(score_max, lut_err));
+                const float pad_add = __fmaf_rn(wamax, lut_err, pad_w_round);
+                const float perp_amax = __fmaf_rn(255.0f, psc, pmin);
+                int mxa = cr.acc, mna = cr.acc;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    mxa = max(mxa, __shfl_xor_sync(kFull, mxa, o));
+                    mna = min(mna, __shfl_xor_sync(kFull, mna, o));
+                }
+                const float s_hi = __fmaf_rn(static_cast<float>(mxa), delta_c, base_c);
+                const float s_lo = __fmaf_rn(static_cast<float>(mna), delta_c, base_c);
+                const float s_absmax = fabsf(s_hi) > fabsf(s_lo) ? fabsf(s_hi) : fabsf(s_lo);
+                const float lb = __fmaf_rn(-slack, perp_amax,
+                                           __fmaf_rn(-wamax, s_absmax, __fsub_rn(__fadd_rn(d2, bmin), pad_add)));
+                if (lb >= distk0) continue;
+            }
+            const float dlo = __fmaf_rn(-slack, cr.perp, cr.P);
+            const bool inm = static_cast<uint32_t>(lane) < n_logic && (pw.disable_prune || dlo < distk0);
+            int pos = -1;
+            for (;;) {
+                const float limit = top.thr_d;
+                const unsigned pass =
+                    __ballot_sync(kFull, inm && lane > pos && (pw.disable_prune || dlo < limit));
+                if (pass == 0u) break;
+                const int l = __ffs(pass) - 1;
+                if (nst == 32) flush();
+                if (lane == 0) {
+                    const size_t slot = static_cast<size_t>(gt) * 32 + l;
+                    st_slot[nst] = static_cast<uint32_t>(slot);
+                    st_g1[nst] = __ldg(ix.g1 + slot);
+                    st_h3[nst] = __fadd_rn(d2, __ldg(ix.h3 + slot));
+                }
+                ++nst;
+                ++n_surv;
+                pos = l;
+                __syncwarp();
+            }
+        }
+        if (nst > 0) flush();
+    }
+    top.store(out_d + static_cast<size_t>(q) * k, out_ids + static_cast<size_t>(q) * k, k);
+    if (lane == 0) {
+        if (thr_out) thr_out[q] = top.thr_d;
+        atomicAdd(stats, n_cand);
+        atomicAdd(stats + 1, n_surv);
+    }
+}
+
+}  // namespace
+
+int launch_pruned_batch(const DevIndex& ix, const float* rq, const uint32_t* probes, const float* pd2, int nq, int np,
+                        int k, const PrunedWork& pw, uint8_t* lut8, float* scal, uint32_t* out_ids, float* out_d,
+                        cudaStream_t s) {
+    if (nq == 0) return 0;
+    pruned_lut_kernel<<<static_cast<unsigned>(nq), 256, 0, s>>>(rq, ix.pd, ix.B, ix.bits, pw.w_cls0, pw.w_cls1, lut8,
+                                                               scal);
+    E8QC_CUDA(cudaGetLastError());
+    int dev = 0;
+    E8QC_CUDA(cudaGetDevice(&dev));
+    const void* fn = nullptr;
+    size_t smem = 0;
+    switch (ix.bits) {
+#define E8QC_CASE(b)                                                                                         \
+    case b:                                                                                                  \
+        fn = reinterpret_cast<const void*>(pruned_cascade_kernel<b>);                                        \
+        smem = static_cast<size_t>(2 * (1 << b) * table_rep(b)) * 4 + kCWarps * cascade_warp_bytes<b>(ix.pd, ix.B); \
+        break;
+        E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
+        E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
+        E8QC_CASE(13)
+#undef E8QC_CASE
+        default: fail(E8QC_EINVAL, "bits out of range");
+    }
+    if (smem > 227 * 1024) fail(E8QC_EINVAL, "the pruned search does not fit this device (padded_dim too large)");
+    {
+        static size_t configured[64][14] = {};
+        if (configured[dev & 63][ix.bits] < smem) {
+            E8QC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+            configured[dev & 63][ix.bits] = smem;
+        }
+    }
+    const unsigned grid = static_cast<unsigned>((nq + kCWarps - 1) / kCWarps);
+    switch (ix.bits) {
+#define E8QC_CASE(b)                                                                                       \
+    case b:                                                                                                \
+        pruned_cascade_kernel<b><<<grid, kCWarps * 32, smem, s>>>(ix, rq, lut8, scal, probes, pd2, nq, np, k, pw, \
+                                                                  out_ids, out_d, pw.thr, pw.stats);      \
+        break;
+        E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
+        E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
+        E8QC_CASE(13)
+#undef E8QC_CASE
+        default: break;
+    }
+    E8QC_CUDA(cudaGetLastError());
+    return 2;
 }
 
 namespace {

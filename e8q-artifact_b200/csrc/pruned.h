@@ -41,6 +41,14 @@ int pruned_max_grid(const DevIndex& ix, int stash_tiles);
 // One query (route results in rw): cooperative launch of `grid` CTAs.
 int launch_pruned(const DevIndex& ix, const float* rq, const RouteWork& rw, int nprobe, int k, const ScanWork& sw,
                   const PrunedWork& pw, uint32_t* out_ids, float* out_d, cudaStream_t s);
+// Batched form (nq queries, probes / pd2: nq x np from the batched route):
+// per-query u8 LUTs (lut8: nq*B*32 bytes, scal: nq*4 floats, scratch), then
+// one warp per query scanning in the reference's order with its running
+// heap; out rows of k; pw.thr (if set) gets each query's final k-th distance
+// and pw.stats the candidate / survivor counts.
+int launch_pruned_batch(const DevIndex& ix, const float* rq, const uint32_t* probes, const float* pd2, int nq, int np,
+                        int k, const PrunedWork& pw, uint8_t* lut8, float* scal, uint32_t* out_ids, float* out_d,
+                        cudaStream_t s);
 // The coarse plane of every tile from the codes (rowA byte of block b = the
 // top bit of each stored digit field, digit i at bit 7 - i).
 int launch_build_rowa(const DevIndex& ix, int ntiles, uint4* rowa, cudaStream_t s);
