@@ -25,6 +25,8 @@ stands in for the public corpora (no network).
            beside it the int8 tensor ops against an int8 MMA rate measured in
            the run with the library's tcgen05 probe.
   plain_gpu_qps: the plain one-query-per-launch GPU scan on the same index.
+  pruned_gpu_qps: the reference's search semantics on the GPU (mode "pruned",
+                  E8qIndex.search's default) on one batch of queries.
   serving: open-loop Poisson load through e8qlib.Server (U{1..64} queries per
            request) at fractions of `value`: achieved QPS, p50/p99/max ms;
            the loads with the headline k and nprobe, then one of uneven
@@ -736,17 +738,16 @@ def run_sweep(a):
         oi = torch.empty(nmax, b.k, dtype=torch.int32, device=dev)
         od = torch.empty(nmax, b.k, dtype=torch.float32, device=dev)
         if with_plain:
-            for mode in ("plain", "pruned"):
-                ms = ev_time(lambda: idx.search_ptr(q.data_ptr(), 256, b.k, nprobe, oi.data_ptr(), od.data_ptr(),
-                                                    mode, sp), 2)
-                row[mode + "_qps"] = round(256 / (ms / 1000.0), 1)
+            ms = ev_time(lambda: idx.search_ptr(q.data_ptr(), 256, b.k, nprobe, oi.data_ptr(), od.data_ptr(),
+                                                "plain", sp), 2)
+            row["plain_qps"] = round(256 / (ms / 1000.0), 1)
             idx.profile_start()
             idx.search_ptr(q[256:].data_ptr(), 64, b.k, nprobe, oi.data_ptr(), od.data_ptr(), "plain", sp)
             torch.cuda.synchronize()
             pr = plain_roofline(idx.profile_stop(), b, peak, pk_kind)
             row["plain_scan_frac"] = pr["frac"]
             row["plain_scan_us"] = pr["launch_us"]
-        for mode in ("batched", "precision"):
+        for mode in ("batched", "precision", "pruned"):
             for nb in batches:
                 reps = 5 if nb >= 256 else 20
                 ms = ev_time(lambda: idx.search_ptr(q.data_ptr(), nb, b.k, nprobe, oi.data_ptr(), od.data_ptr(),
@@ -1005,6 +1006,22 @@ def main():
         torch.cuda.synchronize()
         plain_qps = pb / (p0.elapsed_time(p1) / 1000.0)
 
+    # the reference's own search semantics (mode "pruned", E8qIndex.search's
+    # default: its running-heap cascade, one warp per query) on a full batch
+    pruned_qps = None
+    if a.path != "plain":
+        rb = min(a.batch, q.shape[0] // 2)
+        ri = torch.empty(rb, a.k, dtype=torch.int32, device=dev)
+        rdd = torch.empty(rb, a.k, dtype=torch.float32, device=dev)
+        idx.search_ptr(q.data_ptr(), rb, a.k, a.nprobe, ri.data_ptr(), rdd.data_ptr(), "pruned", sp)
+        torch.cuda.synchronize()
+        r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        r0.record(stream)
+        idx.search_ptr(q[rb:2 * rb].data_ptr(), rb, a.k, a.nprobe, ri.data_ptr(), rdd.data_ptr(), "pruned", sp)
+        r1.record(stream)
+        torch.cuda.synchronize()
+        pruned_qps = rb / (r0.elapsed_time(r1) / 1000.0)
+
     # serving: open-loop Poisson load through the server at fractions of the
     # measured batch throughput
     serving = None
@@ -1066,6 +1083,7 @@ def main():
                    "relerr_mean": round(err_mean, 6), "relerr_p99": round(err_p99, 6),
                    "relerr_max": round(err_max, 6),
                    "plain_gpu_qps": None if plain_qps is None else round(plain_qps, 1),
+                   "pruned_gpu_qps": None if pruned_qps is None else round(pruned_qps, 1),
                    "plain_scan_frac": roofline.get("plain_scan", {}).get("frac")},
         "recall_at_10": round(recall, 4), "build_s": round(build_s, 2),
         "relerr": {"mean": round(err_mean, 6), "p99": round(err_p99, 6), "max": round(err_max, 6),
@@ -1073,6 +1091,7 @@ def main():
         "clocks": clk.summary(), "gpu_launches": int(launches), "roofline": roofline,
         "e2e": e2e, "cpu_baseline": cpu,
         "plain_gpu_qps": None if plain_qps is None else round(plain_qps, 1),
+        "pruned_gpu_qps": None if pruned_qps is None else round(pruned_qps, 1),
         "serving": serving, "me8q": me8q, "step_breakdown": step_breakdown,
     }
     if rank == 0:

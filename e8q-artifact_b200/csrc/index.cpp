@@ -336,7 +336,7 @@ void pruned_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size
     uint64_t launches = static_cast<uint64_t>(ensure_pruned_planes(x, s));
     // route + per-query probes (the batched route; its pair grouping is unused)
     launches += static_cast<uint64_t>(batched_prepare(x->view, ws, rq_all, nq, nullptr, nprobe, 1, 64, 1, s));
-    ws.ensure_pruned(1, nq);
+    ws.ensure_pruned(nq);
     ws.f_lut.ensure(nq * static_cast<size_t>(x->B) * 32);
     ws.f_qrun.ensure(nq * 16);
     double w_cls[2];

@@ -1,36 +1,24 @@
-// Pruned one-query search: the reference's production search path
-// (E8qIndex::Search with pruning, src/index/e8q_search.cpp:215-293) as one
-// cooperative kernel per query.
+// The reference's production search (E8qIndex::Search with pruning,
+// src/index/e8q_search.cpp:215-293; ScanClusterAvx512,
+// src/simd/e8q_search_avx512.cpp:552-751) for a batch of queries.
 //
 // The reference scans lists in probe order with a running k-heap: a coarse
 // pass prices one rowA byte per 8-dim block (the digits' top bits) against a
 // u8 LUT of the query (PrepareQuery, e8q_search.cpp:20-73), a per-vector
-// lower bound from the zero-parallel-residual scan banks
-// (ScanClusterAvx512, src/simd/e8q_search_avx512.cpp:552-751;
-// OrthoBatchHeader, src/index/e8q_scan_common.hpp:141-156)
+// lower bound from the zero-parallel-residual scan banks (OrthoBatchHeader,
+// src/index/e8q_scan_common.hpp:141-156)
 //   dlo = (d2 + base - W*S - |W|*lut_err - W_round) - z * r_horizon * Omega
-// rejects vectors that cannot beat the heap's current k-th distance, and the
-// survivors are refined exactly. On the GPU the threshold cannot evolve
-// sequentially, so it is fixed up front from the best candidates:
-//   1. every CTA builds the query's u8 LUT (the reference's arithmetic: fp64
-//      sums, one u8 step for the whole table, round-to-nearest-even), streams
-//      the rowA plane of its tiles (lane = vector, B bytes each), forms each
-//      vector's coarse estimate dc and the bound terms P = dc - |W|*lut_err and
-//      Omega, keeps P and Omega in shared memory, and its best S by dc,
-//      S = min(max(4k, 32), 128) (at least k);
-//   2. a grid barrier; every CTA selects the S best coarse estimates of the
-//      whole query (ties by probe-space key), scores them exactly (the seeds)
-//      and takes T = the k-th best seed distance -- an upper bound of the
-//      answer's k-th distance, the same in every CTA;
-//   3. dlo(T) = P - z * r_horizon(T) * Omega with r_horizon = sqrt(min(T, d2))
-//      (the reference's rule); vectors with dlo < T that are not seeds are
-//      refined exactly, two per warp at a time (a half-warp per vector);
-//   4. the warps' top-k lists reduce per CTA (CTA 0 also holds the seeds) and
-//      the last CTA reduces the CTAs' lists.
-// The bound and its parameters are the reference's bit for bit; only the
-// threshold differs (a fixed T instead of the heap's k-th at the time), so the
-// top-k equals the reference's whenever its bound holds for the answer.
-// With disable_prune every candidate is refined (T = +inf).
+// rejects vectors that cannot beat the heap's current k-th distance, a
+// whole-batch test skips 32-row batches, and the survivors are staged 32 at
+// a time and refined exactly. Every decision depends on the heap after the
+// previous ones, so the GPU gives each query one warp that takes them in the
+// reference's order (pruned_cascade_kernel): the 32 rows of a batch are its
+// 32 lanes (coarse pass, bound), the staged rows are refined a half-warp per
+// row, and the heap is the warp's top-k in the (distance, id) order, the
+// reference heap's. pruned_lut_kernel builds the LUTs first (the
+// reference's arithmetic: fp64 sums, one u8 step for the table,
+// round-to-nearest-even); build_rowa_kernel and ortho_bank_kernel build the
+// coarse plane and the scan banks once per index.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -46,21 +34,6 @@ namespace e8qc {
 namespace {
 
 using namespace scan1;
-
-constexpr uint32_t kErrBarrier = 1u;  // the grid barrier gave up (host: E8QC_ETIMEOUT)
-constexpr uint64_t kBarrierNs = 2000000000ull;
-
-__device__ __forceinline__ uint64_t timer_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
-    uint32_t v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
 
 // Padded floats per decode unit of the query in shared memory: units are
 // whole steps (plus the odd rates' 8-block tail); the 4-float pad puts the
@@ -155,338 +128,6 @@ __device__ __forceinline__ Coarse coarse_lane(const uint4* __restrict__ rowa, in
     return r;
 }
 
-// Where tile t (probe space) of this query lives.
-struct TileRef {
-    int p;
-    uint32_t gt;      // global tile
-    uint32_t nvalid;  // vectors of the tile that exist
-    float d2;
-};
-
-__device__ __forceinline__ TileRef resolve_tile(const DevIndex& ix, const RouteWork& rw, const uint32_t* off,
-                                                int nprobe, uint32_t t) {
-    TileRef r;
-    r.p = find_probe(off, nprobe, t);
-    const uint2 info = __ldcg(rw.probe_info + r.p);  // (first tile, vectors) of the probed list
-    const uint32_t local = t - off[r.p];
-    r.gt = info.x + local;
-    r.nvalid = min(32u, info.y - local * 32u);
-    r.d2 = __ldcg(rw.probe_d2 + r.p);
-    return r;
-}
-
-template <int BITS>
-__global__ void __launch_bounds__(kWarps * 32, 1) pruned_kernel(DevIndex ix, const float* __restrict__ rq,
-                                                               RouteWork rw, int nprobe, int k, ScanWork sw,
-                                                               PrunedWork pw, uint32_t* __restrict__ out_ids,
-                                                               float* __restrict__ out_d) {
-    using G = StepGeo<BITS>;
-    constexpr int Q = 1 << BITS, REP = table_rep(BITS), SBLK = G::SBLK, QS = qstep_floats<BITS>();
-    constexpr int nt = kWarps * 32;
-    extern __shared__ __align__(128) unsigned char smem[];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int B = ix.B;
-    const int nsteps = B / SBLK;
-    const bool tail = (B % SBLK) != 0;
-    const int nunits = nsteps + (tail ? 1 : 0);
-    // shared-memory carve (pruned_smem_bytes)
-    float* tabrep = reinterpret_cast<float*>(smem);                                 // 2*Q*REP
-    float* sq = tabrep + 2 * Q * REP;                                               // nunits*QS
-    uint8_t* lut = reinterpret_cast<uint8_t*>(sq + nunits * QS);                    // B*32 (16-aligned)
-    float* stash = reinterpret_cast<float*>(lut + ((B * 32 + 15) & ~15));           // stash_tiles*64
-    uint32_t* soff = reinterpret_cast<uint32_t*>(stash + pw.stash_tiles * 64);      // kToffCap + 4
-    float* sm_d = reinterpret_cast<float*>(soff + kToffCap + 4);                    // kWarps*kMaxK
-    uint32_t* sm_id = reinterpret_cast<uint32_t*>(sm_d + kWarps * kMaxK);
-    float* sv_d = reinterpret_cast<float*>(sm_id + kWarps * kMaxK);                // kSelCap
-    uint32_t* sv_id = reinterpret_cast<uint32_t*>(sv_d + kSelCapWide);
-    float* seed_dc = reinterpret_cast<float*>(sv_id + kSelCap);                    // kMaxK
-    uint32_t* seed_key = reinterpret_cast<uint32_t*>(seed_dc + kMaxK);
-    float* seed_d = reinterpret_cast<float*>(seed_key + kMaxK);
-    uint32_t* seed_id = reinterpret_cast<uint32_t*>(seed_d + kMaxK);
-    __shared__ float s_scal[4];
-    __shared__ unsigned s_hc;
-    __shared__ float s_T;
-    __shared__ int s_ok;
-    __shared__ bool s_last;
-    __shared__ unsigned long long s_stats[2];  // the CTA's candidates and survivors
-
-    // ---- prologue: query (padded units), level table copies, tile offsets, LUT
-    for (int i = tid; i < ix.pd; i += nt) {
-        const int u = i / (SBLK * 8), r = i - u * (SBLK * 8);
-        sq[u * QS + r] = rq[i];
-    }
-    for (int e = tid; e < 2 * Q * REP; e += nt) tabrep[e] = ix.tab[e / REP];
-    const bool off_in_smem = nprobe <= kToffCap;
-    if (off_in_smem)
-        for (int i = tid; i <= nprobe; i += nt) soff[i] = __ldcg(rw.tile_off + i);
-    if (tid == 0) {
-        s_hc = 0u;
-        s_stats[0] = s_stats[1] = 0ull;
-    }
-    __syncthreads();
-    // LUT entry e = blk*32 + v: v < 16 prices the low nibble (digits 4..7),
-    // v >= 16 the high nibble (digits 0..3); fp64 sums in the reference's order
-    auto cf_of = [&](int e) -> float {
-        const int blk = e >> 5, v = e & 15, hi = (e >> 4) & 1;
-        const float* qb = rq + blk * 8 + (hi ? 0 : 4);
-        double acc = 0.0;
-#pragma unroll
-        for (int h = 0; h < 4; ++h) {
-            const int bit = (v >> (3 - h)) & 1;
-            const int dim = hi ? h : 4 + h;
-            const double m = (BITS == 1 && dim == 7) ? 0.0 : (bit ? pw.w_cls1 : pw.w_cls0);
-            acc = __fma_rn(static_cast<double>(__ldg(qb + h)), m, acc);
-        }
-        return __double2float_rn(acc);
-    };
-    {
-        unsigned mx = 0u;
-        for (int e = tid; e < B * 32; e += nt) mx = max(mx, __float_as_uint(fabsf(cf_of(e))));
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFull, mx, o));
-        if (lane == 0) atomicMax(&s_hc, mx);
-    }
-    __syncthreads();
-    {
-        const float hc = __uint_as_float(s_hc);
-        const float delta = hc > 0.0f ? __fdiv_rn(__fmul_rn(2.0f, hc), 255.0f) : 1.0f;
-        const float qinv = __fdiv_rn(1.0f, delta), qoff = __fdiv_rn(hc, delta);
-        for (int e = tid; e < B * 32; e += nt) {
-            const unsigned u = static_cast<unsigned>(__float2int_rn(__fmaf_rn(cf_of(e), qinv, qoff)));
-            lut[e] = static_cast<uint8_t>(u > 255u ? 255u : u);
-        }
-        if (tid == 0) {
-            s_scal[0] = delta;
-            s_scal[1] = __fmul_rn(-hc, static_cast<float>(2 * B));
-            s_scal[2] = __fmul_rn(__fmul_rn(2.0f, __fsqrt_rn(static_cast<float>(B))), delta);
-            s_scal[3] = __fmul_rn(static_cast<float>(B), __fmaf_rn(255.0f, delta, __fmul_rn(2.0f, hc)));
-        }
-    }
-    __syncthreads();
-    const uint32_t* off = off_in_smem ? soff : rw.tile_off;
-    const uint32_t tb_addr = smem_addr(tabrep) + static_cast<uint32_t>(lane % REP) * 4u;
-    const uint32_t T = __ldcg(rw.total_tiles);
-    const uint32_t Gd = gridDim.x;
-    const uint32_t per_cta = T > blockIdx.x ? (T - blockIdx.x + Gd - 1) / Gd : 0;
-
-    // ---- phase 1: coarse pass, bound terms, the CTA's best ns coarse estimates
-    const int ns = min(kMaxK, max(k, max(4 * k, 32)));  // seeds per query
-    WarpTopK top;
-    top.init(ns);
-    unsigned long long cand_w = 0;
-    for (uint32_t j = warp; j < per_cta; j += kWarps) {
-        const uint32_t t = blockIdx.x + j * Gd;
-        const TileRef tr = resolve_tile(ix, rw, off, nprobe, t);
-        const Coarse cr = coarse_lane(pw.rowa + static_cast<size_t>(tr.gt) * pw.nrc * 32, pw.nrc, B, lut,
-                                      pw.banks + static_cast<size_t>(tr.gt) * 128, tr.d2, s_scal);
-        if (j < static_cast<uint32_t>(pw.stash_tiles)) {
-            stash[j * 64 + lane] = cr.P;
-            stash[j * 64 + 32 + lane] = cr.perp;
-        }
-        const uint32_t key = t * 32u + lane;
-        top.offer(cr.dc, static_cast<uint32_t>(lane) < tr.nvalid, [&] { return key; });
-        cand_w += tr.nvalid;
-    }
-    top.store(sm_d + warp * ns, sm_id + warp * ns, ns);
-    __syncthreads();
-    {
-        float* cd = pw.seed_dc + static_cast<size_t>(blockIdx.x) * kMaxK;
-        uint32_t* ck = pw.seed_key + static_cast<size_t>(blockIdx.x) * kMaxK;
-        if (!block_select(sm_d, sm_id, kWarps, ns, sv_d, sv_id, cd, ck, kSelCapWide)) {
-            __syncthreads();
-            block_sort_select(sm_d, sm_id, kWarps, ns, cd, ck);
-        }
-    }
-
-    // ---- grid barrier (co-resident CTAs: cooperative launch), bounded
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) {
-        atomicAdd(pw.counters, 1u);
-        int ok = 1;
-        const uint64_t t0 = timer_ns();
-        while (ld_acquire(pw.counters) < Gd) {
-            if (timer_ns() - t0 > kBarrierNs) {
-                ok = 0;
-                atomicOr(pw.err, kErrBarrier);
-                break;
-            }
-            __nanosleep(64);
-        }
-        s_ok = ok;
-    }
-    __syncthreads();
-    if (!s_ok) return;
-
-    // ---- phase 2: the query's ns best coarse estimates (seeds), scored exactly
-    {
-        const int Gi = static_cast<int>(Gd);
-        __syncthreads();
-        if (!block_select_g(pw.seed_dc, pw.seed_key, Gi, kMaxK, ns, sv_d, sv_id, seed_dc, seed_key, kSelCapWide)) {
-            __syncthreads();
-            top.init(ns);
-            for (int e0 = warp * 32; e0 < Gi * ns; e0 += nt) {
-                const int e = e0 + lane;
-                const bool okj = e < Gi * ns;
-                float dd = inf_f();
-                uint32_t kk = 0xFFFFFFFFu;
-                if (okj) {
-                    const int c = e / ns, jj = e - c * ns;
-                    dd = __ldcg(pw.seed_dc + static_cast<size_t>(c) * kMaxK + jj);
-                    kk = __ldcg(pw.seed_key + static_cast<size_t>(c) * kMaxK + jj);
-                }
-                top.offer_pair(dd, kk, okj && kk != 0xFFFFFFFFu);
-            }
-            top.store(sm_d + warp * ns, sm_id + warp * ns, ns);
-            __syncthreads();
-            if (!block_select(sm_d, sm_id, kWarps, ns, sv_d, sv_id, seed_dc, seed_key, kSelCapWide)) {
-                __syncthreads();
-                block_sort_select(sm_d, sm_id, kWarps, ns, seed_dc, seed_key);
-            }
-        }
-        __syncthreads();
-    }
-    for (int s0 = 2 * warp; s0 < ns; s0 += 2 * kWarps) {
-        const int s = s0 + (lane >> 4);
-        const uint32_t key = s < ns ? seed_key[s] : 0xFFFFFFFFu;
-        const bool act = key != 0xFFFFFFFFu;
-        TileRef tr{0, 0u, 0u, 0.0f};
-        uint32_t lv = 0;
-        if (act) {
-            tr = resolve_tile(ix, rw, off, nprobe, key >> 5);
-            lv = key & 31u;
-        }
-        const float S = exact_half<BITS>(ix.codes + static_cast<size_t>(tr.gt) * ix.nch * 32 + lv, act, nsteps, tail,
-                                         sq, tb_addr);
-        if (act && (lane & 15) == 0) {
-            const size_t slot = static_cast<size_t>(tr.gt) * 32u + lv;
-            seed_d[s] = __fmaf_rn(-__fmul_rn(2.0f, __ldg(ix.g1 + slot)), S, __fadd_rn(tr.d2, __ldg(ix.h3 + slot)));
-            seed_id[s] = __ldg(ix.ids + slot);
-        } else if ((lane & 15) == 0 && s < ns) {
-            seed_d[s] = inf_f();
-            seed_id[s] = 0xFFFFFFFFu;
-        }
-    }
-    __syncthreads();
-    // T = the k-th best seed distance (+inf with fewer than k seeds or with
-    // pruning off): the seed whose rank among the seeds is k - 1
-    if (tid == 0) s_T = inf_f();
-    __syncthreads();
-    for (int s = tid; s < ns; s += nt) {
-        if (seed_key[s] == 0xFFFFFFFFu) continue;
-        int r = 0;
-        for (int j = 0; j < ns; ++j)
-            r += (seed_key[j] != 0xFFFFFFFFu && better(seed_d[j], seed_id[j], seed_d[s], seed_id[s])) ? 1 : 0;
-        if (r == k - 1 && !pw.disable_prune) s_T = seed_d[s];
-    }
-    __syncthreads();
-    if (tid == 0 && blockIdx.x == 0 && pw.thr) *pw.thr = s_T;
-    const float Tthr = s_T;
-
-    // ---- phase 3: survivors of the bound, refined exactly
-    top.init(k);
-    unsigned long long surv_w = 0;
-    for (uint32_t j = warp; j < per_cta; j += kWarps) {
-        const uint32_t t = blockIdx.x + j * Gd;
-        const TileRef tr = resolve_tile(ix, rw, off, nprobe, t);
-        float P, perp;
-        if (j < static_cast<uint32_t>(pw.stash_tiles)) {
-            P = stash[j * 64 + lane];
-            perp = stash[j * 64 + 32 + lane];
-        } else {
-            const Coarse cr = coarse_lane(pw.rowa + static_cast<size_t>(tr.gt) * pw.nrc * 32, pw.nrc, B, lut,
-                                          pw.banks + static_cast<size_t>(tr.gt) * 128, tr.d2, s_scal);
-            P = cr.P;
-            perp = cr.perp;
-        }
-        const float rh = (Tthr < tr.d2) ? __fsqrt_rn(fmaxf(0.0f, Tthr)) : __fsqrt_rn(fmaxf(0.0f, tr.d2));
-        const float dlo = __fmaf_rn(-__fmul_rn(pw.z, rh), perp, P);
-        bool surv = static_cast<uint32_t>(lane) < tr.nvalid && dlo < Tthr;
-        if (surv) {
-            const uint32_t key = t * 32u + lane;
-            for (int s = 0; s < ns; ++s)
-                if (seed_key[s] == key) surv = false;
-        }
-        uint32_t mask = __ballot_sync(kFull, surv);
-        surv_w += __popc(mask);
-        while (mask) {
-            const int v0 = __ffs(mask) - 1;
-            mask &= mask - 1;
-            const int v1 = mask ? __ffs(mask) - 1 : -1;
-            if (v1 >= 0) mask &= mask - 1;
-            const int my = lane < 16 ? v0 : v1;
-            const bool act = my >= 0;
-            const uint32_t lv = act ? static_cast<uint32_t>(my) : 0u;
-            const float S = exact_half<BITS>(ix.codes + static_cast<size_t>(tr.gt) * ix.nch * 32 + lv, act, nsteps,
-                                             tail, sq, tb_addr);
-            const size_t slot = static_cast<size_t>(tr.gt) * 32u + lv;
-            float dist = inf_f();
-            if (act) dist = __fmaf_rn(-__fmul_rn(2.0f, __ldg(ix.g1 + slot)), S, __fadd_rn(tr.d2, __ldg(ix.h3 + slot)));
-            top.offer(dist, act && (lane & 15) == 0, [&] { return __ldg(ix.ids + slot); });
-        }
-    }
-    if (blockIdx.x == 0 && warp == 0) {
-        for (int s0 = 0; s0 < ns; s0 += 32) {
-            const int s = s0 + lane;
-            const bool okj = s < ns && seed_key[s] != 0xFFFFFFFFu;
-            top.offer_pair(okj ? seed_d[s] : inf_f(), okj ? seed_id[s] : 0xFFFFFFFFu, okj);
-        }
-    }
-    // counters: per CTA in shared memory, then one global add each (thousands
-    // of same-address global atomics from every warp serialise in L2)
-    if (lane == 0) {
-        atomicAdd(&s_stats[0], cand_w);
-        atomicAdd(&s_stats[1], surv_w);
-    }
-
-    // ---- phase 4: CTA reduction, then the last CTA reduces the CTAs' lists
-    top.store(sm_d + warp * k, sm_id + warp * k, k);
-    __syncthreads();
-    if (tid == 0) {
-        atomicAdd(pw.stats + 0, s_stats[0]);
-        atomicAdd(pw.stats + 1, s_stats[1]);
-    }
-    float* cta_d = sw.part_d + static_cast<size_t>(blockIdx.x) * kMaxK;
-    uint32_t* cta_id = sw.part_id + static_cast<size_t>(blockIdx.x) * kMaxK;
-    if (!block_select(sm_d, sm_id, kWarps, k, sv_d, sv_id, cta_d, cta_id, kSelCapWide)) {
-        __syncthreads();
-        block_sort_select(sm_d, sm_id, kWarps, k, cta_d, cta_id);
-    }
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) s_last = atomicAdd(pw.counters + 1, 1u) == Gd - 1;
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    const int Gi = static_cast<int>(Gd);
-    if (!block_select_g(sw.part_d, sw.part_id, Gi, kMaxK, k, sv_d, sv_id, out_d, out_ids, kSelCapWide)) {
-        __syncthreads();
-        top.init(k);
-        for (int e0 = warp * 32; e0 < Gi * k; e0 += nt) {
-            const int e = e0 + lane;
-            const bool okj = e < Gi * k;
-            float dd = inf_f();
-            uint32_t ii = 0xFFFFFFFFu;
-            if (okj) {
-                const int c = e / k, jj = e - c * k;
-                dd = __ldcg(sw.part_d + static_cast<size_t>(c) * kMaxK + jj);
-                ii = __ldcg(sw.part_id + static_cast<size_t>(c) * kMaxK + jj);
-            }
-            top.offer_pair(dd, ii, okj && ii != 0xFFFFFFFFu);
-        }
-        top.store(sm_d + warp * k, sm_id + warp * k, k);
-        __syncthreads();
-        if (!block_select(sm_d, sm_id, kWarps, k, sv_d, sv_id, out_d, out_ids, kSelCapWide)) {
-            __syncthreads();
-            block_sort_select(sm_d, sm_id, kWarps, k, out_d, out_ids);
-        }
-    }
-    if (tid == 0) {
-        pw.counters[0] = 0u;
-        pw.counters[1] = 0u;
-    }
-}
-
 // rowA byte of every block of every slot: bit 7 - i = the top bit of stored
 // digit field i (digit 7's field holds the branch in its lowest bit, which
 // at b = 1 is the whole field: the reference's rowA bit 0 is then the branch).
@@ -521,90 +162,7 @@ __global__ void build_rowa_kernel(DevIndex ix, int ntiles, int nrc, uint4* __res
     out[i] = make_uint4(outw[0], outw[1], outw[2], outw[3]);
 }
 
-template <int BITS>
-int launch_bits(const DevIndex& ix, const float* rq, const RouteWork& rw, int nprobe, int k, const ScanWork& sw,
-                const PrunedWork& pw, uint32_t* out_ids, float* out_d, cudaStream_t s) {
-    const size_t smem = pruned_smem_bytes(ix, pw.stash_tiles);
-    static size_t configured[64] = {};
-    int dev = 0;
-    E8QC_CUDA(cudaGetDevice(&dev));
-    if (configured[dev & 63] < smem) {
-        E8QC_CUDA(cudaFuncSetAttribute(pruned_kernel<BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       static_cast<int>(smem)));
-        configured[dev & 63] = smem;
-    }
-    DevIndex ixa = ix;
-    const float* rqa = rq;
-    RouteWork rwa = rw;
-    int npa = nprobe, ka = k;
-    ScanWork swa = sw;
-    PrunedWork pwa = pw;
-    uint32_t* oi = out_ids;
-    float* od = out_d;
-    void* args[] = {&ixa, &rqa, &rwa, &npa, &ka, &swa, &pwa, &oi, &od};
-    E8QC_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(pruned_kernel<BITS>), dim3(sw.grid),
-                                          dim3(kWarps * 32), args, smem, s));
-    return 1;
-}
-
 }  // namespace
-
-size_t pruned_smem_bytes(const DevIndex& ix, int stash_tiles) {
-    const int q = 1 << ix.bits;
-    const int sblk = (ix.bits & 1) ? 16 : 8;
-    const int nunits = ix.B / sblk + ((ix.B % sblk) ? 1 : 0);
-    size_t b = static_cast<size_t>(2) * q * table_rep(ix.bits) * 4;
-    b += static_cast<size_t>(nunits) * (sblk * 8 + 4) * 4;
-    b += (static_cast<size_t>(ix.B) * 32 + 15) & ~static_cast<size_t>(15);
-    b += static_cast<size_t>(stash_tiles) * 64 * 4;
-    b += static_cast<size_t>(kToffCap + 4) * 4;
-    b += static_cast<size_t>(kWarps) * kMaxK * 8;
-    b += static_cast<size_t>(kSelCapWide) * 8;
-    b += static_cast<size_t>(kMaxK) * 16;
-    return b;
-}
-
-int pruned_stash_cap(const DevIndex& ix) {
-    const size_t base = pruned_smem_bytes(ix, 0);
-    const size_t budget = 225 * 1024;
-    return base >= budget ? 0 : static_cast<int>((budget - base) / 256);
-}
-
-int launch_pruned(const DevIndex& ix, const float* rq, const RouteWork& rw, int nprobe, int k, const ScanWork& sw,
-                  const PrunedWork& pw, uint32_t* out_ids, float* out_d, cudaStream_t s) {
-    if (pruned_smem_bytes(ix, pw.stash_tiles) > 227 * 1024)
-        fail(E8QC_EINVAL, "padded dimension too large for the pruned scan's shared memory");
-    switch (ix.bits) {
-#define E8QC_CASE(b) \
-    case b: return launch_bits<b>(ix, rq, rw, nprobe, k, sw, pw, out_ids, out_d, s);
-        E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
-        E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
-        E8QC_CASE(13)
-#undef E8QC_CASE
-        default: fail(E8QC_EINVAL, "bits out of range");
-    }
-    return 0;
-}
-
-int pruned_max_grid(const DevIndex& ix, int stash_tiles) {
-    const size_t smem = pruned_smem_bytes(ix, stash_tiles);
-    int dev = 0, sms = 0, per_sm = 0;
-    E8QC_CUDA(cudaGetDevice(&dev));
-    E8QC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const void* fn = nullptr;
-    switch (ix.bits) {
-#define E8QC_CASE(b) \
-    case b: fn = reinterpret_cast<const void*>(pruned_kernel<b>); break;
-        E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
-        E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
-        E8QC_CASE(13)
-#undef E8QC_CASE
-        default: fail(E8QC_EINVAL, "bits out of range");
-    }
-    E8QC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    E8QC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kWarps * 32, smem));
-    return per_sm * sms;
-}
 
 namespace {
 

@@ -1,6 +1,6 @@
-// Pruned one-query search (the reference's production search path on the
-// GPU): coarse rowA pass + zero-parallel-residual lower bound + exact refine
-// of the survivors. See pruned.cu.
+// The reference's production (pruned) search on the GPU: coarse rowA pass +
+// zero-parallel-residual lower bound + exact refine of the survivors, one warp
+// per query in the reference's order. See pruned.cu.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -16,31 +16,17 @@ namespace e8qc {
 inline int rowa_chunks(int blocks) { return (blocks + 15) / 16; }
 
 struct PrunedWork {
-    float* seed_dc;              // grid * kMaxK: per-CTA best coarse estimates
-    uint32_t* seed_key;          // grid * kMaxK: their probe-space keys (tile * 32 + lane)
-    uint32_t* counters;          // [0] grid-barrier arrivals, [1] CTAs finished (self-resetting)
     unsigned long long* stats;   // [0] candidates scanned, [1] survivors refined (accumulated)
-    float* thr;                  // this query's threshold (the k-th exact seed distance), or NULL
-    uint32_t* err;               // device error word (a grid barrier that gave up)
+    float* thr;                  // per query: the heap's final k-th distance, or NULL
+    uint32_t* err;               // device error word
     const uint8_t* banks;        // ntiles * 128: the scan-bank header of every tile
     const uint4* rowa;           // ntiles * nrc * 32 chunks
     int nrc;                     // rowa_chunks(B)
     float z;                     // OrthoQuantile(prune_alpha, max(4k, 32))
     double w_cls0, w_cls1;       // branch-averaged level mean of each top-bit class
     int disable_prune;           // 1: every candidate is refined (the reference's set_disable_prune)
-    int stash_tiles;             // tiles per CTA whose bound terms stay in shared memory
 };
 
-// Dynamic shared memory of the pruned kernel with `stash_tiles` stashed tiles.
-size_t pruned_smem_bytes(const DevIndex& ix, int stash_tiles);
-// Largest stash that fits the 227 KB shared-memory budget.
-int pruned_stash_cap(const DevIndex& ix);
-// CTAs of the pruned kernel that can be resident at once on this device
-// (the cooperative launch's limit).
-int pruned_max_grid(const DevIndex& ix, int stash_tiles);
-// One query (route results in rw): cooperative launch of `grid` CTAs.
-int launch_pruned(const DevIndex& ix, const float* rq, const RouteWork& rw, int nprobe, int k, const ScanWork& sw,
-                  const PrunedWork& pw, uint32_t* out_ids, float* out_d, cudaStream_t s);
 // Batched form (nq queries, probes / pd2: nq x np from the batched route):
 // per-query u8 LUTs (lut8: nq*B*32 bytes, scal: nq*4 floats, scratch), then
 // one warp per query scanning in the reference's order with its running

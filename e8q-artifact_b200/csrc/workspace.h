@@ -140,18 +140,9 @@ struct Workspace {
         E8QC_CUDA(cudaMemset(route_counter.p, 0, 4));
         route_cap = nlist;
     }
-    void ensure_pruned(size_t grid, size_t nq) {
+    void ensure_pruned(size_t nq) {
         ensure_err();
-        if (grid > pr_grid_cap) {
-            pr_dc.alloc(grid * kMaxK * 4);
-            pr_key.alloc(grid * kMaxK * 4);
-            pr_grid_cap = grid;
-        }
-        if (!pr_counters.p) {
-            pr_counters.alloc(8);
-            E8QC_CUDA(cudaMemset(pr_counters.p, 0, 8));
-            pr_stats.alloc(16);
-        }
+        if (!pr_stats.p) pr_stats.alloc(16);
         if (nq > pr_thr_cap) {
             pr_thr.alloc(nq * 4);
             pr_thr_cap = nq;

@@ -57,14 +57,16 @@ extern "C" {
 /* PRUNED is the reference's production search (E8qIndex::Search with its
  * coarse gate, src/index/e8q_search.cpp:215-293): a coarse pass prices one
  * rowA byte per 8-dim block against the query's u8 LUT (PrepareQuery), the
- * zero-parallel-residual bound of the scan banks rejects vectors that cannot
- * beat the threshold, and the survivors are scored exactly. The threshold is
- * the k-th exact distance among the query's k best coarse estimates (fixed
- * per query rather than the reference's running heap); the bound, its LUT and
- * banks and prune_alpha are the reference's. With set_disable_prune every
+ * zero-parallel-residual bound of the scan banks rejects vectors (and whole
+ * 32-row batches) that cannot beat the running heap's k-th distance, and the
+ * survivors are staged 32 at a time and scored exactly. One warp per query
+ * takes these decisions in the reference's order against the same heap, so
+ * the survivors and results are the reference's; the bound, its LUT and
+ * banks and prune_alpha are the reference's. Throughput comes from the batch
+ * (one query alone is one warp's work). With set_disable_prune every
  * candidate is scored (the reference's plain scan). stats: candidates scanned
  * and survivors refined. On an ME8Q index (e8qc_me8q_search_mode) the mode
- * replays the reference's FastScan cascade in its own order instead. */
+ * replays the reference's FastScan cascade the same way. */
 #define E8QC_MODE_PRUNED 3
 
 /* Maximum top-k (include/e8qlib/index/e8q.hpp:44 kMaxK). */
@@ -90,11 +92,10 @@ typedef struct e8qc_stats {
    changes or the index is rebuilt); its stats carry the graph's kernel count
    and its whole device time, staging copies included, as scan_us. */
 
-/* The pruning threshold of each query of the last E8QC_MODE_PRUNED search on
- * this index (its first nq queries; +inf where pruning was off or fewer than
- * k candidates existed): the k-th exact distance among the query's k best
- * coarse estimates. No reference counterpart (the reference's threshold is
- * its running heap); for checking the bound. */
+/* The final pruning threshold of each query of the last E8QC_MODE_PRUNED
+ * search on this index (its first nq queries): the running heap's k-th
+ * distance at the end, +inf where fewer than k candidates survived. No
+ * reference counterpart; for checking the bound. */
 int e8qc_e8q_pruned_thresholds(e8qc_index* idx, float* out, size_t nq);
 
 typedef struct e8qc_info {
