@@ -353,10 +353,27 @@ void pruned_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size
     pw.w_cls1 = w_cls[1];
     pw.disable_prune = x->disable_prune ? 1 : 0;
     E8QC_CUDA(cudaMemsetAsync(ws.pr_stats.p, 0, 16, s));
-    launches += static_cast<uint64_t>(launch_pruned_batch(
-        x->view, rq_all, ws.b_probes.as<uint32_t>(), ws.b_pd2.as<float>(), static_cast<int>(nq),
-        static_cast<int>(nprobe), static_cast<int>(k), pw, ws.f_lut.as<uint8_t>(), ws.f_qrun.as<float>(), ids_d, d_d,
-        s));
+    // the probed rows' coarse values are kept per group of queries, within a
+    // 2 GB budget
+    PrunedScratch sc{};
+    sc.max_tiles = std::max<size_t>(1, max_tiles_for(x, nprobe));
+    const size_t per_q = sc.max_tiles * 32 * 12;
+    sc.group = static_cast<int>(std::max<size_t>(1, std::min<size_t>(nq, (size_t{2} << 30) / per_q)));
+    ws.p2_toff.ensure(static_cast<size_t>(sc.group) * (nprobe + 1) * 4);
+    ws.p2_acc.ensure(static_cast<size_t>(sc.group) * sc.max_tiles * 32 * 4);
+    ws.p2_P.ensure(static_cast<size_t>(sc.group) * sc.max_tiles * 32 * 4);
+    ws.p2_perp.ensure(static_cast<size_t>(sc.group) * sc.max_tiles * 32 * 4);
+    sc.lut8 = ws.f_lut.as<uint8_t>();
+    sc.scal = ws.f_qrun.as<float>();
+    sc.toff = ws.p2_toff.as<uint32_t>();
+    sc.c_acc = ws.p2_acc.as<int>();
+    sc.c_P = ws.p2_P.as<float>();
+    sc.c_perp = ws.p2_perp.as<float>();
+    sc.out_ids = ids_d;
+    sc.out_d = d_d;
+    launches += static_cast<uint64_t>(launch_pruned_batch(x->view, rq_all, ws.b_probes.as<uint32_t>(),
+                                                          ws.b_pd2.as<float>(), static_cast<int>(nq),
+                                                          static_cast<int>(nprobe), static_cast<int>(k), pw, sc, s));
     ws.pr_last_nq = nq;
     if (st) {
         unsigned long long cs[2] = {0, 0};

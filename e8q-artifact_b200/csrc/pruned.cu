@@ -217,6 +217,75 @@ __global__ void pruned_lut_kernel(const float* __restrict__ rq, int pd, int B, i
     }
 }
 
+// Per query (one warp): exclusive prefix over its probes (in the route's list
+// order) of their tile counts: toff[qi][p], toff[qi][np] = the query's tiles.
+__global__ void pruned_toff_kernel(const DevIndex ix, const uint32_t* __restrict__ probes, int q0, int nqg, int np,
+                                   uint32_t* __restrict__ toff) {
+    const int lane = threadIdx.x & 31;
+    const int qi = static_cast<int>((static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    if (qi >= nqg) return;
+    const uint32_t* pr = probes + static_cast<size_t>(q0 + qi) * np;
+    uint32_t* out = toff + static_cast<size_t>(qi) * (np + 1);
+    uint32_t run = 0;
+    for (int p0 = 0; p0 < np; p0 += 32) {
+        const int p = p0 + lane;
+        const uint32_t t = p < np ? (ix.list_len[pr[p]] + 31u) / 32u : 0u;
+        uint32_t inc = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(kFull, inc, o);
+            if (lane >= o) inc += v;
+        }
+        if (p < np) out[p] = run + inc - t;
+        run += __shfl_sync(kFull, inc, 31);
+    }
+    if (lane == 0) out[np] = run;
+}
+
+// The heap-independent half of every tile a query probes, at full
+// parallelism: one warp per (query, tile), lane = row: the u8 LUT sum and the
+// bound terms P and Omega (coarse_lane) into [qi][tile][lane] arrays.
+__global__ void __launch_bounds__(256) pruned_coarse_kernel(
+    const DevIndex ix, const uint8_t* __restrict__ lut8, const float* __restrict__ scal_all,
+    const uint32_t* __restrict__ probes, const float* __restrict__ pd2, const uint32_t* __restrict__ toff, int q0,
+    int np, size_t max_tiles, PrunedWork pw, int* __restrict__ c_acc, float* __restrict__ c_P,
+    float* __restrict__ c_perp) {
+    extern __shared__ __align__(16) unsigned char lsm[];
+    const int qi = blockIdx.y, q = q0 + qi;
+    const int B = ix.B;
+    const uint32_t* to = toff + static_cast<size_t>(qi) * (np + 1);
+    const uint32_t T = to[np];
+    const uint32_t t0 = blockIdx.x * 8u;
+    if (t0 >= T) return;  // CTA-uniform, before any barrier
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(lut8 + static_cast<size_t>(q) * B * 32);
+        uint4* dst = reinterpret_cast<uint4*>(lsm);
+        for (int e = threadIdx.x; e < B * 2; e += blockDim.x) dst[e] = src[e];
+    }
+    float scal[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) scal[i] = scal_all[static_cast<size_t>(q) * 4 + i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint32_t t = t0 + (threadIdx.x >> 5);
+    if (t >= T) return;
+    int lo = 0, hi = np;  // the probe whose tiles hold t: to[lo] <= t < to[lo + 1]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (to[mid] <= t) lo = mid;
+        else hi = mid;
+    }
+    const uint32_t L = probes[static_cast<size_t>(q) * np + lo];
+    const float d2 = pd2[static_cast<size_t>(q) * np + lo];
+    const uint32_t gt = ix.tile_begin[L] + (t - to[lo]);
+    const Coarse cr = coarse_lane(pw.rowa + static_cast<size_t>(gt) * pw.nrc * 32, pw.nrc, B, lsm,
+                                  pw.banks + static_cast<size_t>(gt) * 128, d2, scal);
+    const size_t o = (static_cast<size_t>(qi) * max_tiles + t) * 32 + lane;
+    c_acc[o] = cr.acc;
+    c_P[o] = cr.P;
+    c_perp[o] = cr.perp;
+}
+
 // Per-warp shared memory of the cascade kernel: the query in padded units,
 // its u8 LUT, the staged rows (slot, g1, d2 + h3) and their distances.
 template <int BITS>
@@ -241,9 +310,10 @@ __host__ __device__ inline size_t cascade_warp_bytes(int pd, int B) {
 template <int BITS>
 __global__ void __launch_bounds__(kCWarps * 32, 1) pruned_cascade_kernel(
     DevIndex ix, const float* __restrict__ rq_all, const uint8_t* __restrict__ lut8, const float* __restrict__ scal_all,
-    const uint32_t* __restrict__ probes, const float* __restrict__ pd2, int nq, int np, int k, PrunedWork pw,
-    uint32_t* __restrict__ out_ids, float* __restrict__ out_d, float* __restrict__ thr_out,
-    unsigned long long* __restrict__ stats) {
+    const uint32_t* __restrict__ probes, const float* __restrict__ pd2, int q0, int nqg, int np, int k, PrunedWork pw,
+    const uint32_t* __restrict__ toff, size_t max_tiles, const int* __restrict__ c_acc, const float* __restrict__ c_P,
+    const float* __restrict__ c_perp, uint32_t* __restrict__ out_ids, float* __restrict__ out_d,
+    float* __restrict__ thr_out, unsigned long long* __restrict__ stats) {
     using G = StepGeo<BITS>;
     constexpr int Q = 1 << BITS, REP = table_rep(BITS), SBLK = G::SBLK, QS = qstep_floats<BITS>();
     extern __shared__ __align__(128) unsigned char smem[];
@@ -255,8 +325,10 @@ __global__ void __launch_bounds__(kCWarps * 32, 1) pruned_cascade_kernel(
     float* tabrep = reinterpret_cast<float*>(smem);  // 2*Q*REP, the CTA's
     for (int e = tid; e < 2 * Q * REP; e += blockDim.x) tabrep[e] = ix.tab[e / REP];
     __syncthreads();
-    const int q = blockIdx.x * kCWarps + warp;
-    if (q >= nq) return;  // warp-uniform; no block barrier follows
+    const int qi = blockIdx.x * kCWarps + warp;
+    if (qi >= nqg) return;  // warp-uniform; no block barrier follows
+    const int q = q0 + qi;
+    const uint32_t* to = toff + static_cast<size_t>(qi) * (np + 1);
     unsigned char* wb = smem + static_cast<size_t>(2 * Q * REP) * 4 +
                         static_cast<size_t>(warp) * cascade_warp_bytes<BITS>(ix.pd, B);
     float* sq = reinterpret_cast<float*>(wb);                                        // nunits*QS
@@ -270,11 +342,8 @@ __global__ void __launch_bounds__(kCWarps * 32, 1) pruned_cascade_kernel(
         const int u = i / (SBLK * 8), r = i - u * (SBLK * 8);
         sq[u * QS + r] = rq[i];
     }
-    {
-        const uint4* src = reinterpret_cast<const uint4*>(lut8 + static_cast<size_t>(q) * B * 32);
-        uint4* dst = reinterpret_cast<uint4*>(lut);
-        for (int e = lane; e < B * 2; e += 32) dst[e] = src[e];
-    }
+    (void)lut;
+    (void)lut8;
     float scal[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) scal[i] = scal_all[static_cast<size_t>(q) * 4 + i];
@@ -322,13 +391,34 @@ __global__ void __launch_bounds__(kCWarps * 32, 1) pruned_cascade_kernel(
         const float d2 = __uint_as_float(static_cast<uint32_t>(best >> 32));
         const uint32_t len = ix.list_len[L], tile0 = ix.tile_begin[L];
         if (len == 0) continue;
+        // this probe's position in the route's list order: its tiles' offset
+        int pp = 0;
+        {
+            unsigned found = 0u;
+            for (int p0 = 0; p0 < np && found == 0u; p0 += 32) {
+                found = __ballot_sync(kFull, p0 + lane < np && pr[p0 + lane] == L);
+                if (found) pp = p0 + __ffs(found) - 1;
+            }
+        }
+        const uint32_t tb0 = to[pp];
         const float sqrt_d2 = __fsqrt_rn(d2 > 0.0f ? d2 : 0.0f);
+        const size_t cbase = (static_cast<size_t>(qi) * max_tiles + tb0) * 32 + lane;
+        int nx_acc = c_acc[cbase];
+        float nx_P = c_P[cbase], nx_perp = c_perp[cbase];
         for (uint32_t i0 = 0; i0 < len; i0 += 32) {
             const uint32_t n_logic = min(32u, len - i0);
             const uint32_t gt = tile0 + (i0 >> 5);
             const uint8_t* hdr = pw.banks + static_cast<size_t>(gt) * 128;
-            const Coarse cr = coarse_lane(pw.rowa + static_cast<size_t>(gt) * pw.nrc * 32, pw.nrc, B, lut, hdr, d2,
-                                          scal);
+            Coarse cr;
+            cr.acc = nx_acc;
+            cr.P = nx_P;
+            cr.perp = nx_perp;
+            if (i0 + 32 < len) {  // the next tile's values stream in while this one is decided
+                const size_t o = cbase + static_cast<size_t>((i0 >> 5) + 1) * 32;
+                nx_acc = c_acc[o];
+                nx_P = c_P[o];
+                nx_perp = c_perp[o];
+            }
             n_cand += n_logic;
             const float distk0 = top.thr_d;
             const float r_h = distk0 < d2 ? __fsqrt_rn(distk0 > 0.0f ? distk0 : 0.0f) : sqrt_d2;
@@ -390,12 +480,13 @@ __global__ void __launch_bounds__(kCWarps * 32, 1) pruned_cascade_kernel(
 }  // namespace
 
 int launch_pruned_batch(const DevIndex& ix, const float* rq, const uint32_t* probes, const float* pd2, int nq, int np,
-                        int k, const PrunedWork& pw, uint8_t* lut8, float* scal, uint32_t* out_ids, float* out_d,
-                        cudaStream_t s) {
+                        int k, const PrunedWork& pw, const PrunedScratch& sc, cudaStream_t s) {
     if (nq == 0) return 0;
-    pruned_lut_kernel<<<static_cast<unsigned>(nq), 256, 0, s>>>(rq, ix.pd, ix.B, ix.bits, pw.w_cls0, pw.w_cls1, lut8,
-                                                               scal);
+    int launches = 0;
+    pruned_lut_kernel<<<static_cast<unsigned>(nq), 256, 0, s>>>(rq, ix.pd, ix.B, ix.bits, pw.w_cls0, pw.w_cls1,
+                                                               sc.lut8, sc.scal);
     E8QC_CUDA(cudaGetLastError());
+    ++launches;
     int dev = 0;
     E8QC_CUDA(cudaGetDevice(&dev));
     const void* fn = nullptr;
@@ -413,28 +504,46 @@ int launch_pruned_batch(const DevIndex& ix, const float* rq, const uint32_t* pro
         default: fail(E8QC_EINVAL, "bits out of range");
     }
     if (smem > 227 * 1024) fail(E8QC_EINVAL, "the pruned search does not fit this device (padded_dim too large)");
+    const size_t lsm = static_cast<size_t>(ix.B) * 32;
     {
         static size_t configured[64][14] = {};
         if (configured[dev & 63][ix.bits] < smem) {
             E8QC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
             configured[dev & 63][ix.bits] = smem;
         }
+        static size_t conf_l[64] = {};
+        if (lsm > 48 * 1024 && conf_l[dev & 63] < lsm) {
+            E8QC_CUDA(cudaFuncSetAttribute(pruned_coarse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(lsm)));
+            conf_l[dev & 63] = lsm;
+        }
     }
-    const unsigned grid = static_cast<unsigned>((nq + kCWarps - 1) / kCWarps);
-    switch (ix.bits) {
-#define E8QC_CASE(b)                                                                                       \
-    case b:                                                                                                \
-        pruned_cascade_kernel<b><<<grid, kCWarps * 32, smem, s>>>(ix, rq, lut8, scal, probes, pd2, nq, np, k, pw, \
-                                                                  out_ids, out_d, pw.thr, pw.stats);      \
+    for (int q0 = 0; q0 < nq; q0 += sc.group) {
+        const int g = nq - q0 < sc.group ? nq - q0 : sc.group;
+        pruned_toff_kernel<<<static_cast<unsigned>((g + 7) / 8), 256, 0, s>>>(ix, probes, q0, g, np, sc.toff);
+        E8QC_CUDA(cudaGetLastError());
+        dim3 cg(static_cast<unsigned>((sc.max_tiles + 7) / 8), static_cast<unsigned>(g));
+        pruned_coarse_kernel<<<cg, 256, lsm, s>>>(ix, sc.lut8, sc.scal, probes, pd2, sc.toff, q0, np, sc.max_tiles, pw,
+                                                  sc.c_acc, sc.c_P, sc.c_perp);
+        E8QC_CUDA(cudaGetLastError());
+        const unsigned grid = static_cast<unsigned>((g + kCWarps - 1) / kCWarps);
+        switch (ix.bits) {
+#define E8QC_CASE(b)                                                                                        \
+    case b:                                                                                                 \
+        pruned_cascade_kernel<b><<<grid, kCWarps * 32, smem, s>>>(ix, rq, sc.lut8, sc.scal, probes, pd2, q0, g, np, k, \
+                                                                  pw, sc.toff, sc.max_tiles, sc.c_acc, sc.c_P,   \
+                                                                  sc.c_perp, sc.out_ids, sc.out_d, pw.thr, pw.stats); \
         break;
-        E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
-        E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
-        E8QC_CASE(13)
+            E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
+            E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
+            E8QC_CASE(13)
 #undef E8QC_CASE
-        default: break;
+            default: break;
+        }
+        E8QC_CUDA(cudaGetLastError());
+        launches += 3;
     }
-    E8QC_CUDA(cudaGetLastError());
-    return 2;
+    return launches;
 }
 
 namespace {

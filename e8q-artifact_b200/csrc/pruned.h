@@ -27,14 +27,32 @@ struct PrunedWork {
     int disable_prune;           // 1: every candidate is refined (the reference's set_disable_prune)
 };
 
+// Scratch of the batched form: per-query u8 LUTs (lut8: nq*B*32 bytes) and
+// scalars (scal: nq*4); per group of `group` queries the tile offsets (toff:
+// group*(np+1)) and every probed row's LUT sum and bound terms (c_acc, c_P,
+// c_perp: group*max_tiles*32 each, max_tiles = the most tiles a query's
+// probes can hold); out rows of k.
+struct PrunedScratch {
+    uint8_t* lut8;
+    float* scal;
+    uint32_t* toff;
+    int* c_acc;
+    float* c_P;
+    float* c_perp;
+    size_t max_tiles;
+    int group;
+    uint32_t* out_ids;
+    float* out_d;
+};
+
 // Batched form (nq queries, probes / pd2: nq x np from the batched route):
-// per-query u8 LUTs (lut8: nq*B*32 bytes, scal: nq*4 floats, scratch), then
-// one warp per query scanning in the reference's order with its running
-// heap; out rows of k; pw.thr (if set) gets each query's final k-th distance
-// and pw.stats the candidate / survivor counts.
+// the LUTs, then per group of queries the tile offsets, the heap-independent
+// coarse values of every probed row at full parallelism, and one warp per
+// query taking the reference's decisions in its order with its running heap
+// from them; pw.thr (if set) gets each query's final k-th distance and
+// pw.stats the candidate / survivor counts.
 int launch_pruned_batch(const DevIndex& ix, const float* rq, const uint32_t* probes, const float* pd2, int nq, int np,
-                        int k, const PrunedWork& pw, uint8_t* lut8, float* scal, uint32_t* out_ids, float* out_d,
-                        cudaStream_t s);
+                        int k, const PrunedWork& pw, const PrunedScratch& sc, cudaStream_t s);
 // The coarse plane of every tile from the codes (rowA byte of block b = the
 // top bit of each stored digit field, digit i at bit 7 - i).
 int launch_build_rowa(const DevIndex& ix, int ntiles, uint4* rowa, cudaStream_t s);

@@ -67,13 +67,14 @@ struct Workspace {
     // tensor-core routing: int8 slice planes and per-row scale / norms of the
     // queries and the centroids
     DevBuf r_qplane, r_cplane, r_qmeta, r_cmeta, r_ub;
-    // pruned path: per-CTA best coarse estimates and keys, the grid-barrier
-    // and finish counters, candidate/survivor counts, per-query thresholds
-    DevBuf pr_dc, pr_key, pr_counters, pr_stats, pr_thr;
-    // ME8Q pruned path: per-query u8 LUTs, per-run scalars, LUT steps,
-    // thresholds, and the candidate / survivor counts
+    // pruned path: candidate/survivor counts, per-query final k-th distances,
+    // and per group of queries the tile offsets and the probed rows' coarse
+    // values (LUT sum, bound terms)
+    DevBuf pr_stats, pr_thr, p2_toff, p2_acc, p2_P, p2_perp;
+    size_t pr_thr_cap = 0, pr_last_nq = 0;
+    // pruned paths' per-query u8 LUTs and scalars (both indexes), and the
+    // ME8Q path's LUT steps, thresholds and candidate / survivor counts
     DevBuf f_lut, f_qrun, f_delta, f_thr, f_counts;
-    size_t pr_grid_cap = 0, pr_thr_cap = 0, pr_last_nq = 0;
     // tuning of the grouped paths (chosen by the autotuner): work-queue order
     // (0: longest list first, 1: list id order) and the precision scan's
     // shared-memory ring depth (4, 6 or 8 K-chunk stages)
