@@ -353,12 +353,15 @@ void pruned_search(e8qc_index* x, const float* rq_all, size_t nq, size_t k, size
     pw.w_cls1 = w_cls[1];
     pw.disable_prune = x->disable_prune ? 1 : 0;
     E8QC_CUDA(cudaMemsetAsync(ws.pr_stats.p, 0, 16, s));
-    // the probed rows' coarse values are kept per group of queries, within a
-    // 2 GB budget
+    // the probed rows' coarse values are kept per group of queries, within
+    // min(8 GB, a quarter of the free device memory)
     PrunedScratch sc{};
     sc.max_tiles = std::max<size_t>(1, max_tiles_for(x, nprobe));
     const size_t per_q = sc.max_tiles * 32 * 12;
-    sc.group = static_cast<int>(std::max<size_t>(1, std::min<size_t>(nq, (size_t{2} << 30) / per_q)));
+    size_t free_b = 0, total_b = 0;
+    E8QC_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t budget = std::min<size_t>(size_t{8} << 30, free_b / 4);
+    sc.group = static_cast<int>(std::max<size_t>(1, std::min<size_t>(nq, budget / per_q)));
     ws.p2_toff.ensure(static_cast<size_t>(sc.group) * (nprobe + 1) * 4);
     ws.p2_acc.ensure(static_cast<size_t>(sc.group) * sc.max_tiles * 32 * 4);
     ws.p2_P.ensure(static_cast<size_t>(sc.group) * sc.max_tiles * 32 * 4);
