@@ -287,14 +287,12 @@ __global__ void __launch_bounds__(256) pruned_coarse_kernel(
 }
 
 // Per-warp shared memory of the cascade kernel: the query in padded units,
-// its u8 LUT, the staged rows (slot, g1, d2 + h3) and their distances.
+// the staged rows (slot, g1, d2 + h3) and their distances.
 template <int BITS>
-__host__ __device__ inline size_t cascade_warp_bytes(int pd, int B) {
+__host__ __device__ inline size_t cascade_warp_bytes(int B) {
     using G = StepGeo<BITS>;
     const int nunits = B / G::SBLK + ((B % G::SBLK) != 0 ? 1 : 0);
-    const size_t b = static_cast<size_t>(nunits) * qstep_floats<BITS>() * 4 + ((static_cast<size_t>(B) * 32 + 15) & ~static_cast<size_t>(15)) +
-                     32 * 16;
-    (void)pd;
+    const size_t b = static_cast<size_t>(nunits) * qstep_floats<BITS>() * 4 + 32 * 16;
     return (b + 15) / 16 * 16;
 }
 
@@ -308,7 +306,7 @@ __host__ __device__ inline size_t cascade_warp_bytes(int pd, int B) {
 // taken again after each one. The heap is the warp's top-k in the (distance,
 // id) order, the reference heap's order.
 template <int BITS>
-__global__ void __launch_bounds__(kCWarps * 32, 1) pruned_cascade_kernel(
+__global__ void __launch_bounds__(kCWarps * 32, 2) pruned_cascade_kernel(
     DevIndex ix, const float* __restrict__ rq_all, const uint8_t* __restrict__ lut8, const float* __restrict__ scal_all,
     const uint32_t* __restrict__ probes, const float* __restrict__ pd2, int q0, int nqg, int np, int k, PrunedWork pw,
     const uint32_t* __restrict__ toff, size_t max_tiles, const int* __restrict__ c_acc, const float* __restrict__ c_P,
@@ -330,10 +328,9 @@ __global__ void __launch_bounds__(kCWarps * 32, 1) pruned_cascade_kernel(
     const int q = q0 + qi;
     const uint32_t* to = toff + static_cast<size_t>(qi) * (np + 1);
     unsigned char* wb = smem + static_cast<size_t>(2 * Q * REP) * 4 +
-                        static_cast<size_t>(warp) * cascade_warp_bytes<BITS>(ix.pd, B);
+                        static_cast<size_t>(warp) * cascade_warp_bytes<BITS>(B);
     float* sq = reinterpret_cast<float*>(wb);                                        // nunits*QS
-    uint8_t* lut = reinterpret_cast<uint8_t*>(sq + nunits * QS);                     // B*32
-    uint32_t* st_slot = reinterpret_cast<uint32_t*>(lut + ((B * 32 + 15) & ~15));   // 32
+    uint32_t* st_slot = reinterpret_cast<uint32_t*>(sq + nunits * QS);               // 32
     float* st_g1 = reinterpret_cast<float*>(st_slot + 32);                           // 32
     float* st_h3 = st_g1 + 32;                                                       // 32
     float* st_d = st_h3 + 32;                                                        // 32
@@ -342,8 +339,7 @@ __global__ void __launch_bounds__(kCWarps * 32, 1) pruned_cascade_kernel(
         const int u = i / (SBLK * 8), r = i - u * (SBLK * 8);
         sq[u * QS + r] = rq[i];
     }
-    (void)lut;
-    (void)lut8;
+    (void)lut8;  // the LUT was applied by pruned_coarse_kernel
     float scal[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) scal[i] = scal_all[static_cast<size_t>(q) * 4 + i];
@@ -495,7 +491,7 @@ int launch_pruned_batch(const DevIndex& ix, const float* rq, const uint32_t* pro
 #define E8QC_CASE(b)                                                                                         \
     case b:                                                                                                  \
         fn = reinterpret_cast<const void*>(pruned_cascade_kernel<b>);                                        \
-        smem = static_cast<size_t>(2 * (1 << b) * table_rep(b)) * 4 + kCWarps * cascade_warp_bytes<b>(ix.pd, ix.B); \
+        smem = static_cast<size_t>(2 * (1 << b) * table_rep(b)) * 4 + kCWarps * cascade_warp_bytes<b>(ix.B); \
         break;
         E8QC_CASE(1) E8QC_CASE(2) E8QC_CASE(3) E8QC_CASE(4) E8QC_CASE(5) E8QC_CASE(6)
         E8QC_CASE(7) E8QC_CASE(8) E8QC_CASE(9) E8QC_CASE(10) E8QC_CASE(11) E8QC_CASE(12)
