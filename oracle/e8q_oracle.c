@@ -1298,162 +1298,6 @@ void orc_e8q_search_pruned(const orc_e8q_index* x, const uint8_t* banks_in, floa
     free(own);
 }
 
-typedef struct {
-    float dc, P, perp, d2;
-    uint32_t key;
-    size_t pos;
-} orc_cand;
-
-static int better_key(float d1, uint32_t k1, float d2, uint32_t k2) {
-    return d1 < d2 || (d1 == d2 && k1 < k2);
-}
-
-void orc_e8q_search_pruned_at(const orc_e8q_index* x, const uint8_t* banks_in, float alpha,
-                              int disable_prune, const float* queries, size_t nq, size_t k,
-                              size_t nprobe, const float* thr, uint32_t* out_ids, float* out_dists,
-                              uint64_t* cand_out, uint64_t* surv_out, int threads) {
-    const size_t nbatches = orc_e8q_banks(x, NULL);
-    uint8_t* own = NULL;
-    const uint8_t* banks = banks_in;
-    if (!banks) {
-        own = (uint8_t*)malloc(nbatches * 128 + 1);
-        orc_e8q_banks(x, own);
-        banks = own;
-    }
-    size_t* bfirst = (size_t*)malloc(sizeof(size_t) * (x->nlist + 1));
-    bfirst[0] = 0;
-    for (size_t c = 0; c < x->nlist; ++c)
-        bfirst[c + 1] = bfirst[c] + (size_t)((x->list_begin[c + 1] - x->list_begin[c] + 31) / 32);
-    const size_t k_eff = 4 * k > 32 ? 4 * k : 32;
-    const float z = orc_ortho_quantile((double)alpha, k_eff);
-    const size_t nseed = k_eff < 128 ? k_eff : (k > 128 ? k : 128);
-    const int B = x->blocks;
-#pragma omp parallel num_threads(threads > 0 ? threads : 1)
-    {
-        float* rq = (float*)malloc(sizeof(float) * x->padded_dim);
-        uint32_t* probes = (uint32_t*)malloc(sizeof(uint32_t) * x->nlist);
-        float* pd2 = (float*)malloc(sizeof(float) * x->nlist);
-        uint8_t* lut = (uint8_t*)malloc((size_t)B * 32);
-        orc_cand* cs = (orc_cand*)malloc(sizeof(orc_cand) * (x->n + 1));
-        size_t* seed = (size_t*)malloc(sizeof(size_t) * (nseed + 1));
-        float* res_d = (float*)malloc(sizeof(float) * (x->n + nseed + 1));
-        uint32_t* res_i = (uint32_t*)malloc(sizeof(uint32_t) * (x->n + nseed + 1));
-        char* is_seed = (char*)malloc(x->n + 1);
-#pragma omp for schedule(dynamic, 1)
-        for (long long qi = 0; qi < (long long)nq; ++qi) {
-            float scal[4];
-            orc_e8q_prepare_query(x, queries + (size_t)qi * x->dim, rq);
-            orc_e8q_prepare_lut(x->bits, B, rq, lut, scal);
-            const float delta_c = scal[0], base_c = scal[1], lut_err = scal[2], score_max = scal[3];
-            const size_t take = nprobe < x->nlist ? nprobe : x->nlist;
-            orc_e8q_route(x, rq, take, probes, pd2);
-            size_t nc = 0;
-            uint32_t tile = 0;
-            for (size_t p = 0; p < take; ++p) {
-                const size_t c = probes[p];
-                const float d2 = pd2[p];
-                const uint64_t lo = x->list_begin[c], cnt = x->list_begin[c + 1] - lo;
-                for (uint64_t off = 0; off < cnt; off += 32, ++tile) {
-                    const uint8_t* bp = banks + (bfirst[c] + (size_t)(off / 32)) * 128;
-                    float sc[7];
-                    memcpy(sc, bp + 96, sizeof(sc));
-                    const float pad_w_round = 0.5F * sc[3] * (score_max + lut_err);
-                    const float bmin_d2 = (sc[0] + d2) - pad_w_round;
-                    const size_t n_logic = (size_t)(cnt - off < 32 ? cnt - off : 32);
-                    for (size_t t = 0; t < n_logic; ++t) {
-                        const size_t pos = (size_t)(lo + off + t);
-                        const int32_t acc = orc_e8q_coarse(x, pos, lut);
-                        const float scv = fmaf((float)acc, delta_c, base_c);
-                        const float base_term = fmaf((float)bp[t], sc[1], bmin_d2);
-                        const float weight = fmaf((float)bp[32 + t], sc[3], sc[2]);
-                        orc_cand* e = &cs[nc++];
-                        e->perp = fmaf((float)bp[64 + t], sc[5], sc[4]);
-                        e->dc = fmaf(-weight, scv, base_term);
-                        e->P = fmaf(-fabsf(weight), lut_err, e->dc);
-                        e->d2 = d2;
-                        e->key = tile * 32u + (uint32_t)t;
-                        e->pos = pos;
-                    }
-                }
-            }
-            /* seeds: the nseed best (dc, key) */
-            size_t ns = 0;
-            for (size_t i = 0; i < nc; ++i) is_seed[i] = 0;
-            for (size_t s = 0; s < nseed && s < nc; ++s) {
-                size_t bi = (size_t)-1;
-                for (size_t i = 0; i < nc; ++i) {
-                    if (is_seed[i]) continue;
-                    if (bi == (size_t)-1 || better_key(cs[i].dc, cs[i].key, cs[bi].dc, cs[bi].key)) bi = i;
-                }
-                is_seed[bi] = 1;
-                seed[ns++] = bi;
-            }
-            size_t nr = 0;
-            for (size_t s = 0; s < ns; ++s) {
-                const orc_cand* e = &cs[seed[s]];
-                const float S = orc_e8q_refine_score(x, e->pos, rq);
-                res_d[nr] = fmaf(-(2.0F * x->g1[e->pos]), S, e->d2 + x->h3[e->pos]);
-                res_i[nr] = x->ids[e->pos];
-                ++nr;
-            }
-            /* T = the k-th best seed distance */
-            float T = INFINITY;
-            if (ns >= k && !disable_prune) {
-                float* tmp_d = (float*)malloc(sizeof(float) * ns);
-                uint32_t* tmp_i = (uint32_t*)malloc(sizeof(uint32_t) * ns);
-                memcpy(tmp_d, res_d, sizeof(float) * ns);
-                memcpy(tmp_i, res_i, sizeof(uint32_t) * ns);
-                for (size_t j = 0; j < k; ++j) {
-                    size_t bi = j;
-                    for (size_t t = j + 1; t < ns; ++t)
-                        if (better(tmp_d[t], tmp_i[t], tmp_d[bi], tmp_i[bi])) bi = t;
-                    float td = tmp_d[j]; tmp_d[j] = tmp_d[bi]; tmp_d[bi] = td;
-                    uint32_t ti = tmp_i[j]; tmp_i[j] = tmp_i[bi]; tmp_i[bi] = ti;
-                }
-                T = tmp_d[k - 1];
-                free(tmp_d);
-                free(tmp_i);
-            }
-            if (thr) T = thr[qi];
-            uint64_t surv = 0;
-            for (size_t i = 0; i < nc; ++i) {
-                if (is_seed[i]) continue;
-                const orc_cand* e = &cs[i];
-                const float rh = (T < e->d2) ? sqrtf(T > 0.0F ? T : 0.0F) : sqrtf(e->d2 > 0.0F ? e->d2 : 0.0F);
-                const float dlo = fmaf(-(z * rh), e->perp, e->P);
-                if (!(dlo < T)) continue;
-                ++surv;
-                const float S = orc_e8q_refine_score(x, e->pos, rq);
-                res_d[nr] = fmaf(-(2.0F * x->g1[e->pos]), S, e->d2 + x->h3[e->pos]);
-                res_i[nr] = x->ids[e->pos];
-                ++nr;
-            }
-            /* best k of seeds and survivors */
-            uint32_t* oid = out_ids + (size_t)qi * k;
-            float* od = out_dists + (size_t)qi * k;
-            for (size_t j = 0; j < k; ++j) {
-                if (j < nr) {
-                    size_t bi = j;
-                    for (size_t t = j + 1; t < nr; ++t)
-                        if (better(res_d[t], res_i[t], res_d[bi], res_i[bi])) bi = t;
-                    float td = res_d[j]; res_d[j] = res_d[bi]; res_d[bi] = td;
-                    uint32_t ti = res_i[j]; res_i[j] = res_i[bi]; res_i[bi] = ti;
-                    oid[j] = res_i[j];
-                    od[j] = res_d[j];
-                } else {
-                    oid[j] = 0xFFFFFFFFu;
-                    od[j] = INFINITY;
-                }
-            }
-            if (cand_out) cand_out[qi] = nc;
-            if (surv_out) surv_out[qi] = surv;
-        }
-        free(rq); free(probes); free(pd2); free(lut); free(cs); free(seed); free(res_d); free(res_i);
-        free(is_seed);
-    }
-    free(bfirst);
-    free(own);
-}
 
 /* ProbeBoundW: src/index/e8q_oracle.cpp:103-218. Query and base row are
  * rotated and centred like the build's rows; the exact reconstruction uses

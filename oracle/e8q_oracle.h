@@ -135,18 +135,6 @@ void orc_e8q_search_pruned(const orc_e8q_index* idx, const uint8_t* banks, float
                            size_t nprobe, uint32_t* out_ids, float* out_dists, uint64_t* cand,
                            uint64_t* surv, int threads);
 
-/* The same bound with one threshold per query (the GPU pruned search's
- * semantics): seeds = the min(max(4k, 32), 128) best coarse estimates dc
- * of the query (at least k; ties by probe-space key, tile * 32 + lane with
- * tiles numbered across the probed lists in probe order), scored exactly;
- * T = thr[q] when thr is given, else the k-th best seed distance (+inf with
- * fewer than k candidates or pruning off); survivors = non-seed candidates with dlo(T) < T; the result is the
- * best k of seeds and survivors (exact distances). cand/surv per query. */
-void orc_e8q_search_pruned_at(const orc_e8q_index* idx, const uint8_t* banks, float alpha,
-                              int disable_prune, const float* queries, size_t nq, size_t k,
-                              size_t nprobe, const float* thr, uint32_t* out_ids, float* out_dists,
-                              uint64_t* cand, uint64_t* surv, int threads);
-
 /* ProbeBoundW (src/index/e8q_oracle.cpp:103-218): for the stored vector `id`
  * whose raw build input is base_row, the normalised discrepancy
  * (d_coarse^2 - d^2) / (r_q * Omega) of the zero-parallel-residual bound,

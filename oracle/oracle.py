@@ -87,9 +87,6 @@ def lib() -> C.CDLL:
         L.orc_e8q_search_pruned.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_int, _f32p,
                                             C.c_size_t, C.c_size_t, C.c_size_t, _u32p, _f32p,
                                             C.c_void_p, C.c_void_p, C.c_int]
-        L.orc_e8q_search_pruned_at.argtypes = [C.c_void_p, C.c_void_p, C.c_float, C.c_int, _f32p,
-                                               C.c_size_t, C.c_size_t, C.c_size_t, C.c_void_p, _u32p,
-                                               _f32p, C.c_void_p, C.c_void_p, C.c_int]
         L.orc_me8q_variance.argtypes = [_f32p, C.c_size_t, C.c_size_t, C.c_size_t, _f32p]
         L.orc_me8q_allocate.argtypes = [_f32p, C.c_size_t, C.c_float, C.c_int, C.c_double,
                                         C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
@@ -329,24 +326,6 @@ class OracleE8qIndex:
     def refine_score(self, pos, rot_q):
         return float(lib().orc_e8q_refine_score(self._p, pos, np.ascontiguousarray(rot_q, np.float32)))
 
-    def search_pruned_at(self, queries, k, nprobe, thr=None, alpha=1.0, disable_prune=False, banks=None,
-                         threads=8):
-        """The bound with one threshold per query (thr, else the k-th exact
-        distance of the query's k best coarse estimates): ids, dists and
-        per-query (candidates, survivors)."""
-        queries = np.ascontiguousarray(np.atleast_2d(queries), np.float32)
-        nq = queries.shape[0]
-        ids = np.zeros((nq, k), np.uint32)
-        dists = np.zeros((nq, k), np.float32)
-        cand = np.zeros(nq, np.uint64)
-        surv = np.zeros(nq, np.uint64)
-        th = None if thr is None else np.ascontiguousarray(thr, np.float32)
-        bk = None if banks is None else np.ascontiguousarray(banks, np.uint8)
-        lib().orc_e8q_search_pruned_at(self._p, None if bk is None else bk.ctypes.data, alpha,
-                                       1 if disable_prune else 0, queries, nq, k, nprobe,
-                                       None if th is None else th.ctypes.data, ids, dists,
-                                       cand.ctypes.data, surv.ctypes.data, threads)
-        return ids, dists, cand, surv
 
     def search_pruned(self, queries, k, nprobe, alpha=1.0, disable_prune=False, banks=None, threads=8):
         """The reference's shipped sequential pruned search; returns ids,
