@@ -135,6 +135,8 @@ ME8Q_PRUNED_CASES = [
     ("d96_a6_k20", 96, 6.0, 11, "", 2500, 8, 0.5, 24, 20, 3, 0.0),
     ("d150_a3_a001", 150, 3.0, 0, "", 4000, 10, 0.5, 24, 16, 4, 0.01),
     ("d64_a1", 64, 1.0, 3, "", 2000, 6, 0.5, 16, 10, 3, 0.0),
+    ("d192_k100_np_all", 192, 3.0, 5, "", 3000, 8, 0.5, 12, 100, 20, 0.0),
+    ("d256_spec_r1", 256, 3.0, 9, "64:5,64:1,64:3,64:0", 3500, 10, 0.5, 16, 16, 4, 0.3),
 ]
 
 

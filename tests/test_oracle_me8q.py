@@ -49,7 +49,8 @@ def test_me8q_plan_edges(oracle_lib):
         O.parse_plan_spec("60:3,68:0", 128)
 
 
-PRUNED_CASES = ["d200_a4", "d200_spec", "d96_a6_k20", "d150_a3_a001", "d64_a1"]
+PRUNED_CASES = ["d200_a4", "d200_spec", "d96_a6_k20", "d150_a3_a001", "d64_a1",
+                "d192_k100_np_all", "d256_spec_r1"]
 
 
 @pytest.mark.parametrize("name", PRUNED_CASES)
